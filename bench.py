@@ -1,0 +1,418 @@
+"""Benchmark: 3D Laplace FMM evaluation throughput on one B200 (or N replicas).
+
+Workload (one step = one full FMM evaluation, ``drive_fmm``): 1,000,000
+points that are both sources and targets (exclude_self), 50% on the unit
+sphere surface and 50% Plummer (scale 0.1), strengths N(0, 1), expansion
+order 10, max_particles_in_box 32. Synthetic, seeded inputs; the tree,
+interaction lists and M2L tables are built once before timing (reported
+separately). ``value`` is Mpts/s of the mixed-precision form with inputs
+resident in HBM; the FP64 form is timed the same way for the ratio; the
+accuracy of both is the relative L2 error on 4,096 sampled targets against
+an FP64 direct sum. ``e2e`` runs the public API with host buffers (H2D of the
+strengths, D2H of the potentials inside the timed region).
+
+``--impl reference`` times the FP64 CPU restatement of sumpy's algorithm
+(the oracle, C + OpenMP on all host cores) on a bounded sample of the same
+workload and prints the same metric.
+
+Multi-GPU (torchrun): each rank evaluates its own replica; no collective on
+the data path (the problem does not shard in this build); value = points of
+all ranks / max over ranks of the step time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "3D Laplace FMM Mpts/s @ relL2<=1e-6 (mixed vs FP64 GPU); adjoint/forward ratio"
+NPOINTS = 1_000_000
+ORDER = 10
+MAX_PARTICLES = 32
+NSAMPLE = 4096
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--npoints", type=int, default=NPOINTS)
+    ap.add_argument("--order", type=int, default=ORDER)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip timing the FP64 form")
+    ap.add_argument("--stage-times", action="store_true", help="print per-stage times")
+    return ap.parse_args()
+
+
+def workload(npoints, seed=2024):
+    from tests._pointsets import sphere_plummer
+    pts = sphere_plummer(npoints, seed)
+    q = np.random.default_rng(44).standard_normal(npoints)
+    return pts, q
+
+
+# {{{ reference arm / CPU baseline (oracle)
+
+def cpu_fmm_rate(npoints, order, seed=2024, target_seconds=10.0, min_points=5000):
+    """Time the oracle FMM on a sample sized to take about target_seconds."""
+    from oracle import oracle as O
+    from sumpy_b200.tree import build_all
+    n = max(min_points, min(npoints, 20000))
+    while True:
+        pts, q = workload(n, seed)
+        tree, trav, tcls = build_all(pts, None, MAX_PARTICLES)
+        t0 = time.perf_counter()
+        O.run_fmm(tree, trav, tcls, order, q, exclude_self=True)
+        dt = time.perf_counter() - t0
+        if dt > 0.3 * target_seconds or n >= npoints:
+            return n, dt
+        n = min(npoints, int(n * min(8.0, target_seconds / max(dt, 1e-3))))
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from sumpy_b200.tree import build_all
+    n, _ = cpu_fmm_rate(args.npoints, args.order, target_seconds=4.0)
+    pts, q = workload(n)
+    tree, trav, tcls = build_all(pts, None, MAX_PARTICLES)
+    for _ in range(args.warmup):
+        O.run_fmm(tree, trav, tcls, args.order, q, exclude_self=True)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.run_fmm(tree, trav, tcls, args.order, q, exclude_self=True)
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    value = n * args.steps / tot / 1e6
+    cores = os.cpu_count()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mpts/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"laplace3d_fmm_sphere_plummer_n{args.npoints}_p{args.order}",
+                   "sample_points": n, "order": args.order,
+                   "max_particles_in_box": MAX_PARTICLES, "exclude_self": True},
+        "cpu_baseline": {"value": value, "unit": "Mpts/s", "cores": cores, "kind": "port",
+                         "sample": f"{n}-point sample of the same distribution, p={args.order}, "
+                                   f"FP64 C/OpenMP oracle (sumpy's algorithm restated), "
+                                   f"{cores} threads"},
+        "e2e": {"value": value, "unit": "Mpts/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+# }}}
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        rows = [r.split(",") for r in (self.out or "").strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+
+    from sumpy_b200 import (
+        P2P, LaplaceKernel, SumpyExpansionWrangler, SumpyTreeIndependentDataForWrangler,
+        drive_fmm)
+    from sumpy_b200 import _capi
+    from sumpy_b200.expansion import (
+        LinearPDEConformingVolumeTaylorLocalExpansion as LExp,
+        LinearPDEConformingVolumeTaylorMultipoleExpansion as MExp)
+    from sumpy_b200.tree import build_all
+
+    # cpu baseline first, before any process pool / GPU work competes for the host
+    cpu_line = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        n, dt = cpu_fmm_rate(args.npoints, args.order, target_seconds=12.0)
+        cores = os.cpu_count()
+        cpu_line = {"value": n / dt / 1e6, "unit": "Mpts/s", "cores": cores, "kind": "port",
+                    "sample": f"{n}-point sample of the same distribution, p={args.order}, "
+                              f"FP64 C/OpenMP oracle, {cores} threads, {dt:.1f} s"}
+
+    pts, q = workload(args.npoints)
+    t0 = time.perf_counter()
+    tree, trav, tcls = build_all(pts, None, MAX_PARTICLES)
+    t_tree = time.perf_counter() - t0
+    knl = LaplaceKernel(3)
+    ti = SumpyTreeIndependentDataForWrangler(
+        None, lambda o, **kw: MExp(knl, o), lambda o, **kw: LExp(knl, o), [knl],
+        exclude_self=True)
+
+    def wrangler(precision):
+        return SumpyExpansionWrangler(ti, trav, np.float64, lambda k, a, t, lev: args.order,
+                                      precision=precision, device=dev)
+
+    q_dev = torch.as_tensor(q, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def timed(fn, steps):
+        """Per-step CUDA-event times with an L2 flush between steps."""
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(steps)]
+        torch.cuda.synchronize()
+        barrier()
+        for i in range(steps):
+            flush.fill_(float(i))
+            evs[i][0].record()
+            fn()
+            evs[i][1].record()
+        torch.cuda.synchronize()
+        barrier()
+        ms = [a.elapsed_time(b) for a, b in evs]
+        tot = torch.tensor([sum(ms)], device=dev)
+        if world > 1:
+            dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+        return float(tot.item()) / steps, ms
+
+    # setup (plans, tables) outside timing
+    t0 = time.perf_counter()
+    w_mx = wrangler("mixed")
+    drive_fmm(None, w_mx, [q_dev])
+    torch.cuda.synchronize()
+    t_setup = time.perf_counter() - t0
+
+    for _ in range(args.warmup):
+        drive_fmm(None, w_mx, [q_dev])
+    _capi.launch_counter.reset()
+    with ClockSampler(local_rank) as clk:
+        ms_mx, _ = timed(lambda: drive_fmm(None, w_mx, [q_dev]), args.steps)
+    launches = _capi.launch_counter.value
+    clocks = clk.summary()
+
+    # e2e through the public API with host buffers
+    q_host = torch.as_tensor(q).pin_memory()
+    pot_host = torch.empty(args.npoints, dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        qd = q_host.to(dev, non_blocking=True)
+        (pot,) = drive_fmm(None, w_mx, [qd])
+        pot_host.copy_(pot, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    ms_e2e, _ = timed(e2e_step, args.steps)
+
+    # FP64 form
+    ms_64 = None
+    w_64 = None
+    if not args.no_fp64:
+        w_64 = wrangler("fp64")
+        for _ in range(max(1, args.warmup)):
+            drive_fmm(None, w_64, [q_dev])
+        ms_64, _ = timed(lambda: drive_fmm(None, w_64, [q_dev]), args.steps)
+
+    # accuracy on sampled targets against the FP64 direct sum
+    rng = np.random.default_rng(99)
+    sample = rng.choice(args.npoints, size=min(NSAMPLE, args.npoints), replace=False)
+    (ref,) = P2P([knl], exclude_self=True)(None, pts[:, sample], pts, (q,),
+                                           target_to_source=sample, device=dev)
+    (pot_mx,) = drive_fmm(None, w_mx, [q_dev])
+    ref = ref.cpu().numpy()
+
+    def rel(p):
+        return float(np.linalg.norm(p[sample] - ref) / np.linalg.norm(ref))
+
+    err_mx = rel(pot_mx.cpu().numpy())
+    err_64 = rel(drive_fmm(None, w_64, [q_dev])[0].cpu().numpy()) if w_64 is not None else None
+
+    stage_ms, roof = stage_breakdown(w_mx, trav, q_dev, dev)
+
+    value = world * args.npoints / (ms_mx * 1e-3) / 1e6
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpts/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mx,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {
+            "workload": f"laplace3d_fmm_sphere_plummer_n{args.npoints}_p{args.order}",
+            "npoints": args.npoints, "order": args.order,
+            "max_particles_in_box": MAX_PARTICLES, "exclude_self": True,
+            "precision": "mixed (FP32 near field with FP64 offsets and sums; FP64 elsewhere)",
+            "l2": "flushed between steps (256 MB write outside the timed events)",
+            "parallelism": f"replicas x{world}",
+            "tree_build_s": round(t_tree, 3), "setup_s": round(t_setup, 3),
+        },
+        "accuracy": {"relL2_mixed": err_mx, "relL2_fp64": err_64, "targets_sampled": len(sample),
+                     "reference": "FP64 direct sum (GPU kernel sumpy_p2p_direct_f64)"},
+        "fp64": {"value": (world * args.npoints / (ms_64 * 1e-3) / 1e6) if ms_64 else None,
+                 "ms_per_step": ms_64},
+        "mixed_over_fp64": (ms_64 / ms_mx) if ms_64 else None,
+        "adjoint_forward_ratio": None,
+        "stage_ms": stage_ms,
+        "roofline": roof,
+        "cpu_baseline": cpu_line,
+        "e2e": {"value": world * args.npoints / (ms_e2e * 1e-3) / 1e6, "unit": "Mpts/s",
+                "h2d_bytes_per_step": 8 * args.npoints, "d2h_bytes_per_step": 8 * args.npoints},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def stage_breakdown(w, trav, q_dev, dev):
+    """Per-stage device times of one FMM (CUDA events between the wrangler
+    calls on the launching stream) and the roofline of the dominant stage."""
+    import torch
+    peaks = {}
+    pk = ROOT / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peaks = json.loads(pk.read_text())
+    ev = []
+
+    def mark(name):
+        e = torch.cuda.Event(enable_timing=True)
+        e.record()
+        ev.append((name, e))
+
+    torch.cuda.synchronize()
+    mark("start")
+    qd = w.reorder_sources(q_dev)
+    mark("reorder")
+    mp = w.form_multipoles(None, trav.level_start_source_box_nrs, trav.source_boxes, [qd])
+    mark("p2m")
+    mp = w.coarsen_multipoles(None, trav.level_start_source_parent_box_nrs,
+                              trav.source_parent_boxes, mp)
+    mark("m2m")
+    pd = w.eval_direct(None, trav.target_boxes, trav.neighbor_source_boxes_starts,
+                       trav.neighbor_source_boxes_lists, [qd])
+    mark("p2p")
+    loc = w.multipole_to_local(None, trav.level_start_target_or_target_parent_box_nrs,
+                               trav.target_or_target_parent_boxes, trav.from_sep_siblings_starts,
+                               trav.from_sep_siblings_lists, mp)
+    mark("m2l")
+    w.eval_multipoles(None, trav.target_boxes_sep_smaller_by_source_level,
+                      trav.from_sep_smaller_by_level, mp)
+    mark("m2p")
+    pl = w.form_locals(None, trav.level_start_target_or_target_parent_box_nrs,
+                       trav.target_or_target_parent_boxes, trav.from_sep_bigger_starts,
+                       trav.from_sep_bigger_lists, [qd])
+    mark("p2l")
+    loc = w.refine_locals(None, trav.level_start_target_or_target_parent_box_nrs,
+                          trav.target_or_target_parent_boxes, loc + pl)
+    mark("l2l")
+    w.eval_locals(None, trav.level_start_target_box_nrs, trav.target_boxes, loc)
+    mark("l2p")
+    torch.cuda.synchronize()
+    stage = {}
+    for (n0, e0), (n1, e1) in zip(ev, ev[1:]):
+        stage[n1] = e0.elapsed_time(e1)
+
+    # algorithmic work
+    tree = w.tree
+    n = (w.level_orders[0] + 1) ** 2
+    tb = trav.target_boxes
+    ns = trav.neighbor_source_boxes_starts
+    nl = trav.neighbor_source_boxes_lists
+    cnt_t = tree.box_target_counts_nonchild[tb].astype(np.int64)
+    src_per_list = np.add.reduceat(
+        tree.box_source_counts_nonchild[nl].astype(np.int64), ns[:-1]) if len(nl) else 0
+    empty = np.diff(ns) == 0
+    src_per_list = np.where(empty, 0, src_per_list)
+    pairs = int((cnt_t * src_per_list).sum()) - (tree.ntargets if tree.sources_are_targets else 0)
+    m2l_entries = len(trav.from_sep_siblings_lists)
+    work = {
+        "p2p": {"flops": 11 * pairs, "pairs": pairs},
+        "m2l": {"flops": 2 * n * n * m2l_entries, "entries": m2l_entries},
+    }
+    dom = max(("p2p", "m2l"), key=lambda k: stage[k])
+    ach = work[dom]["flops"] / (stage[dom] * 1e-3) / 1e12
+    peak = peaks.get("bf16_tflops", 1590.0)
+    roof = {
+        "kernel": {"p2p": "p2p_csr_kernel<mixed>", "m2l": "m2l_f64_kernel<128>"}[dom],
+        "bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+        "frac": ach / peak, "traffic": None,
+        "peak_source": "MEASURED_PEAKS.json bf16_tflops (of measured)" if peaks else "fallback",
+        "work": work[dom],
+        "note": "FP64/FP32 CUDA-core kernel: its own pipe peak is below the bf16 "
+                "tensor figure used as the denominator",
+    }
+    return stage, roof
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,208 @@
+/*
+ * sumpy_b200.h -- C-ABI of the B200 (sm_100a) FMM evaluation kernels.
+ *
+ * Each entry point replaces one loopy kernel that sumpy's expansion wrangler
+ * (sumpy/fmm.py:264-1086) launches per tree level, with the same argument
+ * meaning: box-number arrays and CSR lists from the tree/traversal, level
+ * views of the expansion arrays ("base_ibox" = first box number of the
+ * level; expansion of box b at row b - base_ibox, coefficients contiguous),
+ * SoA coordinates ([3][n] with the given stride), and in-place outputs.
+ *
+ * Conventions (sumpy MEMO): a = center - source, b = target - center,
+ * d = target center - source center. Kernel 1/|x| for 3D Laplace; `scale`
+ * (1/(4 pi)) multiplies point outputs only. Coefficients are sumpy's stored
+ * set of the LinearPDEConformingVolumeTaylor expansions: the (p+1)^2
+ * multi-indices with mi0 < 2 ordered by (|mi|, mi0, mi1, mi2)
+ * (sumpy/expansion/__init__.py:643-752).
+ *
+ * All pointers are device pointers unless stated otherwise; nothing is
+ * allocated by any entry point. `stream` is a cudaStream_t (NULL = legacy
+ * default stream). Launches are asynchronous; the return value reports
+ * argument errors and launch errors only. Errors from a kernel's own checks
+ * are written to the optional `status` word (device int32, 0 = ok) where an
+ * entry takes one.
+ *
+ * Return codes: 0 ok, 1 bad argument, 2 CUDA launch error, 3 unsupported
+ * order/size. sumpy_last_error() gives a message for the calling thread.
+ */
+#ifndef SUMPY_B200_H
+#define SUMPY_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    SUMPY_OK = 0,
+    SUMPY_EINVAL = 1,
+    SUMPY_ELAUNCH = 2,
+    SUMPY_EUNSUPPORTED = 3
+};
+
+/* Largest expansion order the kernels accept. */
+#define SUMPY_MAX_ORDER 16
+
+int sumpy_version(void);
+const char *sumpy_last_error(void);
+
+/* ------------------------------------------------------------------ */
+/* P2P                                                                  */
+/* ------------------------------------------------------------------ */
+
+/* List-1 near field. Replaces P2PFromCSR.__call__ (sumpy/p2p.py:801-833;
+ * kernel p2p.py:484-799) as called by SumpyExpansionWrangler.eval_direct
+ * (sumpy/fmm.py:697-721):
+ *   result[t] = scale * sum_{src boxes in CSR} sum_s strength[s] / |t - s|
+ * for every target t of every target box (assigned, not accumulated).
+ * target_to_source (may be NULL) excludes the pair s == target_to_source[t]
+ * (exclude_self, p2p.py:162-170). FP64 throughout. */
+int sumpy_p2p_from_csr_f64(
+    int32_t ntgt_boxes, const int32_t *target_boxes,
+    const int32_t *source_box_starts, const int32_t *source_box_lists,
+    const int32_t *box_source_starts, const int32_t *box_source_counts_nonchild,
+    const int32_t *box_target_starts, const int32_t *box_target_counts_nonchild,
+    const double *sources, int64_t source_stride, const double *strength,
+    const double *targets, int64_t target_stride,
+    const int32_t *target_to_source, double scale, double *result, void *stream);
+
+/* Same contract, mixed precision: coordinate differences formed in FP64 and
+ * rounded to FP32, 1/r and the products in FP32, per-box partial sums in
+ * FP32, the target's total in FP64. */
+int sumpy_p2p_from_csr_mixed(
+    int32_t ntgt_boxes, const int32_t *target_boxes,
+    const int32_t *source_box_starts, const int32_t *source_box_lists,
+    const int32_t *box_source_starts, const int32_t *box_source_counts_nonchild,
+    const int32_t *box_target_starts, const int32_t *box_target_counts_nonchild,
+    const double *sources, int64_t source_stride, const double *strength,
+    const double *targets, int64_t target_stride,
+    const int32_t *target_to_source, double scale, double *result, void *stream);
+
+/* All-pairs sum. Replaces P2P.__call__ (sumpy/p2p.py:267-285), the direct
+ * evaluation sumpy's FMM tests compare against (sumpy/test/test_fmm.py:284-286).
+ * result[t] = scale * sum_s strength[s]/|t - s|, skipping s ==
+ * target_to_source[t] when that array is given. FP64. */
+int sumpy_p2p_direct_f64(
+    int64_t ntargets, const double *targets, int64_t target_stride,
+    int64_t nsources, const double *sources, int64_t source_stride,
+    const double *strength, const int32_t *target_to_source, double scale,
+    double *result, void *stream);
+
+/* ------------------------------------------------------------------ */
+/* P2E                                                                  */
+/* ------------------------------------------------------------------ */
+
+/* P2M for the leaf boxes of one level. Replaces P2EFromSingleBox
+ * (sumpy/p2e.py:155-261) as called by form_multipoles (sumpy/fmm.py:609-641);
+ * math of VolumeTaylorMultipoleExpansionBase.coefficients_from_source_vec
+ * (sumpy/expansion/multipole.py:77-114). Expansions of the listed boxes are
+ * assigned. */
+int sumpy_p2e_from_single_box_f64(
+    int order, double rscale, int32_t nsrc_boxes, const int32_t *source_boxes,
+    const double *centers, int64_t center_stride,
+    const int32_t *box_source_starts, const int32_t *box_source_counts_nonchild,
+    const double *sources, int64_t source_stride, const double *strength,
+    int32_t tgt_base_ibox, double *tgt_expansions, void *stream);
+
+/* P2L from List-4 sources for the boxes of one level. Replaces P2EFromCSR
+ * (sumpy/p2e.py:268-388) as called by form_locals (sumpy/fmm.py:963-1002);
+ * math of VolumeTaylorLocalExpansionBase.coefficients_from_source_vec
+ * (sumpy/expansion/local.py:225-271) with LaplaceDerivativeTaker
+ * (sumpy/derivative_taker.py:195-262). Expansions are assigned. */
+int sumpy_p2e_from_csr_f64(
+    int order, double rscale, int32_t ntgt_boxes, const int32_t *target_boxes,
+    const int32_t *source_box_starts, const int32_t *source_box_lists,
+    const double *centers, int64_t center_stride,
+    const int32_t *box_source_starts, const int32_t *box_source_counts_nonchild,
+    const double *sources, int64_t source_stride, const double *strength,
+    int32_t tgt_base_ibox, double *tgt_expansions, void *stream);
+
+/* ------------------------------------------------------------------ */
+/* E2E                                                                  */
+/* ------------------------------------------------------------------ */
+
+/* M2M for the parent boxes of one level. Replaces E2EFromChildren
+ * (sumpy/e2e.py:866-978) as called by coarsen_multipoles (sumpy/fmm.py:643-695);
+ * math of VolumeTaylorMultipoleExpansionBase.translate_from
+ * (sumpy/expansion/multipole.py:159-407): the stored child coefficients,
+ * scaled by (r_src/r_tgt)^|mi|, are shifted one axis at a time by
+ * d = parent center - child center and compressed back to the stored set.
+ * tgt += sum over nonzero box_child_ids[c*child_stride + parent]. */
+int sumpy_e2e_from_children_f64(
+    int src_order, int tgt_order, double src_rscale, double tgt_rscale,
+    int32_t ntgt_boxes, const int32_t *target_boxes,
+    const int32_t *box_child_ids, int64_t child_stride,
+    const double *centers, int64_t center_stride,
+    int32_t src_base_ibox, const double *src_expansions,
+    int32_t tgt_base_ibox, double *tgt_expansions, void *stream);
+
+/* L2L into the boxes of one level. Replaces E2EFromParent
+ * (sumpy/e2e.py:985-1083) as called by refine_locals (sumpy/fmm.py:1004-1045);
+ * math of VolumeTaylorLocalExpansionBase.translate_from
+ * (sumpy/expansion/local.py:311-493): full derivatives from the stored
+ * parent coefficients, truncated Taylor shift by d = child center - parent
+ * center one axis at a time, times (r_tgt/r_src)^|mi|. tgt += result. */
+int sumpy_e2e_from_parent_f64(
+    int src_order, int tgt_order, double src_rscale, double tgt_rscale,
+    int32_t ntgt_boxes, const int32_t *target_boxes, const int32_t *box_parent_ids,
+    const double *centers, int64_t center_stride,
+    int32_t src_base_ibox, const double *src_expansions,
+    int32_t tgt_base_ibox, double *tgt_expansions, void *stream);
+
+/* M2L for one level, applied per translation class as dense GEMMs.
+ * Replaces M2LUsingTranslationClassesDependentData (sumpy/e2e.py:310-558)
+ * with its pre/post-processing and FFTs (sumpy/fmm.py:798-920): in exact
+ * arithmetic L[t] = (r_tgt/r_src)^|t| sum_s M[s] D_c[s+t]
+ * (sumpy/expansion/m2l.py:363-389, 461-537, 679-698), here with
+ * class_matrices[c][t][s] = that operator (row = target coefficient).
+ *
+ * The List-2 CSR of the level (from_sep_siblings_starts/lists with the
+ * per-entry translation class) is supplied regrouped into a schedule:
+ * tiles of tile_width target boxes; for tile i, groups
+ * tile_group_starts[i] .. tile_group_starts[i+1]-1, each one class
+ * group_class[g] (0 <= c < nclasses) and one source box per target slot,
+ * group_sources[g*tile_width + slot] (-1 = none). tile_targets[i*tile_width
+ * + slot] is the target box of each slot (-1 = padding).
+ * tgt[t] += matrix_scale * sum_groups T_c * src[s]. tile_width must be 64. */
+int sumpy_m2l_translation_classes_f64(
+    int order, int32_t ntiles, int32_t tile_width, const int32_t *tile_targets,
+    const int32_t *tile_group_starts, const int32_t *group_class,
+    const int32_t *group_sources, int32_t nclasses, const double *class_matrices,
+    double matrix_scale, int32_t src_base_ibox, const double *src_expansions,
+    int32_t tgt_base_ibox, double *tgt_expansions, void *stream);
+
+/* ------------------------------------------------------------------ */
+/* E2P                                                                  */
+/* ------------------------------------------------------------------ */
+
+/* L2P for the leaf target boxes of one level. Replaces E2PFromSingleBox
+ * (sumpy/e2p.py:123-226) as called by eval_locals (sumpy/fmm.py:1047-1083);
+ * math of VolumeTaylorLocalExpansionBase.evaluate (sumpy/expansion/local.py:
+ * 284-309). result[t] = scale * value (assigned). */
+int sumpy_e2p_from_single_box_f64(
+    int order, double rscale, int32_t ntgt_boxes, const int32_t *target_boxes,
+    const double *centers, int64_t center_stride,
+    int32_t src_base_ibox, const double *src_expansions,
+    const int32_t *box_target_starts, const int32_t *box_target_counts_nonchild,
+    const double *targets, int64_t target_stride, double scale, double *result,
+    void *stream);
+
+/* M2P from List-3 boxes of one source level. Replaces E2PFromCSR
+ * (sumpy/e2p.py:233-343) as called by eval_multipoles (sumpy/fmm.py:922-961);
+ * math of VolumeTaylorMultipoleExpansionBase.evaluate
+ * (sumpy/expansion/multipole.py:131-157). result[t] += scale * value. */
+int sumpy_e2p_from_csr_f64(
+    int order, double rscale, int32_t ntgt_boxes, const int32_t *target_boxes,
+    const int32_t *source_box_starts, const int32_t *source_box_lists,
+    const double *centers, int64_t center_stride,
+    int32_t src_base_ibox, const double *src_expansions,
+    const int32_t *box_target_starts, const int32_t *box_target_counts_nonchild,
+    const double *targets, int64_t target_stride, double scale, double *result,
+    void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,57 @@
+/*
+ * sumpy_b200_tree.h -- host-side octree, interaction lists and translation
+ * classes for 3D point sets.
+ *
+ * sumpy takes its tree, traversal and translation classes from boxtree
+ * (TreeBuilder, FMMTraversalBuilder, TranslationClassesBuilder; called at
+ * sumpy/fmm.py:356-363 and sumpy/test/test_fmm.py:182-189). boxtree is an
+ * external dependency, not part of the sumpy sources, so this library
+ * provides the same products under boxtree's array names: the arrays sumpy's
+ * wrangler reads (sumpy/fmm.py:372-397, 413-418, 543-592, 752-754, 931-948).
+ *
+ * All arrays are host memory. The handle owns them until sumpy_tree_free.
+ */
+#ifndef SUMPY_B200_TREE_H
+#define SUMPY_B200_TREE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    SUMPY_TREE_OK = 0,
+    SUMPY_TREE_EINVAL = 1,
+    SUMPY_TREE_EINTERNAL = 2
+};
+
+/* Build tree + traversal + translation classes.
+ * Replaces boxtree.TreeBuilder.__call__(actx, sources, targets=...,
+ * max_particles_in_box=...) followed by FMMTraversalBuilder and
+ * TranslationClassesBuilder(is_translation_per_level=True), as used at
+ * sumpy/test/test_fmm.py:182-189 and sumpy/fmm.py:356-363.
+ * Coordinates are SoA float64. Pass tx == NULL (or ntargets < 0) when the
+ * targets are the sources; the tree then counts each particle once and
+ * provides a target_to_source array for exclude_self.
+ * Returns SUMPY_TREE_OK and an opaque handle in *handle_out. */
+int sumpy_tree_build(int64_t nsources, const double *sx, const double *sy, const double *sz,
+                     int64_t ntargets, const double *tx, const double *ty, const double *tz,
+                     int max_particles_in_box, int max_levels, void **handle_out);
+
+/* Look up a named array: kind 0 = int32, 1 = float64; length in elements. */
+int sumpy_tree_array_info(void *handle, const char *name, int *kind, int64_t *length);
+
+/* Copy a named array into dst (capacity in bytes). */
+int sumpy_tree_array_copy(void *handle, const char *name, void *dst, int64_t capacity_bytes);
+
+void sumpy_tree_free(void *handle);
+
+/* Message of the last failed call on this thread. */
+const char *sumpy_tree_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

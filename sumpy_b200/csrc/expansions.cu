@@ -1,0 +1,715 @@
+// P2M, P2L, M2M, L2L, L2P and M2P for the compressed 3D Laplace Taylor
+// expansions (sumpy's LinearPDEConformingVolumeTaylor{Multipole,Local}
+// Expansion; stored set mi0 < 2, sumpy/expansion/__init__.py:563-886).
+//
+// Full coefficient sets live in shared memory as dense cubes
+// [i][j][k] (i + j + k <= p). The Laplace projection between stored and
+// full sets (u_mi = -u_{mi-2e0+2e1} - u_{mi-2e0+2e2}) runs as p-1 parallel
+// sweeps over the mi0 planes:
+//   decompress (local -> full, CSEMatVecOperator.matvec,
+//     __init__.py:510-531):           plane i from plane i-2, i = 2..p
+//   compress (full multipole -> stored, transpose_matvec, __init__.py:533-548):
+//                                     plane i-2 gathers from plane i, i = p..2
+//
+// Derivatives of 1/r (P2L, M2P) use LaplaceDerivativeTaker's recurrence
+// (sumpy/derivative_taker.py:211-262) restricted to the stored set, which is
+// closed under it (mi0 never grows).
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace sumpy {
+namespace {
+
+__device__ inline int nfull_of(int p) { return (p + 1) * (p + 2) * (p + 3) / 6; }
+
+// f-th multi-index of the full set in sumpy's order (|mi|, mi0, mi1, mi2)
+__device__ inline void full_mi(int f, int &i, int &j, int &k)
+{
+    int deg = 0;
+    while ((deg + 1) * (deg + 2) * (deg + 3) / 6 <= f) ++deg;
+    int r = f - deg * (deg + 1) * (deg + 2) / 6;
+    i = 0;
+    while (r >= deg - i + 1) { r -= deg - i + 1; ++i; }
+    j = r;
+    k = deg - i - j;
+}
+
+// s-th multi-index of the stored set (inverse of stored_index)
+__device__ inline void stored_mi(int s, int &i, int &j, int &k)
+{
+    int deg = (int)sqrtf((float)s);
+    while (deg * deg > s) --deg;
+    while ((deg + 1) * (deg + 1) <= s) ++deg;
+    int r = s - deg * deg;
+    if (r <= deg) { i = 0; j = r; }
+    else { i = 1; j = r - (deg + 1); }
+    k = deg - i - j;
+}
+
+// t-th pair (J, K) with J + K <= m
+__device__ inline void tri_pair(int t, int m, int &J, int &K)
+{
+    J = 0;
+    while (t > m - J) { t -= m - J + 1; ++J; }
+    K = t;
+}
+
+__device__ inline double ipow(double x, int n)
+{
+    double r = 1.0;
+    for (int q = 0; q < n; ++q) r *= x;
+    return r;
+}
+
+// stored multipole -> nothing; full multipole (cube) -> compressed in place
+// (plane i-2 receives -cube[i][J-2][K] - cube[i][J][K-2]). Block-wide.
+__device__ void compress_cube_block(double *cube, int p)
+{
+    for (int i = p; i >= 2; --i) {
+        const int m = p - i + 2;
+        const int npairs = (m + 1) * (m + 2) / 2;
+        for (int t = threadIdx.x; t < npairs; t += blockDim.x) {
+            int J, K;
+            tri_pair(t, m, J, K);
+            double v = 0.0;
+            if (J >= 2) v += cube[cube_index(p, i, J - 2, K)];
+            if (K >= 2) v += cube[cube_index(p, i, J, K - 2)];
+            cube[cube_index(p, i - 2, J, K)] -= v;
+        }
+        __syncthreads();
+    }
+}
+
+// stored local in planes 0, 1 -> full local (planes 2..p). Block-wide.
+__device__ void decompress_cube_block(double *cube, int p)
+{
+    for (int i = 2; i <= p; ++i) {
+        const int m = p - i;
+        const int npairs = (m + 1) * (m + 2) / 2;
+        for (int t = threadIdx.x; t < npairs; t += blockDim.x) {
+            int J, K;
+            tri_pair(t, m, J, K);
+            cube[cube_index(p, i, J, K)] =
+                -cube[cube_index(p, i - 2, J + 2, K)] - cube[cube_index(p, i - 2, J, K + 2)];
+        }
+        __syncthreads();
+    }
+}
+
+// same, one warp
+__device__ void decompress_cube_warp(double *cube, int p, int lane)
+{
+    for (int i = 2; i <= p; ++i) {
+        const int m = p - i;
+        const int npairs = (m + 1) * (m + 2) / 2;
+        for (int t = lane; t < npairs; t += 32) {
+            int J, K;
+            tri_pair(t, m, J, K);
+            cube[cube_index(p, i, J, K)] =
+                -cube[cube_index(p, i - 2, J + 2, K)] - cube[cube_index(p, i - 2, J, K + 2)];
+        }
+        __syncwarp();
+    }
+}
+
+// Scaled derivatives rscale^|mi| d^mi (1/|x|) for the stored set of order p,
+// written to D[s * stride]; optionally dotted with coeffs (returns the sum).
+__device__ double laplace_stored_derivs(int p, double x, double y, double z, double rscale,
+                                        double *D, int stride, const double *coeffs)
+{
+    const double r2 = x * x + y * y + z * z;
+    const double rinv = rsqrt(r2);
+    const double rinv2 = rinv * rinv;
+    const double R = rscale;
+    const double Rinv = 1.0 / R;
+    const double xs[3] = {x * Rinv, y * Rinv, z * Rinv};
+    const double inv_rs2 = R * R * rinv2;
+    double acc = 0.0;
+    for (int deg = 0; deg <= p; ++deg) {
+        for (int i = 0; i <= min(1, deg); ++i) {
+            for (int j = 0; j <= deg - i; ++j) {
+                const int k = deg - i - j;
+                const int s = deg * deg + i * (deg + 1) + j;
+                double v;
+                if (j <= 1 && k <= 1) {
+                    if (deg == 0) {
+                        v = rinv;
+                    } else if (deg == 1) {
+                        const double c = i ? x : (j ? y : z);
+                        v = -R * c * rinv * rinv2;
+                    } else if (deg == 2) {
+                        const double c1 = i ? x : y;
+                        const double c2 = k ? z : y;
+                        v = 3.0 * R * R * c1 * c2 * rinv * rinv2 * rinv2;
+                    } else {
+                        v = -15.0 * R * R * R * x * y * z * rinv * rinv2 * rinv2 * rinv2;
+                    }
+                } else {
+                    const int d = (j >= 2) ? 1 : 2;
+                    double e = 0.0;
+                    if (i == 1) e -= 2.0 * xs[0] * D[stored_index(0, j, k) * stride];
+                    if (j >= 1) {
+                        const double t1 = D[stored_index(i, j - 1, k) * stride];
+                        const double t2 = (j >= 2) ? D[stored_index(i, j - 2, k) * stride] : 0.0;
+                        if (d == 1) e -= (2 * j - 1) * xs[1] * t1 + (double)(j - 1) * (j - 1) * t2;
+                        else e -= 2 * j * xs[1] * t1 + (double)j * (j - 1) * t2;
+                    }
+                    if (k >= 1) {
+                        const double t1 = D[stored_index(i, j, k - 1) * stride];
+                        const double t2 = (k >= 2) ? D[stored_index(i, j, k - 2) * stride] : 0.0;
+                        if (d == 2) e -= (2 * k - 1) * xs[2] * t1 + (double)(k - 1) * (k - 1) * t2;
+                        else e -= 2 * k * xs[2] * t1 + (double)k * (k - 1) * t2;
+                    }
+                    v = e * inv_rs2;
+                }
+                D[s * stride] = v;
+                if (coeffs) acc += coeffs[s] * v;
+            }
+        }
+    }
+    return acc;
+}
+
+// {{{ P2M
+
+constexpr int P2M_THREADS = 128;
+constexpr int P2M_CHUNK = 32;
+
+__global__ void __launch_bounds__(P2M_THREADS)
+p2m_kernel(int p, double rscale, const int32_t *__restrict__ boxes, const double *__restrict__ centers,
+           int64_t cstride, const int32_t *__restrict__ bss, const int32_t *__restrict__ bsc,
+           const double *__restrict__ sources, int64_t sstride, const double *__restrict__ q,
+           int32_t base, double *__restrict__ out)
+{
+    extern __shared__ double sm[];
+    const int P1 = p + 1;
+    double *cube = sm;                               // P1^3
+    double *pw = cube + P1 * P1 * P1;                // [CHUNK][3][P1]
+    double *qs = pw + P2M_CHUNK * 3 * P1;            // [CHUNK]
+
+    const int32_t b = boxes[blockIdx.x];
+    const double c[3] = {centers[b], centers[cstride + b], centers[2 * cstride + b]};
+    const int32_t s0 = bss[b], ns = bsc[b];
+    const int nfull = nfull_of(p);
+    const double rinv = 1.0 / rscale;
+
+    for (int t = threadIdx.x; t < P1 * P1 * P1; t += blockDim.x) cube[t] = 0.0;
+    __syncthreads();
+
+    for (int sc = 0; sc < ns; sc += P2M_CHUNK) {
+        const int nsc = min(P2M_CHUNK, ns - sc);
+        for (int t = threadIdx.x; t < P2M_CHUNK * 3; t += blockDim.x) {
+            const int s = t / 3, d = t % 3;
+            double *w = pw + (s * 3 + d) * P1;
+            if (s < nsc) {
+                const double a = (c[d] - sources[d * sstride + s0 + sc + s]) * rinv;
+                w[0] = 1.0;
+                for (int k = 1; k <= p; ++k) w[k] = w[k - 1] * a / k;
+                if (d == 0) qs[s] = q[s0 + sc + s];
+            }
+        }
+        __syncthreads();
+        for (int f = threadIdx.x; f < nfull; f += blockDim.x) {
+            int i, j, k;
+            full_mi(f, i, j, k);
+            double acc = 0.0;
+            for (int s = 0; s < nsc; ++s)
+                acc += qs[s] * pw[(s * 3 + 0) * P1 + i] * pw[(s * 3 + 1) * P1 + j] *
+                       pw[(s * 3 + 2) * P1 + k];
+            cube[cube_index(p, i, j, k)] += acc;
+        }
+        __syncthreads();
+    }
+    compress_cube_block(cube, p);
+    const int n = ncoeff_of(p);
+    double *o = out + (int64_t)(b - base) * n;
+    for (int s = threadIdx.x; s < n; s += blockDim.x) {
+        int i, j, k;
+        stored_mi(s, i, j, k);
+        o[s] = cube[cube_index(p, i, j, k)];
+    }
+}
+
+// }}}
+
+// {{{ M2M / L2L (axis-by-axis shifts)
+
+constexpr int E2E_THREADS = 128;
+
+// out[m] = sum_{t=0}^{m_d} in[m with m_d = t] * pw[m_d - t]  (multipole shift)
+__device__ void mpole_shift_axis(const double *in, double *out, int p, int d, const double *pw)
+{
+    const int nfull = nfull_of(p);
+    for (int f = threadIdx.x; f < nfull; f += blockDim.x) {
+        int m[3];
+        full_mi(f, m[0], m[1], m[2]);
+        double acc = 0.0;
+        for (int t = 0; t <= m[d]; ++t) {
+            int q[3] = {m[0], m[1], m[2]};
+            q[d] = t;
+            acc += in[cube_index(p, q[0], q[1], q[2])] * pw[m[d] - t];
+        }
+        out[cube_index(p, m[0], m[1], m[2])] = acc;
+    }
+}
+
+// out[m] = sum_{q=0}^{p-|m|} in[m + q e_d] * pw[q]  (local shift)
+__device__ void local_shift_axis(const double *in, double *out, int p, int d, const double *pw)
+{
+    const int nfull = nfull_of(p);
+    for (int f = threadIdx.x; f < nfull; f += blockDim.x) {
+        int m[3];
+        full_mi(f, m[0], m[1], m[2]);
+        const int deg = m[0] + m[1] + m[2];
+        double acc = 0.0;
+        for (int q = 0; q <= p - deg; ++q) {
+            int s[3] = {m[0], m[1], m[2]};
+            s[d] += q;
+            acc += in[cube_index(p, s[0], s[1], s[2])] * pw[q];
+        }
+        out[cube_index(p, m[0], m[1], m[2])] = acc;
+    }
+}
+
+__global__ void __launch_bounds__(E2E_THREADS)
+m2m_kernel(int ps, int pt, double rsrc, double rtgt, const int32_t *__restrict__ boxes,
+           const int32_t *__restrict__ child_ids, int64_t child_stride,
+           const double *__restrict__ centers, int64_t cstride, int32_t sbase,
+           const double *__restrict__ src, int32_t tbase, double *__restrict__ tgt)
+{
+    extern __shared__ double sm[];
+    const int P1 = pt + 1, C = P1 * P1 * P1;
+    double *A = sm, *B = A + C, *ACC = B + C, *pw = ACC + C;  // pw: [3][P1]
+    const int32_t b = boxes[blockIdx.x];
+    const int ns = ncoeff_of(ps), nt = ncoeff_of(pt), nfull = nfull_of(pt);
+    const double ratio = rsrc / rtgt;
+
+    for (int t = threadIdx.x; t < C; t += blockDim.x) { ACC[t] = 0.0; A[t] = 0.0; B[t] = 0.0; }
+    __syncthreads();
+    for (int slot = 0; slot < 8; ++slot) {
+        const int32_t ch = child_ids[slot * child_stride + b];
+        if (ch == 0) continue;
+        if (threadIdx.x < 3) {
+            const int d = threadIdx.x;
+            const double dd = (centers[d * cstride + b] - centers[d * cstride + ch]) / rtgt;
+            double *w = pw + d * P1;
+            w[0] = 1.0;
+            for (int k = 1; k <= pt; ++k) w[k] = w[k - 1] * dd / k;
+        }
+        const double *cs = src + (int64_t)(ch - sbase) * ns;
+        for (int f = threadIdx.x; f < nfull; f += blockDim.x) {
+            int i, j, k;
+            full_mi(f, i, j, k);
+            const int deg = i + j + k;
+            double v = 0.0;
+            if (i < 2 && deg <= ps) v = cs[stored_index(i, j, k)] * ipow(ratio, deg);
+            A[cube_index(pt, i, j, k)] = v;
+        }
+        __syncthreads();
+        mpole_shift_axis(A, B, pt, 1, pw + 1 * P1);
+        __syncthreads();
+        mpole_shift_axis(B, A, pt, 2, pw + 2 * P1);
+        __syncthreads();
+        mpole_shift_axis(A, B, pt, 0, pw + 0 * P1);
+        __syncthreads();
+        for (int f = threadIdx.x; f < nfull; f += blockDim.x) {
+            int i, j, k;
+            full_mi(f, i, j, k);
+            ACC[cube_index(pt, i, j, k)] += B[cube_index(pt, i, j, k)];
+        }
+        __syncthreads();
+    }
+    compress_cube_block(ACC, pt);
+    double *o = tgt + (int64_t)(b - tbase) * nt;
+    for (int s = threadIdx.x; s < nt; s += blockDim.x) {
+        int i, j, k;
+        stored_mi(s, i, j, k);
+        o[s] += ACC[cube_index(pt, i, j, k)];
+    }
+}
+
+__global__ void __launch_bounds__(E2E_THREADS)
+l2l_kernel(int ps, int pt, double rsrc, double rtgt, const int32_t *__restrict__ boxes,
+           const int32_t *__restrict__ parent_ids, const double *__restrict__ centers,
+           int64_t cstride, int32_t sbase, const double *__restrict__ src, int32_t tbase,
+           double *__restrict__ tgt)
+{
+    extern __shared__ double sm[];
+    const int P1 = ps + 1, C = P1 * P1 * P1;
+    double *A = sm, *B = A + C, *pw = B + C;  // pw: [3][P1]
+    const int32_t b = boxes[blockIdx.x];
+    const int32_t par = parent_ids[b];
+    const int ns = ncoeff_of(ps), nt = ncoeff_of(pt), nfull = nfull_of(ps);
+
+    if (threadIdx.x < 3) {
+        const int d = threadIdx.x;
+        const double dd = (centers[d * cstride + b] - centers[d * cstride + par]) / rsrc;
+        double *w = pw + d * P1;
+        w[0] = 1.0;
+        for (int k = 1; k <= ps; ++k) w[k] = w[k - 1] * dd / k;
+    }
+    const double *cs = src + (int64_t)(par - sbase) * ns;
+    for (int s = threadIdx.x; s < ns; s += blockDim.x) {
+        int i, j, k;
+        stored_mi(s, i, j, k);
+        A[cube_index(ps, i, j, k)] = cs[s];
+    }
+    __syncthreads();
+    decompress_cube_block(A, ps);
+    local_shift_axis(A, B, ps, 0, pw + 0 * P1);
+    __syncthreads();
+    local_shift_axis(B, A, ps, 1, pw + 1 * P1);
+    __syncthreads();
+    local_shift_axis(A, B, ps, 2, pw + 2 * P1);
+    __syncthreads();
+    const double ratio = rtgt / rsrc;
+    double *o = tgt + (int64_t)(b - tbase) * nt;
+    for (int s = threadIdx.x; s < nt; s += blockDim.x) {
+        int i, j, k;
+        stored_mi(s, i, j, k);
+        const int deg = i + j + k;
+        if (deg <= ps) o[s] += B[cube_index(ps, i, j, k)] * ipow(ratio, deg);
+    }
+}
+
+// }}}
+
+// {{{ L2P
+
+constexpr int L2P_MAX_WARPS = 4;
+
+__global__ void l2p_kernel(int p, double rscale, int32_t nboxes, const int32_t *__restrict__ boxes,
+                           const double *__restrict__ centers, int64_t cstride, int32_t sbase,
+                           const double *__restrict__ src, const int32_t *__restrict__ bts,
+                           const int32_t *__restrict__ btc, const double *__restrict__ targets,
+                           int64_t tstride, double scale, double *__restrict__ result)
+{
+    extern __shared__ double sm[];
+    const int P1 = p + 1, C = P1 * P1 * P1;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nwarps = blockDim.x >> 5;
+    const int ib = blockIdx.x * nwarps + warp;
+    if (ib >= nboxes) return;
+    double *cube = sm + warp * (C + P1 + 1);
+    double *inv = cube + C;  // inv[n] = 1/n, n = 1..p+1
+
+    const int32_t b = boxes[ib];
+    const int n = ncoeff_of(p);
+    const double *cs = src + (int64_t)(b - sbase) * n;
+    for (int s = lane; s < n; s += 32) {
+        int i, j, k;
+        stored_mi(s, i, j, k);
+        cube[cube_index(p, i, j, k)] = cs[s];
+    }
+    for (int q = lane; q <= p + 1; q += 32) inv[q] = q ? 1.0 / q : 0.0;
+    __syncwarp();
+    decompress_cube_warp(cube, p, lane);
+
+    const double c[3] = {centers[b], centers[cstride + b], centers[2 * cstride + b]};
+    const double rinv = 1.0 / rscale;
+    const int32_t t0 = bts[b], nt = btc[b];
+    for (int32_t tt = lane; tt < nt; tt += 32) {
+        const int32_t t = t0 + tt;
+        const double x = (targets[t] - c[0]) * rinv;
+        const double y = (targets[tstride + t] - c[1]) * rinv;
+        const double z = (targets[2 * tstride + t] - c[2]) * rinv;
+        double tot = 0.0;
+        for (int i = p; i >= 0; --i) {
+            double sy = 0.0;
+            for (int j = p - i; j >= 0; --j) {
+                double sz = 0.0;
+                const double *row = cube + cube_index(p, i, j, 0);
+                for (int k = p - i - j; k >= 0; --k) sz = row[k] + sz * z * inv[k + 1];
+                sy = sz + sy * y * inv[j + 1];
+            }
+            tot = sy + tot * x * inv[i + 1];
+        }
+        result[t] = scale * tot;
+    }
+}
+
+// }}}
+
+// {{{ M2P / P2L (derivative recurrence, per-lane shared scratch)
+
+constexpr int DSTRIDE = 33;  // lanes per coefficient row + 1 (bank spread)
+
+__global__ void m2p_kernel(int p, double rscale, int32_t ntgt_boxes,
+                           const int32_t *__restrict__ target_boxes,
+                           const int32_t *__restrict__ src_starts, const int32_t *__restrict__ src_lists,
+                           const double *__restrict__ centers, int64_t cstride, int32_t sbase,
+                           const double *__restrict__ src, const int32_t *__restrict__ bts,
+                           const int32_t *__restrict__ btc, const double *__restrict__ targets,
+                           int64_t tstride, double scale, double *__restrict__ result)
+{
+    extern __shared__ double sm[];
+    const int n = ncoeff_of(p);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nwarps = blockDim.x >> 5;
+    const int ib = blockIdx.x * nwarps + warp;
+    if (ib >= ntgt_boxes) return;
+    double *D = sm + warp * (n * DSTRIDE + n);
+    double *M = D + n * DSTRIDE;
+
+    const int32_t tb = target_boxes[ib];
+    const int32_t t0 = bts[tb], nt = btc[tb];
+    const int32_t ls = src_starts[ib], le = src_starts[ib + 1];
+    for (int32_t tc = 0; tc < nt; tc += 32) {
+        const int32_t t = t0 + tc + lane;
+        const bool active = tc + lane < nt;
+        double tx = 0, ty = 0, tz = 0;
+        if (active) { tx = targets[t]; ty = targets[tstride + t]; tz = targets[2 * tstride + t]; }
+        double acc = 0.0;
+        for (int32_t l = ls; l < le; ++l) {
+            const int32_t sb = src_lists[l];
+            const double *cs = src + (int64_t)(sb - sbase) * n;
+            __syncwarp();
+            for (int s = lane; s < n; s += 32) M[s] = cs[s];
+            __syncwarp();
+            if (active)
+                acc += laplace_stored_derivs(p, tx - centers[sb], ty - centers[cstride + sb],
+                                             tz - centers[2 * cstride + sb], rscale, D + lane,
+                                             DSTRIDE, M);
+        }
+        if (active) result[t] += scale * acc;
+    }
+}
+
+__global__ void p2l_kernel(int p, double rscale, int32_t ntgt_boxes,
+                           const int32_t *__restrict__ target_boxes,
+                           const int32_t *__restrict__ src_starts, const int32_t *__restrict__ src_lists,
+                           const double *__restrict__ centers, int64_t cstride,
+                           const int32_t *__restrict__ bss, const int32_t *__restrict__ bsc,
+                           const double *__restrict__ sources, int64_t sstride,
+                           const double *__restrict__ q, int32_t tbase, double *__restrict__ out)
+{
+    extern __shared__ double sm[];
+    const int n = ncoeff_of(p);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nwarps = blockDim.x >> 5;
+    const int ib = blockIdx.x * nwarps + warp;
+    if (ib >= ntgt_boxes) return;
+    double *D = sm + warp * (n * DSTRIDE + n);
+    double *acc = D + n * DSTRIDE;
+
+    const int32_t tb = target_boxes[ib];
+    const double c[3] = {centers[tb], centers[cstride + tb], centers[2 * cstride + tb]};
+    for (int s = lane; s < n; s += 32) acc[s] = 0.0;
+    const int32_t ls = src_starts[ib], le = src_starts[ib + 1];
+    for (int32_t l = ls; l < le; ++l) {
+        const int32_t sb = src_lists[l];
+        const int32_t s0 = bss[sb], ns = bsc[sb];
+        for (int32_t sc = 0; sc < ns; sc += 32) {
+            const int nsc = min(32, ns - sc);
+            __syncwarp();
+            if (lane < nsc) {
+                const int32_t s = s0 + sc + lane;
+                laplace_stored_derivs(p, c[0] - sources[s], c[1] - sources[sstride + s],
+                                      c[2] - sources[2 * sstride + s], rscale, D + lane, DSTRIDE,
+                                      nullptr);
+                const double qq = q[s];
+                for (int k = 0; k < n; ++k) D[k * DSTRIDE + lane] *= qq;
+            }
+            __syncwarp();
+            for (int k = lane; k < n; k += 32) {
+                double sum = 0.0;
+                for (int l2 = 0; l2 < nsc; ++l2) sum += D[k * DSTRIDE + l2];
+                acc[k] += sum;
+            }
+        }
+    }
+    __syncwarp();
+    double *o = out + (int64_t)(tb - tbase) * n;
+    for (int s = lane; s < n; s += 32) o[s] = acc[s];
+}
+
+// }}}
+
+bool order_ok(int p) { return p >= 0 && p <= SUMPY_MAX_ORDER; }
+
+template <typename K>
+int prepare_smem(K kernel, size_t bytes)
+{
+    if (bytes > 227 * 1024) return bad_arg("shared memory request exceeds 227 KB");
+    if (bytes > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)bytes);
+        if (e != cudaSuccess) {
+            set_last_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+            return SUMPY_ELAUNCH;
+        }
+    }
+    return SUMPY_OK;
+}
+
+}  // namespace
+}  // namespace sumpy
+
+using namespace sumpy;
+
+extern "C" {
+
+int sumpy_p2e_from_single_box_f64(int order, double rscale, int32_t nsrc_boxes,
+                                  const int32_t *source_boxes, const double *centers,
+                                  int64_t center_stride, const int32_t *box_source_starts,
+                                  const int32_t *box_source_counts_nonchild,
+                                  const double *sources, int64_t source_stride,
+                                  const double *strength, int32_t tgt_base_ibox,
+                                  double *tgt_expansions, void *stream)
+{
+    if (!order_ok(order)) { set_last_error("p2m: unsupported order"); return SUMPY_EUNSUPPORTED; }
+    if (nsrc_boxes < 0) return bad_arg("p2m: nsrc_boxes < 0");
+    if (nsrc_boxes == 0) return SUMPY_OK;
+    if (!source_boxes || !centers || !box_source_starts || !box_source_counts_nonchild ||
+        !sources || !strength || !tgt_expansions)
+        return bad_arg("p2m: null pointer argument");
+    const int P1 = order + 1;
+    const size_t smem = sizeof(double) * (P1 * P1 * P1 + P2M_CHUNK * 3 * P1 + P2M_CHUNK);
+    int rc = prepare_smem(p2m_kernel, smem);
+    if (rc) return rc;
+    p2m_kernel<<<nsrc_boxes, P2M_THREADS, smem, as_stream(stream)>>>(
+        order, rscale, source_boxes, centers, center_stride, box_source_starts,
+        box_source_counts_nonchild, sources, source_stride, strength, tgt_base_ibox,
+        tgt_expansions);
+    return check_launch("p2m_kernel");
+}
+
+int sumpy_e2e_from_children_f64(int src_order, int tgt_order, double src_rscale,
+                                double tgt_rscale, int32_t ntgt_boxes,
+                                const int32_t *target_boxes, const int32_t *box_child_ids,
+                                int64_t child_stride, const double *centers,
+                                int64_t center_stride, int32_t src_base_ibox,
+                                const double *src_expansions, int32_t tgt_base_ibox,
+                                double *tgt_expansions, void *stream)
+{
+    if (!order_ok(src_order) || !order_ok(tgt_order)) {
+        set_last_error("m2m: unsupported order");
+        return SUMPY_EUNSUPPORTED;
+    }
+    if (ntgt_boxes < 0) return bad_arg("m2m: ntgt_boxes < 0");
+    if (ntgt_boxes == 0) return SUMPY_OK;
+    if (!target_boxes || !box_child_ids || !centers || !src_expansions || !tgt_expansions)
+        return bad_arg("m2m: null pointer argument");
+    const int P1 = tgt_order + 1;
+    const size_t smem = sizeof(double) * (3 * P1 * P1 * P1 + 3 * P1);
+    int rc = prepare_smem(m2m_kernel, smem);
+    if (rc) return rc;
+    m2m_kernel<<<ntgt_boxes, E2E_THREADS, smem, as_stream(stream)>>>(
+        src_order, tgt_order, src_rscale, tgt_rscale, target_boxes, box_child_ids, child_stride,
+        centers, center_stride, src_base_ibox, src_expansions, tgt_base_ibox, tgt_expansions);
+    return check_launch("m2m_kernel");
+}
+
+int sumpy_e2e_from_parent_f64(int src_order, int tgt_order, double src_rscale,
+                              double tgt_rscale, int32_t ntgt_boxes, const int32_t *target_boxes,
+                              const int32_t *box_parent_ids, const double *centers,
+                              int64_t center_stride, int32_t src_base_ibox,
+                              const double *src_expansions, int32_t tgt_base_ibox,
+                              double *tgt_expansions, void *stream)
+{
+    if (!order_ok(src_order) || !order_ok(tgt_order)) {
+        set_last_error("l2l: unsupported order");
+        return SUMPY_EUNSUPPORTED;
+    }
+    if (ntgt_boxes < 0) return bad_arg("l2l: ntgt_boxes < 0");
+    if (ntgt_boxes == 0) return SUMPY_OK;
+    if (!target_boxes || !box_parent_ids || !centers || !src_expansions || !tgt_expansions)
+        return bad_arg("l2l: null pointer argument");
+    const int P1 = src_order + 1;
+    const size_t smem = sizeof(double) * (2 * P1 * P1 * P1 + 3 * P1);
+    int rc = prepare_smem(l2l_kernel, smem);
+    if (rc) return rc;
+    l2l_kernel<<<ntgt_boxes, E2E_THREADS, smem, as_stream(stream)>>>(
+        src_order, tgt_order, src_rscale, tgt_rscale, target_boxes, box_parent_ids, centers,
+        center_stride, src_base_ibox, src_expansions, tgt_base_ibox, tgt_expansions);
+    return check_launch("l2l_kernel");
+}
+
+int sumpy_e2p_from_single_box_f64(int order, double rscale, int32_t ntgt_boxes,
+                                  const int32_t *target_boxes, const double *centers,
+                                  int64_t center_stride, int32_t src_base_ibox,
+                                  const double *src_expansions, const int32_t *box_target_starts,
+                                  const int32_t *box_target_counts_nonchild,
+                                  const double *targets, int64_t target_stride, double scale,
+                                  double *result, void *stream)
+{
+    if (!order_ok(order)) { set_last_error("l2p: unsupported order"); return SUMPY_EUNSUPPORTED; }
+    if (ntgt_boxes < 0) return bad_arg("l2p: ntgt_boxes < 0");
+    if (ntgt_boxes == 0) return SUMPY_OK;
+    if (!target_boxes || !centers || !src_expansions || !box_target_starts ||
+        !box_target_counts_nonchild || !targets || !result)
+        return bad_arg("l2p: null pointer argument");
+    const int P1 = order + 1;
+    const size_t per_warp = sizeof(double) * (P1 * P1 * P1 + P1 + 1);
+    int warps = (int)std::max<size_t>(1, std::min<size_t>(L2P_MAX_WARPS, (48 * 1024) / per_warp));
+    const size_t smem = per_warp * warps;
+    int rc = prepare_smem(l2p_kernel, smem);
+    if (rc) return rc;
+    const int blocks = (ntgt_boxes + warps - 1) / warps;
+    l2p_kernel<<<blocks, 32 * warps, smem, as_stream(stream)>>>(
+        order, rscale, ntgt_boxes, target_boxes, centers, center_stride, src_base_ibox,
+        src_expansions, box_target_starts, box_target_counts_nonchild, targets, target_stride,
+        scale, result);
+    return check_launch("l2p_kernel");
+}
+
+int sumpy_e2p_from_csr_f64(int order, double rscale, int32_t ntgt_boxes,
+                           const int32_t *target_boxes, const int32_t *source_box_starts,
+                           const int32_t *source_box_lists, const double *centers,
+                           int64_t center_stride, int32_t src_base_ibox,
+                           const double *src_expansions, const int32_t *box_target_starts,
+                           const int32_t *box_target_counts_nonchild, const double *targets,
+                           int64_t target_stride, double scale, double *result, void *stream)
+{
+    if (!order_ok(order)) { set_last_error("m2p: unsupported order"); return SUMPY_EUNSUPPORTED; }
+    if (ntgt_boxes < 0) return bad_arg("m2p: ntgt_boxes < 0");
+    if (ntgt_boxes == 0) return SUMPY_OK;
+    if (!target_boxes || !source_box_starts || !source_box_lists || !centers ||
+        !src_expansions || !box_target_starts || !box_target_counts_nonchild || !targets ||
+        !result)
+        return bad_arg("m2p: null pointer argument");
+    const int n = ncoeff_of(order);
+    const size_t per_warp = sizeof(double) * (n * DSTRIDE + n);
+    const int warps = (int)std::max<size_t>(1, std::min<size_t>(4, (96 * 1024) / per_warp));
+    const size_t smem = per_warp * warps;
+    int rc = prepare_smem(m2p_kernel, smem);
+    if (rc) return rc;
+    const int blocks = (ntgt_boxes + warps - 1) / warps;
+    m2p_kernel<<<blocks, 32 * warps, smem, as_stream(stream)>>>(
+        order, rscale, ntgt_boxes, target_boxes, source_box_starts, source_box_lists, centers,
+        center_stride, src_base_ibox, src_expansions, box_target_starts,
+        box_target_counts_nonchild, targets, target_stride, scale, result);
+    return check_launch("m2p_kernel");
+}
+
+int sumpy_p2e_from_csr_f64(int order, double rscale, int32_t ntgt_boxes,
+                           const int32_t *target_boxes, const int32_t *source_box_starts,
+                           const int32_t *source_box_lists, const double *centers,
+                           int64_t center_stride, const int32_t *box_source_starts,
+                           const int32_t *box_source_counts_nonchild, const double *sources,
+                           int64_t source_stride, const double *strength, int32_t tgt_base_ibox,
+                           double *tgt_expansions, void *stream)
+{
+    if (!order_ok(order)) { set_last_error("p2l: unsupported order"); return SUMPY_EUNSUPPORTED; }
+    if (ntgt_boxes < 0) return bad_arg("p2l: ntgt_boxes < 0");
+    if (ntgt_boxes == 0) return SUMPY_OK;
+    if (!target_boxes || !source_box_starts || !source_box_lists || !centers ||
+        !box_source_starts || !box_source_counts_nonchild || !sources || !strength ||
+        !tgt_expansions)
+        return bad_arg("p2l: null pointer argument");
+    const int n = ncoeff_of(order);
+    const size_t per_warp = sizeof(double) * (n * DSTRIDE + n);
+    const int warps = (int)std::max<size_t>(1, std::min<size_t>(4, (96 * 1024) / per_warp));
+    const size_t smem = per_warp * warps;
+    int rc = prepare_smem(p2l_kernel, smem);
+    if (rc) return rc;
+    const int blocks = (ntgt_boxes + warps - 1) / warps;
+    p2l_kernel<<<blocks, 32 * warps, smem, as_stream(stream)>>>(
+        order, rscale, ntgt_boxes, target_boxes, source_box_starts, source_box_lists, centers,
+        center_stride, box_source_starts, box_source_counts_nonchild, sources, source_stride,
+        strength, tgt_base_ibox, tgt_expansions);
+    return check_launch("p2l_kernel");
+}
+
+}  // extern "C"

@@ -1,0 +1,68 @@
+"""``drive_fmm``: the FMM stage sequence of boxtree's driver.
+
+sumpy's wrangler is driven by ``boxtree.fmm.drive_fmm`` (called at
+sumpy/test/test_fmm.py:280-282), which is outside the sumpy sources. This
+function issues the same wrangler calls in the same order, with the same
+traversal fields (the order sumpy's wrangler documents,
+sumpy/fmm.py:609-1086):
+
+reorder_sources -> form_multipoles (P2M) -> coarsen_multipoles (M2M) ->
+eval_direct (List 1) -> multipole_to_local (List 2) -> eval_multipoles
+(List 3) -> form_locals (List 4) -> refine_locals (L2L) -> eval_locals (L2P)
+-> reorder_potentials -> finalize_potentials.
+"""
+from __future__ import annotations
+
+
+def drive_fmm(actx, wrangler, src_weight_vecs, timing_data=None):
+    trav = wrangler.traversal
+    src_weight_vecs = [wrangler.reorder_sources(w) for w in src_weight_vecs]
+    src_weight_vecs = wrangler.distribute_source_weights(src_weight_vecs)
+
+    mpole_exps = wrangler.form_multipoles(
+        actx, trav.level_start_source_box_nrs, trav.source_boxes, src_weight_vecs)
+    mpole_exps = wrangler.coarsen_multipoles(
+        actx, trav.level_start_source_parent_box_nrs, trav.source_parent_boxes, mpole_exps)
+
+    potentials = wrangler.eval_direct(
+        actx, trav.target_boxes, trav.neighbor_source_boxes_starts,
+        trav.neighbor_source_boxes_lists, src_weight_vecs)
+
+    local_exps = wrangler.multipole_to_local(
+        actx, trav.level_start_target_or_target_parent_box_nrs,
+        trav.target_or_target_parent_boxes, trav.from_sep_siblings_starts,
+        trav.from_sep_siblings_lists, mpole_exps)
+
+    mpole_result = wrangler.eval_multipoles(
+        actx, trav.target_boxes_sep_smaller_by_source_level,
+        trav.from_sep_smaller_by_level, mpole_exps)
+    potentials = [a + b for a, b in zip(potentials, mpole_result)]
+
+    if trav.from_sep_close_smaller_starts is not None:
+        direct = wrangler.eval_direct(
+            actx, trav.target_boxes, trav.from_sep_close_smaller_starts,
+            trav.from_sep_close_smaller_lists, src_weight_vecs)
+        potentials = [a + b for a, b in zip(potentials, direct)]
+
+    local_result = wrangler.form_locals(
+        actx, trav.level_start_target_or_target_parent_box_nrs,
+        trav.target_or_target_parent_boxes, trav.from_sep_bigger_starts,
+        trav.from_sep_bigger_lists, src_weight_vecs)
+    local_exps = local_exps + local_result
+
+    if trav.from_sep_close_bigger_starts is not None:
+        direct = wrangler.eval_direct(
+            actx, trav.target_boxes, trav.from_sep_close_bigger_starts,
+            trav.from_sep_close_bigger_lists, src_weight_vecs)
+        potentials = [a + b for a, b in zip(potentials, direct)]
+
+    local_exps = wrangler.refine_locals(
+        actx, trav.level_start_target_or_target_parent_box_nrs,
+        trav.target_or_target_parent_boxes, local_exps)
+
+    local_result = wrangler.eval_locals(
+        actx, trav.level_start_target_box_nrs, trav.target_boxes, local_exps)
+    potentials = [a + b for a, b in zip(potentials, local_result)]
+
+    result = wrangler.reorder_potentials(potentials)
+    return wrangler.finalize_potentials(actx, result)

@@ -1,0 +1,174 @@
+"""Expansion descriptors and host-side translation tables.
+
+Mirrors the parts of sumpy's expansion classes the FMM path needs:
+``LinearPDEConformingVolumeTaylorMultipoleExpansion`` and
+``LinearPDEConformingVolumeTaylorLocalExpansion`` (sumpy/expansion/
+multipole.py:416-419, local.py:512-515) -- their coefficient identifiers
+and lengths -- plus the dense per-class M2L operators the CUDA GEMM applies.
+
+Coefficient sets (3D Laplace, sumpy/expansion/__init__.py:563-886): the
+full set is every multi-index with |mi| <= p sorted by (|mi|, mi0, mi1, mi2);
+the stored set keeps mi0 < 2, (p+1)^2 of them, in the same order.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from functools import lru_cache
+from typing import Any
+
+import numpy as np
+
+from sumpy_b200.kernel import LaplaceKernel
+
+
+# {{{ index sets
+
+@lru_cache(maxsize=None)
+def full_ids(p: int) -> tuple:
+    return tuple((i, j, deg - i - j)
+                 for deg in range(p + 1)
+                 for i in range(deg + 1)
+                 for j in range(deg - i + 1))
+
+
+@lru_cache(maxsize=None)
+def stored_ids(p: int) -> tuple:
+    return tuple(mi for mi in full_ids(p) if mi[0] < 2)
+
+
+def stored_index(i, j, k):
+    deg = i + j + k
+    return deg * deg + i * (deg + 1) + j
+
+# }}}
+
+
+# {{{ expansion classes
+
+@dataclass(frozen=True)
+class _VolumeTaylorBase:
+    kernel: Any
+    order: int
+    use_rscale: bool | None = None
+
+    def __post_init__(self):
+        if not isinstance(self.kernel, LaplaceKernel):
+            raise NotImplementedError("only LaplaceKernel(3) expansions are implemented")
+        if not 0 <= self.order <= 16:
+            raise ValueError(f"order must be in [0, 16], got {self.order}")
+        if self.use_rscale is False:
+            raise NotImplementedError("expansions are always rscale-scaled")
+
+    @property
+    def dim(self):
+        return 3
+
+    def get_coefficient_identifiers(self):
+        return list(stored_ids(self.order))
+
+    def get_full_coefficient_identifiers(self):
+        return list(full_ids(self.order))
+
+    def __len__(self):
+        return (self.order + 1) ** 2
+
+
+@dataclass(frozen=True)
+class LinearPDEConformingVolumeTaylorMultipoleExpansion(_VolumeTaylorBase):
+    """Compressed Taylor multipole expansion (sumpy/expansion/multipole.py:416)."""
+
+
+@dataclass(frozen=True)
+class LinearPDEConformingVolumeTaylorLocalExpansion(_VolumeTaylorBase):
+    """Compressed Taylor local expansion (sumpy/expansion/local.py:512).
+    ``m2l_translation_override`` is accepted for call compatibility; the B200
+    path always applies M2L as dense per-class operators."""
+    m2l_translation_override: Any = field(default=None, compare=False)
+
+# }}}
+
+
+# {{{ Laplace derivatives and M2L operators
+
+def laplace_derivatives(vecs, rscale, maxdeg, maxi0=1):
+    """Scaled derivatives ``rscale^|mi| d^mi (1/|x|)`` at points ``vecs``
+    (shape (3, m)) for mi0 <= maxi0, |mi| <= maxdeg. Returns an array
+    ``D[i, j, k, m]`` (entries with i + j + k > maxdeg are zero).
+
+    Same recurrence as ``LaplaceDerivativeTaker.diff``
+    (sumpy/derivative_taker.py:211-262), vectorised over points.
+    """
+    x = np.asarray(vecs, dtype=np.float64)
+    m = x.shape[1]
+    R = float(rscale)
+    r2 = (x * x).sum(axis=0)
+    r = np.sqrt(r2)
+    xs = x / R
+    rs2 = r2 / (R * R)
+    M = maxdeg
+    D = np.zeros((maxi0 + 1, M + 1, M + 1, m))
+
+    def get(i, j, k):
+        if i < 0 or j < 0 or k < 0:
+            return 0.0
+        return D[i, j, k]
+
+    for deg in range(M + 1):
+        for i in range(min(maxi0, deg) + 1):
+            for j in range(deg - i + 1):
+                k = deg - i - j
+                mi = (i, j, k)
+                if max(mi) <= 1:
+                    if deg == 0:
+                        v = 1.0 / r
+                    elif deg == 1:
+                        v = -x[mi.index(1)] / (r2 * r) * R
+                    elif deg == 2:
+                        a, b = [ax for ax in range(3) if mi[ax] == 1]
+                        v = 3.0 * x[a] * x[b] / (r2 * r2 * r) * R * R
+                    else:
+                        v = -15.0 * x[0] * x[1] * x[2] / (r2 ** 3 * r) * R ** 3
+                    D[i, j, k] = v
+                    continue
+                d = next(ax for ax in range(3) if mi[ax] >= 2)
+                e = np.zeros(m)
+                for ax in range(3):
+                    n = mi[ax]
+                    m1 = list(mi); m1[ax] -= 1
+                    m2 = list(mi); m2[ax] -= 2
+                    if ax == d:
+                        e = e - (2 * n - 1) * xs[ax] * get(*m1) - (n - 1) ** 2 * get(*m2)
+                    else:
+                        e = e - 2 * n * xs[ax] * get(*m1) - n * (n - 1) * get(*m2)
+                D[i, j, k] = e / rs2
+    return D
+
+
+def m2l_class_matrices(order, vectors, src_rscale, tgt_rscale):
+    """Dense M2L operators T[c, t, s] for translation vectors ``vectors``
+    (shape (3, nclasses), target center - source center).
+
+    T[c, t, s] = (tgt_rscale/src_rscale)^|t| * D_c[s + t], with
+    D_c = src_rscale^|mi| d^mi G(vector_c): the map sumpy applies per class
+    (translation_classes_dependent_data, preprocess, Toeplitz product and
+    postprocess; sumpy/expansion/m2l.py:363-389, 461-537, 539-558, 679-698).
+    Derivatives with mi0 = 2 follow from the Laplace projection.
+    """
+    p = order
+    ids = np.array(stored_ids(p))
+    n = len(ids)
+    D = laplace_derivatives(vectors, src_rscale, 2 * p, maxi0=1)
+    nc = D.shape[-1]
+    M = 2 * p
+    # extend to mi0 == 2 via u_(2,j,k) = -u_(0,j+2,k) - u_(0,j,k+2)
+    full = np.zeros((3, M + 3, M + 3, nc))
+    full[:2, :M + 1, :M + 1] = D
+    full[2, :M + 1, :M + 1] = -full[0, 2:M + 3, :M + 1] - full[0, :M + 1, 2:M + 3]
+    s_plus_t = ids[None, :, :] + ids[:, None, :]          # [t, s, 3]
+    T = full[s_plus_t[..., 0], s_plus_t[..., 1], s_plus_t[..., 2]]  # [t, s, nc]
+    ratio = tgt_rscale / src_rscale
+    deg_t = ids.sum(axis=1)
+    T = T * (ratio ** deg_t)[:, None, None]
+    return np.ascontiguousarray(np.moveaxis(T, -1, 0))   # [c, t, s]
+
+# }}}

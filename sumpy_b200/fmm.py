@@ -1,0 +1,508 @@
+"""Expansion wrangler with sumpy's interface, running the B200 kernels.
+
+``SumpyTreeIndependentDataForWrangler`` and ``SumpyExpansionWrangler`` keep
+the constructor and method signatures of sumpy/fmm.py:99-252 and 264-1086,
+so a boxtree-style ``drive_fmm`` (here :func:`sumpy_b200.drive.drive_fmm`)
+runs unchanged. Arrays are torch CUDA tensors; the ``actx`` arguments are
+accepted for call compatibility and ignored. Each method launches one C-ABI
+entry point (``include/sumpy_b200.h``) per tree level on the current torch
+stream, without host synchronisation.
+
+Storage is sumpy's (sumpy/fmm.py:399-485, 1093-1115): one flat FP64 array
+per expansion kind, level-major, each level a row-major
+``(nboxes_level, ncoeff)`` block.
+
+Beyond sumpy's knobs, the wrangler takes ``precision``: ``"fp64"`` (every
+stage in FP64) or ``"mixed"`` (FP32 near field with FP64 offsets and sums;
+the other stages FP64).
+"""
+from __future__ import annotations
+
+import math
+from functools import cached_property
+
+import numpy as np
+import torch
+
+from sumpy_b200 import _capi
+from sumpy_b200._capi import call, dptr, stream_ptr
+from sumpy_b200.expansion import m2l_class_matrices
+from sumpy_b200.kernel import is_scale_invariant
+
+_i32 = _capi.i32
+_i64 = _capi.i64
+_c = _capi.cint
+_d = _capi.dbl
+
+M2L_TILE = 64
+
+
+def _np_i32(a):
+    if isinstance(a, torch.Tensor):
+        a = a.detach().cpu().numpy()
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+class SumpyTreeIndependentDataForWrangler:
+    """Code-side data of the wrangler (sumpy/fmm.py:99-252)."""
+
+    def __init__(self, array_context, multipole_expansion_factory,
+                 local_expansion_factory, target_kernels, exclude_self=False,
+                 use_rscale=None, strength_usage=None, source_kernels=None):
+        if len(target_kernels) != 1:
+            raise NotImplementedError("exactly one target kernel is supported")
+        if source_kernels is not None and list(source_kernels) != list(target_kernels):
+            raise NotImplementedError("source kernels must equal the target kernel")
+        if strength_usage is not None and list(strength_usage) != [0]:
+            raise NotImplementedError("a single strength vector is supported")
+        self._setup_actx = array_context
+        self.multipole_expansion_factory = multipole_expansion_factory
+        self.local_expansion_factory = local_expansion_factory
+        self.target_kernels = list(target_kernels)
+        self.source_kernels = source_kernels
+        self.exclude_self = exclude_self
+        self.use_rscale = use_rscale
+        self.strength_usage = strength_usage
+        self._mexp = {}
+        self._lexp = {}
+
+    def get_base_kernel(self):
+        return self.target_kernels[0].get_base_kernel()
+
+    def multipole_expansion(self, order):
+        if order not in self._mexp:
+            self._mexp[order] = (self.multipole_expansion_factory(order)
+                                 if self.use_rscale is None else
+                                 self.multipole_expansion_factory(order, use_rscale=self.use_rscale))
+        return self._mexp[order]
+
+    def local_expansion(self, order):
+        if order not in self._lexp:
+            self._lexp[order] = (self.local_expansion_factory(order)
+                                 if self.use_rscale is None else
+                                 self.local_expansion_factory(order, use_rscale=self.use_rscale))
+        return self._lexp[order]
+
+
+class SumpyExpansionWrangler:
+    """B200 implementation of boxtree's ExpansionWranglerInterface with
+    sumpy's constructor (sumpy/fmm.py:304-367)."""
+
+    def __init__(self, tree_indep, traversal, dtype, fmm_level_to_order,
+                 source_extra_kwargs=None, kernel_extra_kwargs=None,
+                 self_extra_kwargs=None, translation_classes_data=None,
+                 preprocessed_mpole_dtype=None, *, _disable_translation_classes=False,
+                 precision="fp64", device=None):
+        if not callable(fmm_level_to_order):
+            raise TypeError("fmm_level_to_order not passed")
+        if np.dtype(dtype) != np.float64:
+            raise NotImplementedError("the 3D Laplace wrangler computes in float64")
+        if precision not in ("fp64", "mixed"):
+            raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
+        self.tree_indep = tree_indep
+        self.traversal = traversal
+        self.tree = traversal.tree
+        self.dtype = np.dtype(dtype)
+        self.precision = precision
+        self.source_extra_kwargs = source_extra_kwargs or {}
+        self.kernel_extra_kwargs = kernel_extra_kwargs or {}
+        self.self_extra_kwargs = self_extra_kwargs or {}
+        self.device = torch.device(device if device is not None else "cuda")
+
+        base_kernel = tree_indep.get_base_kernel()
+        kernel_arg_set = frozenset(self.kernel_extra_kwargs.items())
+        self.level_orders = [fmm_level_to_order(base_kernel, kernel_arg_set, self.tree, lev)
+                             for lev in range(self.tree.nlevels)]
+        for o in self.level_orders:
+            if not 0 <= o <= 16:
+                raise ValueError(f"expansion order {o} outside [0, 16]")
+
+        if _disable_translation_classes:
+            raise NotImplementedError("M2L always uses translation classes on the B200 path")
+        if translation_classes_data is None:
+            from sumpy_b200.tree import TranslationClassesBuilder
+            translation_classes_data, _ = TranslationClassesBuilder()(
+                None, traversal, self.tree, is_translation_per_level=True)
+        self.translation_classes_data = translation_classes_data
+        self.supports_translation_classes = True
+
+        self._devcache = {}
+        self._m2l_plans = {}
+        self._m2l_mats = {}
+
+    # {{{ geometry, storage
+
+    def level_to_rscale(self, level):
+        """sumpy/fmm.py:369-386: rscale = root_extent * 2^-level * 2 / order."""
+        return self.tree.root_extent * (2 ** -level) * 2 / self.level_orders[level]
+
+    @cached_property
+    def tree_level_start_box_nrs(self):
+        return np.asarray(self.tree.level_start_box_nrs, dtype=np.int64)
+
+    def _expansions_level_starts(self, order_to_size):
+        lsb = self.tree_level_start_box_nrs
+        res = [0]
+        for lev in range(self.tree.nlevels):
+            res.append(res[-1] + order_to_size(self.level_orders[lev]) * int(lsb[lev + 1] - lsb[lev]))
+        return res
+
+    @cached_property
+    def _mpole_level_starts(self):
+        return self._expansions_level_starts(
+            lambda o: len(self.tree_indep.multipole_expansion(o)))
+
+    @cached_property
+    def _local_level_starts(self):
+        return self._expansions_level_starts(
+            lambda o: len(self.tree_indep.local_expansion(o)))
+
+    def multipole_expansions_level_starts(self):
+        return self._mpole_level_starts
+
+    def local_expansions_level_starts(self):
+        return self._local_level_starts
+
+    def multipole_expansion_zeros(self, actx=None):
+        return torch.zeros(self._mpole_level_starts[-1], dtype=torch.float64, device=self.device)
+
+    def local_expansion_zeros(self, actx=None):
+        return torch.zeros(self._local_level_starts[-1], dtype=torch.float64, device=self.device)
+
+    def output_zeros(self, actx=None):
+        return [torch.zeros(self.tree.ntargets, dtype=torch.float64, device=self.device)
+                for _ in self.tree_indep.target_kernels]
+
+    def _view(self, exps, level, starts):
+        a, b = starts[level], starts[level + 1]
+        lsb = self.tree_level_start_box_nrs
+        nb = int(lsb[level + 1] - lsb[level])
+        return int(lsb[level]), exps[a:b].view(nb, -1) if nb else exps[a:b]
+
+    def multipole_expansions_view(self, mpole_exps, level):
+        return self._view(mpole_exps, level, self._mpole_level_starts)
+
+    def local_expansions_view(self, local_exps, level):
+        return self._view(local_exps, level, self._local_level_starts)
+
+    def _dev(self, arr, dtype=torch.int32):
+        """Device copy of a host array (cached per array object)."""
+        if isinstance(arr, torch.Tensor):
+            if arr.device.type == "cuda":
+                return arr if arr.dtype == dtype else arr.to(dtype)
+            return arr.to(self.device, dtype)
+        key = id(arr)
+        hit = self._devcache.get(key)
+        if hit is not None and hit[0] is arr:
+            return hit[1]
+        t = torch.as_tensor(np.ascontiguousarray(arr)).to(self.device, dtype)
+        self._devcache[key] = (arr, t)
+        return t
+
+    @cached_property
+    def _geom(self):
+        t = self.tree
+        f64 = torch.float64
+        g = {
+            "centers": self._dev(t.box_centers, f64),
+            "sources": self._dev(t.sources, f64),
+            "targets": self._dev(t.targets, f64),
+            "bss": self._dev(t.box_source_starts),
+            "bsc": self._dev(t.box_source_counts_nonchild),
+            "bts": self._dev(t.box_target_starts),
+            "btc": self._dev(t.box_target_counts_nonchild),
+            "child": self._dev(t.box_child_ids),
+            "parent": self._dev(t.box_parent_ids),
+            "tts": (self._dev(t.target_to_source)
+                    if self.tree_indep.exclude_self else None),
+        }
+        if self.tree_indep.exclude_self and t.target_to_source is None:
+            raise ValueError("exclude_self needs a tree whose sources are its targets")
+        return g
+
+    @property
+    def _scale(self):
+        return self.tree_indep.target_kernels[0].global_scaling_const
+
+    # }}}
+
+    def reorder_sources(self, source_array):
+        idx = self._dev(self.tree.user_source_ids, torch.int64)
+        return source_array[idx]
+
+    def reorder_potentials(self, potentials):
+        idx = self._dev(self.tree.sorted_target_ids, torch.int64)
+        return [p[idx] for p in potentials]
+
+    def distribute_source_weights(self, src_weight_vecs, src_idx_all_ranks=None):
+        return src_weight_vecs
+
+    def gather_potential_results(self, potentials, tgt_idx_all_ranks=None):
+        return potentials
+
+    def finalize_potentials(self, actx, potentials):
+        return potentials
+
+    def _weights(self, src_weight_vecs):
+        (w,) = src_weight_vecs
+        if w.dtype != torch.float64 or not w.is_contiguous():
+            w = w.to(torch.float64).contiguous()
+        return w
+
+    # {{{ stages
+
+    def form_multipoles(self, actx, level_start_source_box_nrs, source_boxes, src_weight_vecs):
+        mpoles = self.multipole_expansion_zeros(actx)
+        lss = _np_i32(level_start_source_box_nrs)
+        boxes = self._dev(source_boxes)
+        g = self._geom
+        w = self._weights(src_weight_vecs)
+        st = stream_ptr()
+        for lev in range(self.tree.nlevels):
+            a, b = int(lss[lev]), int(lss[lev + 1])
+            if a == b:
+                continue
+            base, view = self.multipole_expansions_view(mpoles, lev)
+            call("sumpy_p2e_from_single_box_f64", _c(self.level_orders[lev]),
+                 _d(self.level_to_rscale(lev)), _i32(b - a), dptr(boxes[a:b]),
+                 dptr(g["centers"]), _i64(self.tree.nboxes), dptr(g["bss"]), dptr(g["bsc"]),
+                 dptr(g["sources"]), _i64(self.tree.nsources), dptr(w), _i32(base),
+                 dptr(view), st)
+        return mpoles
+
+    def coarsen_multipoles(self, actx, level_start_source_parent_box_nrs,
+                           source_parent_boxes, mpoles):
+        lsp = _np_i32(level_start_source_parent_box_nrs)
+        boxes = self._dev(source_parent_boxes)
+        g = self._geom
+        st = stream_ptr()
+        for src_lev in range(self.tree.nlevels - 1, 2, -1):
+            tgt_lev = src_lev - 1
+            a, b = int(lsp[tgt_lev]), int(lsp[tgt_lev + 1])
+            if a == b:
+                continue
+            sbase, sview = self.multipole_expansions_view(mpoles, src_lev)
+            tbase, tview = self.multipole_expansions_view(mpoles, tgt_lev)
+            call("sumpy_e2e_from_children_f64", _c(self.level_orders[src_lev]),
+                 _c(self.level_orders[tgt_lev]), _d(self.level_to_rscale(src_lev)),
+                 _d(self.level_to_rscale(tgt_lev)), _i32(b - a), dptr(boxes[a:b]),
+                 dptr(g["child"]), _i64(self.tree.nboxes), dptr(g["centers"]),
+                 _i64(self.tree.nboxes), _i32(sbase), dptr(sview), _i32(tbase), dptr(tview), st)
+        return mpoles
+
+    def eval_direct(self, actx, target_boxes, source_box_starts, source_box_lists,
+                    src_weight_vecs):
+        pot = self.output_zeros(actx)
+        tb = self._dev(target_boxes)
+        if tb.numel() == 0:
+            return pot
+        g = self._geom
+        w = self._weights(src_weight_vecs)
+        fn = ("sumpy_p2p_from_csr_mixed" if self.precision == "mixed"
+              else "sumpy_p2p_from_csr_f64")
+        call(fn, _i32(tb.numel()), dptr(tb), dptr(self._dev(source_box_starts)),
+             dptr(self._dev(source_box_lists)), dptr(g["bss"]), dptr(g["bsc"]),
+             dptr(g["bts"]), dptr(g["btc"]), dptr(g["sources"]), _i64(self.tree.nsources),
+             dptr(w), dptr(g["targets"]), _i64(self.tree.ntargets), dptr(g["tts"]),
+             _d(self._scale), dptr(pot[0]), stream_ptr())
+        return pot
+
+    # {{{ M2L
+
+    def _m2l_matrices(self, lev):
+        """Device tensor [nclasses, n, n] and the level's scalar factor."""
+        order = self.level_orders[lev]
+        kernel = self.tree_indep.get_base_kernel()
+        rscale = self.level_to_rscale(lev)
+        tc = self.translation_classes_data
+        ls = tc.from_sep_siblings_translation_classes_level_starts
+        vecs = tc.from_sep_siblings_translation_class_to_distance_vector[:, ls[lev]:ls[lev + 1]]
+        if is_scale_invariant(kernel):
+            # rscale^|mi| d^mi (1/r) at d = v*h with rscale = 2h/p equals
+            # (1/rscale) times the same derivatives at v*(h/rscale) with unit rscale
+            h = self.tree.root_extent * 2.0 ** -lev
+            key = (order, tuple(np.round(vecs[:, :].ravel() / h, 12)))
+            if key not in self._m2l_mats:
+                unit = m2l_class_matrices(order, vecs / rscale, 1.0, 1.0)
+                self._m2l_mats[key] = torch.as_tensor(unit).to(self.device)
+            return self._m2l_mats[key], 1.0 / rscale
+        key = ("level", lev)
+        if key not in self._m2l_mats:
+            mats = m2l_class_matrices(order, vecs, rscale, rscale)
+            self._m2l_mats[key] = torch.as_tensor(mats).to(self.device)
+        return self._m2l_mats[key], 1.0
+
+    def _m2l_plan(self, lev, tgt_boxes, starts, lists):
+        """Regroup one level's List-2 CSR into (tile, class) GEMM groups.
+
+        Targets are ordered by their octant in the parent, so a tile's
+        targets share the same set of valid classes."""
+        key = (lev, id(lists))
+        if key in self._m2l_plans:
+            return self._m2l_plans[key]
+        tc = self.translation_classes_data
+        cls_ls = tc.from_sep_siblings_translation_classes_level_starts
+        ncls = int(cls_ls[lev + 1] - cls_ls[lev])
+        classes = _np_i32(tc.from_sep_siblings_translation_classes)
+        tgt_boxes = _np_i32(tgt_boxes)
+        starts = np.asarray(starts, dtype=np.int64)
+        lists = _np_i32(lists)
+        counts = np.diff(starts)
+        has = counts > 0
+        tpos = np.nonzero(has)[0]
+        if len(tpos) == 0:
+            self._m2l_plans[key] = None
+            return None
+        coords = self.tree.box_coords[:, tgt_boxes[tpos]]
+        octant = (coords[0] & 1) * 4 + (coords[1] & 1) * 2 + (coords[2] & 1)
+        order = np.lexsort((tgt_boxes[tpos], octant))
+        tpos = tpos[order]
+        ntiles = (len(tpos) + M2L_TILE - 1) // M2L_TILE
+        tile_targets = np.full(ntiles * M2L_TILE, -1, dtype=np.int32)
+        tile_targets[:len(tpos)] = tgt_boxes[tpos]
+        # entries
+        rank = np.empty(len(tgt_boxes), dtype=np.int64)
+        rank[tpos] = np.arange(len(tpos))
+        ent_tgt = np.repeat(np.arange(len(tgt_boxes)), counts)
+        e0, e1 = int(starts[0]), int(starts[-1])
+        ent_src = lists[e0:e1]
+        ent_cls = classes[e0:e1] - int(cls_ls[lev])
+        if ent_cls.size and (ent_cls.min() < 0 or ent_cls.max() >= ncls):
+            raise ValueError(f"translation class out of range on level {lev}")
+        r = rank[ent_tgt]
+        tile = r // M2L_TILE
+        slot = r % M2L_TILE
+        gkey = tile * ncls + ent_cls
+        uniq, inv = np.unique(gkey, return_inverse=True)
+        ngroups = len(uniq)
+        group_sources = np.full((ngroups, M2L_TILE), -1, dtype=np.int32)
+        group_sources[inv, slot] = ent_src
+        group_tile = uniq // ncls
+        group_class = (uniq % ncls).astype(np.int32)
+        tile_group_starts = np.searchsorted(group_tile, np.arange(ntiles + 1)).astype(np.int32)
+        dev = self.device
+        plan = {
+            "ntiles": ntiles,
+            "ngroups": ngroups,
+            "nentries": int(len(ent_src)),
+            "nclasses": ncls,
+            "tile_targets": torch.as_tensor(tile_targets).to(dev),
+            "tile_group_starts": torch.as_tensor(tile_group_starts).to(dev),
+            "group_class": torch.as_tensor(group_class).to(dev),
+            "group_sources": torch.as_tensor(group_sources.ravel()).to(dev),
+        }
+        self._m2l_plans[key] = plan
+        return plan
+
+    def multipole_to_local(self, actx, level_start_target_box_nrs, target_boxes,
+                           src_box_starts, src_box_lists, mpole_exps):
+        local_exps = self.local_expansion_zeros(actx)
+        ltb = _np_i32(level_start_target_box_nrs)
+        tboxes = _np_i32(target_boxes)
+        starts = np.asarray(src_box_starts if not isinstance(src_box_starts, torch.Tensor)
+                            else src_box_starts.cpu().numpy())
+        st = stream_ptr()
+        for lev in range(self.tree.nlevels):
+            a, b = int(ltb[lev]), int(ltb[lev + 1])
+            if a == b or starts[a] == starts[b]:
+                continue
+            plan = self._m2l_plan(lev, tboxes[a:b], starts[a:b + 1], src_box_lists)
+            if plan is None:
+                continue
+            mats, mscale = self._m2l_matrices(lev)
+            sbase, sview = self.multipole_expansions_view(mpole_exps, lev)
+            tbase, tview = self.local_expansions_view(local_exps, lev)
+            self._launch_m2l(lev, plan, mats, mscale, sbase, sview, tbase, tview, st)
+        return local_exps
+
+    def _launch_m2l(self, lev, plan, mats, mscale, sbase, sview, tbase, tview, st):
+        call("sumpy_m2l_translation_classes_f64", _c(self.level_orders[lev]),
+             _i32(plan["ntiles"]), _i32(M2L_TILE), dptr(plan["tile_targets"]),
+             dptr(plan["tile_group_starts"]), dptr(plan["group_class"]),
+             dptr(plan["group_sources"]), _i32(plan["nclasses"]), dptr(mats), _d(mscale),
+             _i32(sbase), dptr(sview), _i32(tbase), dptr(tview), st)
+
+    # }}}
+
+    def eval_multipoles(self, actx, target_boxes_by_source_level, source_boxes_by_level,
+                        mpole_exps):
+        pot = self.output_zeros(actx)
+        g = self._geom
+        st = stream_ptr()
+        for lev, ssn in enumerate(source_boxes_by_level):
+            tb = target_boxes_by_source_level[lev]
+            if len(tb) == 0:
+                continue
+            sbase, sview = self.multipole_expansions_view(mpole_exps, lev)
+            tbd = self._dev(tb)
+            call("sumpy_e2p_from_csr_f64", _c(self.level_orders[lev]),
+                 _d(self.level_to_rscale(lev)), _i32(tbd.numel()), dptr(tbd),
+                 dptr(self._dev(ssn.starts)), dptr(self._dev(ssn.lists)), dptr(g["centers"]),
+                 _i64(self.tree.nboxes), _i32(sbase), dptr(sview), dptr(g["bts"]),
+                 dptr(g["btc"]), dptr(g["targets"]), _i64(self.tree.ntargets),
+                 _d(self._scale), dptr(pot[0]), st)
+        return pot
+
+    def form_locals(self, actx, level_start_target_or_target_parent_box_nrs,
+                    target_or_target_parent_boxes, starts, lists, src_weight_vecs):
+        local_exps = self.local_expansion_zeros(actx)
+        lt = _np_i32(level_start_target_or_target_parent_box_nrs)
+        starts_h = np.asarray(starts if not isinstance(starts, torch.Tensor)
+                              else starts.cpu().numpy())
+        boxes = self._dev(target_or_target_parent_boxes)
+        starts_d = self._dev(starts)
+        lists_d = self._dev(lists)
+        g = self._geom
+        w = self._weights(src_weight_vecs)
+        st = stream_ptr()
+        for lev in range(self.tree.nlevels):
+            a, b = int(lt[lev]), int(lt[lev + 1])
+            if a == b or starts_h[a] == starts_h[b]:
+                continue
+            tbase, tview = self.local_expansions_view(local_exps, lev)
+            call("sumpy_p2e_from_csr_f64", _c(self.level_orders[lev]),
+                 _d(self.level_to_rscale(lev)), _i32(b - a), dptr(boxes[a:b]),
+                 dptr(starts_d[a:b + 1]), dptr(lists_d), dptr(g["centers"]),
+                 _i64(self.tree.nboxes), dptr(g["bss"]), dptr(g["bsc"]), dptr(g["sources"]),
+                 _i64(self.tree.nsources), dptr(w), _i32(tbase), dptr(tview), st)
+        return local_exps
+
+    def refine_locals(self, actx, level_start_target_or_target_parent_box_nrs,
+                      target_or_target_parent_boxes, local_exps):
+        lt = _np_i32(level_start_target_or_target_parent_box_nrs)
+        boxes = self._dev(target_or_target_parent_boxes)
+        g = self._geom
+        st = stream_ptr()
+        for tgt_lev in range(1, self.tree.nlevels):
+            a, b = int(lt[tgt_lev]), int(lt[tgt_lev + 1])
+            if a == b:
+                continue
+            src_lev = tgt_lev - 1
+            sbase, sview = self.local_expansions_view(local_exps, src_lev)
+            tbase, tview = self.local_expansions_view(local_exps, tgt_lev)
+            call("sumpy_e2e_from_parent_f64", _c(self.level_orders[src_lev]),
+                 _c(self.level_orders[tgt_lev]), _d(self.level_to_rscale(src_lev)),
+                 _d(self.level_to_rscale(tgt_lev)), _i32(b - a), dptr(boxes[a:b]),
+                 dptr(g["parent"]), dptr(g["centers"]), _i64(self.tree.nboxes),
+                 _i32(sbase), dptr(sview), _i32(tbase), dptr(tview), st)
+        return local_exps
+
+    def eval_locals(self, actx, level_start_target_box_nrs, target_boxes, local_exps):
+        pot = self.output_zeros(actx)
+        ltb = _np_i32(level_start_target_box_nrs)
+        boxes = self._dev(target_boxes)
+        g = self._geom
+        st = stream_ptr()
+        for lev in range(self.tree.nlevels):
+            a, b = int(ltb[lev]), int(ltb[lev + 1])
+            if a == b:
+                continue
+            sbase, sview = self.local_expansions_view(local_exps, lev)
+            call("sumpy_e2p_from_single_box_f64", _c(self.level_orders[lev]),
+                 _d(self.level_to_rscale(lev)), _i32(b - a), dptr(boxes[a:b]),
+                 dptr(g["centers"]), _i64(self.tree.nboxes), _i32(sbase), dptr(sview),
+                 dptr(g["bts"]), dptr(g["btc"]), dptr(g["targets"]), _i64(self.tree.ntargets),
+                 _d(self._scale), dptr(pot[0]), st)
+        return pot
+
+    # }}}

@@ -1,0 +1,48 @@
+"""All-pairs P2P (sumpy/p2p.py:215-285) on the GPU.
+
+``P2P(target_kernels, exclude_self)(actx, targets, sources, (strength,))``
+returns ``[potential]`` like sumpy's, computed by the FP64 CUDA kernel
+``sumpy_p2p_direct_f64``. sumpy's FMM tests use this as the accuracy
+reference (sumpy/test/test_fmm.py:284-286).
+"""
+from __future__ import annotations
+
+import torch
+
+from sumpy_b200 import _capi
+from sumpy_b200._capi import call, dptr, stream_ptr
+
+
+def _soa(x, device):
+    t = torch.as_tensor(x, dtype=torch.float64)
+    if t.dim() != 2 or t.shape[0] != 3:
+        raise ValueError("points must have shape (3, n)")
+    return t.to(device).contiguous()
+
+
+class P2P:
+    def __init__(self, target_kernels, exclude_self=False, strength_usage=None,
+                 source_kernels=None, value_dtypes=None, name=None):
+        if len(target_kernels) != 1:
+            raise NotImplementedError("exactly one target kernel is supported")
+        self.target_kernels = list(target_kernels)
+        self.exclude_self = exclude_self
+
+    def __call__(self, actx, targets, sources, strength, target_to_source=None,
+                 device="cuda", **kwargs):
+        dev = torch.device(device)
+        t = _soa(targets, dev)
+        s = _soa(sources, dev)
+        (q,) = strength
+        q = torch.as_tensor(q, dtype=torch.float64).to(dev).contiguous()
+        tts = None
+        if self.exclude_self:
+            if target_to_source is None:
+                raise ValueError("exclude_self needs target_to_source")
+            tts = torch.as_tensor(target_to_source).to(dev, torch.int32).contiguous()
+        out = torch.empty(t.shape[1], dtype=torch.float64, device=dev)
+        scale = self.target_kernels[0].global_scaling_const
+        call("sumpy_p2p_direct_f64", _capi.i64(t.shape[1]), dptr(t), _capi.i64(t.shape[1]),
+             _capi.i64(s.shape[1]), dptr(s), _capi.i64(s.shape[1]), dptr(q), dptr(tts),
+             _capi.dbl(scale), dptr(out), stream_ptr())
+        return [out]
