@@ -172,6 +172,35 @@ int sumpy_m2l_translation_classes_f64(
     double matrix_scale, int32_t src_base_ibox, const double *src_expansions,
     int32_t tgt_base_ibox, double *tgt_expansions, void *stream);
 
+/* M2L pre-processing for the tensor-core form: split FP64 values into two
+ * TF32-representable FP32 planes, x ~ hi + lo (hi = tf32(x), lo =
+ * tf32(x - hi), round to nearest), zero-padded from [nmat][rows][cols] to
+ * [nmat][rows_pad][cols_pad]. Plays the role of sumpy's
+ * M2LPreprocessMultipole (sumpy/e2e.py:676-760), which recasts multipoles
+ * into the form the translation consumes; also used once per order on the
+ * class operators. */
+int sumpy_split_tf32x2(
+    int64_t nmat, int32_t rows, int32_t cols, const double *in,
+    int32_t rows_pad, int32_t cols_pad, float *hi, float *lo, void *stream);
+
+/* M2L for one level on the tcgen05 tensor cores, split-FP32 (3xTF32):
+ * same schedule and result contract as sumpy_m2l_translation_classes_f64
+ * (replacing sumpy/e2e.py:310-558 and sumpy/fmm.py:798-920) with
+ * tile_width 128, operators given as TF32 planes mats_hi/mats_lo
+ * [nclasses][rows_pad][k_pad] and the level's multipoles as planes
+ * src_hi/src_lo [nboxes_level][k_pad] (both from sumpy_split_tf32x2).
+ * rows_pad is a multiple of 128, k_pad a multiple of 32. Products
+ * hi*hi + hi*lo + lo*hi accumulate in FP32 (tensor memory) over the tile's
+ * groups; tgt[t] += matrix_scale * result in FP64. status (device int32,
+ * may be NULL) receives a nonzero code if a bounded internal wait expired. */
+int sumpy_m2l_translation_classes_tf32x3(
+    int order, int32_t ntiles, int32_t tile_width, const int32_t *tile_targets,
+    const int32_t *tile_group_starts, const int32_t *group_class,
+    const int32_t *group_sources, int32_t nclasses, const float *mats_hi,
+    const float *mats_lo, int32_t rows_pad, int32_t k_pad, double matrix_scale,
+    int32_t src_base_ibox, const float *src_hi, const float *src_lo,
+    int32_t tgt_base_ibox, double *tgt_expansions, int32_t *status, void *stream);
+
 /* ------------------------------------------------------------------ */
 /* E2P                                                                  */
 /* ------------------------------------------------------------------ */

@@ -1,0 +1,378 @@
+// M2L per translation class on the 5th-generation tensor cores (tcgen05),
+// split-FP32 ("3xTF32") with FP32 accumulation in tensor memory.
+//
+// Same contract as m2l.cu (one dense operator T_c per class, applied to the
+// gathered source multipoles of a tile of target boxes), with each FP64
+// operand x split as x ~ hi + lo, hi = tf32(x), lo = tf32(x - hi), and
+//     T*M ~ T_hi*M_hi + T_hi*M_lo + T_lo*M_hi
+// (the split-precision scheme of Ootomo & Yokota, "Recovering single
+// precision accuracy from Tensor Cores while surpassing the FP32
+// theoretical peak performance", 2022), accumulated in FP32 over all
+// groups of the tile and added to the FP64 local expansions once.
+//
+// CTA = 128 threads, one output tile of 128 coefficient rows x 128 target
+// slots (the MMA is M=128, N=128, K=8 per instruction). Operand tiles are
+// K-major with the 128-byte swizzle: each row (a coefficient row of T_c, or
+// the coefficients of one source multipole) holds 32 fp32 of K in 128
+// bytes; 8 rows form a 1024-byte swizzle atom. K is streamed in chunks of
+// 32 through a 3-stage shared-memory ring filled with cp.async by all
+// threads; one thread issues the 12 MMAs of a chunk (4 K-steps x 3
+// products) and commits them to the stage's mbarrier, which the producers
+// wait on before refilling the stage. All waits are bounded by a clock
+// budget; on expiry the kernel records an error in *status, drains its
+// copies, frees its tensor memory and returns.
+#include <algorithm>
+#include <cstdint>
+#include <string>
+
+#include "common.cuh"
+
+namespace sumpy {
+namespace {
+
+constexpr int TC_TW = 128;      // target slots per tile (MMA N)
+constexpr int TC_M = 128;       // coefficient rows per CTA (MMA M)
+constexpr int TC_KC = 32;       // fp32 K elements per 128-byte row
+constexpr int TC_STAGES = 3;
+constexpr int TC_THREADS = 128;
+constexpr int PLANE = TC_M * 128;          // bytes of one 128 x 32 fp32 operand tile
+constexpr int STAGE = 4 * PLANE;           // A_hi, A_lo, B_hi, B_lo
+constexpr int TC_SMEM = TC_STAGES * STAGE + 1024 /* alignment slack */ + 256 /* barriers */;
+constexpr uint32_t TMEM_COLS = 128;
+constexpr long long WAIT_CYCLES = 4000000000LL;  // ~2 s at 2 GHz
+
+enum { ST_TIMEOUT_MMA = 1, ST_TIMEOUT_DRAIN = 2 };
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, uint32_t src_bytes)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src),
+                 "r"(src_bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(addr), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t addr, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// bounded wait; false on timeout
+__device__ bool mbar_wait(uint32_t addr, uint32_t parity)
+{
+    const long long t0 = clock64();
+    while (!mbar_try_wait(addr, parity)) {
+        if (clock64() - t0 > WAIT_CYCLES) return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row atoms
+// 1024 bytes apart (stride byte offset), descriptor version 1.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3fff);
+    d |= (uint64_t)1 << 16;                 // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;       // stride byte offset
+    d |= (uint64_t)1 << 46;                 // version
+    d |= (uint64_t)2 << 61;                 // 128-byte swizzle
+    return d;
+}
+
+// Instruction descriptor: D f32, A/B tf32, both K-major, N = 128, M = 128.
+constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_TW >> 3) << 17) |
+                           ((uint32_t)(TC_M >> 4) << 24);
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t acc)
+{
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(tmem),
+        "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t mbar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mbar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+        "%12, %13, %14, %15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+struct TcArgs {
+    int n, rows_pad, k_pad;
+    const int32_t *tile_targets, *tile_group_starts, *group_class, *group_sources;
+    const float *mats_hi, *mats_lo;
+    double scale;
+    int32_t sbase;
+    const float *src_hi, *src_lo;
+    int32_t tbase;
+    double *tgt;
+    int32_t *status;
+};
+
+// Fill one stage: A planes from T_c rows [row0, row0+128) x K [k0, k0+32),
+// B planes from the 128 gathered source multipoles (zeros for empty slots).
+__device__ __forceinline__ void load_stage(const TcArgs &a, uint32_t st, int g, int k0, int row0)
+{
+    const int cls = a.group_class[g];
+    const int32_t *gs = a.group_sources + (int64_t)g * TC_TW;
+    for (int c = threadIdx.x; c < TC_M * 8; c += TC_THREADS) {
+        const int r = c >> 3, q = c & 7;
+        const uint32_t dst = r * 128 + ((q ^ (r & 7)) << 4);
+        const int64_t off = ((int64_t)cls * a.rows_pad + row0 + r) * a.k_pad + k0 + 4 * q;
+        cp_async16(st + dst, a.mats_hi + off, 16);
+        cp_async16(st + PLANE + dst, a.mats_lo + off, 16);
+    }
+    for (int c = threadIdx.x; c < TC_TW * 8; c += TC_THREADS) {
+        const int slot = c >> 3, q = c & 7;
+        const int32_t s = gs[slot];
+        const uint32_t dst = slot * 128 + ((q ^ (slot & 7)) << 4);
+        const int64_t off = (int64_t)(s >= 0 ? s - a.sbase : 0) * a.k_pad + k0 + 4 * q;
+        const uint32_t bytes = s >= 0 ? 16u : 0u;
+        cp_async16(st + 2 * PLANE + dst, a.src_hi + off, bytes);
+        cp_async16(st + 3 * PLANE + dst, a.src_lo + off, bytes);
+    }
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 1) m2l_tf32x3_kernel(TcArgs a)
+{
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw = smem_addr(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;          // 1024-byte aligned stages
+    uint8_t *base_ptr = smem_raw + (base - raw);
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(base_ptr + TC_STAGES * STAGE);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + TC_STAGES);
+    const uint32_t mbar0 = smem_addr(mbar);
+
+    const int tile = blockIdx.x;
+    const int row0 = blockIdx.y * TC_M;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                         smem_addr(tmem_slot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < TC_STAGES; ++s) mbar_init(mbar0 + 8 * s, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    const int g0 = a.tile_group_starts[tile], g1 = a.tile_group_starts[tile + 1];
+    const int nkc = a.k_pad / TC_KC;
+    const int total = (g1 - g0) * nkc;
+    bool failed = false;
+
+    // always commit STAGES-1 groups so that wait_group<STAGES-1> in the loop
+    // covers the current iteration even when total < STAGES-1
+    for (int it = 0; it < TC_STAGES - 1; ++it) {
+        if (it < total)
+            load_stage(a, base + (it % TC_STAGES) * STAGE, g0 + it / nkc, (it % nkc) * TC_KC, row0);
+        cp_async_commit();
+    }
+    for (int it = 0; it < total; ++it) {
+        const int pre = it + TC_STAGES - 1;
+        if (pre < total) {
+            const int ps = pre % TC_STAGES;
+            bool ok = true;
+            if (pre >= TC_STAGES) ok = mbar_wait(mbar0 + 8 * ps, ((pre / TC_STAGES) - 1) & 1);
+            if (__syncthreads_or(!ok)) { failed = true; break; }
+            load_stage(a, base + ps * STAGE, g0 + pre / nkc, (pre % nkc) * TC_KC, row0);
+        }
+        cp_async_commit();
+        cp_async_wait<TC_STAGES - 1>();
+        fence_proxy_async();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tc_fence_after();
+            const uint32_t st = base + (it % TC_STAGES) * STAGE;
+            const uint64_t ah = sw128_desc(st), al = sw128_desc(st + PLANE);
+            const uint64_t bh = sw128_desc(st + 2 * PLANE), bl = sw128_desc(st + 3 * PLANE);
+#pragma unroll
+            for (int k = 0; k < TC_KC / 8; ++k) {
+                const uint64_t ko = (uint64_t)(k * 32 >> 4);  // 8 fp32 = 32 bytes along K
+                mma_tf32(tmem, ah + ko, bh + ko, (it > 0 || k > 0) ? 1u : 0u);
+                mma_tf32(tmem, ah + ko, bl + ko, 1u);
+                mma_tf32(tmem, al + ko, bh + ko, 1u);
+            }
+            mma_commit(mbar0 + 8 * (it % TC_STAGES));
+        }
+    }
+
+    if (!failed && total > 0) {
+        const int last = total - 1;
+        const bool ok = mbar_wait(mbar0 + 8 * (last % TC_STAGES), (last / TC_STAGES) & 1);
+        if (__syncthreads_or(!ok)) failed = true;
+    }
+    if (failed) {
+        if (threadIdx.x == 0 && a.status) atomicExch(a.status, ST_TIMEOUT_MMA);
+        cp_async_wait_all();
+        // let any MMA still reading the stages finish before the memory is released
+        for (int s = 0; s < TC_STAGES; ++s) {
+            const long long t0 = clock64();
+            while (clock64() - t0 < 1000000) {}
+        }
+    } else if (total > 0) {
+        tc_fence_after();
+        const int row = row0 + warp * 32 + lane;
+#pragma unroll 1
+        for (int c0 = 0; c0 < TC_TW; c0 += 16) {
+            uint32_t r[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c0, r);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int32_t t = a.tile_targets[(int64_t)tile * TC_TW + c0 + j];
+                if (t >= 0 && row < a.n)
+                    a.tgt[(int64_t)(t - a.tbase) * a.n + row] += a.scale * (double)__uint_as_float(r[j]);
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TMEM_COLS)
+                     : "memory");
+    }
+}
+
+__device__ __forceinline__ float tf32_rna(float x)
+{
+    uint32_t u;
+    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(u) : "f"(x));
+    return __uint_as_float(u);
+}
+
+__global__ void split_tf32x2_kernel(int64_t nmat, int rows, int cols, const double *__restrict__ in,
+                                    int rows_pad, int cols_pad, float *__restrict__ hi,
+                                    float *__restrict__ lo)
+{
+    const int64_t total = nmat * rows_pad * cols_pad;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int c = (int)(e % cols_pad);
+        const int64_t mr = e / cols_pad;
+        const int r = (int)(mr % rows_pad);
+        const int64_t m = mr / rows_pad;
+        const double v = (r < rows && c < cols) ? in[(m * rows + r) * cols + c] : 0.0;
+        const float h = tf32_rna((float)v);
+        hi[e] = h;
+        lo[e] = tf32_rna((float)(v - (double)h));
+    }
+}
+
+}  // namespace
+}  // namespace sumpy
+
+using namespace sumpy;
+
+extern "C" {
+
+int sumpy_split_tf32x2(int64_t nmat, int32_t rows, int32_t cols, const double *in,
+                       int32_t rows_pad, int32_t cols_pad, float *hi, float *lo, void *stream)
+{
+    if (nmat < 0 || rows < 0 || cols < 0 || rows_pad < rows || cols_pad < cols)
+        return bad_arg("split_tf32x2: bad sizes");
+    if (nmat == 0 || rows_pad == 0 || cols_pad == 0) return SUMPY_OK;
+    if ((rows > 0 && cols > 0 && !in) || !hi || !lo) return bad_arg("split_tf32x2: null pointer");
+    const int64_t total = nmat * rows_pad * cols_pad;
+    const int64_t blocks = std::min<int64_t>((total + 255) / 256, 148 * 16);
+    split_tf32x2_kernel<<<(unsigned)blocks, 256, 0, as_stream(stream)>>>(nmat, rows, cols, in, rows_pad,
+                                                                        cols_pad, hi, lo);
+    return check_launch("split_tf32x2_kernel");
+}
+
+int sumpy_m2l_translation_classes_tf32x3(
+    int order, int32_t ntiles, int32_t tile_width, const int32_t *tile_targets,
+    const int32_t *tile_group_starts, const int32_t *group_class, const int32_t *group_sources,
+    int32_t nclasses, const float *mats_hi, const float *mats_lo, int32_t rows_pad, int32_t k_pad,
+    double matrix_scale, int32_t src_base_ibox, const float *src_hi, const float *src_lo,
+    int32_t tgt_base_ibox, double *tgt_expansions, int32_t *status, void *stream)
+{
+    if (order < 0 || order > SUMPY_MAX_ORDER) {
+        set_last_error("m2l_tf32x3: unsupported order");
+        return SUMPY_EUNSUPPORTED;
+    }
+    const int n = ncoeff_of(order);
+    if (tile_width != TC_TW) return bad_arg("m2l_tf32x3: tile_width must be 128");
+    if (rows_pad < n || rows_pad % TC_M) return bad_arg("m2l_tf32x3: rows_pad must be a multiple of 128 >= ncoeff");
+    if (k_pad < n || k_pad % TC_KC) return bad_arg("m2l_tf32x3: k_pad must be a multiple of 32 >= ncoeff");
+    if (ntiles < 0 || nclasses < 0) return bad_arg("m2l_tf32x3: negative size");
+    if (ntiles == 0) return SUMPY_OK;
+    if (!tile_targets || !tile_group_starts || !group_class || !group_sources || !mats_hi ||
+        !mats_lo || !src_hi || !src_lo || !tgt_expansions)
+        return bad_arg("m2l_tf32x3: null pointer argument");
+    if ((reinterpret_cast<uintptr_t>(mats_hi) | reinterpret_cast<uintptr_t>(mats_lo) |
+         reinterpret_cast<uintptr_t>(src_hi) | reinterpret_cast<uintptr_t>(src_lo)) & 15)
+        return bad_arg("m2l_tf32x3: operand planes must be 16-byte aligned");
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return bad_arg("m2l_tf32x3: no device");
+    static bool attr_set[64] = {};
+    if (!attr_set[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(m2l_tf32x3_kernel,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+        if (e != cudaSuccess) {
+            set_last_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+            return SUMPY_ELAUNCH;
+        }
+        attr_set[dev] = true;
+    }
+    TcArgs a;
+    a.n = n; a.rows_pad = rows_pad; a.k_pad = k_pad;
+    a.tile_targets = tile_targets; a.tile_group_starts = tile_group_starts;
+    a.group_class = group_class; a.group_sources = group_sources;
+    a.mats_hi = mats_hi; a.mats_lo = mats_lo; a.scale = matrix_scale;
+    a.sbase = src_base_ibox; a.src_hi = src_hi; a.src_lo = src_lo;
+    a.tbase = tgt_base_ibox; a.tgt = tgt_expansions; a.status = status;
+    dim3 grid(ntiles, (n + TC_M - 1) / TC_M);
+    m2l_tf32x3_kernel<<<grid, TC_THREADS, TC_SMEM, as_stream(stream)>>>(a);
+    return check_launch("m2l_tf32x3_kernel");
+}
+
+}  // extern "C"

@@ -14,7 +14,8 @@ per expansion kind, level-major, each level a row-major
 
 Beyond sumpy's knobs, the wrangler takes ``precision``: ``"fp64"`` (every
 stage in FP64) or ``"mixed"`` (FP32 near field with FP64 offsets and sums;
-the other stages FP64).
+M2L as split-FP32 (3xTF32) GEMMs on the tcgen05 tensor cores with FP32
+accumulation and FP64 results; the other stages FP64).
 """
 from __future__ import annotations
 
@@ -34,7 +35,8 @@ _i64 = _capi.i64
 _c = _capi.cint
 _d = _capi.dbl
 
-M2L_TILE = 64
+M2L_TILE = 64          # FP64 GEMM tile (target boxes)
+M2L_TILE_TC = 128      # tensor-core tile (MMA N)
 
 
 def _np_i32(a):
@@ -129,6 +131,9 @@ class SumpyExpansionWrangler:
         self._devcache = {}
         self._m2l_plans = {}
         self._m2l_mats = {}
+        self._m2l_tc_mats = {}
+        self._m2l_ws = None
+        self._status = torch.zeros(1, dtype=torch.int32, device=self.device)
 
     # {{{ geometry, storage
 
@@ -332,12 +337,13 @@ class SumpyExpansionWrangler:
             self._m2l_mats[key] = torch.as_tensor(mats).to(self.device)
         return self._m2l_mats[key], 1.0
 
-    def _m2l_plan(self, lev, tgt_boxes, starts, lists):
+    def _m2l_plan(self, lev, tgt_boxes, starts, lists, tile=M2L_TILE):
         """Regroup one level's List-2 CSR into (tile, class) GEMM groups.
 
         Targets are ordered by their octant in the parent, so a tile's
         targets share the same set of valid classes."""
-        key = (lev, id(lists))
+        M2L_TILE = tile
+        key = (lev, id(lists), tile)
         if key in self._m2l_plans:
             return self._m2l_plans[key]
         tc = self.translation_classes_data
@@ -402,17 +408,22 @@ class SumpyExpansionWrangler:
         starts = np.asarray(src_box_starts if not isinstance(src_box_starts, torch.Tensor)
                             else src_box_starts.cpu().numpy())
         st = stream_ptr()
+        tc = self.precision == "mixed"
         for lev in range(self.tree.nlevels):
             a, b = int(ltb[lev]), int(ltb[lev + 1])
             if a == b or starts[a] == starts[b]:
                 continue
-            plan = self._m2l_plan(lev, tboxes[a:b], starts[a:b + 1], src_box_lists)
+            plan = self._m2l_plan(lev, tboxes[a:b], starts[a:b + 1], src_box_lists,
+                                  M2L_TILE_TC if tc else M2L_TILE)
             if plan is None:
                 continue
             mats, mscale = self._m2l_matrices(lev)
             sbase, sview = self.multipole_expansions_view(mpole_exps, lev)
             tbase, tview = self.local_expansions_view(local_exps, lev)
-            self._launch_m2l(lev, plan, mats, mscale, sbase, sview, tbase, tview, st)
+            if tc:
+                self._launch_m2l_tc(lev, plan, mats, mscale, sbase, sview, tbase, tview, st)
+            else:
+                self._launch_m2l(lev, plan, mats, mscale, sbase, sview, tbase, tview, st)
         return local_exps
 
     def _launch_m2l(self, lev, plan, mats, mscale, sbase, sview, tbase, tview, st):
@@ -421,6 +432,55 @@ class SumpyExpansionWrangler:
              dptr(plan["tile_group_starts"]), dptr(plan["group_class"]),
              dptr(plan["group_sources"]), _i32(plan["nclasses"]), dptr(mats), _d(mscale),
              _i32(sbase), dptr(sview), _i32(tbase), dptr(tview), st)
+
+    @staticmethod
+    def _tc_pads(n):
+        return (n + 127) // 128 * 128, (n + 31) // 32 * 32
+
+    def _m2l_tc_operands(self, mats):
+        """TF32 hi/lo planes [nclasses][rows_pad][k_pad] of a class-operator set."""
+        key = mats.data_ptr()
+        hit = self._m2l_tc_mats.get(key)
+        if hit is not None:
+            return hit
+        ncls, n, _ = mats.shape
+        rp, kp = self._tc_pads(n)
+        hi = torch.empty((ncls, rp, kp), dtype=torch.float32, device=self.device)
+        lo = torch.empty_like(hi)
+        call("sumpy_split_tf32x2", _i64(ncls), _i32(n), _i32(n), dptr(mats), _i32(rp),
+             _i32(kp), dptr(hi), dptr(lo), stream_ptr())
+        self._m2l_tc_mats[key] = (hi, lo, rp, kp)
+        return self._m2l_tc_mats[key]
+
+    def _m2l_workspace(self, nboxes, kp):
+        need = nboxes * kp
+        if self._m2l_ws is None or self._m2l_ws[0].numel() < need:
+            lsb = self.tree_level_start_box_nrs
+            most = int(np.max(np.diff(lsb))) * kp
+            self._m2l_ws = (torch.empty(most, dtype=torch.float32, device=self.device),
+                            torch.empty(most, dtype=torch.float32, device=self.device))
+        return self._m2l_ws
+
+    def _launch_m2l_tc(self, lev, plan, mats, mscale, sbase, sview, tbase, tview, st):
+        hi, lo, rp, kp = self._m2l_tc_operands(mats)
+        n = sview.shape[1]
+        nb = sview.shape[0]
+        ws_hi, ws_lo = self._m2l_workspace(nb, kp)
+        # M2L pre-processing: this level's multipoles as TF32 hi/lo planes
+        call("sumpy_split_tf32x2", _i64(nb), _i32(1), _i32(n), dptr(sview), _i32(1),
+             _i32(kp), dptr(ws_hi), dptr(ws_lo), st)
+        call("sumpy_m2l_translation_classes_tf32x3", _c(self.level_orders[lev]),
+             _i32(plan["ntiles"]), _i32(M2L_TILE_TC), dptr(plan["tile_targets"]),
+             dptr(plan["tile_group_starts"]), dptr(plan["group_class"]),
+             dptr(plan["group_sources"]), _i32(plan["nclasses"]), dptr(hi), dptr(lo),
+             _i32(rp), _i32(kp), _d(mscale), _i32(sbase), dptr(ws_hi), dptr(ws_lo),
+             _i32(tbase), dptr(tview), dptr(self._status), st)
+
+    def check_status(self):
+        """Raise if a kernel reported an internal error (synchronises)."""
+        code = int(self._status.item())
+        if code:
+            raise RuntimeError(f"a tensor-core M2L wait expired (status {code})")
 
     # }}}
 

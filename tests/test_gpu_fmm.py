@@ -148,8 +148,9 @@ def test_mixed_precision_accuracy(cuda_device):
     qd = torch.as_tensor(q, device=cuda_device)
     e64 = relerr(drive_fmm(None, w64, [qd])[0].cpu(), ref.cpu())
     emx = relerr(drive_fmm(None, wmx, [qd])[0].cpu(), ref.cpu())
+    wmx.check_status()
     # FP32 rounding must stay well below the order-10 truncation error
-    assert emx < max(2 * e64, 1e-6), (e64, emx)
+    assert emx < max(1.2 * e64, 1e-6), (e64, emx)
 
 
 def test_single_box_tree(cuda_device):
@@ -173,3 +174,53 @@ def test_bad_arguments_raise(cuda_device):
         _capi.call("sumpy_p2p_from_csr_f64", _capi.i32(3), None, None, None, None, None,
                    None, None, None, _capi.i64(0), None, None, _capi.i64(0), None,
                    _capi.dbl(1.0), None, None)
+
+
+def test_split_tf32x2(cuda_device):
+    from sumpy_b200 import _capi
+    x = torch.randn(3, 5, 7, dtype=torch.float64, device=cuda_device) * 1e3
+    hi = torch.empty(3, 8, 32, dtype=torch.float32, device=cuda_device)
+    lo = torch.empty_like(hi)
+    _capi.call("sumpy_split_tf32x2", _capi.i64(3), _capi.i32(5), _capi.i32(7),
+               _capi.dptr(x), _capi.i32(8), _capi.i32(32), _capi.dptr(hi), _capi.dptr(lo),
+               _capi.stream_ptr())
+    torch.cuda.synchronize()
+    bits_hi = hi.view(torch.int32) & 0x1FFF
+    bits_lo = lo.view(torch.int32) & 0x1FFF
+    assert int(bits_hi.abs().sum()) == 0 and int(bits_lo.abs().sum()) == 0  # TF32-exact
+    rec = hi[:, :5, :7].double() + lo[:, :5, :7].double()
+    assert float(((rec - x).abs() / x.abs()).max()) < 2.0 ** -21
+    assert float(hi[:, 5:, :].abs().sum() + hi[:, :, 7:].abs().sum()) == 0.0
+
+
+@pytest.mark.parametrize("geom", list(GEOMS))
+@pytest.mark.parametrize("order", [4, 10])
+def test_tensor_core_m2l_matches_fp64(cuda_device, geom, order):
+    """3xTF32 tcgen05 M2L against the FP64 GEMM on the same multipoles."""
+    src, tgt, tree, trav, tcls, q = _setup(geom)
+    excl = tgt is None
+    w64 = make_wrangler(tree, trav, order, exclude_self=excl)
+    wtc = make_wrangler(tree, trav, order, exclude_self=excl, precision="mixed")
+    qd = w64.reorder_sources(torch.as_tensor(q, device=cuda_device))
+    mp = w64.form_multipoles(None, trav.level_start_source_box_nrs, trav.source_boxes, [qd])
+    mp = w64.coarsen_multipoles(None, trav.level_start_source_parent_box_nrs,
+                                trav.source_parent_boxes, mp)
+    args = (None, trav.level_start_target_or_target_parent_box_nrs,
+            trav.target_or_target_parent_boxes, trav.from_sep_siblings_starts,
+            trav.from_sep_siblings_lists, mp)
+    l64 = w64.multipole_to_local(*args)
+    ltc = wtc.multipole_to_local(*args)
+    wtc.check_status()
+    err = relerr(ltc.cpu(), l64.cpu())
+    assert err < 2e-6, err
+
+
+def test_mixed_fmm_matches_fp64_fmm(cuda_device):
+    src, tgt, tree, trav, tcls, q = _setup("sphere_plummer_self")
+    qd = torch.as_tensor(q, device=cuda_device)
+    w64 = make_wrangler(tree, trav, 8, exclude_self=True)
+    wmx = make_wrangler(tree, trav, 8, exclude_self=True, precision="mixed")
+    p64 = drive_fmm(None, w64, [qd])[0].cpu()
+    pmx = drive_fmm(None, wmx, [qd])[0].cpu()
+    wmx.check_status()
+    assert relerr(pmx, p64) < 1e-6
