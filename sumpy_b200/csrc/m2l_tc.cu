@@ -8,19 +8,23 @@
 // (the split-precision scheme of Ootomo & Yokota, "Recovering single
 // precision accuracy from Tensor Cores while surpassing the FP32
 // theoretical peak performance", 2022), accumulated in FP32 over all
-// groups of the tile and added to the FP64 local expansions once.
+// group (one class) of the tile, and summed over the groups in FP64.
+// Long FP32 accumulation chains in the tensor cores lose far more than
+// round-to-nearest FP32 would (measured: ~1e-5 relative after ~190 groups
+// against ~3e-7 when each group is drained to FP64), hence one
+// accumulation session per group.
 //
-// CTA = 128 threads, one output tile of 128 coefficient rows x 128 target
+// CTA = 384 threads, one output tile of 128 coefficient rows x 128 target
 // slots (the MMA is M=128, N=128, K=8 per instruction). Operand tiles are
 // K-major with the 128-byte swizzle: each row (a coefficient row of T_c, or
 // the coefficients of one source multipole) holds 32 fp32 of K in 128
 // bytes; 8 rows form a 1024-byte swizzle atom. K is streamed in chunks of
-// 32 through a 3-stage shared-memory ring filled with cp.async by all
-// threads; one thread issues the 12 MMAs of a chunk (4 K-steps x 3
-// products) and commits them to the stage's mbarrier, which the producers
-// wait on before refilling the stage. All waits are bounded by a clock
-// budget; on expiry the kernel records an error in *status, drains its
-// copies, frees its tensor memory and returns.
+// 32 through a 3-stage shared-memory ring filled with cp.async by the four
+// producer warps; one producer thread issues the 12 MMAs of a chunk (4
+// K-steps x 3 products) and commits them to the stage's mbarrier, which the
+// producers wait on before refilling the stage. All waits are bounded by a
+// clock budget; on expiry the kernel records an error in *status, drains
+// its copies, frees its tensor memory and returns.
 #include <algorithm>
 #include <cstdint>
 #include <string>
@@ -34,14 +38,16 @@ constexpr int TC_TW = 128;      // target slots per tile (MMA N)
 constexpr int TC_M = 128;       // coefficient rows per CTA (MMA M)
 constexpr int TC_KC = 32;       // fp32 K elements per 128-byte row
 constexpr int TC_STAGES = 3;
-constexpr int TC_THREADS = 128;
+constexpr int TC_PRODUCERS = 128;          // warps 0-3
+constexpr int TC_DRAINERS = 256;           // warps 4-11
+constexpr int TC_THREADS = TC_PRODUCERS + TC_DRAINERS;
 constexpr int PLANE = TC_M * 128;          // bytes of one 128 x 32 fp32 operand tile
 constexpr int STAGE = 4 * PLANE;           // A_hi, A_lo, B_hi, B_lo
 constexpr int TC_SMEM = TC_STAGES * STAGE + 1024 /* alignment slack */ + 256 /* barriers */;
-constexpr uint32_t TMEM_COLS = 128;
+constexpr uint32_t TMEM_COLS = 256;         // two 128-column accumulators
 constexpr long long WAIT_CYCLES = 4000000000LL;  // ~2 s at 2 GHz
 
-enum { ST_TIMEOUT_MMA = 1, ST_TIMEOUT_DRAIN = 2 };
+enum { ST_TIMEOUT_MMA = 1 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p)
 {
@@ -79,16 +85,6 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t addr, uint32_t parity)
         : "r"(addr), "r"(parity)
         : "memory");
     return ok != 0;
-}
-
-// bounded wait; false on timeout
-__device__ bool mbar_wait(uint32_t addr, uint32_t parity)
-{
-    const long long t0 = clock64();
-    while (!mbar_try_wait(addr, parity)) {
-        if (clock64() - t0 > WAIT_CYCLES) return false;
-    }
-    return true;
 }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
@@ -152,18 +148,19 @@ struct TcArgs {
 
 // Fill one stage: A planes from T_c rows [row0, row0+128) x K [k0, k0+32),
 // B planes from the 128 gathered source multipoles (zeros for empty slots).
+// Executed by the 128 producer threads.
 __device__ __forceinline__ void load_stage(const TcArgs &a, uint32_t st, int g, int k0, int row0)
 {
     const int cls = a.group_class[g];
     const int32_t *gs = a.group_sources + (int64_t)g * TC_TW;
-    for (int c = threadIdx.x; c < TC_M * 8; c += TC_THREADS) {
+    for (int c = threadIdx.x; c < TC_M * 8; c += TC_PRODUCERS) {
         const int r = c >> 3, q = c & 7;
         const uint32_t dst = r * 128 + ((q ^ (r & 7)) << 4);
         const int64_t off = ((int64_t)cls * a.rows_pad + row0 + r) * a.k_pad + k0 + 4 * q;
         cp_async16(st + dst, a.mats_hi + off, 16);
         cp_async16(st + PLANE + dst, a.mats_lo + off, 16);
     }
-    for (int c = threadIdx.x; c < TC_TW * 8; c += TC_THREADS) {
+    for (int c = threadIdx.x; c < TC_TW * 8; c += TC_PRODUCERS) {
         const int slot = c >> 3, q = c & 7;
         const int32_t s = gs[slot];
         const uint32_t dst = slot * 128 + ((q ^ (slot & 7)) << 4);
@@ -174,15 +171,56 @@ __device__ __forceinline__ void load_stage(const TcArgs &a, uint32_t st, int g, 
     }
 }
 
+// barrier 1 over the producer warps only, OR-reducing a flag
+__device__ __forceinline__ bool producers_sync_or(bool v)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n"
+        " bar.red.or.pred p, 1, %2, q;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(r)
+        : "r"((uint32_t)v), "n"(TC_PRODUCERS)
+        : "memory");
+    return r != 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t addr)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(addr) : "memory");
+}
+
+// bounded wait that also gives up when another thread has aborted
+__device__ bool mbar_wait_or_abort(uint32_t addr, uint32_t parity, volatile int *abort_flag)
+{
+    const long long t0 = clock64();
+    while (!mbar_try_wait(addr, parity)) {
+        if (*abort_flag) return false;
+        if (clock64() - t0 > WAIT_CYCLES) {
+            *abort_flag = 1;
+            return false;
+        }
+    }
+    return true;
+}
+
+// Warp roles: warps 0-3 produce (cp.async into the stage ring; thread 0 also
+// issues the MMAs), warps 4-11 drain. Each group's product accumulates in
+// one of two TMEM accumulators (128 columns each) and is drained into FP64
+// registers of the draining warps right after the group, while the next
+// group accumulates in the other one: no FP32 sum spans more than one group.
+// Draining warp w covers TMEM lanes 32*(w%4).. and 64 of the 128 columns.
 __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tf32x3_kernel(TcArgs a)
 {
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_addr(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;          // 1024-byte aligned stages
     uint8_t *base_ptr = smem_raw + (base - raw);
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(base_ptr + TC_STAGES * STAGE);
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + TC_STAGES);
-    const uint32_t mbar0 = smem_addr(mbar);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(base_ptr + TC_STAGES * STAGE);
+    // bars[0..2] stage MMA done, [3..4] accumulator full, [5..6] accumulator empty
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 8);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+    const uint32_t bar0 = smem_addr(bars);
+    const uint32_t stage_bar = bar0, full_bar = bar0 + 8 * 3, empty_bar = bar0 + 8 * 5;
 
     const int tile = blockIdx.x;
     const int row0 = blockIdx.y * TC_M;
@@ -195,8 +233,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tf32x3_kernel(TcArgs a)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
     }
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < TC_STAGES; ++s) mbar_init(mbar0 + 8 * s, 1);
+    if (threadIdx.x == 32) {
+        for (int s = 0; s < TC_STAGES; ++s) mbar_init(stage_bar + 8 * s, 1);
+        for (int s = 0; s < 2; ++s) {
+            mbar_init(full_bar + 8 * s, 1);
+            mbar_init(empty_bar + 8 * s, TC_DRAINERS);
+        }
+        *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     tc_fence_before();
@@ -205,76 +248,100 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tf32x3_kernel(TcArgs a)
     const uint32_t tmem = *tmem_slot;
 
     const int g0 = a.tile_group_starts[tile], g1 = a.tile_group_starts[tile + 1];
+    const int ng = g1 - g0;
     const int nkc = a.k_pad / TC_KC;
-    const int total = (g1 - g0) * nkc;
-    bool failed = false;
+    const int total = ng * nkc;
 
-    // always commit STAGES-1 groups so that wait_group<STAGES-1> in the loop
-    // covers the current iteration even when total < STAGES-1
-    for (int it = 0; it < TC_STAGES - 1; ++it) {
-        if (it < total)
-            load_stage(a, base + (it % TC_STAGES) * STAGE, g0 + it / nkc, (it % nkc) * TC_KC, row0);
-        cp_async_commit();
-    }
-    for (int it = 0; it < total; ++it) {
-        const int pre = it + TC_STAGES - 1;
-        if (pre < total) {
-            const int ps = pre % TC_STAGES;
+    if (warp < TC_PRODUCERS / 32) {
+        // ---------------- producers / MMA issuer ----------------
+        for (int it = 0; it < TC_STAGES - 1; ++it) {
+            if (it < total)
+                load_stage(a, base + (it % TC_STAGES) * STAGE, g0 + it / nkc, (it % nkc) * TC_KC, row0);
+            cp_async_commit();
+        }
+        for (int it = 0; it < total; ++it) {
+            const int pre = it + TC_STAGES - 1;
             bool ok = true;
-            if (pre >= TC_STAGES) ok = mbar_wait(mbar0 + 8 * ps, ((pre / TC_STAGES) - 1) & 1);
-            if (__syncthreads_or(!ok)) { failed = true; break; }
-            load_stage(a, base + ps * STAGE, g0 + pre / nkc, (pre % nkc) * TC_KC, row0);
-        }
-        cp_async_commit();
-        cp_async_wait<TC_STAGES - 1>();
-        fence_proxy_async();
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            tc_fence_after();
-            const uint32_t st = base + (it % TC_STAGES) * STAGE;
-            const uint64_t ah = sw128_desc(st), al = sw128_desc(st + PLANE);
-            const uint64_t bh = sw128_desc(st + 2 * PLANE), bl = sw128_desc(st + 3 * PLANE);
+            if (pre < total && pre >= TC_STAGES)
+                ok = mbar_wait_or_abort(stage_bar + 8 * (pre % TC_STAGES),
+                                        ((pre / TC_STAGES) - 1) & 1, abort_flag);
+            if (producers_sync_or(!ok || *abort_flag)) break;
+            if (pre < total)
+                load_stage(a, base + (pre % TC_STAGES) * STAGE, g0 + pre / nkc, (pre % nkc) * TC_KC, row0);
+            cp_async_commit();
+            cp_async_wait<TC_STAGES - 1>();
+            fence_proxy_async();
+            producers_sync_or(false);
+            if (threadIdx.x == 0) {
+                const int gi = it / nkc, kc = it % nkc;
+                const int acc = gi & 1;
+                bool go = true;
+                if (kc == 0 && gi >= 2)
+                    go = mbar_wait_or_abort(empty_bar + 8 * acc, ((gi >> 1) - 1) & 1, abort_flag);
+                if (go) {
+                    tc_fence_after();
+                    const uint32_t st = base + (it % TC_STAGES) * STAGE;
+                    const uint64_t ah = sw128_desc(st), al = sw128_desc(st + PLANE);
+                    const uint64_t bh = sw128_desc(st + 2 * PLANE), bl = sw128_desc(st + 3 * PLANE);
+                    const uint32_t d = tmem + (uint32_t)(acc * TC_TW);
 #pragma unroll
-            for (int k = 0; k < TC_KC / 8; ++k) {
-                const uint64_t ko = (uint64_t)(k * 32 >> 4);  // 8 fp32 = 32 bytes along K
-                mma_tf32(tmem, ah + ko, bh + ko, (it > 0 || k > 0) ? 1u : 0u);
-                mma_tf32(tmem, ah + ko, bl + ko, 1u);
-                mma_tf32(tmem, al + ko, bh + ko, 1u);
+                    for (int k = 0; k < TC_KC / 8; ++k) {
+                        const uint64_t ko = (uint64_t)(k * 32 >> 4);  // 8 fp32 = 32 bytes along K
+                        mma_tf32(d, ah + ko, bh + ko, (kc > 0 || k > 0) ? 1u : 0u);
+                        mma_tf32(d, ah + ko, bl + ko, 1u);
+                        mma_tf32(d, al + ko, bh + ko, 1u);
+                    }
+                    mma_commit(stage_bar + 8 * (it % TC_STAGES));
+                    if (kc == nkc - 1) mma_commit(full_bar + 8 * acc);
+                }
             }
-            mma_commit(mbar0 + 8 * (it % TC_STAGES));
+        }
+        cp_async_wait_all();
+    } else {
+        // ---------------- drainers ----------------
+        const int dw = warp - TC_PRODUCERS / 32;      // 0..7
+        const int quad = warp & 3;                      // TMEM lane quadrant of this warp
+        const int half = dw >> 2;                       // which 64 columns
+        double acc64[64];
+#pragma unroll
+        for (int j = 0; j < 64; ++j) acc64[j] = 0.0;
+        bool ok = true;
+        for (int gi = 0; gi < ng && ok; ++gi) {
+            const int acc = gi & 1;
+            ok = mbar_wait_or_abort(full_bar + 8 * acc, (gi >> 1) & 1, abort_flag);
+            if (!ok) break;
+            tc_fence_after();
+            const uint32_t taddr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(acc * TC_TW + half * 64);
+#pragma unroll
+            for (int c0 = 0; c0 < 64; c0 += 16) {
+                uint32_t r[16];
+                tmem_ld16(taddr + c0, r);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) acc64[c0 + j] += (double)__uint_as_float(r[j]);
+            }
+            tc_fence_before();
+            mbar_arrive(empty_bar + 8 * acc);
+        }
+        if (ok && ng > 0) {
+            const int row = row0 + quad * 32 + lane;
+            if (row < a.n) {
+#pragma unroll
+                for (int j = 0; j < 64; ++j) {
+                    const int32_t t = a.tile_targets[(int64_t)tile * TC_TW + half * 64 + j];
+                    if (t >= 0) a.tgt[(int64_t)(t - a.tbase) * a.n + row] += a.scale * acc64[j];
+                }
+            }
         }
     }
 
-    if (!failed && total > 0) {
-        const int last = total - 1;
-        const bool ok = mbar_wait(mbar0 + 8 * (last % TC_STAGES), (last / TC_STAGES) & 1);
-        if (__syncthreads_or(!ok)) failed = true;
-    }
-    if (failed) {
-        if (threadIdx.x == 0 && a.status) atomicExch(a.status, ST_TIMEOUT_MMA);
-        cp_async_wait_all();
-        // let any MMA still reading the stages finish before the memory is released
-        for (int s = 0; s < TC_STAGES; ++s) {
-            const long long t0 = clock64();
-            while (clock64() - t0 < 1000000) {}
-        }
-    } else if (total > 0) {
-        tc_fence_after();
-        const int row = row0 + warp * 32 + lane;
-#pragma unroll 1
-        for (int c0 = 0; c0 < TC_TW; c0 += 16) {
-            uint32_t r[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c0, r);
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int32_t t = a.tile_targets[(int64_t)tile * TC_TW + c0 + j];
-                if (t >= 0 && row < a.n)
-                    a.tgt[(int64_t)(t - a.tbase) * a.n + row] += a.scale * (double)__uint_as_float(r[j]);
-            }
-        }
-    }
+    if (threadIdx.x == 0 && *abort_flag && a.status) atomicExch(a.status, ST_TIMEOUT_MMA);
     tc_fence_before();
     __syncthreads();
+    if (*abort_flag) {
+        // let tensor-core work still in flight finish before the memory is released
+        const long long t0 = clock64();
+        while (clock64() - t0 < 20000000) {}
+    }
     if (warp == 0) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TMEM_COLS)
