@@ -403,7 +403,8 @@ def stage_breakdown(w, trav, q_dev, dev):
     ach = work[dom]["flops"] / (stage[dom] * 1e-3) / 1e12
     peak = peaks.get("bf16_tflops", 1590.0)
     roof = {
-        "kernel": {"p2p": "p2p_csr_kernel<mixed>", "m2l": "m2l_f64_kernel<128>"}[dom],
+        "kernel": {"p2p": "p2p_csr_kernel<mixed>" if w.precision == "mixed" else "p2p_csr_kernel<f64>",
+                   "m2l": "m2l_tf32x3_kernel" if w.precision == "mixed" else "m2l_f64_kernel<128>"}[dom],
         "bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
         "frac": ach / peak, "traffic": None,
         "peak_source": "MEASURED_PEAKS.json bf16_tflops (of measured)" if peaks else "fallback",

@@ -17,6 +17,7 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "derivs.cuh"
 
 namespace sumpy {
 namespace {
@@ -111,64 +112,6 @@ __device__ void decompress_cube_warp(double *cube, int p, int lane)
         }
         __syncwarp();
     }
-}
-
-// Scaled derivatives rscale^|mi| d^mi (1/|x|) for the stored set of order p,
-// written to D[s * stride]; optionally dotted with coeffs (returns the sum).
-__device__ double laplace_stored_derivs(int p, double x, double y, double z, double rscale,
-                                        double *D, int stride, const double *coeffs)
-{
-    const double r2 = x * x + y * y + z * z;
-    const double rinv = rsqrt(r2);
-    const double rinv2 = rinv * rinv;
-    const double R = rscale;
-    const double Rinv = 1.0 / R;
-    const double xs[3] = {x * Rinv, y * Rinv, z * Rinv};
-    const double inv_rs2 = R * R * rinv2;
-    double acc = 0.0;
-    for (int deg = 0; deg <= p; ++deg) {
-        for (int i = 0; i <= min(1, deg); ++i) {
-            for (int j = 0; j <= deg - i; ++j) {
-                const int k = deg - i - j;
-                const int s = deg * deg + i * (deg + 1) + j;
-                double v;
-                if (j <= 1 && k <= 1) {
-                    if (deg == 0) {
-                        v = rinv;
-                    } else if (deg == 1) {
-                        const double c = i ? x : (j ? y : z);
-                        v = -R * c * rinv * rinv2;
-                    } else if (deg == 2) {
-                        const double c1 = i ? x : y;
-                        const double c2 = k ? z : y;
-                        v = 3.0 * R * R * c1 * c2 * rinv * rinv2 * rinv2;
-                    } else {
-                        v = -15.0 * R * R * R * x * y * z * rinv * rinv2 * rinv2 * rinv2;
-                    }
-                } else {
-                    const int d = (j >= 2) ? 1 : 2;
-                    double e = 0.0;
-                    if (i == 1) e -= 2.0 * xs[0] * D[stored_index(0, j, k) * stride];
-                    if (j >= 1) {
-                        const double t1 = D[stored_index(i, j - 1, k) * stride];
-                        const double t2 = (j >= 2) ? D[stored_index(i, j - 2, k) * stride] : 0.0;
-                        if (d == 1) e -= (2 * j - 1) * xs[1] * t1 + (double)(j - 1) * (j - 1) * t2;
-                        else e -= 2 * j * xs[1] * t1 + (double)j * (j - 1) * t2;
-                    }
-                    if (k >= 1) {
-                        const double t1 = D[stored_index(i, j, k - 1) * stride];
-                        const double t2 = (k >= 2) ? D[stored_index(i, j, k - 2) * stride] : 0.0;
-                        if (d == 2) e -= (2 * k - 1) * xs[2] * t1 + (double)(k - 1) * (k - 1) * t2;
-                        else e -= 2 * k * xs[2] * t1 + (double)k * (k - 1) * t2;
-                    }
-                    v = e * inv_rs2;
-                }
-                D[s * stride] = v;
-                if (coeffs) acc += coeffs[s] * v;
-            }
-        }
-    }
-    return acc;
 }
 
 // {{{ P2M
@@ -431,100 +374,7 @@ __global__ void l2p_kernel(int p, double rscale, int32_t nboxes, const int32_t *
 
 // }}}
 
-// {{{ M2P / P2L (derivative recurrence, per-lane shared scratch)
-
 constexpr int DSTRIDE = 33;  // lanes per coefficient row + 1 (bank spread)
-
-__global__ void m2p_kernel(int p, double rscale, int32_t ntgt_boxes,
-                           const int32_t *__restrict__ target_boxes,
-                           const int32_t *__restrict__ src_starts, const int32_t *__restrict__ src_lists,
-                           const double *__restrict__ centers, int64_t cstride, int32_t sbase,
-                           const double *__restrict__ src, const int32_t *__restrict__ bts,
-                           const int32_t *__restrict__ btc, const double *__restrict__ targets,
-                           int64_t tstride, double scale, double *__restrict__ result)
-{
-    extern __shared__ double sm[];
-    const int n = ncoeff_of(p);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nwarps = blockDim.x >> 5;
-    const int ib = blockIdx.x * nwarps + warp;
-    if (ib >= ntgt_boxes) return;
-    double *D = sm + warp * (n * DSTRIDE + n);
-    double *M = D + n * DSTRIDE;
-
-    const int32_t tb = target_boxes[ib];
-    const int32_t t0 = bts[tb], nt = btc[tb];
-    const int32_t ls = src_starts[ib], le = src_starts[ib + 1];
-    for (int32_t tc = 0; tc < nt; tc += 32) {
-        const int32_t t = t0 + tc + lane;
-        const bool active = tc + lane < nt;
-        double tx = 0, ty = 0, tz = 0;
-        if (active) { tx = targets[t]; ty = targets[tstride + t]; tz = targets[2 * tstride + t]; }
-        double acc = 0.0;
-        for (int32_t l = ls; l < le; ++l) {
-            const int32_t sb = src_lists[l];
-            const double *cs = src + (int64_t)(sb - sbase) * n;
-            __syncwarp();
-            for (int s = lane; s < n; s += 32) M[s] = cs[s];
-            __syncwarp();
-            if (active)
-                acc += laplace_stored_derivs(p, tx - centers[sb], ty - centers[cstride + sb],
-                                             tz - centers[2 * cstride + sb], rscale, D + lane,
-                                             DSTRIDE, M);
-        }
-        if (active) result[t] += scale * acc;
-    }
-}
-
-__global__ void p2l_kernel(int p, double rscale, int32_t ntgt_boxes,
-                           const int32_t *__restrict__ target_boxes,
-                           const int32_t *__restrict__ src_starts, const int32_t *__restrict__ src_lists,
-                           const double *__restrict__ centers, int64_t cstride,
-                           const int32_t *__restrict__ bss, const int32_t *__restrict__ bsc,
-                           const double *__restrict__ sources, int64_t sstride,
-                           const double *__restrict__ q, int32_t tbase, double *__restrict__ out)
-{
-    extern __shared__ double sm[];
-    const int n = ncoeff_of(p);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nwarps = blockDim.x >> 5;
-    const int ib = blockIdx.x * nwarps + warp;
-    if (ib >= ntgt_boxes) return;
-    double *D = sm + warp * (n * DSTRIDE + n);
-    double *acc = D + n * DSTRIDE;
-
-    const int32_t tb = target_boxes[ib];
-    const double c[3] = {centers[tb], centers[cstride + tb], centers[2 * cstride + tb]};
-    for (int s = lane; s < n; s += 32) acc[s] = 0.0;
-    const int32_t ls = src_starts[ib], le = src_starts[ib + 1];
-    for (int32_t l = ls; l < le; ++l) {
-        const int32_t sb = src_lists[l];
-        const int32_t s0 = bss[sb], ns = bsc[sb];
-        for (int32_t sc = 0; sc < ns; sc += 32) {
-            const int nsc = min(32, ns - sc);
-            __syncwarp();
-            if (lane < nsc) {
-                const int32_t s = s0 + sc + lane;
-                laplace_stored_derivs(p, c[0] - sources[s], c[1] - sources[sstride + s],
-                                      c[2] - sources[2 * sstride + s], rscale, D + lane, DSTRIDE,
-                                      nullptr);
-                const double qq = q[s];
-                for (int k = 0; k < n; ++k) D[k * DSTRIDE + lane] *= qq;
-            }
-            __syncwarp();
-            for (int k = lane; k < n; k += 32) {
-                double sum = 0.0;
-                for (int l2 = 0; l2 < nsc; ++l2) sum += D[k * DSTRIDE + l2];
-                acc[k] += sum;
-            }
-        }
-    }
-    __syncwarp();
-    double *o = out + (int64_t)(tb - tbase) * n;
-    for (int s = lane; s < n; s += 32) o[s] = acc[s];
-}
-
-// }}}
 
 bool order_ok(int p) { return p >= 0 && p <= SUMPY_MAX_ORDER; }
 
@@ -542,6 +392,162 @@ int prepare_smem(K kernel, size_t bytes)
     }
     return SUMPY_OK;
 }
+
+// {{{ M2P / P2L with register-resident derivative layers
+
+constexpr int E2P_WARPS = 4;
+
+// M2P: one warp per target box; the box's targets occupy g = next_pow2(nt)
+// lanes and the 32/g lane groups stride over the List-3 boxes; a
+// shuffle-xor tree sums the groups.
+template <int P>
+__global__ void __launch_bounds__(32 * E2P_WARPS)
+m2p_reg_kernel(double rscale, int32_t ntgt_boxes, const int32_t *__restrict__ target_boxes,
+               const int32_t *__restrict__ src_starts, const int32_t *__restrict__ src_lists,
+               const double *__restrict__ centers, int64_t cstride, int32_t sbase,
+               const double *__restrict__ src, const int32_t *__restrict__ bts,
+               const int32_t *__restrict__ btc, const double *__restrict__ targets,
+               int64_t tstride, double scale, double *__restrict__ result)
+{
+    constexpr int N = (P + 1) * (P + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ib = blockIdx.x * E2P_WARPS + warp;
+    if (ib >= ntgt_boxes) return;
+    const int32_t tb = target_boxes[ib];
+    const int32_t t0 = bts[tb], nt = btc[tb];
+    const int32_t ls = src_starts[ib], le = src_starts[ib + 1];
+    const double Rinv = 1.0 / rscale;
+    for (int32_t tc = 0; tc < nt; tc += 32) {
+        const int ntc = min(32, nt - tc);
+        int g = 1;
+        while (g < ntc) g <<= 1;
+        const int nph = 32 / g;
+        const int tl = lane & (g - 1), ph = lane / g;
+        const bool active = tl < ntc;
+        const int32_t t = t0 + tc + tl;
+        double tx = 0, ty = 0, tz = 0;
+        if (active) { tx = targets[t]; ty = targets[tstride + t]; tz = targets[2 * tstride + t]; }
+        double acc = 0.0;
+        if (active) {
+            for (int32_t l = ls + ph; l < le; l += nph) {
+                const int32_t sb = src_lists[l];
+                const double *M = src + (int64_t)(sb - sbase) * N;
+                laplace_layers<P>(tx - centers[sb], ty - centers[cstride + sb],
+                                  tz - centers[2 * cstride + sb], rscale, Rinv,
+                                  [&](int s, double v) { acc += __ldg(M + s) * v; });
+            }
+        }
+        for (int off = g; off < 32; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+        if (active && ph == 0) result[t] += scale * acc;
+    }
+}
+
+constexpr int P2L_WARPS = 2;
+
+// P2L: one warp per target box; the sources of all its List-4 boxes are
+// enumerated flat, 32 per round, one per lane; each lane writes q * D of its
+// source into a per-warp shared transpose (stride 33) and every lane then
+// sums its coefficients over the round's sources.
+template <int P>
+__global__ void __launch_bounds__(32 * P2L_WARPS)
+p2l_reg_kernel(double rscale, int32_t ntgt_boxes, const int32_t *__restrict__ target_boxes,
+               const int32_t *__restrict__ src_starts, const int32_t *__restrict__ src_lists,
+               const double *__restrict__ centers, int64_t cstride,
+               const int32_t *__restrict__ bss, const int32_t *__restrict__ bsc,
+               const double *__restrict__ sources, int64_t sstride, const double *__restrict__ q,
+               int32_t tbase, double *__restrict__ out)
+{
+    constexpr int N = (P + 1) * (P + 1);
+    constexpr int NPL = (N + 31) / 32;
+    extern __shared__ double sm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ib = blockIdx.x * P2L_WARPS + warp;
+    if (ib >= ntgt_boxes) return;
+    double *D = sm + warp * (N * DSTRIDE);
+    const int32_t tb = target_boxes[ib];
+    const double c0 = centers[tb], c1 = centers[cstride + tb], c2 = centers[2 * cstride + tb];
+    const int32_t ls = src_starts[ib], le = src_starts[ib + 1];
+    const double Rinv = 1.0 / rscale;
+    int32_t total = 0;
+    for (int32_t l = ls; l < le; ++l) total += bsc[src_lists[l]];
+    double acc[NPL];
+#pragma unroll
+    for (int m = 0; m < NPL; ++m) acc[m] = 0.0;
+    for (int32_t base = 0; base < total; base += 32) {
+        const int nsc = min(32, total - base);
+        if (lane < nsc) {
+            // locate flat source index base + lane
+            int32_t f = base + lane, l = ls, sb = src_lists[ls];
+            while (f >= bsc[sb]) { f -= bsc[sb]; ++l; sb = src_lists[l]; }
+            const int32_t s = bss[sb] + f;
+            const double qq = q[s];
+            laplace_layers<P>(c0 - sources[s], c1 - sources[sstride + s],
+                              c2 - sources[2 * sstride + s], rscale, Rinv,
+                              [&](int k, double v) { D[k * DSTRIDE + lane] = qq * v; });
+        }
+        __syncwarp();
+#pragma unroll
+        for (int m = 0; m < NPL; ++m) {
+            const int k = lane + 32 * m;
+            if (k < N) {
+                double sum = 0.0;
+                for (int l2 = 0; l2 < nsc; ++l2) sum += D[k * DSTRIDE + l2];
+                acc[m] += sum;
+            }
+        }
+        __syncwarp();
+    }
+    double *o = out + (int64_t)(tb - tbase) * N;
+#pragma unroll
+    for (int m = 0; m < NPL; ++m) {
+        const int k = lane + 32 * m;
+        if (k < N) o[k] = acc[m];
+    }
+}
+
+template <int P>
+int launch_m2p_reg(double rscale, int32_t ntgt_boxes, const int32_t *target_boxes,
+                   const int32_t *src_starts, const int32_t *src_lists, const double *centers,
+                   int64_t cstride, int32_t sbase, const double *src, const int32_t *bts,
+                   const int32_t *btc, const double *targets, int64_t tstride, double scale,
+                   double *result, cudaStream_t st)
+{
+    const int blocks = (ntgt_boxes + E2P_WARPS - 1) / E2P_WARPS;
+    m2p_reg_kernel<P><<<blocks, 32 * E2P_WARPS, 0, st>>>(rscale, ntgt_boxes, target_boxes, src_starts,
+                                                         src_lists, centers, cstride, sbase, src, bts,
+                                                         btc, targets, tstride, scale, result);
+    return check_launch("m2p_reg_kernel");
+}
+
+template <int P>
+int launch_p2l_reg(double rscale, int32_t ntgt_boxes, const int32_t *target_boxes,
+                   const int32_t *src_starts, const int32_t *src_lists, const double *centers,
+                   int64_t cstride, const int32_t *bss, const int32_t *bsc, const double *sources,
+                   int64_t sstride, const double *q, int32_t tbase, double *out, cudaStream_t st)
+{
+    constexpr int N = (P + 1) * (P + 1);
+    const size_t smem = sizeof(double) * N * DSTRIDE * P2L_WARPS;
+    int rc = prepare_smem(p2l_reg_kernel<P>, smem);
+    if (rc) return rc;
+    const int blocks = (ntgt_boxes + P2L_WARPS - 1) / P2L_WARPS;
+    p2l_reg_kernel<P><<<blocks, 32 * P2L_WARPS, smem, st>>>(rscale, ntgt_boxes, target_boxes,
+                                                             src_starts, src_lists, centers, cstride,
+                                                             bss, bsc, sources, sstride, q, tbase, out);
+    return check_launch("p2l_reg_kernel");
+}
+
+#define SUMPY_ORDER_SWITCH(p, CALL)                                                             \
+    switch (p) {                                                                               \
+    case 0: return CALL(0); case 1: return CALL(1); case 2: return CALL(2);                    \
+    case 3: return CALL(3); case 4: return CALL(4); case 5: return CALL(5);                    \
+    case 6: return CALL(6); case 7: return CALL(7); case 8: return CALL(8);                    \
+    case 9: return CALL(9); case 10: return CALL(10); case 11: return CALL(11);                \
+    case 12: return CALL(12); case 13: return CALL(13); case 14: return CALL(14);              \
+    case 15: return CALL(15); case 16: return CALL(16);                                        \
+    default: set_last_error("unsupported order"); return SUMPY_EUNSUPPORTED;                   \
+    }
+
+// }}}
 
 }  // namespace
 }  // namespace sumpy
@@ -669,18 +675,13 @@ int sumpy_e2p_from_csr_f64(int order, double rscale, int32_t ntgt_boxes,
         !src_expansions || !box_target_starts || !box_target_counts_nonchild || !targets ||
         !result)
         return bad_arg("m2p: null pointer argument");
-    const int n = ncoeff_of(order);
-    const size_t per_warp = sizeof(double) * (n * DSTRIDE + n);
-    const int warps = (int)std::max<size_t>(1, std::min<size_t>(4, (96 * 1024) / per_warp));
-    const size_t smem = per_warp * warps;
-    int rc = prepare_smem(m2p_kernel, smem);
-    if (rc) return rc;
-    const int blocks = (ntgt_boxes + warps - 1) / warps;
-    m2p_kernel<<<blocks, 32 * warps, smem, as_stream(stream)>>>(
-        order, rscale, ntgt_boxes, target_boxes, source_box_starts, source_box_lists, centers,
-        center_stride, src_base_ibox, src_expansions, box_target_starts,
-        box_target_counts_nonchild, targets, target_stride, scale, result);
-    return check_launch("m2p_kernel");
+#define CALL_M2P(P)                                                                             \
+    launch_m2p_reg<P>(rscale, ntgt_boxes, target_boxes, source_box_starts, source_box_lists,   \
+                      centers, center_stride, src_base_ibox, src_expansions, box_target_starts, \
+                      box_target_counts_nonchild, targets, target_stride, scale, result,        \
+                      as_stream(stream))
+    SUMPY_ORDER_SWITCH(order, CALL_M2P)
+#undef CALL_M2P
 }
 
 int sumpy_p2e_from_csr_f64(int order, double rscale, int32_t ntgt_boxes,
@@ -698,18 +699,13 @@ int sumpy_p2e_from_csr_f64(int order, double rscale, int32_t ntgt_boxes,
         !box_source_starts || !box_source_counts_nonchild || !sources || !strength ||
         !tgt_expansions)
         return bad_arg("p2l: null pointer argument");
-    const int n = ncoeff_of(order);
-    const size_t per_warp = sizeof(double) * (n * DSTRIDE + n);
-    const int warps = (int)std::max<size_t>(1, std::min<size_t>(4, (96 * 1024) / per_warp));
-    const size_t smem = per_warp * warps;
-    int rc = prepare_smem(p2l_kernel, smem);
-    if (rc) return rc;
-    const int blocks = (ntgt_boxes + warps - 1) / warps;
-    p2l_kernel<<<blocks, 32 * warps, smem, as_stream(stream)>>>(
-        order, rscale, ntgt_boxes, target_boxes, source_box_starts, source_box_lists, centers,
-        center_stride, box_source_starts, box_source_counts_nonchild, sources, source_stride,
-        strength, tgt_base_ibox, tgt_expansions);
-    return check_launch("p2l_kernel");
+#define CALL_P2L(P)                                                                             \
+    launch_p2l_reg<P>(rscale, ntgt_boxes, target_boxes, source_box_starts, source_box_lists,   \
+                      centers, center_stride, box_source_starts, box_source_counts_nonchild,    \
+                      sources, source_stride, strength, tgt_base_ibox, tgt_expansions,          \
+                      as_stream(stream))
+    SUMPY_ORDER_SWITCH(order, CALL_P2L)
+#undef CALL_P2L
 }
 
 }  // extern "C"
