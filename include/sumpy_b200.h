@@ -183,23 +183,34 @@ int sumpy_split_tf32x2(
     int64_t nmat, int32_t rows, int32_t cols, const double *in,
     int32_t rows_pad, int32_t cols_pad, float *hi, float *lo, void *stream);
 
-/* M2L for one level on the tcgen05 tensor cores, split-FP32 (3xTF32):
- * same schedule and result contract as sumpy_m2l_translation_classes_f64
- * (replacing sumpy/e2e.py:310-558 and sumpy/fmm.py:798-920) with
- * tile_width 128, operators given as TF32 planes mats_hi/mats_lo
- * [nclasses][rows_pad][k_pad] and the level's multipoles as planes
- * src_hi/src_lo [nboxes_level][k_pad] (both from sumpy_split_tf32x2).
- * rows_pad is a multiple of 128, k_pad a multiple of 32. Products
- * hi*hi + hi*lo + lo*hi accumulate in FP32 (tensor memory) over the tile's
- * groups; tgt[t] += matrix_scale * result in FP64. status (device int32,
- * may be NULL) receives a nonzero code if a bounded internal wait expired. */
+/* M2L on the tcgen05 tensor cores, split-FP32 (3xTF32), for any number of
+ * levels in one launch. Replaces M2LUsingTranslationClassesDependentData
+ * (sumpy/e2e.py:310-558) with its pre/post-processing and FFTs
+ * (sumpy/fmm.py:798-920); same operator as sumpy_m2l_translation_classes_f64.
+ *
+ * Schedule: tiles of 128 target slots (tile_targets[tile*128 + slot], box
+ * numbers, -1 = empty) with a per-tile scale tile_scale[tile] (the level's
+ * operator factor); class groups g with class group_class[g] and one
+ * source box per slot group_sources[g*128 + slot] (-1 = none); work items
+ * i = groups [item_group_begin[i], item_group_end[i]) of tile item_tile[i].
+ * Operators: TF32 planes mats_hi/mats_lo [nclasses][rows_pad][k_pad];
+ * multipoles: TF32 planes src_hi/src_lo [src_nrows][k_pad] (both from
+ * sumpy_split_tf32x2), row of box b = b - src_base_ibox, and the last row
+ * (src_nrows - 1) must be all zeros (it stands in for empty slots).
+ * rows_pad is a multiple of 128, k_pad a multiple of 32.
+ * Each group's products hi*hi + hi*lo + lo*hi accumulate in FP32 tensor
+ * memory and are summed over groups in FP64; tgt[t] += tile_scale * result
+ * with FP64 atomics, so items of one tile may run concurrently. status
+ * (device int32, may be NULL) receives a nonzero code if a bounded internal
+ * wait expired. */
 int sumpy_m2l_translation_classes_tf32x3(
-    int order, int32_t ntiles, int32_t tile_width, const int32_t *tile_targets,
-    const int32_t *tile_group_starts, const int32_t *group_class,
-    const int32_t *group_sources, int32_t nclasses, const float *mats_hi,
-    const float *mats_lo, int32_t rows_pad, int32_t k_pad, double matrix_scale,
-    int32_t src_base_ibox, const float *src_hi, const float *src_lo,
-    int32_t tgt_base_ibox, double *tgt_expansions, int32_t *status, void *stream);
+    int order, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
+    const int32_t *item_group_end, int32_t tile_width, const int32_t *tile_targets,
+    const double *tile_scale, const int32_t *group_class, const int32_t *group_sources,
+    int32_t nclasses, const float *mats_hi, const float *mats_lo, int32_t rows_pad,
+    int32_t k_pad, int32_t src_nrows, int32_t src_base_ibox, const float *src_hi,
+    const float *src_lo, int32_t tgt_base_ibox, double *tgt_expansions, int32_t *status,
+    void *stream);
 
 /* ------------------------------------------------------------------ */
 /* E2P                                                                  */

@@ -14,20 +14,26 @@
 // against ~3e-7 when each group is drained to FP64), hence one
 // accumulation session per group.
 //
-// CTA = 384 threads, one output tile of 128 coefficient rows x 128 target
-// slots (the MMA is M=128, N=128, K=8 per instruction). Operand tiles are
-// K-major with the 128-byte swizzle: each row (a coefficient row of T_c, or
-// the coefficients of one source multipole) holds 32 fp32 of K in 128
-// bytes; 8 rows form a 1024-byte swizzle atom. K is streamed in chunks of
-// 32 through a 3-stage shared-memory ring filled with cp.async by the four
-// producer warps; one producer thread issues the 12 MMAs of a chunk (4
-// K-steps x 3 products) and commits them to the stage's mbarrier, which the
-// producers wait on before refilling the stage. All waits are bounded by a
-// clock budget; on expiry the kernel records an error in *status, drains
-// its copies, frees its tensor memory and returns.
+// CTA = 384 threads, one work item: a range of class groups of one output
+// tile of 128 coefficient rows x 128 target slots (the MMA is M=128, N=128,
+// K=8 per instruction). Operand tiles are K-major with the 128-byte
+// swizzle: each row (a coefficient row of T_c, or the coefficients of one
+// source multipole) holds 32 fp32 of K in 128 bytes; 8 rows form a
+// 1024-byte swizzle atom. K is streamed in chunks of 32 through a 3-stage
+// shared-memory ring: a TMA tiled load per operator plane (1024-byte
+// aligned) and cp.async row copies of the gathered source multipoles, all
+// completing on the stage's "full" mbarrier (TMA byte count plus one
+// asynchronous cp.async arrival per loader thread). One thread issues
+// the 12 MMAs of a chunk (4 K-steps x 3 products) and commits them to the
+// stage's "empty" mbarrier, which the loader waits on before refilling the
+// stage. Every load fills this CTA's own shared memory only. All waits are bounded by a clock
+// budget; on expiry the kernel records an error in *status, lets work in
+// flight finish, frees its tensor memory and returns.
 #include <algorithm>
 #include <cstdint>
 #include <string>
+
+#include <cuda.h>
 
 #include "common.cuh"
 
@@ -38,12 +44,13 @@ constexpr int TC_TW = 128;      // target slots per tile (MMA N)
 constexpr int TC_M = 128;       // coefficient rows per CTA (MMA M)
 constexpr int TC_KC = 32;       // fp32 K elements per 128-byte row
 constexpr int TC_STAGES = 3;
-constexpr int TC_PRODUCERS = 128;          // warps 0-3
+constexpr int TC_LOADERS = 96;             // warps 0-2
 constexpr int TC_DRAINERS = 256;           // warps 4-11
-constexpr int TC_THREADS = TC_PRODUCERS + TC_DRAINERS;
+constexpr int TC_THREADS = 128 + TC_DRAINERS;
 constexpr int PLANE = TC_M * 128;          // bytes of one 128 x 32 fp32 operand tile
 constexpr int STAGE = 4 * PLANE;           // A_hi, A_lo, B_hi, B_lo
 constexpr int TC_SMEM = TC_STAGES * STAGE + 1024 /* alignment slack */ + 256 /* barriers */;
+static_assert(2 * PLANE == 32768, "TMA bytes of a stage");
 constexpr uint32_t TMEM_COLS = 256;         // two 128-column accumulators
 constexpr long long WAIT_CYCLES = 4000000000LL;  // ~2 s at 2 GHz
 
@@ -61,14 +68,11 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, uint32
                  : "memory");
 }
 
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+// arrive on the mbarrier once this thread's earlier cp.async copies have landed
+__device__ __forceinline__ void cp_async_arrive_noinc(uint32_t mbar)
+{
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(mbar) : "memory");
+}
 
 __device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count)
 {
@@ -135,58 +139,38 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
 }
 
 struct TcArgs {
-    int n, rows_pad, k_pad;
-    const int32_t *tile_targets, *tile_group_starts, *group_class, *group_sources;
-    const float *mats_hi, *mats_lo;
-    double scale;
-    int32_t sbase;
+    int n, k_pad;
+    const int32_t *item_tile, *item_g0, *item_g1;
+    const int32_t *tile_targets;
+    const double *tile_scale;
+    const int32_t *group_class, *group_sources;
     const float *src_hi, *src_lo;
+    int32_t src_row_base, zero_row;
     int32_t tbase;
     double *tgt;
     int32_t *status;
 };
 
-// Fill one stage: A planes from T_c rows [row0, row0+128) x K [k0, k0+32),
-// B planes from the 128 gathered source multipoles (zeros for empty slots).
-// Executed by the 128 producer threads.
-__device__ __forceinline__ void load_stage(const TcArgs &a, uint32_t st, int g, int k0, int row0)
-{
-    const int cls = a.group_class[g];
-    const int32_t *gs = a.group_sources + (int64_t)g * TC_TW;
-    for (int c = threadIdx.x; c < TC_M * 8; c += TC_PRODUCERS) {
-        const int r = c >> 3, q = c & 7;
-        const uint32_t dst = r * 128 + ((q ^ (r & 7)) << 4);
-        const int64_t off = ((int64_t)cls * a.rows_pad + row0 + r) * a.k_pad + k0 + 4 * q;
-        cp_async16(st + dst, a.mats_hi + off, 16);
-        cp_async16(st + PLANE + dst, a.mats_lo + off, 16);
-    }
-    for (int c = threadIdx.x; c < TC_TW * 8; c += TC_PRODUCERS) {
-        const int slot = c >> 3, q = c & 7;
-        const int32_t s = gs[slot];
-        const uint32_t dst = slot * 128 + ((q ^ (slot & 7)) << 4);
-        const int64_t off = (int64_t)(s >= 0 ? s - a.sbase : 0) * a.k_pad + k0 + 4 * q;
-        const uint32_t bytes = s >= 0 ? 16u : 0u;
-        cp_async16(st + 2 * PLANE + dst, a.src_hi + off, bytes);
-        cp_async16(st + 3 * PLANE + dst, a.src_lo + off, bytes);
-    }
-}
-
-// barrier 1 over the producer warps only, OR-reducing a flag
-__device__ __forceinline__ bool producers_sync_or(bool v)
-{
-    uint32_t r;
-    asm volatile(
-        "{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n"
-        " bar.red.or.pred p, 1, %2, q;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(r)
-        : "r"((uint32_t)v), "n"(TC_PRODUCERS)
-        : "memory");
-    return r != 0;
-}
-
 __device__ __forceinline__ void mbar_arrive(uint32_t addr)
 {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(addr) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t addr, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(addr), "r"(bytes)
+                 : "memory");
+}
+
+// TMA: one 3D tile (32 fp32 of K x 128 rows x 1 class) of a class-operator plane
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, int c0, int c1,
+                                            int c2, uint32_t mbar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(mbar)
+        : "memory");
 }
 
 // bounded wait that also gives up when another thread has aborted
@@ -203,26 +187,45 @@ __device__ bool mbar_wait_or_abort(uint32_t addr, uint32_t parity, volatile int 
     return true;
 }
 
-// Warp roles: warps 0-3 produce (cp.async into the stage ring; thread 0 also
-// issues the MMAs), warps 4-11 drain. Each group's product accumulates in
-// one of two TMEM accumulators (128 columns each) and is drained into FP64
-// registers of the draining warps right after the group, while the next
-// group accumulates in the other one: no FP32 sum spans more than one group.
-// Draining warp w covers TMEM lanes 32*(w%4).. and 64 of the 128 columns.
-__global__ void __launch_bounds__(TC_THREADS, 1) m2l_tf32x3_kernel(TcArgs a)
+// barrier 1 over the loader warps only, OR-reducing a flag
+__device__ __forceinline__ bool loaders_sync_or(bool v)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n"
+        " bar.red.or.pred p, 1, %2, q;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(r)
+        : "r"((uint32_t)v), "n"(TC_LOADERS)
+        : "memory");
+    return r != 0;
+}
+
+// One CTA per work item = a contiguous range of class groups of one tile.
+// Warp roles: warps 0-2 load (thread 0 also posts the expected TMA bytes),
+// warp 3 lane 0 issues the MMAs, warps 4-11 drain. Each group's product accumulates in one of
+// two TMEM accumulators (128 columns each) and is drained into FP64
+// registers right after the group, while the next group accumulates in the
+// other: no FP32 sum spans more than one group. Draining warp w covers TMEM
+// lanes 32*(w%4).. and 64 of the 128 columns. The item's sums are added to
+// the local expansions with FP64 atomics (a tile may span several items).
+__global__ void __launch_bounds__(TC_THREADS, 1)
+m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
+                  const __grid_constant__ CUtensorMap map_a_lo)
 {
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_addr(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;          // 1024-byte aligned stages
     uint8_t *base_ptr = smem_raw + (base - raw);
     uint64_t *bars = reinterpret_cast<uint64_t *>(base_ptr + TC_STAGES * STAGE);
-    // bars[0..2] stage MMA done, [3..4] accumulator full, [5..6] accumulator empty
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 8);
+    // bars: [0,S) stage full, [S,2S) stage empty, 2S..2S+1 accumulator full,
+    // 2S+2..2S+3 accumulator empty
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * TC_STAGES + 4);
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
     const uint32_t bar0 = smem_addr(bars);
-    const uint32_t stage_bar = bar0, full_bar = bar0 + 8 * 3, empty_bar = bar0 + 8 * 5;
+    const uint32_t full_bar = bar0, empty_bar = bar0 + 8 * TC_STAGES;
+    const uint32_t accf_bar = bar0 + 16 * TC_STAGES, acce_bar = accf_bar + 16;
 
-    const int tile = blockIdx.x;
+    const int item = blockIdx.x;
     const int row0 = blockIdx.y * TC_M;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -234,72 +237,93 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tf32x3_kernel(TcArgs a)
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
     }
     if (threadIdx.x == 32) {
-        for (int s = 0; s < TC_STAGES; ++s) mbar_init(stage_bar + 8 * s, 1);
+        for (int s = 0; s < TC_STAGES; ++s) {
+            mbar_init(full_bar + 8 * s, TC_LOADERS + 1);  // cp.async arrivals + TMA expect-tx
+            mbar_init(empty_bar + 8 * s, 1);
+        }
         for (int s = 0; s < 2; ++s) {
-            mbar_init(full_bar + 8 * s, 1);
-            mbar_init(empty_bar + 8 * s, TC_DRAINERS);
+            mbar_init(accf_bar + 8 * s, 1);
+            mbar_init(acce_bar + 8 * s, TC_DRAINERS);
         }
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (threadIdx.x == 64) {
+        asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&map_a_hi)) : "memory");
+        asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&map_a_lo)) : "memory");
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    const int g0 = a.tile_group_starts[tile], g1 = a.tile_group_starts[tile + 1];
+    const int tile = a.item_tile[item];
+    const int g0 = a.item_g0[item], g1 = a.item_g1[item];
     const int ng = g1 - g0;
     const int nkc = a.k_pad / TC_KC;
     const int total = ng * nkc;
 
-    if (warp < TC_PRODUCERS / 32) {
-        // ---------------- producers / MMA issuer ----------------
-        for (int it = 0; it < TC_STAGES - 1; ++it) {
-            if (it < total)
-                load_stage(a, base + (it % TC_STAGES) * STAGE, g0 + it / nkc, (it % nkc) * TC_KC, row0);
-            cp_async_commit();
-        }
+    if (warp < TC_LOADERS / 32) {
+        // ---------------- loaders ----------------
+        // thread 0: TMA tiles of the two operator planes; all 96 threads:
+        // cp.async row copies of the two source planes (the gathered
+        // multipoles), then an asynchronous arrival on the stage barrier.
         for (int it = 0; it < total; ++it) {
-            const int pre = it + TC_STAGES - 1;
+            const int s = it % TC_STAGES, use = it / TC_STAGES;
             bool ok = true;
-            if (pre < total && pre >= TC_STAGES)
-                ok = mbar_wait_or_abort(stage_bar + 8 * (pre % TC_STAGES),
-                                        ((pre / TC_STAGES) - 1) & 1, abort_flag);
-            if (producers_sync_or(!ok || *abort_flag)) break;
-            if (pre < total)
-                load_stage(a, base + (pre % TC_STAGES) * STAGE, g0 + pre / nkc, (pre % nkc) * TC_KC, row0);
-            cp_async_commit();
-            cp_async_wait<TC_STAGES - 1>();
-            fence_proxy_async();
-            producers_sync_or(false);
+            if (use > 0) ok = mbar_wait_or_abort(empty_bar + 8 * s, (use - 1) & 1, abort_flag);
+            if (loaders_sync_or(!ok || *abort_flag)) break;
+            const int g = g0 + it / nkc, k0 = (it % nkc) * TC_KC;
+            const uint32_t st = base + s * STAGE;
             if (threadIdx.x == 0) {
+                mbar_expect_tx(full_bar + 8 * s, 2 * PLANE);
+                const int cls = a.group_class[g];
+                tma_load_3d(st, &map_a_hi, k0, row0, cls, full_bar + 8 * s);
+                tma_load_3d(st + PLANE, &map_a_lo, k0, row0, cls, full_bar + 8 * s);
+            }
+            const int32_t *gs = a.group_sources + (int64_t)g * TC_TW;
+            for (int c = threadIdx.x; c < TC_TW * 8; c += TC_LOADERS) {
+                const int slot = c >> 3, q = c & 7;
+                const int32_t sb = gs[slot];
+                const uint32_t dst = slot * 128 + ((q ^ (slot & 7)) << 4);
+                const int64_t row = sb >= 0 ? sb - a.src_row_base : a.zero_row;
+                const int64_t off = row * a.k_pad + k0 + 4 * q;
+                cp_async16(st + 2 * PLANE + dst, a.src_hi + off, 16);
+                cp_async16(st + 3 * PLANE + dst, a.src_lo + off, 16);
+            }
+            cp_async_arrive_noinc(full_bar + 8 * s);
+        }
+    } else if (warp == 3) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            for (int it = 0; it < total; ++it) {
+                const int s = it % TC_STAGES, use = it / TC_STAGES;
+                if (!mbar_wait_or_abort(full_bar + 8 * s, use & 1, abort_flag)) break;
                 const int gi = it / nkc, kc = it % nkc;
                 const int acc = gi & 1;
-                bool go = true;
-                if (kc == 0 && gi >= 2)
-                    go = mbar_wait_or_abort(empty_bar + 8 * acc, ((gi >> 1) - 1) & 1, abort_flag);
-                if (go) {
-                    tc_fence_after();
-                    const uint32_t st = base + (it % TC_STAGES) * STAGE;
-                    const uint64_t ah = sw128_desc(st), al = sw128_desc(st + PLANE);
-                    const uint64_t bh = sw128_desc(st + 2 * PLANE), bl = sw128_desc(st + 3 * PLANE);
-                    const uint32_t d = tmem + (uint32_t)(acc * TC_TW);
+                if (kc == 0 && gi >= 2 &&
+                    !mbar_wait_or_abort(acce_bar + 8 * acc, ((gi >> 1) - 1) & 1, abort_flag))
+                    break;
+                tc_fence_after();
+                const uint32_t st = base + s * STAGE;
+                const uint64_t ah = sw128_desc(st), al = sw128_desc(st + PLANE);
+                const uint64_t bh = sw128_desc(st + 2 * PLANE), bl = sw128_desc(st + 3 * PLANE);
+                const uint32_t d = tmem + (uint32_t)(acc * TC_TW);
 #pragma unroll
-                    for (int k = 0; k < TC_KC / 8; ++k) {
-                        const uint64_t ko = (uint64_t)(k * 32 >> 4);  // 8 fp32 = 32 bytes along K
-                        mma_tf32(d, ah + ko, bh + ko, (kc > 0 || k > 0) ? 1u : 0u);
-                        mma_tf32(d, ah + ko, bl + ko, 1u);
-                        mma_tf32(d, al + ko, bh + ko, 1u);
-                    }
-                    mma_commit(stage_bar + 8 * (it % TC_STAGES));
-                    if (kc == nkc - 1) mma_commit(full_bar + 8 * acc);
+                for (int k = 0; k < TC_KC / 8; ++k) {
+                    const uint64_t ko = (uint64_t)(k * 32 >> 4);  // 8 fp32 = 32 bytes along K
+                    mma_tf32(d, ah + ko, bh + ko, (kc > 0 || k > 0) ? 1u : 0u);
+                    mma_tf32(d, ah + ko, bl + ko, 1u);
+                    mma_tf32(d, al + ko, bh + ko, 1u);
                 }
+                mma_commit(empty_bar + 8 * s);
+                if (kc == nkc - 1) mma_commit(accf_bar + 8 * acc);
             }
         }
-        cp_async_wait_all();
-    } else {
+        __syncwarp();
+    } else if (warp >= 4) {
         // ---------------- drainers ----------------
-        const int dw = warp - TC_PRODUCERS / 32;      // 0..7
+        const int dw = warp - 4;                        // 0..7
         const int quad = warp & 3;                      // TMEM lane quadrant of this warp
         const int half = dw >> 2;                       // which 64 columns
         double acc64[64];
@@ -308,7 +332,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tf32x3_kernel(TcArgs a)
         bool ok = true;
         for (int gi = 0; gi < ng && ok; ++gi) {
             const int acc = gi & 1;
-            ok = mbar_wait_or_abort(full_bar + 8 * acc, (gi >> 1) & 1, abort_flag);
+            ok = mbar_wait_or_abort(accf_bar + 8 * acc, (gi >> 1) & 1, abort_flag);
             if (!ok) break;
             tc_fence_after();
             const uint32_t taddr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(acc * TC_TW + half * 64);
@@ -320,15 +344,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tf32x3_kernel(TcArgs a)
                 for (int j = 0; j < 16; ++j) acc64[c0 + j] += (double)__uint_as_float(r[j]);
             }
             tc_fence_before();
-            mbar_arrive(empty_bar + 8 * acc);
+            mbar_arrive(acce_bar + 8 * acc);
         }
         if (ok && ng > 0) {
             const int row = row0 + quad * 32 + lane;
+            const double scale = a.tile_scale[tile];
             if (row < a.n) {
 #pragma unroll
                 for (int j = 0; j < 64; ++j) {
                     const int32_t t = a.tile_targets[(int64_t)tile * TC_TW + half * 64 + j];
-                    if (t >= 0) a.tgt[(int64_t)(t - a.tbase) * a.n + row] += a.scale * acc64[j];
+                    if (t >= 0) atomicAdd(a.tgt + (int64_t)(t - a.tbase) * a.n + row, scale * acc64[j]);
                 }
             }
         }
@@ -338,7 +363,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tf32x3_kernel(TcArgs a)
     tc_fence_before();
     __syncthreads();
     if (*abort_flag) {
-        // let tensor-core work still in flight finish before the memory is released
+        // let copies and tensor-core work still in flight finish before the
+        // shared and tensor memory are released
         const long long t0 = clock64();
         while (clock64() - t0 < 20000000) {}
     }
@@ -395,11 +421,48 @@ int sumpy_split_tf32x2(int64_t nmat, int32_t rows, int32_t cols, const double *i
     return check_launch("split_tf32x2_kernel");
 }
 
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                    const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                    const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                    CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// fp32 tensor map over [dims[rank-1]]...[dims[0]], 128-byte swizzle, box {32, box1, 1}
+static bool make_map(CUtensorMap *m, const float *ptr, int rank, const uint64_t *dims,
+                     uint32_t box1)
+{
+    EncodeTiledFn fn = encode_tiled_fn();
+    if (!fn) return false;
+    cuuint64_t gdim[3], gstride[2];
+    cuuint32_t box[3] = {32, box1, 1}, estr[3] = {1, 1, 1};
+    for (int i = 0; i < rank; ++i) gdim[i] = dims[i];
+    gstride[0] = dims[0] * sizeof(float);
+    if (rank == 3) gstride[1] = dims[0] * dims[1] * sizeof(float);
+    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, const_cast<float *>(ptr), gdim, gstride,
+                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 int sumpy_m2l_translation_classes_tf32x3(
-    int order, int32_t ntiles, int32_t tile_width, const int32_t *tile_targets,
-    const int32_t *tile_group_starts, const int32_t *group_class, const int32_t *group_sources,
+    int order, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
+    const int32_t *item_group_end, int32_t tile_width, const int32_t *tile_targets,
+    const double *tile_scale, const int32_t *group_class, const int32_t *group_sources,
     int32_t nclasses, const float *mats_hi, const float *mats_lo, int32_t rows_pad, int32_t k_pad,
-    double matrix_scale, int32_t src_base_ibox, const float *src_hi, const float *src_lo,
+    int32_t src_nrows, int32_t src_base_ibox, const float *src_hi, const float *src_lo,
     int32_t tgt_base_ibox, double *tgt_expansions, int32_t *status, void *stream)
 {
     if (order < 0 || order > SUMPY_MAX_ORDER) {
@@ -410,10 +473,11 @@ int sumpy_m2l_translation_classes_tf32x3(
     if (tile_width != TC_TW) return bad_arg("m2l_tf32x3: tile_width must be 128");
     if (rows_pad < n || rows_pad % TC_M) return bad_arg("m2l_tf32x3: rows_pad must be a multiple of 128 >= ncoeff");
     if (k_pad < n || k_pad % TC_KC) return bad_arg("m2l_tf32x3: k_pad must be a multiple of 32 >= ncoeff");
-    if (ntiles < 0 || nclasses < 0) return bad_arg("m2l_tf32x3: negative size");
-    if (ntiles == 0) return SUMPY_OK;
-    if (!tile_targets || !tile_group_starts || !group_class || !group_sources || !mats_hi ||
-        !mats_lo || !src_hi || !src_lo || !tgt_expansions)
+    if (nitems < 0 || nclasses <= 0 || src_nrows < 1) return bad_arg("m2l_tf32x3: bad sizes");
+    if (nitems == 0) return SUMPY_OK;
+    if (!item_tile || !item_group_begin || !item_group_end || !tile_targets || !tile_scale ||
+        !group_class || !group_sources || !mats_hi || !mats_lo || !src_hi || !src_lo ||
+        !tgt_expansions)
         return bad_arg("m2l_tf32x3: null pointer argument");
     if ((reinterpret_cast<uintptr_t>(mats_hi) | reinterpret_cast<uintptr_t>(mats_lo) |
          reinterpret_cast<uintptr_t>(src_hi) | reinterpret_cast<uintptr_t>(src_lo)) & 15)
@@ -430,15 +494,22 @@ int sumpy_m2l_translation_classes_tf32x3(
         }
         attr_set[dev] = true;
     }
+    CUtensorMap ma_hi, ma_lo;
+    const uint64_t adims[3] = {(uint64_t)k_pad, (uint64_t)rows_pad, (uint64_t)nclasses};
+    if (!make_map(&ma_hi, mats_hi, 3, adims, TC_M) || !make_map(&ma_lo, mats_lo, 3, adims, TC_M)) {
+        set_last_error("m2l_tf32x3: tensor map encoding failed");
+        return SUMPY_EINVAL;
+    }
     TcArgs a;
-    a.n = n; a.rows_pad = rows_pad; a.k_pad = k_pad;
-    a.tile_targets = tile_targets; a.tile_group_starts = tile_group_starts;
+    a.n = n; a.k_pad = k_pad;
+    a.item_tile = item_tile; a.item_g0 = item_group_begin; a.item_g1 = item_group_end;
+    a.tile_targets = tile_targets; a.tile_scale = tile_scale;
     a.group_class = group_class; a.group_sources = group_sources;
-    a.mats_hi = mats_hi; a.mats_lo = mats_lo; a.scale = matrix_scale;
-    a.sbase = src_base_ibox; a.src_hi = src_hi; a.src_lo = src_lo;
+    a.src_hi = src_hi; a.src_lo = src_lo;
+    a.src_row_base = src_base_ibox; a.zero_row = src_nrows - 1;
     a.tbase = tgt_base_ibox; a.tgt = tgt_expansions; a.status = status;
-    dim3 grid(ntiles, (n + TC_M - 1) / TC_M);
-    m2l_tf32x3_kernel<<<grid, TC_THREADS, TC_SMEM, as_stream(stream)>>>(a);
+    dim3 grid(nitems, rows_pad / TC_M);
+    m2l_tf32x3_kernel<<<grid, TC_THREADS, TC_SMEM, as_stream(stream)>>>(a, ma_hi, ma_lo);
     return check_launch("m2l_tf32x3_kernel");
 }
 

@@ -37,6 +37,7 @@ _d = _capi.dbl
 
 M2L_TILE = 64          # FP64 GEMM tile (target boxes)
 M2L_TILE_TC = 128      # tensor-core tile (MMA N)
+M2L_ITEM_GROUPS = 64   # class groups per tensor-core work item (one CTA)
 
 
 def _np_i32(a):
@@ -408,11 +409,18 @@ class SumpyExpansionWrangler:
         starts = np.asarray(src_box_starts if not isinstance(src_box_starts, torch.Tensor)
                             else src_box_starts.cpu().numpy())
         st = stream_ptr()
+        levels = [lev for lev in range(self.tree.nlevels)
+                  if ltb[lev] != ltb[lev + 1] and starts[ltb[lev]] != starts[ltb[lev + 1]]]
         tc = self.precision == "mixed"
-        for lev in range(self.tree.nlevels):
+        if tc and len({self.level_orders[lev] for lev in levels}) == 1 \
+                and len(set(self.level_orders)) == 1:
+            # every level in one launch (uniform expansion size)
+            plan = self._m2l_tc_plan(tuple(levels), ltb, tboxes, starts, src_box_lists)
+            if plan is not None:
+                self._launch_m2l_tc_merged(plan, mpole_exps, local_exps, st)
+            return local_exps
+        for lev in levels:
             a, b = int(ltb[lev]), int(ltb[lev + 1])
-            if a == b or starts[a] == starts[b]:
-                continue
             plan = self._m2l_plan(lev, tboxes[a:b], starts[a:b + 1], src_box_lists,
                                   M2L_TILE_TC if tc else M2L_TILE)
             if plan is None:
@@ -421,10 +429,76 @@ class SumpyExpansionWrangler:
             sbase, sview = self.multipole_expansions_view(mpole_exps, lev)
             tbase, tview = self.local_expansions_view(local_exps, lev)
             if tc:
-                self._launch_m2l_tc(lev, plan, mats, mscale, sbase, sview, tbase, tview, st)
+                self._launch_m2l_tc_level(lev, plan, mats, mscale, sbase, sview, tbase, tview, st)
             else:
                 self._launch_m2l(lev, plan, mats, mscale, sbase, sview, tbase, tview, st)
         return local_exps
+
+    @staticmethod
+    def _tc_items(tiles):
+        """Split tiles (group ranges) into work items of at most
+        M2L_ITEM_GROUPS groups, largest first (CTAs start roughly in launch
+        order)."""
+        it_tile, it_g0, it_g1 = [], [], []
+        for tile, (g0, g1) in enumerate(tiles):
+            for a in range(g0, g1, M2L_ITEM_GROUPS):
+                it_tile.append(tile)
+                it_g0.append(a)
+                it_g1.append(min(g1, a + M2L_ITEM_GROUPS))
+        it_tile = np.array(it_tile, dtype=np.int32)
+        it_g0 = np.array(it_g0, dtype=np.int32)
+        it_g1 = np.array(it_g1, dtype=np.int32)
+        order = np.argsort(-(it_g1 - it_g0), kind="stable")
+        return it_tile[order], it_g0[order], it_g1[order]
+
+    def _m2l_tc_plan(self, levels, ltb, tboxes, starts, lists):
+        """One tensor-core schedule over all M2L levels: the per-level (tile,
+        class) groups concatenated, class ids offset into a stacked operator
+        set, one scale per tile."""
+        key = ("tc-merged", levels, id(lists))
+        if key in self._m2l_plans:
+            return self._m2l_plans[key]
+        tt, tsc, gcl, gsrc, tiles = [], [], [], [], []
+        mats_list, mats_index = [], {}
+        ntiles = ngroups = 0
+        for lev in levels:
+            a, b = int(ltb[lev]), int(ltb[lev + 1])
+            p = self._m2l_plan(lev, tboxes[a:b], starts[a:b + 1], lists, M2L_TILE_TC)
+            if p is None:
+                continue
+            mats, mscale = self._m2l_matrices(lev)
+            mkey = mats.data_ptr()
+            if mkey not in mats_index:
+                mats_index[mkey] = sum(m.shape[0] for m in mats_list)
+                mats_list.append(mats)
+            tgs = p["tile_group_starts"].cpu().numpy()
+            tiles += [(ngroups + int(tgs[i]), ngroups + int(tgs[i + 1]))
+                      for i in range(p["ntiles"])]
+            tt.append(p["tile_targets"].cpu().numpy())
+            tsc.append(np.full(p["ntiles"], mscale))
+            gcl.append(p["group_class"].cpu().numpy() + mats_index[mkey])
+            gsrc.append(p["group_sources"].cpu().numpy())
+            ntiles += p["ntiles"]
+            ngroups += p["ngroups"]
+        if ntiles == 0:
+            self._m2l_plans[key] = None
+            return None
+        it_tile, it_g0, it_g1 = self._tc_items(tiles)
+        mats = mats_list[0] if len(mats_list) == 1 else torch.cat(mats_list)
+        dev = self.device
+        plan = {
+            "nitems": len(it_tile), "ntiles": ntiles, "ngroups": ngroups,
+            "nclasses": int(mats.shape[0]), "mats": mats,
+            "item_tile": torch.as_tensor(it_tile).to(dev),
+            "item_g0": torch.as_tensor(it_g0).to(dev),
+            "item_g1": torch.as_tensor(it_g1).to(dev),
+            "tile_targets": torch.as_tensor(np.concatenate(tt)).to(dev),
+            "tile_scale": torch.as_tensor(np.concatenate(tsc)).to(dev),
+            "group_class": torch.as_tensor(np.concatenate(gcl).astype(np.int32)).to(dev),
+            "group_sources": torch.as_tensor(np.concatenate(gsrc)).to(dev),
+        }
+        self._m2l_plans[key] = plan
+        return plan
 
     def _launch_m2l(self, lev, plan, mats, mscale, sbase, sview, tbase, tview, st):
         call("sumpy_m2l_translation_classes_f64", _c(self.level_orders[lev]),
@@ -452,29 +526,58 @@ class SumpyExpansionWrangler:
         self._m2l_tc_mats[key] = (hi, lo, rp, kp)
         return self._m2l_tc_mats[key]
 
-    def _m2l_workspace(self, nboxes, kp):
-        need = nboxes * kp
+    def _m2l_workspace(self, nrows, kp):
+        """TF32 hi/lo planes of the source multipoles, [nrows + 1][kp]; the
+        extra last row stays zero (it stands in for empty tile slots)."""
+        need = (nrows + 1) * kp
         if self._m2l_ws is None or self._m2l_ws[0].numel() < need:
-            lsb = self.tree_level_start_box_nrs
-            most = int(np.max(np.diff(lsb))) * kp
-            self._m2l_ws = (torch.empty(most, dtype=torch.float32, device=self.device),
-                            torch.empty(most, dtype=torch.float32, device=self.device))
-        return self._m2l_ws
+            rows = max(nrows, self.tree.nboxes) + 1
+            self._m2l_ws = (torch.empty(rows * kp, dtype=torch.float32, device=self.device),
+                            torch.empty(rows * kp, dtype=torch.float32, device=self.device))
+        hi, lo = self._m2l_ws
+        zero = slice(nrows * kp, (nrows + 1) * kp)
+        hi[zero].zero_()
+        lo[zero].zero_()
+        return hi, lo
 
-    def _launch_m2l_tc(self, lev, plan, mats, mscale, sbase, sview, tbase, tview, st):
-        hi, lo, rp, kp = self._m2l_tc_operands(mats)
-        n = sview.shape[1]
-        nb = sview.shape[0]
+    def _launch_m2l_tc_merged(self, plan, mpole_exps, local_exps, st):
+        hi, lo, rp, kp = self._m2l_tc_operands(plan["mats"])
+        n = plan["mats"].shape[1]
+        nb = self.tree.nboxes
         ws_hi, ws_lo = self._m2l_workspace(nb, kp)
-        # M2L pre-processing: this level's multipoles as TF32 hi/lo planes
+        # M2L pre-processing: every multipole as TF32 hi/lo planes (row = box)
+        call("sumpy_split_tf32x2", _i64(nb), _i32(1), _i32(n), dptr(mpole_exps), _i32(1),
+             _i32(kp), dptr(ws_hi), dptr(ws_lo), st)
+        self._call_m2l_tc(self.level_orders[0], plan, hi, lo, rp, kp, nb + 1, 0, ws_hi, ws_lo,
+                          0, local_exps, st)
+
+    def _call_m2l_tc(self, order, plan, hi, lo, rp, kp, src_nrows, sbase, ws_hi, ws_lo,
+                     tbase, tgt, st):
+        call("sumpy_m2l_translation_classes_tf32x3", _c(order), _i32(plan["nitems"]),
+             dptr(plan["item_tile"]), dptr(plan["item_g0"]), dptr(plan["item_g1"]),
+             _i32(M2L_TILE_TC), dptr(plan["tile_targets"]), dptr(plan["tile_scale"]),
+             dptr(plan["group_class"]), dptr(plan["group_sources"]), _i32(plan["nclasses"]),
+             dptr(hi), dptr(lo), _i32(rp), _i32(kp), _i32(src_nrows), _i32(sbase),
+             dptr(ws_hi), dptr(ws_lo), _i32(tbase), dptr(tgt), dptr(self._status), st)
+
+    def _launch_m2l_tc_level(self, lev, plan, mats, mscale, sbase, sview, tbase, tview, st):
+        hi, lo, rp, kp = self._m2l_tc_operands(mats)
+        nb, n = sview.shape
+        ws_hi, ws_lo = self._m2l_workspace(nb, kp)
         call("sumpy_split_tf32x2", _i64(nb), _i32(1), _i32(n), dptr(sview), _i32(1),
              _i32(kp), dptr(ws_hi), dptr(ws_lo), st)
-        call("sumpy_m2l_translation_classes_tf32x3", _c(self.level_orders[lev]),
-             _i32(plan["ntiles"]), _i32(M2L_TILE_TC), dptr(plan["tile_targets"]),
-             dptr(plan["tile_group_starts"]), dptr(plan["group_class"]),
-             dptr(plan["group_sources"]), _i32(plan["nclasses"]), dptr(hi), dptr(lo),
-             _i32(rp), _i32(kp), _d(mscale), _i32(sbase), dptr(ws_hi), dptr(ws_lo),
-             _i32(tbase), dptr(tview), dptr(self._status), st)
+        key = ("items", lev, id(plan))
+        if key not in self._m2l_plans:
+            tgs = plan["tile_group_starts"].cpu().numpy()
+            tiles = [(int(tgs[i]), int(tgs[i + 1])) for i in range(plan["ntiles"])]
+            it_tile, it_g0, it_g1 = self._tc_items(tiles)
+            dev = self.device
+            self._m2l_plans[key] = dict(
+                plan, nitems=len(it_tile), item_tile=torch.as_tensor(it_tile).to(dev),
+                item_g0=torch.as_tensor(it_g0).to(dev), item_g1=torch.as_tensor(it_g1).to(dev),
+                tile_scale=torch.full((plan["ntiles"],), mscale, dtype=torch.float64, device=dev))
+        self._call_m2l_tc(self.level_orders[lev], self._m2l_plans[key], hi, lo, rp, kp, nb + 1,
+                          sbase, ws_hi, ws_lo, tbase, tview, st)
 
     def check_status(self):
         """Raise if a kernel reported an internal error (synchronises)."""
