@@ -212,6 +212,27 @@ int sumpy_m2l_translation_classes_tf32x3(
     const float *src_lo, int32_t tgt_base_ibox, double *tgt_expansions, int32_t *status,
     void *stream);
 
+/* Same M2L as sumpy_m2l_translation_classes_tf32x3, for callers that cannot
+ * allocate device memory while they run (a host application with a fixed
+ * device-memory budget, an allocation-free real-time loop, code where an
+ * allocation would synchronise the device). No counterpart in sumpy: it
+ * exists only for this interface. Takes the level's FP64 multipoles
+ * (src_expansions, nsrc_boxes rows of ncoeff, box b at row b - src_base_ibox)
+ * and keeps their TF32 planes in a device array built into the library
+ * (8 MiB per GPU, held until exit) instead of caller memory; allocates
+ * nothing. Limit: (nsrc_boxes + 1) * k_pad <= 1,048,576 and k_pad <= 128
+ * (8,191 boxes at order <= 10); larger requests return SUMPY_EINVAL. The
+ * first call on a device looks up the array's device address; make that
+ * call before any stream capture. All calls share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller. */
+int sumpy_m2l_translation_classes_tf32x3_noalloc(
+    int order, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
+    const int32_t *item_group_end, int32_t tile_width, const int32_t *tile_targets,
+    const double *tile_scale, const int32_t *group_class, const int32_t *group_sources,
+    int32_t nclasses, const float *mats_hi, const float *mats_lo, int32_t rows_pad,
+    int32_t k_pad, int32_t nsrc_boxes, int32_t src_base_ibox, const double *src_expansions,
+    int32_t tgt_base_ibox, double *tgt_expansions, int32_t *status, void *stream);
+
 /* ------------------------------------------------------------------ */
 /* E2P                                                                  */
 /* ------------------------------------------------------------------ */

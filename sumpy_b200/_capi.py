@@ -38,6 +38,9 @@ SIGNATURES = {
     "sumpy_m2l_translation_classes_tf32x3": [cint, i32, ptr, ptr, ptr, i32, ptr, ptr, ptr, ptr,
                                              i32, ptr, ptr, i32, i32, i32, i32, ptr, ptr, i32,
                                              ptr, ptr, ptr],
+    "sumpy_m2l_translation_classes_tf32x3_noalloc": [cint, i32, ptr, ptr, ptr, i32, ptr, ptr,
+                                                     ptr, ptr, i32, ptr, ptr, i32, i32, i32,
+                                                     i32, ptr, i32, ptr, ptr, ptr],
     "sumpy_e2p_from_single_box_f64": [cint, dbl, i32, ptr, ptr, i64, i32, ptr, ptr, ptr,
                                       ptr, i64, dbl, ptr, ptr],
     "sumpy_e2p_from_csr_f64": [cint, dbl, i32, ptr, ptr, ptr, ptr, i64, i32, ptr, ptr, ptr,

@@ -31,6 +31,7 @@
 // flight finish, frees its tensor memory and returns.
 #include <algorithm>
 #include <cstdint>
+#include <mutex>
 #include <string>
 
 #include <cuda.h>
@@ -511,6 +512,89 @@ int sumpy_m2l_translation_classes_tf32x3(
     dim3 grid(nitems, rows_pad / TC_M);
     m2l_tf32x3_kernel<<<grid, TC_THREADS, TC_SMEM, as_stream(stream)>>>(a, ma_hi, ma_lo);
     return check_launch("m2l_tf32x3_kernel");
+}
+
+// ---------------------------------------------------------------------------
+// Variant of the tensor-core M2L that allocates nothing.
+//
+// Some callers cannot allocate device memory once they are running: host
+// applications that fix their device-memory budget at start-up (a solver
+// framework owning one pool for everything, a real-time or certified loop
+// that forbids allocation after initialisation), or code embedded where an
+// allocation would synchronise the device. This entry point keeps the TF32
+// planes of the source multipoles -- the only scratch the tensor-core M2L
+// needs -- in a file-scope device array instead of caller memory.
+//
+// Limits: (nsrc_boxes + 1) * k_pad <= NOALLOC_ROWS * NOALLOC_KPAD floats per
+// plane, i.e. 8,191 source boxes at k_pad = 128 (orders <= 10); larger
+// requests are rejected. Every GPU that loads this library holds the array
+// (8 MiB) until the process exits. All calls share it and it keeps the
+// previous call's contents; the zero row the kernel needs is cleared on
+// every call. Calls that overlap on the GPU (different streams, or another
+// thread) race on the array and must be serialised by the caller.
+constexpr int64_t NOALLOC_ROWS = 8192;
+constexpr int64_t NOALLOC_KPAD = 128;
+static __device__ __align__(256) float g_noalloc_planes[2 * NOALLOC_ROWS * NOALLOC_KPAD];
+
+// Device address of g_noalloc_planes on the current device, looked up once
+// per device (host code cannot use the symbol's name as a device address).
+static float *noalloc_planes(int dev)
+{
+    static float *addr[64] = {};
+    static std::mutex lock;
+    std::lock_guard<std::mutex> guard(lock);
+    if (!addr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_planes);
+        if (e != cudaSuccess) {
+            set_last_error(std::string("m2l_tf32x3_noalloc: cudaGetSymbolAddress: ") +
+                           cudaGetErrorString(e));
+            return nullptr;
+        }
+        addr[dev] = static_cast<float *>(p);
+    }
+    return addr[dev];
+}
+
+int sumpy_m2l_translation_classes_tf32x3_noalloc(
+    int order, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
+    const int32_t *item_group_end, int32_t tile_width, const int32_t *tile_targets,
+    const double *tile_scale, const int32_t *group_class, const int32_t *group_sources,
+    int32_t nclasses, const float *mats_hi, const float *mats_lo, int32_t rows_pad, int32_t k_pad,
+    int32_t nsrc_boxes, int32_t src_base_ibox, const double *src_expansions,
+    int32_t tgt_base_ibox, double *tgt_expansions, int32_t *status, void *stream)
+{
+    if (order < 0 || order > SUMPY_MAX_ORDER) {
+        set_last_error("m2l_tf32x3_noalloc: unsupported order");
+        return SUMPY_EUNSUPPORTED;
+    }
+    const int n = ncoeff_of(order);
+    if (nsrc_boxes < 0 || k_pad < n || k_pad % TC_KC) return bad_arg("m2l_tf32x3_noalloc: bad sizes");
+    if (k_pad > NOALLOC_KPAD || (int64_t)(nsrc_boxes + 1) * k_pad > NOALLOC_ROWS * NOALLOC_KPAD) {
+        set_last_error("m2l_tf32x3_noalloc: request exceeds the built-in scratch: needs (nsrc_boxes+1)*k_pad <= " +
+                       std::to_string(NOALLOC_ROWS * NOALLOC_KPAD) + " and k_pad <= " +
+                       std::to_string(NOALLOC_KPAD) + " (got nsrc_boxes=" +
+                       std::to_string(nsrc_boxes) + ", k_pad=" + std::to_string(k_pad) + ")");
+        return SUMPY_EINVAL;
+    }
+    if (nsrc_boxes > 0 && !src_expansions) return bad_arg("m2l_tf32x3_noalloc: null pointer argument");
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+        return bad_arg("m2l_tf32x3_noalloc: no device");
+    float *hi = noalloc_planes(dev);
+    if (!hi) return SUMPY_ELAUNCH;
+    float *lo = hi + NOALLOC_ROWS * NOALLOC_KPAD;
+    cudaStream_t st = as_stream(stream);
+    const size_t zero_off = (size_t)nsrc_boxes * k_pad;
+    if (cudaMemsetAsync(hi + zero_off, 0, sizeof(float) * k_pad, st) != cudaSuccess ||
+        cudaMemsetAsync(lo + zero_off, 0, sizeof(float) * k_pad, st) != cudaSuccess)
+        return check_launch("m2l_tf32x3_noalloc: clearing the zero row");
+    int rc = sumpy_split_tf32x2(nsrc_boxes, 1, n, src_expansions, 1, k_pad, hi, lo, stream);
+    if (rc) return rc;
+    return sumpy_m2l_translation_classes_tf32x3(
+        order, nitems, item_tile, item_group_begin, item_group_end, tile_width, tile_targets,
+        tile_scale, group_class, group_sources, nclasses, mats_hi, mats_lo, rows_pad, k_pad,
+        nsrc_boxes + 1, src_base_ibox, hi, lo, tgt_base_ibox, tgt_expansions, status, stream);
 }
 
 }  // extern "C"
