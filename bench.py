@@ -179,13 +179,8 @@ def main():
     import torch
     import torch.distributed as dist
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-        torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from sumpy_b200.distributed import init as dist_init, max_over_ranks
+    rank, world, local_rank = dist_init("nccl", timeout_s=300)
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
 
@@ -241,10 +236,7 @@ def main():
         torch.cuda.synchronize()
         barrier()
         ms = [a.elapsed_time(b) for a, b in evs]
-        tot = torch.tensor([sum(ms)], device=dev)
-        if world > 1:
-            dist.all_reduce(tot, op=dist.ReduceOp.MAX)
-        return float(tot.item()) / steps, ms
+        return max_over_ranks(sum(ms), device=dev) / steps, ms
 
     # setup (plans, tables) outside timing
     t0 = time.perf_counter()

@@ -287,10 +287,12 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
                 const int slot = c >> 3, q = c & 7;
                 const int32_t sb = gs[slot];
                 const uint32_t dst = slot * 128 + ((q ^ (slot & 7)) << 4);
+                // empty slots: zero-fill without reading memory (source size 0)
                 const int64_t row = sb >= 0 ? sb - a.src_row_base : a.zero_row;
                 const int64_t off = row * a.k_pad + k0 + 4 * q;
-                cp_async16(st + 2 * PLANE + dst, a.src_hi + off, 16);
-                cp_async16(st + 3 * PLANE + dst, a.src_lo + off, 16);
+                const uint32_t bytes = sb >= 0 ? 16u : 0u;
+                cp_async16(st + 2 * PLANE + dst, a.src_hi + off, bytes);
+                cp_async16(st + 3 * PLANE + dst, a.src_lo + off, bytes);
             }
             cp_async_arrive_noinc(full_bar + 8 * s);
         }
