@@ -79,6 +79,29 @@ int sumpy_p2p_from_csr_mixed(
     const double *targets, int64_t target_stride,
     const int32_t *target_to_source, double scale, double *result, void *stream);
 
+/* Gradient form: also writes grad[d*target_stride + t] = scale * sum_s
+ * strength[s] * d/dt_d (1/|t - s|) (sumpy's AxisTargetDerivative applied to
+ * the Laplace kernel, sumpy/kernel.py:2331-2386); result may be NULL. Used
+ * for position gradients of the adjoint. FP64, and mixed precision as
+ * sumpy_p2p_from_csr_mixed. */
+int sumpy_p2p_from_csr_grad_f64(
+    int32_t ntgt_boxes, const int32_t *target_boxes,
+    const int32_t *source_box_starts, const int32_t *source_box_lists,
+    const int32_t *box_source_starts, const int32_t *box_source_counts_nonchild,
+    const int32_t *box_target_starts, const int32_t *box_target_counts_nonchild,
+    const double *sources, int64_t source_stride, const double *strength,
+    const double *targets, int64_t target_stride,
+    const int32_t *target_to_source, double scale, double *result, double *grad, void *stream);
+
+int sumpy_p2p_from_csr_grad_mixed(
+    int32_t ntgt_boxes, const int32_t *target_boxes,
+    const int32_t *source_box_starts, const int32_t *source_box_lists,
+    const int32_t *box_source_starts, const int32_t *box_source_counts_nonchild,
+    const int32_t *box_target_starts, const int32_t *box_target_counts_nonchild,
+    const double *sources, int64_t source_stride, const double *strength,
+    const double *targets, int64_t target_stride,
+    const int32_t *target_to_source, double scale, double *result, double *grad, void *stream);
+
 /* All-pairs sum. Replaces P2P.__call__ (sumpy/p2p.py:267-285), the direct
  * evaluation sumpy's FMM tests compare against (sumpy/test/test_fmm.py:284-286).
  * result[t] = scale * sum_s strength[s]/|t - s|, skipping s ==
@@ -88,6 +111,14 @@ int sumpy_p2p_direct_f64(
     int64_t nsources, const double *sources, int64_t source_stride,
     const double *strength, const int32_t *target_to_source, double scale,
     double *result, void *stream);
+
+/* Gradient of the direct sum: grad[d*target_stride + t] as in
+ * sumpy_p2p_from_csr_grad_f64 over all sources; result may be NULL. */
+int sumpy_p2p_direct_grad_f64(
+    int64_t ntargets, const double *targets, int64_t target_stride,
+    int64_t nsources, const double *sources, int64_t source_stride,
+    const double *strength, const int32_t *target_to_source, double scale,
+    double *result, double *grad, void *stream);
 
 /* ------------------------------------------------------------------ */
 /* P2E                                                                  */
@@ -261,6 +292,28 @@ int sumpy_e2p_from_csr_f64(
     const int32_t *box_target_starts, const int32_t *box_target_counts_nonchild,
     const double *targets, int64_t target_stride, double scale, double *result,
     void *stream);
+
+/* Gradient forms of L2P and M2P: grad[d*target_stride + t] receives the
+ * derivative of the expansion's value with respect to target coordinate d
+ * (assigned for L2P, accumulated for M2P, like the values); result may be
+ * NULL. L2P: (1/rscale) times the local polynomial with coefficients
+ * shifted by e_d; M2P: kernel derivatives of one order more. */
+int sumpy_e2p_from_single_box_grad_f64(
+    int order, double rscale, int32_t ntgt_boxes, const int32_t *target_boxes,
+    const double *centers, int64_t center_stride,
+    int32_t src_base_ibox, const double *src_expansions,
+    const int32_t *box_target_starts, const int32_t *box_target_counts_nonchild,
+    const double *targets, int64_t target_stride, double scale, double *result,
+    double *grad, void *stream);
+
+int sumpy_e2p_from_csr_grad_f64(
+    int order, double rscale, int32_t ntgt_boxes, const int32_t *target_boxes,
+    const int32_t *source_box_starts, const int32_t *source_box_lists,
+    const double *centers, int64_t center_stride,
+    int32_t src_base_ibox, const double *src_expansions,
+    const int32_t *box_target_starts, const int32_t *box_target_counts_nonchild,
+    const double *targets, int64_t target_stride, double scale, double *result,
+    double *grad, void *stream);
 
 #ifdef __cplusplus
 }

@@ -24,6 +24,15 @@ SIGNATURES = {
     "sumpy_p2p_from_csr_mixed": [i32, ptr, ptr, ptr, ptr, ptr, ptr, ptr, ptr, i64, ptr,
                                  ptr, i64, ptr, dbl, ptr, ptr],
     "sumpy_p2p_direct_f64": [i64, ptr, i64, i64, ptr, i64, ptr, ptr, dbl, ptr, ptr],
+    "sumpy_p2p_direct_grad_f64": [i64, ptr, i64, i64, ptr, i64, ptr, ptr, dbl, ptr, ptr, ptr],
+    "sumpy_p2p_from_csr_grad_f64": [i32, ptr, ptr, ptr, ptr, ptr, ptr, ptr, ptr, i64, ptr,
+                                    ptr, i64, ptr, dbl, ptr, ptr, ptr],
+    "sumpy_p2p_from_csr_grad_mixed": [i32, ptr, ptr, ptr, ptr, ptr, ptr, ptr, ptr, i64, ptr,
+                                      ptr, i64, ptr, dbl, ptr, ptr, ptr],
+    "sumpy_e2p_from_single_box_grad_f64": [cint, dbl, i32, ptr, ptr, i64, i32, ptr, ptr, ptr,
+                                           ptr, i64, dbl, ptr, ptr, ptr],
+    "sumpy_e2p_from_csr_grad_f64": [cint, dbl, i32, ptr, ptr, ptr, ptr, i64, i32, ptr, ptr,
+                                    ptr, ptr, i64, dbl, ptr, ptr, ptr],
     "sumpy_p2e_from_single_box_f64": [cint, dbl, i32, ptr, ptr, i64, ptr, ptr, ptr, i64,
                                       ptr, i32, ptr, ptr],
     "sumpy_p2e_from_csr_f64": [cint, dbl, i32, ptr, ptr, ptr, ptr, i64, ptr, ptr, ptr,

@@ -6,7 +6,8 @@
 // degree d-1 and d-2 entries, so three register "layers" of 2P+1 values
 // suffice. With P a template parameter every loop unrolls and every index
 // is a compile-time constant. Within a layer the entry e = i*(deg+1) + j is
-// (i, j, deg-i-j); its stored index is deg^2 + e.
+// (i, j, deg-i-j); its stored index is deg^2 + e. visit(s, i, j, k, value)
+// is called for every entry in stored order.
 #pragma once
 
 namespace sumpy {
@@ -63,7 +64,7 @@ __device__ __forceinline__ void laplace_layers(double x, double y, double z, dou
                 v = t * irs2;
             }
             L0[e] = v;
-            visit(deg * deg + e, v);
+            visit(deg * deg + e, i, j, k, v);
         }
 #pragma unroll
         for (int e = 0; e < 2 * P + 1; ++e) {

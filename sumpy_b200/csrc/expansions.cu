@@ -322,11 +322,33 @@ l2l_kernel(int ps, int pt, double rsrc, double rtgt, const int32_t *__restrict__
 
 constexpr int L2P_MAX_WARPS = 4;
 
+// sum over |mi| <= p - sh of cube[i+di][j+dj][k+dk] x^i y^j z^k / (i! j! k!),
+// nested Horner with inv[n] = 1/n (sh = di + dj + dk)
+__device__ __forceinline__ double horner_cube(const double *cube, const double *inv, int p, int di,
+                                              int dj, int dk, double x, double y, double z)
+{
+    const int q = p - di - dj - dk;
+    double tot = 0.0;
+    for (int i = q; i >= 0; --i) {
+        double sy = 0.0;
+        for (int j = q - i; j >= 0; --j) {
+            double sz = 0.0;
+            const double *row = cube + cube_index(p, i + di, j + dj, dk);
+            for (int k = q - i - j; k >= 0; --k) sz = row[k] + sz * z * inv[k + 1];
+            sy = sz + sy * y * inv[j + 1];
+        }
+        tot = sy + tot * x * inv[i + 1];
+    }
+    return tot;
+}
+
+template <bool GRAD>
 __global__ void l2p_kernel(int p, double rscale, int32_t nboxes, const int32_t *__restrict__ boxes,
                            const double *__restrict__ centers, int64_t cstride, int32_t sbase,
                            const double *__restrict__ src, const int32_t *__restrict__ bts,
                            const int32_t *__restrict__ btc, const double *__restrict__ targets,
-                           int64_t tstride, double scale, double *__restrict__ result)
+                           int64_t tstride, double scale, double *__restrict__ result,
+                           double *__restrict__ grad)
 {
     extern __shared__ double sm[];
     const int P1 = p + 1, C = P1 * P1 * P1;
@@ -357,18 +379,14 @@ __global__ void l2p_kernel(int p, double rscale, int32_t nboxes, const int32_t *
         const double x = (targets[t] - c[0]) * rinv;
         const double y = (targets[tstride + t] - c[1]) * rinv;
         const double z = (targets[2 * tstride + t] - c[2]) * rinv;
-        double tot = 0.0;
-        for (int i = p; i >= 0; --i) {
-            double sy = 0.0;
-            for (int j = p - i; j >= 0; --j) {
-                double sz = 0.0;
-                const double *row = cube + cube_index(p, i, j, 0);
-                for (int k = p - i - j; k >= 0; --k) sz = row[k] + sz * z * inv[k + 1];
-                sy = sz + sy * y * inv[j + 1];
-            }
-            tot = sy + tot * x * inv[i + 1];
+        if (result) result[t] = scale * horner_cube(cube, inv, p, 0, 0, 0, x, y, z);
+        if (GRAD) {
+            // d/dt of sum L[mi] (b/r)^mi / mi! = (1/r) sum L[mi + e_d] (b/r)^mi / mi!
+            const double gs = scale * rinv;
+            grad[t] = p > 0 ? gs * horner_cube(cube, inv, p, 1, 0, 0, x, y, z) : 0.0;
+            grad[tstride + t] = p > 0 ? gs * horner_cube(cube, inv, p, 0, 1, 0, x, y, z) : 0.0;
+            grad[2 * tstride + t] = p > 0 ? gs * horner_cube(cube, inv, p, 0, 0, 1, x, y, z) : 0.0;
         }
-        result[t] = scale * tot;
     }
 }
 
@@ -400,14 +418,15 @@ constexpr int E2P_WARPS = 4;
 // M2P: one warp per target box; the box's targets occupy g = next_pow2(nt)
 // lanes and the 32/g lane groups stride over the List-3 boxes; a
 // shuffle-xor tree sums the groups.
-template <int P>
+template <int P, bool GRAD>
 __global__ void __launch_bounds__(32 * E2P_WARPS)
 m2p_reg_kernel(double rscale, int32_t ntgt_boxes, const int32_t *__restrict__ target_boxes,
                const int32_t *__restrict__ src_starts, const int32_t *__restrict__ src_lists,
                const double *__restrict__ centers, int64_t cstride, int32_t sbase,
                const double *__restrict__ src, const int32_t *__restrict__ bts,
                const int32_t *__restrict__ btc, const double *__restrict__ targets,
-               int64_t tstride, double scale, double *__restrict__ result)
+               int64_t tstride, double scale, double *__restrict__ result,
+               double *__restrict__ grad)
 {
     constexpr int N = (P + 1) * (P + 1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -427,18 +446,48 @@ m2p_reg_kernel(double rscale, int32_t ntgt_boxes, const int32_t *__restrict__ ta
         const int32_t t = t0 + tc + tl;
         double tx = 0, ty = 0, tz = 0;
         if (active) { tx = targets[t]; ty = targets[tstride + t]; tz = targets[2 * tstride + t]; }
-        double acc = 0.0;
+        double acc = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
         if (active) {
             for (int32_t l = ls + ph; l < le; l += nph) {
                 const int32_t sb = src_lists[l];
                 const double *M = src + (int64_t)(sb - sbase) * N;
-                laplace_layers<P>(tx - centers[sb], ty - centers[cstride + sb],
-                                  tz - centers[2 * cstride + sb], rscale, Rinv,
-                                  [&](int s, double v) { acc += __ldg(M + s) * v; });
+                // value: degrees <= P; gradient: d/dt D[mi] = D[mi + e_d] / rscale,
+                // with D on (2, j, k) = -D(0, j+2, k) - D(0, j, k+2)
+                laplace_layers<GRAD ? P + 1 : P>(
+                    tx - centers[sb], ty - centers[cstride + sb], tz - centers[2 * cstride + sb],
+                    rscale, Rinv, [&](int s, int i, int j, int k, double v) {
+                        const int deg = i + j + k;
+                        if (deg <= P) acc += __ldg(M + s) * v;
+                        if (GRAD && deg >= 1) {
+                            if (j >= 1) gy += __ldg(M + stored_index(i, j - 1, k)) * v;
+                            if (k >= 1) gz += __ldg(M + stored_index(i, j, k - 1)) * v;
+                            if (i == 1) {
+                                gx += __ldg(M + stored_index(0, j, k)) * v;
+                            } else {
+                                if (j >= 2) gx -= __ldg(M + stored_index(1, j - 2, k)) * v;
+                                if (k >= 2) gx -= __ldg(M + stored_index(1, j, k - 2)) * v;
+                            }
+                        }
+                    });
             }
         }
-        for (int off = g; off < 32; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-        if (active && ph == 0) result[t] += scale * acc;
+        for (int off = g; off < 32; off <<= 1) {
+            acc += __shfl_xor_sync(0xffffffffu, acc, off);
+            if (GRAD) {
+                gx += __shfl_xor_sync(0xffffffffu, gx, off);
+                gy += __shfl_xor_sync(0xffffffffu, gy, off);
+                gz += __shfl_xor_sync(0xffffffffu, gz, off);
+            }
+        }
+        if (active && ph == 0) {
+            if (result) result[t] += scale * acc;
+            if (GRAD) {
+                const double gs = scale * Rinv;
+                grad[t] += gs * gx;
+                grad[tstride + t] += gs * gy;
+                grad[2 * tstride + t] += gs * gz;
+            }
+        }
     }
 }
 
@@ -483,7 +532,7 @@ p2l_reg_kernel(double rscale, int32_t ntgt_boxes, const int32_t *__restrict__ ta
             const double qq = q[s];
             laplace_layers<P>(c0 - sources[s], c1 - sources[sstride + s],
                               c2 - sources[2 * sstride + s], rscale, Rinv,
-                              [&](int k, double v) { D[k * DSTRIDE + lane] = qq * v; });
+                              [&](int k, int, int, int, double v) { D[k * DSTRIDE + lane] = qq * v; });
         }
         __syncwarp();
 #pragma unroll
@@ -505,17 +554,17 @@ p2l_reg_kernel(double rscale, int32_t ntgt_boxes, const int32_t *__restrict__ ta
     }
 }
 
-template <int P>
+template <int P, bool GRAD>
 int launch_m2p_reg(double rscale, int32_t ntgt_boxes, const int32_t *target_boxes,
                    const int32_t *src_starts, const int32_t *src_lists, const double *centers,
                    int64_t cstride, int32_t sbase, const double *src, const int32_t *bts,
                    const int32_t *btc, const double *targets, int64_t tstride, double scale,
-                   double *result, cudaStream_t st)
+                   double *result, double *grad, cudaStream_t st)
 {
     const int blocks = (ntgt_boxes + E2P_WARPS - 1) / E2P_WARPS;
-    m2p_reg_kernel<P><<<blocks, 32 * E2P_WARPS, 0, st>>>(rscale, ntgt_boxes, target_boxes, src_starts,
-                                                         src_lists, centers, cstride, sbase, src, bts,
-                                                         btc, targets, tstride, scale, result);
+    m2p_reg_kernel<P, GRAD><<<blocks, 32 * E2P_WARPS, 0, st>>>(
+        rscale, ntgt_boxes, target_boxes, src_starts, src_lists, centers, cstride, sbase, src, bts,
+        btc, targets, tstride, scale, result, grad);
     return check_launch("m2p_reg_kernel");
 }
 
@@ -632,6 +681,39 @@ int sumpy_e2e_from_parent_f64(int src_order, int tgt_order, double src_rscale,
     return check_launch("l2l_kernel");
 }
 
+static int launch_l2p(bool grad_on, int order, double rscale, int32_t ntgt_boxes,
+                      const int32_t *target_boxes, const double *centers, int64_t center_stride,
+                      int32_t src_base_ibox, const double *src_expansions,
+                      const int32_t *box_target_starts, const int32_t *box_target_counts_nonchild,
+                      const double *targets, int64_t target_stride, double scale, double *result,
+                      double *grad, void *stream)
+{
+    if (!order_ok(order)) { set_last_error("l2p: unsupported order"); return SUMPY_EUNSUPPORTED; }
+    if (ntgt_boxes < 0) return bad_arg("l2p: ntgt_boxes < 0");
+    if (ntgt_boxes == 0) return SUMPY_OK;
+    if (!target_boxes || !centers || !src_expansions || !box_target_starts ||
+        !box_target_counts_nonchild || !targets || (!result && !grad_on) || (grad_on && !grad))
+        return bad_arg("l2p: null pointer argument");
+    const int P1 = order + 1;
+    const size_t per_warp = sizeof(double) * (P1 * P1 * P1 + P1 + 1);
+    int warps = (int)std::max<size_t>(1, std::min<size_t>(L2P_MAX_WARPS, (48 * 1024) / per_warp));
+    const size_t smem = per_warp * warps;
+    int rc = grad_on ? prepare_smem(l2p_kernel<true>, smem) : prepare_smem(l2p_kernel<false>, smem);
+    if (rc) return rc;
+    const int blocks = (ntgt_boxes + warps - 1) / warps;
+    if (grad_on)
+        l2p_kernel<true><<<blocks, 32 * warps, smem, as_stream(stream)>>>(
+            order, rscale, ntgt_boxes, target_boxes, centers, center_stride, src_base_ibox,
+            src_expansions, box_target_starts, box_target_counts_nonchild, targets, target_stride,
+            scale, result, grad);
+    else
+        l2p_kernel<false><<<blocks, 32 * warps, smem, as_stream(stream)>>>(
+            order, rscale, ntgt_boxes, target_boxes, centers, center_stride, src_base_ibox,
+            src_expansions, box_target_starts, box_target_counts_nonchild, targets, target_stride,
+            scale, result, nullptr);
+    return check_launch("l2p_kernel");
+}
+
 int sumpy_e2p_from_single_box_f64(int order, double rscale, int32_t ntgt_boxes,
                                   const int32_t *target_boxes, const double *centers,
                                   int64_t center_stride, int32_t src_base_ibox,
@@ -640,24 +722,55 @@ int sumpy_e2p_from_single_box_f64(int order, double rscale, int32_t ntgt_boxes,
                                   const double *targets, int64_t target_stride, double scale,
                                   double *result, void *stream)
 {
-    if (!order_ok(order)) { set_last_error("l2p: unsupported order"); return SUMPY_EUNSUPPORTED; }
-    if (ntgt_boxes < 0) return bad_arg("l2p: ntgt_boxes < 0");
+    return launch_l2p(false, order, rscale, ntgt_boxes, target_boxes, centers, center_stride,
+                      src_base_ibox, src_expansions, box_target_starts,
+                      box_target_counts_nonchild, targets, target_stride, scale, result, nullptr,
+                      stream);
+}
+
+int sumpy_e2p_from_single_box_grad_f64(int order, double rscale, int32_t ntgt_boxes,
+                                       const int32_t *target_boxes, const double *centers,
+                                       int64_t center_stride, int32_t src_base_ibox,
+                                       const double *src_expansions,
+                                       const int32_t *box_target_starts,
+                                       const int32_t *box_target_counts_nonchild,
+                                       const double *targets, int64_t target_stride, double scale,
+                                       double *result, double *grad, void *stream)
+{
+    return launch_l2p(true, order, rscale, ntgt_boxes, target_boxes, centers, center_stride,
+                      src_base_ibox, src_expansions, box_target_starts,
+                      box_target_counts_nonchild, targets, target_stride, scale, result, grad,
+                      stream);
+}
+
+static int launch_m2p(bool grad_on, int order, double rscale, int32_t ntgt_boxes,
+                      const int32_t *target_boxes, const int32_t *source_box_starts,
+                      const int32_t *source_box_lists, const double *centers,
+                      int64_t center_stride, int32_t src_base_ibox, const double *src_expansions,
+                      const int32_t *box_target_starts, const int32_t *box_target_counts_nonchild,
+                      const double *targets, int64_t target_stride, double scale, double *result,
+                      double *grad, void *stream)
+{
+    if (!order_ok(order)) { set_last_error("m2p: unsupported order"); return SUMPY_EUNSUPPORTED; }
+    if (ntgt_boxes < 0) return bad_arg("m2p: ntgt_boxes < 0");
     if (ntgt_boxes == 0) return SUMPY_OK;
-    if (!target_boxes || !centers || !src_expansions || !box_target_starts ||
-        !box_target_counts_nonchild || !targets || !result)
-        return bad_arg("l2p: null pointer argument");
-    const int P1 = order + 1;
-    const size_t per_warp = sizeof(double) * (P1 * P1 * P1 + P1 + 1);
-    int warps = (int)std::max<size_t>(1, std::min<size_t>(L2P_MAX_WARPS, (48 * 1024) / per_warp));
-    const size_t smem = per_warp * warps;
-    int rc = prepare_smem(l2p_kernel, smem);
-    if (rc) return rc;
-    const int blocks = (ntgt_boxes + warps - 1) / warps;
-    l2p_kernel<<<blocks, 32 * warps, smem, as_stream(stream)>>>(
-        order, rscale, ntgt_boxes, target_boxes, centers, center_stride, src_base_ibox,
-        src_expansions, box_target_starts, box_target_counts_nonchild, targets, target_stride,
-        scale, result);
-    return check_launch("l2p_kernel");
+    if (!target_boxes || !source_box_starts || !source_box_lists || !centers ||
+        !src_expansions || !box_target_starts || !box_target_counts_nonchild || !targets ||
+        (!result && !grad_on) || (grad_on && !grad))
+        return bad_arg("m2p: null pointer argument");
+#define CALL_M2P(P)                                                                              \
+    (grad_on ? launch_m2p_reg<P, true>(rscale, ntgt_boxes, target_boxes, source_box_starts,     \
+                                       source_box_lists, centers, center_stride, src_base_ibox, \
+                                       src_expansions, box_target_starts,                       \
+                                       box_target_counts_nonchild, targets, target_stride,      \
+                                       scale, result, grad, as_stream(stream))                   \
+             : launch_m2p_reg<P, false>(rscale, ntgt_boxes, target_boxes, source_box_starts,    \
+                                        source_box_lists, centers, center_stride, src_base_ibox, \
+                                        src_expansions, box_target_starts,                      \
+                                        box_target_counts_nonchild, targets, target_stride,     \
+                                        scale, result, nullptr, as_stream(stream)))
+    SUMPY_ORDER_SWITCH(order, CALL_M2P)
+#undef CALL_M2P
 }
 
 int sumpy_e2p_from_csr_f64(int order, double rscale, int32_t ntgt_boxes,
@@ -668,20 +781,25 @@ int sumpy_e2p_from_csr_f64(int order, double rscale, int32_t ntgt_boxes,
                            const int32_t *box_target_counts_nonchild, const double *targets,
                            int64_t target_stride, double scale, double *result, void *stream)
 {
-    if (!order_ok(order)) { set_last_error("m2p: unsupported order"); return SUMPY_EUNSUPPORTED; }
-    if (ntgt_boxes < 0) return bad_arg("m2p: ntgt_boxes < 0");
-    if (ntgt_boxes == 0) return SUMPY_OK;
-    if (!target_boxes || !source_box_starts || !source_box_lists || !centers ||
-        !src_expansions || !box_target_starts || !box_target_counts_nonchild || !targets ||
-        !result)
-        return bad_arg("m2p: null pointer argument");
-#define CALL_M2P(P)                                                                             \
-    launch_m2p_reg<P>(rscale, ntgt_boxes, target_boxes, source_box_starts, source_box_lists,   \
-                      centers, center_stride, src_base_ibox, src_expansions, box_target_starts, \
-                      box_target_counts_nonchild, targets, target_stride, scale, result,        \
-                      as_stream(stream))
-    SUMPY_ORDER_SWITCH(order, CALL_M2P)
-#undef CALL_M2P
+    return launch_m2p(false, order, rscale, ntgt_boxes, target_boxes, source_box_starts,
+                      source_box_lists, centers, center_stride, src_base_ibox, src_expansions,
+                      box_target_starts, box_target_counts_nonchild, targets, target_stride,
+                      scale, result, nullptr, stream);
+}
+
+int sumpy_e2p_from_csr_grad_f64(int order, double rscale, int32_t ntgt_boxes,
+                                const int32_t *target_boxes, const int32_t *source_box_starts,
+                                const int32_t *source_box_lists, const double *centers,
+                                int64_t center_stride, int32_t src_base_ibox,
+                                const double *src_expansions, const int32_t *box_target_starts,
+                                const int32_t *box_target_counts_nonchild,
+                                const double *targets, int64_t target_stride, double scale,
+                                double *result, double *grad, void *stream)
+{
+    return launch_m2p(true, order, rscale, ntgt_boxes, target_boxes, source_box_starts,
+                      source_box_lists, centers, center_stride, src_base_ibox, src_expansions,
+                      box_target_starts, box_target_counts_nonchild, targets, target_stride,
+                      scale, result, grad, stream);
 }
 
 int sumpy_p2e_from_csr_f64(int order, double rscale, int32_t ntgt_boxes,

@@ -95,7 +95,7 @@ class SumpyExpansionWrangler:
                  source_extra_kwargs=None, kernel_extra_kwargs=None,
                  self_extra_kwargs=None, translation_classes_data=None,
                  preprocessed_mpole_dtype=None, *, _disable_translation_classes=False,
-                 precision="fp64", device=None):
+                 precision="fp64", device=None, gradient=False):
         if not callable(fmm_level_to_order):
             raise TypeError("fmm_level_to_order not passed")
         if np.dtype(dtype) != np.float64:
@@ -107,6 +107,7 @@ class SumpyExpansionWrangler:
         self.tree = traversal.tree
         self.dtype = np.dtype(dtype)
         self.precision = precision
+        self.gradient = bool(gradient)
         self.source_extra_kwargs = source_extra_kwargs or {}
         self.kernel_extra_kwargs = kernel_extra_kwargs or {}
         self.self_extra_kwargs = self_extra_kwargs or {}
@@ -176,6 +177,12 @@ class SumpyExpansionWrangler:
         return torch.zeros(self._local_level_starts[-1], dtype=torch.float64, device=self.device)
 
     def output_zeros(self, actx=None):
+        """Potential per target kernel; with ``gradient=True`` the potential
+        and its three target-coordinate derivatives (rows of one (4, n)
+        buffer, so the derivative rows form a contiguous [3][n] block)."""
+        if self.gradient:
+            buf = torch.zeros((4, self.tree.ntargets), dtype=torch.float64, device=self.device)
+            return [buf[0], buf[1], buf[2], buf[3]]
         return [torch.zeros(self.tree.ntargets, dtype=torch.float64, device=self.device)
                 for _ in self.tree_indep.target_kernels]
 
@@ -304,13 +311,18 @@ class SumpyExpansionWrangler:
             return pot
         g = self._geom
         w = self._weights(src_weight_vecs)
-        fn = ("sumpy_p2p_from_csr_mixed" if self.precision == "mixed"
-              else "sumpy_p2p_from_csr_f64")
-        call(fn, _i32(tb.numel()), dptr(tb), dptr(self._dev(source_box_starts)),
-             dptr(self._dev(source_box_lists)), dptr(g["bss"]), dptr(g["bsc"]),
-             dptr(g["bts"]), dptr(g["btc"]), dptr(g["sources"]), _i64(self.tree.nsources),
-             dptr(w), dptr(g["targets"]), _i64(self.tree.ntargets), dptr(g["tts"]),
-             _d(self._scale), dptr(pot[0]), stream_ptr())
+        args = (_i32(tb.numel()), dptr(tb), dptr(self._dev(source_box_starts)),
+                dptr(self._dev(source_box_lists)), dptr(g["bss"]), dptr(g["bsc"]),
+                dptr(g["bts"]), dptr(g["btc"]), dptr(g["sources"]), _i64(self.tree.nsources),
+                dptr(w), dptr(g["targets"]), _i64(self.tree.ntargets), dptr(g["tts"]),
+                _d(self._scale), dptr(pot[0]))
+        mixed = self.precision == "mixed"
+        if self.gradient:
+            call("sumpy_p2p_from_csr_grad_mixed" if mixed else "sumpy_p2p_from_csr_grad_f64",
+                 *args, dptr(pot[1]), stream_ptr())
+        else:
+            call("sumpy_p2p_from_csr_mixed" if mixed else "sumpy_p2p_from_csr_f64",
+                 *args, stream_ptr())
         return pot
 
     # {{{ M2L
@@ -598,12 +610,16 @@ class SumpyExpansionWrangler:
                 continue
             sbase, sview = self.multipole_expansions_view(mpole_exps, lev)
             tbd = self._dev(tb)
-            call("sumpy_e2p_from_csr_f64", _c(self.level_orders[lev]),
-                 _d(self.level_to_rscale(lev)), _i32(tbd.numel()), dptr(tbd),
-                 dptr(self._dev(ssn.starts)), dptr(self._dev(ssn.lists)), dptr(g["centers"]),
-                 _i64(self.tree.nboxes), _i32(sbase), dptr(sview), dptr(g["bts"]),
-                 dptr(g["btc"]), dptr(g["targets"]), _i64(self.tree.ntargets),
-                 _d(self._scale), dptr(pot[0]), st)
+            args = (_c(self.level_orders[lev]), _d(self.level_to_rscale(lev)),
+                    _i32(tbd.numel()), dptr(tbd), dptr(self._dev(ssn.starts)),
+                    dptr(self._dev(ssn.lists)), dptr(g["centers"]), _i64(self.tree.nboxes),
+                    _i32(sbase), dptr(sview), dptr(g["bts"]), dptr(g["btc"]),
+                    dptr(g["targets"]), _i64(self.tree.ntargets), _d(self._scale),
+                    dptr(pot[0]))
+            if self.gradient:
+                call("sumpy_e2p_from_csr_grad_f64", *args, dptr(pot[1]), st)
+            else:
+                call("sumpy_e2p_from_csr_f64", *args, st)
         return pot
 
     def form_locals(self, actx, level_start_target_or_target_parent_box_nrs,
@@ -661,11 +677,14 @@ class SumpyExpansionWrangler:
             if a == b:
                 continue
             sbase, sview = self.local_expansions_view(local_exps, lev)
-            call("sumpy_e2p_from_single_box_f64", _c(self.level_orders[lev]),
-                 _d(self.level_to_rscale(lev)), _i32(b - a), dptr(boxes[a:b]),
-                 dptr(g["centers"]), _i64(self.tree.nboxes), _i32(sbase), dptr(sview),
-                 dptr(g["bts"]), dptr(g["btc"]), dptr(g["targets"]), _i64(self.tree.ntargets),
-                 _d(self._scale), dptr(pot[0]), st)
+            args = (_c(self.level_orders[lev]), _d(self.level_to_rscale(lev)), _i32(b - a),
+                    dptr(boxes[a:b]), dptr(g["centers"]), _i64(self.tree.nboxes), _i32(sbase),
+                    dptr(sview), dptr(g["bts"]), dptr(g["btc"]), dptr(g["targets"]),
+                    _i64(self.tree.ntargets), _d(self._scale), dptr(pot[0]))
+            if self.gradient:
+                call("sumpy_e2p_from_single_box_grad_f64", *args, dptr(pot[1]), st)
+            else:
+                call("sumpy_e2p_from_single_box_f64", *args, st)
         return pot
 
     # }}}

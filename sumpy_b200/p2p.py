@@ -21,12 +21,16 @@ def _soa(x, device):
 
 
 class P2P:
+    """With ``gradient=True`` the call returns ``[potential, d/dx, d/dy, d/dz]``
+    (derivatives with respect to the target coordinates)."""
+
     def __init__(self, target_kernels, exclude_self=False, strength_usage=None,
-                 source_kernels=None, value_dtypes=None, name=None):
+                 source_kernels=None, value_dtypes=None, name=None, gradient=False):
         if len(target_kernels) != 1:
             raise NotImplementedError("exactly one target kernel is supported")
         self.target_kernels = list(target_kernels)
         self.exclude_self = exclude_self
+        self.gradient = gradient
 
     def __call__(self, actx, targets, sources, strength, target_to_source=None,
                  device="cuda", **kwargs):
@@ -40,9 +44,13 @@ class P2P:
             if target_to_source is None:
                 raise ValueError("exclude_self needs target_to_source")
             tts = torch.as_tensor(target_to_source).to(dev, torch.int32).contiguous()
-        out = torch.empty(t.shape[1], dtype=torch.float64, device=dev)
         scale = self.target_kernels[0].global_scaling_const
-        call("sumpy_p2p_direct_f64", _capi.i64(t.shape[1]), dptr(t), _capi.i64(t.shape[1]),
-             _capi.i64(s.shape[1]), dptr(s), _capi.i64(s.shape[1]), dptr(q), dptr(tts),
-             _capi.dbl(scale), dptr(out), stream_ptr())
+        args = (_capi.i64(t.shape[1]), dptr(t), _capi.i64(t.shape[1]), _capi.i64(s.shape[1]),
+                dptr(s), _capi.i64(s.shape[1]), dptr(q), dptr(tts), _capi.dbl(scale))
+        if self.gradient:
+            buf = torch.empty((4, t.shape[1]), dtype=torch.float64, device=dev)
+            call("sumpy_p2p_direct_grad_f64", *args, dptr(buf[0]), dptr(buf[1]), stream_ptr())
+            return [buf[0], buf[1], buf[2], buf[3]]
+        out = torch.empty(t.shape[1], dtype=torch.float64, device=dev)
+        call("sumpy_p2p_direct_f64", *args, dptr(out), stream_ptr())
         return [out]
