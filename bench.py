@@ -290,6 +290,7 @@ def main():
     err_64 = rel(drive_fmm(None, w_64, [q_dev])[0].cpu().numpy()) if w_64 is not None else None
 
     stage_ms, roof = stage_breakdown(w_mx, trav, q_dev, dev)
+    adj = adjoint_bench(dev) if world == 1 else None
 
     value = world * args.npoints / (ms_mx * 1e-3) / 1e6
     line = {
@@ -311,7 +312,8 @@ def main():
         "fp64": {"value": (world * args.npoints / (ms_64 * 1e-3) / 1e6) if ms_64 else None,
                  "ms_per_step": ms_64},
         "mixed_over_fp64": (ms_64 / ms_mx) if ms_64 else None,
-        "adjoint_forward_ratio": None,
+        "adjoint_forward_ratio": adj["ratio"] if adj else None,
+        "adjoint": adj,
         "stage_ms": stage_ms,
         "roofline": roof,
         "cpu_baseline": cpu_line,
@@ -324,6 +326,71 @@ def main():
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def adjoint_bench(dev, steps=3, ns=200_000, nt=50_000, order=8):
+    """Backward/forward time ratio of the differentiable potential: 200k
+    sources on the unit sphere perturbed radially by 0.05*N(0,1), 50k
+    targets uniform in the shell 2 <= r <= 3, p = 8, mixed precision, loss
+    0.5*|phi - phi_ref|^2 with phi_ref the FP64 direct sum at the unperturbed
+    positions. Forward = one FMM; backward = transposed-traversal FMM with
+    gradient-form evaluation (strength and source-position gradients). Trees
+    and schedules are built before timing; times are CUDA events."""
+    import torch
+    from sumpy_b200 import P2P, LaplaceKernel, drive_fmm
+    from sumpy_b200.adjoint import transpose_traversal
+    from sumpy_b200.autograd import _Config, _wrangler
+    from sumpy_b200.tree import build_all
+    rng = np.random.default_rng(7)
+    g = rng.standard_normal((3, ns))
+    u = g / np.linalg.norm(g, axis=0)
+    src = (1 + 0.05 * rng.standard_normal(ns)) * u
+    d = rng.standard_normal((3, nt))
+    d /= np.linalg.norm(d, axis=0)
+    tgt = np.cbrt(8 + 19 * rng.random(nt)) * d
+    q = rng.standard_normal(ns)
+    knl = [LaplaceKernel(3)]
+    (phi_ref,) = P2P(knl)(None, tgt, u, (q,), device=dev)
+    cfg = _Config(order, 32, "mixed", dev)
+    tree, trav, tcls = build_all(src, tgt, 32)
+    tree_t, trav_t, tcls_t = transpose_traversal(tree, trav, tcls)
+    wf = _wrangler(cfg, tree, trav, tcls, False, gradient=False)
+    wb = _wrangler(cfg, tree_t, trav_t, tcls_t, False, gradient=True)
+    qd = torch.as_tensor(q, device=dev)
+
+    def fwd():
+        return drive_fmm(None, wf, [qd])[0]
+
+    phi = fwd()
+    gd = (phi - phi_ref).contiguous()
+
+    def bwd():
+        out = drive_fmm(None, wb, [gd])
+        return out[0], qd * torch.stack(out[1:4])
+
+    def tm(fn):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    t_f, t_b = tm(fwd), tm(bwd)
+    gq, gsrc = bwd()
+    gdn = gd.cpu().numpy()
+    psi = P2P(knl, gradient=True)(None, src, tgt, (gdn,), device=dev)
+    gq_ref = psi[0]
+    gsrc_ref = qd * torch.stack(psi[1:4])
+    rel = lambda a, b: float((a - b).norm() / b.norm())
+    return {"forward_ms": t_f, "backward_ms": t_b, "ratio": t_b / t_f,
+            "grad_strength_relL2_vs_direct": rel(gq, gq_ref),
+            "grad_source_pos_relL2_vs_direct": rel(gsrc, gsrc_ref),
+            "workload": f"sphere(perturbed) {ns} sources -> shell {nt} targets, p={order}, mixed"}
 
 
 def stage_breakdown(w, trav, q_dev, dev):
