@@ -82,22 +82,6 @@ __device__ void compress_cube_block(double *cube, int p)
     }
 }
 
-// stored local in planes 0, 1 -> full local (planes 2..p). Block-wide.
-__device__ void decompress_cube_block(double *cube, int p)
-{
-    for (int i = 2; i <= p; ++i) {
-        const int m = p - i;
-        const int npairs = (m + 1) * (m + 2) / 2;
-        for (int t = threadIdx.x; t < npairs; t += blockDim.x) {
-            int J, K;
-            tri_pair(t, m, J, K);
-            cube[cube_index(p, i, J, K)] =
-                -cube[cube_index(p, i - 2, J + 2, K)] - cube[cube_index(p, i - 2, J, K + 2)];
-        }
-        __syncthreads();
-    }
-}
-
 // same, one warp
 __device__ void decompress_cube_warp(double *cube, int p, int lane)
 {
@@ -178,141 +162,213 @@ p2m_kernel(int p, double rscale, const int32_t *__restrict__ boxes, const double
 
 // {{{ M2M / L2L (axis-by-axis shifts)
 
-constexpr int E2E_THREADS = 128;
-
-// out[m] = sum_{t=0}^{m_d} in[m with m_d = t] * pw[m_d - t]  (multipole shift)
-__device__ void mpole_shift_axis(const double *in, double *out, int p, int d, const double *pw)
+// Index of (i, j, k) in sumpy's full order (|mi|, mi0, mi1, mi2):
+// tetra(deg) + sum_{i' < i} (deg - i' + 1) + j.
+__device__ __forceinline__ int full_index(int i, int j, int k)
 {
-    const int nfull = nfull_of(p);
-    for (int f = threadIdx.x; f < nfull; f += blockDim.x) {
-        int m[3];
-        full_mi(f, m[0], m[1], m[2]);
-        double acc = 0.0;
-        for (int t = 0; t <= m[d]; ++t) {
-            int q[3] = {m[0], m[1], m[2]};
-            q[d] = t;
-            acc += in[cube_index(p, q[0], q[1], q[2])] * pw[m[d] - t];
-        }
-        out[cube_index(p, m[0], m[1], m[2])] = acc;
-    }
+    const int deg = i + j + k;
+    return deg * (deg + 1) * (deg + 2) / 6 + i * (deg + 1) - i * (i - 1) / 2 + j;
 }
 
-// out[m] = sum_{q=0}^{p-|m|} in[m + q e_d] * pw[q]  (local shift)
-__device__ void local_shift_axis(const double *in, double *out, int p, int d, const double *pw)
-{
-    const int nfull = nfull_of(p);
-    for (int f = threadIdx.x; f < nfull; f += blockDim.x) {
-        int m[3];
-        full_mi(f, m[0], m[1], m[2]);
-        const int deg = m[0] + m[1] + m[2];
-        double acc = 0.0;
-        for (int q = 0; q <= p - deg; ++q) {
-            int s[3] = {m[0], m[1], m[2]};
-            s[d] += q;
-            acc += in[cube_index(p, s[0], s[1], s[2])] * pw[q];
-        }
-        out[cube_index(p, m[0], m[1], m[2])] = acc;
-    }
-}
+constexpr int M2M_THREADS = 256;
 
-__global__ void __launch_bounds__(E2E_THREADS)
-m2m_kernel(int ps, int pt, double rsrc, double rtgt, const int32_t *__restrict__ boxes,
-           const int32_t *__restrict__ child_ids, int64_t child_stride,
-           const double *__restrict__ centers, int64_t cstride, int32_t sbase,
-           const double *__restrict__ src, int32_t tbase, double *__restrict__ tgt)
+// M2M with the eight children shifted concurrently: threads run over
+// (child, full coefficient) pairs, each child's full coefficients in a
+// compact buffer of nfull values, so one parent costs three parallel shift
+// passes, one sum over children and one compression.
+__global__ void __launch_bounds__(M2M_THREADS)
+m2m_children_kernel(int ps, int pt, double rsrc, double rtgt, const int32_t *__restrict__ boxes,
+                    const int32_t *__restrict__ child_ids, int64_t child_stride,
+                    const double *__restrict__ centers, int64_t cstride, int32_t sbase,
+                    const double *__restrict__ src, int32_t tbase, double *__restrict__ tgt)
 {
     extern __shared__ double sm[];
-    const int P1 = pt + 1, C = P1 * P1 * P1;
-    double *A = sm, *B = A + C, *ACC = B + C, *pw = ACC + C;  // pw: [3][P1]
+    const int P1 = pt + 1;
+    const int nfull = nfull_of(pt);
+    double *A = sm;                         // [8][nfull]
+    double *B = A + 8 * nfull;              // [8][nfull]
+    double *pw = B + 8 * nfull;             // [8][3][P1]
+    uint32_t *tab = reinterpret_cast<uint32_t *>(pw + 8 * 3 * P1);  // [nfull] packed (i,j,k)
+    __shared__ int32_t kids[8];
+    __shared__ int nkids;
+
     const int32_t b = boxes[blockIdx.x];
-    const int ns = ncoeff_of(ps), nt = ncoeff_of(pt), nfull = nfull_of(pt);
+    const int ns = ncoeff_of(ps), nt = ncoeff_of(pt);
     const double ratio = rsrc / rtgt;
-
-    for (int t = threadIdx.x; t < C; t += blockDim.x) { ACC[t] = 0.0; A[t] = 0.0; B[t] = 0.0; }
+    if (threadIdx.x == 0) {
+        int c = 0;
+        for (int slot = 0; slot < 8; ++slot) {
+            const int32_t ch = child_ids[slot * child_stride + b];
+            if (ch != 0) kids[c++] = ch;
+        }
+        nkids = c;
+    }
+    for (int f = threadIdx.x; f < nfull; f += blockDim.x) {
+        int i, j, k;
+        full_mi(f, i, j, k);
+        tab[f] = (uint32_t)i | ((uint32_t)j << 8) | ((uint32_t)k << 16);
+    }
     __syncthreads();
-    for (int slot = 0; slot < 8; ++slot) {
-        const int32_t ch = child_ids[slot * child_stride + b];
-        if (ch == 0) continue;
-        if (threadIdx.x < 3) {
-            const int d = threadIdx.x;
-            const double dd = (centers[d * cstride + b] - centers[d * cstride + ch]) / rtgt;
-            double *w = pw + d * P1;
-            w[0] = 1.0;
-            for (int k = 1; k <= pt; ++k) w[k] = w[k - 1] * dd / k;
+    const int nk = nkids;
+    for (int t = threadIdx.x; t < nk * 3; t += blockDim.x) {
+        const int c = t / 3, d = t % 3;
+        const int32_t ch = kids[c];
+        const double dd = (centers[d * cstride + b] - centers[d * cstride + ch]) / rtgt;
+        double *w = pw + (c * 3 + d) * P1;
+        w[0] = 1.0;
+        for (int q = 1; q <= pt; ++q) w[q] = w[q - 1] * dd / q;
+    }
+    for (int t = threadIdx.x; t < nk * nfull; t += blockDim.x) {
+        const int c = t / nfull, f = t % nfull;
+        const uint32_t e = tab[f];
+        const int i = e & 0xff, j = (e >> 8) & 0xff, k = e >> 16;
+        const int deg = i + j + k;
+        double v = 0.0;
+        if (i < 2 && deg <= ps)
+            v = src[(int64_t)(kids[c] - sbase) * ns + stored_index(i, j, k)] * ipow(ratio, deg);
+        A[c * nfull + f] = v;
+    }
+    __syncthreads();
+    // axes in the order 1, 2, 0: sumpy/expansion/multipole.py:329 for the axis-0
+    // hyperplanes of the Laplace stored set
+    const int axes[3] = {1, 2, 0};
+    double *in = A, *out = B;
+#pragma unroll 1
+    for (int a = 0; a < 3; ++a) {
+        const int d = axes[a];
+        for (int t = threadIdx.x; t < nk * nfull; t += blockDim.x) {
+            const int c = t / nfull, f = t % nfull;
+            const uint32_t e = tab[f];
+            int m[3] = {(int)(e & 0xff), (int)((e >> 8) & 0xff), (int)(e >> 16)};
+            const double *w = pw + (c * 3 + d) * P1;
+            const double *inc = in + c * nfull;
+            const int md = m[d];
+            double acc = 0.0;
+            for (int q = 0; q <= md; ++q) {
+                m[d] = q;
+                acc += inc[full_index(m[0], m[1], m[2])] * w[md - q];
+            }
+            out[c * nfull + f] = acc;
         }
-        const double *cs = src + (int64_t)(ch - sbase) * ns;
-        for (int f = threadIdx.x; f < nfull; f += blockDim.x) {
-            int i, j, k;
-            full_mi(f, i, j, k);
-            const int deg = i + j + k;
+        __syncthreads();
+        double *sw = in; in = out; out = sw;
+    }
+    // sum over children into out[0..nfull) then compress in place
+    double *accv = out;
+    for (int f = threadIdx.x; f < nfull; f += blockDim.x) {
+        double v = 0.0;
+        for (int c = 0; c < nk; ++c) v += in[c * nfull + f];
+        accv[f] = v;
+    }
+    __syncthreads();
+    for (int i = pt; i >= 2; --i) {
+        const int m = pt - i + 2;
+        const int npairs = (m + 1) * (m + 2) / 2;
+        for (int t = threadIdx.x; t < npairs; t += blockDim.x) {
+            int J, K;
+            tri_pair(t, m, J, K);
             double v = 0.0;
-            if (i < 2 && deg <= ps) v = cs[stored_index(i, j, k)] * ipow(ratio, deg);
-            A[cube_index(pt, i, j, k)] = v;
-        }
-        __syncthreads();
-        mpole_shift_axis(A, B, pt, 1, pw + 1 * P1);
-        __syncthreads();
-        mpole_shift_axis(B, A, pt, 2, pw + 2 * P1);
-        __syncthreads();
-        mpole_shift_axis(A, B, pt, 0, pw + 0 * P1);
-        __syncthreads();
-        for (int f = threadIdx.x; f < nfull; f += blockDim.x) {
-            int i, j, k;
-            full_mi(f, i, j, k);
-            ACC[cube_index(pt, i, j, k)] += B[cube_index(pt, i, j, k)];
+            if (J >= 2) v += accv[full_index(i, J - 2, K)];
+            if (K >= 2) v += accv[full_index(i, J, K - 2)];
+            accv[full_index(i - 2, J, K)] -= v;
         }
         __syncthreads();
     }
-    compress_cube_block(ACC, pt);
     double *o = tgt + (int64_t)(b - tbase) * nt;
-    for (int s = threadIdx.x; s < nt; s += blockDim.x) {
+    for (int s2 = threadIdx.x; s2 < nt; s2 += blockDim.x) {
         int i, j, k;
-        stored_mi(s, i, j, k);
-        o[s] += ACC[cube_index(pt, i, j, k)];
+        stored_mi(s2, i, j, k);
+        o[s2] += accv[full_index(i, j, k)];
     }
 }
 
-__global__ void __launch_bounds__(E2E_THREADS)
-l2l_kernel(int ps, int pt, double rsrc, double rtgt, const int32_t *__restrict__ boxes,
-           const int32_t *__restrict__ parent_ids, const double *__restrict__ centers,
-           int64_t cstride, int32_t sbase, const double *__restrict__ src, int32_t tbase,
-           double *__restrict__ tgt)
+constexpr int L2L_BOXES = 8;
+
+// L2L for up to eight target boxes per CTA, concurrently: each box's parent
+// local is decompressed into the box's own compact buffer (p-1 sweeps over
+// the mi0 planes, all boxes at once), then shifted one axis at a time
+// (axes 0, 1, 2) and accumulated into the box's local.
+__global__ void __launch_bounds__(M2M_THREADS)
+l2l_boxes_kernel(int ps, int pt, double rsrc, double rtgt, int32_t nboxes,
+                 const int32_t *__restrict__ boxes, const int32_t *__restrict__ parent_ids,
+                 const double *__restrict__ centers, int64_t cstride, int32_t sbase,
+                 const double *__restrict__ src, int32_t tbase, double *__restrict__ tgt)
 {
     extern __shared__ double sm[];
-    const int P1 = ps + 1, C = P1 * P1 * P1;
-    double *A = sm, *B = A + C, *pw = B + C;  // pw: [3][P1]
-    const int32_t b = boxes[blockIdx.x];
-    const int32_t par = parent_ids[b];
-    const int ns = ncoeff_of(ps), nt = ncoeff_of(pt), nfull = nfull_of(ps);
+    const int P1 = ps + 1;
+    const int nfull = nfull_of(ps);
+    double *A = sm;                                   // [8][nfull]
+    double *B = A + L2L_BOXES * nfull;                // [8][nfull]
+    double *pw = B + L2L_BOXES * nfull;               // [8][3][P1]
+    uint32_t *tab = reinterpret_cast<uint32_t *>(pw + L2L_BOXES * 3 * P1);
+    const int b0 = blockIdx.x * L2L_BOXES;
+    const int nk = min(L2L_BOXES, nboxes - b0);
+    const int ns = ncoeff_of(ps), nt = ncoeff_of(pt);
 
-    if (threadIdx.x < 3) {
-        const int d = threadIdx.x;
+    for (int f = threadIdx.x; f < nfull; f += blockDim.x) {
+        int i, j, k;
+        full_mi(f, i, j, k);
+        tab[f] = (uint32_t)i | ((uint32_t)j << 8) | ((uint32_t)k << 16);
+    }
+    for (int t = threadIdx.x; t < nk * 3; t += blockDim.x) {
+        const int c = t / 3, d = t % 3;
+        const int32_t b = boxes[b0 + c];
+        const int32_t par = parent_ids[b];
         const double dd = (centers[d * cstride + b] - centers[d * cstride + par]) / rsrc;
-        double *w = pw + d * P1;
+        double *w = pw + (c * 3 + d) * P1;
         w[0] = 1.0;
-        for (int k = 1; k <= ps; ++k) w[k] = w[k - 1] * dd / k;
+        for (int q = 1; q <= ps; ++q) w[q] = w[q - 1] * dd / q;
     }
-    const double *cs = src + (int64_t)(par - sbase) * ns;
-    for (int s = threadIdx.x; s < ns; s += blockDim.x) {
+    for (int t = threadIdx.x; t < nk * ns; t += blockDim.x) {
+        const int c = t / ns, s2 = t % ns;
+        const int32_t par = parent_ids[boxes[b0 + c]];
         int i, j, k;
-        stored_mi(s, i, j, k);
-        A[cube_index(ps, i, j, k)] = cs[s];
+        stored_mi(s2, i, j, k);
+        A[c * nfull + full_index(i, j, k)] = src[(int64_t)(par - sbase) * ns + s2];
     }
     __syncthreads();
-    decompress_cube_block(A, ps);
-    local_shift_axis(A, B, ps, 0, pw + 0 * P1);
-    __syncthreads();
-    local_shift_axis(B, A, ps, 1, pw + 1 * P1);
-    __syncthreads();
-    local_shift_axis(A, B, ps, 2, pw + 2 * P1);
-    __syncthreads();
+    for (int i = 2; i <= ps; ++i) {
+        const int m = ps - i;
+        const int npairs = (m + 1) * (m + 2) / 2;
+        for (int t = threadIdx.x; t < nk * npairs; t += blockDim.x) {
+            const int c = t / npairs;
+            int J, K;
+            tri_pair(t % npairs, m, J, K);
+            double *a = A + c * nfull;
+            a[full_index(i, J, K)] = -a[full_index(i - 2, J + 2, K)] - a[full_index(i - 2, J, K + 2)];
+        }
+        __syncthreads();
+    }
+    double *in = A, *out = B;
+#pragma unroll 1
+    for (int d = 0; d < 3; ++d) {
+        for (int t = threadIdx.x; t < nk * nfull; t += blockDim.x) {
+            const int c = t / nfull, f = t % nfull;
+            const uint32_t e = tab[f];
+            int m[3] = {(int)(e & 0xff), (int)((e >> 8) & 0xff), (int)(e >> 16)};
+            const int deg = m[0] + m[1] + m[2];
+            const double *w = pw + (c * 3 + d) * P1;
+            const double *inc = in + c * nfull;
+            const int md = m[d];
+            double acc = 0.0;
+            for (int q = 0; q <= ps - deg; ++q) {
+                m[d] = md + q;
+                acc += inc[full_index(m[0], m[1], m[2])] * w[q];
+            }
+            out[c * nfull + f] = acc;
+        }
+        __syncthreads();
+        double *sw = in; in = out; out = sw;
+    }
     const double ratio = rtgt / rsrc;
-    double *o = tgt + (int64_t)(b - tbase) * nt;
-    for (int s = threadIdx.x; s < nt; s += blockDim.x) {
+    for (int t = threadIdx.x; t < nk * nt; t += blockDim.x) {
+        const int c = t / nt, s2 = t % nt;
         int i, j, k;
-        stored_mi(s, i, j, k);
+        stored_mi(s2, i, j, k);
         const int deg = i + j + k;
-        if (deg <= ps) o[s] += B[cube_index(ps, i, j, k)] * ipow(ratio, deg);
+        if (deg <= ps)
+            tgt[(int64_t)(boxes[b0 + c] - tbase) * nt + s2] +=
+                in[c * nfull + full_index(i, j, k)] * ipow(ratio, deg);
     }
 }
 
@@ -647,13 +703,14 @@ int sumpy_e2e_from_children_f64(int src_order, int tgt_order, double src_rscale,
     if (!target_boxes || !box_child_ids || !centers || !src_expansions || !tgt_expansions)
         return bad_arg("m2m: null pointer argument");
     const int P1 = tgt_order + 1;
-    const size_t smem = sizeof(double) * (3 * P1 * P1 * P1 + 3 * P1);
-    int rc = prepare_smem(m2m_kernel, smem);
+    const int nfull = (tgt_order + 1) * (tgt_order + 2) * (tgt_order + 3) / 6;
+    const size_t smem = sizeof(double) * (16 * nfull + 8 * 3 * P1) + sizeof(uint32_t) * nfull;
+    int rc = prepare_smem(m2m_children_kernel, smem);
     if (rc) return rc;
-    m2m_kernel<<<ntgt_boxes, E2E_THREADS, smem, as_stream(stream)>>>(
+    m2m_children_kernel<<<ntgt_boxes, M2M_THREADS, smem, as_stream(stream)>>>(
         src_order, tgt_order, src_rscale, tgt_rscale, target_boxes, box_child_ids, child_stride,
         centers, center_stride, src_base_ibox, src_expansions, tgt_base_ibox, tgt_expansions);
-    return check_launch("m2m_kernel");
+    return check_launch("m2m_children_kernel");
 }
 
 int sumpy_e2e_from_parent_f64(int src_order, int tgt_order, double src_rscale,
@@ -672,13 +729,16 @@ int sumpy_e2e_from_parent_f64(int src_order, int tgt_order, double src_rscale,
     if (!target_boxes || !box_parent_ids || !centers || !src_expansions || !tgt_expansions)
         return bad_arg("l2l: null pointer argument");
     const int P1 = src_order + 1;
-    const size_t smem = sizeof(double) * (2 * P1 * P1 * P1 + 3 * P1);
-    int rc = prepare_smem(l2l_kernel, smem);
+    const int nfull = (src_order + 1) * (src_order + 2) * (src_order + 3) / 6;
+    const size_t smem = sizeof(double) * (2 * L2L_BOXES * nfull + L2L_BOXES * 3 * P1) +
+                        sizeof(uint32_t) * nfull;
+    int rc = prepare_smem(l2l_boxes_kernel, smem);
     if (rc) return rc;
-    l2l_kernel<<<ntgt_boxes, E2E_THREADS, smem, as_stream(stream)>>>(
-        src_order, tgt_order, src_rscale, tgt_rscale, target_boxes, box_parent_ids, centers,
-        center_stride, src_base_ibox, src_expansions, tgt_base_ibox, tgt_expansions);
-    return check_launch("l2l_kernel");
+    const int blocks = (ntgt_boxes + L2L_BOXES - 1) / L2L_BOXES;
+    l2l_boxes_kernel<<<blocks, M2M_THREADS, smem, as_stream(stream)>>>(
+        src_order, tgt_order, src_rscale, tgt_rscale, ntgt_boxes, target_boxes, box_parent_ids,
+        centers, center_stride, src_base_ibox, src_expansions, tgt_base_ibox, tgt_expansions);
+    return check_launch("l2l_boxes_kernel");
 }
 
 static int launch_l2p(bool grad_on, int order, double rscale, int32_t ntgt_boxes,
