@@ -181,27 +181,30 @@ int sumpy_e2e_from_parent_f64(
     int32_t src_base_ibox, const double *src_expansions,
     int32_t tgt_base_ibox, double *tgt_expansions, void *stream);
 
-/* M2L for one level, applied per translation class as dense GEMMs.
- * Replaces M2LUsingTranslationClassesDependentData (sumpy/e2e.py:310-558)
- * with its pre/post-processing and FFTs (sumpy/fmm.py:798-920): in exact
- * arithmetic L[t] = (r_tgt/r_src)^|t| sum_s M[s] D_c[s+t]
- * (sumpy/expansion/m2l.py:363-389, 461-537, 679-698), here with
- * class_matrices[c][t][s] = that operator (row = target coefficient).
+/* M2L applied per translation class as dense FP64 GEMMs, any number of
+ * levels in one launch. Replaces M2LUsingTranslationClassesDependentData
+ * (sumpy/e2e.py:310-558) with its pre/post-processing and FFTs
+ * (sumpy/fmm.py:798-920): in exact arithmetic L[t] = (r_tgt/r_src)^|t|
+ * sum_s M[s] D_c[s+t] (sumpy/expansion/m2l.py:363-389, 461-537, 679-698),
+ * here with class_matrices[c][t][s] = that operator (row = target
+ * coefficient), nclasses of them.
  *
- * The List-2 CSR of the level (from_sep_siblings_starts/lists with the
- * per-entry translation class) is supplied regrouped into a schedule:
- * tiles of tile_width target boxes; for tile i, groups
- * tile_group_starts[i] .. tile_group_starts[i+1]-1, each one class
- * group_class[g] (0 <= c < nclasses) and one source box per target slot,
- * group_sources[g*tile_width + slot] (-1 = none). tile_targets[i*tile_width
- * + slot] is the target box of each slot (-1 = padding).
- * tgt[t] += matrix_scale * sum_groups T_c * src[s]. tile_width must be 64. */
+ * The List-2 CSR (from_sep_siblings_starts/lists with the per-entry
+ * translation class) is supplied regrouped into a schedule: tiles of
+ * tile_width (= 64) target slots, tile_targets[tile*64 + slot] (box
+ * numbers, -1 = empty), one scale per tile (tile_scale, the level's
+ * operator factor); class groups g with class group_class[g] and one source
+ * box per slot group_sources[g*64 + slot] (-1 = none); work items i = groups
+ * [item_group_begin[i], item_group_end[i]) of tile item_tile[i]. Source box
+ * b's expansion is row b - src_base_ibox of src_expansions, target box t's
+ * row t - tgt_base_ibox of tgt_expansions.
+ * tgt[t] += tile_scale * sum_groups T_c * src[s], with FP64 atomics. */
 int sumpy_m2l_translation_classes_f64(
-    int order, int32_t ntiles, int32_t tile_width, const int32_t *tile_targets,
-    const int32_t *tile_group_starts, const int32_t *group_class,
-    const int32_t *group_sources, int32_t nclasses, const double *class_matrices,
-    double matrix_scale, int32_t src_base_ibox, const double *src_expansions,
-    int32_t tgt_base_ibox, double *tgt_expansions, void *stream);
+    int order, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
+    const int32_t *item_group_end, int32_t tile_width, const int32_t *tile_targets,
+    const double *tile_scale, const int32_t *group_class, const int32_t *group_sources,
+    int32_t nclasses, const double *class_matrices, int32_t src_base_ibox,
+    const double *src_expansions, int32_t tgt_base_ibox, double *tgt_expansions, void *stream);
 
 /* M2L pre-processing for the tensor-core form: split FP64 values into two
  * TF32-representable FP32 planes, x ~ hi + lo (hi = tf32(x), lo =

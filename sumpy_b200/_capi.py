@@ -41,8 +41,8 @@ SIGNATURES = {
                                     i32, ptr, i32, ptr, ptr],
     "sumpy_e2e_from_parent_f64": [cint, cint, dbl, dbl, i32, ptr, ptr, ptr, i64, i32, ptr,
                                   i32, ptr, ptr],
-    "sumpy_m2l_translation_classes_f64": [cint, i32, i32, ptr, ptr, ptr, ptr, i32, ptr,
-                                          dbl, i32, ptr, i32, ptr, ptr],
+    "sumpy_m2l_translation_classes_f64": [cint, i32, ptr, ptr, ptr, i32, ptr, ptr, ptr, ptr,
+                                          i32, ptr, i32, ptr, i32, ptr, ptr],
     "sumpy_split_tf32x2": [i64, i32, i32, ptr, i32, i32, ptr, ptr, ptr],
     "sumpy_m2l_translation_classes_tf32x3": [cint, i32, ptr, ptr, ptr, i32, ptr, ptr, ptr, ptr,
                                              i32, ptr, ptr, i32, i32, i32, i32, ptr, ptr, i32,

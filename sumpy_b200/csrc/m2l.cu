@@ -6,42 +6,82 @@
 // arithmetic each class c is the linear map
 //     L[t] += (r_tgt/r_src)^|t| sum_s M[s] D_c[s+t]
 // so with T_c[t][s] (one n x n matrix per class, built on the host) the
-// level's M2L is sum_c T_c * M[:, sources of class c].
+// M2L of a level is sum_c T_c * M[:, sources of class c].
 //
-// Work unit: a tile of 64 target boxes. The host groups the tile's List-2
-// entries by class; each group is one GEMM step C += T_c * B_g with B_g the
-// gathered source multipoles (one per target slot, zero where absent).
-// The accumulator C (rows of the tile x 64 targets) stays in registers over
-// all of the tile's groups and is added to the local expansions once.
-// A CTA covers ROWS (64 or 128) output rows; more rows use gridDim.y.
-// Thread (ty, tx) owns rows ty + (ROWS/8) r and target slots tx + 8 c
-// (r, c < 8), so each shared-memory read of a k-step is conflict-free.
+// Schedule (same form as the tensor-core kernel): tiles of 64 target boxes
+// with one scale each (the level's operator factor), per tile the class
+// groups (one source box per target slot, -1 = none), and work items = up
+// to G consecutive groups of one tile; all levels in one launch. A CTA runs
+// one work item for ROWS (64 or 128) output rows: C += T_c * B_g over the
+// item's groups, the accumulator in registers, added to the local
+// expansions with FP64 atomics at the end (items of one tile may overlap in
+// time). Thread (ty, tx) owns rows ty + (ROWS/8) r and target slots
+// tx + 8 c (r, c < 8): each shared-memory read of a k-step is conflict-free.
+// The next k-chunk of both operands is fetched into registers while the
+// current one is multiplied.
 #include "common.cuh"
 
 namespace sumpy {
 namespace {
 
 constexpr int TW = 64;  // target boxes per tile
-constexpr int KC = 16;  // k-chunk
+constexpr int KC = 8;   // k-chunk
+
+template <int ROWS>
+struct Chunk {
+    static constexpr int NT = ROWS;
+    static constexpr int A_PER = ROWS * KC / NT;  // = KC
+    static constexpr int B_PER = TW * KC / NT;
+    double a[A_PER];
+    double b[B_PER];
+};
+
+template <int ROWS>
+__device__ __forceinline__ void fetch(Chunk<ROWS> &ch, const double *__restrict__ A,
+                                      const double *__restrict__ src, const int32_t *srcs, int n,
+                                      int row0, int k0, int32_t sbase)
+{
+    constexpr int NT = ROWS;
+#pragma unroll
+    for (int u = 0; u < Chunk<ROWS>::A_PER; ++u) {
+        const int idx = threadIdx.x + u * NT;
+        const int r = idx / KC, kk = idx % KC;
+        const int row = row0 + r, k = k0 + kk;
+        ch.a[u] = (row < n && k < n) ? A[(int64_t)row * n + k] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < Chunk<ROWS>::B_PER; ++u) {
+        const int idx = threadIdx.x + u * NT;
+        const int slot = idx / KC, kk = idx % KC;
+        const int32_t s = srcs[slot];
+        const int k = k0 + kk;
+        ch.b[u] = (s >= 0 && k < n) ? src[(int64_t)(s - sbase) * n + k] : 0.0;
+    }
+}
 
 template <int ROWS>
 __global__ void __launch_bounds__(ROWS)
-m2l_f64_kernel(int n, const int32_t *__restrict__ tile_targets,
-               const int32_t *__restrict__ tile_group_starts, const int32_t *__restrict__ group_class,
+m2l_f64_kernel(int n, const int32_t *__restrict__ item_tile, const int32_t *__restrict__ item_g0,
+               const int32_t *__restrict__ item_g1, const int32_t *__restrict__ tile_targets,
+               const double *__restrict__ tile_scale, const int32_t *__restrict__ group_class,
                const int32_t *__restrict__ group_sources, const double *__restrict__ mats,
-               double scale, int32_t sbase, const double *__restrict__ src, int32_t tbase,
+               int32_t sbase, const double *__restrict__ src, int32_t tbase,
                double *__restrict__ tgt)
 {
     constexpr int NT = ROWS;          // (ROWS / 8) x 8 threads
     constexpr int RG = ROWS / 8;      // row groups
-    __shared__ double As[KC][ROWS + 1];
-    __shared__ double Bs[KC][TW + 1];
-    __shared__ int32_t srcs[TW];
+    __shared__ double As[2][KC][ROWS + 1];
+    __shared__ double Bs[2][KC][TW + 1];
+    __shared__ int32_t srcs[2][TW];
 
-    const int tile = blockIdx.x;
+    const int item = blockIdx.x;
+    const int tile = item_tile[item];
+    const int g0 = item_g0[item], g1 = item_g1[item];
     const int row0 = blockIdx.y * ROWS;
     const int tid = threadIdx.x;
     const int tx = tid % 8, ty = tid / 8;
+    const int nkc = (n + KC - 1) / KC;
+    const int total = (g1 - g0) * nkc;
 
     double acc[8][8];
 #pragma unroll
@@ -49,41 +89,59 @@ m2l_f64_kernel(int n, const int32_t *__restrict__ tile_targets,
 #pragma unroll
         for (int c = 0; c < 8; ++c) acc[r][c] = 0.0;
 
-    const int g0 = tile_group_starts[tile], g1 = tile_group_starts[tile + 1];
-    for (int g = g0; g < g1; ++g) {
-        const int cls = group_class[g];
-        const double *A = mats + (int64_t)cls * n * n;
+    auto load_srcs = [&](int g, int buf) {
+        for (int s = tid; s < TW; s += NT) srcs[buf][s] = group_sources[(int64_t)g * TW + s];
+    };
+    auto store = [&](const Chunk<ROWS> &ch, int buf) {
+#pragma unroll
+        for (int u = 0; u < Chunk<ROWS>::A_PER; ++u) {
+            const int idx = tid + u * NT;
+            As[buf][idx % KC][idx / KC] = ch.a[u];
+        }
+#pragma unroll
+        for (int u = 0; u < Chunk<ROWS>::B_PER; ++u) {
+            const int idx = tid + u * NT;
+            Bs[buf][idx % KC][idx / KC] = ch.b[u];
+        }
+    };
+
+    if (total > 0) {
+        Chunk<ROWS> ch;
+        load_srcs(g0, 0);
         __syncthreads();
-        for (int s = tid; s < TW; s += NT) srcs[s] = group_sources[(int64_t)g * TW + s];
+        fetch<ROWS>(ch, mats + (int64_t)group_class[g0] * n * n, src, srcs[0], n, row0, 0, sbase);
+        store(ch, 0);
         __syncthreads();
-        for (int k0 = 0; k0 < n; k0 += KC) {
-            for (int idx = tid; idx < ROWS * KC; idx += NT) {
-                const int r = idx / KC, kk = idx % KC;
-                const int row = row0 + r, k = k0 + kk;
-                As[kk][r] = (row < n && k < n) ? A[(int64_t)row * n + k] : 0.0;
+        for (int it = 0; it < total; ++it) {
+            const int buf = it & 1;
+            const int nxt = it + 1;
+            if (nxt < total) {
+                const int g = g0 + nxt / nkc, kc = nxt % nkc;
+                const int sb = (g - g0) & 1;
+                if (kc == 0) {
+                    load_srcs(g, sb);
+                    __syncthreads();
+                }
+                fetch<ROWS>(ch, mats + (int64_t)group_class[g] * n * n, src, srcs[sb], n, row0,
+                            kc * KC, sbase);
             }
-            for (int idx = tid; idx < TW * KC; idx += NT) {
-                const int slot = idx / KC, kk = idx % KC;
-                const int32_t s = srcs[slot];
-                const int k = k0 + kk;
-                Bs[kk][slot] = (s >= 0 && k < n) ? src[(int64_t)(s - sbase) * n + k] : 0.0;
-            }
-            __syncthreads();
 #pragma unroll 4
             for (int kk = 0; kk < KC; ++kk) {
                 double a[8], b[8];
 #pragma unroll
-                for (int r = 0; r < 8; ++r) a[r] = As[kk][ty + RG * r];
+                for (int r = 0; r < 8; ++r) a[r] = As[buf][kk][ty + RG * r];
 #pragma unroll
-                for (int c = 0; c < 8; ++c) b[c] = Bs[kk][tx + 8 * c];
+                for (int c = 0; c < 8; ++c) b[c] = Bs[buf][kk][tx + 8 * c];
 #pragma unroll
                 for (int r = 0; r < 8; ++r)
 #pragma unroll
                     for (int c = 0; c < 8; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
             }
+            if (nxt < total) store(ch, buf ^ 1);
             __syncthreads();
         }
     }
+    const double scale = tile_scale[tile];
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
         const int32_t t = tile_targets[(int64_t)tile * TW + tx + 8 * c];
@@ -92,7 +150,7 @@ m2l_f64_kernel(int n, const int32_t *__restrict__ tile_targets,
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
             const int row = row0 + ty + RG * r;
-            if (row < n) o[row] += scale * acc[r][c];
+            if (row < n) atomicAdd(o + row, scale * acc[r][c]);
         }
     }
 }
@@ -104,39 +162,37 @@ using namespace sumpy;
 
 extern "C" {
 
-int sumpy_m2l_translation_classes_f64(int order, int32_t ntiles, int32_t tile_width,
-                                      const int32_t *tile_targets,
-                                      const int32_t *tile_group_starts,
-                                      const int32_t *group_class, const int32_t *group_sources,
-                                      int32_t nclasses, const double *class_matrices,
-                                      double matrix_scale, int32_t src_base_ibox,
-                                      const double *src_expansions, int32_t tgt_base_ibox,
-                                      double *tgt_expansions, void *stream)
+int sumpy_m2l_translation_classes_f64(
+    int order, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
+    const int32_t *item_group_end, int32_t tile_width, const int32_t *tile_targets,
+    const double *tile_scale, const int32_t *group_class, const int32_t *group_sources,
+    int32_t nclasses, const double *class_matrices, int32_t src_base_ibox,
+    const double *src_expansions, int32_t tgt_base_ibox, double *tgt_expansions, void *stream)
 {
     if (order < 0 || order > SUMPY_MAX_ORDER) {
         set_last_error("m2l: unsupported order");
         return SUMPY_EUNSUPPORTED;
     }
     if (tile_width != TW) return bad_arg("m2l: tile_width must be 64");
-    if (ntiles < 0 || nclasses < 0) return bad_arg("m2l: negative size");
-    if (ntiles == 0) return SUMPY_OK;
-    if (!tile_targets || !tile_group_starts || !group_class || !group_sources ||
-        !class_matrices || !src_expansions || !tgt_expansions)
+    if (nitems < 0 || nclasses < 0) return bad_arg("m2l: negative size");
+    if (nitems == 0) return SUMPY_OK;
+    if (!item_tile || !item_group_begin || !item_group_end || !tile_targets || !tile_scale ||
+        !group_class || !group_sources || !class_matrices || !src_expansions || !tgt_expansions)
         return bad_arg("m2l: null pointer argument");
     const int n = ncoeff_of(order);
     cudaStream_t st = as_stream(stream);
     if (n <= 64) {
-        dim3 grid(ntiles, 1);
-        m2l_f64_kernel<64><<<grid, 64, 0, st>>>(n, tile_targets, tile_group_starts, group_class,
-                                                group_sources, class_matrices, matrix_scale,
-                                                src_base_ibox, src_expansions, tgt_base_ibox,
-                                                tgt_expansions);
+        dim3 grid(nitems, 1);
+        m2l_f64_kernel<64><<<grid, 64, 0, st>>>(n, item_tile, item_group_begin, item_group_end,
+                                                tile_targets, tile_scale, group_class,
+                                                group_sources, class_matrices, src_base_ibox,
+                                                src_expansions, tgt_base_ibox, tgt_expansions);
     } else {
-        dim3 grid(ntiles, (n + 127) / 128);
-        m2l_f64_kernel<128><<<grid, 128, 0, st>>>(n, tile_targets, tile_group_starts,
-                                                  group_class, group_sources, class_matrices,
-                                                  matrix_scale, src_base_ibox, src_expansions,
-                                                  tgt_base_ibox, tgt_expansions);
+        dim3 grid(nitems, (n + 127) / 128);
+        m2l_f64_kernel<128><<<grid, 128, 0, st>>>(n, item_tile, item_group_begin, item_group_end,
+                                                  tile_targets, tile_scale, group_class,
+                                                  group_sources, class_matrices, src_base_ibox,
+                                                  src_expansions, tgt_base_ibox, tgt_expansions);
     }
     return check_launch("m2l_f64_kernel");
 }

@@ -424,33 +424,40 @@ class SumpyExpansionWrangler:
         levels = [lev for lev in range(self.tree.nlevels)
                   if ltb[lev] != ltb[lev + 1] and starts[ltb[lev]] != starts[ltb[lev + 1]]]
         tc = self.precision == "mixed"
-        if tc and len({self.level_orders[lev] for lev in levels}) == 1 \
+        tile = M2L_TILE_TC if tc else M2L_TILE
+        if len({self.level_orders[lev] for lev in levels}) == 1 \
                 and len(set(self.level_orders)) == 1:
-            # every level in one launch (uniform expansion size)
-            plan = self._m2l_tc_plan(tuple(levels), ltb, tboxes, starts, src_box_lists)
+            # every level in one launch (uniform expansion size: the flat
+            # level-major arrays are [nboxes][ncoeff])
+            plan = self._m2l_merged_plan(tuple(levels), ltb, tboxes, starts, src_box_lists, tile)
             if plan is not None:
-                self._launch_m2l_tc_merged(plan, mpole_exps, local_exps, st)
+                if tc:
+                    self._launch_m2l_tc_merged(plan, mpole_exps, local_exps, st)
+                else:
+                    self._call_m2l_f64(self.level_orders[0], plan, plan["mats"], 0, mpole_exps,
+                                       0, local_exps, st)
             return local_exps
         for lev in levels:
             a, b = int(ltb[lev]), int(ltb[lev + 1])
-            plan = self._m2l_plan(lev, tboxes[a:b], starts[a:b + 1], src_box_lists,
-                                  M2L_TILE_TC if tc else M2L_TILE)
+            plan = self._m2l_plan(lev, tboxes[a:b], starts[a:b + 1], src_box_lists, tile)
             if plan is None:
                 continue
             mats, mscale = self._m2l_matrices(lev)
             sbase, sview = self.multipole_expansions_view(mpole_exps, lev)
             tbase, tview = self.local_expansions_view(local_exps, lev)
+            items = self._level_items(lev, plan, mscale)
             if tc:
-                self._launch_m2l_tc_level(lev, plan, mats, mscale, sbase, sview, tbase, tview, st)
+                self._launch_m2l_tc_level(lev, items, mats, sbase, sview, tbase, tview, st)
             else:
-                self._launch_m2l(lev, plan, mats, mscale, sbase, sview, tbase, tview, st)
+                self._call_m2l_f64(self.level_orders[lev], items, mats, sbase, sview, tbase,
+                                   tview, st)
         return local_exps
 
     @staticmethod
     def _tc_items(tiles):
         """Split tiles (group ranges) into work items of at most
         M2L_ITEM_GROUPS groups, largest first (CTAs start roughly in launch
-        order)."""
+        order). The same schedule serves the FP64 and the tensor-core GEMMs."""
         it_tile, it_g0, it_g1 = [], [], []
         for tile, (g0, g1) in enumerate(tiles):
             for a in range(g0, g1, M2L_ITEM_GROUPS):
@@ -463,11 +470,11 @@ class SumpyExpansionWrangler:
         order = np.argsort(-(it_g1 - it_g0), kind="stable")
         return it_tile[order], it_g0[order], it_g1[order]
 
-    def _m2l_tc_plan(self, levels, ltb, tboxes, starts, lists):
-        """One tensor-core schedule over all M2L levels: the per-level (tile,
-        class) groups concatenated, class ids offset into a stacked operator
-        set, one scale per tile."""
-        key = ("tc-merged", levels, id(lists))
+    def _m2l_merged_plan(self, levels, ltb, tboxes, starts, lists, tile):
+        """One GEMM schedule over all M2L levels: the per-level (tile, class)
+        groups concatenated, class ids offset into a stacked operator set,
+        one scale per tile, work items over the groups."""
+        key = ("merged", levels, id(lists), tile)
         if key in self._m2l_plans:
             return self._m2l_plans[key]
         tt, tsc, gcl, gsrc, tiles = [], [], [], [], []
@@ -475,7 +482,7 @@ class SumpyExpansionWrangler:
         ntiles = ngroups = 0
         for lev in levels:
             a, b = int(ltb[lev]), int(ltb[lev + 1])
-            p = self._m2l_plan(lev, tboxes[a:b], starts[a:b + 1], lists, M2L_TILE_TC)
+            p = self._m2l_plan(lev, tboxes[a:b], starts[a:b + 1], lists, tile)
             if p is None:
                 continue
             mats, mscale = self._m2l_matrices(lev)
@@ -512,12 +519,27 @@ class SumpyExpansionWrangler:
         self._m2l_plans[key] = plan
         return plan
 
-    def _launch_m2l(self, lev, plan, mats, mscale, sbase, sview, tbase, tview, st):
-        call("sumpy_m2l_translation_classes_f64", _c(self.level_orders[lev]),
-             _i32(plan["ntiles"]), _i32(M2L_TILE), dptr(plan["tile_targets"]),
-             dptr(plan["tile_group_starts"]), dptr(plan["group_class"]),
-             dptr(plan["group_sources"]), _i32(plan["nclasses"]), dptr(mats), _d(mscale),
-             _i32(sbase), dptr(sview), _i32(tbase), dptr(tview), st)
+    def _level_items(self, lev, plan, mscale):
+        """Work items of one level's plan (levels of different expansion sizes
+        run one launch each)."""
+        key = ("items", lev, id(plan))
+        if key not in self._m2l_plans:
+            tgs = plan["tile_group_starts"].cpu().numpy()
+            tiles = [(int(tgs[i]), int(tgs[i + 1])) for i in range(plan["ntiles"])]
+            it_tile, it_g0, it_g1 = self._tc_items(tiles)
+            dev = self.device
+            self._m2l_plans[key] = dict(
+                plan, nitems=len(it_tile), item_tile=torch.as_tensor(it_tile).to(dev),
+                item_g0=torch.as_tensor(it_g0).to(dev), item_g1=torch.as_tensor(it_g1).to(dev),
+                tile_scale=torch.full((plan["ntiles"],), mscale, dtype=torch.float64, device=dev))
+        return self._m2l_plans[key]
+
+    def _call_m2l_f64(self, order, plan, mats, sbase, src, tbase, tgt, st):
+        call("sumpy_m2l_translation_classes_f64", _c(order), _i32(plan["nitems"]),
+             dptr(plan["item_tile"]), dptr(plan["item_g0"]), dptr(plan["item_g1"]),
+             _i32(M2L_TILE), dptr(plan["tile_targets"]), dptr(plan["tile_scale"]),
+             dptr(plan["group_class"]), dptr(plan["group_sources"]), _i32(mats.shape[0]),
+             dptr(mats), _i32(sbase), dptr(src), _i32(tbase), dptr(tgt), st)
 
     @staticmethod
     def _tc_pads(n):
@@ -572,23 +594,13 @@ class SumpyExpansionWrangler:
              dptr(hi), dptr(lo), _i32(rp), _i32(kp), _i32(src_nrows), _i32(sbase),
              dptr(ws_hi), dptr(ws_lo), _i32(tbase), dptr(tgt), dptr(self._status), st)
 
-    def _launch_m2l_tc_level(self, lev, plan, mats, mscale, sbase, sview, tbase, tview, st):
+    def _launch_m2l_tc_level(self, lev, items, mats, sbase, sview, tbase, tview, st):
         hi, lo, rp, kp = self._m2l_tc_operands(mats)
         nb, n = sview.shape
         ws_hi, ws_lo = self._m2l_workspace(nb, kp)
         call("sumpy_split_tf32x2", _i64(nb), _i32(1), _i32(n), dptr(sview), _i32(1),
              _i32(kp), dptr(ws_hi), dptr(ws_lo), st)
-        key = ("items", lev, id(plan))
-        if key not in self._m2l_plans:
-            tgs = plan["tile_group_starts"].cpu().numpy()
-            tiles = [(int(tgs[i]), int(tgs[i + 1])) for i in range(plan["ntiles"])]
-            it_tile, it_g0, it_g1 = self._tc_items(tiles)
-            dev = self.device
-            self._m2l_plans[key] = dict(
-                plan, nitems=len(it_tile), item_tile=torch.as_tensor(it_tile).to(dev),
-                item_g0=torch.as_tensor(it_g0).to(dev), item_g1=torch.as_tensor(it_g1).to(dev),
-                tile_scale=torch.full((plan["ntiles"],), mscale, dtype=torch.float64, device=dev))
-        self._call_m2l_tc(self.level_orders[lev], self._m2l_plans[key], hi, lo, rp, kp, nb + 1,
+        self._call_m2l_tc(self.level_orders[lev], items, hi, lo, rp, kp, nb + 1,
                           sbase, ws_hi, ws_lo, tbase, tview, st)
 
     def check_status(self):
