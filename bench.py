@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip timing the FP64 form")
     ap.add_argument("--stage-times", action="store_true", help="print per-stage times")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 512-problem batch")
     return ap.parse_args()
 
 
@@ -291,6 +292,7 @@ def main():
 
     stage_ms, roof = stage_breakdown(w_mx, trav, q_dev, dev)
     adj = adjoint_bench(dev) if world == 1 else None
+    batch = batched_bench(dev) if world == 1 and not args.no_batch else None
 
     value = world * args.npoints / (ms_mx * 1e-3) / 1e6
     line = {
@@ -314,6 +316,7 @@ def main():
         "mixed_over_fp64": (ms_64 / ms_mx) if ms_64 else None,
         "adjoint_forward_ratio": adj["ratio"] if adj else None,
         "adjoint": adj,
+        "batched": batch,
         "stage_ms": stage_ms,
         "roofline": roof,
         "cpu_baseline": cpu_line,
@@ -391,6 +394,125 @@ def adjoint_bench(dev, steps=3, ns=200_000, nt=50_000, order=8):
             "grad_strength_relL2_vs_direct": rel(gq, gq_ref),
             "grad_source_pos_relL2_vs_direct": rel(gsrc, gsrc_ref),
             "workload": f"sphere(perturbed) {ns} sources -> shell {nt} targets, p={order}, mixed"}
+
+
+def batch_problems(nproblems=512):
+    """The batched workload: problem i draws from seed 1000 + i its size
+    N_i = floor(exp(U(ln 1000, ln 65536))), N_i points U[0,1]^3 (sources =
+    targets) and N_i strengths N(0, 1)."""
+    srcs, qs = [], []
+    for i in range(nproblems):
+        rng = np.random.default_rng(1000 + i)
+        n = int(np.floor(np.exp(rng.uniform(np.log(1000), np.log(65536)))))
+        srcs.append(rng.random((3, n)))
+        qs.append(rng.standard_normal(n))
+    return srcs, qs
+
+
+def batched_bench(dev, steps=5, warmup=3, nproblems=512, order=8, nseq=16):
+    """512 independent problems (p = 8, mixed, max 32 per box, exclude_self)
+    as one forest: CUDA-graph replay and eager launches of the whole batch,
+    against the same problems evaluated one drive_fmm at a time (the first
+    ``nseq`` problems, rate extrapolated by points). Accuracy: relative L2
+    error on 4 problems (512 sampled targets each) against the FP64 direct
+    sum. L2 flushed between timed batches."""
+    import torch
+    from sumpy_b200 import (P2P, LaplaceKernel, SumpyExpansionWrangler,
+                            SumpyTreeIndependentDataForWrangler, drive_fmm)
+    from sumpy_b200 import _capi
+    from sumpy_b200.batch import BatchedLaplaceFMM
+    from sumpy_b200.expansion import (
+        LinearPDEConformingVolumeTaylorLocalExpansion as LExp,
+        LinearPDEConformingVolumeTaylorMultipoleExpansion as MExp)
+    from sumpy_b200.tree import build_all
+    box = [[0.0, 1.0]] * 3
+    srcs, qs = batch_problems(nproblems)
+    ntot = sum(q.size for q in qs)
+    t0 = time.perf_counter()
+    b = BatchedLaplaceFMM(srcs, order=order, max_particles_in_box=MAX_PARTICLES,
+                          precision="mixed", bbox=box, device=dev, use_graph=True,
+                          autotune=True)
+    t_build = time.perf_counter() - t0
+    w_dev = torch.as_tensor(np.concatenate(qs), device=dev)
+    t0 = time.perf_counter()
+    b.capture()
+    t_capture = time.perf_counter() - t0
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(steps)]
+        torch.cuda.synchronize()
+        for i in range(steps):
+            flush.fill_(float(i))
+            evs[i][0].record()
+            fn()
+            evs[i][1].record()
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(c) for a, c in evs) / steps
+
+    ms_graph = timed(lambda: b.evaluate(w_dev))
+    b.use_graph = False
+    _capi.launch_counter.reset()
+    b.evaluate(w_dev)
+    launches = _capi.launch_counter.value
+    ms_eager = timed(lambda: b.evaluate(w_dev))
+    b.use_graph = True
+    b.check_status()
+
+    # one problem at a time (what a loop over sumpy FMMs does), first nseq problems
+    knl = LaplaceKernel(3)
+    ti = SumpyTreeIndependentDataForWrangler(
+        None, lambda o, **kw: MExp(knl, o), lambda o, **kw: LExp(knl, o), [knl],
+        exclude_self=True)
+    seq = []
+    for i in range(nseq):
+        _, trav, tcls = build_all(srcs[i], None, MAX_PARTICLES, bbox=box)
+        wr = SumpyExpansionWrangler(ti, trav, np.float64, lambda *a: order,
+                                    translation_classes_data=tcls, precision="mixed",
+                                    device=dev)
+        seq.append((wr, torch.as_tensor(qs[i], device=dev)))
+    nseq_pts = sum(q.numel() for _, q in seq)
+
+    def run_seq():
+        for wr, q in seq:
+            drive_fmm(None, wr, [q])
+
+    ms_seq = timed(run_seq)
+    seq_rate = nseq_pts / (ms_seq * 1e-3) / 1e6
+
+    # accuracy on 4 problems
+    pots = b(w_dev)
+    errs = []
+    rng = np.random.default_rng(5)
+    for i in (0, 1, nproblems // 2, nproblems - 1):
+        n = qs[i].size
+        smp = rng.choice(n, size=min(512, n), replace=False)
+        (ref,) = P2P([knl], exclude_self=True)(None, srcs[i][:, smp], srcs[i], (qs[i],),
+                                               target_to_source=smp, device=dev)
+        ref = ref.cpu().numpy()
+        got = pots[i].cpu().numpy()[smp]
+        errs.append(float(np.linalg.norm(got - ref) / np.linalg.norm(ref)))
+    return {
+        "workload": f"{nproblems} problems U[0,1]^3, N_i=floor(exp(U(ln 1000, ln 65536))) "
+                    f"(seed 1000+i), p={order}, mixed, exclude_self",
+        "total_points": int(ntot), "nboxes": int(b.tree.nboxes),
+        "graph": {"ms_per_batch": ms_graph, "Mpts_s": ntot / (ms_graph * 1e-3) / 1e6,
+                  "problems_s": nproblems / (ms_graph * 1e-3)},
+        "eager": {"ms_per_batch": ms_eager, "Mpts_s": ntot / (ms_eager * 1e-3) / 1e6,
+                  "launches_per_batch": launches},
+        "one_problem_at_a_time": {
+            "Mpts_s": seq_rate, "problems_timed": nseq, "points_timed": int(nseq_pts),
+            "ms_for_timed": ms_seq,
+            "note": "drive_fmm per problem, warm, same kernels; whole-batch time "
+                    "extrapolated by points"},
+        "batch_over_one_at_a_time": (ntot / (ms_graph * 1e-3) / 1e6) / seq_rate,
+        "m2l_item_groups": b.wrangler.m2l_item_groups,
+        "relL2_vs_direct": errs,
+        "forest_build_s": round(t_build, 2), "capture_s": round(t_capture, 2),
+    }
 
 
 def stage_breakdown(w, trav, q_dev, dev):

@@ -39,6 +39,19 @@ int sumpy_tree_build(int64_t nsources, const double *sx, const double *sy, const
                      int64_t ntargets, const double *tx, const double *ty, const double *tz,
                      int max_particles_in_box, int max_levels, void **handle_out);
 
+/* sumpy_tree_build with a caller-fixed root box [bbox_min, bbox_min + root_extent]^3
+ * instead of the particles' bounding cube. Trees built in one box share their
+ * box sizes, rscales and translation-class vectors level by level, which is
+ * what lets sumpy_b200.forest merge many problems into one level-major box
+ * numbering. boxtree's TreeBuilder takes the same option as its
+ * bbox argument. Particles outside the box are an error (SUMPY_TREE_EINVAL);
+ * a coordinate equal to the upper bound goes to the last cell. */
+int sumpy_tree_build_in_box(int64_t nsources, const double *sx, const double *sy,
+                            const double *sz, int64_t ntargets, const double *tx,
+                            const double *ty, const double *tz, int max_particles_in_box,
+                            int max_levels, const double *bbox_min, double root_extent,
+                            void **handle_out);
+
 /* Look up a named array: kind 0 = int32, 1 = float64; length in elements. */
 int sumpy_tree_array_info(void *handle, const char *name, int *kind, int64_t *length);
 

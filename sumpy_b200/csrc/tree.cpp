@@ -265,6 +265,16 @@ int sumpy_tree_build(int64_t nsources, const double *sx, const double *sy, const
                      int64_t ntargets, const double *tx, const double *ty, const double *tz,
                      int max_particles_in_box, int max_levels, void **handle_out)
 {
+    return sumpy_tree_build_in_box(nsources, sx, sy, sz, ntargets, tx, ty, tz,
+                                   max_particles_in_box, max_levels, nullptr, 0.0, handle_out);
+}
+
+int sumpy_tree_build_in_box(int64_t nsources, const double *sx, const double *sy,
+                            const double *sz, int64_t ntargets, const double *tx,
+                            const double *ty, const double *tz, int max_particles_in_box,
+                            int max_levels, const double *bbox_min, double root_extent,
+                            void **handle_out)
+{
     try {
         if (!handle_out) { g_last_error = "handle_out is NULL"; return SUMPY_TREE_EINVAL; }
         *handle_out = nullptr;
@@ -295,13 +305,27 @@ int sumpy_tree_build(int64_t nsources, const double *sx, const double *sy, const
         upd(sx, sy, sz, nsources);
         if (!sat) upd(tx, ty, tz, ntargets);
         if (nsources + (sat ? 0 : ntargets) == 0) { for (int d = 0; d < 3; ++d) { lo[d] = 0; hi[d] = 0; } }
-        double ext = 0;
-        for (int d = 0; d < 3; ++d) ext = std::max(ext, hi[d] - lo[d]);
-        if (ext == 0) ext = 1.0;
-        // enlarge slightly so that the maximal coordinates fall inside the root box
-        B.root_extent = ext * (1.0 + 1e-9);
-        for (int d = 0; d < 3; ++d)
-            B.bbox_min[d] = lo[d] - 0.5 * (B.root_extent - (hi[d] - lo[d]));
+        if (bbox_min) {
+            // caller-fixed root box (trees of a batch share their level geometry)
+            if (!(root_extent > 0) || !std::isfinite(root_extent))
+                throw std::string("root_extent must be positive and finite");
+            for (int d = 0; d < 3; ++d) {
+                if (!std::isfinite(bbox_min[d])) throw std::string("non-finite bbox_min");
+                if (nsources + (sat ? 0 : ntargets) > 0 &&
+                    (lo[d] < bbox_min[d] || hi[d] > bbox_min[d] + root_extent))
+                    throw std::string("a particle lies outside the given root box");
+                B.bbox_min[d] = bbox_min[d];
+            }
+            B.root_extent = root_extent;
+        } else {
+            double ext = 0;
+            for (int d = 0; d < 3; ++d) ext = std::max(ext, hi[d] - lo[d]);
+            if (ext == 0) ext = 1.0;
+            // enlarge slightly so that the maximal coordinates fall inside the root box
+            B.root_extent = ext * (1.0 + 1e-9);
+            for (int d = 0; d < 3; ++d)
+                B.bbox_min[d] = lo[d] - 0.5 * (B.root_extent - (hi[d] - lo[d]));
+        }
 
         compute_keys(sx, sy, sz, nsources, B.bbox_min, B.root_extent, B.skey);
         sort_by_key(B.skey, B.sperm);

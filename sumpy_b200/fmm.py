@@ -15,7 +15,9 @@ per expansion kind, level-major, each level a row-major
 Beyond sumpy's knobs, the wrangler takes ``precision``: ``"fp64"`` (every
 stage in FP64) or ``"mixed"`` (FP32 near field with FP64 offsets and sums;
 M2L as split-FP32 (3xTF32) GEMMs on the tcgen05 tensor cores with FP32
-accumulation and FP64 results; the other stages FP64).
+accumulation and FP64 results; the other stages FP64), ``gradient`` (also
+return the potential's gradient at the targets) and ``m2l_item_groups`` (class
+groups per M2L work item, one CTA each; :mod:`sumpy_b200.autotune` picks it).
 """
 from __future__ import annotations
 
@@ -95,7 +97,7 @@ class SumpyExpansionWrangler:
                  source_extra_kwargs=None, kernel_extra_kwargs=None,
                  self_extra_kwargs=None, translation_classes_data=None,
                  preprocessed_mpole_dtype=None, *, _disable_translation_classes=False,
-                 precision="fp64", device=None, gradient=False):
+                 precision="fp64", device=None, gradient=False, m2l_item_groups=None):
         if not callable(fmm_level_to_order):
             raise TypeError("fmm_level_to_order not passed")
         if np.dtype(dtype) != np.float64:
@@ -136,6 +138,9 @@ class SumpyExpansionWrangler:
         self._m2l_tc_mats = {}
         self._m2l_ws = None
         self._status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self.m2l_item_groups = int(m2l_item_groups or M2L_ITEM_GROUPS)
+        if self.m2l_item_groups < 1:
+            raise ValueError("m2l_item_groups must be >= 1")
 
     # {{{ geometry, storage
 
@@ -453,17 +458,16 @@ class SumpyExpansionWrangler:
                                    tview, st)
         return local_exps
 
-    @staticmethod
-    def _tc_items(tiles):
+    def _tc_items(self, tiles):
         """Split tiles (group ranges) into work items of at most
-        M2L_ITEM_GROUPS groups, largest first (CTAs start roughly in launch
+        ``m2l_item_groups`` groups, largest first (CTAs start roughly in launch
         order). The same schedule serves the FP64 and the tensor-core GEMMs."""
         it_tile, it_g0, it_g1 = [], [], []
         for tile, (g0, g1) in enumerate(tiles):
-            for a in range(g0, g1, M2L_ITEM_GROUPS):
+            for a in range(g0, g1, self.m2l_item_groups):
                 it_tile.append(tile)
                 it_g0.append(a)
-                it_g1.append(min(g1, a + M2L_ITEM_GROUPS))
+                it_g1.append(min(g1, a + self.m2l_item_groups))
         it_tile = np.array(it_tile, dtype=np.int32)
         it_g0 = np.array(it_g0, dtype=np.int32)
         it_g1 = np.array(it_g1, dtype=np.int32)
@@ -474,7 +478,7 @@ class SumpyExpansionWrangler:
         """One GEMM schedule over all M2L levels: the per-level (tile, class)
         groups concatenated, class ids offset into a stacked operator set,
         one scale per tile, work items over the groups."""
-        key = ("merged", levels, id(lists), tile)
+        key = ("merged", levels, id(lists), tile, self.m2l_item_groups)
         if key in self._m2l_plans:
             return self._m2l_plans[key]
         tt, tsc, gcl, gsrc, tiles = [], [], [], [], []
@@ -522,7 +526,7 @@ class SumpyExpansionWrangler:
     def _level_items(self, lev, plan, mscale):
         """Work items of one level's plan (levels of different expansion sizes
         run one launch each)."""
-        key = ("items", lev, id(plan))
+        key = ("items", lev, id(plan), self.m2l_item_groups)
         if key not in self._m2l_plans:
             tgs = plan["tile_group_starts"].cpu().numpy()
             tiles = [(int(tgs[i]), int(tgs[i + 1])) for i in range(plan["ntiles"])]

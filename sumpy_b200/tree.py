@@ -156,9 +156,13 @@ class TranslationClassesInfo:
     from_sep_siblings_translation_classes_level_starts: np.ndarray
 
 
-def build_all(sources, targets=None, max_particles_in_box=30, max_levels=None):
+def build_all(sources, targets=None, max_particles_in_box=30, max_levels=None, bbox=None):
     """Build :class:`Tree`, :class:`FMMTraversalInfo` and
-    :class:`TranslationClassesInfo` in one call of the host library."""
+    :class:`TranslationClassesInfo` in one call of the host library.
+
+    ``bbox``, as boxtree's ``TreeBuilder(..., bbox=...)``: a ``(3, 2)`` array
+    of per-axis ``[min, max]``; the root box is the cube at ``min`` with the
+    largest side. Without it the root box is the particles' bounding cube."""
     src = _soa(sources, "sources")
     tgt = None if targets is None else _soa(targets, "targets")
     lib = _tree_lib()
@@ -175,13 +179,20 @@ def build_all(sources, targets=None, max_particles_in_box=30, max_levels=None):
     else:
         tx, ty, tz = (np.ascontiguousarray(tgt[i]) for i in range(3))
         ntgt = tgt.shape[1]
-    rc = lib.sumpy_tree_build(
+    if bbox is None:
+        bmin, ext = None, 0.0
+    else:
+        bb = np.asarray(bbox, dtype=np.float64).reshape(3, 2)
+        bmin = np.ascontiguousarray(bb[:, 0])
+        ext = float(np.max(bb[:, 1] - bb[:, 0]))
+    rc = lib.sumpy_tree_build_in_box(
         ctypes.c_int64(src.shape[1]), p(sx), p(sy), p(sz),
         ctypes.c_int64(ntgt),
         None if tx is None else p(tx), None if ty is None else p(ty),
         None if tz is None else p(tz),
         ctypes.c_int(int(max_particles_in_box)),
         ctypes.c_int(0 if max_levels is None else int(max_levels)),
+        None if bmin is None else p(bmin), ctypes.c_double(ext),
         ctypes.byref(h))
     if rc != 0:
         raise ValueError(lib.sumpy_tree_last_error().decode())
@@ -269,12 +280,12 @@ class TreeBuilder:
         self.actx = actx
 
     def __call__(self, actx, particles, targets=None, max_particles_in_box=None,
-                 max_levels=None, debug=False, kind="adaptive", **kwargs):
+                 max_levels=None, debug=False, kind="adaptive", bbox=None, **kwargs):
         if max_particles_in_box is None:
             raise TypeError("max_particles_in_box must be given")
         if kind not in ("adaptive", "adaptive-level-restricted") and kind is not None:
             raise NotImplementedError(f"tree kind '{kind}'")
-        tree, _, _ = build_all(particles, targets, max_particles_in_box, max_levels)
+        tree, _, _ = build_all(particles, targets, max_particles_in_box, max_levels, bbox=bbox)
         return tree, None
 
 
