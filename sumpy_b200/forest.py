@@ -47,52 +47,49 @@ class Forest:
 
 
 def _cat(parts, dtype=np.int32):
-    return np.concatenate(parts).astype(dtype) if parts else np.zeros(0, dtype=dtype)
+    if not parts:
+        return np.zeros(0, dtype=dtype)
+    return np.concatenate(parts, dtype=dtype, casting="unsafe")
 
 
 def _level_sorted(lists, level_starts, maps, nl):
     """Merge per-problem level-sorted box lists: level by level, problem
-    after problem. Returns the merged list, its level starts and, per
-    problem, the merged position of each of its entries."""
-    out, ls, pos = [], np.zeros(nl + 1, dtype=np.int32), []
-    for i in range(len(lists)):
-        pos.append(np.empty(len(lists[i]), dtype=np.int64))
+    after problem. Returns the merged list, its level starts and the row
+    blocks ``(problem, begin, end)`` (per-problem row ranges) in merged
+    order."""
+    out, ls, blocks = [], np.zeros(nl + 1, dtype=np.int32), []
     n = 0
     for lev in range(nl):
         for i, (lst, st) in enumerate(zip(lists, level_starts)):
             if lev + 1 >= len(st):
                 continue
             a, b = int(st[lev]), int(st[lev + 1])
+            if a == b:
+                continue
             out.append(maps[i][lst[a:b]])
-            pos[i][a:b] = np.arange(n, n + b - a)
+            blocks.append((i, a, b))
             n += b - a
         ls[lev + 1] = n
-    return _cat(out), ls, pos
+    return _cat(out), ls, blocks
 
 
-def _merge_csr(row_pos, nrows, starts, lists, maps, values=None):
-    """Merge per-problem CSR lists whose rows moved to ``row_pos`` (merged
-    row index of each per-problem row); entries are box ids mapped by
+def _merge_csr(blocks, starts, lists, maps, values=None):
+    """Merge per-problem CSR lists row block by row block (``blocks`` as
+    returned by :func:`_level_sorted`); entries are box ids mapped by
     ``maps``; ``values`` ride along unchanged."""
-    counts = np.zeros(nrows, dtype=np.int64)
-    for i, st in enumerate(starts):
-        counts[row_pos[i]] = np.diff(np.asarray(st, dtype=np.int64))
-    new_starts = np.zeros(nrows + 1, dtype=np.int64)
-    np.cumsum(counts, out=new_starts[1:])
-    out = np.empty(int(new_starts[-1]), dtype=np.int32)
-    vout = None if values is None else np.empty(int(new_starts[-1]), dtype=np.int32)
-    for i, st in enumerate(starts):
-        st = np.asarray(st, dtype=np.int64)
-        if len(st) <= 1:
-            continue
-        cnt = np.diff(st)
-        dst0 = np.repeat(new_starts[row_pos[i]], cnt)
-        within = np.arange(int(st[-1] - st[0])) - np.repeat(st[:-1] - st[0], cnt)
-        ent = np.asarray(lists[i])[int(st[0]):int(st[-1])]
-        out[dst0 + within] = maps[i][ent]
+    counts, out, vout = [], [], []
+    for i, a, b in blocks:
+        st = np.asarray(starts[i], dtype=np.int64)
+        counts.append(np.diff(st[a:b + 1]))
+        e0, e1 = int(st[a]), int(st[b])
+        out.append(maps[i][np.asarray(lists[i])[e0:e1]])
         if values is not None:
-            vout[dst0 + within] = np.asarray(values[i])[int(st[0]):int(st[-1])]
-    return new_starts.astype(np.int32), out, vout
+            vout.append(np.asarray(values[i])[e0:e1])
+    counts = _cat(counts, np.int64)
+    new_starts = np.zeros(len(counts) + 1, dtype=np.int64)
+    np.cumsum(counts, out=new_starts[1:])
+    return (new_starts.astype(np.int32), _cat(out),
+            None if values is None else _cat(vout))
 
 
 def merge_trees(parts):
@@ -128,7 +125,7 @@ def merge_trees(parts):
     for i, t in enumerate(trees):
         lev = np.asarray(t.box_levels, dtype=np.int64)
         ls = np.asarray(t.level_start_box_nrs, dtype=np.int64)
-        maps.append((off[i, lev] + np.arange(t.nboxes) - ls[lev]).astype(np.int64))
+        maps.append((off[i, lev] + np.arange(t.nboxes) - ls[lev]).astype(np.int32))
     NB = int(LS[-1])
 
     # }}}
@@ -199,35 +196,36 @@ def merge_trees(parts):
                              [np.asarray(getattr(tr, lsname)) for tr in travs], maps, nl)
 
     sb, sb_ls, _ = boxes("source_boxes", "level_start_source_box_nrs")
-    tb, tb_ls, tb_pos = boxes("target_boxes", "level_start_target_box_nrs")
+    tb, tb_ls, tb_blk = boxes("target_boxes", "level_start_target_box_nrs")
     spb, spb_ls, _ = boxes("source_parent_boxes", "level_start_source_parent_box_nrs")
-    ttp, ttp_ls, ttp_pos = boxes("target_or_target_parent_boxes",
+    ttp, ttp_ls, ttp_blk = boxes("target_or_target_parent_boxes",
                                  "level_start_target_or_target_parent_box_nrs")
 
-    l1s, l1l, _ = _merge_csr(tb_pos, len(tb), [tr.neighbor_source_boxes_starts for tr in travs],
+    l1s, l1l, _ = _merge_csr(tb_blk, [tr.neighbor_source_boxes_starts for tr in travs],
                              [tr.neighbor_source_boxes_lists for tr in travs], maps)
-    l2s, l2l, l2c = _merge_csr(ttp_pos, len(ttp), [tr.from_sep_siblings_starts for tr in travs],
+    l2s, l2l, l2c = _merge_csr(ttp_blk, [tr.from_sep_siblings_starts for tr in travs],
                                [tr.from_sep_siblings_lists for tr in travs], maps,
                                values=[tc.from_sep_siblings_translation_classes
                                        for tc in tclss])
-    l4s, l4l, _ = _merge_csr(ttp_pos, len(ttp), [tr.from_sep_bigger_starts for tr in travs],
+    l4s, l4l, _ = _merge_csr(ttp_blk, [tr.from_sep_bigger_starts for tr in travs],
                              [tr.from_sep_bigger_lists for tr in travs], maps)
 
     by_level_tb, by_level = [], []
     for lev in range(nl):
-        rows, parts3, n = [], [], 0
+        rows, blk = [], []
         for i, tr in enumerate(travs):
             if lev >= len(tr.from_sep_smaller_by_level):
                 continue
             tbs = np.asarray(tr.target_boxes_sep_smaller_by_source_level[lev], dtype=np.int64)
+            if len(tbs) == 0:
+                continue
             rows.append(maps[i][tbs])
-            pos = np.arange(n, n + len(tbs))
-            n += len(tbs)
-            csr = tr.from_sep_smaller_by_level[lev]
-            if len(csr.starts) > 1:
-                parts3.append((pos, csr.starts, csr.lists, maps[i]))
-        s3, l3, _ = _merge_csr([q[0] for q in parts3], n, [q[1] for q in parts3],
-                               [q[2] for q in parts3], [q[3] for q in parts3])
+            blk.append((i, 0, len(tbs)))
+        s3, l3, _ = _merge_csr(
+            blk, [tr.from_sep_smaller_by_level[lev].starts if lev < len(
+                tr.from_sep_smaller_by_level) else None for tr in travs],
+            [tr.from_sep_smaller_by_level[lev].lists if lev < len(
+                tr.from_sep_smaller_by_level) else None for tr in travs], maps)
         by_level_tb.append(_cat(rows))
         by_level.append(FromSepSmallerCSR(starts=s3, lists=l3))
 
