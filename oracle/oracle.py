@@ -1,4 +1,5 @@
-"""ctypes front end of the FP64 CPU oracle (``oracle/fmm_oracle.c``).
+"""ctypes front end of the FP64 CPU oracle (``oracle/fmm_oracle.c`` for
+Laplace, ``oracle/helmholtz_oracle.c`` for Helmholtz).
 
 TEST INFRASTRUCTURE ONLY: imported by ``tests/``, by the smoke check in
 ``__graft_entry__.py`` and by the CPU-baseline / reference arm of
@@ -136,6 +137,91 @@ def m2l(p, rsrc, rtgt, dvec, coeffs):
 # }}}
 
 
+# {{{ Helmholtz point-level operators (helmholtz_oracle.c; complex128)
+
+def _c128(a):
+    return np.ascontiguousarray(a, dtype=np.complex128)
+
+
+def helm_p2m(p, rscale, k, center, sources, strengths):
+    s = _f64(sources)
+    q = _c128(strengths)
+    out = np.zeros(ncoeff(p), dtype=np.complex128)
+    lib().oracle_helm_p2m_point(_i(p), _d(rscale), _d(k), _ptr(_f64(center)),
+                                _i(s.shape[1]), _ptr(_f64(s[0])), _ptr(_f64(s[1])),
+                                _ptr(_f64(s[2])), _ptr(q), _ptr(out))
+    return out
+
+
+def helm_p2l(p, rscale, k, center, sources, strengths):
+    s = _f64(sources)
+    q = _c128(strengths)
+    out = np.zeros(ncoeff(p), dtype=np.complex128)
+    lib().oracle_helm_p2l_point(_i(p), _d(rscale), _d(k), _ptr(_f64(center)),
+                                _i(s.shape[1]), _ptr(_f64(s[0])), _ptr(_f64(s[1])),
+                                _ptr(_f64(s[2])), _ptr(q), _ptr(out))
+    return out
+
+
+def helm_l2p(p, rscale, k, coeffs, bvec):
+    out = np.zeros(1, dtype=np.complex128)
+    lib().oracle_helm_l2p_point(_i(p), _d(rscale), _d(k), _ptr(_c128(coeffs)),
+                                _ptr(_f64(bvec)), _ptr(out))
+    return out[0]
+
+
+def helm_m2p(p, rscale, k, coeffs, bvec):
+    out = np.zeros(1, dtype=np.complex128)
+    lib().oracle_helm_m2p_point(_i(p), _d(rscale), _d(k), _ptr(_c128(coeffs)),
+                                _ptr(_f64(bvec)), _ptr(out))
+    return out[0]
+
+
+def helm_m2m(psrc, ptgt, rsrc, rtgt, k, dvec, coeffs):
+    out = np.zeros(ncoeff(ptgt), dtype=np.complex128)
+    lib().oracle_helm_m2m_point(_i(psrc), _i(ptgt), _d(rsrc), _d(rtgt), _d(k),
+                                _ptr(_f64(dvec)), _ptr(_c128(coeffs)), _ptr(out))
+    return out
+
+
+def helm_l2l(psrc, ptgt, rsrc, rtgt, k, dvec, coeffs):
+    out = np.zeros(ncoeff(ptgt), dtype=np.complex128)
+    lib().oracle_helm_l2l_point(_i(psrc), _i(ptgt), _d(rsrc), _d(rtgt), _d(k),
+                                _ptr(_f64(dvec)), _ptr(_c128(coeffs)), _ptr(out))
+    return out
+
+
+def helm_m2l(p, rsrc, rtgt, k, dvec, coeffs):
+    out = np.zeros(ncoeff(p), dtype=np.complex128)
+    lib().oracle_helm_m2l_point(_i(p), _d(rsrc), _d(rtgt), _d(k), _ptr(_f64(dvec)),
+                                _ptr(_c128(coeffs)), _ptr(out))
+    return out
+
+
+def helm_derivs(x, rscale, k, maxdeg):
+    """D[i][j][l] = rscale^|mi| d^mi (e^{ikr}/r) at x for mi0 <= 1, |mi| <= maxdeg."""
+    out = np.zeros((2, maxdeg + 1, maxdeg + 1), dtype=np.complex128)
+    lib().oracle_helm_derivs(_ptr(_f64(x)), _d(rscale), _d(k), _i(maxdeg), _ptr(out))
+    return out
+
+
+def helm_p2p_direct(targets, sources, k, strengths, target_to_source=None):
+    """FP64 direct sum 1/(4 pi) sum_s q_s e^{ik|t-s|}/|t-s| (complex strengths)."""
+    t = _f64(targets)
+    s = _f64(sources)
+    q = _c128(strengths)
+    pot = np.zeros(t.shape[1], dtype=np.complex128)
+    tts = None if target_to_source is None else _i32a(target_to_source)
+    tx, ty, tz = (_f64(t[i]) for i in range(3))
+    sx, sy, sz = (_f64(s[i]) for i in range(3))
+    lib().oracle_helm_p2p_direct(_i64(t.shape[1]), _ptr(tx), _ptr(ty), _ptr(tz),
+                                 _i64(s.shape[1]), _ptr(sx), _ptr(sy), _ptr(sz), _d(k),
+                                 _ptr(q), _ptr(tts), _ptr(pot))
+    return pot
+
+# }}}
+
+
 # {{{ direct sum
 
 def p2p_direct(targets, sources, strengths, target_to_source=None):
@@ -158,7 +244,7 @@ def p2p_direct(targets, sources, strengths, target_to_source=None):
 # {{{ whole FMM over a tree
 
 def run_fmm(tree, trav, tcls, order, weights, exclude_self=False,
-            rscale_fn=None, stages=None):
+            rscale_fn=None, stages=None, helmholtz_k=None):
     """FP64 FMM in boxtree ``drive_fmm`` order, on host numpy arrays.
 
     :arg tree, trav, tcls: host objects from :mod:`sumpy_b200.tree`
@@ -168,9 +254,17 @@ def run_fmm(tree, trav, tcls, order, weights, exclude_self=False,
     :arg stages: optional dict; when given, intermediate arrays are stored
         into it (``mpoles``, ``locals``, per-stage potentials) for stage-level
         comparisons.
+    :arg helmholtz_k: run the Helmholtz oracle (``helmholtz_oracle.c``,
+        G = e^{ikr}/r, complex strengths and results) with this wave number.
     :returns: potentials in user target order.
     """
     L = lib()
+    H = helmholtz_k is not None
+    kk = [_d(helmholtz_k)] if H else []
+    dt = np.complex128 if H else np.float64
+
+    def fn(name):
+        return getattr(L, ("oracle_helm_" if H else "oracle_") + name)
     p = order
     nc = ncoeff(p)
     nlev = tree.nlevels
@@ -190,13 +284,13 @@ def run_fmm(tree, trav, tcls, order, weights, exclude_self=False,
             return rscale_fn(lev)
         return tree.root_extent * 2.0 ** (-lev) * 2.0 / p
 
-    q = _f64(np.asarray(weights)[tree.user_source_ids])
+    q = np.ascontiguousarray(np.asarray(weights)[tree.user_source_ids], dtype=dt)
     tts = None
     if exclude_self:
         tts = _i32a(tree.target_to_source)
 
-    mpoles = np.zeros(tree.nboxes * nc)
-    locs = np.zeros(tree.nboxes * nc)
+    mpoles = np.zeros(tree.nboxes * nc, dtype=dt)
+    locs = np.zeros(tree.nboxes * nc, dtype=dt)
 
     def lview(arr, lev):
         return arr[lsb[lev] * nc:lsb[lev + 1] * nc]
@@ -208,7 +302,7 @@ def run_fmm(tree, trav, tcls, order, weights, exclude_self=False,
         if a == b:
             continue
         boxes = _i32a(trav.source_boxes[a:b])
-        L.oracle_p2m_level(_i(p), _d(rscale(lev)), _i32(b - a), _ptr(boxes),
+        fn("p2m_level")(_i(p), _d(rscale(lev)), *kk, _i32(b - a), _ptr(boxes),
                            _i32(lsb[lev]), _ptr(cx), _ptr(cy), _ptr(cz),
                            _ptr(bss), _ptr(bsc), _ptr(sx), _ptr(sy), _ptr(sz),
                            _ptr(q), _ptr(lview(mpoles, lev)))
@@ -220,7 +314,7 @@ def run_fmm(tree, trav, tcls, order, weights, exclude_self=False,
         if a == b:
             continue
         boxes = _i32a(trav.source_parent_boxes[a:b])
-        L.oracle_m2m_level(_i(p), _i(p), _d(rscale(src_lev)), _d(rscale(tgt_lev)),
+        fn("m2m_level")(_i(p), _i(p), _d(rscale(src_lev)), _d(rscale(tgt_lev)), *kk,
                            _i32(b - a), _ptr(boxes), _ptr(child), _i64(child.shape[1]),
                            _ptr(cx), _ptr(cy), _ptr(cz),
                            _i32(lsb[src_lev]), _ptr(lview(mpoles, src_lev)),
@@ -229,13 +323,13 @@ def run_fmm(tree, trav, tcls, order, weights, exclude_self=False,
         stages["mpoles"] = mpoles.copy()
 
     # eval_direct (List 1)
-    pot_direct = np.zeros(tree.ntargets)
+    pot_direct = np.zeros(tree.ntargets, dtype=dt)
     tb = _i32a(trav.target_boxes)
     if len(tb):
-        L.oracle_p2p_csr(_i32(len(tb)), _ptr(tb), _ptr(_i32a(trav.neighbor_source_boxes_starts)),
+        fn("p2p_csr")(_i32(len(tb)), _ptr(tb), _ptr(_i32a(trav.neighbor_source_boxes_starts)),
                          _ptr(_i32a(trav.neighbor_source_boxes_lists)),
                          _ptr(bss), _ptr(bsc), _ptr(bts), _ptr(btc),
-                         _ptr(sx), _ptr(sy), _ptr(sz), _ptr(q),
+                         _ptr(sx), _ptr(sy), _ptr(sz), *kk, _ptr(q),
                          _ptr(tx), _ptr(ty), _ptr(tz), _ptr(tts), _ptr(pot_direct))
 
     # multipole_to_local (List 2)
@@ -253,7 +347,7 @@ def run_fmm(tree, trav, tcls, order, weights, exclude_self=False,
             continue
         boxes = _i32a(tpb[a:b])
         starts = _i32a(np.asarray(s2s[a:b + 1]))
-        L.oracle_m2l_level(_i(p), _d(rscale(lev)), _i32(b - a), _ptr(boxes),
+        fn("m2l_level")(_i(p), _d(rscale(lev)), *kk, _i32(b - a), _ptr(boxes),
                            _ptr(starts), _ptr(s2l), _ptr(ecls),
                            _i32(cls_ls[lev + 1] - cls_ls[lev]), _i32(cls_ls[lev]),
                            _ptr(cvec), _i64(cvec.shape[1]), _i32(lsb[lev]),
@@ -262,13 +356,13 @@ def run_fmm(tree, trav, tcls, order, weights, exclude_self=False,
         stages["m2l_locals"] = m2l_locs.copy()
 
     # eval_multipoles (List 3)
-    pot_m2p = np.zeros(tree.ntargets)
+    pot_m2p = np.zeros(tree.ntargets, dtype=dt)
     for lev in range(nlev):
         tgt = trav.target_boxes_sep_smaller_by_source_level[lev]
         if len(tgt) == 0:
             continue
         lst = trav.from_sep_smaller_by_level[lev]
-        L.oracle_m2p_level(_i(p), _d(rscale(lev)), _i32(len(tgt)), _ptr(_i32a(tgt)),
+        fn("m2p_level")(_i(p), _d(rscale(lev)), *kk, _i32(len(tgt)), _ptr(_i32a(tgt)),
                            _ptr(_i32a(lst.starts)), _ptr(_i32a(lst.lists)),
                            _ptr(cx), _ptr(cy), _ptr(cz), _i32(lsb[lev]),
                            _ptr(lview(mpoles, lev)), _ptr(bts), _ptr(btc),
@@ -284,7 +378,7 @@ def run_fmm(tree, trav, tcls, order, weights, exclude_self=False,
             continue
         boxes = _i32a(tpb[a:b])
         starts = _i32a(np.asarray(s4s[a:b + 1]))
-        L.oracle_p2l_level(_i(p), _d(rscale(lev)), _i32(b - a), _ptr(boxes),
+        fn("p2l_level")(_i(p), _d(rscale(lev)), *kk, _i32(b - a), _ptr(boxes),
                            _ptr(starts), _ptr(s4l), _ptr(cx), _ptr(cy), _ptr(cz),
                            _ptr(bss), _ptr(bsc), _ptr(sx), _ptr(sy), _ptr(sz),
                            _ptr(q), _i32(lsb[lev]), _ptr(lview(p2l_locs, lev)))
@@ -297,7 +391,7 @@ def run_fmm(tree, trav, tcls, order, weights, exclude_self=False,
             continue
         src_lev = tgt_lev - 1
         boxes = _i32a(tpb[a:b])
-        L.oracle_l2l_level(_i(p), _i(p), _d(rscale(src_lev)), _d(rscale(tgt_lev)),
+        fn("l2l_level")(_i(p), _i(p), _d(rscale(src_lev)), _d(rscale(tgt_lev)), *kk,
                            _i32(b - a), _ptr(boxes), _ptr(parent),
                            _ptr(cx), _ptr(cy), _ptr(cz),
                            _i32(lsb[src_lev]), _ptr(lview(locs, src_lev)),
@@ -306,14 +400,14 @@ def run_fmm(tree, trav, tcls, order, weights, exclude_self=False,
         stages["locals"] = locs.copy()
 
     # eval_locals
-    pot_l2p = np.zeros(tree.ntargets)
+    pot_l2p = np.zeros(tree.ntargets, dtype=dt)
     ltb = trav.level_start_target_box_nrs
     for lev in range(nlev):
         a, b = ltb[lev], ltb[lev + 1]
         if a == b:
             continue
         boxes = _i32a(trav.target_boxes[a:b])
-        L.oracle_l2p_level(_i(p), _d(rscale(lev)), _i32(b - a), _ptr(boxes),
+        fn("l2p_level")(_i(p), _d(rscale(lev)), *kk, _i32(b - a), _ptr(boxes),
                            _ptr(cx), _ptr(cy), _ptr(cz), _i32(lsb[lev]),
                            _ptr(lview(locs, lev)), _ptr(bts), _ptr(btc),
                            _ptr(tx), _ptr(ty), _ptr(tz), _ptr(pot_l2p))

@@ -3,7 +3,9 @@
 This script is test infrastructure. It is run by hand in a container that has
 the sumpy source tree (``SUMPY_REFERENCE`` env var, default ``/root/reference``)
 and sympy installed; the GPU test box never runs it. It writes
-``tests/golden/laplace3d_operators.json``, which the tests read.
+``tests/golden/laplace3d_operators.json`` and
+``tests/golden/helmholtz3d_operators.json``, which the tests read
+(``python tests/golden/make_golden.py [laplace] [helmholtz]``).
 
 sumpy itself cannot be imported normally here: its package ``__init__`` pulls
 in pyopencl/loopy/boxtree, none of which are installed. The expansion math
@@ -23,7 +25,10 @@ modules import is used only when generating loopy code. So this script
 * subclasses sumpy's ``LaplaceKernel`` only to return the sympy expression
   ``1/|d|`` directly (sumpy builds it via pymbolic, ``sumpy/kernel.py:650-658``),
   leaving ``get_derivative_taker`` (``LaplaceDerivativeTaker``) and
-  ``get_pde_as_diff_op`` (the Laplacian) as sumpy defines them.
+  ``get_pde_as_diff_op`` (the Laplacian) as sumpy defines them; and sumpy's
+  ``HelmholtzKernel`` (``sumpy/kernel.py:755-844``) the same way with
+  ``exp(i k |d|)/|d|`` at k = 5/2, keeping ``HelmholtzDerivativeTaker``
+  (``sumpy/derivative_taker.py:354-389``) and the PDE Laplacian + k^2.
 
 For each order it then calls, on symbolic inputs, the same methods sumpy's
 loopy kernels are generated from, and evaluates the results at fixed inputs
@@ -190,13 +195,9 @@ def _install_placeholders():
 # }}}
 
 
-def main():
-    _install_placeholders()
+def _kernels():
     import sympy
 
-    import sumpy.expansion.local as local_mod
-    import sumpy.expansion.m2l as m2l_mod
-    import sumpy.expansion.multipole as mpole_mod
     import sumpy.kernel as kernel_mod
 
     class Laplace3D(kernel_mod.LaplaceKernel):
@@ -214,20 +215,55 @@ def main():
         def __eq__(self, other):
             return isinstance(other, Laplace3D)
 
-    knl = Laplace3D()
+    class Helmholtz3D(kernel_mod.HelmholtzKernel):
+        """sumpy's HelmholtzKernel(3) with the wave number fixed at HELM_K;
+        get_derivative_taker (HelmholtzDerivativeTaker) and
+        get_pde_as_diff_op (Laplacian + k^2, symbol ``k``) are sumpy's."""
+
+        def __init__(self):
+            object.__setattr__(self, "dim", 3)
+            object.__setattr__(self, "expression", "helmholtz3d")
+            object.__setattr__(self, "global_scaling_const", "1/(4pi)")
+            object.__setattr__(self, "helmholtz_k_name", "k")
+            object.__setattr__(self, "allow_evanescent", False)
+
+        def get_expression(self, dvec):
+            r = sympy.sqrt(sum(d**2 for d in dvec))
+            return sympy.exp(sympy.I * HELM_K * r) / r
+
+        def __hash__(self):
+            return hash("helmholtz3d-golden")
+
+        def __eq__(self, other):
+            return isinstance(other, Helmholtz3D)
+
+    return Laplace3D(), Helmholtz3D()
+
+
+HELM_K = None   # set in main (a sympy Rational)
+
+
+def generate(knl, orders, out_path, label, complex_valued, extra_subs):
+    import sympy
+
+    import sumpy.expansion.local as local_mod
+    import sumpy.expansion.m2l as m2l_mod
+    import sumpy.expansion.multipole as mpole_mod
+
     rng = np.random.default_rng(2024)
 
     def exact(x):
         return sympy.Rational(Fraction(float(x)))
 
     def ev(expr, subs):
-        return float(sympy.N(sympy.sympify(expr).doit().xreplace(subs), 40))
+        v = complex(sympy.N(sympy.sympify(expr).doit().xreplace(subs), 40))
+        return [v.real, v.imag] if complex_valued else v.real
 
     vec_syms = sympy.Matrix(sympy.symbols("v0:3"))
     r_src, r_tgt = sympy.symbols("rsrc rtgt")
 
     cases = []
-    for order in (2, 3, 4, 5):
+    for order in orders:
         mpole = mpole_mod.LinearPDEConformingVolumeTaylorMultipoleExpansion(
             knl, order, use_rscale=True)
         local = local_mod.LinearPDEConformingVolumeTaylorLocalExpansion(
@@ -253,6 +289,7 @@ def main():
             s = {vec_syms[i]: exact(v[i]) for i in range(3)}
             s.update({r_src: exact(rs), r_tgt: exact(rt)})
             s.update({coeff_syms[i]: exact(cin[i]) for i in range(n)})
+            s.update(extra_subs)
             s.update(dict(extra))
             return s
 
@@ -291,16 +328,37 @@ def main():
         case["m2l_ratio"] = {"dvec": d_ml.tolist(),
                              "out": [ev(e, vsubs(d_ml)) for e in m2l2]}
         cases.append(case)
-        print(f"order {order}: n={n} done", flush=True)
+        print(f"{label} order {order}: n={n} done", flush=True)
 
-    OUT.write_text(json.dumps({
+    return {
         "generator": "tests/golden/make_golden.py",
-        "kernel": "LaplaceKernel(3), expression 1/|d| (scaling applied on output)",
         "expansions": "LinearPDEConformingVolumeTaylor{Multipole,Local}Expansion",
         "conventions": {"avec": "center - source", "bvec": "target - center",
                         "dvec": "target center - source center"},
-        "cases": cases}, indent=1))
-    print("wrote", OUT)
+        "cases": cases}
+
+
+def main():
+    global HELM_K
+    _install_placeholders()
+    import sympy
+    HELM_K = sympy.Rational(5, 2)
+    lap, helm = _kernels()
+    which = sys.argv[1:] or ["laplace", "helmholtz"]
+    if "laplace" in which:
+        data = generate(lap, (2, 3, 4, 5), OUT, "laplace", False, {})
+        data["kernel"] = "LaplaceKernel(3), expression 1/|d| (scaling applied on output)"
+        OUT.write_text(json.dumps(data, indent=1))
+        print("wrote", OUT)
+    if "helmholtz" in which:
+        out = OUT.with_name("helmholtz3d_operators.json")
+        data = generate(helm, (2, 3, 4), out, "helmholtz", True,
+                        {sympy.Symbol("k"): HELM_K})
+        data["kernel"] = ("HelmholtzKernel(3), expression exp(i k |d|)/|d| with k = 5/2 "
+                          "(scaling applied on output); complex values as [re, im]")
+        data["k"] = float(HELM_K)
+        out.write_text(json.dumps(data, indent=1))
+        print("wrote", out)
 
 
 if __name__ == "__main__":
