@@ -318,6 +318,107 @@ int sumpy_e2p_from_csr_grad_f64(
     const double *targets, int64_t target_stride, double scale, double *result,
     double *grad, void *stream);
 
+/* ------------------------------------------------------------------------
+ * 3D Helmholtz kernel G = exp(i k r) / r (sumpy/kernel.py:755-844), the same
+ * loopy kernels as above instantiated for HelmholtzKernel(3): complex data
+ * (strengths, expansions, results) as interleaved (re, im) float64 pairs,
+ * i.e. complex128 arrays; coordinates real. k is the (real) wave number
+ * sumpy passes as the kernel argument "k". Expansions use the Helmholtz PDE
+ * projection u_mi = -u_{mi-2e0+2e1} - u_{mi-2e0+2e2} - k^2 rscale^2 u_{mi-2e0}.
+ * Arguments otherwise as for the Laplace entry points above.
+ * ------------------------------------------------------------------------ */
+
+/* P2PFromCSR (sumpy/p2p.py:484-833) */
+int sumpy_helmholtz_p2p_from_csr_f64(
+    int32_t ntgt_boxes, const int32_t *target_boxes, const int32_t *source_box_starts,
+    const int32_t *source_box_lists, const int32_t *box_source_starts,
+    const int32_t *box_source_counts_nonchild, const int32_t *box_target_starts,
+    const int32_t *box_target_counts_nonchild, const double *sources, int64_t source_stride,
+    double k, const double *strength, const double *targets, int64_t target_stride,
+    const int32_t *target_to_source, double scale, double *result, void *stream);
+
+/* Same with complex64 arithmetic on FP64 coordinate differences, FP64 sums
+ * per source box. */
+int sumpy_helmholtz_p2p_from_csr_mixed(
+    int32_t ntgt_boxes, const int32_t *target_boxes, const int32_t *source_box_starts,
+    const int32_t *source_box_lists, const int32_t *box_source_starts,
+    const int32_t *box_source_counts_nonchild, const int32_t *box_target_starts,
+    const int32_t *box_target_counts_nonchild, const double *sources, int64_t source_stride,
+    double k, const double *strength, const double *targets, int64_t target_stride,
+    const int32_t *target_to_source, double scale, double *result, void *stream);
+
+/* P2P (sumpy/p2p.py:215-285), all pairs */
+int sumpy_helmholtz_p2p_direct_f64(
+    int64_t ntargets, const double *targets, int64_t target_stride, int64_t nsources,
+    const double *sources, int64_t source_stride, double k, const double *strength,
+    const int32_t *target_to_source, double scale, double *result, void *stream);
+
+/* P2EFromSingleBox (sumpy/p2e.py:155-261) */
+int sumpy_helmholtz_p2e_from_single_box_f64(
+    int order, double rscale, double k, int32_t nsrc_boxes, const int32_t *source_boxes,
+    const double *centers, int64_t center_stride, const int32_t *box_source_starts,
+    const int32_t *box_source_counts_nonchild, const double *sources, int64_t source_stride,
+    const double *strength, int32_t tgt_base_ibox, double *tgt_expansions, void *stream);
+
+/* E2EFromChildren (sumpy/e2e.py:866-978) */
+int sumpy_helmholtz_e2e_from_children_f64(
+    int src_order, int tgt_order, double src_rscale, double tgt_rscale, double k,
+    int32_t ntgt_boxes, const int32_t *target_boxes, const int32_t *box_child_ids,
+    int64_t child_stride, const double *centers, int64_t center_stride, int32_t src_base_ibox,
+    const double *src_expansions, int32_t tgt_base_ibox, double *tgt_expansions, void *stream);
+
+/* E2EFromParent (sumpy/e2e.py:985-1083) */
+int sumpy_helmholtz_e2e_from_parent_f64(
+    int src_order, int tgt_order, double src_rscale, double tgt_rscale, double k,
+    int32_t ntgt_boxes, const int32_t *target_boxes, const int32_t *box_parent_ids,
+    const double *centers, int64_t center_stride, int32_t src_base_ibox,
+    const double *src_expansions, int32_t tgt_base_ibox, double *tgt_expansions, void *stream);
+
+/* M2L per translation class (sumpy/e2e.py:310-859) on complex expansions:
+ * class_matrices are the real embeddings [nclasses][2n][2n] (n = (order+1)^2)
+ * of the complex operators, blocks [[Re, -Im], [Im, Re]]; otherwise as
+ * sumpy_m2l_translation_classes_f64 with 2n real values per box. */
+int sumpy_helmholtz_m2l_translation_classes_f64(
+    int order, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
+    const int32_t *item_group_end, int32_t tile_width, const int32_t *tile_targets,
+    const double *tile_scale, const int32_t *group_class, const int32_t *group_sources,
+    int32_t nclasses, const double *class_matrices, int32_t src_base_ibox,
+    const double *src_expansions, int32_t tgt_base_ibox, double *tgt_expansions, void *stream);
+
+/* Same on the tensor cores (split TF32 planes of the real embeddings, rows
+ * and k padded for 2n; see sumpy_m2l_translation_classes_tf32x3). */
+int sumpy_helmholtz_m2l_translation_classes_tf32x3(
+    int order, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
+    const int32_t *item_group_end, int32_t tile_width, const int32_t *tile_targets,
+    const double *tile_scale, const int32_t *group_class, const int32_t *group_sources,
+    int32_t nclasses, const float *mats_hi, const float *mats_lo, int32_t rows_pad, int32_t k_pad,
+    int32_t src_nrows, int32_t src_base_ibox, const float *src_hi, const float *src_lo,
+    int32_t tgt_base_ibox, double *tgt_expansions, int32_t *status, void *stream);
+
+/* E2PFromSingleBox (sumpy/e2p.py:123-226): result assigned */
+int sumpy_helmholtz_e2p_from_single_box_f64(
+    int order, double rscale, double k, int32_t ntgt_boxes, const int32_t *target_boxes,
+    const double *centers, int64_t center_stride, int32_t src_base_ibox,
+    const double *src_expansions, const int32_t *box_target_starts,
+    const int32_t *box_target_counts_nonchild, const double *targets, int64_t target_stride,
+    double scale, double *result, void *stream);
+
+/* E2PFromCSR (sumpy/e2p.py:233-343): result accumulated */
+int sumpy_helmholtz_e2p_from_csr_f64(
+    int order, double rscale, double k, int32_t ntgt_boxes, const int32_t *target_boxes,
+    const int32_t *source_box_starts, const int32_t *source_box_lists, const double *centers,
+    int64_t center_stride, int32_t src_base_ibox, const double *src_expansions,
+    const int32_t *box_target_starts, const int32_t *box_target_counts_nonchild,
+    const double *targets, int64_t target_stride, double scale, double *result, void *stream);
+
+/* P2EFromCSR (sumpy/p2e.py:268-388): expansions accumulated */
+int sumpy_helmholtz_p2e_from_csr_f64(
+    int order, double rscale, double k, int32_t ntgt_boxes, const int32_t *target_boxes,
+    const int32_t *source_box_starts, const int32_t *source_box_lists, const double *centers,
+    int64_t center_stride, const int32_t *box_source_starts,
+    const int32_t *box_source_counts_nonchild, const double *sources, int64_t source_stride,
+    const double *strength, int32_t tgt_base_ibox, double *tgt_expansions, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

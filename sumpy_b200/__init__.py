@@ -12,11 +12,12 @@ from sumpy_b200.expansion import (
     LinearPDEConformingVolumeTaylorMultipoleExpansion,
 )
 from sumpy_b200.fmm import SumpyExpansionWrangler, SumpyTreeIndependentDataForWrangler
-from sumpy_b200.kernel import LaplaceKernel
+from sumpy_b200.kernel import HelmholtzKernel, LaplaceKernel
 from sumpy_b200.p2p import P2P
 
 __all__ = [
     "P2P",
+    "HelmholtzKernel",
     "LaplaceKernel",
     "LinearPDEConformingVolumeTaylorLocalExpansion",
     "LinearPDEConformingVolumeTaylorMultipoleExpansion",

@@ -54,6 +54,31 @@ SIGNATURES = {
                                       ptr, i64, dbl, ptr, ptr],
     "sumpy_e2p_from_csr_f64": [cint, dbl, i32, ptr, ptr, ptr, ptr, i64, i32, ptr, ptr, ptr,
                                ptr, i64, dbl, ptr, ptr],
+    # Helmholtz
+    "sumpy_helmholtz_p2p_from_csr_f64": [i32, ptr, ptr, ptr, ptr, ptr, ptr, ptr, ptr, i64, dbl,
+                                         ptr, ptr, i64, ptr, dbl, ptr, ptr],
+    "sumpy_helmholtz_p2p_from_csr_mixed": [i32, ptr, ptr, ptr, ptr, ptr, ptr, ptr, ptr, i64,
+                                           dbl, ptr, ptr, i64, ptr, dbl, ptr, ptr],
+    "sumpy_helmholtz_p2p_direct_f64": [i64, ptr, i64, i64, ptr, i64, dbl, ptr, ptr, dbl, ptr,
+                                       ptr],
+    "sumpy_helmholtz_p2e_from_single_box_f64": [cint, dbl, dbl, i32, ptr, ptr, i64, ptr, ptr,
+                                                ptr, i64, ptr, i32, ptr, ptr],
+    "sumpy_helmholtz_e2e_from_children_f64": [cint, cint, dbl, dbl, dbl, i32, ptr, ptr, i64,
+                                              ptr, i64, i32, ptr, i32, ptr, ptr],
+    "sumpy_helmholtz_e2e_from_parent_f64": [cint, cint, dbl, dbl, dbl, i32, ptr, ptr, ptr, i64,
+                                            i32, ptr, i32, ptr, ptr],
+    "sumpy_helmholtz_m2l_translation_classes_f64": [cint, i32, ptr, ptr, ptr, i32, ptr, ptr,
+                                                    ptr, ptr, i32, ptr, i32, ptr, i32, ptr,
+                                                    ptr],
+    "sumpy_helmholtz_m2l_translation_classes_tf32x3": [cint, i32, ptr, ptr, ptr, i32, ptr, ptr,
+                                                       ptr, ptr, i32, ptr, ptr, i32, i32, i32,
+                                                       i32, ptr, ptr, i32, ptr, ptr, ptr],
+    "sumpy_helmholtz_e2p_from_single_box_f64": [cint, dbl, dbl, i32, ptr, ptr, i64, i32, ptr,
+                                                ptr, ptr, ptr, i64, dbl, ptr, ptr],
+    "sumpy_helmholtz_e2p_from_csr_f64": [cint, dbl, dbl, i32, ptr, ptr, ptr, ptr, i64, i32,
+                                         ptr, ptr, ptr, ptr, i64, dbl, ptr, ptr],
+    "sumpy_helmholtz_p2e_from_csr_f64": [cint, dbl, dbl, i32, ptr, ptr, ptr, ptr, i64, ptr,
+                                         ptr, ptr, i64, ptr, i32, ptr, ptr],
 }
 
 _RESTYPES = {

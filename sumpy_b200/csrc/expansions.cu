@@ -18,50 +18,10 @@
 
 #include "common.cuh"
 #include "derivs.cuh"
+#include "taylor.cuh"
 
 namespace sumpy {
 namespace {
-
-__device__ inline int nfull_of(int p) { return (p + 1) * (p + 2) * (p + 3) / 6; }
-
-// f-th multi-index of the full set in sumpy's order (|mi|, mi0, mi1, mi2)
-__device__ inline void full_mi(int f, int &i, int &j, int &k)
-{
-    int deg = 0;
-    while ((deg + 1) * (deg + 2) * (deg + 3) / 6 <= f) ++deg;
-    int r = f - deg * (deg + 1) * (deg + 2) / 6;
-    i = 0;
-    while (r >= deg - i + 1) { r -= deg - i + 1; ++i; }
-    j = r;
-    k = deg - i - j;
-}
-
-// s-th multi-index of the stored set (inverse of stored_index)
-__device__ inline void stored_mi(int s, int &i, int &j, int &k)
-{
-    int deg = (int)sqrtf((float)s);
-    while (deg * deg > s) --deg;
-    while ((deg + 1) * (deg + 1) <= s) ++deg;
-    int r = s - deg * deg;
-    if (r <= deg) { i = 0; j = r; }
-    else { i = 1; j = r - (deg + 1); }
-    k = deg - i - j;
-}
-
-// t-th pair (J, K) with J + K <= m
-__device__ inline void tri_pair(int t, int m, int &J, int &K)
-{
-    J = 0;
-    while (t > m - J) { t -= m - J + 1; ++J; }
-    K = t;
-}
-
-__device__ inline double ipow(double x, int n)
-{
-    double r = 1.0;
-    for (int q = 0; q < n; ++q) r *= x;
-    return r;
-}
 
 // stored multipole -> nothing; full multipole (cube) -> compressed in place
 // (plane i-2 receives -cube[i][J-2][K] - cube[i][J][K-2]). Block-wide.
@@ -161,14 +121,6 @@ p2m_kernel(int p, double rscale, const int32_t *__restrict__ boxes, const double
 // }}}
 
 // {{{ M2M / L2L (axis-by-axis shifts)
-
-// Index of (i, j, k) in sumpy's full order (|mi|, mi0, mi1, mi2):
-// tetra(deg) + sum_{i' < i} (deg - i' + 1) + j.
-__device__ __forceinline__ int full_index(int i, int j, int k)
-{
-    const int deg = i + j + k;
-    return deg * (deg + 1) * (deg + 2) / 6 + i * (deg + 1) - i * (i - 1) / 2 + j;
-}
 
 constexpr int M2M_THREADS = 256;
 
@@ -449,23 +401,6 @@ __global__ void l2p_kernel(int p, double rscale, int32_t nboxes, const int32_t *
 // }}}
 
 constexpr int DSTRIDE = 33;  // lanes per coefficient row + 1 (bank spread)
-
-bool order_ok(int p) { return p >= 0 && p <= SUMPY_MAX_ORDER; }
-
-template <typename K>
-int prepare_smem(K kernel, size_t bytes)
-{
-    if (bytes > 227 * 1024) return bad_arg("shared memory request exceeds 227 KB");
-    if (bytes > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)bytes);
-        if (e != cudaSuccess) {
-            set_last_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
-            return SUMPY_ELAUNCH;
-        }
-    }
-    return SUMPY_OK;
-}
 
 // {{{ M2P / P2L with register-resident derivative layers
 

@@ -1,0 +1,1087 @@
+// 3D Helmholtz FMM kernels: G = exp(i k r) / r (sumpy's HelmholtzKernel(3),
+// sumpy/kernel.py:755-844) with the compressed Taylor expansions
+// (stored set mi0 < 2). Complex values are interleaved (re, im) pairs
+// (double2), which is how a complex128 array is laid out.
+//
+// What differs from the Laplace kernels:
+//  * P2M, M2M, L2L and L2P are real-linear maps with real coefficients (k is
+//    real), applied here to complex data. The PDE projection gains a term:
+//    u_mi = -u_{mi-2e0+2e1} - u_{mi-2e0+2e2} - kappa u_{mi-2e0} with
+//    kappa = k^2 rscale^2 (sumpy/expansion/__init__.py:754-886 for the PDE
+//    Laplacian + k^2, sumpy/kernel.py:838-844).
+//  * M2P and P2L need D(mi) = rs^|mi| d^mi G for the stored mi. sumpy takes
+//    them with Tausch's recursion for radial functions
+//    (RadialDerivativeTaker / HelmholtzDerivativeTaker,
+//    sumpy/derivative_taker.py:269-389). Here the same quantities come from
+//    its closed form: with u = r^2/2, G = F(u) and g_Q = F^(Q)(u) =
+//    ((1/r) d/dr)^Q G, the chain rule on the separable u = sum x_a^2/2 gives
+//        d^mi G = sum_{q_a} g_{q0+q1+q2} prod_a C[m_a][q_a] x_a^(2 q_a - m_a),
+//        C[m][q] = m! / ((2q - m)! (m - q)! 2^(m - q)),  ceil(m/2) <= q <= m,
+//    so with n = x/r, rho = rs/r and gamma_Q = r^(2Q) g_Q,
+//        D(mi) = rho^|mi| sum_{q_a} gamma_{q0+q1+q2} prod_a C[m_a][q_a] n_a^(2q_a - m_a),
+//    gamma_0 = e^{ikr}/r, gamma_1 = (ikr - 1) e^{ikr}/r,
+//    gamma_Q = -(2Q - 1) gamma_{Q-1} - (kr)^2 gamma_{Q-2}
+//    (sumpy's q >= 2 step for g_q multiplied by r^(2Q)). For stored mi,
+//    m_0 <= 1 and the axis-0 factor is 1 or n_0.
+//  * P2P evaluates q e^{ikr}/r with complex strengths.
+//  * M2L reuses the real GEMM kernels (m2l.cu, m2l_tc.cu) on the real
+//    embedding [[Re, -Im], [Im, Re]] of the complex class operators.
+#include <algorithm>
+
+#include "common.cuh"
+#include "taylor.cuh"
+
+namespace sumpy {
+namespace {
+
+using z2 = double2;
+
+__device__ __forceinline__ z2 zmk(double a, double b) { return make_double2(a, b); }
+__device__ __forceinline__ z2 zadd(z2 a, z2 b) { return zmk(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ z2 zscal(double s, z2 a) { return zmk(s * a.x, s * a.y); }
+__device__ __forceinline__ z2 zmul(z2 a, z2 b)
+{
+    return zmk(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+// acc + s * a (s real)
+__device__ __forceinline__ z2 zaxpy(double s, z2 a, z2 acc)
+{
+    return zmk(fma(s, a.x, acc.x), fma(s, a.y, acc.y));
+}
+// acc + a * b
+__device__ __forceinline__ z2 zfma(z2 a, z2 b, z2 acc)
+{
+    return zmk(fma(a.x, b.x, fma(-a.y, b.y, acc.x)), fma(a.x, b.y, fma(a.y, b.x, acc.y)));
+}
+
+// C[m][q] of the closed form above; m is one axis of a stored multi-index,
+// so m <= SUMPY_MAX_ORDER.
+constexpr int CM = SUMPY_MAX_ORDER + 1;
+struct FaaTable {
+    double v[CM][CM];
+};
+constexpr FaaTable make_faa_table()
+{
+    FaaTable t{};
+    double f[CM] = {};
+    f[0] = 1.0;
+    for (int i = 1; i < CM; ++i) f[i] = f[i - 1] * i;
+    for (int m = 0; m < CM; ++m)
+        for (int q = 0; q < CM; ++q) {
+            const int a = 2 * q - m, b = m - q;
+            double v = 0.0;
+            if (a >= 0 && b >= 0) {
+                double p2 = 1.0;
+                for (int i = 0; i < b; ++i) p2 *= 2.0;
+                v = f[m] / (f[a] * f[b] * p2);
+            }
+            t.v[m][q] = v;
+        }
+    return t;
+}
+__constant__ FaaTable c_faa = make_faa_table();
+
+// gamma_Q, Q = 0..qmax, at distance r
+__device__ __forceinline__ void helm_gammas(double r, double k, int qmax, double *gr, double *gi,
+                                            int stride)
+{
+    double sn, cs;
+    sincos(k * r, &sn, &cs);
+    const double ri = 1.0 / r;
+    z2 g0 = zmk(cs * ri, sn * ri);
+    // (ikr - 1) e^{ikr} / r
+    z2 g1 = zmul(zmk(-1.0, k * r), g0);
+    gr[0] = g0.x; gi[0] = g0.y;
+    if (qmax >= 1) { gr[stride] = g1.x; gi[stride] = g1.y; }
+    const double kr2 = (k * r) * (k * r);
+    for (int q = 2; q <= qmax; ++q) {
+        const z2 g2 = zmk(-(2.0 * q - 1.0) * g1.x - kr2 * g0.x, -(2.0 * q - 1.0) * g1.y - kr2 * g0.y);
+        gr[q * stride] = g2.x; gi[q * stride] = g2.y;
+        g0 = g1; g1 = g2;
+    }
+}
+
+// sum_{q1, q2} C[j][q1] C[l][q2] N1[2q1-j] N2[2q2-l] gamma[q1+q2+i] for one
+// stored mi = (i, j, l); tables strided by `st`.
+__device__ __forceinline__ z2 helm_mi_sum(int i, int j, int l, const double *N1, const double *N2,
+                                          const double *gr, const double *gi, int st)
+{
+    z2 s = zmk(0.0, 0.0);
+    for (int q1 = (j + 1) >> 1; q1 <= j; ++q1) {
+        const double a1 = c_faa.v[j][q1] * N1[(2 * q1 - j) * st];
+        double sr = 0.0, si = 0.0;
+        for (int q2 = (l + 1) >> 1; q2 <= l; ++q2) {
+            const double a2 = c_faa.v[l][q2] * N2[(2 * q2 - l) * st];
+            const int Q = q1 + q2 + i;
+            sr = fma(a2, gr[Q * st], sr);
+            si = fma(a2, gi[Q * st], si);
+        }
+        s.x = fma(a1, sr, s.x);
+        s.y = fma(a1, si, s.y);
+    }
+    return s;
+}
+
+// {{{ P2P
+
+constexpr int HP2P_WARPS = 8;
+
+struct HSrc {
+    double x, y, z, qr, qi;
+};
+
+// List 1 (P2PFromCSR, sumpy/p2p.py:484-799) for G = e^{ikr}/r: one warp per
+// target box, targets on g = next_pow2(nt) lanes, 32/g lane groups striding
+// the staged sources, shuffle-xor sum. MIXED: FP64 coordinate difference
+// rounded to FP32, FP32 distance, phase and products per source box, FP64
+// totals. Results are assigned.
+template <bool MIXED>
+__global__ void __launch_bounds__(32 * HP2P_WARPS)
+hp2p_csr_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_boxes,
+                const int32_t *__restrict__ src_box_starts, const int32_t *__restrict__ src_box_lists,
+                const int32_t *__restrict__ box_src_starts, const int32_t *__restrict__ box_src_counts,
+                const int32_t *__restrict__ box_tgt_starts, const int32_t *__restrict__ box_tgt_counts,
+                const double *__restrict__ sources, int64_t sstride, const z2 *__restrict__ strength,
+                const double *__restrict__ targets, int64_t tstride,
+                const int32_t *__restrict__ target_to_source, double k, double scale,
+                z2 *__restrict__ result)
+{
+    __shared__ HSrc buf[HP2P_WARPS][32];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int ib = blockIdx.x * HP2P_WARPS + warp;
+    if (ib >= ntgt_boxes) return;
+    HSrc *wb = buf[warp];
+    const float kf = (float)k;
+
+    const int32_t tb = target_boxes[ib];
+    const int32_t t0 = box_tgt_starts[tb];
+    const int32_t nt = box_tgt_counts[tb];
+    const int32_t ls = src_box_starts[ib], le = src_box_starts[ib + 1];
+
+    for (int32_t tc = 0; tc < nt; tc += 32) {
+        const int ntc = min(32, nt - tc);
+        int g = 1;
+        while (g < ntc) g <<= 1;
+        const int nph = 32 / g;
+        const int tl = lane & (g - 1);
+        const int ph = lane / g;
+        const bool active = tl < ntc;
+        const int32_t t = t0 + tc + tl;
+        double tx = 0, ty = 0, tz = 0;
+        int32_t self = -1;
+        if (active) {
+            tx = targets[t];
+            ty = targets[tstride + t];
+            tz = targets[2 * tstride + t];
+            if (target_to_source) self = target_to_source[t];
+        }
+        double ar = 0.0, ai = 0.0;
+        for (int32_t l = ls; l < le; ++l) {
+            const int32_t sb = src_box_lists[l];
+            const int32_t s0 = box_src_starts[sb];
+            const int32_t ns = box_src_counts[sb];
+            float arf = 0.f, aif = 0.f;
+            for (int32_t sc = 0; sc < ns; sc += 32) {
+                const int nsc = min(32, ns - sc);
+                if (lane < nsc) {
+                    const int32_t s = s0 + sc + lane;
+                    const z2 q = strength[s];
+                    wb[lane].x = sources[s];
+                    wb[lane].y = sources[sstride + s];
+                    wb[lane].z = sources[2 * sstride + s];
+                    wb[lane].qr = q.x;
+                    wb[lane].qi = q.y;
+                }
+                __syncwarp();
+                if (active) {
+                    for (int j = ph; j < nsc; j += nph) {
+                        if (s0 + sc + j == self) continue;
+                        const HSrc sp = wb[j];
+                        if (MIXED) {
+                            const float dx = (float)(tx - sp.x);
+                            const float dy = (float)(ty - sp.y);
+                            const float dz = (float)(tz - sp.z);
+                            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                            const float ri = rsqrtf(r2);
+                            float sn, cs;
+                            sincosf(kf * (r2 * ri), &sn, &cs);
+                            const float wr = cs * ri, wi = sn * ri;
+                            const float qr = (float)sp.qr, qi = (float)sp.qi;
+                            arf = fmaf(qr, wr, fmaf(-qi, wi, arf));
+                            aif = fmaf(qr, wi, fmaf(qi, wr, aif));
+                        } else {
+                            const double dx = tx - sp.x, dy = ty - sp.y, dz = tz - sp.z;
+                            const double r2 = dx * dx + dy * dy + dz * dz;
+                            const double ri = rsqrt(r2);
+                            double sn, cs;
+                            sincos(k * (r2 * ri), &sn, &cs);
+                            const double wr = cs * ri, wi = sn * ri;
+                            ar = fma(sp.qr, wr, fma(-sp.qi, wi, ar));
+                            ai = fma(sp.qr, wi, fma(sp.qi, wr, ai));
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+            if (MIXED) {
+                ar += (double)arf;
+                ai += (double)aif;
+            }
+        }
+        for (int off = g; off < 32; off <<= 1) {
+            ar += __shfl_xor_sync(0xffffffffu, ar, off);
+            ai += __shfl_xor_sync(0xffffffffu, ai, off);
+        }
+        if (active && ph == 0) result[t] = zmk(scale * ar, scale * ai);
+    }
+}
+
+constexpr int HDIRECT_THREADS = 256;
+
+// all pairs, FP64 (sumpy/p2p.py:215-285)
+__global__ void __launch_bounds__(HDIRECT_THREADS)
+hp2p_direct_kernel(int64_t ntgt, const double *__restrict__ targets, int64_t tstride, int64_t nsrc,
+                   const double *__restrict__ sources, int64_t sstride,
+                   const z2 *__restrict__ strength, const int32_t *__restrict__ target_to_source,
+                   double k, double scale, z2 *__restrict__ result)
+{
+    __shared__ HSrc tile[HDIRECT_THREADS];
+    const int64_t t = (int64_t)blockIdx.x * HDIRECT_THREADS + threadIdx.x;
+    const bool active = t < ntgt;
+    double tx = 0, ty = 0, tz = 0;
+    int64_t self = -1;
+    if (active) {
+        tx = targets[t];
+        ty = targets[tstride + t];
+        tz = targets[2 * tstride + t];
+        if (target_to_source) self = target_to_source[t];
+    }
+    double ar = 0.0, ai = 0.0;
+    for (int64_t s0 = 0; s0 < nsrc; s0 += HDIRECT_THREADS) {
+        const int64_t s = s0 + threadIdx.x;
+        if (s < nsrc) {
+            const z2 q = strength[s];
+            tile[threadIdx.x] = HSrc{sources[s], sources[sstride + s], sources[2 * sstride + s],
+                                     q.x, q.y};
+        }
+        __syncthreads();
+        const int n = (int)min((int64_t)HDIRECT_THREADS, nsrc - s0);
+        if (active) {
+            for (int j = 0; j < n; ++j) {
+                if (s0 + j == self) continue;
+                const double dx = tx - tile[j].x, dy = ty - tile[j].y, dz = tz - tile[j].z;
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                const double ri = rsqrt(r2);
+                double sn, cs;
+                sincos(k * (r2 * ri), &sn, &cs);
+                const double wr = cs * ri, wi = sn * ri;
+                ar = fma(tile[j].qr, wr, fma(-tile[j].qi, wi, ar));
+                ai = fma(tile[j].qr, wi, fma(tile[j].qi, wr, ai));
+            }
+        }
+        __syncthreads();
+    }
+    if (active) result[t] = zmk(scale * ar, scale * ai);
+}
+
+// }}}
+
+// {{{ P2M
+
+constexpr int HP2M_THREADS = 128;
+constexpr int HP2M_CHUNK = 32;
+
+// full multipole cube -> compressed in place (transposed Helmholtz
+// projection, planes p..2 in turn; plane i-2 gathers from plane i)
+__device__ void h_compress_cube_block(z2 *cube, int p, double kappa)
+{
+    for (int i = p; i >= 2; --i) {
+        const int m = p - i + 2;
+        const int npairs = (m + 1) * (m + 2) / 2;
+        for (int t = threadIdx.x; t < npairs; t += blockDim.x) {
+            int J, K;
+            tri_pair(t, m, J, K);
+            z2 v = zmk(0.0, 0.0);
+            if (J >= 2) v = zadd(v, cube[cube_index(p, i, J - 2, K)]);
+            if (K >= 2) v = zadd(v, cube[cube_index(p, i, J, K - 2)]);
+            if (J + K <= p - i) v = zaxpy(kappa, cube[cube_index(p, i, J, K)], v);
+            z2 &o = cube[cube_index(p, i - 2, J, K)];
+            o = zmk(o.x - v.x, o.y - v.y);
+        }
+        __syncthreads();
+    }
+}
+
+// P2EFromSingleBox (sumpy/p2e.py:155-261; multipole.py:77-114)
+__global__ void __launch_bounds__(HP2M_THREADS)
+hp2m_kernel(int p, double rscale, double kappa, const int32_t *__restrict__ boxes,
+            const double *__restrict__ centers, int64_t cstride, const int32_t *__restrict__ bss,
+            const int32_t *__restrict__ bsc, const double *__restrict__ sources, int64_t sstride,
+            const z2 *__restrict__ q, int32_t base, z2 *__restrict__ out)
+{
+    extern __shared__ __align__(16) double sm[];
+    const int P1 = p + 1;
+    z2 *cube = reinterpret_cast<z2 *>(sm);                // P1^3
+    double *pw = reinterpret_cast<double *>(cube + P1 * P1 * P1);  // [CHUNK][3][P1]
+    z2 *qs = reinterpret_cast<z2 *>(pw + HP2M_CHUNK * 3 * P1);     // [CHUNK]
+
+    const int32_t b = boxes[blockIdx.x];
+    const double c[3] = {centers[b], centers[cstride + b], centers[2 * cstride + b]};
+    const int32_t s0 = bss[b], ns = bsc[b];
+    const int nfull = nfull_of(p);
+    const double rinv = 1.0 / rscale;
+
+    for (int t = threadIdx.x; t < P1 * P1 * P1; t += blockDim.x) cube[t] = zmk(0.0, 0.0);
+    __syncthreads();
+    for (int sc = 0; sc < ns; sc += HP2M_CHUNK) {
+        const int nsc = min(HP2M_CHUNK, ns - sc);
+        for (int t = threadIdx.x; t < HP2M_CHUNK * 3; t += blockDim.x) {
+            const int s = t / 3, d = t % 3;
+            double *w = pw + (s * 3 + d) * P1;
+            if (s < nsc) {
+                const double a = (c[d] - sources[d * sstride + s0 + sc + s]) * rinv;
+                w[0] = 1.0;
+                for (int kk = 1; kk <= p; ++kk) w[kk] = w[kk - 1] * a / kk;
+                if (d == 0) qs[s] = q[s0 + sc + s];
+            }
+        }
+        __syncthreads();
+        for (int f = threadIdx.x; f < nfull; f += blockDim.x) {
+            int i, j, kk;
+            full_mi(f, i, j, kk);
+            z2 acc = zmk(0.0, 0.0);
+            for (int s = 0; s < nsc; ++s)
+                acc = zaxpy(pw[(s * 3 + 0) * P1 + i] * pw[(s * 3 + 1) * P1 + j] *
+                                pw[(s * 3 + 2) * P1 + kk],
+                            qs[s], acc);
+            cube[cube_index(p, i, j, kk)] = zadd(cube[cube_index(p, i, j, kk)], acc);
+        }
+        __syncthreads();
+    }
+    h_compress_cube_block(cube, p, kappa);
+    const int n = ncoeff_of(p);
+    z2 *o = out + (int64_t)(b - base) * n;
+    for (int s = threadIdx.x; s < n; s += blockDim.x) {
+        int i, j, kk;
+        stored_mi(s, i, j, kk);
+        o[s] = cube[cube_index(p, i, j, kk)];
+    }
+}
+
+// }}}
+
+// {{{ M2M / L2L
+
+constexpr int HE2E_THREADS = 256;
+
+// E2EFromChildren (sumpy/e2e.py:866-978; multipole.py:159-407): the
+// children's stored coefficients in the parent's full slots times
+// (r_child/r_parent)^|mi|, shifted along axes 1, 2, 0 (all children of the
+// parent concurrently), summed, compressed with kappa_parent; accumulated.
+__global__ void __launch_bounds__(HE2E_THREADS)
+hm2m_kernel(int ps, int pt, double rsrc, double rtgt, double kappa_t,
+            const int32_t *__restrict__ boxes, const int32_t *__restrict__ child_ids,
+            int64_t child_stride, const double *__restrict__ centers, int64_t cstride,
+            int32_t sbase, const z2 *__restrict__ src, int32_t tbase, z2 *__restrict__ tgt)
+{
+    extern __shared__ __align__(16) double sm[];
+    const int P1 = pt + 1;
+    const int nfull = nfull_of(pt);
+    z2 *A = reinterpret_cast<z2 *>(sm);     // [8][nfull]
+    z2 *B = A + 8 * nfull;                  // [8][nfull]
+    double *pw = reinterpret_cast<double *>(B + 8 * nfull);        // [8][3][P1]
+    uint32_t *tab = reinterpret_cast<uint32_t *>(pw + 8 * 3 * P1);  // [nfull]
+    __shared__ int32_t kids[8];
+    __shared__ int nkids;
+
+    const int32_t b = boxes[blockIdx.x];
+    const int ns = ncoeff_of(ps), nt = ncoeff_of(pt);
+    const double ratio = rsrc / rtgt;
+    if (threadIdx.x == 0) {
+        int c = 0;
+        for (int slot = 0; slot < 8; ++slot) {
+            const int32_t ch = child_ids[slot * child_stride + b];
+            if (ch != 0) kids[c++] = ch;
+        }
+        nkids = c;
+    }
+    for (int f = threadIdx.x; f < nfull; f += blockDim.x) {
+        int i, j, k;
+        full_mi(f, i, j, k);
+        tab[f] = (uint32_t)i | ((uint32_t)j << 8) | ((uint32_t)k << 16);
+    }
+    __syncthreads();
+    const int nk = nkids;
+    for (int t = threadIdx.x; t < nk * 3; t += blockDim.x) {
+        const int c = t / 3, d = t % 3;
+        const int32_t ch = kids[c];
+        const double dd = (centers[d * cstride + b] - centers[d * cstride + ch]) / rtgt;
+        double *w = pw + (c * 3 + d) * P1;
+        w[0] = 1.0;
+        for (int q = 1; q <= pt; ++q) w[q] = w[q - 1] * dd / q;
+    }
+    for (int t = threadIdx.x; t < nk * nfull; t += blockDim.x) {
+        const int c = t / nfull, f = t % nfull;
+        const uint32_t e = tab[f];
+        const int i = e & 0xff, j = (e >> 8) & 0xff, k = e >> 16;
+        const int deg = i + j + k;
+        z2 v = zmk(0.0, 0.0);
+        if (i < 2 && deg <= ps)
+            v = zscal(ipow(ratio, deg), src[(int64_t)(kids[c] - sbase) * ns + stored_index(i, j, k)]);
+        A[c * nfull + f] = v;
+    }
+    __syncthreads();
+    const int axes[3] = {1, 2, 0};
+    z2 *in = A, *out = B;
+#pragma unroll 1
+    for (int a = 0; a < 3; ++a) {
+        const int d = axes[a];
+        for (int t = threadIdx.x; t < nk * nfull; t += blockDim.x) {
+            const int c = t / nfull, f = t % nfull;
+            const uint32_t e = tab[f];
+            int m[3] = {(int)(e & 0xff), (int)((e >> 8) & 0xff), (int)(e >> 16)};
+            const double *w = pw + (c * 3 + d) * P1;
+            const z2 *inc = in + c * nfull;
+            const int md = m[d];
+            z2 acc = zmk(0.0, 0.0);
+            for (int q = 0; q <= md; ++q) {
+                m[d] = q;
+                acc = zaxpy(w[md - q], inc[full_index(m[0], m[1], m[2])], acc);
+            }
+            out[c * nfull + f] = acc;
+        }
+        __syncthreads();
+        z2 *sw = in; in = out; out = sw;
+    }
+    z2 *accv = out;
+    for (int f = threadIdx.x; f < nfull; f += blockDim.x) {
+        z2 v = zmk(0.0, 0.0);
+        for (int c = 0; c < nk; ++c) v = zadd(v, in[c * nfull + f]);
+        accv[f] = v;
+    }
+    __syncthreads();
+    for (int i = pt; i >= 2; --i) {
+        const int m = pt - i + 2;
+        const int npairs = (m + 1) * (m + 2) / 2;
+        for (int t = threadIdx.x; t < npairs; t += blockDim.x) {
+            int J, K;
+            tri_pair(t, m, J, K);
+            z2 v = zmk(0.0, 0.0);
+            if (J >= 2) v = zadd(v, accv[full_index(i, J - 2, K)]);
+            if (K >= 2) v = zadd(v, accv[full_index(i, J, K - 2)]);
+            if (J + K <= pt - i) v = zaxpy(kappa_t, accv[full_index(i, J, K)], v);
+            z2 &o = accv[full_index(i - 2, J, K)];
+            o = zmk(o.x - v.x, o.y - v.y);
+        }
+        __syncthreads();
+    }
+    z2 *o = tgt + (int64_t)(b - tbase) * nt;
+    for (int s2 = threadIdx.x; s2 < nt; s2 += blockDim.x) {
+        int i, j, k;
+        stored_mi(s2, i, j, k);
+        o[s2] = zadd(o[s2], accv[full_index(i, j, k)]);
+    }
+}
+
+constexpr int HL2L_BOXES = 4;
+
+// E2EFromParent (sumpy/e2e.py:985-1083; local.py:346-464): parent local
+// decompressed with kappa_parent, Taylor-shifted along axes 0, 1, 2
+// (truncated at the parent's order), times (r_child/r_parent)^|mi|,
+// accumulated into the child; HL2L_BOXES children per CTA.
+__global__ void __launch_bounds__(HE2E_THREADS)
+hl2l_kernel(int ps, int pt, double rsrc, double rtgt, double kappa_s, int32_t nboxes,
+            const int32_t *__restrict__ boxes, const int32_t *__restrict__ parent_ids,
+            const double *__restrict__ centers, int64_t cstride, int32_t sbase,
+            const z2 *__restrict__ src, int32_t tbase, z2 *__restrict__ tgt)
+{
+    extern __shared__ __align__(16) double sm[];
+    const int P1 = ps + 1;
+    const int nfull = nfull_of(ps);
+    z2 *A = reinterpret_cast<z2 *>(sm);
+    z2 *B = A + HL2L_BOXES * nfull;
+    double *pw = reinterpret_cast<double *>(B + HL2L_BOXES * nfull);
+    uint32_t *tab = reinterpret_cast<uint32_t *>(pw + HL2L_BOXES * 3 * P1);
+    const int b0 = blockIdx.x * HL2L_BOXES;
+    const int nk = min(HL2L_BOXES, nboxes - b0);
+    const int ns = ncoeff_of(ps), nt = ncoeff_of(pt);
+
+    for (int f = threadIdx.x; f < nfull; f += blockDim.x) {
+        int i, j, k;
+        full_mi(f, i, j, k);
+        tab[f] = (uint32_t)i | ((uint32_t)j << 8) | ((uint32_t)k << 16);
+    }
+    for (int t = threadIdx.x; t < nk * 3; t += blockDim.x) {
+        const int c = t / 3, d = t % 3;
+        const int32_t b = boxes[b0 + c];
+        const int32_t par = parent_ids[b];
+        const double dd = (centers[d * cstride + b] - centers[d * cstride + par]) / rsrc;
+        double *w = pw + (c * 3 + d) * P1;
+        w[0] = 1.0;
+        for (int q = 1; q <= ps; ++q) w[q] = w[q - 1] * dd / q;
+    }
+    for (int t = threadIdx.x; t < nk * ns; t += blockDim.x) {
+        const int c = t / ns, s2 = t % ns;
+        const int32_t par = parent_ids[boxes[b0 + c]];
+        int i, j, k;
+        stored_mi(s2, i, j, k);
+        A[c * nfull + full_index(i, j, k)] = src[(int64_t)(par - sbase) * ns + s2];
+    }
+    __syncthreads();
+    for (int i = 2; i <= ps; ++i) {
+        const int m = ps - i;
+        const int npairs = (m + 1) * (m + 2) / 2;
+        for (int t = threadIdx.x; t < nk * npairs; t += blockDim.x) {
+            const int c = t / npairs;
+            int J, K;
+            tri_pair(t % npairs, m, J, K);
+            z2 *a = A + c * nfull;
+            const z2 u1 = a[full_index(i - 2, J + 2, K)], u2 = a[full_index(i - 2, J, K + 2)];
+            const z2 u0 = a[full_index(i - 2, J, K)];
+            a[full_index(i, J, K)] = zmk(-u1.x - u2.x - kappa_s * u0.x, -u1.y - u2.y - kappa_s * u0.y);
+        }
+        __syncthreads();
+    }
+    z2 *in = A, *out = B;
+#pragma unroll 1
+    for (int d = 0; d < 3; ++d) {
+        for (int t = threadIdx.x; t < nk * nfull; t += blockDim.x) {
+            const int c = t / nfull, f = t % nfull;
+            const uint32_t e = tab[f];
+            int m[3] = {(int)(e & 0xff), (int)((e >> 8) & 0xff), (int)(e >> 16)};
+            const int deg = m[0] + m[1] + m[2];
+            const double *w = pw + (c * 3 + d) * P1;
+            const z2 *inc = in + c * nfull;
+            const int md = m[d];
+            z2 acc = zmk(0.0, 0.0);
+            for (int q = 0; q <= ps - deg; ++q) {
+                m[d] = md + q;
+                acc = zaxpy(w[q], inc[full_index(m[0], m[1], m[2])], acc);
+            }
+            out[c * nfull + f] = acc;
+        }
+        __syncthreads();
+        z2 *sw = in; in = out; out = sw;
+    }
+    const double ratio = rtgt / rsrc;
+    for (int t = threadIdx.x; t < nk * nt; t += blockDim.x) {
+        const int c = t / nt, s2 = t % nt;
+        int i, j, k;
+        stored_mi(s2, i, j, k);
+        const int deg = i + j + k;
+        if (deg <= ps) {
+            z2 &o = tgt[(int64_t)(boxes[b0 + c] - tbase) * nt + s2];
+            o = zaxpy(ipow(ratio, deg), in[c * nfull + full_index(i, j, k)], o);
+        }
+    }
+}
+
+// }}}
+
+// {{{ L2P
+
+constexpr int HL2P_WARPS = 2;
+
+__device__ __forceinline__ z2 h_horner_cube(const z2 *cube, const double *inv, int p, double x,
+                                            double y, double z)
+{
+    z2 tot = zmk(0.0, 0.0);
+    for (int i = p; i >= 0; --i) {
+        z2 sy = zmk(0.0, 0.0);
+        for (int j = p - i; j >= 0; --j) {
+            z2 sz = zmk(0.0, 0.0);
+            const z2 *row = cube + cube_index(p, i, j, 0);
+            for (int k = p - i - j; k >= 0; --k) sz = zaxpy(z * inv[k + 1], sz, row[k]);
+            sy = zaxpy(y * inv[j + 1], sy, sz);
+        }
+        tot = zaxpy(x * inv[i + 1], tot, sy);
+    }
+    return tot;
+}
+
+// E2PFromSingleBox (sumpy/e2p.py:123-226; local.py:284-309): one warp per
+// leaf, decompressed cube in shared memory, nested Horner per target;
+// result assigned (times the kernel scaling).
+__global__ void __launch_bounds__(32 * HL2P_WARPS)
+hl2p_kernel(int p, double rscale, double kappa, int32_t nboxes, const int32_t *__restrict__ boxes,
+            const double *__restrict__ centers, int64_t cstride, int32_t sbase,
+            const z2 *__restrict__ src, const int32_t *__restrict__ bts,
+            const int32_t *__restrict__ btc, const double *__restrict__ targets, int64_t tstride,
+            double scale, z2 *__restrict__ result)
+{
+    extern __shared__ __align__(16) double sm[];
+    const int P1 = p + 1, C = P1 * P1 * P1;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ib = blockIdx.x * HL2P_WARPS + warp;
+    if (ib >= nboxes) return;
+    z2 *cube = reinterpret_cast<z2 *>(sm) + warp * C;
+    double *inv = reinterpret_cast<double *>(reinterpret_cast<z2 *>(sm) + HL2P_WARPS * C) +
+                  warp * (P1 + 1);
+
+    const int32_t b = boxes[ib];
+    const int n = ncoeff_of(p);
+    const z2 *cs = src + (int64_t)(b - sbase) * n;
+    for (int s = lane; s < n; s += 32) {
+        int i, j, k;
+        stored_mi(s, i, j, k);
+        cube[cube_index(p, i, j, k)] = cs[s];
+    }
+    for (int q = lane; q <= p + 1; q += 32) inv[q] = q ? 1.0 / q : 0.0;
+    __syncwarp();
+    for (int i = 2; i <= p; ++i) {
+        const int m = p - i;
+        const int npairs = (m + 1) * (m + 2) / 2;
+        for (int t = lane; t < npairs; t += 32) {
+            int J, K;
+            tri_pair(t, m, J, K);
+            const z2 u1 = cube[cube_index(p, i - 2, J + 2, K)];
+            const z2 u2 = cube[cube_index(p, i - 2, J, K + 2)];
+            const z2 u0 = cube[cube_index(p, i - 2, J, K)];
+            cube[cube_index(p, i, J, K)] =
+                zmk(-u1.x - u2.x - kappa * u0.x, -u1.y - u2.y - kappa * u0.y);
+        }
+        __syncwarp();
+    }
+    const double c[3] = {centers[b], centers[cstride + b], centers[2 * cstride + b]};
+    const double rinv = 1.0 / rscale;
+    const int32_t t0 = bts[b], nt = btc[b];
+    for (int32_t tt = lane; tt < nt; tt += 32) {
+        const int32_t t = t0 + tt;
+        const double x = (targets[t] - c[0]) * rinv;
+        const double y = (targets[tstride + t] - c[1]) * rinv;
+        const double z = (targets[2 * tstride + t] - c[2]) * rinv;
+        result[t] = zscal(scale, h_horner_cube(cube, inv, p, x, y, z));
+    }
+}
+
+// }}}
+
+// {{{ M2P / P2L (derivatives from the closed form)
+
+constexpr int HM2P_WARPS = 2;
+
+// E2PFromCSR (List 3; sumpy/e2p.py:233-343, multipole.py:131-157): one warp
+// per target box, lanes over its targets; per List-3 box the multipole is
+// staged in shared memory and each lane sums M[mi] D(mi)(t - c) over the
+// stored mi with its own tables (lane-strided in shared memory).
+// Accumulates into result.
+__global__ void __launch_bounds__(32 * HM2P_WARPS)
+hm2p_kernel(int p, double rscale, double k, int32_t ntgt_boxes,
+            const int32_t *__restrict__ target_boxes, const int32_t *__restrict__ src_starts,
+            const int32_t *__restrict__ src_lists, const double *__restrict__ centers,
+            int64_t cstride, int32_t sbase, const z2 *__restrict__ src,
+            const int32_t *__restrict__ bts, const int32_t *__restrict__ btc,
+            const double *__restrict__ targets, int64_t tstride, double scale,
+            z2 *__restrict__ result)
+{
+    extern __shared__ __align__(16) double sm[];
+    const int P1 = p + 1;
+    const int n = ncoeff_of(p);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ib = blockIdx.x * HM2P_WARPS + warp;
+    if (ib >= ntgt_boxes) return;
+    // per warp: M[n] z2, then lane tables N1, N2, RH, GR, GI: [P1][32] each
+    const int per_warp = 2 * n + 5 * P1 * 32;
+    double *base = sm + warp * per_warp;
+    z2 *M = reinterpret_cast<z2 *>(base);
+    double *N1 = base + 2 * n + lane;
+    double *N2 = N1 + P1 * 32;
+    double *RH = N2 + P1 * 32;
+    double *GR = RH + P1 * 32;
+    double *GI = GR + P1 * 32;
+
+    const int32_t tb = target_boxes[ib];
+    const int32_t t0 = bts[tb], nt = btc[tb];
+    const int32_t ls = src_starts[ib], le = src_starts[ib + 1];
+    for (int32_t tc = 0; tc < nt; tc += 32) {
+        const bool active = tc + lane < nt;
+        const int32_t t = t0 + tc + lane;
+        double tx = 0, ty = 0, tz = 0;
+        if (active) {
+            tx = targets[t];
+            ty = targets[tstride + t];
+            tz = targets[2 * tstride + t];
+        }
+        z2 acc = zmk(0.0, 0.0);
+        for (int32_t l = ls; l < le; ++l) {
+            const int32_t sb = src_lists[l];
+            __syncwarp();
+            for (int s = lane; s < n; s += 32) M[s] = src[(int64_t)(sb - sbase) * n + s];
+            __syncwarp();
+            if (!active) continue;
+            const double x0 = tx - centers[sb], x1 = ty - centers[cstride + sb],
+                         x2 = tz - centers[2 * cstride + sb];
+            const double r = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
+            const double ri = 1.0 / r;
+            const double n0 = x0 * ri, n1 = x1 * ri, n2 = x2 * ri;
+            const double rho = rscale * ri;
+            double a1 = 1.0, a2 = 1.0, ar = 1.0;
+            for (int e = 0; e <= p; ++e) {
+                N1[e * 32] = a1; N2[e * 32] = a2; RH[e * 32] = ar;
+                a1 *= n1; a2 *= n2; ar *= rho;
+            }
+            helm_gammas(r, k, p, GR, GI, 32);
+            int mi = 0;
+            for (int d = 0; d <= p; ++d) {
+                const double rd = RH[d * 32];
+                for (int i = 0; i <= min(1, d); ++i) {
+                    const double fi = rd * (i ? n0 : 1.0);
+                    for (int j = 0; j <= d - i; ++j, ++mi) {
+                        const z2 s = helm_mi_sum(i, j, d - i - j, N1, N2, GR, GI, 32);
+                        acc = zfma(M[mi], zscal(fi, s), acc);
+                    }
+                }
+            }
+        }
+        if (active) {
+            z2 &o = result[t];
+            o = zaxpy(scale, acc, o);
+        }
+    }
+}
+
+constexpr int HP2L_WARPS = 2;
+constexpr int HP2L_MAXU = (SUMPY_MAX_ORDER + 1) * (SUMPY_MAX_ORDER + 1) / 32 + 1;
+
+// P2EFromCSR (List 4; sumpy/p2e.py:268-388, local.py:225-271): one warp per
+// target box; the box's List-4 sources go 32 at a time: each lane writes the
+// tables of one source to shared memory (source-major), then each lane owns
+// the stored coefficients lane + 32 u and sums q_s D(mi)(c - s) over the
+// staged sources. Accumulates into the box's local.
+__global__ void __launch_bounds__(32 * HP2L_WARPS)
+hp2l_kernel(int p, double rscale, double k, int32_t ntgt_boxes,
+            const int32_t *__restrict__ target_boxes, const int32_t *__restrict__ src_starts,
+            const int32_t *__restrict__ src_lists, const double *__restrict__ centers,
+            int64_t cstride, const int32_t *__restrict__ bss, const int32_t *__restrict__ bsc,
+            const double *__restrict__ sources, int64_t sstride, const z2 *__restrict__ q,
+            int32_t tbase, z2 *__restrict__ tgt)
+{
+    extern __shared__ __align__(16) double sm[];
+    const int P1 = p + 1;
+    const int n = ncoeff_of(p);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ib = blockIdx.x * HP2L_WARPS + warp;
+    if (ib >= ntgt_boxes) return;
+    // per source: N1, N2, RH, GR, GI [P1] each, then n0, qr, qi
+    const int per_src = 5 * P1 + 3;
+    double *base = sm + warp * 32 * per_src;
+
+    const int32_t tb = target_boxes[ib];
+    const double c[3] = {centers[tb], centers[cstride + tb], centers[2 * cstride + tb]};
+    z2 acc[HP2L_MAXU];
+#pragma unroll
+    for (int u = 0; u < HP2L_MAXU; ++u) acc[u] = zmk(0.0, 0.0);
+
+    const int32_t ls = src_starts[ib], le = src_starts[ib + 1];
+    for (int32_t l = ls; l < le; ++l) {
+        const int32_t sb = src_lists[l];
+        const int32_t s0 = bss[sb], ns = bsc[sb];
+        for (int32_t sc = 0; sc < ns; sc += 32) {
+            const int nsc = min(32, ns - sc);
+            __syncwarp();
+            if (lane < nsc) {
+                const int32_t s = s0 + sc + lane;
+                double *T = base + lane * per_src;
+                const double x0 = c[0] - sources[s], x1 = c[1] - sources[sstride + s],
+                             x2 = c[2] - sources[2 * sstride + s];
+                const double r = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
+                const double ri = 1.0 / r;
+                const double n1 = x1 * ri, n2 = x2 * ri, rho = rscale * ri;
+                double a1 = 1.0, a2 = 1.0, ar = 1.0;
+                for (int e = 0; e <= p; ++e) {
+                    T[e] = a1; T[P1 + e] = a2; T[2 * P1 + e] = ar;
+                    a1 *= n1; a2 *= n2; ar *= rho;
+                }
+                helm_gammas(r, k, p, T + 3 * P1, T + 4 * P1, 1);
+                const z2 qs = q[s];
+                T[5 * P1] = x0 * ri;
+                T[5 * P1 + 1] = qs.x;
+                T[5 * P1 + 2] = qs.y;
+            }
+            __syncwarp();
+#pragma unroll
+            for (int u = 0; u < HP2L_MAXU; ++u) {
+                const int mi = lane + 32 * u;
+                if (mi >= n) break;
+                int i, j, l2;
+                stored_mi(mi, i, j, l2);
+                const int d = i + j + l2;
+                z2 a = acc[u];
+                for (int s = 0; s < nsc; ++s) {
+                    const double *T = base + s * per_src;
+                    const z2 sum = helm_mi_sum(i, j, l2, T, T + P1, T + 3 * P1, T + 4 * P1, 1);
+                    const double f = T[2 * P1 + d] * (i ? T[5 * P1] : 1.0);
+                    a = zfma(zmk(T[5 * P1 + 1], T[5 * P1 + 2]), zscal(f, sum), a);
+                }
+                acc[u] = a;
+            }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < HP2L_MAXU; ++u) {
+        const int mi = lane + 32 * u;
+        if (mi >= n) break;
+        z2 &o = tgt[(int64_t)(tb - tbase) * n + mi];
+        o = zadd(o, acc[u]);
+    }
+}
+
+// }}}
+
+}  // namespace
+}  // namespace sumpy
+
+using namespace sumpy;
+
+namespace {
+
+inline const z2 *cz(const double *p) { return reinterpret_cast<const z2 *>(p); }
+inline z2 *mz(double *p) { return reinterpret_cast<z2 *>(p); }
+
+template <bool MIXED>
+int launch_hp2p(int32_t ntgt_boxes, const int32_t *target_boxes, const int32_t *ss,
+                const int32_t *sl, const int32_t *bss, const int32_t *bsc, const int32_t *bts,
+                const int32_t *btc, const double *sources, int64_t sstride, double k,
+                const double *strength, const double *targets, int64_t tstride,
+                const int32_t *tts, double scale, double *result, void *stream)
+{
+    if (ntgt_boxes < 0) return bad_arg("helmholtz p2p: ntgt_boxes < 0");
+    if (ntgt_boxes == 0) return SUMPY_OK;
+    if (!target_boxes || !ss || !sl || !bss || !bsc || !bts || !btc || !sources || !strength ||
+        !targets || !result)
+        return bad_arg("helmholtz p2p: null pointer argument");
+    const unsigned blocks = (unsigned)((ntgt_boxes + HP2P_WARPS - 1) / HP2P_WARPS);
+    hp2p_csr_kernel<MIXED><<<blocks, 32 * HP2P_WARPS, 0, as_stream(stream)>>>(
+        ntgt_boxes, target_boxes, ss, sl, bss, bsc, bts, btc, sources, sstride, cz(strength),
+        targets, tstride, tts, k, scale, mz(result));
+    return check_launch("hp2p_csr_kernel");
+}
+
+}  // namespace
+
+extern "C" {
+
+int sumpy_helmholtz_p2p_from_csr_f64(int32_t ntgt_boxes, const int32_t *target_boxes,
+                                     const int32_t *source_box_starts,
+                                     const int32_t *source_box_lists,
+                                     const int32_t *box_source_starts,
+                                     const int32_t *box_source_counts_nonchild,
+                                     const int32_t *box_target_starts,
+                                     const int32_t *box_target_counts_nonchild,
+                                     const double *sources, int64_t source_stride, double k,
+                                     const double *strength, const double *targets,
+                                     int64_t target_stride, const int32_t *target_to_source,
+                                     double scale, double *result, void *stream)
+{
+    return launch_hp2p<false>(ntgt_boxes, target_boxes, source_box_starts, source_box_lists,
+                              box_source_starts, box_source_counts_nonchild, box_target_starts,
+                              box_target_counts_nonchild, sources, source_stride, k, strength,
+                              targets, target_stride, target_to_source, scale, result, stream);
+}
+
+int sumpy_helmholtz_p2p_from_csr_mixed(int32_t ntgt_boxes, const int32_t *target_boxes,
+                                       const int32_t *source_box_starts,
+                                       const int32_t *source_box_lists,
+                                       const int32_t *box_source_starts,
+                                       const int32_t *box_source_counts_nonchild,
+                                       const int32_t *box_target_starts,
+                                       const int32_t *box_target_counts_nonchild,
+                                       const double *sources, int64_t source_stride, double k,
+                                       const double *strength, const double *targets,
+                                       int64_t target_stride, const int32_t *target_to_source,
+                                       double scale, double *result, void *stream)
+{
+    return launch_hp2p<true>(ntgt_boxes, target_boxes, source_box_starts, source_box_lists,
+                             box_source_starts, box_source_counts_nonchild, box_target_starts,
+                             box_target_counts_nonchild, sources, source_stride, k, strength,
+                             targets, target_stride, target_to_source, scale, result, stream);
+}
+
+int sumpy_helmholtz_p2p_direct_f64(int64_t ntargets, const double *targets, int64_t target_stride,
+                                   int64_t nsources, const double *sources,
+                                   int64_t source_stride, double k, const double *strength,
+                                   const int32_t *target_to_source, double scale, double *result,
+                                   void *stream)
+{
+    if (ntargets < 0 || nsources < 0) return bad_arg("helmholtz p2p_direct: negative size");
+    if (ntargets == 0) return SUMPY_OK;
+    if (!targets || !result || (nsources > 0 && (!sources || !strength)))
+        return bad_arg("helmholtz p2p_direct: null pointer argument");
+    const unsigned blocks = (unsigned)((ntargets + HDIRECT_THREADS - 1) / HDIRECT_THREADS);
+    hp2p_direct_kernel<<<blocks, HDIRECT_THREADS, 0, as_stream(stream)>>>(
+        ntargets, targets, target_stride, nsources, sources, source_stride, cz(strength),
+        target_to_source, k, scale, mz(result));
+    return check_launch("hp2p_direct_kernel");
+}
+
+int sumpy_helmholtz_p2e_from_single_box_f64(int order, double rscale, double k,
+                                            int32_t nsrc_boxes, const int32_t *source_boxes,
+                                            const double *centers, int64_t center_stride,
+                                            const int32_t *box_source_starts,
+                                            const int32_t *box_source_counts_nonchild,
+                                            const double *sources, int64_t source_stride,
+                                            const double *strength, int32_t tgt_base_ibox,
+                                            double *tgt_expansions, void *stream)
+{
+    if (!order_ok(order)) { set_last_error("helmholtz p2m: unsupported order"); return SUMPY_EUNSUPPORTED; }
+    if (nsrc_boxes < 0) return bad_arg("helmholtz p2m: nsrc_boxes < 0");
+    if (nsrc_boxes == 0) return SUMPY_OK;
+    if (!source_boxes || !centers || !box_source_starts || !box_source_counts_nonchild ||
+        !sources || !strength || !tgt_expansions)
+        return bad_arg("helmholtz p2m: null pointer argument");
+    const int P1 = order + 1;
+    const size_t smem = sizeof(z2) * P1 * P1 * P1 + sizeof(double) * HP2M_CHUNK * 3 * P1 +
+                        sizeof(z2) * HP2M_CHUNK;
+    int rc = prepare_smem(hp2m_kernel, smem);
+    if (rc) return rc;
+    hp2m_kernel<<<nsrc_boxes, HP2M_THREADS, smem, as_stream(stream)>>>(
+        order, rscale, k * k * rscale * rscale, source_boxes, centers, center_stride,
+        box_source_starts, box_source_counts_nonchild, sources, source_stride, cz(strength),
+        tgt_base_ibox, mz(tgt_expansions));
+    return check_launch("hp2m_kernel");
+}
+
+int sumpy_helmholtz_e2e_from_children_f64(int src_order, int tgt_order, double src_rscale,
+                                          double tgt_rscale, double k, int32_t ntgt_boxes,
+                                          const int32_t *target_boxes,
+                                          const int32_t *box_child_ids, int64_t child_stride,
+                                          const double *centers, int64_t center_stride,
+                                          int32_t src_base_ibox, const double *src_expansions,
+                                          int32_t tgt_base_ibox, double *tgt_expansions,
+                                          void *stream)
+{
+    if (!order_ok(src_order) || !order_ok(tgt_order)) {
+        set_last_error("helmholtz m2m: unsupported order");
+        return SUMPY_EUNSUPPORTED;
+    }
+    if (ntgt_boxes < 0) return bad_arg("helmholtz m2m: ntgt_boxes < 0");
+    if (ntgt_boxes == 0) return SUMPY_OK;
+    if (!target_boxes || !box_child_ids || !centers || !src_expansions || !tgt_expansions)
+        return bad_arg("helmholtz m2m: null pointer argument");
+    const int nfull = (tgt_order + 1) * (tgt_order + 2) * (tgt_order + 3) / 6;
+    const size_t smem = sizeof(z2) * 16 * nfull + sizeof(double) * 8 * 3 * (tgt_order + 1) +
+                        sizeof(uint32_t) * nfull;
+    int rc = prepare_smem(hm2m_kernel, smem);
+    if (rc) return rc;
+    hm2m_kernel<<<ntgt_boxes, HE2E_THREADS, smem, as_stream(stream)>>>(
+        src_order, tgt_order, src_rscale, tgt_rscale, k * k * tgt_rscale * tgt_rscale,
+        target_boxes, box_child_ids, child_stride, centers, center_stride, src_base_ibox,
+        cz(src_expansions), tgt_base_ibox, mz(tgt_expansions));
+    return check_launch("hm2m_kernel");
+}
+
+int sumpy_helmholtz_e2e_from_parent_f64(int src_order, int tgt_order, double src_rscale,
+                                        double tgt_rscale, double k, int32_t ntgt_boxes,
+                                        const int32_t *target_boxes, const int32_t *box_parent_ids,
+                                        const double *centers, int64_t center_stride,
+                                        int32_t src_base_ibox, const double *src_expansions,
+                                        int32_t tgt_base_ibox, double *tgt_expansions,
+                                        void *stream)
+{
+    if (!order_ok(src_order) || !order_ok(tgt_order)) {
+        set_last_error("helmholtz l2l: unsupported order");
+        return SUMPY_EUNSUPPORTED;
+    }
+    if (ntgt_boxes < 0) return bad_arg("helmholtz l2l: ntgt_boxes < 0");
+    if (ntgt_boxes == 0) return SUMPY_OK;
+    if (!target_boxes || !box_parent_ids || !centers || !src_expansions || !tgt_expansions)
+        return bad_arg("helmholtz l2l: null pointer argument");
+    const int nfull = (src_order + 1) * (src_order + 2) * (src_order + 3) / 6;
+    const size_t smem = sizeof(z2) * 2 * HL2L_BOXES * nfull +
+                        sizeof(double) * HL2L_BOXES * 3 * (src_order + 1) + sizeof(uint32_t) * nfull;
+    int rc = prepare_smem(hl2l_kernel, smem);
+    if (rc) return rc;
+    const unsigned blocks = (unsigned)((ntgt_boxes + HL2L_BOXES - 1) / HL2L_BOXES);
+    hl2l_kernel<<<blocks, HE2E_THREADS, smem, as_stream(stream)>>>(
+        src_order, tgt_order, src_rscale, tgt_rscale, k * k * src_rscale * src_rscale, ntgt_boxes,
+        target_boxes, box_parent_ids, centers, center_stride, src_base_ibox, cz(src_expansions),
+        tgt_base_ibox, mz(tgt_expansions));
+    return check_launch("hl2l_kernel");
+}
+
+int sumpy_helmholtz_e2p_from_single_box_f64(int order, double rscale, double k,
+                                            int32_t ntgt_boxes, const int32_t *target_boxes,
+                                            const double *centers, int64_t center_stride,
+                                            int32_t src_base_ibox, const double *src_expansions,
+                                            const int32_t *box_target_starts,
+                                            const int32_t *box_target_counts_nonchild,
+                                            const double *targets, int64_t target_stride,
+                                            double scale, double *result, void *stream)
+{
+    if (!order_ok(order)) { set_last_error("helmholtz l2p: unsupported order"); return SUMPY_EUNSUPPORTED; }
+    if (ntgt_boxes < 0) return bad_arg("helmholtz l2p: ntgt_boxes < 0");
+    if (ntgt_boxes == 0) return SUMPY_OK;
+    if (!target_boxes || !centers || !src_expansions || !box_target_starts ||
+        !box_target_counts_nonchild || !targets || !result)
+        return bad_arg("helmholtz l2p: null pointer argument");
+    const int P1 = order + 1;
+    const size_t smem = (sizeof(z2) * P1 * P1 * P1 + sizeof(double) * (P1 + 1)) * HL2P_WARPS;
+    int rc = prepare_smem(hl2p_kernel, smem);
+    if (rc) return rc;
+    const unsigned blocks = (unsigned)((ntgt_boxes + HL2P_WARPS - 1) / HL2P_WARPS);
+    hl2p_kernel<<<blocks, 32 * HL2P_WARPS, smem, as_stream(stream)>>>(
+        order, rscale, k * k * rscale * rscale, ntgt_boxes, target_boxes, centers, center_stride,
+        src_base_ibox, cz(src_expansions), box_target_starts, box_target_counts_nonchild, targets,
+        target_stride, scale, mz(result));
+    return check_launch("hl2p_kernel");
+}
+
+int sumpy_helmholtz_e2p_from_csr_f64(int order, double rscale, double k, int32_t ntgt_boxes,
+                                     const int32_t *target_boxes, const int32_t *source_box_starts,
+                                     const int32_t *source_box_lists, const double *centers,
+                                     int64_t center_stride, int32_t src_base_ibox,
+                                     const double *src_expansions,
+                                     const int32_t *box_target_starts,
+                                     const int32_t *box_target_counts_nonchild,
+                                     const double *targets, int64_t target_stride, double scale,
+                                     double *result, void *stream)
+{
+    if (!order_ok(order)) { set_last_error("helmholtz m2p: unsupported order"); return SUMPY_EUNSUPPORTED; }
+    if (ntgt_boxes < 0) return bad_arg("helmholtz m2p: ntgt_boxes < 0");
+    if (ntgt_boxes == 0) return SUMPY_OK;
+    if (!target_boxes || !source_box_starts || !source_box_lists || !centers ||
+        !src_expansions || !box_target_starts || !box_target_counts_nonchild || !targets ||
+        !result)
+        return bad_arg("helmholtz m2p: null pointer argument");
+    const int P1 = order + 1;
+    const size_t smem = sizeof(double) * HM2P_WARPS * (2 * ncoeff_of(order) + 5 * P1 * 32);
+    int rc = prepare_smem(hm2p_kernel, smem);
+    if (rc) return rc;
+    const unsigned blocks = (unsigned)((ntgt_boxes + HM2P_WARPS - 1) / HM2P_WARPS);
+    hm2p_kernel<<<blocks, 32 * HM2P_WARPS, smem, as_stream(stream)>>>(
+        order, rscale, k, ntgt_boxes, target_boxes, source_box_starts, source_box_lists, centers,
+        center_stride, src_base_ibox, cz(src_expansions), box_target_starts,
+        box_target_counts_nonchild, targets, target_stride, scale, mz(result));
+    return check_launch("hm2p_kernel");
+}
+
+int sumpy_helmholtz_p2e_from_csr_f64(int order, double rscale, double k, int32_t ntgt_boxes,
+                                     const int32_t *target_boxes, const int32_t *source_box_starts,
+                                     const int32_t *source_box_lists, const double *centers,
+                                     int64_t center_stride, const int32_t *box_source_starts,
+                                     const int32_t *box_source_counts_nonchild,
+                                     const double *sources, int64_t source_stride,
+                                     const double *strength, int32_t tgt_base_ibox,
+                                     double *tgt_expansions, void *stream)
+{
+    if (!order_ok(order)) { set_last_error("helmholtz p2l: unsupported order"); return SUMPY_EUNSUPPORTED; }
+    if (ntgt_boxes < 0) return bad_arg("helmholtz p2l: ntgt_boxes < 0");
+    if (ntgt_boxes == 0) return SUMPY_OK;
+    if (!target_boxes || !source_box_starts || !source_box_lists || !centers ||
+        !box_source_starts || !box_source_counts_nonchild || !sources || !strength ||
+        !tgt_expansions)
+        return bad_arg("helmholtz p2l: null pointer argument");
+    const int P1 = order + 1;
+    const size_t smem = sizeof(double) * HP2L_WARPS * 32 * (5 * P1 + 3);
+    int rc = prepare_smem(hp2l_kernel, smem);
+    if (rc) return rc;
+    const unsigned blocks = (unsigned)((ntgt_boxes + HP2L_WARPS - 1) / HP2L_WARPS);
+    hp2l_kernel<<<blocks, 32 * HP2L_WARPS, smem, as_stream(stream)>>>(
+        order, rscale, k, ntgt_boxes, target_boxes, source_box_starts, source_box_lists, centers,
+        center_stride, box_source_starts, box_source_counts_nonchild, sources, source_stride,
+        cz(strength), tgt_base_ibox, mz(tgt_expansions));
+    return check_launch("hp2l_kernel");
+}
+
+}  // extern "C"

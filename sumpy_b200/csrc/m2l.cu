@@ -160,26 +160,21 @@ m2l_f64_kernel(int n, const int32_t *__restrict__ item_tile, const int32_t *__re
 
 using namespace sumpy;
 
-extern "C" {
-
-int sumpy_m2l_translation_classes_f64(
-    int order, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
+// n = real coefficients per expansion row (ncoeff, or 2 ncoeff for complex
+// data as interleaved (re, im) with real-embedded operators).
+static int m2l_f64_launch(
+    int n, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
     const int32_t *item_group_end, int32_t tile_width, const int32_t *tile_targets,
     const double *tile_scale, const int32_t *group_class, const int32_t *group_sources,
     int32_t nclasses, const double *class_matrices, int32_t src_base_ibox,
     const double *src_expansions, int32_t tgt_base_ibox, double *tgt_expansions, void *stream)
 {
-    if (order < 0 || order > SUMPY_MAX_ORDER) {
-        set_last_error("m2l: unsupported order");
-        return SUMPY_EUNSUPPORTED;
-    }
     if (tile_width != TW) return bad_arg("m2l: tile_width must be 64");
     if (nitems < 0 || nclasses < 0) return bad_arg("m2l: negative size");
     if (nitems == 0) return SUMPY_OK;
     if (!item_tile || !item_group_begin || !item_group_end || !tile_targets || !tile_scale ||
         !group_class || !group_sources || !class_matrices || !src_expansions || !tgt_expansions)
         return bad_arg("m2l: null pointer argument");
-    const int n = ncoeff_of(order);
     cudaStream_t st = as_stream(stream);
     if (n <= 64) {
         dim3 grid(nitems, 1);
@@ -195,6 +190,42 @@ int sumpy_m2l_translation_classes_f64(
                                                   src_expansions, tgt_base_ibox, tgt_expansions);
     }
     return check_launch("m2l_f64_kernel");
+}
+
+extern "C" {
+
+int sumpy_m2l_translation_classes_f64(
+    int order, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
+    const int32_t *item_group_end, int32_t tile_width, const int32_t *tile_targets,
+    const double *tile_scale, const int32_t *group_class, const int32_t *group_sources,
+    int32_t nclasses, const double *class_matrices, int32_t src_base_ibox,
+    const double *src_expansions, int32_t tgt_base_ibox, double *tgt_expansions, void *stream)
+{
+    if (order < 0 || order > SUMPY_MAX_ORDER) {
+        set_last_error("m2l: unsupported order");
+        return SUMPY_EUNSUPPORTED;
+    }
+    return m2l_f64_launch(ncoeff_of(order), nitems, item_tile, item_group_begin, item_group_end,
+                          tile_width, tile_targets, tile_scale, group_class, group_sources,
+                          nclasses, class_matrices, src_base_ibox, src_expansions, tgt_base_ibox,
+                          tgt_expansions, stream);
+}
+
+int sumpy_helmholtz_m2l_translation_classes_f64(
+    int order, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
+    const int32_t *item_group_end, int32_t tile_width, const int32_t *tile_targets,
+    const double *tile_scale, const int32_t *group_class, const int32_t *group_sources,
+    int32_t nclasses, const double *class_matrices, int32_t src_base_ibox,
+    const double *src_expansions, int32_t tgt_base_ibox, double *tgt_expansions, void *stream)
+{
+    if (order < 0 || order > SUMPY_MAX_ORDER) {
+        set_last_error("helmholtz m2l: unsupported order");
+        return SUMPY_EUNSUPPORTED;
+    }
+    return m2l_f64_launch(2 * ncoeff_of(order), nitems, item_tile, item_group_begin,
+                          item_group_end, tile_width, tile_targets, tile_scale, group_class,
+                          group_sources, nclasses, class_matrices, src_base_ibox, src_expansions,
+                          tgt_base_ibox, tgt_expansions, stream);
 }
 
 }  // extern "C"

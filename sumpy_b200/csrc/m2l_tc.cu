@@ -460,19 +460,19 @@ static bool make_map(CUtensorMap *m, const float *ptr, int rank, const uint64_t 
     return r == CUDA_SUCCESS;
 }
 
-int sumpy_m2l_translation_classes_tf32x3(
-    int order, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
+}  // extern "C"
+
+// n = real coefficients per expansion row: ncoeff for real data, 2 ncoeff for
+// complex data stored as interleaved (re, im) with the real embedding of the
+// complex operators.
+static int m2l_tf32x3_launch(
+    int n, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
     const int32_t *item_group_end, int32_t tile_width, const int32_t *tile_targets,
     const double *tile_scale, const int32_t *group_class, const int32_t *group_sources,
     int32_t nclasses, const float *mats_hi, const float *mats_lo, int32_t rows_pad, int32_t k_pad,
     int32_t src_nrows, int32_t src_base_ibox, const float *src_hi, const float *src_lo,
     int32_t tgt_base_ibox, double *tgt_expansions, int32_t *status, void *stream)
 {
-    if (order < 0 || order > SUMPY_MAX_ORDER) {
-        set_last_error("m2l_tf32x3: unsupported order");
-        return SUMPY_EUNSUPPORTED;
-    }
-    const int n = ncoeff_of(order);
     if (tile_width != TC_TW) return bad_arg("m2l_tf32x3: tile_width must be 128");
     if (rows_pad < n || rows_pad % TC_M) return bad_arg("m2l_tf32x3: rows_pad must be a multiple of 128 >= ncoeff");
     if (k_pad < n || k_pad % TC_KC) return bad_arg("m2l_tf32x3: k_pad must be a multiple of 32 >= ncoeff");
@@ -514,6 +514,46 @@ int sumpy_m2l_translation_classes_tf32x3(
     dim3 grid(nitems, rows_pad / TC_M);
     m2l_tf32x3_kernel<<<grid, TC_THREADS, TC_SMEM, as_stream(stream)>>>(a, ma_hi, ma_lo);
     return check_launch("m2l_tf32x3_kernel");
+}
+
+extern "C" {
+
+int sumpy_m2l_translation_classes_tf32x3(
+    int order, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
+    const int32_t *item_group_end, int32_t tile_width, const int32_t *tile_targets,
+    const double *tile_scale, const int32_t *group_class, const int32_t *group_sources,
+    int32_t nclasses, const float *mats_hi, const float *mats_lo, int32_t rows_pad, int32_t k_pad,
+    int32_t src_nrows, int32_t src_base_ibox, const float *src_hi, const float *src_lo,
+    int32_t tgt_base_ibox, double *tgt_expansions, int32_t *status, void *stream)
+{
+    if (order < 0 || order > SUMPY_MAX_ORDER) {
+        set_last_error("m2l_tf32x3: unsupported order");
+        return SUMPY_EUNSUPPORTED;
+    }
+    return m2l_tf32x3_launch(ncoeff_of(order), nitems, item_tile, item_group_begin,
+                             item_group_end, tile_width, tile_targets, tile_scale, group_class,
+                             group_sources, nclasses, mats_hi, mats_lo, rows_pad, k_pad,
+                             src_nrows, src_base_ibox, src_hi, src_lo, tgt_base_ibox,
+                             tgt_expansions, status, stream);
+}
+
+int sumpy_helmholtz_m2l_translation_classes_tf32x3(
+    int order, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
+    const int32_t *item_group_end, int32_t tile_width, const int32_t *tile_targets,
+    const double *tile_scale, const int32_t *group_class, const int32_t *group_sources,
+    int32_t nclasses, const float *mats_hi, const float *mats_lo, int32_t rows_pad, int32_t k_pad,
+    int32_t src_nrows, int32_t src_base_ibox, const float *src_hi, const float *src_lo,
+    int32_t tgt_base_ibox, double *tgt_expansions, int32_t *status, void *stream)
+{
+    if (order < 0 || order > SUMPY_MAX_ORDER) {
+        set_last_error("helmholtz m2l_tf32x3: unsupported order");
+        return SUMPY_EUNSUPPORTED;
+    }
+    return m2l_tf32x3_launch(2 * ncoeff_of(order), nitems, item_tile, item_group_begin,
+                             item_group_end, tile_width, tile_targets, tile_scale, group_class,
+                             group_sources, nclasses, mats_hi, mats_lo, rows_pad, k_pad,
+                             src_nrows, src_base_ibox, src_hi, src_lo, tgt_base_ibox,
+                             tgt_expansions, status, stream);
 }
 
 // ---------------------------------------------------------------------------

@@ -6,9 +6,11 @@ Mirrors the parts of sumpy's expansion classes the FMM path needs:
 multipole.py:416-419, local.py:512-515) -- their coefficient identifiers
 and lengths -- plus the dense per-class M2L operators the CUDA GEMM applies.
 
-Coefficient sets (3D Laplace, sumpy/expansion/__init__.py:563-886): the
-full set is every multi-index with |mi| <= p sorted by (|mi|, mi0, mi1, mi2);
-the stored set keeps mi0 < 2, (p+1)^2 of them, in the same order.
+Coefficient sets (3D Laplace and Helmholtz, sumpy/expansion/__init__.py:563-886):
+the full set is every multi-index with |mi| <= p sorted by (|mi|, mi0, mi1, mi2);
+the stored set keeps mi0 < 2, (p+1)^2 of them, in the same order. The
+projection that restores the others is u_mi = -u_{mi-2e0+2e1} -
+u_{mi-2e0+2e2} - k^2 rscale^2 u_{mi-2e0} (k = 0 for Laplace).
 """
 from __future__ import annotations
 
@@ -18,7 +20,7 @@ from typing import Any
 
 import numpy as np
 
-from sumpy_b200.kernel import LaplaceKernel
+from sumpy_b200.kernel import HelmholtzKernel, LaplaceKernel
 
 
 # {{{ index sets
@@ -52,8 +54,9 @@ class _VolumeTaylorBase:
     use_rscale: bool | None = None
 
     def __post_init__(self):
-        if not isinstance(self.kernel, LaplaceKernel):
-            raise NotImplementedError("only LaplaceKernel(3) expansions are implemented")
+        if not isinstance(self.kernel, (LaplaceKernel, HelmholtzKernel)):
+            raise NotImplementedError(
+                "only LaplaceKernel(3) and HelmholtzKernel(3) expansions are implemented")
         if not 0 <= self.order <= 16:
             raise ValueError(f"order must be in [0, 16], got {self.order}")
         if self.use_rscale is False:
@@ -170,5 +173,101 @@ def m2l_class_matrices(order, vectors, src_rscale, tgt_rscale):
     deg_t = ids.sum(axis=1)
     T = T * (ratio ** deg_t)[:, None, None]
     return np.ascontiguousarray(np.moveaxis(T, -1, 0))   # [c, t, s]
+
+# }}}
+
+
+# {{{ Helmholtz derivatives and M2L operators
+
+def helmholtz_derivatives(vecs, rscale, k, maxdeg, maxi0=1):
+    """Scaled derivatives ``rscale^|mi| d^mi (exp(i k r)/r)`` at points
+    ``vecs`` (shape (3, m)) for mi0 <= maxi0, |mi| <= maxdeg, as a complex
+    array ``D[i, j, l, m]``.
+
+    The recursion of ``RadialDerivativeTaker.diff`` with the Helmholtz base
+    functions of ``HelmholtzDerivativeTaker.diff``
+    (sumpy/derivative_taker.py:296-389), vectorised over points: with
+    g_q = ((1/r) d/dr)^q G, D(mi, q) = x_a rs D(mi - e_a, q + 1) for the first
+    axis a with mi_a == 1, else (mi_a - 1) rs^2 D(mi - 2e_a, q + 1) +
+    x_a rs D(mi - e_a, q + 1) for the first axis with mi_a >= 2;
+    D(0, q) = g_q, g_0 = e^{ikr}/r, g_1 = (ikr - 1) e^{ikr}/r^3,
+    g_q = (-(2q - 1) g_{q-1} - k^2 g_{q-2}) / r^2.
+    """
+    x = np.asarray(vecs, dtype=np.float64)
+    m = x.shape[1]
+    rs = float(rscale)
+    r2 = (x * x).sum(axis=0)
+    r = np.sqrt(r2)
+    eikr = np.exp(1j * k * r)
+    M = maxdeg
+    E = {}
+    g = []
+    for q in range(M + 1):
+        if q == 0:
+            v = eikr / r
+        elif q == 1:
+            v = (1j * k * r - 1.0) * eikr / (r2 * r)
+        else:
+            v = (-(2 * q - 1) * g[q - 1] - k * k * g[q - 2]) / r2
+        g.append(v)
+        E[(0, 0, 0, q)] = v
+    for deg in range(1, M + 1):
+        for i in range(min(maxi0, deg) + 1):
+            for j in range(deg - i + 1):
+                l = deg - i - j
+                mi = (i, j, l)
+                if 1 in mi:
+                    ax, two = mi.index(1), False
+                else:
+                    ax, two = next(a for a in range(3) if mi[a] >= 2), True
+                m1 = list(mi); m1[ax] -= 1
+                m2 = list(mi); m2[ax] -= 2
+                for q in range(M - deg + 1):
+                    v = x[ax] * rs * E[(*m1, q + 1)]
+                    if two:
+                        v = v + (mi[ax] - 1) * rs * rs * E[(*m2, q + 1)]
+                    E[(i, j, l, q)] = v
+    D = np.zeros((maxi0 + 1, M + 1, M + 1, m), dtype=np.complex128)
+    for (i, j, l, q), v in E.items():
+        if q == 0:
+            D[i, j, l] = v
+    return D
+
+
+def helmholtz_m2l_class_matrices(order, vectors, src_rscale, tgt_rscale, k):
+    """Complex dense M2L operators T[c, t, s] of the Helmholtz kernel: as
+    :func:`m2l_class_matrices`, with derivatives of exp(i k r)/r and the
+    mi0 = 2 entries from the Helmholtz projection
+    u_(2,j,l) = -u_(0,j+2,l) - u_(0,j,l+2) - k^2 src_rscale^2 u_(0,j,l)
+    (get_full_kernel_derivatives_from_stored at the source rscale,
+    sumpy/expansion/m2l.py:501-523)."""
+    p = order
+    ids = np.array(stored_ids(p))
+    D = helmholtz_derivatives(vectors, src_rscale, k, 2 * p, maxi0=1)
+    nc = D.shape[-1]
+    M = 2 * p
+    kappa = (k * src_rscale) ** 2
+    full = np.zeros((3, M + 3, M + 3, nc), dtype=np.complex128)
+    full[:2, :M + 1, :M + 1] = D
+    full[2, :M + 1, :M + 1] = (-full[0, 2:M + 3, :M + 1] - full[0, :M + 1, 2:M + 3]
+                               - kappa * full[0, :M + 1, :M + 1])
+    s_plus_t = ids[None, :, :] + ids[:, None, :]
+    T = full[s_plus_t[..., 0], s_plus_t[..., 1], s_plus_t[..., 2]]
+    ratio = tgt_rscale / src_rscale
+    T = T * (ratio ** ids.sum(axis=1))[:, None, None]
+    return np.ascontiguousarray(np.moveaxis(T, -1, 0))
+
+
+def real_embedding(T):
+    """[c, t, s] complex -> [c, 2t + a, 2s + b] real with blocks
+    [[Re, -Im], [Im, Re]]: applied to coefficient vectors stored as
+    interleaved (re, im) pairs it is the complex product."""
+    c, n, _ = T.shape
+    R = np.empty((c, n, 2, n, 2))
+    R[:, :, 0, :, 0] = T.real
+    R[:, :, 0, :, 1] = -T.imag
+    R[:, :, 1, :, 0] = T.imag
+    R[:, :, 1, :, 1] = T.real
+    return R.reshape(c, 2 * n, 2 * n)
 
 # }}}

@@ -29,8 +29,12 @@ import torch
 
 from sumpy_b200 import _capi
 from sumpy_b200._capi import call, dptr, stream_ptr
-from sumpy_b200.expansion import m2l_class_matrices
-from sumpy_b200.kernel import is_scale_invariant
+from sumpy_b200.expansion import (
+    helmholtz_m2l_class_matrices,
+    m2l_class_matrices,
+    real_embedding,
+)
+from sumpy_b200.kernel import HelmholtzKernel, helmholtz_k, is_scale_invariant
 
 _i32 = _capi.i32
 _i64 = _capi.i64
@@ -100,8 +104,6 @@ class SumpyExpansionWrangler:
                  precision="fp64", device=None, gradient=False, m2l_item_groups=None):
         if not callable(fmm_level_to_order):
             raise TypeError("fmm_level_to_order not passed")
-        if np.dtype(dtype) != np.float64:
-            raise NotImplementedError("the 3D Laplace wrangler computes in float64")
         if precision not in ("fp64", "mixed"):
             raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
         self.tree_indep = tree_indep
@@ -116,6 +118,16 @@ class SumpyExpansionWrangler:
         self.device = torch.device(device if device is not None else "cuda")
 
         base_kernel = tree_indep.get_base_kernel()
+        self.helmholtz = isinstance(base_kernel, HelmholtzKernel)
+        if self.helmholtz:
+            if np.dtype(dtype) != np.complex128:
+                raise NotImplementedError("the 3D Helmholtz wrangler computes in complex128")
+            if self.gradient:
+                raise NotImplementedError("gradient outputs are implemented for Laplace only")
+            self.k = helmholtz_k(base_kernel, self.kernel_extra_kwargs)
+        elif np.dtype(dtype) != np.float64:
+            raise NotImplementedError("the 3D Laplace wrangler computes in float64")
+        self._tdtype = torch.complex128 if self.helmholtz else torch.float64
         kernel_arg_set = frozenset(self.kernel_extra_kwargs.items())
         self.level_orders = [fmm_level_to_order(base_kernel, kernel_arg_set, self.tree, lev)
                              for lev in range(self.tree.nlevels)]
@@ -176,10 +188,10 @@ class SumpyExpansionWrangler:
         return self._local_level_starts
 
     def multipole_expansion_zeros(self, actx=None):
-        return torch.zeros(self._mpole_level_starts[-1], dtype=torch.float64, device=self.device)
+        return torch.zeros(self._mpole_level_starts[-1], dtype=self._tdtype, device=self.device)
 
     def local_expansion_zeros(self, actx=None):
-        return torch.zeros(self._local_level_starts[-1], dtype=torch.float64, device=self.device)
+        return torch.zeros(self._local_level_starts[-1], dtype=self._tdtype, device=self.device)
 
     def output_zeros(self, actx=None):
         """Potential per target kernel; with ``gradient=True`` the potential
@@ -188,7 +200,7 @@ class SumpyExpansionWrangler:
         if self.gradient:
             buf = torch.zeros((4, self.tree.ntargets), dtype=torch.float64, device=self.device)
             return [buf[0], buf[1], buf[2], buf[3]]
-        return [torch.zeros(self.tree.ntargets, dtype=torch.float64, device=self.device)
+        return [torch.zeros(self.tree.ntargets, dtype=self._tdtype, device=self.device)
                 for _ in self.tree_indep.target_kernels]
 
     def _view(self, exps, level, starts):
@@ -263,9 +275,18 @@ class SumpyExpansionWrangler:
 
     def _weights(self, src_weight_vecs):
         (w,) = src_weight_vecs
-        if w.dtype != torch.float64 or not w.is_contiguous():
-            w = w.to(torch.float64).contiguous()
+        if w.dtype != self._tdtype or not w.is_contiguous():
+            w = w.to(self._tdtype).contiguous()
         return w
+
+    def _entry(self, name):
+        """C-ABI entry point name of a stage for this wrangler's kernel."""
+        return name.replace("sumpy_", "sumpy_helmholtz_", 1) if self.helmholtz else name
+
+    @property
+    def _kargs(self):
+        """The wave number argument of the Helmholtz entry points."""
+        return [_d(self.k)] if self.helmholtz else []
 
     # {{{ stages
 
@@ -281,8 +302,8 @@ class SumpyExpansionWrangler:
             if a == b:
                 continue
             base, view = self.multipole_expansions_view(mpoles, lev)
-            call("sumpy_p2e_from_single_box_f64", _c(self.level_orders[lev]),
-                 _d(self.level_to_rscale(lev)), _i32(b - a), dptr(boxes[a:b]),
+            call(self._entry("sumpy_p2e_from_single_box_f64"), _c(self.level_orders[lev]),
+                 _d(self.level_to_rscale(lev)), *self._kargs, _i32(b - a), dptr(boxes[a:b]),
                  dptr(g["centers"]), _i64(self.tree.nboxes), dptr(g["bss"]), dptr(g["bsc"]),
                  dptr(g["sources"]), _i64(self.tree.nsources), dptr(w), _i32(base),
                  dptr(view), st)
@@ -301,9 +322,10 @@ class SumpyExpansionWrangler:
                 continue
             sbase, sview = self.multipole_expansions_view(mpoles, src_lev)
             tbase, tview = self.multipole_expansions_view(mpoles, tgt_lev)
-            call("sumpy_e2e_from_children_f64", _c(self.level_orders[src_lev]),
+            call(self._entry("sumpy_e2e_from_children_f64"), _c(self.level_orders[src_lev]),
                  _c(self.level_orders[tgt_lev]), _d(self.level_to_rscale(src_lev)),
-                 _d(self.level_to_rscale(tgt_lev)), _i32(b - a), dptr(boxes[a:b]),
+                 _d(self.level_to_rscale(tgt_lev)), *self._kargs, _i32(b - a),
+                 dptr(boxes[a:b]),
                  dptr(g["child"]), _i64(self.tree.nboxes), dptr(g["centers"]),
                  _i64(self.tree.nboxes), _i32(sbase), dptr(sview), _i32(tbase), dptr(tview), st)
         return mpoles
@@ -319,9 +341,13 @@ class SumpyExpansionWrangler:
         args = (_i32(tb.numel()), dptr(tb), dptr(self._dev(source_box_starts)),
                 dptr(self._dev(source_box_lists)), dptr(g["bss"]), dptr(g["bsc"]),
                 dptr(g["bts"]), dptr(g["btc"]), dptr(g["sources"]), _i64(self.tree.nsources),
-                dptr(w), dptr(g["targets"]), _i64(self.tree.ntargets), dptr(g["tts"]),
-                _d(self._scale), dptr(pot[0]))
+                *self._kargs, dptr(w), dptr(g["targets"]), _i64(self.tree.ntargets),
+                dptr(g["tts"]), _d(self._scale), dptr(pot[0]))
         mixed = self.precision == "mixed"
+        if self.helmholtz:
+            call("sumpy_helmholtz_p2p_from_csr_mixed" if mixed
+                 else "sumpy_helmholtz_p2p_from_csr_f64", *args, stream_ptr())
+            return pot
         if self.gradient:
             call("sumpy_p2p_from_csr_grad_mixed" if mixed else "sumpy_p2p_from_csr_grad_f64",
                  *args, dptr(pot[1]), stream_ptr())
@@ -340,6 +366,13 @@ class SumpyExpansionWrangler:
         tc = self.translation_classes_data
         ls = tc.from_sep_siblings_translation_classes_level_starts
         vecs = tc.from_sep_siblings_translation_class_to_distance_vector[:, ls[lev]:ls[lev + 1]]
+        if self.helmholtz:
+            # complex operators per level, applied as their real embedding
+            key = ("helmholtz", lev, order)
+            if key not in self._m2l_mats:
+                T = helmholtz_m2l_class_matrices(order, vecs, rscale, rscale, self.k)
+                self._m2l_mats[key] = torch.as_tensor(real_embedding(T)).to(self.device)
+            return self._m2l_mats[key], 1.0
         if is_scale_invariant(kernel):
             # rscale^|mi| d^mi (1/r) at d = v*h with rscale = 2h/p equals
             # (1/rscale) times the same derivatives at v*(h/rscale) with unit rscale
@@ -539,7 +572,7 @@ class SumpyExpansionWrangler:
         return self._m2l_plans[key]
 
     def _call_m2l_f64(self, order, plan, mats, sbase, src, tbase, tgt, st):
-        call("sumpy_m2l_translation_classes_f64", _c(order), _i32(plan["nitems"]),
+        call(self._entry("sumpy_m2l_translation_classes_f64"), _c(order), _i32(plan["nitems"]),
              dptr(plan["item_tile"]), dptr(plan["item_g0"]), dptr(plan["item_g1"]),
              _i32(M2L_TILE), dptr(plan["tile_targets"]), dptr(plan["tile_scale"]),
              dptr(plan["group_class"]), dptr(plan["group_sources"]), _i32(mats.shape[0]),
@@ -591,7 +624,8 @@ class SumpyExpansionWrangler:
 
     def _call_m2l_tc(self, order, plan, hi, lo, rp, kp, src_nrows, sbase, ws_hi, ws_lo,
                      tbase, tgt, st):
-        call("sumpy_m2l_translation_classes_tf32x3", _c(order), _i32(plan["nitems"]),
+        call(self._entry("sumpy_m2l_translation_classes_tf32x3"), _c(order),
+             _i32(plan["nitems"]),
              dptr(plan["item_tile"]), dptr(plan["item_g0"]), dptr(plan["item_g1"]),
              _i32(M2L_TILE_TC), dptr(plan["tile_targets"]), dptr(plan["tile_scale"]),
              dptr(plan["group_class"]), dptr(plan["group_sources"]), _i32(plan["nclasses"]),
@@ -600,7 +634,7 @@ class SumpyExpansionWrangler:
 
     def _launch_m2l_tc_level(self, lev, items, mats, sbase, sview, tbase, tview, st):
         hi, lo, rp, kp = self._m2l_tc_operands(mats)
-        nb, n = sview.shape
+        nb, n = sview.shape[0], mats.shape[1]   # real values per box
         ws_hi, ws_lo = self._m2l_workspace(nb, kp)
         call("sumpy_split_tf32x2", _i64(nb), _i32(1), _i32(n), dptr(sview), _i32(1),
              _i32(kp), dptr(ws_hi), dptr(ws_lo), st)
@@ -626,7 +660,7 @@ class SumpyExpansionWrangler:
                 continue
             sbase, sview = self.multipole_expansions_view(mpole_exps, lev)
             tbd = self._dev(tb)
-            args = (_c(self.level_orders[lev]), _d(self.level_to_rscale(lev)),
+            args = (_c(self.level_orders[lev]), _d(self.level_to_rscale(lev)), *self._kargs,
                     _i32(tbd.numel()), dptr(tbd), dptr(self._dev(ssn.starts)),
                     dptr(self._dev(ssn.lists)), dptr(g["centers"]), _i64(self.tree.nboxes),
                     _i32(sbase), dptr(sview), dptr(g["bts"]), dptr(g["btc"]),
@@ -635,7 +669,7 @@ class SumpyExpansionWrangler:
             if self.gradient:
                 call("sumpy_e2p_from_csr_grad_f64", *args, dptr(pot[1]), st)
             else:
-                call("sumpy_e2p_from_csr_f64", *args, st)
+                call(self._entry("sumpy_e2p_from_csr_f64"), *args, st)
         return pot
 
     def form_locals(self, actx, level_start_target_or_target_parent_box_nrs,
@@ -655,8 +689,8 @@ class SumpyExpansionWrangler:
             if a == b or starts_h[a] == starts_h[b]:
                 continue
             tbase, tview = self.local_expansions_view(local_exps, lev)
-            call("sumpy_p2e_from_csr_f64", _c(self.level_orders[lev]),
-                 _d(self.level_to_rscale(lev)), _i32(b - a), dptr(boxes[a:b]),
+            call(self._entry("sumpy_p2e_from_csr_f64"), _c(self.level_orders[lev]),
+                 _d(self.level_to_rscale(lev)), *self._kargs, _i32(b - a), dptr(boxes[a:b]),
                  dptr(starts_d[a:b + 1]), dptr(lists_d), dptr(g["centers"]),
                  _i64(self.tree.nboxes), dptr(g["bss"]), dptr(g["bsc"]), dptr(g["sources"]),
                  _i64(self.tree.nsources), dptr(w), _i32(tbase), dptr(tview), st)
@@ -675,9 +709,10 @@ class SumpyExpansionWrangler:
             src_lev = tgt_lev - 1
             sbase, sview = self.local_expansions_view(local_exps, src_lev)
             tbase, tview = self.local_expansions_view(local_exps, tgt_lev)
-            call("sumpy_e2e_from_parent_f64", _c(self.level_orders[src_lev]),
+            call(self._entry("sumpy_e2e_from_parent_f64"), _c(self.level_orders[src_lev]),
                  _c(self.level_orders[tgt_lev]), _d(self.level_to_rscale(src_lev)),
-                 _d(self.level_to_rscale(tgt_lev)), _i32(b - a), dptr(boxes[a:b]),
+                 _d(self.level_to_rscale(tgt_lev)), *self._kargs, _i32(b - a),
+                 dptr(boxes[a:b]),
                  dptr(g["parent"]), dptr(g["centers"]), _i64(self.tree.nboxes),
                  _i32(sbase), dptr(sview), _i32(tbase), dptr(tview), st)
         return local_exps
@@ -693,14 +728,14 @@ class SumpyExpansionWrangler:
             if a == b:
                 continue
             sbase, sview = self.local_expansions_view(local_exps, lev)
-            args = (_c(self.level_orders[lev]), _d(self.level_to_rscale(lev)), _i32(b - a),
-                    dptr(boxes[a:b]), dptr(g["centers"]), _i64(self.tree.nboxes), _i32(sbase),
+            args = (_c(self.level_orders[lev]), _d(self.level_to_rscale(lev)), *self._kargs,
+                    _i32(b - a), dptr(boxes[a:b]), dptr(g["centers"]), _i64(self.tree.nboxes), _i32(sbase),
                     dptr(sview), dptr(g["bts"]), dptr(g["btc"]), dptr(g["targets"]),
                     _i64(self.tree.ntargets), _d(self._scale), dptr(pot[0]))
             if self.gradient:
                 call("sumpy_e2p_from_single_box_grad_f64", *args, dptr(pot[1]), st)
             else:
-                call("sumpy_e2p_from_single_box_f64", *args, st)
+                call(self._entry("sumpy_e2p_from_single_box_f64"), *args, st)
         return pot
 
     # }}}

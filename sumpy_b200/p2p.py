@@ -2,8 +2,10 @@
 
 ``P2P(target_kernels, exclude_self)(actx, targets, sources, (strength,))``
 returns ``[potential]`` like sumpy's, computed by the FP64 CUDA kernel
-``sumpy_p2p_direct_f64``. sumpy's FMM tests use this as the accuracy
-reference (sumpy/test/test_fmm.py:284-286).
+``sumpy_p2p_direct_f64`` (``sumpy_helmholtz_p2p_direct_f64`` for a
+``HelmholtzKernel``, whose wave number comes as a keyword argument, e.g.
+``k=10``, as in sumpy). sumpy's FMM tests use this as the accuracy reference
+(sumpy/test/test_fmm.py:284-286).
 """
 from __future__ import annotations
 
@@ -11,6 +13,7 @@ import torch
 
 from sumpy_b200 import _capi
 from sumpy_b200._capi import call, dptr, stream_ptr
+from sumpy_b200.kernel import HelmholtzKernel, helmholtz_k
 
 
 def _soa(x, device):
@@ -38,13 +41,25 @@ class P2P:
         t = _soa(targets, dev)
         s = _soa(sources, dev)
         (q,) = strength
-        q = torch.as_tensor(q, dtype=torch.float64).to(dev).contiguous()
+        knl = self.target_kernels[0]
+        helm = isinstance(knl, HelmholtzKernel)
+        if helm and self.gradient:
+            raise NotImplementedError("gradient outputs are implemented for Laplace only")
+        qdt = torch.complex128 if helm else torch.float64
+        q = torch.as_tensor(q).to(dev, qdt).contiguous()
         tts = None
         if self.exclude_self:
             if target_to_source is None:
                 raise ValueError("exclude_self needs target_to_source")
             tts = torch.as_tensor(target_to_source).to(dev, torch.int32).contiguous()
-        scale = self.target_kernels[0].global_scaling_const
+        scale = knl.global_scaling_const
+        if helm:
+            out = torch.empty(t.shape[1], dtype=torch.complex128, device=dev)
+            call("sumpy_helmholtz_p2p_direct_f64", _capi.i64(t.shape[1]), dptr(t),
+                 _capi.i64(t.shape[1]), _capi.i64(s.shape[1]), dptr(s), _capi.i64(s.shape[1]),
+                 _capi.dbl(helmholtz_k(knl, kwargs)), dptr(q), dptr(tts), _capi.dbl(scale),
+                 dptr(out), stream_ptr())
+            return [out]
         args = (_capi.i64(t.shape[1]), dptr(t), _capi.i64(t.shape[1]), _capi.i64(s.shape[1]),
                 dptr(s), _capi.i64(s.shape[1]), dptr(q), dptr(tts), _capi.dbl(scale))
         if self.gradient:
