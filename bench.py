@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true", help="skip timing the FP64 form")
     ap.add_argument("--stage-times", action="store_true", help="print per-stage times")
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-problem batch")
+    ap.add_argument("--no-helmholtz", action="store_true",
+                    help="skip the 500k-point Helmholtz workload")
     return ap.parse_args()
 
 
@@ -121,26 +123,81 @@ def run_reference(args):
 
 
 class ClockSampler:
+    """SM clock and clock-event reasons sampled DURING a timed region: an NVML
+    thread polling every 5 ms (read-only queries), so that even a region of a
+    few tens of milliseconds gets samples; nvidia-smi at its 100 ms floor as
+    the fallback when NVML is unavailable."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, period_s=0.005):
         self.gpu = gpu_index
+        self.period = period_s
         self.proc = None
+        self.thread = None
+        self.samples = []
+        self.max_mhz = None
+        self.out = ""
+
+    def _nvml_loop(self, nv, h, bits):
+        while not self._stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((float(sm), [n for n, b in bits if rs & b]))
+            except Exception:  # noqa: BLE001 (a failed read is skipped)
+                pass
+            self._stop.wait(self.period)
 
     def __enter__(self):
+        import threading
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            import torch
+            uuid = None
+            try:
+                uuid = str(torch.cuda.get_device_properties(self.gpu).uuid)
+            except Exception:  # noqa: BLE001
+                uuid = None
+            h = None
+            if uuid:
+                for cand in (uuid, "GPU-" + uuid):
+                    try:
+                        h = nv.nvmlDeviceGetHandleByUUID(cand)
+                        break
+                    except Exception:  # noqa: BLE001
+                        h = None
+            if h is None:
+                h = nv.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            bits = [("hw_slowdown", nv.nvmlClocksEventReasonHwSlowdown),
+                    ("hw_thermal_slowdown", nv.nvmlClocksEventReasonHwThermalSlowdown),
+                    ("sw_thermal_slowdown", nv.nvmlClocksEventReasonSwThermalSlowdown),
+                    ("sw_power_cap", nv.nvmlClocksEventReasonSwPowerCap)]
+            self._stop = threading.Event()
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h, bits),
+                                           daemon=True)
+            self.thread.start()
+            return self
+        except Exception:  # noqa: BLE001 (no NVML: fall back to nvidia-smi)
+            self.thread = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
         return self
 
     def __exit__(self, *exc):
-        self.out = ""
+        if self.thread is not None:
+            self._stop.set()
+            self.thread.join(timeout=2)
+            return
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -148,27 +205,26 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
                 self.out, _ = self.proc.communicate()
+            for r in (self.out or "").strip().splitlines():
+                r = [x.strip() for x in r.split(",")]
+                if len(r) < 9:
+                    continue
+                try:
+                    sm = float(r[1])
+                    self.max_mhz = float(r[2])
+                except ValueError:
+                    continue
+                self.samples.append(
+                    (sm, [nm for nm, v in zip(self.NAMES, r[5:9]) if v.lower() == "active"]))
 
     def summary(self):
-        rows = [r.split(",") for r in (self.out or "").strip().splitlines() if r.strip()]
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in rows:
-            r = [x.strip() for x in r]
-            if len(r) < 9:
-                continue
-            try:
-                sm.append(float(r[1]))
-                mx = float(r[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, r[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [], "samples": 0}
+        reasons = sorted({n for _, rs in self.samples for n in rs})
+        return {"sm_mhz": float(np.median([s for s, _ in self.samples])),
+                "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(self.samples),
+                "source": "nvml" if self.thread is not None else "nvidia-smi"}
 
 
 def main():
@@ -293,6 +349,8 @@ def main():
     stage_ms, roof = stage_breakdown(w_mx, trav, q_dev, dev)
     adj = adjoint_bench(dev) if world == 1 else None
     batch = batched_bench(dev) if world == 1 and not args.no_batch else None
+    helm = helmholtz_bench(dev) if world == 1 and not args.no_helmholtz else None
+    uni = uniform_bench(dev, cpu=not args.no_cpu_baseline) if world == 1 else None
 
     value = world * args.npoints / (ms_mx * 1e-3) / 1e6
     line = {
@@ -317,6 +375,8 @@ def main():
         "adjoint_forward_ratio": adj["ratio"] if adj else None,
         "adjoint": adj,
         "batched": batch,
+        "helmholtz": helm,
+        "uniform_p6": uni,
         "stage_ms": stage_ms,
         "roofline": roof,
         "cpu_baseline": cpu_line,
@@ -515,7 +575,127 @@ def batched_bench(dev, steps=5, warmup=3, nproblems=512, order=8, nseq=16):
     }
 
 
-def stage_breakdown(w, trav, q_dev, dev):
+def uniform_bench(dev, steps=5, warmup=3, n=20_000, order=6, cpu=True):
+    """The reference's own CPU-runnable case: 20k sources and 20k separate
+    targets U[0,1]^3 (seeds 15, 18; strengths seed 44), p = 6, max 30 per box,
+    FP64 end to end. GPU time (CUDA events), accuracy against the FP64 GPU
+    direct sum, and as its CPU baseline the oracle (C + OpenMP, all host
+    threads) on the same tree."""
+    import torch
+    from sumpy_b200 import (P2P, LaplaceKernel, SumpyExpansionWrangler,
+                            SumpyTreeIndependentDataForWrangler, drive_fmm)
+    from sumpy_b200.expansion import (
+        LinearPDEConformingVolumeTaylorLocalExpansion as LExp,
+        LinearPDEConformingVolumeTaylorMultipoleExpansion as MExp)
+    from sumpy_b200.tree import build_all
+    src = np.random.default_rng(15).random((3, n))
+    tgt = np.random.default_rng(18).random((3, n))
+    q = np.random.default_rng(44).standard_normal(n)
+    tree, trav, tcls = build_all(src, tgt, 30)
+    knl = LaplaceKernel(3)
+    ti = SumpyTreeIndependentDataForWrangler(
+        None, lambda o, **kw: MExp(knl, o), lambda o, **kw: LExp(knl, o), [knl])
+    w = SumpyExpansionWrangler(ti, trav, np.float64, lambda *a: order,
+                               translation_classes_data=tcls, device=dev)
+    qd = torch.as_tensor(q, device=dev)
+    for _ in range(warmup):
+        drive_fmm(None, w, [qd])
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        (pot,) = drive_fmm(None, w, [qd])
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    (ref,) = P2P([knl])(None, tgt, src, (q,), device=dev)
+    out = {"workload": f"uniform {n} sources + {n} targets, p={order}, FP64",
+           "ms_per_step": ms, "Mpts_s": n / (ms * 1e-3) / 1e6,
+           "relL2_vs_direct": float((pot - ref).norm() / ref.norm())}
+    if cpu:
+        from oracle import oracle as O
+        t0 = time.perf_counter()
+        O.run_fmm(tree, trav, tcls, order, q)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"ms_per_step": 1e3 * dt, "cores": os.cpu_count(), "kind": "port",
+                               "sample": "the same 20k + 20k evaluation, FP64 C/OpenMP oracle"}
+        out["gpu_over_cpu"] = 1e3 * dt / ms
+    return out
+
+
+def helmholtz_bench(dev, steps=3, warmup=2, npoints=500_000, order=14, k=10.0):
+    """3D Helmholtz (G = e^{ikr}/r, k = 10): 500k points on the unit sphere
+    (sources = targets, exclude_self), strengths N(0,1) + i N(0,1), p = 14,
+    max 32 per box. Mixed (complex64 near field on FP64 offsets, split-TF32
+    M2L on the real embedding) and FP64 forms timed with CUDA events (L2
+    flushed between steps); accuracy on 2,048 sampled targets against the
+    complex128 GPU direct sum; per-stage times of the mixed form."""
+    import torch
+    from sumpy_b200 import (P2P, HelmholtzKernel, SumpyExpansionWrangler,
+                            SumpyTreeIndependentDataForWrangler, drive_fmm)
+    from sumpy_b200.expansion import (
+        LinearPDEConformingVolumeTaylorLocalExpansion as LExp,
+        LinearPDEConformingVolumeTaylorMultipoleExpansion as MExp)
+    from sumpy_b200.tree import build_all
+    rng = np.random.default_rng(2025)
+    g = rng.standard_normal((3, npoints))
+    pts = g / np.linalg.norm(g, axis=0)
+    q = rng.standard_normal(npoints) + 1j * rng.standard_normal(npoints)
+    t0 = time.perf_counter()
+    tree, trav, tcls = build_all(pts, None, MAX_PARTICLES)
+    t_tree = time.perf_counter() - t0
+    knl = HelmholtzKernel(3)
+    ti = SumpyTreeIndependentDataForWrangler(
+        None, lambda o, **kw: MExp(knl, o), lambda o, **kw: LExp(knl, o), [knl],
+        exclude_self=True)
+    qd = torch.as_tensor(q, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(steps)]
+        torch.cuda.synchronize()
+        for i in range(steps):
+            flush.fill_(float(i))
+            evs[i][0].record()
+            fn()
+            evs[i][1].record()
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(c) for a, c in evs) / steps
+
+    smp = rng.choice(npoints, size=2048, replace=False)
+    (ref,) = P2P([knl], exclude_self=True)(None, pts[:, smp], pts, (q,),
+                                           target_to_source=smp, device=dev, k=k)
+    ref = ref.cpu().numpy()
+    out = {"workload": f"unit sphere n={npoints}, k={k}, p={order}, complex strengths, "
+                       f"exclude_self, max {MAX_PARTICLES} per box",
+           "tree_build_s": round(t_tree, 3), "m2l_entries": int(len(trav.from_sep_siblings_lists))}
+    for precision in ("mixed", "fp64"):
+        t0 = time.perf_counter()
+        w = SumpyExpansionWrangler(ti, trav, np.complex128, lambda *a: order,
+                                   kernel_extra_kwargs={"k": k}, translation_classes_data=tcls,
+                                   precision=precision, device=dev)
+        (pot,) = drive_fmm(None, w, [qd])
+        torch.cuda.synchronize()
+        setup = time.perf_counter() - t0
+        ms = timed(lambda: drive_fmm(None, w, [qd]))
+        w.check_status()
+        got = pot.cpu().numpy()[smp]
+        out[precision] = {"Mpts_s": npoints / (ms * 1e-3) / 1e6, "ms_per_step": ms,
+                          "relL2_vs_direct": float(np.linalg.norm(got - ref) /
+                                                   np.linalg.norm(ref)),
+                          "setup_s": round(setup, 2)}
+        if precision == "mixed":
+            out["stage_ms_mixed"], _ = stage_breakdown(w, trav, qd, dev, roofline=False)
+        del w
+        torch.cuda.empty_cache()
+    out["mixed_over_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    return out
+
+
+def stage_breakdown(w, trav, q_dev, dev, roofline=True):
     """Per-stage device times of one FMM (CUDA events between the wrangler
     calls on the launching stream) and the roofline of the dominant stage."""
     import torch
@@ -562,6 +742,8 @@ def stage_breakdown(w, trav, q_dev, dev):
     stage = {}
     for (n0, e0), (n1, e1) in zip(ev, ev[1:]):
         stage[n1] = e0.elapsed_time(e1)
+    if not roofline:
+        return stage, None
 
     # algorithmic work
     tree = w.tree
