@@ -27,6 +27,7 @@
 //  * M2L reuses the real GEMM kernels (m2l.cu, m2l_tc.cu) on the real
 //    embedding [[Re, -Im], [Im, Re]] of the complex class operators.
 #include <algorithm>
+#include <utility>
 
 #include "common.cuh"
 #include "taylor.cuh"
@@ -78,48 +79,6 @@ constexpr FaaTable make_faa_table()
             t.v[m][q] = v;
         }
     return t;
-}
-__constant__ FaaTable c_faa = make_faa_table();
-
-// gamma_Q, Q = 0..qmax, at distance r
-__device__ __forceinline__ void helm_gammas(double r, double k, int qmax, double *gr, double *gi,
-                                            int stride)
-{
-    double sn, cs;
-    sincos(k * r, &sn, &cs);
-    const double ri = 1.0 / r;
-    z2 g0 = zmk(cs * ri, sn * ri);
-    // (ikr - 1) e^{ikr} / r
-    z2 g1 = zmul(zmk(-1.0, k * r), g0);
-    gr[0] = g0.x; gi[0] = g0.y;
-    if (qmax >= 1) { gr[stride] = g1.x; gi[stride] = g1.y; }
-    const double kr2 = (k * r) * (k * r);
-    for (int q = 2; q <= qmax; ++q) {
-        const z2 g2 = zmk(-(2.0 * q - 1.0) * g1.x - kr2 * g0.x, -(2.0 * q - 1.0) * g1.y - kr2 * g0.y);
-        gr[q * stride] = g2.x; gi[q * stride] = g2.y;
-        g0 = g1; g1 = g2;
-    }
-}
-
-// sum_{q1, q2} C[j][q1] C[l][q2] N1[2q1-j] N2[2q2-l] gamma[q1+q2+i] for one
-// stored mi = (i, j, l); tables strided by `st`.
-__device__ __forceinline__ z2 helm_mi_sum(int i, int j, int l, const double *N1, const double *N2,
-                                          const double *gr, const double *gi, int st)
-{
-    z2 s = zmk(0.0, 0.0);
-    for (int q1 = (j + 1) >> 1; q1 <= j; ++q1) {
-        const double a1 = c_faa.v[j][q1] * N1[(2 * q1 - j) * st];
-        double sr = 0.0, si = 0.0;
-        for (int q2 = (l + 1) >> 1; q2 <= l; ++q2) {
-            const double a2 = c_faa.v[l][q2] * N2[(2 * q2 - l) * st];
-            const int Q = q1 + q2 + i;
-            sr = fma(a2, gr[Q * st], sr);
-            si = fma(a2, gi[Q * st], si);
-        }
-        s.x = fma(a1, sr, s.x);
-        s.y = fma(a1, si, s.y);
-    }
-    return s;
 }
 
 // {{{ P2P
@@ -657,174 +616,331 @@ hl2p_kernel(int p, double rscale, double kappa, int32_t nboxes, const int32_t *_
 
 // }}}
 
-// {{{ M2P / P2L (derivatives from the closed form)
+// {{{ M2P / P2L (derivatives from the closed form, in registers)
 
-constexpr int HM2P_WARPS = 2;
+// stored index s -> (degree, i, j): s = d^2 + i (d + 1) + j
+__host__ __device__ constexpr int stored_deg(int s)
+{
+    int d = 0;
+    while ((d + 1) * (d + 1) <= s) ++d;
+    return d;
+}
+__host__ __device__ constexpr int stored_i(int s) { return s - stored_deg(s) * stored_deg(s) <= stored_deg(s) ? 0 : 1; }
+__host__ __device__ constexpr int stored_j(int s)
+{
+    return s - stored_deg(s) * stored_deg(s) - stored_i(s) * (stored_deg(s) + 1);
+}
+
+// Scaled form used by the kernels below: with v = x / rs and
+// gt_Q = rs^(2Q) g_Q (= rho^(2Q) gamma_Q),
+//     D(i, j, l) = sum_{q1, q2} C[j][q1] C[l][q2] v1^(2q1-j) v2^(2q2-l) v0^i gt_{q1+q2+i},
+//     gt_0 = e^{ikr}/r, gt_1 = u (ikr - 1) gt_0,
+//     gt_Q = -(2Q - 1) u gt_{Q-1} - (k rs)^2 u gt_{Q-2},  u = (rs/r)^2,
+// so the live state per evaluation point is v and gt_0..P.
+template <int P>
+struct HelmTables {
+    double v0, v1, v2, v1s, v2s;   // v, v1^2, v2^2
+    double gr[P + 1], gi[P + 1];
+};
+
+// a * b that the compiler may neither merge with an identical product of
+// another term nor move: keeps the per-axis factors out of the live
+// register set (merged across all terms they would stay live and spill).
+__device__ __forceinline__ double opaque_mul(double a, double b)
+{
+    double r;
+    asm volatile("mul.rn.f64 %0, %1, %2;" : "=d"(r) : "d"(a), "d"(b));
+    return r;
+}
+
+// The coefficients as compile-time constants (immediates in the code, which
+// the compiler rematerialises instead of keeping loaded values live).
+constexpr FaaTable kFaa = make_faa_table();
+
+// one (q1, q2) product of a term: tr/ti += C[L][Q2] v2^(2 Q2 - L) gt_{Q1+Q2+I}
+template <int P, int I, int L, int Q1, int Q2>
+__device__ __forceinline__ void helm_q2(const HelmTables<P> &t, double &tr, double &ti, double &p2)
+{
+    constexpr double c = kFaa.v[L][Q2];
+    const double a2 = c * p2;
+    tr = fma(a2, t.gr[Q1 + Q2 + I], tr);
+    ti = fma(a2, t.gi[Q1 + Q2 + I], ti);
+    if constexpr (Q2 < L) p2 = opaque_mul(p2, t.v2s);
+}
+
+// the q1 = Q1 slice of a term: sr/si += C[J][Q1] v1^(2 Q1 - J) sum_q2 (...)
+template <int P, int I, int J, int L, int Q1, int... K2>
+__device__ __forceinline__ void helm_q1(const HelmTables<P> &t, double &sr, double &si, double &p1,
+                                        std::integer_sequence<int, K2...>)
+{
+    double tr = 0.0, ti = 0.0;
+    double p2 = opaque_mul((L & 1) ? t.v2 : 1.0, 1.0);
+    (helm_q2<P, I, L, Q1, (L + 1) / 2 + K2>(t, tr, ti, p2), ...);
+    constexpr double c = kFaa.v[J][Q1];
+    const double a1 = c * p1;
+    sr = fma(a1, tr, sr);
+    si = fma(a1, ti, si);
+    if constexpr (Q1 < J) p1 = opaque_mul(p1, t.v1s);
+}
+
+template <int P, int I, int J, int L, int... K1>
+__device__ __forceinline__ z2 helm_term_impl(const HelmTables<P> &t,
+                                             std::integer_sequence<int, K1...>)
+{
+    double sr = 0.0, si = 0.0;
+    // running power v1^(2 q1 - J) (and v2^(2 q2 - L) in helm_q1), produced
+    // by opaque products so that no power is shared across terms
+    double p1 = opaque_mul((J & 1) ? t.v1 : 1.0, 1.0);
+    (helm_q1<P, I, J, L, (J + 1) / 2 + K1>(t, sr, si, p1,
+                                            std::make_integer_sequence<int, L / 2 + 1>{}),
+     ...);
+    return I ? zmk(t.v0 * sr, t.v0 * si) : zmk(sr, si);
+}
+
+// D of the stored coefficient S (compile-time), from the tables
+template <int P, int S>
+__device__ __forceinline__ z2 helm_term(const HelmTables<P> &t)
+{
+    constexpr int d = stored_deg(S), i = stored_i(S), j = stored_j(S), l = d - i - j;
+    return helm_term_impl<P, i, j, l>(t, std::make_integer_sequence<int, j / 2 + 1>{});
+}
+
+// the terms of one degree D (stored indices D^2 .. (D+1)^2 - 1)
+template <int P, int S, typename F>
+__device__ __forceinline__ void helm_step(const HelmTables<P> &t, F &f)
+{
+    f(std::integral_constant<int, S>{}, helm_term<P, S>(t));
+    // ordered after the term's own volatile products: the next term starts
+    // only once this one has been consumed (f fences its registers too)
+    asm volatile("" ::: "memory");
+}
+
+template <int P, int D, typename F, int... R>
+__device__ __forceinline__ void helm_degree(const HelmTables<P> &t, F &f,
+                                            std::integer_sequence<int, R...>)
+{
+    (helm_step<P, D * D + R>(t, f), ...);
+}
+
+// run degree d (a runtime value) with the degree-D code: each degree is its
+// own block, so the scheduler never interleaves more than one degree's
+// 2D + 1 terms (all (P+1)^2 at once would not fit in registers)
+template <int P, typename F, int... D>
+__device__ __forceinline__ void helm_dispatch(int d, const HelmTables<P> &t, F &f,
+                                              std::integer_sequence<int, D...>)
+{
+    ((d == D ? helm_degree<P, D>(t, f, std::make_integer_sequence<int, 2 * D + 1>{})
+             : void()),
+     ...);
+}
+
+// D(mi) = rs^|mi| d^mi (e^{ikr}/r) at x for every stored mi of order <= P,
+// in stored order s = 0, 1, ..., (P+1)^2 - 1: f(std::integral_constant<int, s>, D).
+template <int P, typename F>
+__device__ __forceinline__ void helm_layers(double x0, double x1, double x2, double rs, double k,
+                                            F &&f)
+{
+    HelmTables<P> t;
+    const double r2 = x0 * x0 + x1 * x1 + x2 * x2;
+    const double ri = rsqrt(r2);
+    const double r = r2 * ri;
+    const double rsi = 1.0 / rs;
+    t.v0 = x0 * rsi;
+    t.v1 = x1 * rsi;
+    t.v2 = x2 * rsi;
+    t.v1s = t.v1 * t.v1;
+    t.v2s = t.v2 * t.v2;
+    const double u = rs * rs * ri * ri;
+    double sn, cs;
+    sincos(k * r, &sn, &cs);
+    t.gr[0] = cs * ri;
+    t.gi[0] = sn * ri;
+    if constexpr (P >= 1) {
+        const double kr = k * r;
+        t.gr[1] = u * (-t.gr[0] - kr * t.gi[0]);
+        t.gi[1] = u * (-t.gi[0] + kr * t.gr[0]);
+        const double ku = (k * rs) * (k * rs) * u;
+#pragma unroll
+        for (int q = 2; q <= P; ++q) {
+            t.gr[q] = -(2.0 * q - 1.0) * u * t.gr[q - 1] - ku * t.gr[q - 2];
+            t.gi[q] = -(2.0 * q - 1.0) * u * t.gi[q - 1] - ku * t.gi[q - 2];
+        }
+    }
+#pragma unroll 1
+    for (int d = 0; d <= P; ++d)
+        helm_dispatch<P>(d, t, f, std::make_integer_sequence<int, P + 1>{});
+}
+
+// read-only 16-byte load of p[S], kept in program order and addressed with
+// an immediate offset (plain loads of the multipole would be hoisted above
+// all terms, with one live address each)
+template <int S>
+__device__ __forceinline__ z2 ordered_load(const z2 *p)
+{
+    z2 v;
+    asm volatile("ld.global.nc.v2.f64 {%0, %1}, [%2+%3];"
+                 : "=d"(v.x), "=d"(v.y)
+                 : "l"(p), "n"(S * 16));
+    return v;
+}
+
+constexpr int HM2P_WARPS = 4;
 
 // E2PFromCSR (List 3; sumpy/e2p.py:233-343, multipole.py:131-157): one warp
-// per target box, lanes over its targets; per List-3 box the multipole is
-// staged in shared memory and each lane sums M[mi] D(mi)(t - c) over the
-// stored mi with its own tables (lane-strided in shared memory).
-// Accumulates into result.
+// per target box; the box's targets occupy g = next_pow2(nt) lanes and the
+// 32/g lane groups stride over the List-3 boxes; each lane sums M[s] D(s)
+// with D from helm_layers; shuffle-xor sum; accumulated into result.
+template <int P>
 __global__ void __launch_bounds__(32 * HM2P_WARPS)
-hm2p_kernel(int p, double rscale, double k, int32_t ntgt_boxes,
-            const int32_t *__restrict__ target_boxes, const int32_t *__restrict__ src_starts,
-            const int32_t *__restrict__ src_lists, const double *__restrict__ centers,
-            int64_t cstride, int32_t sbase, const z2 *__restrict__ src,
-            const int32_t *__restrict__ bts, const int32_t *__restrict__ btc,
-            const double *__restrict__ targets, int64_t tstride, double scale,
-            z2 *__restrict__ result)
+hm2p_reg_kernel(double rscale, double k, int32_t ntgt_boxes,
+                const int32_t *__restrict__ target_boxes, const int32_t *__restrict__ src_starts,
+                const int32_t *__restrict__ src_lists, const double *__restrict__ centers,
+                int64_t cstride, int32_t sbase, const z2 *__restrict__ src,
+                const int32_t *__restrict__ bts, const int32_t *__restrict__ btc,
+                const double *__restrict__ targets, int64_t tstride, double scale,
+                z2 *__restrict__ result)
 {
-    extern __shared__ __align__(16) double sm[];
-    const int P1 = p + 1;
-    const int n = ncoeff_of(p);
+    constexpr int N = (P + 1) * (P + 1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ib = blockIdx.x * HM2P_WARPS + warp;
     if (ib >= ntgt_boxes) return;
-    // per warp: M[n] z2, then lane tables N1, N2, RH, GR, GI: [P1][32] each
-    const int per_warp = 2 * n + 5 * P1 * 32;
-    double *base = sm + warp * per_warp;
-    z2 *M = reinterpret_cast<z2 *>(base);
-    double *N1 = base + 2 * n + lane;
-    double *N2 = N1 + P1 * 32;
-    double *RH = N2 + P1 * 32;
-    double *GR = RH + P1 * 32;
-    double *GI = GR + P1 * 32;
-
     const int32_t tb = target_boxes[ib];
     const int32_t t0 = bts[tb], nt = btc[tb];
     const int32_t ls = src_starts[ib], le = src_starts[ib + 1];
     for (int32_t tc = 0; tc < nt; tc += 32) {
-        const bool active = tc + lane < nt;
-        const int32_t t = t0 + tc + lane;
+        const int ntc = min(32, nt - tc);
+        int g = 1;
+        while (g < ntc) g <<= 1;
+        const int nph = 32 / g;
+        const int tl = lane & (g - 1), ph = lane / g;
+        const bool active = tl < ntc;
+        const int32_t t = t0 + tc + tl;
         double tx = 0, ty = 0, tz = 0;
+        if (active) { tx = targets[t]; ty = targets[tstride + t]; tz = targets[2 * tstride + t]; }
+        double ar = 0.0, ai = 0.0;
         if (active) {
-            tx = targets[t];
-            ty = targets[tstride + t];
-            tz = targets[2 * tstride + t];
-        }
-        z2 acc = zmk(0.0, 0.0);
-        for (int32_t l = ls; l < le; ++l) {
-            const int32_t sb = src_lists[l];
-            __syncwarp();
-            for (int s = lane; s < n; s += 32) M[s] = src[(int64_t)(sb - sbase) * n + s];
-            __syncwarp();
-            if (!active) continue;
-            const double x0 = tx - centers[sb], x1 = ty - centers[cstride + sb],
-                         x2 = tz - centers[2 * cstride + sb];
-            const double r = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
-            const double ri = 1.0 / r;
-            const double n0 = x0 * ri, n1 = x1 * ri, n2 = x2 * ri;
-            const double rho = rscale * ri;
-            double a1 = 1.0, a2 = 1.0, ar = 1.0;
-            for (int e = 0; e <= p; ++e) {
-                N1[e * 32] = a1; N2[e * 32] = a2; RH[e * 32] = ar;
-                a1 *= n1; a2 *= n2; ar *= rho;
-            }
-            helm_gammas(r, k, p, GR, GI, 32);
-            int mi = 0;
-            for (int d = 0; d <= p; ++d) {
-                const double rd = RH[d * 32];
-                for (int i = 0; i <= min(1, d); ++i) {
-                    const double fi = rd * (i ? n0 : 1.0);
-                    for (int j = 0; j <= d - i; ++j, ++mi) {
-                        const z2 s = helm_mi_sum(i, j, d - i - j, N1, N2, GR, GI, 32);
-                        acc = zfma(M[mi], zscal(fi, s), acc);
-                    }
-                }
+            for (int32_t l = ls + ph; l < le; l += nph) {
+                const int32_t sb = src_lists[l];
+                const z2 *M = src + (int64_t)(sb - sbase) * N;
+                helm_layers<P>(tx - centers[sb], ty - centers[cstride + sb],
+                               tz - centers[2 * cstride + sb], rscale, k,
+                               [&](auto sc, z2 v) {
+                                   const z2 m = ordered_load<decltype(sc)::value>(M);
+                                   ar = fma(m.x, v.x, fma(-m.y, v.y, ar));
+                                   ai = fma(m.x, v.y, fma(m.y, v.x, ai));
+                                   asm volatile("" : "+d"(ar), "+d"(ai));
+                               });
             }
         }
-        if (active) {
+        for (int off = g; off < 32; off <<= 1) {
+            ar += __shfl_xor_sync(0xffffffffu, ar, off);
+            ai += __shfl_xor_sync(0xffffffffu, ai, off);
+        }
+        if (active && ph == 0) {
             z2 &o = result[t];
-            o = zaxpy(scale, acc, o);
+            o = zmk(fma(scale, ar, o.x), fma(scale, ai, o.y));
         }
     }
 }
 
 constexpr int HP2L_WARPS = 2;
-constexpr int HP2L_MAXU = (SUMPY_MAX_ORDER + 1) * (SUMPY_MAX_ORDER + 1) / 32 + 1;
 
 // P2EFromCSR (List 4; sumpy/p2e.py:268-388, local.py:225-271): one warp per
-// target box; the box's List-4 sources go 32 at a time: each lane writes the
-// tables of one source to shared memory (source-major), then each lane owns
-// the stored coefficients lane + 32 u and sums q_s D(mi)(c - s) over the
-// staged sources. Accumulates into the box's local.
+// target box; the sources of its List-4 boxes are enumerated flat, 32 per
+// round, one per lane. The coefficients come out of helm_layers in stored
+// order; every 32 of them pass through a per-warp shared tile
+// [coefficient][source] (stride 33), where each lane sums its coefficient
+// over the round's sources. Accumulated into the box's local.
+template <int P>
 __global__ void __launch_bounds__(32 * HP2L_WARPS)
-hp2l_kernel(int p, double rscale, double k, int32_t ntgt_boxes,
-            const int32_t *__restrict__ target_boxes, const int32_t *__restrict__ src_starts,
-            const int32_t *__restrict__ src_lists, const double *__restrict__ centers,
-            int64_t cstride, const int32_t *__restrict__ bss, const int32_t *__restrict__ bsc,
-            const double *__restrict__ sources, int64_t sstride, const z2 *__restrict__ q,
-            int32_t tbase, z2 *__restrict__ tgt)
+hp2l_reg_kernel(double rscale, double k, int32_t ntgt_boxes,
+                const int32_t *__restrict__ target_boxes, const int32_t *__restrict__ src_starts,
+                const int32_t *__restrict__ src_lists, const double *__restrict__ centers,
+                int64_t cstride, const int32_t *__restrict__ bss, const int32_t *__restrict__ bsc,
+                const double *__restrict__ sources, int64_t sstride, const z2 *__restrict__ q,
+                int32_t tbase, z2 *__restrict__ out)
 {
-    extern __shared__ __align__(16) double sm[];
-    const int P1 = p + 1;
-    const int n = ncoeff_of(p);
+    constexpr int N = (P + 1) * (P + 1);
+    constexpr int NPL = (N + 31) / 32;
+    __shared__ z2 tile[HP2L_WARPS][32][33];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ib = blockIdx.x * HP2L_WARPS + warp;
     if (ib >= ntgt_boxes) return;
-    // per source: N1, N2, RH, GR, GI [P1] each, then n0, qr, qi
-    const int per_src = 5 * P1 + 3;
-    double *base = sm + warp * 32 * per_src;
-
+    z2 (*T)[33] = tile[warp];
     const int32_t tb = target_boxes[ib];
-    const double c[3] = {centers[tb], centers[cstride + tb], centers[2 * cstride + tb]};
-    z2 acc[HP2L_MAXU];
-#pragma unroll
-    for (int u = 0; u < HP2L_MAXU; ++u) acc[u] = zmk(0.0, 0.0);
-
+    const double c0 = centers[tb], c1 = centers[cstride + tb], c2 = centers[2 * cstride + tb];
     const int32_t ls = src_starts[ib], le = src_starts[ib + 1];
-    for (int32_t l = ls; l < le; ++l) {
-        const int32_t sb = src_lists[l];
-        const int32_t s0 = bss[sb], ns = bsc[sb];
-        for (int32_t sc = 0; sc < ns; sc += 32) {
-            const int nsc = min(32, ns - sc);
-            __syncwarp();
-            if (lane < nsc) {
-                const int32_t s = s0 + sc + lane;
-                double *T = base + lane * per_src;
-                const double x0 = c[0] - sources[s], x1 = c[1] - sources[sstride + s],
-                             x2 = c[2] - sources[2 * sstride + s];
-                const double r = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
-                const double ri = 1.0 / r;
-                const double n1 = x1 * ri, n2 = x2 * ri, rho = rscale * ri;
-                double a1 = 1.0, a2 = 1.0, ar = 1.0;
-                for (int e = 0; e <= p; ++e) {
-                    T[e] = a1; T[P1 + e] = a2; T[2 * P1 + e] = ar;
-                    a1 *= n1; a2 *= n2; ar *= rho;
-                }
-                helm_gammas(r, k, p, T + 3 * P1, T + 4 * P1, 1);
-                const z2 qs = q[s];
-                T[5 * P1] = x0 * ri;
-                T[5 * P1 + 1] = qs.x;
-                T[5 * P1 + 2] = qs.y;
-            }
-            __syncwarp();
+    int32_t total = 0;
+    for (int32_t l = ls; l < le; ++l) total += bsc[src_lists[l]];
+    z2 acc[NPL];
 #pragma unroll
-            for (int u = 0; u < HP2L_MAXU; ++u) {
-                const int mi = lane + 32 * u;
-                if (mi >= n) break;
-                int i, j, l2;
-                stored_mi(mi, i, j, l2);
-                const int d = i + j + l2;
-                z2 a = acc[u];
-                for (int s = 0; s < nsc; ++s) {
-                    const double *T = base + s * per_src;
-                    const z2 sum = helm_mi_sum(i, j, l2, T, T + P1, T + 3 * P1, T + 4 * P1, 1);
-                    const double f = T[2 * P1 + d] * (i ? T[5 * P1] : 1.0);
-                    a = zfma(zmk(T[5 * P1 + 1], T[5 * P1 + 2]), zscal(f, sum), a);
-                }
-                acc[u] = a;
-            }
+    for (int m = 0; m < NPL; ++m) acc[m] = zmk(0.0, 0.0);
+    for (int32_t base = 0; base < total; base += 32) {
+        const int nsc = min(32, total - base);
+        // inactive lanes evaluate at a harmless point with zero strength
+        double x0 = 1.0, x1 = 0.0, x2 = 0.0;
+        z2 qq = zmk(0.0, 0.0);
+        if (lane < nsc) {
+            int32_t f = base + lane, l = ls, sb = src_lists[ls];
+            while (f >= bsc[sb]) { f -= bsc[sb]; ++l; sb = src_lists[l]; }
+            const int32_t s = bss[sb] + f;
+            qq = q[s];
+            x0 = c0 - sources[s];
+            x1 = c1 - sources[sstride + s];
+            x2 = c2 - sources[2 * sstride + s];
         }
+        helm_layers<P>(x0, x1, x2, rscale, k, [&](auto sc, z2 v) {
+            constexpr int s = decltype(sc)::value;
+            T[s & 31][lane] = zmul(qq, v);
+            if ((s & 31) == 31 || s == N - 1) {
+                __syncwarp();
+                const int row = lane;
+                if ((s & ~31) + row <= s) {
+                    double sr = 0.0, si = 0.0;
+                    for (int l2 = 0; l2 < nsc; ++l2) {
+                        const z2 w = T[row][l2];
+                        sr += w.x;
+                        si += w.y;
+                    }
+                    acc[s >> 5] = zadd(acc[s >> 5], zmk(sr, si));
+                }
+                __syncwarp();
+            }
+        });
     }
+    z2 *o = out + (int64_t)(tb - tbase) * N;
 #pragma unroll
-    for (int u = 0; u < HP2L_MAXU; ++u) {
-        const int mi = lane + 32 * u;
-        if (mi >= n) break;
-        z2 &o = tgt[(int64_t)(tb - tbase) * n + mi];
-        o = zadd(o, acc[u]);
+    for (int m = 0; m < NPL; ++m) {
+        const int kk = lane + 32 * m;
+        if (kk < N) o[kk] = zadd(o[kk], acc[m]);
     }
+}
+
+template <int P>
+int launch_hm2p(double rscale, double k, int32_t ntgt_boxes, const int32_t *target_boxes,
+                const int32_t *src_starts, const int32_t *src_lists, const double *centers,
+                int64_t cstride, int32_t sbase, const z2 *src, const int32_t *bts,
+                const int32_t *btc, const double *targets, int64_t tstride, double scale,
+                z2 *result, cudaStream_t st)
+{
+    const int blocks = (ntgt_boxes + HM2P_WARPS - 1) / HM2P_WARPS;
+    hm2p_reg_kernel<P><<<blocks, 32 * HM2P_WARPS, 0, st>>>(
+        rscale, k, ntgt_boxes, target_boxes, src_starts, src_lists, centers, cstride, sbase, src,
+        bts, btc, targets, tstride, scale, result);
+    return check_launch("hm2p_reg_kernel");
+}
+
+template <int P>
+int launch_hp2l(double rscale, double k, int32_t ntgt_boxes, const int32_t *target_boxes,
+                const int32_t *src_starts, const int32_t *src_lists, const double *centers,
+                int64_t cstride, const int32_t *bss, const int32_t *bsc, const double *sources,
+                int64_t sstride, const z2 *q, int32_t tbase, z2 *out, cudaStream_t st)
+{
+    const int blocks = (ntgt_boxes + HP2L_WARPS - 1) / HP2L_WARPS;
+    hp2l_reg_kernel<P><<<blocks, 32 * HP2L_WARPS, 0, st>>>(
+        rscale, k, ntgt_boxes, target_boxes, src_starts, src_lists, centers, cstride, bss, bsc,
+        sources, sstride, q, tbase, out);
+    return check_launch("hp2l_reg_kernel");
 }
 
 // }}}
@@ -1044,16 +1160,13 @@ int sumpy_helmholtz_e2p_from_csr_f64(int order, double rscale, double k, int32_t
         !src_expansions || !box_target_starts || !box_target_counts_nonchild || !targets ||
         !result)
         return bad_arg("helmholtz m2p: null pointer argument");
-    const int P1 = order + 1;
-    const size_t smem = sizeof(double) * HM2P_WARPS * (2 * ncoeff_of(order) + 5 * P1 * 32);
-    int rc = prepare_smem(hm2p_kernel, smem);
-    if (rc) return rc;
-    const unsigned blocks = (unsigned)((ntgt_boxes + HM2P_WARPS - 1) / HM2P_WARPS);
-    hm2p_kernel<<<blocks, 32 * HM2P_WARPS, smem, as_stream(stream)>>>(
-        order, rscale, k, ntgt_boxes, target_boxes, source_box_starts, source_box_lists, centers,
-        center_stride, src_base_ibox, cz(src_expansions), box_target_starts,
-        box_target_counts_nonchild, targets, target_stride, scale, mz(result));
-    return check_launch("hm2p_kernel");
+#define CALL_HM2P(P)                                                                             \
+    launch_hm2p<P>(rscale, k, ntgt_boxes, target_boxes, source_box_starts, source_box_lists,     \
+                   centers, center_stride, src_base_ibox, cz(src_expansions), box_target_starts, \
+                   box_target_counts_nonchild, targets, target_stride, scale, mz(result),        \
+                   as_stream(stream))
+    SUMPY_ORDER_SWITCH(order, CALL_HM2P)
+#undef CALL_HM2P
 }
 
 int sumpy_helmholtz_p2e_from_csr_f64(int order, double rscale, double k, int32_t ntgt_boxes,
@@ -1072,16 +1185,13 @@ int sumpy_helmholtz_p2e_from_csr_f64(int order, double rscale, double k, int32_t
         !box_source_starts || !box_source_counts_nonchild || !sources || !strength ||
         !tgt_expansions)
         return bad_arg("helmholtz p2l: null pointer argument");
-    const int P1 = order + 1;
-    const size_t smem = sizeof(double) * HP2L_WARPS * 32 * (5 * P1 + 3);
-    int rc = prepare_smem(hp2l_kernel, smem);
-    if (rc) return rc;
-    const unsigned blocks = (unsigned)((ntgt_boxes + HP2L_WARPS - 1) / HP2L_WARPS);
-    hp2l_kernel<<<blocks, 32 * HP2L_WARPS, smem, as_stream(stream)>>>(
-        order, rscale, k, ntgt_boxes, target_boxes, source_box_starts, source_box_lists, centers,
-        center_stride, box_source_starts, box_source_counts_nonchild, sources, source_stride,
-        cz(strength), tgt_base_ibox, mz(tgt_expansions));
-    return check_launch("hp2l_kernel");
+#define CALL_HP2L(P)                                                                             \
+    launch_hp2l<P>(rscale, k, ntgt_boxes, target_boxes, source_box_starts, source_box_lists,     \
+                   centers, center_stride, box_source_starts, box_source_counts_nonchild,        \
+                   sources, source_stride, cz(strength), tgt_base_ibox, mz(tgt_expansions),      \
+                   as_stream(stream))
+    SUMPY_ORDER_SWITCH(order, CALL_HP2L)
+#undef CALL_HP2L
 }
 
 }  // extern "C"

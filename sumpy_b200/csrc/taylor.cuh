@@ -76,3 +76,16 @@ int prepare_smem(K kernel, size_t bytes)
 }
 
 }  // namespace sumpy
+
+// dispatch a runtime order to a template instantiation CALL(P), P = 0..16
+#define SUMPY_ORDER_SWITCH(p, CALL)                                                             \
+    switch (p) {                                                                               \
+    case 0: return CALL(0); case 1: return CALL(1); case 2: return CALL(2);                    \
+    case 3: return CALL(3); case 4: return CALL(4); case 5: return CALL(5);                    \
+    case 6: return CALL(6); case 7: return CALL(7); case 8: return CALL(8);                    \
+    case 9: return CALL(9); case 10: return CALL(10); case 11: return CALL(11);                \
+    case 12: return CALL(12); case 13: return CALL(13); case 14: return CALL(14);              \
+    case 15: return CALL(15); case 16: return CALL(16);                                        \
+    default: set_last_error("unsupported order"); return SUMPY_EUNSUPPORTED;                   \
+    }
+
