@@ -55,6 +55,11 @@ def parse():
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-problem batch")
     ap.add_argument("--no-helmholtz", action="store_true",
                     help="skip the 500k-point Helmholtz workload")
+    ap.add_argument("--only", choices=["mixed", "fp64", "batch", "helmholtz", "uniform"],
+                    help="run one workload alone (--steps/--warmup apply) and print its result; "
+                         "for profiling")
+    ap.add_argument("--helmholtz-npoints", type=int, default=500_000)
+    ap.add_argument("--helmholtz-precision", choices=["mixed", "fp64", "both"], default="both")
     return ap.parse_args()
 
 
@@ -250,9 +255,23 @@ def main():
         LinearPDEConformingVolumeTaylorMultipoleExpansion as MExp)
     from sumpy_b200.tree import build_all
 
+    if args.only in ("batch", "helmholtz", "uniform"):
+        if args.only == "batch":
+            res = batched_bench(dev, steps=args.steps, warmup=args.warmup)
+        elif args.only == "helmholtz":
+            precs = (("mixed", "fp64") if args.helmholtz_precision == "both"
+                     else (args.helmholtz_precision,))
+            res = helmholtz_bench(dev, steps=args.steps, warmup=args.warmup,
+                                  npoints=args.helmholtz_npoints, precisions=precs)
+        else:
+            res = uniform_bench(dev, steps=args.steps, warmup=args.warmup, cpu=False)
+        if rank == 0:
+            print(json.dumps({"only": args.only, "result": res}), flush=True)
+        return
+
     # cpu baseline first, before any process pool / GPU work competes for the host
     cpu_line = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.only is None:
         n, dt = cpu_fmm_rate(args.npoints, args.order, target_seconds=12.0)
         cores = os.cpu_count()
         cpu_line = {"value": n / dt / 1e6, "unit": "Mpts/s", "cores": cores, "kind": "port",
@@ -294,6 +313,16 @@ def main():
         barrier()
         ms = [a.elapsed_time(b) for a, b in evs]
         return max_over_ranks(sum(ms), device=dev) / steps, ms
+
+    if args.only in ("mixed", "fp64"):
+        w = wrangler(args.only)
+        for _ in range(max(1, args.warmup)):
+            drive_fmm(None, w, [q_dev])
+        ms, _ = timed(lambda: drive_fmm(None, w, [q_dev]), args.steps)
+        if rank == 0:
+            print(json.dumps({"only": args.only, "result": {
+                "ms_per_step": ms, "Mpts_s": args.npoints / (ms * 1e-3) / 1e6}}), flush=True)
+        return
 
     # setup (plans, tables) outside timing
     t0 = time.perf_counter()
@@ -623,7 +652,8 @@ def uniform_bench(dev, steps=5, warmup=3, n=20_000, order=6, cpu=True):
     return out
 
 
-def helmholtz_bench(dev, steps=3, warmup=2, npoints=500_000, order=14, k=10.0):
+def helmholtz_bench(dev, steps=3, warmup=2, npoints=500_000, order=14, k=10.0,
+                    precisions=("mixed", "fp64")):
     """3D Helmholtz (G = e^{ikr}/r, k = 10): 500k points on the unit sphere
     (sources = targets, exclude_self), strengths N(0,1) + i N(0,1), p = 14,
     max 32 per box. Mixed (complex64 near field on FP64 offsets, split-TF32
@@ -672,7 +702,7 @@ def helmholtz_bench(dev, steps=3, warmup=2, npoints=500_000, order=14, k=10.0):
     out = {"workload": f"unit sphere n={npoints}, k={k}, p={order}, complex strengths, "
                        f"exclude_self, max {MAX_PARTICLES} per box",
            "tree_build_s": round(t_tree, 3), "m2l_entries": int(len(trav.from_sep_siblings_lists))}
-    for precision in ("mixed", "fp64"):
+    for precision in precisions:
         t0 = time.perf_counter()
         w = SumpyExpansionWrangler(ti, trav, np.complex128, lambda *a: order,
                                    kernel_extra_kwargs={"k": k}, translation_classes_data=tcls,
@@ -691,7 +721,8 @@ def helmholtz_bench(dev, steps=3, warmup=2, npoints=500_000, order=14, k=10.0):
             out["stage_ms_mixed"], _ = stage_breakdown(w, trav, qd, dev, roofline=False)
         del w
         torch.cuda.empty_cache()
-    out["mixed_over_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    if "fp64" in out and "mixed" in out:
+        out["mixed_over_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
     return out
 
 
