@@ -803,9 +803,19 @@ def stage_breakdown(w, trav, q_dev, dev, roofline=True):
         "frac": ach / peak, "traffic": None,
         "peak_source": "MEASURED_PEAKS.json bf16_tflops (of measured)" if peaks else "fallback",
         "work": work[dom],
-        "note": "FP64/FP32 CUDA-core kernel: its own pipe peak is below the bf16 "
-                "tensor figure used as the denominator",
     }
+    if dom == "m2l" and w.precision == "mixed":
+        roof["note"] = ("tcgen05 split-TF32 GEMM; algorithmic flops = 2 n^2 per List-2 entry "
+                        "(not the x3 split products, empty slots or padding); the stage time "
+                        "includes the TF32 split pre-pass (~1.4 % of it)")
+        if tree.nsources == NPOINTS and n == (ORDER + 1) ** 2:
+            # dram__bytes_read.sum + dram__bytes_write.sum of this launch on this workload,
+            # one ncu capture: profiles/m2l_tf32x3_sphere_plummer_1M_p10.md
+            roof["traffic"] = 1.227e9 + 0.195e9
+            roof["traffic_unit"] = "bytes per launch (ncu capture)"
+    else:
+        roof["note"] = ("CUDA-core kernel: its own pipe peak is below the bf16 tensor figure "
+                        "used as the denominator")
     return stage, roof
 
 
