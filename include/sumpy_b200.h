@@ -318,6 +318,26 @@ int sumpy_e2p_from_csr_grad_f64(
     const double *targets, int64_t target_stride, double scale, double *result,
     double *grad, void *stream);
 
+/* Mixed-precision E2PFromCSR (List 3) and P2EFromCSR (List 4) for the mixed
+ * form: FP64 offsets rounded to FP32, derivative recurrence and products in
+ * FP32 per source box / source, FP64 sums. Arguments as the _f64 entries. */
+int sumpy_e2p_from_csr_mixed(
+    int order, double rscale, int32_t ntgt_boxes, const int32_t *target_boxes,
+    const int32_t *source_box_starts, const int32_t *source_box_lists,
+    const double *centers, int64_t center_stride,
+    int32_t src_base_ibox, const double *src_expansions,
+    const int32_t *box_target_starts, const int32_t *box_target_counts_nonchild,
+    const double *targets, int64_t target_stride, double scale, double *result,
+    void *stream);
+
+int sumpy_p2e_from_csr_mixed(
+    int order, double rscale, int32_t ntgt_boxes, const int32_t *target_boxes,
+    const int32_t *source_box_starts, const int32_t *source_box_lists,
+    const double *centers, int64_t center_stride,
+    const int32_t *box_source_starts, const int32_t *box_source_counts_nonchild,
+    const double *sources, int64_t source_stride, const double *strength,
+    int32_t tgt_base_ibox, double *tgt_expansions, void *stream);
+
 /* ------------------------------------------------------------------------
  * 3D Helmholtz kernel G = exp(i k r) / r (sumpy/kernel.py:755-844), the same
  * loopy kernels as above instantiated for HelmholtzKernel(3): complex data

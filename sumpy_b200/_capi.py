@@ -54,6 +54,10 @@ SIGNATURES = {
                                       ptr, i64, dbl, ptr, ptr],
     "sumpy_e2p_from_csr_f64": [cint, dbl, i32, ptr, ptr, ptr, ptr, i64, i32, ptr, ptr, ptr,
                                ptr, i64, dbl, ptr, ptr],
+    "sumpy_e2p_from_csr_mixed": [cint, dbl, i32, ptr, ptr, ptr, ptr, i64, i32, ptr, ptr, ptr,
+                                 ptr, i64, dbl, ptr, ptr],
+    "sumpy_p2e_from_csr_mixed": [cint, dbl, i32, ptr, ptr, ptr, ptr, i64, ptr, ptr, ptr,
+                                 i64, ptr, i32, ptr, ptr],
     # Helmholtz
     "sumpy_helmholtz_p2p_from_csr_f64": [i32, ptr, ptr, ptr, ptr, ptr, ptr, ptr, ptr, i64, dbl,
                                          ptr, ptr, i64, ptr, dbl, ptr, ptr],

@@ -545,6 +545,111 @@ p2l_reg_kernel(double rscale, int32_t ntgt_boxes, const int32_t *__restrict__ ta
     }
 }
 
+// Mixed-precision M2P / P2L: the FP64 offset (target - center,
+// center - source) rounded to FP32, the derivative layers and the products
+// with the coefficients in FP32, per List-3 box / per source; sums over
+// boxes (M2P) and sources (P2L) in FP64.
+template <int P>
+__global__ void __launch_bounds__(32 * E2P_WARPS)
+m2p_mixed_kernel(double rscale, int32_t ntgt_boxes, const int32_t *__restrict__ target_boxes,
+                 const int32_t *__restrict__ src_starts, const int32_t *__restrict__ src_lists,
+                 const double *__restrict__ centers, int64_t cstride, int32_t sbase,
+                 const double *__restrict__ src, const int32_t *__restrict__ bts,
+                 const int32_t *__restrict__ btc, const double *__restrict__ targets,
+                 int64_t tstride, double scale, double *__restrict__ result)
+{
+    constexpr int N = (P + 1) * (P + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ib = blockIdx.x * E2P_WARPS + warp;
+    if (ib >= ntgt_boxes) return;
+    const int32_t tb = target_boxes[ib];
+    const int32_t t0 = bts[tb], nt = btc[tb];
+    const int32_t ls = src_starts[ib], le = src_starts[ib + 1];
+    const float R = (float)rscale, Rinv = (float)(1.0 / rscale);
+    for (int32_t tc = 0; tc < nt; tc += 32) {
+        const int ntc = min(32, nt - tc);
+        int g = 1;
+        while (g < ntc) g <<= 1;
+        const int nph = 32 / g;
+        const int tl = lane & (g - 1), ph = lane / g;
+        const bool active = tl < ntc;
+        const int32_t t = t0 + tc + tl;
+        double tx = 0, ty = 0, tz = 0;
+        if (active) { tx = targets[t]; ty = targets[tstride + t]; tz = targets[2 * tstride + t]; }
+        double acc = 0.0;
+        if (active) {
+            for (int32_t l = ls + ph; l < le; l += nph) {
+                const int32_t sb = src_lists[l];
+                const double *M = src + (int64_t)(sb - sbase) * N;
+                float accf = 0.f;
+                laplace_layers<P, float>(
+                    (float)(tx - centers[sb]), (float)(ty - centers[cstride + sb]),
+                    (float)(tz - centers[2 * cstride + sb]), R, Rinv,
+                    [&](int s, int, int, int, float v) { accf = fmaf((float)__ldg(M + s), v, accf); });
+                acc += (double)accf;
+            }
+        }
+        for (int off = g; off < 32; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+        if (active && ph == 0) result[t] += scale * acc;
+    }
+}
+
+template <int P>
+__global__ void __launch_bounds__(32 * P2L_WARPS)
+p2l_mixed_kernel(double rscale, int32_t ntgt_boxes, const int32_t *__restrict__ target_boxes,
+                 const int32_t *__restrict__ src_starts, const int32_t *__restrict__ src_lists,
+                 const double *__restrict__ centers, int64_t cstride,
+                 const int32_t *__restrict__ bss, const int32_t *__restrict__ bsc,
+                 const double *__restrict__ sources, int64_t sstride, const double *__restrict__ q,
+                 int32_t tbase, double *__restrict__ out)
+{
+    constexpr int N = (P + 1) * (P + 1);
+    constexpr int NPL = (N + 31) / 32;
+    extern __shared__ float smf[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ib = blockIdx.x * P2L_WARPS + warp;
+    if (ib >= ntgt_boxes) return;
+    float *D = smf + warp * (N * DSTRIDE);
+    const int32_t tb = target_boxes[ib];
+    const double c0 = centers[tb], c1 = centers[cstride + tb], c2 = centers[2 * cstride + tb];
+    const int32_t ls = src_starts[ib], le = src_starts[ib + 1];
+    const float R = (float)rscale, Rinv = (float)(1.0 / rscale);
+    int32_t total = 0;
+    for (int32_t l = ls; l < le; ++l) total += bsc[src_lists[l]];
+    double acc[NPL];
+#pragma unroll
+    for (int m = 0; m < NPL; ++m) acc[m] = 0.0;
+    for (int32_t base = 0; base < total; base += 32) {
+        const int nsc = min(32, total - base);
+        if (lane < nsc) {
+            int32_t f = base + lane, l = ls, sb = src_lists[ls];
+            while (f >= bsc[sb]) { f -= bsc[sb]; ++l; sb = src_lists[l]; }
+            const int32_t s = bss[sb] + f;
+            const float qq = (float)q[s];
+            laplace_layers<P, float>((float)(c0 - sources[s]), (float)(c1 - sources[sstride + s]),
+                                     (float)(c2 - sources[2 * sstride + s]), R, Rinv,
+                                     [&](int k, int, int, int, float v) { D[k * DSTRIDE + lane] = qq * v; });
+        }
+        __syncwarp();
+#pragma unroll
+        for (int m = 0; m < NPL; ++m) {
+            const int k = lane + 32 * m;
+            if (k < N) {
+                float sum = 0.f;
+                for (int l2 = 0; l2 < nsc; ++l2) sum += D[k * DSTRIDE + l2];
+                acc[m] += (double)sum;
+            }
+        }
+        __syncwarp();
+    }
+    double *o = out + (int64_t)(tb - tbase) * N;
+#pragma unroll
+    for (int m = 0; m < NPL; ++m) {
+        const int k = lane + 32 * m;
+        if (k < N) o[k] = acc[m];
+    }
+}
+
 template <int P, bool GRAD>
 int launch_m2p_reg(double rscale, int32_t ntgt_boxes, const int32_t *target_boxes,
                    const int32_t *src_starts, const int32_t *src_lists, const double *centers,
@@ -808,6 +913,62 @@ int sumpy_p2e_from_csr_f64(int order, double rscale, int32_t ntgt_boxes,
                       as_stream(stream))
     SUMPY_ORDER_SWITCH(order, CALL_P2L)
 #undef CALL_P2L
+}
+
+int sumpy_e2p_from_csr_mixed(int order, double rscale, int32_t ntgt_boxes,
+                             const int32_t *target_boxes, const int32_t *source_box_starts,
+                             const int32_t *source_box_lists, const double *centers,
+                             int64_t center_stride, int32_t src_base_ibox,
+                             const double *src_expansions, const int32_t *box_target_starts,
+                             const int32_t *box_target_counts_nonchild, const double *targets,
+                             int64_t target_stride, double scale, double *result, void *stream)
+{
+    if (!order_ok(order)) { set_last_error("m2p mixed: unsupported order"); return SUMPY_EUNSUPPORTED; }
+    if (ntgt_boxes < 0) return bad_arg("m2p mixed: ntgt_boxes < 0");
+    if (ntgt_boxes == 0) return SUMPY_OK;
+    if (!target_boxes || !source_box_starts || !source_box_lists || !centers ||
+        !src_expansions || !box_target_starts || !box_target_counts_nonchild || !targets || !result)
+        return bad_arg("m2p mixed: null pointer argument");
+    const int blocks = (ntgt_boxes + E2P_WARPS - 1) / E2P_WARPS;
+#define CALL_M2PM(P)                                                                             \
+    (m2p_mixed_kernel<P><<<blocks, 32 * E2P_WARPS, 0, as_stream(stream)>>>(                     \
+         rscale, ntgt_boxes, target_boxes, source_box_starts, source_box_lists, centers,        \
+         center_stride, src_base_ibox, src_expansions, box_target_starts,                       \
+         box_target_counts_nonchild, targets, target_stride, scale, result),                    \
+     check_launch("m2p_mixed_kernel"))
+    SUMPY_ORDER_SWITCH(order, CALL_M2PM)
+#undef CALL_M2PM
+}
+
+int sumpy_p2e_from_csr_mixed(int order, double rscale, int32_t ntgt_boxes,
+                             const int32_t *target_boxes, const int32_t *source_box_starts,
+                             const int32_t *source_box_lists, const double *centers,
+                             int64_t center_stride, const int32_t *box_source_starts,
+                             const int32_t *box_source_counts_nonchild, const double *sources,
+                             int64_t source_stride, const double *strength,
+                             int32_t tgt_base_ibox, double *tgt_expansions, void *stream)
+{
+    if (!order_ok(order)) { set_last_error("p2l mixed: unsupported order"); return SUMPY_EUNSUPPORTED; }
+    if (ntgt_boxes < 0) return bad_arg("p2l mixed: ntgt_boxes < 0");
+    if (ntgt_boxes == 0) return SUMPY_OK;
+    if (!target_boxes || !source_box_starts || !source_box_lists || !centers ||
+        !box_source_starts || !box_source_counts_nonchild || !sources || !strength ||
+        !tgt_expansions)
+        return bad_arg("p2l mixed: null pointer argument");
+    const int blocks = (ntgt_boxes + P2L_WARPS - 1) / P2L_WARPS;
+#define CALL_P2LM(P)                                                                             \
+    (prepare_smem(p2l_mixed_kernel<P>,                                                           \
+                  sizeof(float) * (P + 1) * (P + 1) * DSTRIDE * P2L_WARPS)                       \
+         ? SUMPY_ELAUNCH                                                                         \
+         : (p2l_mixed_kernel<P><<<blocks, 32 * P2L_WARPS,                                        \
+                                  sizeof(float) * (P + 1) * (P + 1) * DSTRIDE * P2L_WARPS,       \
+                                  as_stream(stream)>>>(                                          \
+                rscale, ntgt_boxes, target_boxes, source_box_starts, source_box_lists, centers, \
+                center_stride, box_source_starts, box_source_counts_nonchild, sources,          \
+                source_stride, strength, tgt_base_ibox, tgt_expansions),                        \
+            check_launch("p2l_mixed_kernel")))
+    SUMPY_ORDER_SWITCH(order, CALL_P2LM)
+#undef CALL_P2LM
 }
 
 }  // extern "C"

@@ -271,3 +271,103 @@ def real_embedding(T):
     return R.reshape(c, 2 * n, 2 * n)
 
 # }}}
+
+
+# {{{ M2M / L2L as dense per-octant operators
+
+def _full_index_map(p):
+    ids = full_ids(p)
+    return {mi: f for f, mi in enumerate(ids)}, ids
+
+
+def _shift_axis(V, p, ids, fidx, axis, dd, truncate_to=None):
+    """Taylor shift of full coefficient columns V[full, cols] along one axis:
+    multipole form out[mi] = sum_{q <= mi_a} V[mi with mi_a = q] dd^(mi_a - q)/(mi_a - q)!
+    (truncate_to is None), local form out[mi] = sum_{q <= P - |mi|}
+    V[mi + q e_a] dd^q / q! (truncate_to = P)."""
+    from math import factorial
+    out = np.zeros_like(V)
+    for f, mi in enumerate(ids):
+        if truncate_to is None:
+            for q in range(mi[axis] + 1):
+                m = list(mi); m[axis] = q
+                out[f] += V[fidx[tuple(m)]] * dd ** (mi[axis] - q) / factorial(mi[axis] - q)
+        else:
+            deg = sum(mi)
+            for q in range(truncate_to - deg + 1):
+                m = list(mi); m[axis] += q
+                out[f] += V[fidx[tuple(m)]] * dd ** q / factorial(q)
+    return out
+
+
+def _project(V, p, ids, fidx, kappa=0.0):
+    """stored-embedded full columns -> full (the PDE projection, planes in order)."""
+    V = V.copy()
+    for f, mi in enumerate(ids):
+        if mi[0] >= 2:
+            i, j, k = mi
+            V[f] = (-V[fidx[(i - 2, j + 2, k)]] - V[fidx[(i - 2, j, k + 2)]]
+                    - kappa * V[fidx[(i - 2, j, k)]])
+    return V
+
+
+def _compress(V, p, ids, fidx, kappa=0.0):
+    """full columns -> stored rows (transposed projection, rows in reverse)."""
+    V = V.copy()
+    for f in range(len(ids) - 1, -1, -1):
+        i, j, k = ids[f]
+        if i >= 2:
+            V[fidx[(i - 2, j + 2, k)]] -= V[f]
+            V[fidx[(i - 2, j, k + 2)]] -= V[f]
+            V[fidx[(i - 2, j, k)]] -= kappa * V[f]
+    return V[[fidx[mi] for mi in stored_ids(p)]]
+
+
+def m2m_operator(order, src_rscale, tgt_rscale, dvec, kappa=0.0):
+    """Dense M2M map [n_tgt, n_src] for one child -> parent offset
+    ``dvec`` = parent center - child center: the child's stored coefficients
+    in the parent's full slots times (r_src/r_tgt)^|mi|, shifted along axes
+    1, 2, 0 by dvec/r_tgt, then compressed (sumpy/expansion/multipole.py:
+    159-407). kappa = k^2 r_tgt^2 for Helmholtz."""
+    p = order
+    fidx, ids = _full_index_map(p)
+    st = stored_ids(p)
+    n = len(st)
+    V = np.zeros((len(ids), n))
+    ratio = src_rscale / tgt_rscale
+    for s, mi in enumerate(st):
+        V[fidx[mi], s] = ratio ** sum(mi)
+    for axis in (1, 2, 0):
+        V = _shift_axis(V, p, ids, fidx, axis, dvec[axis] / tgt_rscale)
+    return _compress(V, p, ids, fidx, kappa)
+
+
+def l2l_operator(order, src_rscale, tgt_rscale, dvec, kappa=0.0):
+    """Dense L2L map [n_tgt, n_src] for one parent -> child offset ``dvec`` =
+    child center - parent center: full derivatives from the stored ones
+    (projection at r_src, kappa = k^2 r_src^2 for Helmholtz), truncated
+    Taylor shift along axes 0, 1, 2 by dvec/r_src, times (r_tgt/r_src)^|mi|
+    on the stored entries (sumpy/expansion/local.py:346-464)."""
+    p = order
+    fidx, ids = _full_index_map(p)
+    st = stored_ids(p)
+    n = len(st)
+    V = np.zeros((len(ids), n))
+    for s, mi in enumerate(st):
+        V[fidx[mi], s] = 1.0
+    V = _project(V, p, ids, fidx, kappa)
+    for axis in (0, 1, 2):
+        V = _shift_axis(V, p, ids, fidx, axis, dvec[axis] / src_rscale, truncate_to=p)
+    ratio = tgt_rscale / src_rscale
+    rows = np.array([fidx[mi] for mi in st])
+    deg = np.array([sum(mi) for mi in st])
+    return V[rows] * (ratio ** deg)[:, None]
+
+
+def octant_offsets(h_child):
+    """The 8 child-center offsets from the parent center, octant o = 4 bx + 2 by + bz
+    (bit set = + side), for children of side h_child."""
+    return np.array([[(1 if (o >> (2 - a)) & 1 else -1) * 0.5 * h_child for a in range(3)]
+                     for o in range(8)])
+
+# }}}

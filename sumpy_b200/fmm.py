@@ -13,9 +13,9 @@ per expansion kind, level-major, each level a row-major
 ``(nboxes_level, ncoeff)`` block.
 
 Beyond sumpy's knobs, the wrangler takes ``precision``: ``"fp64"`` (every
-stage in FP64) or ``"mixed"`` (FP32 near field with FP64 offsets and sums;
-M2L as split-FP32 (3xTF32) GEMMs on the tcgen05 tensor cores with FP32
-accumulation and FP64 results; the other stages FP64), ``gradient`` (also
+stage in FP64) or ``"mixed"`` (FP32 near field, M2P and P2L with FP64
+offsets and sums; M2L and M2M as split-FP32 (3xTF32) GEMMs on the tcgen05
+tensor cores with FP32 accumulation and FP64 results; the other stages FP64), ``gradient`` (also
 return the potential's gradient at the targets) and ``m2l_item_groups`` (class
 groups per M2L work item, one CTA each; :mod:`sumpy_b200.autotune` picks it).
 """
@@ -31,7 +31,10 @@ from sumpy_b200 import _capi
 from sumpy_b200._capi import call, dptr, stream_ptr
 from sumpy_b200.expansion import (
     helmholtz_m2l_class_matrices,
+    l2l_operator,
     m2l_class_matrices,
+    m2m_operator,
+    octant_offsets,
     real_embedding,
 )
 from sumpy_b200.kernel import HelmholtzKernel, helmholtz_k, is_scale_invariant
@@ -150,6 +153,12 @@ class SumpyExpansionWrangler:
         self._m2l_tc_mats = {}
         self._m2l_ws = None
         self._status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        # mixed form: M2M as a tensor-core GEMM; L2L as an FP64 GEMM (the
+        # 3xTF32 L2L compounds its FP32 group sums down the levels: ~3x the
+        # mixed form's error on the 1M-point benchmark; see _tc_translations)
+        self.tc_m2m = True
+        self.tc_l2l = False
+        self.gemm_l2l = False
         self.m2l_item_groups = int(m2l_item_groups or M2L_ITEM_GROUPS)
         if self.m2l_item_groups < 1:
             raise ValueError("m2l_item_groups must be >= 1")
@@ -311,6 +320,9 @@ class SumpyExpansionWrangler:
 
     def coarsen_multipoles(self, actx, level_start_source_parent_box_nrs,
                            source_parent_boxes, mpoles):
+        if self._tc_translations and self.tc_m2m:
+            return self._coarsen_tc(level_start_source_parent_box_nrs, source_parent_boxes,
+                                    mpoles)
         lsp = _np_i32(level_start_source_parent_box_nrs)
         boxes = self._dev(source_parent_boxes)
         g = self._geom
@@ -641,6 +653,147 @@ class SumpyExpansionWrangler:
         self._call_m2l_tc(self.level_orders[lev], items, hi, lo, rp, kp, nb + 1,
                           sbase, ws_hi, ws_lo, tbase, tview, st)
 
+    # {{{ M2M / L2L as per-octant GEMMs on the tensor cores (mixed form)
+
+    @cached_property
+    def _tc_translations(self):
+        """Mixed Laplace form with one order on every level: M2M and L2L are
+        then the same eight dense maps (one per child octant) on every level
+        (rscale ratio 1/2 and offset/rscale = order/8 do not depend on the
+        level), applied as grouped GEMMs by the tensor-core kernel."""
+        return (self.precision == "mixed" and not self.helmholtz
+                and len(set(self.level_orders)) == 1)
+
+    def _octant_operator_planes(self, kind):
+        key = ("octant-ops", kind)
+        if key not in self._m2l_tc_mats:
+            order = self.level_orders[0]
+            # any level pair gives the same maps; take levels 2 -> 3 (rscale as
+            # level_to_rscale, sumpy/fmm.py:369-386)
+            r_par = self.tree.root_extent * 2.0 ** -2 * 2 / order
+            r_ch = self.tree.root_extent * 2.0 ** -3 * 2 / order
+            h_ch = self.tree.root_extent * 2.0 ** -3
+            offs = octant_offsets(h_ch)          # child center - parent center
+            if kind == "m2m":
+                ops = [m2m_operator(order, r_ch, r_par, -offs[o]) for o in range(8)]
+            else:
+                ops = [l2l_operator(order, r_par, r_ch, offs[o]) for o in range(8)]
+            mats = torch.as_tensor(np.stack(ops)).to(self.device)
+            hi, lo, rp, kp = self._m2l_tc_operands(mats)
+            self._m2l_tc_mats[key] = (mats, hi, lo, rp, kp)
+        return self._m2l_tc_mats[key]
+
+    def _octants(self, boxes):
+        c = self.tree.box_coords[:, boxes]
+        return ((c[0] & 1) * 4 + (c[1] & 1) * 2 + (c[2] & 1)).astype(np.int32)
+
+    def _octant_plan(self, key, targets, sources, tw=M2L_TILE_TC):
+        """GEMM schedule for per-octant maps: ``targets`` (box ids) in tiles of
+        ``tw`` (128 for the tensor cores, 64 for the FP64 GEMM), one group per
+        octant present in a tile, ``sources[o][i]`` the source box of target i
+        for octant o (-1 = none)."""
+        if key in self._m2l_plans:
+            return self._m2l_plans[key]
+        nt = len(targets)
+        ntiles = (nt + tw - 1) // tw
+        tile_targets = np.full(ntiles * tw, -1, dtype=np.int32)
+        tile_targets[:nt] = targets
+        src = np.full((8, ntiles * tw), -1, dtype=np.int32)
+        src[:, :nt] = sources
+        groups, classes, tiles = [], [], []
+        for t in range(ntiles):
+            g0 = len(groups)
+            blk = src[:, t * tw:(t + 1) * tw]
+            for o in range(8):
+                if (blk[o] >= 0).any():
+                    groups.append(blk[o])
+                    classes.append(o)
+            tiles.append((g0, len(groups)))
+        it_tile, it_g0, it_g1 = self._tc_items(tiles)
+        dev = self.device
+        plan = {
+            "nitems": len(it_tile), "nclasses": 8,
+            "item_tile": torch.as_tensor(it_tile).to(dev),
+            "item_g0": torch.as_tensor(it_g0).to(dev),
+            "item_g1": torch.as_tensor(it_g1).to(dev),
+            "tile_targets": torch.as_tensor(tile_targets).to(dev),
+            "tile_scale": torch.ones(ntiles, dtype=torch.float64, device=dev),
+            "group_class": torch.as_tensor(np.array(classes, dtype=np.int32)).to(dev),
+            "group_sources": torch.as_tensor(
+                np.stack(groups).astype(np.int32).ravel() if groups
+                else np.zeros(0, dtype=np.int32)).to(dev),
+        }
+        self._m2l_plans[key] = plan
+        return plan
+
+    def _octant_gemm(self, kind, plan, sview, sbase, tview, tbase, st, fp64=False):
+        mats, hi, lo, rp, kp = self._octant_operator_planes(kind)
+        if fp64:
+            self._call_m2l_f64(self.level_orders[0], plan, mats, sbase, sview, tbase, tview,
+                               st)
+            return
+        nb, n = sview.shape
+        ws_hi, ws_lo = self._m2l_workspace(nb, kp)
+        call("sumpy_split_tf32x2", _i64(nb), _i32(1), _i32(n), dptr(sview), _i32(1),
+             _i32(kp), dptr(ws_hi), dptr(ws_lo), st)
+        self._call_m2l_tc(self.level_orders[0], plan, hi, lo, rp, kp, nb + 1, sbase,
+                          ws_hi, ws_lo, tbase, tview, st)
+
+    def _coarsen_tc(self, level_start_source_parent_box_nrs, source_parent_boxes, mpoles):
+        lsp = _np_i32(level_start_source_parent_box_nrs)
+        parents_all = _np_i32(source_parent_boxes)
+        child = np.asarray(self.tree.box_child_ids)
+        st = stream_ptr()
+        for src_lev in range(self.tree.nlevels - 1, 2, -1):
+            tgt_lev = src_lev - 1
+            a, b = int(lsp[tgt_lev]), int(lsp[tgt_lev + 1])
+            if a == b:
+                continue
+            key = ("m2m-plan", tgt_lev, id(source_parent_boxes))
+            if key not in self._m2l_plans:
+                parents = parents_all[a:b]
+                kids = child[:, parents]                       # [slot][parent]
+                srcs = np.full((8, len(parents)), -1, dtype=np.int32)
+                for slot in range(kids.shape[0]):
+                    ch = kids[slot]
+                    has = ch > 0
+                    oc = self._octants(ch[has])
+                    srcs[oc, np.nonzero(has)[0]] = ch[has]
+                self._octant_plan(key, parents, srcs)
+            plan = self._m2l_plans[key]
+            sbase, sview = self.multipole_expansions_view(mpoles, src_lev)
+            tbase, tview = self.multipole_expansions_view(mpoles, tgt_lev)
+            self._octant_gemm("m2m", plan, sview, sbase, tview, tbase, st)
+        return mpoles
+
+    def _refine_tc(self, level_start_target_or_target_parent_box_nrs,
+                   target_or_target_parent_boxes, local_exps, fp64=False):
+        lt = _np_i32(level_start_target_or_target_parent_box_nrs)
+        boxes_all = _np_i32(target_or_target_parent_boxes)
+        parent = np.asarray(self.tree.box_parent_ids)
+        st = stream_ptr()
+        for tgt_lev in range(1, self.tree.nlevels):
+            a, b = int(lt[tgt_lev]), int(lt[tgt_lev + 1])
+            if a == b:
+                continue
+            key = ("l2l-plan", tgt_lev, id(target_or_target_parent_boxes), fp64)
+            if key not in self._m2l_plans:
+                kids = boxes_all[a:b]
+                oc = self._octants(kids)
+                order = np.argsort(oc, kind="stable")   # octant-pure tiles
+                kids, oc = kids[order], oc[order]
+                srcs = np.full((8, len(kids)), -1, dtype=np.int32)
+                srcs[oc, np.arange(len(kids))] = parent[kids]
+                self._octant_plan(key, kids, srcs, M2L_TILE if fp64 else M2L_TILE_TC)
+            plan = self._m2l_plans[key]
+            src_lev = tgt_lev - 1
+            sbase, sview = self.local_expansions_view(local_exps, src_lev)
+            tbase, tview = self.local_expansions_view(local_exps, tgt_lev)
+            self._octant_gemm("l2l", plan, sview, sbase, tview, tbase, st, fp64=fp64)
+        return local_exps
+
+    # }}}
+
     def check_status(self):
         """Raise if a kernel reported an internal error (synchronises)."""
         code = int(self._status.item())
@@ -668,6 +821,8 @@ class SumpyExpansionWrangler:
                     dptr(pot[0]))
             if self.gradient:
                 call("sumpy_e2p_from_csr_grad_f64", *args, dptr(pot[1]), st)
+            elif self.precision == "mixed" and not self.helmholtz:
+                call("sumpy_e2p_from_csr_mixed", *args, st)
             else:
                 call(self._entry("sumpy_e2p_from_csr_f64"), *args, st)
         return pot
@@ -689,7 +844,9 @@ class SumpyExpansionWrangler:
             if a == b or starts_h[a] == starts_h[b]:
                 continue
             tbase, tview = self.local_expansions_view(local_exps, lev)
-            call(self._entry("sumpy_p2e_from_csr_f64"), _c(self.level_orders[lev]),
+            name = ("sumpy_p2e_from_csr_mixed" if self.precision == "mixed" and not self.helmholtz
+                    else self._entry("sumpy_p2e_from_csr_f64"))
+            call(name, _c(self.level_orders[lev]),
                  _d(self.level_to_rscale(lev)), *self._kargs, _i32(b - a), dptr(boxes[a:b]),
                  dptr(starts_d[a:b + 1]), dptr(lists_d), dptr(g["centers"]),
                  _i64(self.tree.nboxes), dptr(g["bss"]), dptr(g["bsc"]), dptr(g["sources"]),
@@ -698,6 +855,10 @@ class SumpyExpansionWrangler:
 
     def refine_locals(self, actx, level_start_target_or_target_parent_box_nrs,
                       target_or_target_parent_boxes, local_exps):
+        if self._tc_translations and (self.tc_l2l or self.gemm_l2l):
+            return self._refine_tc(level_start_target_or_target_parent_box_nrs,
+                                   target_or_target_parent_boxes, local_exps,
+                                   fp64=not self.tc_l2l)
         lt = _np_i32(level_start_target_or_target_parent_box_nrs)
         boxes = self._dev(target_or_target_parent_boxes)
         g = self._geom

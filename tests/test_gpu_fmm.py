@@ -224,3 +224,33 @@ def test_mixed_fmm_matches_fp64_fmm(cuda_device):
     pmx = drive_fmm(None, wmx, [qd])[0].cpu()
     wmx.check_status()
     assert relerr(pmx, p64) < 1e-6
+
+
+@pytest.mark.parametrize("geom", list(GEOMS))
+@pytest.mark.parametrize("order", [4, 10])
+def test_tensor_core_m2m_l2l_match_fp64(cuda_device, geom, order):
+    """Mixed form: M2M and L2L as per-octant 3xTF32 GEMMs against the FP64
+    shift kernels on the same inputs."""
+    src, tgt, tree, trav, tcls, q = _setup(geom)
+    excl = tgt is None
+    w64 = make_wrangler(tree, trav, order, exclude_self=excl)
+    wtc = make_wrangler(tree, trav, order, exclude_self=excl, precision="mixed")
+    assert wtc._tc_translations
+    qd = w64.reorder_sources(torch.as_tensor(q, device=cuda_device))
+    mp = w64.form_multipoles(None, trav.level_start_source_box_nrs, trav.source_boxes, [qd])
+    m64 = w64.coarsen_multipoles(None, trav.level_start_source_parent_box_nrs,
+                                 trav.source_parent_boxes, mp.clone())
+    mtc = wtc.coarsen_multipoles(None, trav.level_start_source_parent_box_nrs,
+                                 trav.source_parent_boxes, mp.clone())
+    wtc.check_status()
+    assert relerr(mtc.cpu(), m64.cpu()) < 1e-6
+    loc = w64.multipole_to_local(None, trav.level_start_target_or_target_parent_box_nrs,
+                                 trav.target_or_target_parent_boxes,
+                                 trav.from_sep_siblings_starts, trav.from_sep_siblings_lists,
+                                 m64)
+    args = (None, trav.level_start_target_or_target_parent_box_nrs,
+            trav.target_or_target_parent_boxes)
+    l64 = w64.refine_locals(*args, loc.clone())
+    ltc = wtc.refine_locals(*args, loc.clone())
+    wtc.check_status()
+    assert relerr(ltc.cpu(), l64.cpu()) < 1e-6
