@@ -2,22 +2,47 @@
 
 sumpy's wrangler is driven by ``boxtree.fmm.drive_fmm`` (called at
 sumpy/test/test_fmm.py:280-282), which is outside the sumpy sources. This
-function issues the same wrangler calls in the same order, with the same
-traversal fields (the order sumpy's wrangler documents,
+function issues the same wrangler calls with the same traversal fields and
+returns the same result (the order sumpy's wrangler documents,
 sumpy/fmm.py:609-1086):
 
 reorder_sources -> form_multipoles (P2M) -> coarsen_multipoles (M2M) ->
 eval_direct (List 1) -> multipole_to_local (List 2) -> eval_multipoles
 (List 3) -> form_locals (List 4) -> refine_locals (L2L) -> eval_locals (L2P)
 -> reorder_potentials -> finalize_potentials.
+
+On a CUDA wrangler the stages that do not depend on the multipole chain run
+on a second stream: List 1 and List 4 need only the strengths, List 3 only
+the finished multipoles, so they overlap P2M, M2M and M2L (whose coarse
+levels leave most SMs idle). The side stream forks from the caller's stream
+after the strengths are reordered and joins it before the first use of its
+results; the returned potentials are ordered on the caller's stream like
+every other result, and the whole sequence can be captured in a CUDA graph.
 """
 from __future__ import annotations
+
+
+def _side_stream(wrangler):
+    import torch
+    dev = getattr(wrangler, "device", None)
+    if dev is None or getattr(dev, "type", None) != "cuda" or not getattr(
+            wrangler, "concurrent_stages", False):
+        return None
+    s = getattr(wrangler, "_side_stream", None)
+    if s is None:
+        s = torch.cuda.Stream(dev)
+        wrangler._side_stream = s
+    return s
 
 
 def drive_fmm(actx, wrangler, src_weight_vecs, timing_data=None):
     trav = wrangler.traversal
     src_weight_vecs = [wrangler.reorder_sources(w) for w in src_weight_vecs]
     src_weight_vecs = wrangler.distribute_source_weights(src_weight_vecs)
+
+    side = _side_stream(wrangler)
+    if side is not None:
+        return _drive_concurrent(actx, wrangler, trav, src_weight_vecs, side)
 
     mpole_exps = wrangler.form_multipoles(
         actx, trav.level_start_source_box_nrs, trav.source_boxes, src_weight_vecs)
@@ -56,6 +81,10 @@ def drive_fmm(actx, wrangler, src_weight_vecs, timing_data=None):
             trav.from_sep_close_bigger_lists, src_weight_vecs)
         potentials = [a + b for a, b in zip(potentials, direct)]
 
+    return _finish(actx, wrangler, trav, potentials, local_exps)
+
+
+def _finish(actx, wrangler, trav, potentials, local_exps):
     local_exps = wrangler.refine_locals(
         actx, trav.level_start_target_or_target_parent_box_nrs,
         trav.target_or_target_parent_boxes, local_exps)
@@ -66,3 +95,51 @@ def drive_fmm(actx, wrangler, src_weight_vecs, timing_data=None):
 
     result = wrangler.reorder_potentials(potentials)
     return wrangler.finalize_potentials(actx, result)
+
+
+def _drive_concurrent(actx, wrangler, trav, src_weight_vecs, side):
+    import torch
+    main = torch.cuda.current_stream(side.device)
+    getattr(wrangler, "_geom", None)             # shared device geometry, made on this stream
+    side.wait_stream(main)                       # strengths reordered
+    with torch.cuda.stream(side):
+        potentials = wrangler.eval_direct(
+            actx, trav.target_boxes, trav.neighbor_source_boxes_starts,
+            trav.neighbor_source_boxes_lists, src_weight_vecs)
+        local_result = wrangler.form_locals(
+            actx, trav.level_start_target_or_target_parent_box_nrs,
+            trav.target_or_target_parent_boxes, trav.from_sep_bigger_starts,
+            trav.from_sep_bigger_lists, src_weight_vecs)
+
+    mpole_exps = wrangler.form_multipoles(
+        actx, trav.level_start_source_box_nrs, trav.source_boxes, src_weight_vecs)
+    mpole_exps = wrangler.coarsen_multipoles(
+        actx, trav.level_start_source_parent_box_nrs, trav.source_parent_boxes, mpole_exps)
+
+    side.wait_stream(main)                       # multipoles finished
+    with torch.cuda.stream(side):
+        mpole_result = wrangler.eval_multipoles(
+            actx, trav.target_boxes_sep_smaller_by_source_level,
+            trav.from_sep_smaller_by_level, mpole_exps)
+        potentials = [a + b for a, b in zip(potentials, mpole_result)]
+
+    local_exps = wrangler.multipole_to_local(
+        actx, trav.level_start_target_or_target_parent_box_nrs,
+        trav.target_or_target_parent_boxes, trav.from_sep_siblings_starts,
+        trav.from_sep_siblings_lists, mpole_exps)
+
+    main.wait_stream(side)                       # join
+    for t in (*potentials, local_result, mpole_exps, *src_weight_vecs):
+        t.record_stream(side)                    # used on both streams
+    for t in (*potentials, local_result):
+        t.record_stream(main)
+    local_exps = local_exps + local_result
+
+    for starts, lists in ((trav.from_sep_close_smaller_starts, trav.from_sep_close_smaller_lists),
+                          (trav.from_sep_close_bigger_starts, trav.from_sep_close_bigger_lists)):
+        if starts is not None:
+            direct = wrangler.eval_direct(actx, trav.target_boxes, starts, lists,
+                                          src_weight_vecs)
+            potentials = [a + b for a, b in zip(potentials, direct)]
+
+    return _finish(actx, wrangler, trav, potentials, local_exps)

@@ -153,6 +153,8 @@ class SumpyExpansionWrangler:
         self._m2l_tc_mats = {}
         self._m2l_ws = None
         self._status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        # drive_fmm runs List 1, 3 and 4 on a second stream (sumpy_b200.drive)
+        self.concurrent_stages = True
         # mixed form: M2M as a tensor-core GEMM; L2L as an FP64 GEMM (the
         # 3xTF32 L2L compounds its FP32 group sums down the levels: ~3x the
         # mixed form's error on the 1M-point benchmark; see _tc_translations)
