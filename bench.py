@@ -719,6 +719,19 @@ def helmholtz_bench(dev, steps=3, warmup=2, npoints=500_000, order=14, k=10.0,
                           "setup_s": round(setup, 2)}
         if precision == "mixed":
             out["stage_ms_mixed"], _ = stage_breakdown(w, trav, qd, dev, roofline=False)
+            # adjoint with respect to the strengths: the FMM on the transposed
+            # traversal (sumpy_b200.autograd.HelmholtzFMM's backward)
+            from sumpy_b200.adjoint import transpose_traversal
+            tree_t, trav_t, tcls_t = transpose_traversal(tree, trav, tcls)
+            wa = SumpyExpansionWrangler(ti, trav_t, np.complex128, lambda *a: order,
+                                        kernel_extra_kwargs={"k": k},
+                                        translation_classes_data=tcls_t,
+                                        precision=precision, device=dev)
+            gd = pot.conj().contiguous()
+            drive_fmm(None, wa, [gd])
+            ms_adj = timed(lambda: drive_fmm(None, wa, [gd]))
+            out["adjoint_forward_ratio_mixed"] = ms_adj / ms
+            del wa
         del w
         torch.cuda.empty_cache()
     if "fp64" in out and "mixed" in out:

@@ -1,5 +1,6 @@
-"""Differentiable 3D Laplace FMM: ``torch.autograd.Function`` with a
-hand-written backward.
+"""Differentiable 3D Laplace and Helmholtz FMMs: ``torch.autograd.Function``s
+with hand-written backwards (:class:`LaplaceFMM`: strengths and positions;
+:class:`HelmholtzFMM`: complex strengths).
 
 ``LaplaceFMM(order, ...)(strengths, sources, targets=None)`` returns the
 potential phi(x_t) = sum_s q_s / (4 pi |x_t - x_s|) at the targets (at the
@@ -29,7 +30,7 @@ from sumpy_b200.expansion import (
     LinearPDEConformingVolumeTaylorMultipoleExpansion,
 )
 from sumpy_b200.fmm import SumpyExpansionWrangler, SumpyTreeIndependentDataForWrangler
-from sumpy_b200.kernel import LaplaceKernel
+from sumpy_b200.kernel import HelmholtzKernel, LaplaceKernel
 from sumpy_b200.tree import build_all
 
 
@@ -106,3 +107,77 @@ class LaplaceFMM:
     def __call__(self, strengths, sources, targets=None):
         """strengths: (ns,), sources: (3, ns), targets: (3, nt) or None."""
         return _FMMFunction.apply(strengths, sources, targets, self.cfg)
+
+
+@dataclass(frozen=True)
+class _HConfig:
+    order: int
+    k: float
+    max_particles_in_box: int
+    precision: str
+    device: torch.device
+
+
+def _helm_wrangler(cfg, tree, trav, tcls, exclude_self):
+    knl = HelmholtzKernel(3)
+    ti = SumpyTreeIndependentDataForWrangler(
+        None, lambda o, **kw: LinearPDEConformingVolumeTaylorMultipoleExpansion(knl, o),
+        lambda o, **kw: LinearPDEConformingVolumeTaylorLocalExpansion(knl, o), [knl],
+        exclude_self=exclude_self)
+    return SumpyExpansionWrangler(ti, trav, np.complex128, lambda kn, a, t, lev: cfg.order,
+                                  kernel_extra_kwargs={"k": cfg.k},
+                                  translation_classes_data=tcls, precision=cfg.precision,
+                                  device=cfg.device)
+
+
+class _HelmholtzFunction(torch.autograd.Function):
+    """phi = F q for complex strengths q. With PyTorch's convention for
+    complex gradients, q.grad = F^H g = conj(F^T conj(g)); F^T is the FMM on
+    the transposed traversal (G(x - y) = G(y - x) and D(-x) = S D(x) hold for
+    every radial kernel, and the Helmholtz projection keeps the parity of
+    |mi|, so the derivation in sumpy_b200.adjoint carries over)."""
+
+    @staticmethod
+    def forward(ctx, strengths, sources, targets, cfg):
+        self_eval = targets is None
+        src = sources.detach().to("cpu", torch.float64).numpy()
+        tgt = None if self_eval else targets.detach().to("cpu", torch.float64).numpy()
+        tree, trav, tcls = build_all(src, tgt, cfg.max_particles_in_box)
+        w = _helm_wrangler(cfg, tree, trav, tcls, self_eval)
+        q = strengths.detach().to(cfg.device, torch.complex128).contiguous()
+        (phi,) = drive_fmm(None, w, [q])
+        ctx.cfg = cfg
+        ctx.self_eval = self_eval
+        ctx.geometry = (tree, trav, tcls)
+        return phi
+
+    @staticmethod
+    def backward(ctx, g):
+        cfg = ctx.cfg
+        if not ctx.needs_input_grad[0]:
+            return None, None, None, None
+        tree_t, trav_t, tcls_t = transpose_traversal(*ctx.geometry)
+        wa = _helm_wrangler(cfg, tree_t, trav_t, tcls_t, ctx.self_eval)
+        g = g.to(cfg.device, torch.complex128).conj().contiguous()
+        (psi,) = drive_fmm(None, wa, [g])
+        return psi.conj(), None, None, None
+
+
+class HelmholtzFMM:
+    """Callable FMM for the 3D Helmholtz potential
+    phi(x_t) = sum_s q_s e^{ik|x_t - x_s|} / (4 pi |x_t - x_s|), differentiable
+    with respect to the complex strengths (the adjoint FMM).
+
+    :arg order: expansion order (same on every level).
+    :arg k: real wave number.
+    :arg precision: ``"fp64"`` or ``"mixed"``.
+    """
+
+    def __init__(self, order=14, k=1.0, max_particles_in_box=32, precision="fp64",
+                 device="cuda"):
+        self.cfg = _HConfig(int(order), float(k), int(max_particles_in_box), precision,
+                            torch.device(device))
+
+    def __call__(self, strengths, sources, targets=None):
+        """strengths: (ns,) complex, sources: (3, ns), targets: (3, nt) or None."""
+        return _HelmholtzFunction.apply(strengths, sources, targets, self.cfg)

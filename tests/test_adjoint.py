@@ -230,3 +230,83 @@ def test_gpu_gradient_stages_are_exact_derivatives(cuda_device, stage):
         g = out[1 + d]
         assert float(g.abs().max()) > 0
         assert float((g - fd).abs().max() / g.abs().max()) < 1e-6, (stage, d)
+
+
+# {{{ Helmholtz (complex strengths)
+
+@pytest.mark.parametrize("case", ["separate", "self"])
+def test_helmholtz_transposed_traversal_is_exact_transpose(case):
+    """<F q, g> = <q, F^T g> (bilinear) on the Helmholtz oracle, k = 10."""
+    src, tgt = _separate()
+    if case == "self":
+        tgt = None
+    tree, trav, tcls = build_all(src, tgt, 12)
+    tree_t, trav_t, tcls_t = transpose_traversal(tree, trav, tcls)
+    rng = np.random.default_rng(4)
+    q = rng.standard_normal(tree.nsources) + 1j * rng.standard_normal(tree.nsources)
+    g = rng.standard_normal(tree.ntargets) + 1j * rng.standard_normal(tree.ntargets)
+    excl = case == "self"
+    for p in (3, 6):
+        fq = O.run_fmm(tree, trav, tcls, p, q, exclude_self=excl, helmholtz_k=10.0)
+        ftg = O.run_fmm(tree_t, trav_t, tcls_t, p, g, exclude_self=excl, helmholtz_k=10.0)
+        lhs, rhs = complex(fq @ g), complex(q @ ftg)
+        scale = float(np.abs(fq).sum() * np.abs(g).max())
+        assert abs(lhs - rhs) < 1e-13 * scale, (p, lhs, rhs)
+
+
+def fmm_direct(knl, tp, src, q, tts, k):
+    from sumpy_b200 import P2P
+    return P2P(knl, exclude_self=tts is not None)(None, tp, src, (q,), target_to_source=tts,
+                                                  k=k)[0]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("self_eval", [False, True])
+def test_gpu_helmholtz_strength_gradient(cuda_device, self_eval):
+    """q.grad of L = 0.5 |phi - phi_ref|^2 (PyTorch's complex convention:
+    dL/dRe q + i dL/dIm q) against the direct-sum adjoint F^H (phi - phi_ref)
+    and against central differences of the FMM itself."""
+    from sumpy_b200 import P2P, HelmholtzKernel
+    from sumpy_b200.autograd import HelmholtzFMM
+    src, tgt, _ = _shell_problem(3000, 1200)
+    rng = np.random.default_rng(8)
+    q0 = rng.standard_normal(src.shape[1]) + 1j * rng.standard_normal(src.shape[1])
+    k = 6.0
+    fmm = HelmholtzFMM(order=12, k=k, precision="fp64", device=cuda_device)
+    s = torch.as_tensor(src, device=cuda_device)
+    t = None if self_eval else torch.as_tensor(tgt, device=cuda_device)
+    tp = src if self_eval else tgt
+    knl = [HelmholtzKernel(3)]
+    tts = np.arange(src.shape[1]) if self_eval else None
+    (phi_ref,) = P2P(knl, exclude_self=self_eval)(None, tp, src, (0.5 * q0,),
+                                                   target_to_source=tts, k=k)
+
+    def loss(qv):
+        phi = fmm(qv, s, t)
+        return 0.5 * ((phi - phi_ref).abs() ** 2).sum(), phi
+
+    q = torch.as_tensor(q0, device=cuda_device).requires_grad_(True)
+    L, phi = loss(q)
+    L.backward()
+    g = (phi - phi_ref).detach()
+    # F^H g = conj(F^T conj(g)), F^T = the direct sum with the roles swapped
+    (ftg,) = P2P(knl, exclude_self=self_eval)(None, src, tp, (g.conj().cpu().numpy(),),
+                                              target_to_source=tts, k=k)
+    ref = ftg.conj()
+    err = float((q.grad - ref).norm() / ref.norm())
+    # the same order's forward error against the direct sum bounds it
+    fwd = float((phi.detach() - fmm_direct(knl, tp, src, q0, tts, k)).norm()
+                / fmm_direct(knl, tp, src, q0, tts, k).norm())
+    assert err < max(1e-5, 20 * fwd), (err, fwd)
+    h = 1e-4
+    for i in (0, 17, 1234):
+        for unit in (1.0, 1j):
+            qp = torch.as_tensor(q0, device=cuda_device).clone()
+            qm = qp.clone()
+            qp[i] += h * unit
+            qm[i] -= h * unit
+            fd = (float(loss(qp)[0]) - float(loss(qm)[0])) / (2 * h)
+            an = float(q.grad[i].real if unit == 1.0 else q.grad[i].imag)
+            assert abs(fd - an) < 1e-6 * max(abs(fd), 1.0), (i, unit, fd, an)
+
+# }}}
