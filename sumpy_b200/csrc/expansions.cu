@@ -23,25 +23,6 @@
 namespace sumpy {
 namespace {
 
-// stored multipole -> nothing; full multipole (cube) -> compressed in place
-// (plane i-2 receives -cube[i][J-2][K] - cube[i][J][K-2]). Block-wide.
-__device__ void compress_cube_block(double *cube, int p)
-{
-    for (int i = p; i >= 2; --i) {
-        const int m = p - i + 2;
-        const int npairs = (m + 1) * (m + 2) / 2;
-        for (int t = threadIdx.x; t < npairs; t += blockDim.x) {
-            int J, K;
-            tri_pair(t, m, J, K);
-            double v = 0.0;
-            if (J >= 2) v += cube[cube_index(p, i, J - 2, K)];
-            if (K >= 2) v += cube[cube_index(p, i, J, K - 2)];
-            cube[cube_index(p, i - 2, J, K)] -= v;
-        }
-        __syncthreads();
-    }
-}
-
 // same, one warp
 __device__ void decompress_cube_warp(double *cube, int p, int lane)
 {
@@ -60,61 +41,125 @@ __device__ void decompress_cube_warp(double *cube, int p, int lane)
 
 // {{{ P2M
 
-constexpr int P2M_THREADS = 128;
-constexpr int P2M_CHUNK = 32;
-
-__global__ void __launch_bounds__(P2M_THREADS)
-p2m_kernel(int p, double rscale, const int32_t *__restrict__ boxes, const double *__restrict__ centers,
-           int64_t cstride, const int32_t *__restrict__ bss, const int32_t *__restrict__ bsc,
-           const double *__restrict__ sources, int64_t sstride, const double *__restrict__ q,
-           int32_t base, double *__restrict__ out)
+// warps per CTA: four while their static tables fit in 48 KB, else two
+template <int P>
+__host__ __device__ constexpr int p2m_warps()
 {
-    extern __shared__ double sm[];
-    const int P1 = p + 1;
-    double *cube = sm;                               // P1^3
-    double *pw = cube + P1 * P1 * P1;                // [CHUNK][3][P1]
-    double *qs = pw + P2M_CHUNK * 3 * P1;            // [CHUNK]
+    return (3 * (P + 1) * 33 + (P + 1) * (P + 2) * (P + 3) / 6 + 32) * 8 * 4 <= 48 * 1024 ? 4
+                                                                                            : 2;
+}
 
-    const int32_t b = boxes[blockIdx.x];
+// P2M with one warp per box and the full coefficients in registers: lane u
+// owns the (i, j) pairs u, u + 32, ... (i + j <= P) and accumulates the
+// column k = 0..P-i-j of each, so a (source, coefficient) term costs one
+// FMA with a broadcast power w2[k]; per source t = q w0[i] w1[j] is formed
+// once per pair. Sources go 32 at a time, one per lane for the power
+// tables (a/r)^k / k!. The columns are then written to a per-warp compact
+// full-index buffer, compressed by the p-1 plane sweeps (warp-synchronous)
+// and stored. Same arithmetic as p2m_kernel (multipole.py:77-114 and the
+// transposed projection), ordered differently.
+template <int P>
+__global__ void __launch_bounds__(32 * p2m_warps<P>())
+p2m_warp_kernel(double rscale, int32_t nboxes, const int32_t *__restrict__ boxes,
+                const double *__restrict__ centers, int64_t cstride,
+                const int32_t *__restrict__ bss, const int32_t *__restrict__ bsc,
+                const double *__restrict__ sources, int64_t sstride,
+                const double *__restrict__ q, int32_t base, double *__restrict__ out)
+{
+    constexpr int P1 = P + 1;
+    constexpr int NPAIR = P1 * (P1 + 1) / 2;
+    constexpr int NU = (NPAIR + 31) / 32;
+    constexpr int NFULL = P1 * (P1 + 1) * (P1 + 2) / 6;
+    constexpr int N = P1 * P1;
+    constexpr int W = p2m_warps<P>();
+    __shared__ double w[W][3][P1][33];   // [axis][power][source] (+1 pad)
+    __shared__ double qs[W][32];
+    __shared__ double full[W][NFULL];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ib = blockIdx.x * W + warp;
+    if (ib >= nboxes) return;
+    const int32_t b = boxes[ib];
     const double c[3] = {centers[b], centers[cstride + b], centers[2 * cstride + b]};
     const int32_t s0 = bss[b], ns = bsc[b];
-    const int nfull = nfull_of(p);
     const double rinv = 1.0 / rscale;
 
-    for (int t = threadIdx.x; t < P1 * P1 * P1; t += blockDim.x) cube[t] = 0.0;
-    __syncthreads();
+    // the (i, j) pairs of this lane
+    int pi[NU], pj[NU];
+#pragma unroll
+    for (int u = 0; u < NU; ++u) {
+        int t = lane + 32 * u, i = 0;
+        if (t >= NPAIR) t = 0;  // idle slot, never stored
+        while (t > P - i) { t -= P - i + 1; ++i; }
+        pi[u] = i;
+        pj[u] = t;
+    }
+    double acc[NU][P1];
+#pragma unroll
+    for (int u = 0; u < NU; ++u)
+#pragma unroll
+        for (int k = 0; k < P1; ++k) acc[u][k] = 0.0;
 
-    for (int sc = 0; sc < ns; sc += P2M_CHUNK) {
-        const int nsc = min(P2M_CHUNK, ns - sc);
-        for (int t = threadIdx.x; t < P2M_CHUNK * 3; t += blockDim.x) {
-            const int s = t / 3, d = t % 3;
-            double *w = pw + (s * 3 + d) * P1;
-            if (s < nsc) {
-                const double a = (c[d] - sources[d * sstride + s0 + sc + s]) * rinv;
-                w[0] = 1.0;
-                for (int k = 1; k <= p; ++k) w[k] = w[k - 1] * a / k;
-                if (d == 0) qs[s] = q[s0 + sc + s];
+    for (int32_t sc = 0; sc < ns; sc += 32) {
+        const int nsc = min(32, ns - sc);
+        if (lane < nsc) {
+            const int32_t s = s0 + sc + lane;
+            qs[warp][lane] = q[s];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const double a = (c[d] - sources[d * sstride + s]) * rinv;
+                double v = 1.0;
+                w[warp][d][0][lane] = 1.0;
+#pragma unroll
+                for (int k = 1; k < P1; ++k) {
+                    v = v * a / k;
+                    w[warp][d][k][lane] = v;
+                }
             }
         }
-        __syncthreads();
-        for (int f = threadIdx.x; f < nfull; f += blockDim.x) {
-            int i, j, k;
-            full_mi(f, i, j, k);
-            double acc = 0.0;
-            for (int s = 0; s < nsc; ++s)
-                acc += qs[s] * pw[(s * 3 + 0) * P1 + i] * pw[(s * 3 + 1) * P1 + j] *
-                       pw[(s * 3 + 2) * P1 + k];
-            cube[cube_index(p, i, j, k)] += acc;
+        __syncwarp();
+        for (int so = 0; so < nsc; ++so) {
+            const double qq = qs[warp][so];
+#pragma unroll
+            for (int u = 0; u < NU; ++u) {
+                const double t = qq * w[warp][0][pi[u]][so] * w[warp][1][pj[u]][so];
+                const int kmax = P - pi[u] - pj[u];
+#pragma unroll
+                for (int k = 0; k < P1; ++k)
+                    if (k <= kmax) acc[u][k] = fma(t, w[warp][2][k][so], acc[u][k]);
+            }
         }
-        __syncthreads();
+        __syncwarp();
     }
-    compress_cube_block(cube, p);
-    const int n = ncoeff_of(p);
-    double *o = out + (int64_t)(b - base) * n;
-    for (int s = threadIdx.x; s < n; s += blockDim.x) {
+    double *F = full[warp];
+#pragma unroll
+    for (int u = 0; u < NU; ++u) {
+        if (lane + 32 * u < NPAIR) {
+            const int kmax = P - pi[u] - pj[u];
+#pragma unroll
+            for (int k = 0; k < P1; ++k)
+                if (k <= kmax) F[full_index(pi[u], pj[u], k)] = acc[u][k];
+        }
+    }
+    __syncwarp();
+    // transposed projection: plane i-2 gathers from plane i, i = P..2
+    for (int i = P; i >= 2; --i) {
+        const int m = P - i + 2;
+        const int npairs = (m + 1) * (m + 2) / 2;
+        for (int t = lane; t < npairs; t += 32) {
+            int J, K;
+            tri_pair(t, m, J, K);
+            double v = 0.0;
+            if (J >= 2) v += F[full_index(i, J - 2, K)];
+            if (K >= 2) v += F[full_index(i, J, K - 2)];
+            F[full_index(i - 2, J, K)] -= v;
+        }
+        __syncwarp();
+    }
+    double *o = out + (int64_t)(b - base) * N;
+    for (int st = lane; st < N; st += 32) {
         int i, j, k;
-        stored_mi(s, i, j, k);
-        o[s] = cube[cube_index(p, i, j, k)];
+        stored_mi(st, i, j, k);
+        o[st] = F[full_index(i, j, k)];
     }
 }
 
@@ -704,15 +749,15 @@ int sumpy_p2e_from_single_box_f64(int order, double rscale, int32_t nsrc_boxes,
     if (!source_boxes || !centers || !box_source_starts || !box_source_counts_nonchild ||
         !sources || !strength || !tgt_expansions)
         return bad_arg("p2m: null pointer argument");
-    const int P1 = order + 1;
-    const size_t smem = sizeof(double) * (P1 * P1 * P1 + P2M_CHUNK * 3 * P1 + P2M_CHUNK);
-    int rc = prepare_smem(p2m_kernel, smem);
-    if (rc) return rc;
-    p2m_kernel<<<nsrc_boxes, P2M_THREADS, smem, as_stream(stream)>>>(
-        order, rscale, source_boxes, centers, center_stride, box_source_starts,
-        box_source_counts_nonchild, sources, source_stride, strength, tgt_base_ibox,
-        tgt_expansions);
-    return check_launch("p2m_kernel");
+#define CALL_P2M(P)                                                                              \
+    (p2m_warp_kernel<P><<<(nsrc_boxes + p2m_warps<P>() - 1) / p2m_warps<P>(),                    \
+                          32 * p2m_warps<P>(), 0, as_stream(stream)>>>(                           \
+         rscale, nsrc_boxes, source_boxes, centers, center_stride, box_source_starts,           \
+         box_source_counts_nonchild, sources, source_stride, strength, tgt_base_ibox,           \
+         tgt_expansions),                                                                       \
+     check_launch("p2m_warp_kernel"))
+    SUMPY_ORDER_SWITCH(order, CALL_P2M)
+#undef CALL_P2M
 }
 
 int sumpy_e2e_from_children_f64(int src_order, int tgt_order, double src_rscale,

@@ -11,27 +11,32 @@ eval_direct (List 1) -> multipole_to_local (List 2) -> eval_multipoles
 (List 3) -> form_locals (List 4) -> refine_locals (L2L) -> eval_locals (L2P)
 -> reorder_potentials -> finalize_potentials.
 
-On a CUDA wrangler the stages that do not depend on the multipole chain run
-on a second stream: List 1 and List 4 need only the strengths, List 3 only
-the finished multipoles, so they overlap P2M, M2M and M2L (whose coarse
-levels leave most SMs idle). The side stream forks from the caller's stream
-after the strengths are reordered and joins it before the first use of its
-results; the returned potentials are ordered on the caller's stream like
-every other result, and the whole sequence can be captured in a CUDA graph.
+On a CUDA wrangler the multipole/local chain (P2M, M2M, M2L, L2L, L2P) runs
+on a high-priority stream and the stages that do not depend on it on a
+low-priority one: List 1 and List 4 need only the strengths, List 3 only the
+finished multipoles, so they fill the SMs the chain leaves idle (its coarse
+levels) without delaying it. Both streams fork from the caller's stream
+after the strengths are reordered and join back before the potentials are
+returned; the results are ordered on the caller's stream like every other
+result, and the whole sequence can be captured in a CUDA graph.
 """
 from __future__ import annotations
 
 
-def _side_stream(wrangler):
+def _side_streams(wrangler):
+    """(critical, side) streams of a CUDA wrangler that allows concurrent
+    stages: the multipole/local chain on a high-priority stream, the
+    independent stages on a low-priority one."""
     import torch
     dev = getattr(wrangler, "device", None)
     if dev is None or getattr(dev, "type", None) != "cuda" or not getattr(
             wrangler, "concurrent_stages", False):
         return None
-    s = getattr(wrangler, "_side_stream", None)
+    s = getattr(wrangler, "_streams", None)
     if s is None:
-        s = torch.cuda.Stream(dev)
-        wrangler._side_stream = s
+        lo, hi = torch.cuda.Stream.priority_range()
+        s = (torch.cuda.Stream(dev, priority=hi), torch.cuda.Stream(dev, priority=lo))
+        wrangler._streams = s
     return s
 
 
@@ -40,9 +45,9 @@ def drive_fmm(actx, wrangler, src_weight_vecs, timing_data=None):
     src_weight_vecs = [wrangler.reorder_sources(w) for w in src_weight_vecs]
     src_weight_vecs = wrangler.distribute_source_weights(src_weight_vecs)
 
-    side = _side_stream(wrangler)
-    if side is not None:
-        return _drive_concurrent(actx, wrangler, trav, src_weight_vecs, side)
+    streams = _side_streams(wrangler)
+    if streams is not None:
+        return _drive_concurrent(actx, wrangler, trav, src_weight_vecs, *streams)
 
     mpole_exps = wrangler.form_multipoles(
         actx, trav.level_start_source_box_nrs, trav.source_boxes, src_weight_vecs)
@@ -97,11 +102,21 @@ def _finish(actx, wrangler, trav, potentials, local_exps):
     return wrangler.finalize_potentials(actx, result)
 
 
-def _drive_concurrent(actx, wrangler, trav, src_weight_vecs, side):
+def _drive_concurrent(actx, wrangler, trav, src_weight_vecs, crit, side):
     import torch
-    main = torch.cuda.current_stream(side.device)
+    main = torch.cuda.current_stream(crit.device)
     getattr(wrangler, "_geom", None)             # shared device geometry, made on this stream
-    side.wait_stream(main)                       # strengths reordered
+    crit.wait_stream(main)                       # strengths reordered
+    side.wait_stream(main)
+    for t in src_weight_vecs:
+        t.record_stream(crit)
+        t.record_stream(side)
+    with torch.cuda.stream(crit):
+        mpole_exps = wrangler.form_multipoles(
+            actx, trav.level_start_source_box_nrs, trav.source_boxes, src_weight_vecs)
+        mpole_exps = wrangler.coarsen_multipoles(
+            actx, trav.level_start_source_parent_box_nrs, trav.source_parent_boxes,
+            mpole_exps)
     with torch.cuda.stream(side):
         potentials = wrangler.eval_direct(
             actx, trav.target_boxes, trav.neighbor_source_boxes_starts,
@@ -110,36 +125,31 @@ def _drive_concurrent(actx, wrangler, trav, src_weight_vecs, side):
             actx, trav.level_start_target_or_target_parent_box_nrs,
             trav.target_or_target_parent_boxes, trav.from_sep_bigger_starts,
             trav.from_sep_bigger_lists, src_weight_vecs)
-
-    mpole_exps = wrangler.form_multipoles(
-        actx, trav.level_start_source_box_nrs, trav.source_boxes, src_weight_vecs)
-    mpole_exps = wrangler.coarsen_multipoles(
-        actx, trav.level_start_source_parent_box_nrs, trav.source_parent_boxes, mpole_exps)
-
-    side.wait_stream(main)                       # multipoles finished
-    with torch.cuda.stream(side):
+        side.wait_stream(crit)                   # multipoles finished
         mpole_result = wrangler.eval_multipoles(
             actx, trav.target_boxes_sep_smaller_by_source_level,
             trav.from_sep_smaller_by_level, mpole_exps)
         potentials = [a + b for a, b in zip(potentials, mpole_result)]
-
-    local_exps = wrangler.multipole_to_local(
-        actx, trav.level_start_target_or_target_parent_box_nrs,
-        trav.target_or_target_parent_boxes, trav.from_sep_siblings_starts,
-        trav.from_sep_siblings_lists, mpole_exps)
-
-    main.wait_stream(side)                       # join
-    for t in (*potentials, local_result, mpole_exps, *src_weight_vecs):
-        t.record_stream(side)                    # used on both streams
-    for t in (*potentials, local_result):
+    mpole_exps.record_stream(side)
+    with torch.cuda.stream(crit):
+        local_exps = wrangler.multipole_to_local(
+            actx, trav.level_start_target_or_target_parent_box_nrs,
+            trav.target_or_target_parent_boxes, trav.from_sep_siblings_starts,
+            trav.from_sep_siblings_lists, mpole_exps)
+        crit.wait_stream(side)                   # join
+        for t in (*potentials, local_result):
+            t.record_stream(crit)
+        local_exps = local_exps + local_result
+        for starts, lists in ((trav.from_sep_close_smaller_starts,
+                               trav.from_sep_close_smaller_lists),
+                              (trav.from_sep_close_bigger_starts,
+                               trav.from_sep_close_bigger_lists)):
+            if starts is not None:
+                direct = wrangler.eval_direct(actx, trav.target_boxes, starts, lists,
+                                              src_weight_vecs)
+                potentials = [a + b for a, b in zip(potentials, direct)]
+        result = _finish(actx, wrangler, trav, potentials, local_exps)
+    main.wait_stream(crit)
+    for t in result:
         t.record_stream(main)
-    local_exps = local_exps + local_result
-
-    for starts, lists in ((trav.from_sep_close_smaller_starts, trav.from_sep_close_smaller_lists),
-                          (trav.from_sep_close_bigger_starts, trav.from_sep_close_bigger_lists)):
-        if starts is not None:
-            direct = wrangler.eval_direct(actx, trav.target_boxes, starts, lists,
-                                          src_weight_vecs)
-            potentials = [a + b for a, b in zip(potentials, direct)]
-
-    return _finish(actx, wrangler, trav, potentials, local_exps)
+    return result
