@@ -604,9 +604,13 @@ m2p_mixed_kernel(double rscale, int32_t ntgt_boxes, const int32_t *__restrict__ 
                  int64_t tstride, double scale, double *__restrict__ result)
 {
     constexpr int N = (P + 1) * (P + 1);
+    // per warp: the multipoles of the (up to 32) List-3 boxes of one round,
+    // one per lane group, as FP32 (read back as broadcasts within a group)
+    extern __shared__ float smm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ib = blockIdx.x * E2P_WARPS + warp;
     if (ib >= ntgt_boxes) return;
+    float *Ms = smm + warp * (32 * N);
     const int32_t tb = target_boxes[ib];
     const int32_t t0 = bts[tb], nt = btc[tb];
     const int32_t ls = src_starts[ib], le = src_starts[ib + 1];
@@ -622,15 +626,23 @@ m2p_mixed_kernel(double rscale, int32_t ntgt_boxes, const int32_t *__restrict__ 
         double tx = 0, ty = 0, tz = 0;
         if (active) { tx = targets[t]; ty = targets[tstride + t]; tz = targets[2 * tstride + t]; }
         double acc = 0.0;
-        if (active) {
-            for (int32_t l = ls + ph; l < le; l += nph) {
-                const int32_t sb = src_lists[l];
-                const double *M = src + (int64_t)(sb - sbase) * N;
+        for (int32_t l0 = ls; l0 < le; l0 += nph) {
+            const int nb = min(nph, le - l0);
+            // stage the round's boxes: box r's coefficients at Ms[r * N ...]
+            __syncwarp();
+            for (int e = lane; e < nb * N; e += 32) {
+                const int r = e / N, s = e - r * N;
+                Ms[r * N + s] = (float)src[(int64_t)(src_lists[l0 + r] - sbase) * N + s];
+            }
+            __syncwarp();
+            if (active && ph < nb) {
+                const int32_t sb = src_lists[l0 + ph];
+                const float *M = Ms + ph * N;
                 float accf = 0.f;
                 laplace_layers<P, float>(
                     (float)(tx - centers[sb]), (float)(ty - centers[cstride + sb]),
                     (float)(tz - centers[2 * cstride + sb]), R, Rinv,
-                    [&](int s, int, int, int, float v) { accf = fmaf((float)__ldg(M + s), v, accf); });
+                    [&](int s, int, int, int, float v) { accf = fmaf(M[s], v, accf); });
                 acc += (double)accf;
             }
         }
@@ -976,11 +988,15 @@ int sumpy_e2p_from_csr_mixed(int order, double rscale, int32_t ntgt_boxes,
         return bad_arg("m2p mixed: null pointer argument");
     const int blocks = (ntgt_boxes + E2P_WARPS - 1) / E2P_WARPS;
 #define CALL_M2PM(P)                                                                             \
-    (m2p_mixed_kernel<P><<<blocks, 32 * E2P_WARPS, 0, as_stream(stream)>>>(                     \
-         rscale, ntgt_boxes, target_boxes, source_box_starts, source_box_lists, centers,        \
-         center_stride, src_base_ibox, src_expansions, box_target_starts,                       \
-         box_target_counts_nonchild, targets, target_stride, scale, result),                    \
-     check_launch("m2p_mixed_kernel"))
+    (prepare_smem(m2p_mixed_kernel<P>, sizeof(float) * 32 * (P + 1) * (P + 1) * E2P_WARPS)      \
+         ? SUMPY_ELAUNCH                                                                         \
+         : (m2p_mixed_kernel<P><<<blocks, 32 * E2P_WARPS,                                        \
+                                  sizeof(float) * 32 * (P + 1) * (P + 1) * E2P_WARPS,            \
+                                  as_stream(stream)>>>(                                          \
+                rscale, ntgt_boxes, target_boxes, source_box_starts, source_box_lists, centers, \
+                center_stride, src_base_ibox, src_expansions, box_target_starts,                \
+                box_target_counts_nonchild, targets, target_stride, scale, result),             \
+            check_launch("m2p_mixed_kernel")))
     SUMPY_ORDER_SWITCH(order, CALL_M2PM)
 #undef CALL_M2PM
 }
