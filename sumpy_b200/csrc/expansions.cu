@@ -395,6 +395,21 @@ __device__ __forceinline__ double horner_cube(const double *cube, const double *
     return tot;
 }
 
+// sum over j + k <= p - i of cube[i][j][k] y^j z^k / (j! k!) (one x-plane)
+__device__ __forceinline__ double horner_plane(const double *cube, const double *inv, int p,
+                                               int i, double y, double z)
+{
+    const int q = p - i;
+    double sy = 0.0;
+    for (int j = q; j >= 0; --j) {
+        double sz = 0.0;
+        const double *row = cube + cube_index(p, i, j, 0);
+        for (int k = q - j; k >= 0; --k) sz = row[k] + sz * z * inv[k + 1];
+        sy = sz + sy * y * inv[j + 1];
+    }
+    return sy;
+}
+
 template <bool GRAD>
 __global__ void l2p_kernel(int p, double rscale, int32_t nboxes, const int32_t *__restrict__ boxes,
                            const double *__restrict__ centers, int64_t cstride, int32_t sbase,
@@ -427,6 +442,38 @@ __global__ void l2p_kernel(int p, double rscale, int32_t nboxes, const int32_t *
     const double c[3] = {centers[b], centers[cstride + b], centers[2 * cstride + b]};
     const double rinv = 1.0 / rscale;
     const int32_t t0 = bts[b], nt = btc[b];
+    if (!GRAD && result) {
+        // values: the box's targets on g = next_pow2(nt) lanes, the 32/g lane
+        // groups split the x-planes i = ph, ph + nph, ... of each target's
+        // polynomial; shuffle-xor sum over the groups
+        for (int32_t tc = 0; tc < nt; tc += 32) {
+            const int ntc = min(32, nt - tc);
+            int g = 1;
+            while (g < ntc) g <<= 1;
+            const int nph = 32 / g;
+            const int tl = lane & (g - 1), ph = lane / g;
+            const bool active = tl < ntc;
+            const int32_t t = t0 + tc + tl;
+            double v = 0.0;
+            // groups beyond the last plane (ph > p: few targets, many groups)
+            // have nothing to sum; inv[] holds 1/n for n <= p + 1 only
+            if (active && ph <= p) {
+                const double x = (targets[t] - c[0]) * rinv;
+                const double y = (targets[tstride + t] - c[1]) * rinv;
+                const double z = (targets[2 * tstride + t] - c[2]) * rinv;
+                // x^i / i! for i = ph, ph + nph, ... (indices of inv[] stay <= p)
+                double xi = 1.0;
+                for (int i = 1; i <= ph; ++i) xi *= x * inv[i];
+                for (int i = ph; i <= p; i += nph) {
+                    v += xi * horner_plane(cube, inv, p, i, y, z);
+                    for (int q = i + 1; q <= i + nph && q <= p; ++q) xi *= x * inv[q];
+                }
+            }
+            for (int off = g; off < 32; off <<= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+            if (active && ph == 0) result[t] = scale * v;
+        }
+        return;
+    }
     for (int32_t tt = lane; tt < nt; tt += 32) {
         const int32_t t = t0 + tt;
         const double x = (targets[t] - c[0]) * rinv;
