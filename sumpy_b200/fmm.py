@@ -659,28 +659,42 @@ class SumpyExpansionWrangler:
 
     @cached_property
     def _tc_translations(self):
-        """Mixed Laplace form with one order on every level: M2M and L2L are
-        then the same eight dense maps (one per child octant) on every level
-        (rscale ratio 1/2 and offset/rscale = order/8 do not depend on the
-        level), applied as grouped GEMMs by the tensor-core kernel."""
-        return (self.precision == "mixed" and not self.helmholtz
-                and len(set(self.level_orders)) == 1)
+        """Mixed form with one order on every level: M2M (and optionally L2L)
+        as eight dense maps per level (one per child octant), applied as
+        grouped GEMMs by the tensor-core kernel. For Laplace the maps are the
+        same on every level (rscale ratio 1/2 and offset/rscale = order/8 do
+        not depend on it); for Helmholtz they depend on the level through
+        k^2 rscale^2 and act on the interleaved complex coefficients as their
+        block-diagonal real embedding."""
+        return self.precision == "mixed" and len(set(self.level_orders)) == 1
 
-    def _octant_operator_planes(self, kind):
-        key = ("octant-ops", kind)
+    def _octant_operator_planes(self, kind, parent_level=2):
+        # Laplace: any level pair gives the same maps (take levels 2 -> 3)
+        lev = parent_level if self.helmholtz else 2
+        key = ("octant-ops", kind, lev)
         if key not in self._m2l_tc_mats:
             order = self.level_orders[0]
-            # any level pair gives the same maps; take levels 2 -> 3 (rscale as
-            # level_to_rscale, sumpy/fmm.py:369-386)
-            r_par = self.tree.root_extent * 2.0 ** -2 * 2 / order
-            r_ch = self.tree.root_extent * 2.0 ** -3 * 2 / order
-            h_ch = self.tree.root_extent * 2.0 ** -3
+            # rscale as level_to_rscale (sumpy/fmm.py:369-386)
+            r_par = self.tree.root_extent * 2.0 ** -lev * 2 / order
+            r_ch = self.tree.root_extent * 2.0 ** -(lev + 1) * 2 / order
+            h_ch = self.tree.root_extent * 2.0 ** -(lev + 1)
             offs = octant_offsets(h_ch)          # child center - parent center
+            k2 = self.k ** 2 if self.helmholtz else 0.0
             if kind == "m2m":
-                ops = [m2m_operator(order, r_ch, r_par, -offs[o]) for o in range(8)]
+                ops = [m2m_operator(order, r_ch, r_par, -offs[o], k2 * r_par ** 2)
+                       for o in range(8)]
             else:
-                ops = [l2l_operator(order, r_par, r_ch, offs[o]) for o in range(8)]
-            mats = torch.as_tensor(np.stack(ops)).to(self.device)
+                ops = [l2l_operator(order, r_par, r_ch, offs[o], k2 * r_par ** 2)
+                       for o in range(8)]
+            ops = np.stack(ops)
+            if self.helmholtz:
+                # real maps on interleaved (re, im): rows/cols 2t + a, a in {0, 1}
+                n = ops.shape[1]
+                emb = np.zeros((8, n, 2, n, 2))
+                emb[:, :, 0, :, 0] = ops
+                emb[:, :, 1, :, 1] = ops
+                ops = emb.reshape(8, 2 * n, 2 * n)
+            mats = torch.as_tensor(ops).to(self.device)
             hi, lo, rp, kp = self._m2l_tc_operands(mats)
             self._m2l_tc_mats[key] = (mats, hi, lo, rp, kp)
         return self._m2l_tc_mats[key]
@@ -728,13 +742,14 @@ class SumpyExpansionWrangler:
         self._m2l_plans[key] = plan
         return plan
 
-    def _octant_gemm(self, kind, plan, sview, sbase, tview, tbase, st, fp64=False):
-        mats, hi, lo, rp, kp = self._octant_operator_planes(kind)
+    def _octant_gemm(self, kind, plan, sview, sbase, tview, tbase, st, fp64=False,
+                     parent_level=2):
+        mats, hi, lo, rp, kp = self._octant_operator_planes(kind, parent_level)
         if fp64:
             self._call_m2l_f64(self.level_orders[0], plan, mats, sbase, sview, tbase, tview,
                                st)
             return
-        nb, n = sview.shape
+        nb, n = sview.shape[0], mats.shape[1]   # real values per box
         ws_hi, ws_lo = self._m2l_workspace(nb, kp)
         call("sumpy_split_tf32x2", _i64(nb), _i32(1), _i32(n), dptr(sview), _i32(1),
              _i32(kp), dptr(ws_hi), dptr(ws_lo), st)
@@ -765,7 +780,8 @@ class SumpyExpansionWrangler:
             plan = self._m2l_plans[key]
             sbase, sview = self.multipole_expansions_view(mpoles, src_lev)
             tbase, tview = self.multipole_expansions_view(mpoles, tgt_lev)
-            self._octant_gemm("m2m", plan, sview, sbase, tview, tbase, st)
+            self._octant_gemm("m2m", plan, sview, sbase, tview, tbase, st,
+                              parent_level=tgt_lev)
         return mpoles
 
     def _refine_tc(self, level_start_target_or_target_parent_box_nrs,
@@ -857,7 +873,7 @@ class SumpyExpansionWrangler:
 
     def refine_locals(self, actx, level_start_target_or_target_parent_box_nrs,
                       target_or_target_parent_boxes, local_exps):
-        if self._tc_translations and (self.tc_l2l or self.gemm_l2l):
+        if self._tc_translations and not self.helmholtz and (self.tc_l2l or self.gemm_l2l):
             return self._refine_tc(level_start_target_or_target_parent_box_nrs,
                                    target_or_target_parent_boxes, local_exps,
                                    fp64=not self.tc_l2l)
