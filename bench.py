@@ -37,7 +37,15 @@ sys.path.insert(0, str(ROOT))
 METRIC = "3D Laplace FMM Mpts/s @ relL2<=1e-6 (mixed vs FP64 GPU); adjoint/forward ratio"
 NPOINTS = 1_000_000
 ORDER = 10
-MAX_PARTICLES = 32
+# max_particles_in_box of the 1M-point workload (the workload leaves it open): the fastest
+# mixed form in a sweep over 32..192 on this GPU (32: 11.0 ms, 64: 10.1, 96: 9.6, 128: 10.0,
+# 192: 13.7 ms; accuracy against the direct sum 3.5e-6 for all). The FP64 form is timed on
+# the same tree (like for like) and, separately, on its own fastest tree (FP64_MAX_PARTICLES).
+MAX_PARTICLES = 96
+FP64_MAX_PARTICLES = 128
+HELMHOLTZ_MAX_PARTICLES = 64   # same sweep for the Helmholtz workload: 32: 46 ms, 64: 21 ms
+BATCH_MAX_PARTICLES = 32       # the batched workload's own setting
+ADJOINT_MAX_PARTICLES = 32
 NSAMPLE = 4096
 
 
@@ -361,6 +369,20 @@ def main():
             drive_fmm(None, w_64, [q_dev])
         ms_64, _ = timed(lambda: drive_fmm(None, w_64, [q_dev]), args.steps)
 
+    # FP64 on its own fastest tree (larger leaves favour the slower FP64 M2L)
+    fp64_best = None
+    if not args.no_fp64 and args.npoints == NPOINTS and args.order == ORDER:
+        tree_b, trav_b, tcls_b = build_all(pts, None, FP64_MAX_PARTICLES)
+        w_b = SumpyExpansionWrangler(ti, trav_b, np.float64, lambda k, a, t, lev: args.order,
+                                     translation_classes_data=tcls_b, precision="fp64",
+                                     device=dev)
+        for _ in range(max(1, args.warmup)):
+            drive_fmm(None, w_b, [q_dev])
+        ms_b, _ = timed(lambda: drive_fmm(None, w_b, [q_dev]), args.steps)
+        fp64_best = {"max_particles_in_box": FP64_MAX_PARTICLES, "ms_per_step": ms_b,
+                     "value": world * args.npoints / (ms_b * 1e-3) / 1e6}
+        del w_b, tree_b, trav_b, tcls_b
+
     # accuracy on sampled targets against the FP64 direct sum
     rng = np.random.default_rng(99)
     sample = rng.choice(args.npoints, size=min(NSAMPLE, args.npoints), replace=False)
@@ -375,7 +397,8 @@ def main():
     err_mx = rel(pot_mx.cpu().numpy())
     err_64 = rel(drive_fmm(None, w_64, [q_dev])[0].cpu().numpy()) if w_64 is not None else None
 
-    stage_ms, roof = stage_breakdown(w_mx, trav, q_dev, dev)
+    pipes = pipe_peaks_measured(dev)
+    stage_ms, roof, roof_m2l = stage_breakdown(w_mx, trav, q_dev, dev, pipe_peaks=pipes)
     adj = adjoint_bench(dev) if world == 1 else None
     batch = batched_bench(dev) if world == 1 and not args.no_batch else None
     helm = helmholtz_bench(dev) if world == 1 and not args.no_helmholtz else None
@@ -391,7 +414,8 @@ def main():
             "workload": f"laplace3d_fmm_sphere_plummer_n{args.npoints}_p{args.order}",
             "npoints": args.npoints, "order": args.order,
             "max_particles_in_box": MAX_PARTICLES, "exclude_self": True,
-            "precision": "mixed (FP32 near field with FP64 offsets and sums; FP64 elsewhere)",
+            "precision": "mixed (FP32 near field, M2P, P2L with FP64 offsets and sums; "
+                         "3xTF32 tensor-core M2L and M2M; FP64 elsewhere)",
             "l2": "flushed between steps (256 MB write outside the timed events)",
             "parallelism": f"replicas x{world}",
             "tree_build_s": round(t_tree, 3), "setup_s": round(t_setup, 3),
@@ -401,6 +425,8 @@ def main():
         "fp64": {"value": (world * args.npoints / (ms_64 * 1e-3) / 1e6) if ms_64 else None,
                  "ms_per_step": ms_64},
         "mixed_over_fp64": (ms_64 / ms_mx) if ms_64 else None,
+        "fp64_own_best_tree": fp64_best,
+        "mixed_over_fp64_own_best": (fp64_best["ms_per_step"] / ms_mx) if fp64_best else None,
         "adjoint_forward_ratio": adj["ratio"] if adj else None,
         "adjoint": adj,
         "batched": batch,
@@ -408,6 +434,8 @@ def main():
         "uniform_p6": uni,
         "stage_ms": stage_ms,
         "roofline": roof,
+        "roofline_m2l": roof_m2l,
+        "measured_pipe_peaks": pipes,
         "cpu_baseline": cpu_line,
         "e2e": {"value": world * args.npoints / (ms_e2e * 1e-3) / 1e6, "unit": "Mpts/s",
                 "h2d_bytes_per_step": 8 * args.npoints, "d2h_bytes_per_step": 8 * args.npoints},
@@ -443,8 +471,8 @@ def adjoint_bench(dev, steps=3, ns=200_000, nt=50_000, order=8):
     q = rng.standard_normal(ns)
     knl = [LaplaceKernel(3)]
     (phi_ref,) = P2P(knl)(None, tgt, u, (q,), device=dev)
-    cfg = _Config(order, 32, "mixed", dev)
-    tree, trav, tcls = build_all(src, tgt, 32)
+    cfg = _Config(order, ADJOINT_MAX_PARTICLES, "mixed", dev)
+    tree, trav, tcls = build_all(src, tgt, ADJOINT_MAX_PARTICLES)
     tree_t, trav_t, tcls_t = transpose_traversal(tree, trav, tcls)
     wf = _wrangler(cfg, tree, trav, tcls, False, gradient=False)
     wb = _wrangler(cfg, tree_t, trav_t, tcls_t, False, gradient=True)
@@ -518,7 +546,7 @@ def batched_bench(dev, steps=5, warmup=3, nproblems=512, order=8, nseq=16):
     srcs, qs = batch_problems(nproblems)
     ntot = sum(q.size for q in qs)
     t0 = time.perf_counter()
-    b = BatchedLaplaceFMM(srcs, order=order, max_particles_in_box=MAX_PARTICLES,
+    b = BatchedLaplaceFMM(srcs, order=order, max_particles_in_box=BATCH_MAX_PARTICLES,
                           precision="mixed", bbox=box, device=dev, use_graph=True,
                           autotune=True)
     t_build = time.perf_counter() - t0
@@ -558,7 +586,7 @@ def batched_bench(dev, steps=5, warmup=3, nproblems=512, order=8, nseq=16):
         exclude_self=True)
     seq = []
     for i in range(nseq):
-        _, trav, tcls = build_all(srcs[i], None, MAX_PARTICLES, bbox=box)
+        _, trav, tcls = build_all(srcs[i], None, BATCH_MAX_PARTICLES, bbox=box)
         wr = SumpyExpansionWrangler(ti, trav, np.float64, lambda *a: order,
                                     translation_classes_data=tcls, precision="mixed",
                                     device=dev)
@@ -672,7 +700,7 @@ def helmholtz_bench(dev, steps=3, warmup=2, npoints=500_000, order=14, k=10.0,
     pts = g / np.linalg.norm(g, axis=0)
     q = rng.standard_normal(npoints) + 1j * rng.standard_normal(npoints)
     t0 = time.perf_counter()
-    tree, trav, tcls = build_all(pts, None, MAX_PARTICLES)
+    tree, trav, tcls = build_all(pts, None, HELMHOLTZ_MAX_PARTICLES)
     t_tree = time.perf_counter() - t0
     knl = HelmholtzKernel(3)
     ti = SumpyTreeIndependentDataForWrangler(
@@ -700,7 +728,7 @@ def helmholtz_bench(dev, steps=3, warmup=2, npoints=500_000, order=14, k=10.0,
                                            target_to_source=smp, device=dev, k=k)
     ref = ref.cpu().numpy()
     out = {"workload": f"unit sphere n={npoints}, k={k}, p={order}, complex strengths, "
-                       f"exclude_self, max {MAX_PARTICLES} per box",
+                       f"exclude_self, max {HELMHOLTZ_MAX_PARTICLES} per box",
            "tree_build_s": round(t_tree, 3), "m2l_entries": int(len(trav.from_sep_siblings_lists))}
     for precision in precisions:
         t0 = time.perf_counter()
@@ -722,7 +750,7 @@ def helmholtz_bench(dev, steps=3, warmup=2, npoints=500_000, order=14, k=10.0,
                                                    np.linalg.norm(ref)),
                           "setup_s": round(setup, 2)}
         if precision == "mixed":
-            out["stage_ms_mixed"], _ = stage_breakdown(w, trav, qd, dev, roofline=False)
+            out["stage_ms_mixed"] = stage_breakdown(w, trav, qd, dev, roofline=False)[0]
             # adjoint with respect to the strengths: the FMM on the transposed
             # traversal (sumpy_b200.autograd.HelmholtzFMM's backward)
             from sumpy_b200.adjoint import transpose_traversal
@@ -743,7 +771,7 @@ def helmholtz_bench(dev, steps=3, warmup=2, npoints=500_000, order=14, k=10.0,
     return out
 
 
-def stage_breakdown(w, trav, q_dev, dev, roofline=True):
+def stage_breakdown(w, trav, q_dev, dev, roofline=True, pipe_peaks=None):
     """Per-stage device times of one FMM (CUDA events between the wrangler
     calls on the launching stream) and the roofline of the dominant stage."""
     import torch
@@ -796,9 +824,9 @@ def stage_breakdown(w, trav, q_dev, dev, roofline=True):
     passes = [one_pass() for _ in range(3)]
     stage = {k: float(np.median([ps[k] for ps in passes])) for k in passes[0]}
     if not roofline:
-        return stage, None
+        return stage, None, None
 
-    # algorithmic work
+    # algorithmic work per stage (the units the stage processes)
     tree = w.tree
     n = (w.level_orders[0] + 1) ** 2
     tb = trav.target_boxes
@@ -811,34 +839,109 @@ def stage_breakdown(w, trav, q_dev, dev, roofline=True):
     src_per_list = np.where(empty, 0, src_per_list)
     pairs = int((cnt_t * src_per_list).sum()) - (tree.ntargets if tree.sources_are_targets else 0)
     m2l_entries = len(trav.from_sep_siblings_lists)
-    work = {
-        "p2p": {"flops": 11 * pairs, "pairs": pairs},
-        "m2l": {"flops": 2 * n * n * m2l_entries, "entries": m2l_entries},
+    m2p_pairs = 0
+    for tbs, csr in zip(trav.target_boxes_sep_smaller_by_source_level,
+                        trav.from_sep_smaller_by_level):
+        if len(tbs):
+            m2p_pairs += int((tree.box_target_counts_nonchild[np.asarray(tbs)].astype(np.int64)
+                              * np.diff(np.asarray(csr.starts))).sum())
+    mixed = w.precision == "mixed"
+    kernels = {
+        "m2l": "m2l_tf32x3_kernel" if mixed else "m2l_f64_kernel<128>",
+        "m2p": "m2p_mixed_kernel<P>" if mixed else "m2p_reg_kernel<P>",
+        "p2p": "p2p_csr_kernel<mixed>" if mixed else "p2p_csr_kernel<f64>",
+        "p2l": "p2l_mixed_kernel<P>" if mixed else "p2l_reg_kernel<P>",
     }
-    dom = max(("p2p", "m2l"), key=lambda k: stage[k])
-    ach = work[dom]["flops"] / (stage[dom] * 1e-3) / 1e12
-    peak = peaks.get("bf16_tflops", 1590.0)
-    roof = {
-        "kernel": {"p2p": "p2p_csr_kernel<mixed>" if w.precision == "mixed" else "p2p_csr_kernel<f64>",
-                   "m2l": "m2l_tf32x3_kernel" if w.precision == "mixed" else "m2l_f64_kernel<128>"}[dom],
-        "bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
-        "frac": ach / peak, "traffic": None,
-        "peak_source": "MEASURED_PEAKS.json bf16_tflops (of measured)" if peaks else "fallback",
-        "work": work[dom],
-    }
-    if dom == "m2l" and w.precision == "mixed":
-        roof["note"] = ("tcgen05 split-TF32 GEMM; algorithmic flops = 2 n^2 per List-2 entry "
-                        "(not the x3 split products, empty slots or padding); the stage time "
-                        "includes the TF32 split pre-pass (~1.4 % of it)")
-        if tree.nsources == NPOINTS and n == (ORDER + 1) ** 2:
-            # dram__bytes_read.sum + dram__bytes_write.sum of this launch on this workload,
-            # one ncu capture: profiles/m2l_tf32x3_sphere_plummer_1M_p10.md
-            roof["traffic"] = 1.227e9 + 0.195e9
-            roof["traffic_unit"] = "bytes per launch (ncu capture)"
+    peak_bf16 = peaks.get("bf16_tflops", 1590.0)
+    peak_hbm = peaks.get("hbm_gbs", 6650.0)
+    src = "MEASURED_PEAKS.json (of measured)" if peaks else "fallback"
+
+    def m2l_roof():
+        ach = 2 * n * n * m2l_entries / (stage["m2l"] * 1e-3) / 1e12
+        r = {"kernel": kernels["m2l"], "bound": "tensor", "achieved": ach, "peak": peak_bf16,
+             "unit": "TFLOP/s", "frac": ach / peak_bf16, "traffic": None,
+             "peak_source": "bf16_tflops " + src,
+             "work": {"flops": 2 * n * n * m2l_entries, "entries": m2l_entries,
+                      "per_unit": "2 n^2 flops per List-2 entry"}}
+        if mixed:
+            r["note"] = ("tcgen05 split-TF32 GEMM; algorithmic flops = 2 n^2 per List-2 entry "
+                         "(not the x3 split products, empty slots or padding); the stage time "
+                         "includes the TF32 split pre-pass")
+        # dram__bytes_read.sum + dram__bytes_write.sum of this launch on the 1M-point
+        # workload, one ncu capture per leaf size (profiles/m2l_tf32x3_sphere_plummer_1M_p10.md)
+        captured = {32: 1.227e9 + 0.195e9, 96: 247.1e6 + 37.3e6}
+        if mixed and tree.nsources == NPOINTS and n == (ORDER + 1) ** 2 and \
+                MAX_PARTICLES in captured and \
+                int(tree.box_source_counts_nonchild.max()) <= MAX_PARTICLES:
+            r["traffic"] = captured[MAX_PARTICLES]
+            r["traffic_unit"] = "bytes per launch (ncu capture)"
+        return r
+
+    # the dominant stage, with the stage's own roofline: M2L the tensor cores,
+    # P2P the FP32 (mixed) / FP64 pipe, M2P and P2L HBM with 40 B per
+    # evaluation (one target's or source's coordinates and value) -- they are
+    # compute-bound at this order, so their FLOP/s against the measured
+    # FP32/FP64 GEMM rate as well
+    dom = max(("m2l", "m2p", "p2p", "p2l"), key=lambda k: stage[k])
+    fp = pipe_peaks or {}
+    if dom == "m2l":
+        roof = m2l_roof()
+    elif dom == "p2p":
+        pk = fp.get("fp32_tflops" if mixed else "fp64_tflops")
+        ach = 11 * pairs / (stage["p2p"] * 1e-3) / 1e12
+        roof = {"kernel": kernels["p2p"], "bound": "fp32" if mixed else "fp64",
+                "achieved": ach, "peak": pk, "unit": "TFLOP/s",
+                "frac": (ach / pk) if pk else None, "traffic": None,
+                "peak_source": "torch.matmul FP32/FP64 GEMM measured in this run",
+                "work": {"flops": 11 * pairs, "pairs": pairs, "per_unit": "11 flops per pair"}}
     else:
-        roof["note"] = ("CUDA-core kernel: its own pipe peak is below the bf16 tensor figure "
-                        "used as the denominator")
-    return stage, roof
+        units = m2p_pairs if dom == "m2p" else int(
+            tree.box_source_counts_nonchild[np.asarray(trav.from_sep_bigger_lists)].sum())
+        nbytes = 40 * units
+        flops = units * 10 * n
+        ach = nbytes / (stage[dom] * 1e-3) / 1e9
+        pk = fp.get("fp32_tflops" if mixed else "fp64_tflops")
+        ftf = flops / (stage[dom] * 1e-3) / 1e12
+        roof = {"kernel": kernels[dom], "bound": "hbm", "achieved": ach, "peak": peak_hbm,
+                "unit": "GB/s", "frac": ach / peak_hbm, "traffic": None,
+                "peak_source": "hbm_gbs " + src,
+                "work": {"bytes": nbytes, "evaluations": units,
+                         "per_unit": "40 B per (target, List-3 box) / (List-4 source, box)"},
+                "flops": {"achieved_tflops": ftf, "peak_tflops": pk,
+                          "per_unit": "~10 n flops per evaluation",
+                          "frac": (ftf / pk) if pk else None}}
+    roof["dominant_stage"] = dom
+    return stage, roof, m2l_roof()
+
+
+def pipe_peaks_measured(dev):
+    """FP32 and FP64 CUDA-core rates measured here: torch.matmul GEMMs with
+    TF32 disabled (cuBLAS SGEMM / DGEMM), best of 5, CUDA events."""
+    import torch
+    out = {}
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        for name, dt, m in (("fp32_tflops", torch.float32, 8192),
+                            ("fp64_tflops", torch.float64, 4096)):
+            a = torch.randn(m, m, device=dev, dtype=dt)
+            b = torch.randn(m, m, device=dev, dtype=dt)
+            torch.matmul(a, b)
+            best = None
+            for _ in range(5):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                torch.matmul(a, b)
+                e1.record()
+                torch.cuda.synchronize()
+                t = e0.elapsed_time(e1)
+                best = t if best is None else min(best, t)
+            out[name] = 2.0 * m ** 3 / (best * 1e-3) / 1e12
+            del a, b
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+    return out
 
 
 if __name__ == "__main__":

@@ -641,6 +641,8 @@ p2l_reg_kernel(double rscale, int32_t ntgt_boxes, const int32_t *__restrict__ ta
 // center - source) rounded to FP32, the derivative layers and the products
 // with the coefficients in FP32, per List-3 box / per source; sums over
 // boxes (M2P) and sources (P2L) in FP64.
+constexpr int M2P_GROUPS = 8;   // lane groups (List-3 boxes in flight) per warp, mixed M2P
+
 template <int P>
 __global__ void __launch_bounds__(32 * E2P_WARPS)
 m2p_mixed_kernel(double rscale, int32_t ntgt_boxes, const int32_t *__restrict__ target_boxes,
@@ -651,20 +653,21 @@ m2p_mixed_kernel(double rscale, int32_t ntgt_boxes, const int32_t *__restrict__ 
                  int64_t tstride, double scale, double *__restrict__ result)
 {
     constexpr int N = (P + 1) * (P + 1);
-    // per warp: the multipoles of the (up to 32) List-3 boxes of one round,
-    // one per lane group, as FP32 (read back as broadcasts within a group)
+    // per warp: the multipoles of the (up to M2P_GROUPS) List-3 boxes of one
+    // round, one per lane group, as FP32 (read back as broadcasts within a
+    // group); lane groups have at least 32 / M2P_GROUPS lanes
     extern __shared__ float smm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ib = blockIdx.x * E2P_WARPS + warp;
     if (ib >= ntgt_boxes) return;
-    float *Ms = smm + warp * (32 * N);
+    float *Ms = smm + warp * (M2P_GROUPS * N);
     const int32_t tb = target_boxes[ib];
     const int32_t t0 = bts[tb], nt = btc[tb];
     const int32_t ls = src_starts[ib], le = src_starts[ib + 1];
     const float R = (float)rscale, Rinv = (float)(1.0 / rscale);
     for (int32_t tc = 0; tc < nt; tc += 32) {
         const int ntc = min(32, nt - tc);
-        int g = 1;
+        int g = 32 / M2P_GROUPS;
         while (g < ntc) g <<= 1;
         const int nph = 32 / g;
         const int tl = lane & (g - 1), ph = lane / g;
@@ -1035,10 +1038,11 @@ int sumpy_e2p_from_csr_mixed(int order, double rscale, int32_t ntgt_boxes,
         return bad_arg("m2p mixed: null pointer argument");
     const int blocks = (ntgt_boxes + E2P_WARPS - 1) / E2P_WARPS;
 #define CALL_M2PM(P)                                                                             \
-    (prepare_smem(m2p_mixed_kernel<P>, sizeof(float) * 32 * (P + 1) * (P + 1) * E2P_WARPS)      \
+    (prepare_smem(m2p_mixed_kernel<P>,                                                           \
+                  sizeof(float) * M2P_GROUPS * (P + 1) * (P + 1) * E2P_WARPS)                    \
          ? SUMPY_ELAUNCH                                                                         \
          : (m2p_mixed_kernel<P><<<blocks, 32 * E2P_WARPS,                                        \
-                                  sizeof(float) * 32 * (P + 1) * (P + 1) * E2P_WARPS,            \
+                                  sizeof(float) * M2P_GROUPS * (P + 1) * (P + 1) * E2P_WARPS,    \
                                   as_stream(stream)>>>(                                          \
                 rscale, ntgt_boxes, target_boxes, source_box_starts, source_box_lists, centers, \
                 center_stride, src_base_ibox, src_expansions, box_target_starts,                \
