@@ -338,6 +338,39 @@ int sumpy_p2e_from_csr_mixed(
     const double *sources, int64_t source_stride, const double *strength,
     int32_t tgt_base_ibox, double *tgt_expansions, void *stream);
 
+/* The mixed List-3 and List-4 stages of all levels in one launch each, over
+ * work items cut by the host (the per-level E2PFromCSR / P2EFromCSR calls of
+ * sumpy/fmm.py:600-690 merged; same arithmetic as the _mixed entries above).
+ * All levels share one order; expansions are the flat [nboxes][(order+1)^2]
+ * arrays (box-major over all levels, as with a level-independent order).
+ *
+ * sumpy_mpoles_to_f32: dst[b][s] = (float) src[b][s] for s < (order+1)^2,
+ *   0 up to the row stride npad = ((order+1)^2 + 3) & ~3.
+ * sumpy_e2p_from_items_mixed: items int32 [nitems][4] (16-byte aligned) =
+ *   {first target, first index into source_box_lists, number of List-3
+ *   boxes, ntargets (1..32) | source level << 8}; the item's targets are
+ *   consecutive; level_rscales[level] is that level's rscale;
+ *   src_expansions_f32 from sumpy_mpoles_to_f32 (16-byte aligned). Adds
+ *   scale * potential into result with atomics.
+ * sumpy_p2e_from_items_mixed: items {target box, first index into
+ *   source_index, number of sources, target level}; source_index lists the
+ *   sources of each target box's List-4 boxes. Adds into tgt_expansions
+ *   ([nboxes][(order+1)^2]) with atomics. */
+int sumpy_mpoles_to_f32(int order, int64_t nboxes, const double *src_expansions, float *dst,
+                        void *stream);
+
+int sumpy_e2p_from_items_mixed(
+    int order, int32_t nitems, const int32_t *items, const double *level_rscales,
+    const int32_t *source_box_lists, const double *centers, int64_t center_stride,
+    const float *src_expansions_f32, const double *targets, int64_t target_stride,
+    double scale, double *result, void *stream);
+
+int sumpy_p2e_from_items_mixed(
+    int order, int32_t nitems, const int32_t *items, const double *level_rscales,
+    const int32_t *source_index, const double *centers, int64_t center_stride,
+    const double *sources, int64_t source_stride, const double *strength,
+    double *tgt_expansions, void *stream);
+
 /* ------------------------------------------------------------------------
  * 3D Helmholtz kernel G = exp(i k r) / r (sumpy/kernel.py:755-844), the same
  * loopy kernels as above instantiated for HelmholtzKernel(3): complex data

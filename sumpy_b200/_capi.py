@@ -58,6 +58,11 @@ SIGNATURES = {
                                  ptr, i64, dbl, ptr, ptr],
     "sumpy_p2e_from_csr_mixed": [cint, dbl, i32, ptr, ptr, ptr, ptr, i64, ptr, ptr, ptr,
                                  i64, ptr, i32, ptr, ptr],
+    "sumpy_mpoles_to_f32": [cint, i64, ptr, ptr, ptr],
+    "sumpy_e2p_from_items_mixed": [cint, i32, ptr, ptr, ptr, ptr, i64, ptr, ptr, i64, dbl,
+                                   ptr, ptr],
+    "sumpy_p2e_from_items_mixed": [cint, i32, ptr, ptr, ptr, ptr, i64, ptr, i64, ptr, ptr,
+                                   ptr],
     # Helmholtz
     "sumpy_helmholtz_p2p_from_csr_f64": [i32, ptr, ptr, ptr, ptr, ptr, ptr, ptr, ptr, i64, dbl,
                                          ptr, ptr, i64, ptr, dbl, ptr, ptr],

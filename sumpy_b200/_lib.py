@@ -54,15 +54,41 @@ def _cuda_sources():
     return [CSRC / s for s in CU_SOURCES]
 
 
+OBJ_DIR = ROOT / "_build"
+
+
 def build_cuda_library(force=False, extra_flags=()) -> Path:
+    """Compile each CUDA source to an object under ``_build/`` (in parallel,
+    only those older than their source or a header), then link the shared
+    library."""
+    from concurrent.futures import ThreadPoolExecutor
     srcs = _cuda_sources()
     headers = list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
-    newest = max(p.stat().st_mtime for p in srcs + headers)
-    if force or not CUDA_LIB.exists() or CUDA_LIB.stat().st_mtime < newest:
-        cmd = [NVCC, *ARCH_FLAGS, "-O3", "-lineinfo", "-std=c++17", "-shared",
-               "-Xcompiler", "-fPIC", "-ccbin", HOST_CXX, "-I", str(INCLUDE),
-               "-o", str(CUDA_LIB), *map(str, srcs), *extra_flags]
-        _run(cmd)
+    newest_header = max(p.stat().st_mtime for p in headers)
+    objs = [OBJ_DIR / (s.stem + ".o") for s in srcs]
+    # without objects (a copied tree): a library newer than every source is current
+    if not force and not extra_flags and not any(o.exists() for o in objs) and \
+            CUDA_LIB.exists() and CUDA_LIB.stat().st_mtime >= max(
+                newest_header, max(p.stat().st_mtime for p in srcs)):
+        return CUDA_LIB
+    OBJ_DIR.mkdir(exist_ok=True)
+    stale = [(s, o) for s, o in zip(srcs, objs)
+             if force or extra_flags or not o.exists()
+             or o.stat().st_mtime < max(s.stat().st_mtime, newest_header)]
+
+    def compile_one(so):
+        s, o = so
+        _run([NVCC, *ARCH_FLAGS, "-O3", "-lineinfo", "-std=c++17", "-c",
+              "-Xcompiler", "-fPIC", "-ccbin", HOST_CXX, "-I", str(INCLUDE),
+              "-o", str(o), str(s), *extra_flags])
+
+    if stale:
+        with ThreadPoolExecutor(max_workers=len(stale)) as ex:
+            list(ex.map(compile_one, stale))
+    if stale or not CUDA_LIB.exists() or \
+            CUDA_LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
+        _run([NVCC, *ARCH_FLAGS, "-shared", "-ccbin", HOST_CXX, "-o", str(CUDA_LIB),
+              *map(str, objs)])
     return CUDA_LIB
 
 

@@ -757,6 +757,196 @@ p2l_mixed_kernel(double rscale, int32_t ntgt_boxes, const int32_t *__restrict__ 
     }
 }
 
+// {{{ mixed M2P / P2L over flat work items (all levels in one launch)
+
+// The per-level launches above give one warp a whole target box: a box
+// with a long List 3 (up to ~300 rounds at 1M points) runs alone at the end
+// of its level while the rest of the GPU idles, and the levels run one after
+// another. Here the host cuts the work into items of a few rounds each,
+// over all levels, longest first; items of one target box add their partial
+// sums with FP64 atomics.
+
+__device__ __forceinline__ void cpa16(void *dst, const void *src)
+{
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int NPEND>
+__device__ __forceinline__ void cpa_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(NPEND) : "memory");
+}
+
+// stored coefficients per box in the FP32 multipole copy: N rounded up to a
+// multiple of 4 (16-byte rows for cp.async)
+__host__ __device__ constexpr int npad_of(int p) { return (((p + 1) * (p + 1)) + 3) & ~3; }
+
+constexpr int ITEM_WARPS = 4;
+#ifndef SUMPY_P2L_REG_MAX_N
+#define SUMPY_P2L_REG_MAX_N 128   // P2L items keep per-lane sums in registers up to this N
+#endif
+constexpr int M2PI_GROUPS = 8;   // max lane groups (List-3 boxes in flight) per warp
+
+// FP64 multipoles [nboxes][N] -> FP32 [nboxes][NP], zero padded
+__global__ void mpole_f32_kernel(int n, int np, int64_t nboxes, const double *__restrict__ src,
+                                 float *__restrict__ dst)
+{
+    const int64_t total = nboxes * np;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = e / np;
+        const int s = (int)(e - b * np);
+        dst[e] = s < n ? (float)src[b * n + s] : 0.f;
+    }
+}
+
+// item = {first target, first List-3 entry, number of List-3 boxes,
+//         targets (1..32) | source level << 8}
+template <int P>
+__global__ void __launch_bounds__(32 * ITEM_WARPS)
+m2p_items_kernel(int32_t nitems, const int4 *__restrict__ items,
+                 const double *__restrict__ level_rscale, const int32_t *__restrict__ src_lists,
+                 const double *__restrict__ centers, int64_t cstride,
+                 const float *__restrict__ mp32, const double *__restrict__ targets,
+                 int64_t tstride, double scale, double *__restrict__ result)
+{
+    constexpr int NP = npad_of(P);
+    constexpr int C = NP / 4;
+    extern __shared__ __align__(16) float smi[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int it = blockIdx.x * ITEM_WARPS + warp;
+    if (it >= nitems) return;
+    float *buf = smi + warp * (2 * M2PI_GROUPS * NP);
+    const int4 item = items[it];
+    const int32_t t0 = item.x, l0 = item.y, nb = item.z;
+    const int ntc = item.w & 0xff, lev = item.w >> 8;
+    int g = 32 / M2PI_GROUPS;
+    while (g < ntc) g <<= 1;
+    const int nph = 32 / g;
+    const int tl = lane & (g - 1), ph = lane / g;
+    const bool active = tl < ntc;
+    const int32_t t = t0 + tl;
+    double tx = 0, ty = 0, tz = 0;
+    if (active) { tx = targets[t]; ty = targets[tstride + t]; tz = targets[2 * tstride + t]; }
+    const double rs = level_rscale[lev];
+    const float R = (float)rs, Rinv = (float)(1.0 / rs);
+    const int nrounds = (nb + nph - 1) / nph;
+
+    // round r's boxes (nph at most) into buffer r & 1
+    auto stage = [&](int r) {
+        const int first = r * nph, cnt = min(nph, nb - first);
+        float *dst = buf + (r & 1) * (M2PI_GROUPS * NP);
+        for (int e = lane; e < cnt * C; e += 32) {
+            const int k = e / C, c = e - k * C;
+            const int32_t sb = src_lists[l0 + first + k];
+            cpa16(dst + k * NP + 4 * c, mp32 + (int64_t)sb * NP + 4 * c);
+        }
+        cpa_commit();
+    };
+    stage(0);
+    double acc = 0.0;
+    for (int r = 0; r < nrounds; ++r) {
+        if (r + 1 < nrounds) {
+            stage(r + 1);
+            cpa_wait<1>();
+        } else {
+            cpa_wait<0>();
+        }
+        __syncwarp();
+        const int k = r * nph + ph;
+        if (active && k < nb) {
+            const int32_t sb = src_lists[l0 + k];
+            const float *M = buf + (r & 1) * (M2PI_GROUPS * NP) + ph * NP;
+            // four partial sums: a dependent chain of N / 4 FMAs, not N
+            float a4[4] = {0.f, 0.f, 0.f, 0.f};
+            laplace_layers<P, float>(
+                (float)(tx - centers[sb]), (float)(ty - centers[cstride + sb]),
+                (float)(tz - centers[2 * cstride + sb]), R, Rinv,
+                [&](int s, int, int, int, float v) { a4[s & 3] = fmaf(M[s], v, a4[s & 3]); });
+            acc += (double)((a4[0] + a4[1]) + (a4[2] + a4[3]));
+        }
+        __syncwarp();   // buffer r & 1 is refilled by round r + 2's copies
+    }
+    for (int off = g; off < 32; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if (active && ph == 0) atomicAdd(result + t, scale * acc);
+}
+
+// P2L item = {target box, first entry of the flat List-4 source index
+// array, number of sources (<= 32 * rounds), target level}. Each lane keeps
+// its own FP32 sums q D over its sources in registers (N <= 128) and the
+// warp transposes them through shared memory once per item; higher orders
+// transpose every round.
+template <int P>
+__global__ void __launch_bounds__(32 * ITEM_WARPS)
+p2l_items_kernel(int32_t nitems, const int4 *__restrict__ items,
+                 const double *__restrict__ level_rscale, const int32_t *__restrict__ src_index,
+                 const double *__restrict__ centers, int64_t cstride,
+                 const double *__restrict__ sources, int64_t sstride, const double *__restrict__ q,
+                 double *__restrict__ out)
+{
+    constexpr int N = (P + 1) * (P + 1);
+    constexpr int NPL = (N + 31) / 32;
+    constexpr bool REG = N <= SUMPY_P2L_REG_MAX_N;
+    extern __shared__ float smf[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int it = blockIdx.x * ITEM_WARPS + warp;
+    if (it >= nitems) return;
+    float *D = smf + warp * (N * DSTRIDE);
+    const int4 item = items[it];
+    const int32_t tb = item.x, f0 = item.y, cnt = item.z, lev = item.w;
+    const double c0 = centers[tb], c1 = centers[cstride + tb], c2 = centers[2 * cstride + tb];
+    const double rs = level_rscale[lev];
+    const float R = (float)rs, Rinv = (float)(1.0 / rs);
+    float own[REG ? N : 1];
+#pragma unroll
+    for (int s = 0; s < (REG ? N : 1); ++s) own[s] = 0.f;
+    double acc[NPL];
+#pragma unroll
+    for (int m = 0; m < NPL; ++m) acc[m] = 0.0;
+
+    auto transpose_sum = [&](int nsrc) {
+        __syncwarp();
+#pragma unroll
+        for (int m = 0; m < NPL; ++m) {
+            const int k = lane + 32 * m;
+            if (k < N) {
+                float sum = 0.f;
+                for (int l2 = 0; l2 < nsrc; ++l2) sum += D[k * DSTRIDE + l2];
+                acc[m] += (double)sum;
+            }
+        }
+        __syncwarp();
+    };
+    for (int32_t base = 0; base < cnt; base += 32) {
+        const int nsc = min(32, cnt - base);
+        if (lane < nsc) {
+            const int32_t s = src_index[f0 + base + lane];
+            const float qq = (float)q[s];
+            laplace_layers<P, float>(
+                (float)(c0 - sources[s]), (float)(c1 - sources[sstride + s]),
+                (float)(c2 - sources[2 * sstride + s]), R, Rinv, [&](int k, int, int, int, float v) {
+                    if constexpr (REG) own[k] = fmaf(qq, v, own[k]);
+                    else D[k * DSTRIDE + lane] = qq * v;
+                });
+        }
+        if constexpr (!REG) transpose_sum(nsc);
+    }
+    if constexpr (REG) {
+#pragma unroll
+        for (int s = 0; s < N; ++s) D[s * DSTRIDE + lane] = own[s];
+        transpose_sum(min(32, cnt));
+    }
+    double *o = out + (int64_t)tb * N;
+#pragma unroll
+    for (int m = 0; m < NPL; ++m) {
+        const int k = lane + 32 * m;
+        if (k < N) atomicAdd(o + k, acc[m]);
+    }
+}
+
+// }}}
+
 template <int P, bool GRAD>
 int launch_m2p_reg(double rscale, int32_t ntgt_boxes, const int32_t *target_boxes,
                    const int32_t *src_starts, const int32_t *src_lists, const double *centers,
@@ -1081,6 +1271,78 @@ int sumpy_p2e_from_csr_mixed(int order, double rscale, int32_t ntgt_boxes,
             check_launch("p2l_mixed_kernel")))
     SUMPY_ORDER_SWITCH(order, CALL_P2LM)
 #undef CALL_P2LM
+}
+
+int sumpy_mpoles_to_f32(int order, int64_t nboxes, const double *src_expansions, float *dst,
+                        void *stream)
+{
+    if (!order_ok(order)) { set_last_error("mpoles_to_f32: unsupported order"); return SUMPY_EUNSUPPORTED; }
+    if (nboxes < 0) return bad_arg("mpoles_to_f32: nboxes < 0");
+    if (nboxes == 0) return SUMPY_OK;
+    if (!src_expansions || !dst) return bad_arg("mpoles_to_f32: null pointer argument");
+    const int np = npad_of(order);
+    const int64_t total = nboxes * np;
+    const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
+    mpole_f32_kernel<<<blocks, 256, 0, as_stream(stream)>>>(ncoeff_of(order), np, nboxes,
+                                                            src_expansions, dst);
+    return check_launch("mpole_f32_kernel");
+}
+
+int sumpy_e2p_from_items_mixed(int order, int32_t nitems, const int32_t *items,
+                               const double *level_rscales, const int32_t *source_box_lists,
+                               const double *centers, int64_t center_stride,
+                               const float *src_expansions_f32, const double *targets,
+                               int64_t target_stride, double scale, double *result, void *stream)
+{
+    if (!order_ok(order)) { set_last_error("m2p items: unsupported order"); return SUMPY_EUNSUPPORTED; }
+    if (nitems < 0) return bad_arg("m2p items: nitems < 0");
+    if (nitems == 0) return SUMPY_OK;
+    if (!items || !level_rscales || !source_box_lists || !centers || !src_expansions_f32 ||
+        !targets || !result)
+        return bad_arg("m2p items: null pointer argument");
+    if ((reinterpret_cast<uintptr_t>(items) | reinterpret_cast<uintptr_t>(src_expansions_f32)) & 15)
+        return bad_arg("m2p items: items and FP32 expansions must be 16-byte aligned");
+    const int blocks = (nitems + ITEM_WARPS - 1) / ITEM_WARPS;
+#define CALL_M2PI(P)                                                                             \
+    (prepare_smem(m2p_items_kernel<P>, sizeof(float) * 2 * M2PI_GROUPS * npad_of(P) * ITEM_WARPS) \
+         ? SUMPY_ELAUNCH                                                                         \
+         : (m2p_items_kernel<P><<<blocks, 32 * ITEM_WARPS,                                       \
+                                  sizeof(float) * 2 * M2PI_GROUPS * npad_of(P) * ITEM_WARPS,     \
+                                  as_stream(stream)>>>(                                          \
+                nitems, reinterpret_cast<const int4 *>(items), level_rscales, source_box_lists, \
+                centers, center_stride, src_expansions_f32, targets, target_stride, scale,      \
+                result),                                                                         \
+            check_launch("m2p_items_kernel")))
+    SUMPY_ORDER_SWITCH(order, CALL_M2PI)
+#undef CALL_M2PI
+}
+
+int sumpy_p2e_from_items_mixed(int order, int32_t nitems, const int32_t *items,
+                               const double *level_rscales, const int32_t *source_index,
+                               const double *centers, int64_t center_stride,
+                               const double *sources, int64_t source_stride,
+                               const double *strength, double *tgt_expansions, void *stream)
+{
+    if (!order_ok(order)) { set_last_error("p2l items: unsupported order"); return SUMPY_EUNSUPPORTED; }
+    if (nitems < 0) return bad_arg("p2l items: nitems < 0");
+    if (nitems == 0) return SUMPY_OK;
+    if (!items || !level_rscales || !source_index || !centers || !sources || !strength ||
+        !tgt_expansions)
+        return bad_arg("p2l items: null pointer argument");
+    if (reinterpret_cast<uintptr_t>(items) & 15)
+        return bad_arg("p2l items: items must be 16-byte aligned");
+    const int blocks = (nitems + ITEM_WARPS - 1) / ITEM_WARPS;
+#define CALL_P2LI(P)                                                                             \
+    (prepare_smem(p2l_items_kernel<P>, sizeof(float) * (P + 1) * (P + 1) * DSTRIDE * ITEM_WARPS) \
+         ? SUMPY_ELAUNCH                                                                         \
+         : (p2l_items_kernel<P><<<blocks, 32 * ITEM_WARPS,                                       \
+                                  sizeof(float) * (P + 1) * (P + 1) * DSTRIDE * ITEM_WARPS,      \
+                                  as_stream(stream)>>>(                                          \
+                nitems, reinterpret_cast<const int4 *>(items), level_rscales, source_index,     \
+                centers, center_stride, sources, source_stride, strength, tgt_expansions),      \
+            check_launch("p2l_items_kernel")))
+    SUMPY_ORDER_SWITCH(order, CALL_P2LI)
+#undef CALL_P2LI
 }
 
 }  // extern "C"

@@ -47,6 +47,100 @@ _d = _capi.dbl
 M2L_TILE = 64          # FP64 GEMM tile (target boxes)
 M2L_TILE_TC = 128      # tensor-core tile (MMA N)
 M2L_ITEM_GROUPS = 64   # class groups per tensor-core work item (one CTA)
+ITEM_ROUNDS = 4        # rounds (one source box / 32 sources each) per mixed M2P / P2L item
+M2P_ITEM_GROUPS = 8    # lane groups per warp in the M2P item kernel (fixed by the kernel)
+
+
+def _npad(order):
+    """Row stride of the FP32 multipole copy (sumpy_mpoles_to_f32)."""
+    return ((order + 1) ** 2 + 3) & ~3
+
+
+def _expand_ranges(starts, counts):
+    """Concatenation of range(starts[i], starts[i] + counts[i]) over i."""
+    counts = np.asarray(counts, dtype=np.int64)
+    total = int(counts.sum())
+    if total == 0:
+        return np.zeros(0, dtype=np.int64)
+    first = np.cumsum(counts) - counts
+    return np.repeat(np.asarray(starts, dtype=np.int64) - first, counts) + np.arange(total)
+
+
+def m2p_items(tree, target_boxes_by_source_level, source_boxes_by_level,
+              rounds=ITEM_ROUNDS, groups=M2P_ITEM_GROUPS):
+    """Work items of the one-launch mixed M2P (sumpy_e2p_from_items_mixed).
+
+    Each target box's targets go 32 per chunk; a chunk of ntc targets runs on
+    lane groups of g = max(32 / groups, next_pow2(ntc)) lanes, 32 / g source
+    boxes per round, and an item takes ``rounds`` rounds of its chunk's
+    List-3 boxes. Returns (items int32 [n, 4] longest first, the levels'
+    source box lists concatenated)."""
+    bts = np.asarray(tree.box_target_starts, dtype=np.int64)
+    btc = np.asarray(tree.box_target_counts_nonchild, dtype=np.int64)
+    out, cost, lists = [], [], []
+    off = 0
+    for lev, ssn in enumerate(source_boxes_by_level):
+        tb = np.asarray(target_boxes_by_source_level[lev], dtype=np.int64)
+        lst = np.asarray(ssn.lists, dtype=np.int32)
+        if len(tb) == 0:
+            lists.append(lst)
+            off += len(lst)
+            continue
+        starts = np.asarray(ssn.starts, dtype=np.int64)
+        ln = np.diff(starts)[:len(tb)]
+        nt = btc[tb]
+        nch = np.where((ln > 0) & (nt > 0), (nt + 31) // 32, 0)
+        cb = np.repeat(np.arange(len(tb)), nch)
+        ci = _expand_ranges(np.zeros(len(tb), dtype=np.int64), nch)
+        ntc = np.minimum(32, nt[cb] - 32 * ci)
+        t0 = bts[tb][cb] + 32 * ci
+        g = np.full(len(ntc), 32 // groups, dtype=np.int64)
+        while (g < ntc).any():
+            g = np.where(g < ntc, 2 * g, g)
+        nph = 32 // g
+        per = nph * rounds
+        lnc = ln[cb]
+        nit = (lnc + per - 1) // per
+        ic = np.repeat(np.arange(len(ntc)), nit)
+        j = _expand_ranges(np.zeros(len(ntc), dtype=np.int64), nit)
+        nb = np.minimum(per[ic], lnc[ic] - j * per[ic])
+        l0 = starts[cb][ic] + off + j * per[ic]
+        out.append(np.stack([t0[ic], l0, nb, ntc[ic] | (lev << 8)], axis=1))
+        cost.append((nb + nph[ic] - 1) // nph[ic])
+        lists.append(lst)
+        off += len(lst)
+    if not out:
+        return np.zeros((0, 4), np.int32), np.concatenate(lists) if lists else np.zeros(0, np.int32)
+    items = np.concatenate(out)
+    order = np.argsort(-np.concatenate(cost), kind="stable")
+    return np.ascontiguousarray(items[order], dtype=np.int32), np.concatenate(lists)
+
+
+def p2l_items(tree, level_starts, target_boxes, starts, lists, rounds=ITEM_ROUNDS):
+    """Work items of the one-launch mixed P2L (sumpy_p2e_from_items_mixed):
+    the sources of each target box's List-4 boxes as one flat index array,
+    cut into items of at most 32 * ``rounds`` sources. Returns (items int32
+    [n, 4] longest first, source index int32)."""
+    bss = np.asarray(tree.box_source_starts, dtype=np.int64)
+    bsc = np.asarray(tree.box_source_counts_nonchild, dtype=np.int64)
+    starts = np.asarray(starts, dtype=np.int64)
+    lists = np.asarray(lists, dtype=np.int64)
+    cnt = bsc[lists]
+    src_index = _expand_ranges(bss[lists], cnt)
+    F = np.concatenate([[0], np.cumsum(cnt)])
+    ntb = len(starts) - 1
+    f0 = F[starts[:-1]]
+    n = F[starts[1:]] - f0
+    lev_of = np.repeat(np.arange(len(level_starts) - 1), np.diff(np.asarray(level_starts)))[:ntb]
+    per = 32 * rounds
+    nit = (n + per - 1) // per
+    it = np.repeat(np.arange(ntb), nit)
+    j = _expand_ranges(np.zeros(ntb, dtype=np.int64), nit)
+    c = np.minimum(per, n[it] - j * per)
+    items = np.stack([np.asarray(target_boxes, dtype=np.int64)[it], f0[it] + j * per, c,
+                      lev_of[it]], axis=1)
+    order = np.argsort(-c, kind="stable")
+    return np.ascontiguousarray(items[order], dtype=np.int32), src_index.astype(np.int32)
 
 
 def _np_i32(a):
@@ -161,6 +255,9 @@ class SumpyExpansionWrangler:
         self.tc_m2m = True
         self.tc_l2l = False
         self.gemm_l2l = False
+        # mixed List 3 / List 4: all levels in one launch over host-cut work
+        # items (False: one launch per level, a warp per target box)
+        self.item_kernels = True
         self.m2l_item_groups = int(m2l_item_groups or M2L_ITEM_GROUPS)
         if self.m2l_item_groups < 1:
             raise ValueError("m2l_item_groups must be >= 1")
@@ -820,9 +917,57 @@ class SumpyExpansionWrangler:
 
     # }}}
 
+    @property
+    def _items_path(self):
+        """Mixed Laplace List 3 / List 4 through the one-launch item kernels
+        (needs one order on every level: flat [nboxes][ncoeff] storage)."""
+        return (self.item_kernels and self.precision == "mixed" and not self.helmholtz
+                and not self.gradient and len(set(self.level_orders)) == 1)
+
+    @cached_property
+    def _level_rscales(self):
+        return torch.tensor([self.level_to_rscale(lev) if self.level_orders[lev] else 1.0
+                             for lev in range(self.tree.nlevels)],
+                            dtype=torch.float64, device=self.device)
+
+    def _cached_items(self, key, objs, build):
+        hit = self._devcache.get(key)
+        if hit is not None and all(a is b for a, b in zip(hit[0], objs)):
+            return hit[1]
+        val = build()
+        self._devcache[key] = (objs, val)
+        return val
+
+    def _eval_multipoles_items(self, target_boxes_by_source_level, source_boxes_by_level,
+                               mpole_exps, pot):
+        def build():
+            items, lists = m2p_items(self.tree, target_boxes_by_source_level,
+                                     source_boxes_by_level)
+            return (torch.as_tensor(items).to(self.device),
+                    torch.as_tensor(lists).to(self.device))
+        items, lists = self._cached_items(
+            "m2p_items", (target_boxes_by_source_level, source_boxes_by_level), build)
+        if items.shape[0] == 0:
+            return pot
+        order = self.level_orders[0]
+        g = self._geom
+        st = stream_ptr()
+        mp32 = torch.empty(self.tree.nboxes * _npad(order), dtype=torch.float32,
+                           device=self.device)
+        call("sumpy_mpoles_to_f32", _c(order), _i64(self.tree.nboxes), dptr(mpole_exps),
+             dptr(mp32), st)
+        call("sumpy_e2p_from_items_mixed", _c(order), _i32(items.shape[0]), dptr(items),
+             dptr(self._level_rscales), dptr(lists), dptr(g["centers"]),
+             _i64(self.tree.nboxes), dptr(mp32), dptr(g["targets"]), _i64(self.tree.ntargets),
+             _d(self._scale), dptr(pot[0]), st)
+        return pot
+
     def eval_multipoles(self, actx, target_boxes_by_source_level, source_boxes_by_level,
                         mpole_exps):
         pot = self.output_zeros(actx)
+        if self._items_path:
+            return self._eval_multipoles_items(target_boxes_by_source_level,
+                                               source_boxes_by_level, mpole_exps, pot)
         g = self._geom
         st = stream_ptr()
         for lev, ssn in enumerate(source_boxes_by_level):
@@ -848,6 +993,24 @@ class SumpyExpansionWrangler:
     def form_locals(self, actx, level_start_target_or_target_parent_box_nrs,
                     target_or_target_parent_boxes, starts, lists, src_weight_vecs):
         local_exps = self.local_expansion_zeros(actx)
+        if self._items_path and not isinstance(starts, torch.Tensor) \
+                and not isinstance(lists, torch.Tensor):
+            def build():
+                items, sidx = p2l_items(self.tree, level_start_target_or_target_parent_box_nrs,
+                                        target_or_target_parent_boxes, starts, lists)
+                return (torch.as_tensor(items).to(self.device),
+                        torch.as_tensor(sidx).to(self.device))
+            items, sidx = self._cached_items(
+                "p2l_items", (level_start_target_or_target_parent_box_nrs,
+                              target_or_target_parent_boxes, starts, lists), build)
+            if items.shape[0]:
+                g = self._geom
+                w = self._weights(src_weight_vecs)
+                call("sumpy_p2e_from_items_mixed", _c(self.level_orders[0]),
+                     _i32(items.shape[0]), dptr(items), dptr(self._level_rscales), dptr(sidx),
+                     dptr(g["centers"]), _i64(self.tree.nboxes), dptr(g["sources"]),
+                     _i64(self.tree.nsources), dptr(w), dptr(local_exps), stream_ptr())
+            return local_exps
         lt = _np_i32(level_start_target_or_target_parent_box_nrs)
         starts_h = np.asarray(starts if not isinstance(starts, torch.Tensor)
                               else starts.cpu().numpy())

@@ -1,0 +1,80 @@
+"""The one-launch mixed M2P and P2L (work items over all levels,
+sumpy_e2p_from_items_mixed / sumpy_p2e_from_items_mixed) against the FP64
+stages and the per-level mixed launches they replace, on leaf sizes that give
+long List 3 / List 4 (several items per target box) and short ones.
+
+Tolerance: both mixed forms take FP32 derivatives and products on FP64
+offsets; per stage they agree with FP64 to ~1e-7 relative (asserted 1e-6).
+"""
+import numpy as np
+import pytest
+import torch
+
+from sumpy_b200 import (
+    LaplaceKernel,
+    LinearPDEConformingVolumeTaylorLocalExpansion as LExp,
+    LinearPDEConformingVolumeTaylorMultipoleExpansion as MExp,
+    SumpyExpansionWrangler,
+    SumpyTreeIndependentDataForWrangler,
+    drive_fmm,
+)
+from sumpy_b200.tree import build_all
+from tests._pointsets import sphere_plummer, uniform_cube
+
+pytestmark = pytest.mark.gpu
+
+
+def relerr(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def _wrangler(trav, tcls, order, precision, items, exclude_self):
+    knl = LaplaceKernel(3)
+    ti = SumpyTreeIndependentDataForWrangler(
+        None, lambda o, **kw: MExp(knl, o), lambda o, **kw: LExp(knl, o), [knl],
+        exclude_self=exclude_self)
+    w = SumpyExpansionWrangler(ti, trav, np.float64, lambda *a: order,
+                               translation_classes_data=tcls, precision=precision)
+    w.item_kernels = items
+    return w
+
+
+def _list3_list4(w, trav, q):
+    qd = w.reorder_sources(torch.as_tensor(q, device="cuda"))
+    mp = w.form_multipoles(None, trav.level_start_source_box_nrs, trav.source_boxes, [qd])
+    mp = w.coarsen_multipoles(None, trav.level_start_source_parent_box_nrs,
+                              trav.source_parent_boxes, mp)
+    pm = w.eval_multipoles(None, trav.target_boxes_sep_smaller_by_source_level,
+                           trav.from_sep_smaller_by_level, mp)[0]
+    pl = w.form_locals(None, trav.level_start_target_or_target_parent_box_nrs,
+                       trav.target_or_target_parent_boxes, trav.from_sep_bigger_starts,
+                       trav.from_sep_bigger_lists, [qd])
+    return pm.cpu().numpy(), pl.cpu().numpy()
+
+
+@pytest.mark.parametrize("mpb", [8, 40, 96])
+@pytest.mark.parametrize("order", [4, 10])
+def test_items_match_fp64_and_per_level(cuda_device, mpb, order):
+    src = sphere_plummer(40000, 7)
+    tree, trav, tcls = build_all(src, None, mpb)
+    q = np.random.default_rng(3).standard_normal(src.shape[1])
+    f64 = _list3_list4(_wrangler(trav, tcls, order, "fp64", False, True), trav, q)
+    lev = _list3_list4(_wrangler(trav, tcls, order, "mixed", False, True), trav, q)
+    itm = _list3_list4(_wrangler(trav, tcls, order, "mixed", True, True), trav, q)
+    for k in range(2):
+        assert np.abs(f64[k]).max() > 0
+        assert relerr(itm[k], f64[k]) < 1e-6, (k, relerr(itm[k], f64[k]))
+        assert relerr(itm[k], lev[k]) < 1e-6, (k, relerr(itm[k], lev[k]))
+
+
+def test_items_end_to_end_separate_targets(cuda_device):
+    src, tgt = uniform_cube(20000, 15), uniform_cube(15000, 18)
+    src[:, :5000] *= 0.05          # a dense cluster: long List 3 / List 4
+    tree, trav, tcls = build_all(src, tgt, 24)
+    q = torch.as_tensor(np.random.default_rng(5).standard_normal(src.shape[1]), device="cuda")
+    ref = drive_fmm(None, _wrangler(trav, tcls, 8, "fp64", False, False), [q])[0].cpu()
+    w = _wrangler(trav, tcls, 8, "mixed", True, False)
+    out = drive_fmm(None, w, [q])[0].cpu()
+    w.check_status()
+    assert relerr(out, ref) < 2e-6
