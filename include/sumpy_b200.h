@@ -356,6 +356,30 @@ int sumpy_p2e_from_csr_mixed(
  *   source_index, number of sources, target level}; source_index lists the
  *   sources of each target box's List-4 boxes. Adds into tgt_expansions
  *   ([nboxes][(order+1)^2]) with atomics. */
+/* P2EFromSingleBox (P2M) and E2PFromSingleBox (L2P) of all levels in one
+ * launch each (sumpy/fmm.py:540-563 and 729-760 loop over levels), FP64,
+ * flat [nboxes][(order+1)^2] expansions as above.
+ * sumpy_p2e_from_single_box_levels_f64: box_levels[i] is the level of
+ *   source_boxes[i] (its rscale = level_rscales[level]); any box order (the
+ *   host lists the largest first). Assigns the boxes' multipoles.
+ * sumpy_e2p_from_single_box_packed_f64: items int32 [nitems][2] (8-byte
+ *   aligned) = {first slot, number of slots (1..8)}; slots int32 [][4]
+ *   (16-byte aligned) = {box, first target, number of targets, level}, at
+ *   most 32 targets per item, a box's targets in one or more slots.
+ *   Assigns scale * potential to each listed target. */
+int sumpy_p2e_from_single_box_levels_f64(
+    int order, int32_t nsrc_boxes, const int32_t *source_boxes, const int32_t *box_levels,
+    const double *level_rscales, const double *centers, int64_t center_stride,
+    const int32_t *box_source_starts, const int32_t *box_source_counts_nonchild,
+    const double *sources, int64_t source_stride, const double *strength,
+    double *expansions, void *stream);
+
+int sumpy_e2p_from_single_box_packed_f64(
+    int order, int32_t nitems, const int32_t *items, const int32_t *slots,
+    const double *level_rscales, const double *centers, int64_t center_stride,
+    const double *src_expansions, const double *targets, int64_t target_stride,
+    double scale, double *result, void *stream);
+
 int sumpy_mpoles_to_f32(int order, int64_t nboxes, const double *src_expansions, float *dst,
                         void *stream);
 

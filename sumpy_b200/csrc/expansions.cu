@@ -64,7 +64,9 @@ p2m_warp_kernel(double rscale, int32_t nboxes, const int32_t *__restrict__ boxes
                 const double *__restrict__ centers, int64_t cstride,
                 const int32_t *__restrict__ bss, const int32_t *__restrict__ bsc,
                 const double *__restrict__ sources, int64_t sstride,
-                const double *__restrict__ q, int32_t base, double *__restrict__ out)
+                const double *__restrict__ q, int32_t base, double *__restrict__ out,
+                const int32_t *__restrict__ box_level = nullptr,
+                const double *__restrict__ level_rscale = nullptr)
 {
     constexpr int P1 = P + 1;
     constexpr int NPAIR = P1 * (P1 + 1) / 2;
@@ -81,7 +83,8 @@ p2m_warp_kernel(double rscale, int32_t nboxes, const int32_t *__restrict__ boxes
     const int32_t b = boxes[ib];
     const double c[3] = {centers[b], centers[cstride + b], centers[2 * cstride + b]};
     const int32_t s0 = bss[b], ns = bsc[b];
-    const double rinv = 1.0 / rscale;
+    // all levels in one launch: the box's own level's rscale
+    const double rinv = 1.0 / (level_rscale ? level_rscale[box_level[ib]] : rscale);
 
     // the (i, j) pairs of this lane
     int pi[NU], pj[NU];
@@ -757,6 +760,125 @@ p2l_mixed_kernel(double rscale, int32_t ntgt_boxes, const int32_t *__restrict__ 
     }
 }
 
+// {{{ L2P over packed items (all levels in one launch)
+
+// Full coefficients of one box in the layout [(j, k) pairs, j-major][i]:
+// the x-run of pair (j, k) holds i = 0..P-j-k contiguously.
+// (closed form of: the pairs (j', k') before (j, k) times their run lengths)
+template <int P>
+__host__ __device__ constexpr int jki_offset(int j, int k)
+{
+    constexpr int A = P + 1;
+    return A * (A + 1) * (A + 2) / 6 - (A - j) * (A - j + 1) * (A - j + 2) / 6 + k * (A - j) -
+           k * (k - 1) / 2;
+}
+
+constexpr int L2PK_SLOTS = 8;   // boxes per warp item
+
+// warps per CTA: four while the slots' coefficients fit in 200 KB, else two
+template <int P>
+__host__ __device__ constexpr int l2pk_warps()
+{
+    return 8 * L2PK_SLOTS * (P + 1) * (P + 2) * (P + 3) / 6 * 4 <= 200 * 1024 ? 4 : 2;
+}
+
+// One warp evaluates up to 32 targets taken from up to 8 boxes (slots; a
+// box with more than 32 targets spans several items). The slots' locals
+// are decompressed together (p - 1 plane sweeps, sumpy's
+// CSEMatVecOperator.matvec), then lane l evaluates its target as
+//   sum_(j,k) y^j z^k / (j! k!) * sum_i c[i][j][k] x^i / i!
+// with x, y, z scaled by the box's rscale and the power tables in
+// registers: 286 FMAs at p = 10 with compile-time indices, the x-runs of
+// its own box read from shared memory (at p = 10 the eight slot bases,
+// 2288 bytes apart, fall on distinct banks).
+// item = {first slot, number of slots}; slot = {box, first target,
+// number of targets, level}; results are assigned.
+template <int P>
+__global__ void __launch_bounds__(32 * l2pk_warps<P>())
+l2p_packed_kernel(int32_t nitems, const int2 *__restrict__ items, const int4 *__restrict__ slots,
+                  const double *__restrict__ level_rscale, const double *__restrict__ centers,
+                  int64_t cstride, const double *__restrict__ loc,
+                  const double *__restrict__ targets, int64_t tstride, double scale,
+                  double *__restrict__ result)
+{
+    constexpr int P1 = P + 1;
+    constexpr int N = P1 * P1;
+    constexpr int NF = P1 * (P1 + 1) * (P1 + 2) / 6;
+    extern __shared__ __align__(16) double sml[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int it = blockIdx.x * l2pk_warps<P>() + warp;
+    if (it >= nitems) return;
+    double *cubes = sml + warp * (L2PK_SLOTS * NF);
+    const int2 item = items[it];
+    const int nsl = item.y;
+
+    // this lane's slot and target
+    int my = -1, off = lane;
+    int4 sl = make_int4(0, 0, 0, 0);
+    for (int q = 0; q < nsl; ++q) {
+        const int4 v = slots[item.x + q];
+        if (my < 0) {
+            if (off < v.z) { my = q; sl = v; } else { off -= v.z; }
+        }
+    }
+    // stored -> full layout, all slots
+    for (int e = lane; e < nsl * N; e += 32) {
+        const int q = e / N, st = e - q * N;
+        int i, j, k;
+        stored_mi(st, i, j, k);
+        const int32_t b = slots[item.x + q].x;
+        cubes[q * NF + jki_offset<P>(j, k) + i] = loc[(int64_t)b * N + st];
+    }
+    __syncwarp();
+    // decompress: plane i from plane i - 2, i = 2..P (all slots per sweep)
+    for (int i = 2; i <= P; ++i) {
+        const int m = P - i;
+        const int npairs = (m + 1) * (m + 2) / 2;
+        for (int e = lane; e < nsl * npairs; e += 32) {
+            const int q = e / npairs;
+            int J, K;
+            tri_pair(e - q * npairs, m, J, K);
+            double *c = cubes + q * NF;
+            c[jki_offset<P>(J, K) + i] =
+                -c[jki_offset<P>(J + 2, K) + i - 2] - c[jki_offset<P>(J, K + 2) + i - 2];
+        }
+        __syncwarp();
+    }
+    if (my < 0) return;
+    const int32_t b = sl.x, t = sl.y + off;
+    const double rs = level_rscale[sl.w], rinv = 1.0 / rs;
+    const double x = (targets[t] - centers[b]) * rinv;
+    const double y = (targets[tstride + t] - centers[cstride + b]) * rinv;
+    const double z = (targets[2 * tstride + t] - centers[2 * cstride + b]) * rinv;
+    double xp[P1], yp[P1], zp[P1];
+    xp[0] = yp[0] = zp[0] = 1.0;
+#pragma unroll
+    for (int n = 1; n <= P; ++n) {
+        const double inv_n = 1.0 / n;   // compile-time constant
+        xp[n] = xp[n - 1] * x * inv_n;
+        yp[n] = yp[n - 1] * y * inv_n;
+        zp[n] = zp[n - 1] * z * inv_n;
+    }
+    const double *c = cubes + my * NF;
+    double pot = 0.0;
+#pragma unroll
+    for (int j = 0; j <= P; ++j) {
+        double pj = 0.0;
+#pragma unroll
+        for (int k = 0; k <= P - j; ++k) {
+            const double *run = c + jki_offset<P>(j, k);
+            double r = 0.0;
+#pragma unroll
+            for (int i = P - j - k; i >= 0; --i) r = fma(run[i], xp[i], r);
+            pj = fma(zp[k], r, pj);
+        }
+        pot = fma(yp[j], pj, pot);
+    }
+    result[t] = scale * pot;
+}
+
+// }}}
+
 // {{{ mixed M2P / P2L over flat work items (all levels in one launch)
 
 // The per-level launches above give one warp a whole target box: a box
@@ -1271,6 +1393,64 @@ int sumpy_p2e_from_csr_mixed(int order, double rscale, int32_t ntgt_boxes,
             check_launch("p2l_mixed_kernel")))
     SUMPY_ORDER_SWITCH(order, CALL_P2LM)
 #undef CALL_P2LM
+}
+
+int sumpy_p2e_from_single_box_levels_f64(int order, int32_t nsrc_boxes,
+                                         const int32_t *source_boxes, const int32_t *box_levels,
+                                         const double *level_rscales, const double *centers,
+                                         int64_t center_stride, const int32_t *box_source_starts,
+                                         const int32_t *box_source_counts_nonchild,
+                                         const double *sources, int64_t source_stride,
+                                         const double *strength, double *expansions,
+                                         void *stream)
+{
+    if (!order_ok(order)) { set_last_error("p2m levels: unsupported order"); return SUMPY_EUNSUPPORTED; }
+    if (nsrc_boxes < 0) return bad_arg("p2m levels: nsrc_boxes < 0");
+    if (nsrc_boxes == 0) return SUMPY_OK;
+    if (!source_boxes || !box_levels || !level_rscales || !centers || !box_source_starts ||
+        !box_source_counts_nonchild || !sources || !strength || !expansions)
+        return bad_arg("p2m levels: null pointer argument");
+#define CALL_P2ML(P)                                                                             \
+    (p2m_warp_kernel<P><<<(nsrc_boxes + p2m_warps<P>() - 1) / p2m_warps<P>(),                    \
+                          32 * p2m_warps<P>(), 0, as_stream(stream)>>>(                           \
+         0.0, nsrc_boxes, source_boxes, centers, center_stride, box_source_starts,              \
+         box_source_counts_nonchild, sources, source_stride, strength, 0, expansions,           \
+         box_levels, level_rscales),                                                            \
+     check_launch("p2m_warp_kernel"))
+    SUMPY_ORDER_SWITCH(order, CALL_P2ML)
+#undef CALL_P2ML
+}
+
+int sumpy_e2p_from_single_box_packed_f64(int order, int32_t nitems, const int32_t *items,
+                                         const int32_t *slots, const double *level_rscales,
+                                         const double *centers, int64_t center_stride,
+                                         const double *src_expansions, const double *targets,
+                                         int64_t target_stride, double scale, double *result,
+                                         void *stream)
+{
+    if (!order_ok(order)) { set_last_error("l2p packed: unsupported order"); return SUMPY_EUNSUPPORTED; }
+    if (nitems < 0) return bad_arg("l2p packed: nitems < 0");
+    if (nitems == 0) return SUMPY_OK;
+    if (!items || !slots || !level_rscales || !centers || !src_expansions || !targets || !result)
+        return bad_arg("l2p packed: null pointer argument");
+    if ((reinterpret_cast<uintptr_t>(items) & 7) || (reinterpret_cast<uintptr_t>(slots) & 15))
+        return bad_arg("l2p packed: items must be 8-byte and slots 16-byte aligned");
+#define NF_OF(P) ((P + 1) * (P + 2) * (P + 3) / 6)
+#define CALL_L2PK(P)                                                                             \
+    (prepare_smem(l2p_packed_kernel<P>,                                                          \
+                  sizeof(double) * L2PK_SLOTS * NF_OF(P) * l2pk_warps<P>())                      \
+         ? SUMPY_ELAUNCH                                                                         \
+         : (l2p_packed_kernel<P><<<(nitems + l2pk_warps<P>() - 1) / l2pk_warps<P>(),             \
+                                   32 * l2pk_warps<P>(),                                         \
+                                   sizeof(double) * L2PK_SLOTS * NF_OF(P) * l2pk_warps<P>(),    \
+                                   as_stream(stream)>>>(                                         \
+                nitems, reinterpret_cast<const int2 *>(items),                                  \
+                reinterpret_cast<const int4 *>(slots), level_rscales, centers, center_stride,   \
+                src_expansions, targets, target_stride, scale, result),                         \
+            check_launch("l2p_packed_kernel")))
+    SUMPY_ORDER_SWITCH(order, CALL_L2PK)
+#undef CALL_L2PK
+#undef NF_OF
 }
 
 int sumpy_mpoles_to_f32(int order, int64_t nboxes, const double *src_expansions, float *dst,

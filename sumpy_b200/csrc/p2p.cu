@@ -18,7 +18,7 @@ struct SrcPt {
     double x, y, z, q;
 };
 
-template <bool MIXED, bool GRAD = false>
+template <bool GRAD = false>
 __global__ void __launch_bounds__(32 * P2P_WARPS)
 p2p_csr_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_boxes,
                const int32_t *__restrict__ src_box_starts, const int32_t *__restrict__ src_box_lists,
@@ -63,7 +63,6 @@ p2p_csr_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_boxes,
             const int32_t sb = src_box_lists[l];
             const int32_t s0 = box_src_starts[sb];
             const int32_t ns = box_src_counts[sb];
-            float accf = 0.f, gxf = 0.f, gyf = 0.f, gzf = 0.f;
             for (int32_t sc = 0; sc < ns; sc += 32) {
                 const int nsc = min(32, ns - sc);
                 if (lane < nsc) {
@@ -79,41 +78,21 @@ p2p_csr_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_boxes,
                         const int32_t s = s0 + sc + j;
                         if (s == self) continue;
                         const SrcPt sp = wb[j];
-                        if (MIXED) {
-                            const float dx = (float)(tx - sp.x);
-                            const float dy = (float)(ty - sp.y);
-                            const float dz = (float)(tz - sp.z);
-                            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                            const float ri = rsqrtf(r2);
-                            const float qr = (float)sp.q * ri;
-                            accf += qr;
-                            if (GRAD) {
-                                // d/dt (q/|t-s|) = -q (t-s)/|t-s|^3
-                                const float w = qr * ri * ri;
-                                gxf = fmaf(-w, dx, gxf);
-                                gyf = fmaf(-w, dy, gyf);
-                                gzf = fmaf(-w, dz, gzf);
-                            }
-                        } else {
-                            const double dx = tx - sp.x, dy = ty - sp.y, dz = tz - sp.z;
-                            const double r2 = dx * dx + dy * dy + dz * dz;
-                            const double ri = rsqrt(r2);
-                            const double qr = sp.q * ri;
-                            acc += qr;
-                            if (GRAD) {
-                                const double w = qr * ri * ri;
-                                gx -= w * dx;
-                                gy -= w * dy;
-                                gz -= w * dz;
-                            }
+                        const double dx = tx - sp.x, dy = ty - sp.y, dz = tz - sp.z;
+                        const double r2 = dx * dx + dy * dy + dz * dz;
+                        const double ri = rsqrt(r2);
+                        const double qr = sp.q * ri;
+                        acc += qr;
+                        if (GRAD) {
+                            // d/dt (q/|t-s|) = -q (t-s)/|t-s|^3
+                            const double w = qr * ri * ri;
+                            gx -= w * dx;
+                            gy -= w * dy;
+                            gz -= w * dz;
                         }
                     }
                 }
                 __syncwarp();
-            }
-            if (MIXED) {
-                acc += (double)accf;
-                if (GRAD) { gx += (double)gxf; gy += (double)gyf; gz += (double)gzf; }
             }
         }
         for (int off = g; off < 32; off <<= 1) {
@@ -134,6 +113,191 @@ p2p_csr_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_boxes,
         }
     }
 }
+
+// {{{ mixed-precision List 1 over a flat source sequence
+
+// The mixed form above costs three FP64 subtractions and four FP64->FP32
+// conversions per pair, and stages each source box separately (a 33-source
+// box is a batch of 32 and a batch of 1). Here each coordinate is split once
+// per staged source into hi + lo FP32 parts (x = hi + lo to ~2^-48
+// relative), so a pair's offset (t_hi - s_hi) + (t_lo - s_lo) is FP32
+// arithmetic accurate to a few FP32 ulps of the offset itself; the sources of
+// all boxes in a target box's list form one flat sequence (a warp prefix sum
+// over up to 32 list entries per window), staged 32 at a time into a
+// double-buffered shared slot while the next batch's loads are in flight.
+// Per 32 sources the FP32 partial sums are added into FP64.
+constexpr int P2PF_WARPS = 8;
+
+__device__ __forceinline__ void split_hl(double v, float &hi, float &lo)
+{
+    hi = __double2float_rn(v);
+    lo = __double2float_rn(v - (double)hi);
+}
+
+template <bool GRAD>
+__global__ void __launch_bounds__(32 * P2PF_WARPS)
+p2p_flat_mixed_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_boxes,
+                      const int32_t *__restrict__ src_box_starts,
+                      const int32_t *__restrict__ src_box_lists,
+                      const int32_t *__restrict__ box_src_starts,
+                      const int32_t *__restrict__ box_src_counts,
+                      const int32_t *__restrict__ box_tgt_starts,
+                      const int32_t *__restrict__ box_tgt_counts,
+                      const double *__restrict__ sources, int64_t sstride,
+                      const double *__restrict__ strength, const double *__restrict__ targets,
+                      int64_t tstride, const int32_t *__restrict__ target_to_source, double scale,
+                      double *__restrict__ result, double *__restrict__ grad)
+{
+    __shared__ float4 shi[P2PF_WARPS][2][32];   // x, y, z hi parts, q
+    __shared__ float4 slo[P2PF_WARPS][2][32];   // x, y, z lo parts
+    const unsigned FULL = 0xffffffffu;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ib = blockIdx.x * P2PF_WARPS + warp;
+    if (ib >= ntgt_boxes) return;  // whole warp leaves together
+    const int32_t tb = target_boxes[ib];
+    const int32_t t0 = box_tgt_starts[tb], nt = box_tgt_counts[tb];
+    const int32_t ls = src_box_starts[ib], le = src_box_starts[ib + 1];
+
+    for (int32_t tc = 0; tc < nt; tc += 32) {
+        const int ntc = min(32, nt - tc);
+        int g = 1;
+        while (g < ntc) g <<= 1;
+        const int nph = 32 / g;
+        const int tl = lane & (g - 1), ph = lane / g;
+        const bool active = tl < ntc;
+        const int32_t t = t0 + tc + tl;
+        float txh = 0.f, txl = 0.f, tyh = 0.f, tyl = 0.f, tzh = 0.f, tzl = 0.f;
+        int32_t self = -1;
+        if (active) {
+            split_hl(targets[t], txh, txl);
+            split_hl(targets[tstride + t], tyh, tyl);
+            split_hl(targets[2 * tstride + t], tzh, tzl);
+            if (target_to_source) self = target_to_source[t];
+        }
+        double acc = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+        for (int32_t w0 = ls; w0 < le; w0 += 32) {
+            // one window of up to 32 list entries: lane k holds entry k's
+            // source range; inclusive prefix sum of the counts
+            const int nw = min(32, le - w0);
+            int32_t bs0 = 0, bn = 0;
+            if (lane < nw) {
+                const int32_t sb = src_box_lists[w0 + lane];
+                bs0 = box_src_starts[sb];
+                bn = box_src_counts[sb];
+            }
+            int32_t cum = bn;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int32_t v = __shfl_up_sync(FULL, cum, o);
+                if (lane >= o) cum += v;
+            }
+            const int32_t S = __shfl_sync(FULL, cum, 31);
+            // flat position of this lane's own source in the window, if any
+            int32_t fself = -1;
+            if (target_to_source) {
+                for (int k = 0; k < nw; ++k) {
+                    const int32_t b0 = __shfl_sync(FULL, bs0, k);
+                    const int32_t n = __shfl_sync(FULL, bn, k);
+                    const int32_t c = __shfl_sync(FULL, cum, k);
+                    if (self >= b0 && self < b0 + n) fself = c - n + (self - b0);
+                }
+            }
+            // source of flat index f (f < S): entry k = #lanes with cum <= f
+            auto locate = [&](int32_t f) {
+                int k = 0;
+#pragma unroll
+                for (int step = 16; step >= 1; step >>= 1) {
+                    const int32_t v = __shfl_sync(FULL, cum, k + step - 1);
+                    if (v <= f) k += step;
+                }
+                const int32_t b0 = __shfl_sync(FULL, bs0, k);
+                const int32_t c = __shfl_sync(FULL, cum, k);
+                const int32_t n = __shfl_sync(FULL, bn, k);
+                return b0 + f - (c - n);
+            };
+            const int nbat = (S + 31) / 32;
+            double px = 0, py = 0, pz = 0, pq = 0;
+            {
+                const int32_t s = locate(min(lane, max(S - 1, 0)));
+                if (lane < S) {
+                    px = sources[s]; py = sources[sstride + s]; pz = sources[2 * sstride + s];
+                    pq = strength[s];
+                }
+            }
+            for (int bt = 0; bt < nbat; ++bt) {
+                const int nsc = min(32, S - 32 * bt);
+                const int slot = bt & 1;
+                if (lane < nsc) {
+                    float4 h, l;
+                    split_hl(px, h.x, l.x);
+                    split_hl(py, h.y, l.y);
+                    split_hl(pz, h.z, l.z);
+                    h.w = (float)pq;
+                    l.w = 0.f;
+                    shi[warp][slot][lane] = h;
+                    slo[warp][slot][lane] = l;
+                }
+                if (bt + 1 < nbat) {
+                    const int32_t f = 32 * (bt + 1) + lane;
+                    const int32_t s = locate(min(f, S - 1));
+                    if (f < S) {
+                        px = sources[s]; py = sources[sstride + s];
+                        pz = sources[2 * sstride + s]; pq = strength[s];
+                    }
+                }
+                __syncwarp();
+                if (active) {
+                    const int jself = fself - 32 * bt;   // outside [0, nsc) if not here
+                    float accf = 0.f, gxf = 0.f, gyf = 0.f, gzf = 0.f;
+#pragma unroll 4
+                    for (int j = ph; j < nsc; j += nph) {
+                        const float4 h = shi[warp][slot][j];
+                        const float4 l = slo[warp][slot][j];
+                        const float dx = (txh - h.x) + (txl - l.x);
+                        const float dy = (tyh - h.y) + (tyl - l.y);
+                        const float dz = (tzh - h.z) + (tzl - l.z);
+                        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                        const float ri = rsqrtf(r2);
+                        if (j != jself) {
+                            if (GRAD) {
+                                const float qr = h.w * ri;
+                                const float w = qr * ri * ri;
+                                accf += qr;
+                                gxf = fmaf(-w, dx, gxf);
+                                gyf = fmaf(-w, dy, gyf);
+                                gzf = fmaf(-w, dz, gzf);
+                            } else {
+                                accf = fmaf(h.w, ri, accf);
+                            }
+                        }
+                    }
+                    acc += (double)accf;
+                    if (GRAD) { gx += (double)gxf; gy += (double)gyf; gz += (double)gzf; }
+                }
+                // slot is rewritten by batch bt + 2, after the next __syncwarp
+            }
+            __syncwarp();   // the next window restages slot 0
+        }
+        for (int off = g; off < 32; off <<= 1) {
+            acc += __shfl_xor_sync(FULL, acc, off);
+            if (GRAD) {
+                gx += __shfl_xor_sync(FULL, gx, off);
+                gy += __shfl_xor_sync(FULL, gy, off);
+                gz += __shfl_xor_sync(FULL, gz, off);
+            }
+        }
+        if (active && ph == 0) {
+            if (result) result[t] = scale * acc;
+            if (GRAD) {
+                grad[t] = scale * gx;
+                grad[tstride + t] = scale * gy;
+                grad[2 * tstride + t] = scale * gz;
+            }
+        }
+    }
+}
+
+// }}}
 
 constexpr int DIRECT_THREADS = 256;
 
@@ -206,8 +370,15 @@ int launch_p2p_csr(int32_t ntgt_boxes, const int32_t *target_boxes, const int32_
     if (!target_boxes || !ss || !sl || !bss || !bsc || !bts || !btc || !sources || !strength ||
         !targets || (!result && !GRAD) || (GRAD && !grad))
         return bad_arg("p2p: null pointer argument");
+    if (MIXED) {
+        const int blocks = (ntgt_boxes + P2PF_WARPS - 1) / P2PF_WARPS;
+        p2p_flat_mixed_kernel<GRAD><<<blocks, 32 * P2PF_WARPS, 0, as_stream(stream)>>>(
+            ntgt_boxes, target_boxes, ss, sl, bss, bsc, bts, btc, sources, sstride, strength,
+            targets, tstride, tts, scale, result, grad);
+        return check_launch("p2p_flat_mixed_kernel");
+    }
     const int blocks = (ntgt_boxes + P2P_WARPS - 1) / P2P_WARPS;
-    p2p_csr_kernel<MIXED, GRAD><<<blocks, 32 * P2P_WARPS, 0, as_stream(stream)>>>(
+    p2p_csr_kernel<GRAD><<<blocks, 32 * P2P_WARPS, 0, as_stream(stream)>>>(
         ntgt_boxes, target_boxes, ss, sl, bss, bsc, bts, btc, sources, sstride, strength,
         targets, tstride, tts, scale, result, grad);
     return check_launch("p2p_csr_kernel");

@@ -49,6 +49,7 @@ M2L_TILE_TC = 128      # tensor-core tile (MMA N)
 M2L_ITEM_GROUPS = 64   # class groups per tensor-core work item (one CTA)
 ITEM_ROUNDS = 4        # rounds (one source box / 32 sources each) per mixed M2P / P2L item
 M2P_ITEM_GROUPS = 8    # lane groups per warp in the M2P item kernel (fixed by the kernel)
+L2P_ITEM_SLOTS = 8     # boxes per packed L2P item (fixed by the kernel)
 
 
 def _npad(order):
@@ -116,6 +117,46 @@ def m2p_items(tree, target_boxes_by_source_level, source_boxes_by_level,
     return np.ascontiguousarray(items[order], dtype=np.int32), np.concatenate(lists)
 
 
+def _box_levels(level_starts, n):
+    return np.repeat(np.arange(len(level_starts) - 1),
+                     np.diff(np.asarray(level_starts, dtype=np.int64)))[:n]
+
+
+def l2p_items(tree, level_starts, target_boxes, max_slots=L2P_ITEM_SLOTS):
+    """Packed work items of the one-launch L2P
+    (sumpy_e2p_from_single_box_packed_f64): a box's targets go 32 per slot;
+    slots of fewer than 32 targets share an item (next fit, largest first)
+    up to 32 targets and ``max_slots`` slots. Returns (items int32 [n, 2] =
+    first slot, number of slots; slots int32 [m, 4] = box, first target,
+    number of targets, level)."""
+    bts = np.asarray(tree.box_target_starts, dtype=np.int64)
+    btc = np.asarray(tree.box_target_counts_nonchild, dtype=np.int64)
+    tb = np.asarray(target_boxes, dtype=np.int64)
+    lev = _box_levels(level_starts, len(tb))
+    nt = btc[tb]
+    nfull = nt // 32
+    fb = np.repeat(np.arange(len(tb)), nfull)
+    fc = _expand_ranges(np.zeros(len(tb), dtype=np.int64), nfull)
+    full = np.stack([tb[fb], bts[tb][fb] + 32 * fc, np.full(len(fb), 32), lev[fb]], axis=1)
+    rem = nt - 32 * nfull
+    rb = np.nonzero(rem > 0)[0]
+    rb = rb[np.argsort(-rem[rb], kind="stable")]
+    part = np.stack([tb[rb], bts[tb][rb] + 32 * nfull[rb], rem[rb], lev[rb]], axis=1)
+    slots = np.concatenate([full.reshape(-1, 4), part.reshape(-1, 4)]).astype(np.int32)
+    items = [(i, 1) for i in range(len(full))]
+    first, cnt, tot = len(full), 0, 0
+    for i, r in enumerate(part[:, 2], start=len(full)):
+        if cnt and (tot + r > 32 or cnt == max_slots):
+            items.append((first, cnt))
+            first, cnt, tot = i, 0, 0
+        cnt += 1
+        tot += int(r)
+    if cnt:
+        items.append((first, cnt))
+    return (np.ascontiguousarray(np.array(items, dtype=np.int32).reshape(-1, 2)),
+            np.ascontiguousarray(slots))
+
+
 def p2l_items(tree, level_starts, target_boxes, starts, lists, rounds=ITEM_ROUNDS):
     """Work items of the one-launch mixed P2L (sumpy_p2e_from_items_mixed):
     the sources of each target box's List-4 boxes as one flat index array,
@@ -131,7 +172,7 @@ def p2l_items(tree, level_starts, target_boxes, starts, lists, rounds=ITEM_ROUND
     ntb = len(starts) - 1
     f0 = F[starts[:-1]]
     n = F[starts[1:]] - f0
-    lev_of = np.repeat(np.arange(len(level_starts) - 1), np.diff(np.asarray(level_starts)))[:ntb]
+    lev_of = _box_levels(level_starts, ntb)
     per = 32 * rounds
     nit = (n + per - 1) // per
     it = np.repeat(np.arange(ntb), nit)
@@ -258,6 +299,8 @@ class SumpyExpansionWrangler:
         # mixed List 3 / List 4: all levels in one launch over host-cut work
         # items (False: one launch per level, a warp per target box)
         self.item_kernels = True
+        # P2M and L2P of all levels in one launch (one order on every level)
+        self.merge_levels = True
         self.m2l_item_groups = int(m2l_item_groups or M2L_ITEM_GROUPS)
         if self.m2l_item_groups < 1:
             raise ValueError("m2l_item_groups must be >= 1")
@@ -400,11 +443,27 @@ class SumpyExpansionWrangler:
 
     def form_multipoles(self, actx, level_start_source_box_nrs, source_boxes, src_weight_vecs):
         mpoles = self.multipole_expansion_zeros(actx)
-        lss = _np_i32(level_start_source_box_nrs)
-        boxes = self._dev(source_boxes)
         g = self._geom
         w = self._weights(src_weight_vecs)
         st = stream_ptr()
+        if self._merged_levels and not isinstance(source_boxes, torch.Tensor):
+            def build():
+                sb = np.asarray(source_boxes, dtype=np.int64)
+                lev = _box_levels(level_start_source_box_nrs, len(sb))
+                order = np.argsort(-np.asarray(self.tree.box_source_counts_nonchild)[sb],
+                                   kind="stable")
+                return (torch.as_tensor(sb[order].astype(np.int32)).to(self.device),
+                        torch.as_tensor(lev[order].astype(np.int32)).to(self.device))
+            boxes, levs = self._cached_items(
+                "p2m_boxes", (level_start_source_box_nrs, source_boxes), build)
+            if boxes.numel():
+                call("sumpy_p2e_from_single_box_levels_f64", _c(self.level_orders[0]),
+                     _i32(boxes.numel()), dptr(boxes), dptr(levs), dptr(self._level_rscales),
+                     dptr(g["centers"]), _i64(self.tree.nboxes), dptr(g["bss"]), dptr(g["bsc"]),
+                     dptr(g["sources"]), _i64(self.tree.nsources), dptr(w), dptr(mpoles), st)
+            return mpoles
+        lss = _np_i32(level_start_source_box_nrs)
+        boxes = self._dev(source_boxes)
         for lev in range(self.tree.nlevels):
             a, b = int(lss[lev]), int(lss[lev + 1])
             if a == b:
@@ -602,16 +661,18 @@ class SumpyExpansionWrangler:
                                    tview, st)
         return local_exps
 
-    def _tc_items(self, tiles):
+    def _tc_items(self, tiles, groups_per_item=None):
         """Split tiles (group ranges) into work items of at most
-        ``m2l_item_groups`` groups, largest first (CTAs start roughly in launch
-        order). The same schedule serves the FP64 and the tensor-core GEMMs."""
+        ``groups_per_item`` (default ``m2l_item_groups``) groups, largest first
+        (CTAs start roughly in launch order). The same schedule serves the
+        FP64 and the tensor-core GEMMs."""
+        gpi = int(groups_per_item or self.m2l_item_groups)
         it_tile, it_g0, it_g1 = [], [], []
         for tile, (g0, g1) in enumerate(tiles):
-            for a in range(g0, g1, self.m2l_item_groups):
+            for a in range(g0, g1, gpi):
                 it_tile.append(tile)
                 it_g0.append(a)
-                it_g1.append(min(g1, a + self.m2l_item_groups))
+                it_g1.append(min(g1, a + gpi))
         it_tile = np.array(it_tile, dtype=np.int32)
         it_g0 = np.array(it_g0, dtype=np.int32)
         it_g1 = np.array(it_g1, dtype=np.int32)
@@ -822,7 +883,12 @@ class SumpyExpansionWrangler:
                     groups.append(blk[o])
                     classes.append(o)
             tiles.append((g0, len(groups)))
-        it_tile, it_g0, it_g1 = self._tc_items(tiles)
+        # a level's octant GEMM is on the level-serial M2M / L2L chain: cut
+        # it into enough items (CTAs) to cover the GPU twice, down to one
+        # octant group per item, so few tiles do not leave one CTA pipelining
+        # all eight groups
+        gpi = min(8, max(1, -(-len(groups) // (2 * self._sm_count))))
+        it_tile, it_g0, it_g1 = self._tc_items(tiles, gpi)
         dev = self.device
         plan = {
             "nitems": len(it_tile), "nclasses": 8,
@@ -916,6 +982,15 @@ class SumpyExpansionWrangler:
             raise RuntimeError(f"a tensor-core M2L wait expired (status {code})")
 
     # }}}
+
+    @cached_property
+    def _sm_count(self):
+        return torch.cuda.get_device_properties(self.device).multi_processor_count
+
+    @property
+    def _merged_levels(self):
+        return (self.merge_levels and not self.helmholtz and not self.gradient
+                and len(set(self.level_orders)) == 1)
 
     @property
     def _items_path(self):
@@ -1061,10 +1136,24 @@ class SumpyExpansionWrangler:
 
     def eval_locals(self, actx, level_start_target_box_nrs, target_boxes, local_exps):
         pot = self.output_zeros(actx)
-        ltb = _np_i32(level_start_target_box_nrs)
-        boxes = self._dev(target_boxes)
         g = self._geom
         st = stream_ptr()
+        if self._merged_levels and not isinstance(target_boxes, torch.Tensor):
+            def build():
+                items, slots = l2p_items(self.tree, level_start_target_box_nrs, target_boxes)
+                return (torch.as_tensor(items).to(self.device),
+                        torch.as_tensor(slots).to(self.device))
+            items, slots = self._cached_items(
+                "l2p_items", (level_start_target_box_nrs, target_boxes), build)
+            if items.shape[0]:
+                call("sumpy_e2p_from_single_box_packed_f64", _c(self.level_orders[0]),
+                     _i32(items.shape[0]), dptr(items), dptr(slots), dptr(self._level_rscales),
+                     dptr(g["centers"]), _i64(self.tree.nboxes), dptr(local_exps),
+                     dptr(g["targets"]), _i64(self.tree.ntargets), _d(self._scale),
+                     dptr(pot[0]), st)
+            return pot
+        ltb = _np_i32(level_start_target_box_nrs)
+        boxes = self._dev(target_boxes)
         for lev in range(self.tree.nlevels):
             a, b = int(ltb[lev]), int(ltb[lev + 1])
             if a == b:

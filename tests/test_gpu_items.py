@@ -78,3 +78,36 @@ def test_items_end_to_end_separate_targets(cuda_device):
     out = drive_fmm(None, w, [q])[0].cpu()
     w.check_status()
     assert relerr(out, ref) < 2e-6
+
+
+@pytest.mark.parametrize("order", [1, 3, 10, 16])
+def test_merged_p2m_and_packed_l2p_match_per_level(cuda_device, order):
+    """P2M of all levels in one launch gives the per-level multipoles bit for
+    bit (same per-box arithmetic); the packed L2P agrees with the per-level
+    L2P to FP64 rounding; end to end likewise."""
+    src, tgt = sphere_plummer(30000, 9), uniform_cube(20000, 4)
+    tree, trav, tcls = build_all(src, tgt, 40)
+    q = torch.as_tensor(np.random.default_rng(8).standard_normal(src.shape[1]), device="cuda")
+    ws = []
+    for merged in (False, True):
+        w = _wrangler(trav, tcls, order, "fp64", False, False)
+        w.merge_levels = merged
+        ws.append(w)
+    qs = ws[0].reorder_sources(q)
+    mps = [w.form_multipoles(None, trav.level_start_source_box_nrs, trav.source_boxes, [qs])
+           for w in ws]
+    assert torch.equal(mps[0], mps[1])
+    w = ws[0]
+    mp = w.coarsen_multipoles(None, trav.level_start_source_parent_box_nrs,
+                              trav.source_parent_boxes, mps[0])
+    loc = w.multipole_to_local(None, trav.level_start_target_or_target_parent_box_nrs,
+                               trav.target_or_target_parent_boxes, trav.from_sep_siblings_starts,
+                               trav.from_sep_siblings_lists, mp)
+    loc = w.refine_locals(None, trav.level_start_target_or_target_parent_box_nrs,
+                          trav.target_or_target_parent_boxes, loc)
+    pe = [ww.eval_locals(None, trav.level_start_target_box_nrs, trav.target_boxes, loc)[0].cpu()
+          for ww in ws]
+    assert np.abs(pe[0].numpy()).max() > 0
+    assert relerr(pe[1], pe[0]) < 1e-13
+    pots = [drive_fmm(None, ww, [q])[0].cpu() for ww in ws]
+    assert relerr(pots[1], pots[0]) < 1e-13

@@ -87,3 +87,34 @@ def test_items_of_empty_lists():
                             trav.target_or_target_parent_boxes, trav.from_sep_bigger_starts,
                             trav.from_sep_bigger_lists)
     assert items.shape == (0, 4) and sidx.size == 0
+
+
+def test_l2p_packing_covers_targets_once(traversal):
+    from sumpy_b200.fmm import L2P_ITEM_SLOTS, l2p_items
+    tree, trav, _ = traversal
+    items, slots = l2p_items(tree, trav.level_start_target_box_nrs, trav.target_boxes)
+    assert items.dtype == np.int32 and items.shape[1] == 2 and slots.shape[1] == 4
+    seen = np.zeros(tree.ntargets, dtype=np.int64)
+    lev_of = {}
+    for lev in range(tree.nlevels):
+        a, b = trav.level_start_target_box_nrs[lev:lev + 2]
+        for tb in trav.target_boxes[a:b]:
+            lev_of[int(tb)] = lev
+    for first, n in items:
+        assert 1 <= n <= L2P_ITEM_SLOTS
+        sl = slots[first:first + n]
+        assert sl[:, 2].sum() <= 32 and (sl[:, 2] >= 1).all()
+        for box, t0, cnt, lev in sl:
+            assert lev == lev_of[int(box)] == tree.box_levels[box]
+            assert tree.box_target_starts[box] <= t0
+            assert t0 + cnt <= tree.box_target_starts[box] + tree.box_target_counts_nonchild[box]
+            seen[t0:t0 + cnt] += 1
+    # every target of a target box exactly once (the slots tile each box)
+    want = np.zeros(tree.ntargets, dtype=np.int64)
+    for tb in trav.target_boxes:
+        t0 = tree.box_target_starts[tb]
+        want[t0:t0 + tree.box_target_counts_nonchild[tb]] = 1
+    np.testing.assert_array_equal(seen, want)
+    # packing is dense: slots cover all items contiguously, lanes mostly used
+    assert items[0, 0] == 0 and (items[1:, 0] == np.cumsum(items[:, 1])[:-1]).all()
+    assert want.sum() / (32 * len(items)) > 0.75
