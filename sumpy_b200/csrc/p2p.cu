@@ -124,14 +124,65 @@ p2p_csr_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_boxes,
 // arithmetic accurate to a few FP32 ulps of the offset itself; the sources of
 // all boxes in a target box's list form one flat sequence (a warp prefix sum
 // over up to 32 list entries per window), staged 32 at a time into a
-// double-buffered shared slot while the next batch's loads are in flight.
-// Per 32 sources the FP32 partial sums are added into FP64.
+// double-buffered shared slot while the next batch's loads are in flight; a
+// short last batch is padded with zero-strength sources far away (1e18), so
+// every batch is 32 sources. Targets: a chunk of ntc <= 32 targets takes
+// ntc lanes per phase and 32 / ntc phases, phase ph taking the batch's
+// sources j = ph (mod phases). Self-interaction is tested only in batches
+// that hold some lane's own source. Per batch the FP32 partial sums are
+// added into FP64.
 constexpr int P2PF_WARPS = 8;
+constexpr float P2PF_FAR = 1e18f;
 
 __device__ __forceinline__ void split_hl(double v, float &hi, float &lo)
 {
     hi = __double2float_rn(v);
     lo = __double2float_rn(v - (double)hi);
+}
+
+struct P2PTarget {
+    float xh, xl, yh, yl, zh, zl;
+};
+
+// 1/sqrt(x) by the MUFU approximation, denormal inputs flushed (PTX
+// rsqrt.approx.ftz.f32, relative error below 2^-22): r^2 of a List-1 pair
+// is zero (excluded self pair) or far above the FP32 denormal range
+__device__ __forceinline__ float rsqrt_ftz(float x)
+{
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// sources j = j0, j0 + step, ... < 32 of one staged batch against one target
+template <bool CHECK, bool GRAD, int STEP>
+__device__ __forceinline__ void p2p_batch(const float4 *__restrict__ hi, const float4 *__restrict__ lo,
+                                          const P2PTarget &t, int j0, int step, int jself,
+                                          float &acc, float &gx, float &gy, float &gz)
+{
+    const int st = STEP ? STEP : step;
+#pragma unroll(STEP ? 32 : 4)
+    for (int j = j0; j < 32; j += st) {
+        const float4 h = hi[j];
+        const float4 l = lo[j];
+        const float dx = (t.xh - h.x) + (t.xl - l.x);
+        const float dy = (t.yh - h.y) + (t.yl - l.y);
+        const float dz = (t.zh - h.z) + (t.zl - l.z);
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        const float ri = rsqrt_ftz(r2);
+        if (CHECK && j == jself) continue;
+        if (GRAD) {
+            // d/dt (q/|t-s|) = -q (t-s)/|t-s|^3
+            const float qr = h.w * ri;
+            const float w = qr * ri * ri;
+            acc += qr;
+            gx = fmaf(-w, dx, gx);
+            gy = fmaf(-w, dy, gy);
+            gz = fmaf(-w, dz, gz);
+        } else {
+            acc = fmaf(h.w, ri, acc);
+        }
+    }
 }
 
 template <bool GRAD>
@@ -150,6 +201,7 @@ p2p_flat_mixed_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_box
 {
     __shared__ float4 shi[P2PF_WARPS][2][32];   // x, y, z hi parts, q
     __shared__ float4 slo[P2PF_WARPS][2][32];   // x, y, z lo parts
+    __shared__ double red[P2PF_WARPS][GRAD ? 4 : 1][32];
     const unsigned FULL = 0xffffffffu;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ib = blockIdx.x * P2PF_WARPS + warp;
@@ -160,18 +212,16 @@ p2p_flat_mixed_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_box
 
     for (int32_t tc = 0; tc < nt; tc += 32) {
         const int ntc = min(32, nt - tc);
-        int g = 1;
-        while (g < ntc) g <<= 1;
-        const int nph = 32 / g;
-        const int tl = lane & (g - 1), ph = lane / g;
-        const bool active = tl < ntc;
+        const int nph = 32 / ntc;
+        const int tl = lane % ntc, ph = lane / ntc;
+        const bool active = ph < nph;
         const int32_t t = t0 + tc + tl;
-        float txh = 0.f, txl = 0.f, tyh = 0.f, tyl = 0.f, tzh = 0.f, tzl = 0.f;
+        P2PTarget tg = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         int32_t self = -1;
         if (active) {
-            split_hl(targets[t], txh, txl);
-            split_hl(targets[tstride + t], tyh, tyl);
-            split_hl(targets[2 * tstride + t], tzh, tzl);
+            split_hl(targets[t], tg.xh, tg.xl);
+            split_hl(targets[tstride + t], tg.yh, tg.yl);
+            split_hl(targets[2 * tstride + t], tg.zh, tg.zl);
             if (target_to_source) self = target_to_source[t];
         }
         double acc = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
@@ -216,7 +266,7 @@ p2p_flat_mixed_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_box
                 return b0 + f - (c - n);
             };
             const int nbat = (S + 31) / 32;
-            double px = 0, py = 0, pz = 0, pq = 0;
+            double px = P2PF_FAR, py = P2PF_FAR, pz = P2PF_FAR, pq = 0.0;
             {
                 const int32_t s = locate(min(lane, max(S - 1, 0)));
                 if (lane < S) {
@@ -225,9 +275,8 @@ p2p_flat_mixed_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_box
                 }
             }
             for (int bt = 0; bt < nbat; ++bt) {
-                const int nsc = min(32, S - 32 * bt);
                 const int slot = bt & 1;
-                if (lane < nsc) {
+                {
                     float4 h, l;
                     split_hl(px, h.x, l.x);
                     split_hl(py, h.y, l.y);
@@ -240,60 +289,55 @@ p2p_flat_mixed_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_box
                 if (bt + 1 < nbat) {
                     const int32_t f = 32 * (bt + 1) + lane;
                     const int32_t s = locate(min(f, S - 1));
+                    px = py = pz = P2PF_FAR;
+                    pq = 0.0;
                     if (f < S) {
                         px = sources[s]; py = sources[sstride + s];
                         pz = sources[2 * sstride + s]; pq = strength[s];
                     }
                 }
                 __syncwarp();
+                const int jself = fself - 32 * bt;   // outside [0, 32) if not in this batch
+                const bool check = __any_sync(FULL, active && jself >= 0 && jself < 32);
                 if (active) {
-                    const int jself = fself - 32 * bt;   // outside [0, nsc) if not here
-                    float accf = 0.f, gxf = 0.f, gyf = 0.f, gzf = 0.f;
-#pragma unroll 4
-                    for (int j = ph; j < nsc; j += nph) {
-                        const float4 h = shi[warp][slot][j];
-                        const float4 l = slo[warp][slot][j];
-                        const float dx = (txh - h.x) + (txl - l.x);
-                        const float dy = (tyh - h.y) + (tyl - l.y);
-                        const float dz = (tzh - h.z) + (tzl - l.z);
-                        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                        const float ri = rsqrtf(r2);
-                        if (j != jself) {
-                            if (GRAD) {
-                                const float qr = h.w * ri;
-                                const float w = qr * ri * ri;
-                                accf += qr;
-                                gxf = fmaf(-w, dx, gxf);
-                                gyf = fmaf(-w, dy, gyf);
-                                gzf = fmaf(-w, dz, gzf);
-                            } else {
-                                accf = fmaf(h.w, ri, accf);
-                            }
-                        }
+                    float a = 0.f, ax = 0.f, ay = 0.f, az = 0.f;
+                    const float4 *H = shi[warp][slot], *L = slo[warp][slot];
+                    if (nph == 1) {
+                        if (check) p2p_batch<true, GRAD, 1>(H, L, tg, 0, 1, jself, a, ax, ay, az);
+                        else p2p_batch<false, GRAD, 1>(H, L, tg, 0, 1, jself, a, ax, ay, az);
+                    } else {
+                        if (check) p2p_batch<true, GRAD, 0>(H, L, tg, ph, nph, jself, a, ax, ay, az);
+                        else p2p_batch<false, GRAD, 0>(H, L, tg, ph, nph, jself, a, ax, ay, az);
                     }
-                    acc += (double)accf;
-                    if (GRAD) { gx += (double)gxf; gy += (double)gyf; gz += (double)gzf; }
+                    acc += (double)a;
+                    if (GRAD) { gx += (double)ax; gy += (double)ay; gz += (double)az; }
                 }
                 // slot is rewritten by batch bt + 2, after the next __syncwarp
             }
             __syncwarp();   // the next window restages slot 0
         }
-        for (int off = g; off < 32; off <<= 1) {
-            acc += __shfl_xor_sync(FULL, acc, off);
+        // sum the phases (lanes tl, tl + ntc, ...) through shared memory
+        red[warp][0][lane] = acc;
+        if (GRAD) { red[warp][1][lane] = gx; red[warp][2][lane] = gy; red[warp][3][lane] = gz; }
+        __syncwarp();
+        if (lane < ntc) {
+            double v = 0.0, vx = 0.0, vy = 0.0, vz = 0.0;
+            for (int q = 0; q < nph; ++q) {
+                v += red[warp][0][lane + q * ntc];
+                if (GRAD) {
+                    vx += red[warp][1][lane + q * ntc];
+                    vy += red[warp][2][lane + q * ntc];
+                    vz += red[warp][3][lane + q * ntc];
+                }
+            }
+            if (result) result[t] = scale * v;
             if (GRAD) {
-                gx += __shfl_xor_sync(FULL, gx, off);
-                gy += __shfl_xor_sync(FULL, gy, off);
-                gz += __shfl_xor_sync(FULL, gz, off);
+                grad[t] = scale * vx;
+                grad[tstride + t] = scale * vy;
+                grad[2 * tstride + t] = scale * vz;
             }
         }
-        if (active && ph == 0) {
-            if (result) result[t] = scale * acc;
-            if (GRAD) {
-                grad[t] = scale * gx;
-                grad[tstride + t] = scale * gy;
-                grad[2 * tstride + t] = scale * gz;
-            }
-        }
+        __syncwarp();
     }
 }
 

@@ -290,12 +290,16 @@ class SumpyExpansionWrangler:
         self._status = torch.zeros(1, dtype=torch.int32, device=self.device)
         # drive_fmm runs List 1, 3 and 4 on a second stream (sumpy_b200.drive)
         self.concurrent_stages = True
-        # mixed form: M2M as a tensor-core GEMM; L2L as an FP64 GEMM (the
-        # 3xTF32 L2L compounds its FP32 group sums down the levels: ~3x the
-        # mixed form's error on the 1M-point benchmark; see _tc_translations)
+        # one order on every level: M2M and L2L as eight dense maps per level
+        # applied as grouped GEMMs. Mixed form: M2M on the tensor cores
+        # (3xTF32), L2L as an FP64 GEMM (the 3xTF32 L2L compounds its FP32
+        # group sums down the levels: ~3x the mixed form's error on the
+        # 1M-point benchmark); FP64 form: both as FP64 GEMMs. Laplace only for
+        # the FP64 GEMMs; Helmholtz mixed uses the tensor-core M2M.
         self.tc_m2m = True
         self.tc_l2l = False
-        self.gemm_l2l = False
+        self.gemm_l2l = True
+        self.gemm_m2m = True
         # mixed List 3 / List 4: all levels in one launch over host-cut work
         # items (False: one launch per level, a warp per target box)
         self.item_kernels = True
@@ -481,6 +485,9 @@ class SumpyExpansionWrangler:
         if self._tc_translations and self.tc_m2m:
             return self._coarsen_tc(level_start_source_parent_box_nrs, source_parent_boxes,
                                     mpoles)
+        if self.gemm_m2m and self.precision == "fp64" and self._gemm_fp64_ok:
+            return self._coarsen_tc(level_start_source_parent_box_nrs, source_parent_boxes,
+                                    mpoles, fp64=True)
         lsp = _np_i32(level_start_source_parent_box_nrs)
         boxes = self._dev(source_parent_boxes)
         g = self._geom
@@ -919,7 +926,13 @@ class SumpyExpansionWrangler:
         self._call_m2l_tc(self.level_orders[0], plan, hi, lo, rp, kp, nb + 1, sbase,
                           ws_hi, ws_lo, tbase, tview, st)
 
-    def _coarsen_tc(self, level_start_source_parent_box_nrs, source_parent_boxes, mpoles):
+    @property
+    def _gemm_fp64_ok(self):
+        """M2M / L2L as FP64 octant GEMMs: Laplace, one order on every level."""
+        return not self.helmholtz and len(set(self.level_orders)) == 1
+
+    def _coarsen_tc(self, level_start_source_parent_box_nrs, source_parent_boxes, mpoles,
+                    fp64=False):
         lsp = _np_i32(level_start_source_parent_box_nrs)
         parents_all = _np_i32(source_parent_boxes)
         child = np.asarray(self.tree.box_child_ids)
@@ -929,7 +942,7 @@ class SumpyExpansionWrangler:
             a, b = int(lsp[tgt_lev]), int(lsp[tgt_lev + 1])
             if a == b:
                 continue
-            key = ("m2m-plan", tgt_lev, id(source_parent_boxes))
+            key = ("m2m-plan", tgt_lev, id(source_parent_boxes), fp64)
             if key not in self._m2l_plans:
                 parents = parents_all[a:b]
                 kids = child[:, parents]                       # [slot][parent]
@@ -939,11 +952,11 @@ class SumpyExpansionWrangler:
                     has = ch > 0
                     oc = self._octants(ch[has])
                     srcs[oc, np.nonzero(has)[0]] = ch[has]
-                self._octant_plan(key, parents, srcs)
+                self._octant_plan(key, parents, srcs, M2L_TILE if fp64 else M2L_TILE_TC)
             plan = self._m2l_plans[key]
             sbase, sview = self.multipole_expansions_view(mpoles, src_lev)
             tbase, tview = self.multipole_expansions_view(mpoles, tgt_lev)
-            self._octant_gemm("m2m", plan, sview, sbase, tview, tbase, st,
+            self._octant_gemm("m2m", plan, sview, sbase, tview, tbase, st, fp64=fp64,
                               parent_level=tgt_lev)
         return mpoles
 
@@ -1111,10 +1124,10 @@ class SumpyExpansionWrangler:
 
     def refine_locals(self, actx, level_start_target_or_target_parent_box_nrs,
                       target_or_target_parent_boxes, local_exps):
-        if self._tc_translations and not self.helmholtz and (self.tc_l2l or self.gemm_l2l):
+        tc = self._tc_translations and not self.helmholtz and self.tc_l2l
+        if tc or (self.gemm_l2l and self._gemm_fp64_ok):
             return self._refine_tc(level_start_target_or_target_parent_box_nrs,
-                                   target_or_target_parent_boxes, local_exps,
-                                   fp64=not self.tc_l2l)
+                                   target_or_target_parent_boxes, local_exps, fp64=not tc)
         lt = _np_i32(level_start_target_or_target_parent_box_nrs)
         boxes = self._dev(target_or_target_parent_boxes)
         g = self._geom

@@ -111,3 +111,30 @@ def test_merged_p2m_and_packed_l2p_match_per_level(cuda_device, order):
     assert relerr(pe[1], pe[0]) < 1e-13
     pots = [drive_fmm(None, ww, [q])[0].cpu() for ww in ws]
     assert relerr(pots[1], pots[0]) < 1e-13
+
+
+@pytest.mark.parametrize("order", [2, 10])
+def test_fp64_gemm_m2m_l2l_match_shift_kernels(cuda_device, order):
+    """FP64 form: M2M and L2L as per-octant FP64 GEMMs (the default with one
+    order on every level) against the per-box axis-shift kernels."""
+    src = sphere_plummer(30000, 12)
+    tree, trav, tcls = build_all(src, None, 30)
+    q = torch.as_tensor(np.random.default_rng(2).standard_normal(src.shape[1]), device="cuda")
+    wg = _wrangler(trav, tcls, order, "fp64", False, True)
+    wk = _wrangler(trav, tcls, order, "fp64", False, True)
+    wk.gemm_m2m = wk.gemm_l2l = False
+    qs = wg.reorder_sources(q)
+    mp = wg.form_multipoles(None, trav.level_start_source_box_nrs, trav.source_boxes, [qs])
+    outs = []
+    for w in (wg, wk):
+        m = w.coarsen_multipoles(None, trav.level_start_source_parent_box_nrs,
+                                 trav.source_parent_boxes, mp.clone())
+        loc = wg.multipole_to_local(None, trav.level_start_target_or_target_parent_box_nrs,
+                                    trav.target_or_target_parent_boxes,
+                                    trav.from_sep_siblings_starts, trav.from_sep_siblings_lists,
+                                    m)
+        loc = w.refine_locals(None, trav.level_start_target_or_target_parent_box_nrs,
+                              trav.target_or_target_parent_boxes, loc)
+        outs.append((m.cpu().numpy(), loc.cpu().numpy()))
+    assert relerr(outs[0][0], outs[1][0]) < 1e-13
+    assert relerr(outs[0][1], outs[1][1]) < 1e-13
