@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--only", choices=["mixed", "fp64", "batch", "helmholtz", "uniform"],
                     help="run one workload alone (--steps/--warmup apply) and print its result; "
                          "for profiling")
+    ap.add_argument("--eager", action="store_true",
+                    help="with --only: launch kernel by kernel instead of replaying a CUDA graph")
     ap.add_argument("--helmholtz-npoints", type=int, default=500_000)
     ap.add_argument("--helmholtz-precision", choices=["mixed", "fp64", "both"], default="both")
     return ap.parse_args()
@@ -295,9 +297,11 @@ def main():
         None, lambda o, **kw: MExp(knl, o), lambda o, **kw: LExp(knl, o), [knl],
         exclude_self=True)
 
-    def wrangler(precision):
+    def wrangler(precision, graph=True):
+        # graph: drive_fmm replays the evaluation from a CUDA graph (one host
+        # call per step); the eager form launches each kernel from Python
         return SumpyExpansionWrangler(ti, trav, np.float64, lambda k, a, t, lev: args.order,
-                                      precision=precision, device=dev)
+                                      precision=precision, device=dev, cuda_graph=graph)
 
     q_dev = torch.as_tensor(q, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
@@ -323,7 +327,7 @@ def main():
         return max_over_ranks(sum(ms), device=dev) / steps, ms
 
     if args.only in ("mixed", "fp64"):
-        w = wrangler(args.only)
+        w = wrangler(args.only, graph=not args.eager)
         for _ in range(max(1, args.warmup)):
             drive_fmm(None, w, [q_dev])
         ms, _ = timed(lambda: drive_fmm(None, w, [q_dev]), args.steps)
@@ -332,12 +336,19 @@ def main():
                 "ms_per_step": ms, "Mpts_s": args.npoints / (ms * 1e-3) / 1e6}}), flush=True)
         return
 
-    # setup (plans, tables) outside timing
+    # setup (plans, tables, graph capture) outside timing
     t0 = time.perf_counter()
     w_mx = wrangler("mixed")
     drive_fmm(None, w_mx, [q_dev])
     torch.cuda.synchronize()
     t_setup = time.perf_counter() - t0
+
+    # the same evaluation launched kernel by kernel from Python
+    w_mx.cuda_graph = False
+    for _ in range(max(1, args.warmup)):
+        drive_fmm(None, w_mx, [q_dev])
+    ms_eager, _ = timed(lambda: drive_fmm(None, w_mx, [q_dev]), args.steps)
+    w_mx.cuda_graph = True
 
     for _ in range(args.warmup):
         drive_fmm(None, w_mx, [q_dev])
@@ -352,8 +363,8 @@ def main():
     pot_host = torch.empty(args.npoints, dtype=torch.float64).pin_memory()
 
     def e2e_step():
-        qd = q_host.to(dev, non_blocking=True)
-        (pot,) = drive_fmm(None, w_mx, [qd])
+        # strengths copied from pinned host memory into the graph's input
+        (pot,) = drive_fmm(None, w_mx, [q_host])
         pot_host.copy_(pot, non_blocking=True)
 
     for _ in range(2):
@@ -375,7 +386,7 @@ def main():
         tree_b, trav_b, tcls_b = build_all(pts, None, FP64_MAX_PARTICLES)
         w_b = SumpyExpansionWrangler(ti, trav_b, np.float64, lambda k, a, t, lev: args.order,
                                      translation_classes_data=tcls_b, precision="fp64",
-                                     device=dev)
+                                     device=dev, cuda_graph=True)
         for _ in range(max(1, args.warmup)):
             drive_fmm(None, w_b, [q_dev])
         ms_b, _ = timed(lambda: drive_fmm(None, w_b, [q_dev]), args.steps)
@@ -418,8 +429,12 @@ def main():
                          "3xTF32 tensor-core M2L and M2M; FP64 elsewhere)",
             "l2": "flushed between steps (256 MB write outside the timed events)",
             "parallelism": f"replicas x{world}",
+            "launch": "drive_fmm replaying a CUDA graph of the whole evaluation "
+                      "(wrangler cuda_graph=True); eager timing beside it",
             "tree_build_s": round(t_tree, 3), "setup_s": round(t_setup, 3),
         },
+        "eager": {"ms_per_step": ms_eager,
+                  "value": world * args.npoints / (ms_eager * 1e-3) / 1e6},
         "accuracy": {"relL2_mixed": err_mx, "relL2_fp64": err_64, "targets_sampled": len(sample),
                      "reference": "FP64 direct sum (GPU kernel sumpy_p2p_direct_f64)"},
         "fp64": {"value": (world * args.npoints / (ms_64 * 1e-3) / 1e6) if ms_64 else None,

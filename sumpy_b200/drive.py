@@ -41,6 +41,52 @@ def _side_streams(wrangler):
 
 
 def drive_fmm(actx, wrangler, src_weight_vecs, timing_data=None):
+    if getattr(wrangler, "cuda_graph", False):
+        return _drive_graphed(actx, wrangler, src_weight_vecs)
+    return _drive_eager(actx, wrangler, src_weight_vecs)
+
+
+def _drive_graphed(actx, wrangler, src_weight_vecs):
+    """The same stage sequence replayed from a CUDA graph: captured on the
+    first call (after one eager pass that builds the wrangler's plans and
+    operator tables) with static copies of the strengths; every call copies
+    the strengths in (host or device), replays, and returns copies of the
+    static potentials. The graph is kept per input signature; it records the
+    wrangler's state at capture (traversal, precision and stage switches)."""
+    import torch
+    dev = wrangler.device
+    key = tuple((tuple(w.shape), w.dtype) for w in src_weight_vecs)
+    cache = getattr(wrangler, "_graph_cache", None)
+    if cache is None or cache[0] != key:
+        static = [torch.empty(w.shape, dtype=w.dtype, device=dev) for w in src_weight_vecs]
+        for s, w in zip(static, src_weight_vecs):
+            s.copy_(w)
+        cur = torch.cuda.current_stream(dev)
+        warm = torch.cuda.Stream(dev)
+        warm.wait_stream(cur)
+        with torch.cuda.stream(warm):
+            _drive_eager(actx, wrangler, static)
+        cur.wait_stream(warm)
+        torch.cuda.synchronize(dev)
+        from sumpy_b200._capi import launch_counter
+        graph = torch.cuda.CUDAGraph()
+        n0 = launch_counter.value
+        with torch.cuda.graph(graph):
+            out = _drive_eager(actx, wrangler, static)
+        # C-ABI launches recorded in the graph; each replay runs them again
+        nlaunch = launch_counter.value - n0
+        launch_counter.value = n0
+        wrangler._graph_cache = cache = (key, graph, static, out, nlaunch)
+    _, graph, static, out, nlaunch = cache
+    for s, w in zip(static, src_weight_vecs):
+        s.copy_(w, non_blocking=True)
+    graph.replay()
+    from sumpy_b200._capi import launch_counter
+    launch_counter.value += nlaunch
+    return [o.clone() for o in out]
+
+
+def _drive_eager(actx, wrangler, src_weight_vecs):
     trav = wrangler.traversal
     src_weight_vecs = [wrangler.reorder_sources(w) for w in src_weight_vecs]
     src_weight_vecs = wrangler.distribute_source_weights(src_weight_vecs)

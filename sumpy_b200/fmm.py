@@ -16,8 +16,10 @@ Beyond sumpy's knobs, the wrangler takes ``precision``: ``"fp64"`` (every
 stage in FP64) or ``"mixed"`` (FP32 near field, M2P and P2L with FP64
 offsets and sums; M2L and M2M as split-FP32 (3xTF32) GEMMs on the tcgen05
 tensor cores with FP32 accumulation and FP64 results; the other stages FP64), ``gradient`` (also
-return the potential's gradient at the targets) and ``m2l_item_groups`` (class
-groups per M2L work item, one CTA each; :mod:`sumpy_b200.autotune` picks it).
+return the potential's gradient at the targets), ``m2l_item_groups`` (class
+groups per M2L work item, one CTA each; :mod:`sumpy_b200.autotune` picks it)
+and ``cuda_graph`` (``drive_fmm`` replays the evaluation from a captured CUDA
+graph).
 """
 from __future__ import annotations
 
@@ -239,7 +241,8 @@ class SumpyExpansionWrangler:
                  source_extra_kwargs=None, kernel_extra_kwargs=None,
                  self_extra_kwargs=None, translation_classes_data=None,
                  preprocessed_mpole_dtype=None, *, _disable_translation_classes=False,
-                 precision="fp64", device=None, gradient=False, m2l_item_groups=None):
+                 precision="fp64", device=None, gradient=False, m2l_item_groups=None,
+                 cuda_graph=False):
         if not callable(fmm_level_to_order):
             raise TypeError("fmm_level_to_order not passed")
         if precision not in ("fp64", "mixed"):
@@ -305,6 +308,9 @@ class SumpyExpansionWrangler:
         self.item_kernels = True
         # P2M and L2P of all levels in one launch (one order on every level)
         self.merge_levels = True
+        # drive_fmm replays the whole evaluation from a CUDA graph (one host
+        # call per evaluation instead of one per kernel launch)
+        self.cuda_graph = bool(cuda_graph)
         self.m2l_item_groups = int(m2l_item_groups or M2L_ITEM_GROUPS)
         if self.m2l_item_groups < 1:
             raise ValueError("m2l_item_groups must be >= 1")
