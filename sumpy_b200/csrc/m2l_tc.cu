@@ -269,12 +269,28 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
         // thread 0: TMA tiles of the two operator planes; all 96 threads:
         // cp.async row copies of the two source planes (the gathered
         // multipoles), then an asynchronous arrival on the stage barrier.
+        // A thread's (slot, 16-byte column) chunks are c = tid + 96 u; the
+        // group's source boxes of those slots are loaded once per group, one
+        // group ahead (the same rows serve all K chunks of the group).
+        constexpr int NU = (TC_TW * 8 + TC_LOADERS - 1) / TC_LOADERS;
+        int32_t sb_cur[NU], sb_nxt[NU];
+        auto load_rows = [&](int g, int32_t *dst) {
+            const int32_t *gs = a.group_sources + (int64_t)g * TC_TW;
+#pragma unroll
+            for (int u = 0; u < NU; ++u) {
+                const int c = threadIdx.x + u * TC_LOADERS;
+                dst[u] = c < TC_TW * 8 ? gs[c >> 3] : -1;
+            }
+        };
+        if (ng > 0) load_rows(g0, sb_cur);
         for (int it = 0; it < total; ++it) {
             const int s = it % TC_STAGES, use = it / TC_STAGES;
+            const int gi = it / nkc, kc = it % nkc;
+            if (kc == 0 && gi + 1 < ng) load_rows(g0 + gi + 1, sb_nxt);
             bool ok = true;
             if (use > 0) ok = mbar_wait_or_abort(empty_bar + 8 * s, (use - 1) & 1, abort_flag);
             if (loaders_sync_or(!ok || *abort_flag)) break;
-            const int g = g0 + it / nkc, k0 = (it % nkc) * TC_KC;
+            const int g = g0 + gi, k0 = kc * TC_KC;
             const uint32_t st = base + s * STAGE;
             if (threadIdx.x == 0) {
                 mbar_expect_tx(full_bar + 8 * s, 2 * PLANE);
@@ -282,19 +298,26 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
                 tma_load_3d(st, &map_a_hi, k0, row0, cls, full_bar + 8 * s);
                 tma_load_3d(st + PLANE, &map_a_lo, k0, row0, cls, full_bar + 8 * s);
             }
-            const int32_t *gs = a.group_sources + (int64_t)g * TC_TW;
-            for (int c = threadIdx.x; c < TC_TW * 8; c += TC_LOADERS) {
-                const int slot = c >> 3, q = c & 7;
-                const int32_t sb = gs[slot];
-                const uint32_t dst = slot * 128 + ((q ^ (slot & 7)) << 4);
-                // empty slots: zero-fill without reading memory (source size 0)
-                const int64_t row = sb >= 0 ? sb - a.src_row_base : a.zero_row;
-                const int64_t off = row * a.k_pad + k0 + 4 * q;
-                const uint32_t bytes = sb >= 0 ? 16u : 0u;
-                cp_async16(st + 2 * PLANE + dst, a.src_hi + off, bytes);
-                cp_async16(st + 3 * PLANE + dst, a.src_lo + off, bytes);
+#pragma unroll
+            for (int u = 0; u < NU; ++u) {
+                const int c = threadIdx.x + u * TC_LOADERS;
+                if (c < TC_TW * 8) {
+                    const int slot = c >> 3, q = c & 7;
+                    const int32_t sb = sb_cur[u];
+                    const uint32_t dst = slot * 128 + ((q ^ (slot & 7)) << 4);
+                    // empty slots: zero-fill without reading memory (source size 0)
+                    const int64_t row = sb >= 0 ? sb - a.src_row_base : a.zero_row;
+                    const int64_t off = row * a.k_pad + k0 + 4 * q;
+                    const uint32_t bytes = sb >= 0 ? 16u : 0u;
+                    cp_async16(st + 2 * PLANE + dst, a.src_hi + off, bytes);
+                    cp_async16(st + 3 * PLANE + dst, a.src_lo + off, bytes);
+                }
             }
             cp_async_arrive_noinc(full_bar + 8 * s);
+            if (kc == nkc - 1) {
+#pragma unroll
+                for (int u = 0; u < NU; ++u) sb_cur[u] = sb_nxt[u];
+            }
         }
     } else if (warp == 3) {
         // ---------------- MMA issuer ----------------
