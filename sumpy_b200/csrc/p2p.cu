@@ -185,8 +185,39 @@ __device__ __forceinline__ void p2p_batch(const float4 *__restrict__ hi, const f
     }
 }
 
+// The same for all 32 sources against one target, two sources per
+// instruction with the packed FP32 pairs of sm_100 (FADD2 / FMUL2 / FFMA2):
+// source pair m holds sources 2m and 2m + 1 as {-x_hi, -y_hi} {-z_hi, q}
+// {-x_lo, -y_lo} {-z_lo, -} (float2 halves); per pair the same roundings as
+// p2p_batch, the sum kept as two partial sums.
+__device__ __forceinline__ void p2p_batch_packed(const float4 *__restrict__ P0,
+                                                 const float4 *__restrict__ P1,
+                                                 const float4 *__restrict__ P2,
+                                                 const float4 *__restrict__ P3,
+                                                 const P2PTarget &t, float &acc)
+{
+    const float2 txh = make_float2(t.xh, t.xh), txl = make_float2(t.xl, t.xl);
+    const float2 tyh = make_float2(t.yh, t.yh), tyl = make_float2(t.yl, t.yl);
+    const float2 tzh = make_float2(t.zh, t.zh), tzl = make_float2(t.zl, t.zl);
+    float2 a2 = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const float4 p0 = P0[m], p1 = P1[m], p2 = P2[m], p3 = P3[m];
+        const float2 dx = __fadd2_rn(__fadd2_rn(txh, make_float2(p0.x, p0.y)),
+                                     __fadd2_rn(txl, make_float2(p2.x, p2.y)));
+        const float2 dy = __fadd2_rn(__fadd2_rn(tyh, make_float2(p0.z, p0.w)),
+                                     __fadd2_rn(tyl, make_float2(p2.z, p2.w)));
+        const float2 dz = __fadd2_rn(__fadd2_rn(tzh, make_float2(p1.x, p1.y)),
+                                     __fadd2_rn(tzl, make_float2(p3.x, p3.y)));
+        const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+        const float2 ri = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+        a2 = __ffma2_rn(make_float2(p1.z, p1.w), ri, a2);
+    }
+    acc += a2.x + a2.y;
+}
+
 template <bool GRAD>
-__global__ void __launch_bounds__(32 * P2PF_WARPS)
+__global__ void __launch_bounds__(32 * P2PF_WARPS, 4)
 p2p_flat_mixed_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_boxes,
                       const int32_t *__restrict__ src_box_starts,
                       const int32_t *__restrict__ src_box_lists,
@@ -201,6 +232,7 @@ p2p_flat_mixed_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_box
 {
     __shared__ float4 shi[P2PF_WARPS][2][32];   // x, y, z hi parts, q
     __shared__ float4 slo[P2PF_WARPS][2][32];   // x, y, z lo parts
+    __shared__ float4 spk[P2PF_WARPS][2][4][16];   // the same as source pairs (packed path)
     __shared__ double red[P2PF_WARPS][GRAD ? 4 : 1][32];
     const unsigned FULL = 0xffffffffu;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -285,6 +317,17 @@ p2p_flat_mixed_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_box
                     l.w = 0.f;
                     shi[warp][slot][lane] = h;
                     slo[warp][slot][lane] = l;
+                    if (!GRAD) {
+                        float *pk = reinterpret_cast<float *>(spk[warp][slot][0]);
+                        const int m = lane >> 1, hh = lane & 1;
+                        pk[0 * 64 + 4 * m + hh] = -h.x;
+                        pk[0 * 64 + 4 * m + 2 + hh] = -h.y;
+                        pk[1 * 64 + 4 * m + hh] = -h.z;
+                        pk[1 * 64 + 4 * m + 2 + hh] = h.w;
+                        pk[2 * 64 + 4 * m + hh] = -l.x;
+                        pk[2 * 64 + 4 * m + 2 + hh] = -l.y;
+                        pk[3 * 64 + 4 * m + hh] = -l.z;
+                    }
                 }
                 if (bt + 1 < nbat) {
                     const int32_t f = 32 * (bt + 1) + lane;
@@ -303,8 +346,14 @@ p2p_flat_mixed_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_box
                     float a = 0.f, ax = 0.f, ay = 0.f, az = 0.f;
                     const float4 *H = shi[warp][slot], *L = slo[warp][slot];
                     if (nph == 1) {
-                        if (check) p2p_batch<true, GRAD, 1>(H, L, tg, 0, 1, jself, a, ax, ay, az);
-                        else p2p_batch<false, GRAD, 1>(H, L, tg, 0, 1, jself, a, ax, ay, az);
+                        if (check) {
+                            p2p_batch<true, GRAD, 1>(H, L, tg, 0, 1, jself, a, ax, ay, az);
+                        } else if constexpr (GRAD) {
+                            p2p_batch<false, GRAD, 1>(H, L, tg, 0, 1, jself, a, ax, ay, az);
+                        } else {
+                            p2p_batch_packed(spk[warp][slot][0], spk[warp][slot][1],
+                                             spk[warp][slot][2], spk[warp][slot][3], tg, a);
+                        }
                     } else {
                         if (check) p2p_batch<true, GRAD, 0>(H, L, tg, ph, nph, jself, a, ax, ay, az);
                         else p2p_batch<false, GRAD, 0>(H, L, tg, ph, nph, jself, a, ax, ay, az);

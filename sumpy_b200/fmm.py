@@ -513,6 +513,29 @@ class SumpyExpansionWrangler:
                  _i64(self.tree.nboxes), _i32(sbase), dptr(sview), _i32(tbase), dptr(tview), st)
         return mpoles
 
+    def _cost_sorted_csr(self, target_boxes, starts, lists):
+        """The List-1 CSR with its target boxes in decreasing order of
+        pairs (targets x list sources): warps of similar length share a CTA
+        and the longest start first. Results are per target, so the order
+        does not change them."""
+        def build():
+            tb = np.asarray(target_boxes, dtype=np.int64)
+            st = np.asarray(starts, dtype=np.int64)
+            ls = np.asarray(lists, dtype=np.int64)
+            cnt = np.diff(st)
+            bsc = np.asarray(self.tree.box_source_counts_nonchild, dtype=np.int64)
+            csum = np.concatenate([[0], np.cumsum(bsc[ls])])
+            pairs = np.asarray(self.tree.box_target_counts_nonchild, dtype=np.int64)[tb] * \
+                (csum[st[1:]] - csum[st[:-1]])
+            order = np.argsort(-pairs, kind="stable")
+            ncnt = cnt[order]
+            nst = np.concatenate([[0], np.cumsum(ncnt)])
+            nls = ls[_expand_ranges(st[:-1][order], ncnt)]
+            return tuple(torch.as_tensor(a.astype(np.int32)).to(self.device)
+                         for a in (tb[order], nst, nls))
+        return self._cached_items(("p2p_sorted", id(lists)), (target_boxes, starts, lists),
+                                  build)
+
     def eval_direct(self, actx, target_boxes, source_box_starts, source_box_lists,
                     src_weight_vecs):
         pot = self.output_zeros(actx)
@@ -521,8 +544,13 @@ class SumpyExpansionWrangler:
             return pot
         g = self._geom
         w = self._weights(src_weight_vecs)
-        args = (_i32(tb.numel()), dptr(tb), dptr(self._dev(source_box_starts)),
-                dptr(self._dev(source_box_lists)), dptr(g["bss"]), dptr(g["bsc"]),
+        if not any(isinstance(a, torch.Tensor)
+                   for a in (target_boxes, source_box_starts, source_box_lists)):
+            tb, st_d, ls_d = self._cost_sorted_csr(target_boxes, source_box_starts,
+                                                   source_box_lists)
+        else:
+            st_d, ls_d = self._dev(source_box_starts), self._dev(source_box_lists)
+        args = (_i32(tb.numel()), dptr(tb), dptr(st_d), dptr(ls_d), dptr(g["bss"]), dptr(g["bsc"]),
                 dptr(g["bts"]), dptr(g["btc"]), dptr(g["sources"]), _i64(self.tree.nsources),
                 *self._kargs, dptr(w), dptr(g["targets"]), _i64(self.tree.ntargets),
                 dptr(g["tts"]), _d(self._scale), dptr(pot[0]))
