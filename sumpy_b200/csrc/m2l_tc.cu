@@ -16,17 +16,17 @@
 //
 // CTA = 384 threads, one work item: a range of class groups of one output
 // tile of 128 coefficient rows x 128 target slots (the MMA is M=128, N=128,
-// K=8 per instruction). Operand tiles are K-major with the 128-byte
-// swizzle: each row (a coefficient row of T_c, or the coefficients of one
-// source multipole) holds 32 fp32 of K in 128 bytes; 8 rows form a
-// 1024-byte swizzle atom. K is streamed in chunks of 32 through a 3-stage
-// shared-memory ring: a TMA tiled load per operator plane (1024-byte
-// aligned) and cp.async row copies of the gathered source multipoles, all
-// completing on the stage's "full" mbarrier (TMA byte count plus one
-// asynchronous cp.async arrival per loader thread). One thread issues
-// the 12 MMAs of a chunk (4 K-steps x 3 products) and commits them to the
-// stage's "empty" mbarrier, which the loader waits on before refilling the
-// stage. Every load fills this CTA's own shared memory only. All waits are bounded by a clock
+// K=8 per instruction). Operand tiles are K-major and swizzled: each row (a
+// coefficient row of T_c, or the coefficients of one source multipole)
+// holds TC_KC fp32 of K (16 in 64 bytes, or 32 in 128 bytes, with the
+// swizzle of that width); 8 rows form a swizzle atom. K is streamed in
+// chunks of TC_KC through a ring of shared-memory stages (6 of 32 KB, or 3
+// of 64 KB): a TMA tiled load per operator plane and cp.async row copies of
+// the gathered source multipoles, all completing on the stage's "full"
+// mbarrier (TMA byte count plus one asynchronous cp.async arrival per loader
+// thread). One thread issues the MMAs of a chunk (TC_KC / 8 K-steps x 3
+// products) and commits them to the stage's "empty" mbarrier, which the
+// loader waits on before refilling the stage. Every load fills this CTA's own shared memory only. All waits are bounded by a clock
 // budget; on expiry the kernel records an error in *status, lets work in
 // flight finish, frees its tensor memory and returns.
 #include <algorithm>
@@ -43,15 +43,25 @@ namespace {
 
 constexpr int TC_TW = 128;      // target slots per tile (MMA N)
 constexpr int TC_M = 128;       // coefficient rows per CTA (MMA M)
-constexpr int TC_KC = 32;       // fp32 K elements per 128-byte row
-constexpr int TC_STAGES = 3;
+#ifndef SUMPY_TC_KC
+#define SUMPY_TC_KC 32
+#endif
+// K per stage: 32 fp32 (128-byte operand rows and swizzle, three stages) or
+// 16 (64-byte rows and swizzle, six stages in the same shared memory;
+// measured 1.5x slower on the 1M-point M2L: twice the per-stage barrier and
+// issue overhead for the same bytes)
+constexpr int TC_KC = SUMPY_TC_KC;
+static_assert(TC_KC == 16 || TC_KC == 32, "K per stage");
+constexpr int ROWB = 4 * TC_KC;                // bytes per operand row = swizzle span
+constexpr int CPR = ROWB / 16;                 // 16-byte chunks per row
+constexpr int TC_STAGES = TC_KC == 32 ? 3 : 6;
 constexpr int TC_LOADERS = 96;             // warps 0-2
 constexpr int TC_DRAINERS = 256;           // warps 4-11
 constexpr int TC_THREADS = 128 + TC_DRAINERS;
-constexpr int PLANE = TC_M * 128;          // bytes of one 128 x 32 fp32 operand tile
+constexpr int PLANE = TC_M * ROWB;         // bytes of one 128-row operand tile
 constexpr int STAGE = 4 * PLANE;           // A_hi, A_lo, B_hi, B_lo
 constexpr int TC_SMEM = TC_STAGES * STAGE + 1024 /* alignment slack */ + 256 /* barriers */;
-static_assert(2 * PLANE == 32768, "TMA bytes of a stage");
+static_assert(TC_SMEM <= 227 * 1024, "shared memory per CTA");
 constexpr uint32_t TMEM_COLS = 256;         // two 128-column accumulators
 constexpr long long WAIT_CYCLES = 4000000000LL;  // ~2 s at 2 GHz
 
@@ -95,16 +105,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t addr, uint32_t parity)
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
 
-// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row atoms
-// 1024 bytes apart (stride byte offset), descriptor version 1.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr)
+// Shared-memory matrix descriptor: K-major, ROWB-byte swizzle (layout
+// type 2 = 128-byte, 4 = 64-byte), 8-row atoms 8 * ROWB bytes apart (stride
+// byte offset), descriptor version 1.
+__device__ __forceinline__ uint64_t sw_desc(uint32_t saddr)
 {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3fff);
     d |= (uint64_t)1 << 16;                 // leading byte offset (unused for swizzled K-major)
-    d |= (uint64_t)(1024 >> 4) << 32;       // stride byte offset
+    d |= (uint64_t)((8 * ROWB) >> 4) << 32; // stride byte offset
     d |= (uint64_t)1 << 46;                 // version
-    d |= (uint64_t)2 << 61;                 // 128-byte swizzle
+    d |= (uint64_t)(ROWB == 128 ? 2 : 4) << 61;
     return d;
 }
 
@@ -163,7 +174,7 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t addr, uint32_t bytes)
                  : "memory");
 }
 
-// TMA: one 3D tile (32 fp32 of K x 128 rows x 1 class) of a class-operator plane
+// TMA: one 3D tile (TC_KC fp32 of K x 128 rows x 1 class) of a class-operator plane
 __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, int c0, int c1,
                                             int c2, uint32_t mbar)
 {
@@ -272,39 +283,49 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
         // A thread's (slot, 16-byte column) chunks are c = tid + 96 u; the
         // group's source boxes of those slots are loaded once per group, one
         // group ahead (the same rows serve all K chunks of the group).
-        constexpr int NU = (TC_TW * 8 + TC_LOADERS - 1) / TC_LOADERS;
+        constexpr int NU = (TC_TW * CPR + TC_LOADERS - 1) / TC_LOADERS;
         int32_t sb_cur[NU], sb_nxt[NU];
         auto load_rows = [&](int g, int32_t *dst) {
             const int32_t *gs = a.group_sources + (int64_t)g * TC_TW;
 #pragma unroll
             for (int u = 0; u < NU; ++u) {
                 const int c = threadIdx.x + u * TC_LOADERS;
-                dst[u] = c < TC_TW * 8 ? gs[c >> 3] : -1;
+                dst[u] = c < TC_TW * CPR ? gs[c / CPR] : -1;
             }
         };
-        if (ng > 0) load_rows(g0, sb_cur);
+        // thread 0 also reads the group's class (the operator for the TMA
+        // loads) one group ahead
+        int cls_cur = 0, cls_nxt = 0;
+        if (ng > 0) {
+            load_rows(g0, sb_cur);
+            if (threadIdx.x == 0) cls_cur = a.group_class[g0];
+        }
         for (int it = 0; it < total; ++it) {
             const int s = it % TC_STAGES, use = it / TC_STAGES;
             const int gi = it / nkc, kc = it % nkc;
-            if (kc == 0 && gi + 1 < ng) load_rows(g0 + gi + 1, sb_nxt);
+            if (kc == 0 && gi + 1 < ng) {
+                load_rows(g0 + gi + 1, sb_nxt);
+                if (threadIdx.x == 0) cls_nxt = a.group_class[g0 + gi + 1];
+            }
             bool ok = true;
             if (use > 0) ok = mbar_wait_or_abort(empty_bar + 8 * s, (use - 1) & 1, abort_flag);
             if (loaders_sync_or(!ok || *abort_flag)) break;
-            const int g = g0 + gi, k0 = kc * TC_KC;
+            const int k0 = kc * TC_KC;
             const uint32_t st = base + s * STAGE;
             if (threadIdx.x == 0) {
                 mbar_expect_tx(full_bar + 8 * s, 2 * PLANE);
-                const int cls = a.group_class[g];
-                tma_load_3d(st, &map_a_hi, k0, row0, cls, full_bar + 8 * s);
-                tma_load_3d(st + PLANE, &map_a_lo, k0, row0, cls, full_bar + 8 * s);
+                tma_load_3d(st, &map_a_hi, k0, row0, cls_cur, full_bar + 8 * s);
+                tma_load_3d(st + PLANE, &map_a_lo, k0, row0, cls_cur, full_bar + 8 * s);
             }
 #pragma unroll
             for (int u = 0; u < NU; ++u) {
                 const int c = threadIdx.x + u * TC_LOADERS;
-                if (c < TC_TW * 8) {
-                    const int slot = c >> 3, q = c & 7;
+                if (c < TC_TW * CPR) {
+                    const int slot = c / CPR, q = c % CPR;
                     const int32_t sb = sb_cur[u];
-                    const uint32_t dst = slot * 128 + ((q ^ (slot & 7)) << 4);
+                    // the swizzle: 16-byte chunk q of a row XOR address bits 7.. of the row
+                    const uint32_t dst =
+                        slot * ROWB + ((q ^ (((slot * ROWB) >> 7) & (CPR - 1))) << 4);
                     // empty slots: zero-fill without reading memory (source size 0)
                     const int64_t row = sb >= 0 ? sb - a.src_row_base : a.zero_row;
                     const int64_t off = row * a.k_pad + k0 + 4 * q;
@@ -317,6 +338,7 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
             if (kc == nkc - 1) {
 #pragma unroll
                 for (int u = 0; u < NU; ++u) sb_cur[u] = sb_nxt[u];
+                cls_cur = cls_nxt;
             }
         }
     } else if (warp == 3) {
@@ -332,8 +354,8 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
                     break;
                 tc_fence_after();
                 const uint32_t st = base + s * STAGE;
-                const uint64_t ah = sw128_desc(st), al = sw128_desc(st + PLANE);
-                const uint64_t bh = sw128_desc(st + 2 * PLANE), bl = sw128_desc(st + 3 * PLANE);
+                const uint64_t ah = sw_desc(st), al = sw_desc(st + PLANE);
+                const uint64_t bh = sw_desc(st + 2 * PLANE), bl = sw_desc(st + 3 * PLANE);
                 const uint32_t d = tmem + (uint32_t)(acc * TC_TW);
 #pragma unroll
                 for (int k = 0; k < TC_KC / 8; ++k) {
@@ -466,19 +488,20 @@ static EncodeTiledFn encode_tiled_fn()
     return fn;
 }
 
-// fp32 tensor map over [dims[rank-1]]...[dims[0]], 128-byte swizzle, box {32, box1, 1}
+// fp32 tensor map over [dims[rank-1]]...[dims[0]], ROWB-byte swizzle, box {TC_KC, box1, 1}
 static bool make_map(CUtensorMap *m, const float *ptr, int rank, const uint64_t *dims,
                      uint32_t box1)
 {
     EncodeTiledFn fn = encode_tiled_fn();
     if (!fn) return false;
     cuuint64_t gdim[3], gstride[2];
-    cuuint32_t box[3] = {32, box1, 1}, estr[3] = {1, 1, 1};
+    cuuint32_t box[3] = {(cuuint32_t)TC_KC, box1, 1}, estr[3] = {1, 1, 1};
     for (int i = 0; i < rank; ++i) gdim[i] = dims[i];
     gstride[0] = dims[0] * sizeof(float);
     if (rank == 3) gstride[1] = dims[0] * dims[1] * sizeof(float);
     CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, const_cast<float *>(ptr), gdim, gstride,
-                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    ROWB == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
 }
@@ -498,7 +521,7 @@ static int m2l_tf32x3_launch(
 {
     if (tile_width != TC_TW) return bad_arg("m2l_tf32x3: tile_width must be 128");
     if (rows_pad < n || rows_pad % TC_M) return bad_arg("m2l_tf32x3: rows_pad must be a multiple of 128 >= ncoeff");
-    if (k_pad < n || k_pad % TC_KC) return bad_arg("m2l_tf32x3: k_pad must be a multiple of 32 >= ncoeff");
+    if (k_pad < n || k_pad % 32) return bad_arg("m2l_tf32x3: k_pad must be a multiple of 32 >= ncoeff");
     if (nitems < 0 || nclasses <= 0 || src_nrows < 1) return bad_arg("m2l_tf32x3: bad sizes");
     if (nitems == 0) return SUMPY_OK;
     if (!item_tile || !item_group_begin || !item_group_end || !tile_targets || !tile_scale ||
@@ -634,7 +657,7 @@ int sumpy_m2l_translation_classes_tf32x3_noalloc(
         return SUMPY_EUNSUPPORTED;
     }
     const int n = ncoeff_of(order);
-    if (nsrc_boxes < 0 || k_pad < n || k_pad % TC_KC) return bad_arg("m2l_tf32x3_noalloc: bad sizes");
+    if (nsrc_boxes < 0 || k_pad < n || k_pad % 32) return bad_arg("m2l_tf32x3_noalloc: bad sizes");
     if (k_pad > NOALLOC_KPAD || (int64_t)(nsrc_boxes + 1) * k_pad > NOALLOC_ROWS * NOALLOC_KPAD) {
         set_last_error("m2l_tf32x3_noalloc: request exceeds the built-in scratch: needs (nsrc_boxes+1)*k_pad <= " +
                        std::to_string(NOALLOC_ROWS * NOALLOC_KPAD) + " and k_pad <= " +
