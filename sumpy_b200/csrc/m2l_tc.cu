@@ -55,6 +55,14 @@ static_assert(TC_KC == 16 || TC_KC == 32, "K per stage");
 constexpr int ROWB = 4 * TC_KC;                // bytes per operand row = swizzle span
 constexpr int CPR = ROWB / 16;                 // 16-byte chunks per row
 constexpr int TC_STAGES = TC_KC == 32 ? 3 : 6;
+#ifndef SUMPY_TC_GATHER
+#define SUMPY_TC_GATHER 0
+#endif
+// the gathered source rows: cp.async 16-byte copies by three loader warps
+// (0), or TMA gather4 by one loader warp (1: same results, measured 3x
+// slower on the 1M-point M2L -- 64 gather instructions of 512 bytes per
+// stage queue on the SM's one TMA unit)
+constexpr bool TC_GATHER = SUMPY_TC_GATHER != 0;
 constexpr int TC_LOADERS = 96;             // warps 0-2
 constexpr int TC_DRAINERS = 256;           // warps 4-11
 constexpr int TC_THREADS = 128 + TC_DRAINERS;
@@ -185,6 +193,19 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
         : "memory");
 }
 
+// TMA gather of four rows (r0..r3, one row high box of TC_KC fp32 at column
+// c0) of a 2D plane into four consecutive swizzled smem rows
+__device__ __forceinline__ void tma_gather4(uint32_t dst, const CUtensorMap *map, int c0, int r0,
+                                            int r1, int r2, int r3, uint32_t mbar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];\n" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(r0), "r"(r1), "r"(r2), "r"(r3),
+        "r"(mbar)
+        : "memory");
+}
+
 // bounded wait that also gives up when another thread has aborted
 __device__ bool mbar_wait_or_abort(uint32_t addr, uint32_t parity, volatile int *abort_flag)
 {
@@ -222,7 +243,9 @@ __device__ __forceinline__ bool loaders_sync_or(bool v)
 // the local expansions with FP64 atomics (a tile may span several items).
 __global__ void __launch_bounds__(TC_THREADS, 1)
 m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
-                  const __grid_constant__ CUtensorMap map_a_lo)
+                  const __grid_constant__ CUtensorMap map_a_lo,
+                  const __grid_constant__ CUtensorMap map_b_hi,
+                  const __grid_constant__ CUtensorMap map_b_lo)
 {
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_addr(smem_raw);
@@ -250,7 +273,8 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
     }
     if (threadIdx.x == 32) {
         for (int s = 0; s < TC_STAGES; ++s) {
-            mbar_init(full_bar + 8 * s, TC_LOADERS + 1);  // cp.async arrivals + TMA expect-tx
+            // TMA expect-tx (+ the cp.async arrivals of the copying loaders)
+            mbar_init(full_bar + 8 * s, TC_GATHER ? 1 : TC_LOADERS + 1);
             mbar_init(empty_bar + 8 * s, 1);
         }
         for (int s = 0; s < 2; ++s) {
@@ -263,6 +287,10 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
     if (threadIdx.x == 64) {
         asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&map_a_hi)) : "memory");
         asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&map_a_lo)) : "memory");
+        if (TC_GATHER) {
+            asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&map_b_hi)) : "memory");
+            asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&map_b_lo)) : "memory");
+        }
     }
     tc_fence_before();
     __syncthreads();
@@ -275,7 +303,57 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
     const int nkc = a.k_pad / TC_KC;
     const int total = ng * nkc;
 
-    if (warp < TC_LOADERS / 32) {
+    if (TC_GATHER && warp == 0) {
+        // ---------------- loader (one warp, all TMA) ----------------
+        // lane 0: the two operator tiles; lane l: gather4 of slots 4l..4l+3
+        // of both source planes (empty slots read the zero row); lane 0
+        // posts the stage's bytes once. A group's rows and class are read
+        // once per group, one group ahead.
+        const unsigned FULL = 0xffffffffu;
+        int32_t r_cur[4], r_nxt[4];
+        auto load_rows = [&](int g, int32_t *dst) {
+            const int32_t *gs = a.group_sources + (int64_t)g * TC_TW + 4 * lane;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int32_t sb = gs[i];
+                dst[i] = sb >= 0 ? sb - a.src_row_base : a.zero_row;
+            }
+        };
+        int cls_cur = 0, cls_nxt = 0;
+        if (ng > 0) {
+            load_rows(g0, r_cur);
+            if (lane == 0) cls_cur = a.group_class[g0];
+        }
+        for (int it = 0; it < total; ++it) {
+            const int s = it % TC_STAGES, use = it / TC_STAGES;
+            const int gi = it / nkc, kc = it % nkc;
+            if (kc == 0 && gi + 1 < ng) {
+                load_rows(g0 + gi + 1, r_nxt);
+                if (lane == 0) cls_nxt = a.group_class[g0 + gi + 1];
+            }
+            bool ok = true;
+            if (use > 0) ok = mbar_wait_or_abort(empty_bar + 8 * s, (use - 1) & 1, abort_flag);
+            if (__any_sync(FULL, !ok || *abort_flag)) break;
+            const int k0 = kc * TC_KC;
+            const uint32_t st = base + s * STAGE;
+            if (lane == 0) {
+                mbar_expect_tx(full_bar + 8 * s, 4 * PLANE);
+                tma_load_3d(st, &map_a_hi, k0, row0, cls_cur, full_bar + 8 * s);
+                tma_load_3d(st + PLANE, &map_a_lo, k0, row0, cls_cur, full_bar + 8 * s);
+            }
+            __syncwarp();
+            const uint32_t rows4 = (uint32_t)lane * 4 * ROWB;
+            tma_gather4(st + 2 * PLANE + rows4, &map_b_hi, k0, r_cur[0], r_cur[1], r_cur[2],
+                        r_cur[3], full_bar + 8 * s);
+            tma_gather4(st + 3 * PLANE + rows4, &map_b_lo, k0, r_cur[0], r_cur[1], r_cur[2],
+                        r_cur[3], full_bar + 8 * s);
+            if (kc == nkc - 1) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) r_cur[i] = r_nxt[i];
+                cls_cur = cls_nxt;
+            }
+        }
+    } else if (!TC_GATHER && warp < TC_LOADERS / 32) {
         // ---------------- loaders ----------------
         // thread 0: TMA tiles of the two operator planes; all 96 threads:
         // cp.async row copies of the two source planes (the gathered
@@ -543,9 +621,11 @@ static int m2l_tf32x3_launch(
         }
         attr_set[dev] = true;
     }
-    CUtensorMap ma_hi, ma_lo;
+    CUtensorMap ma_hi, ma_lo, mb_hi, mb_lo;
     const uint64_t adims[3] = {(uint64_t)k_pad, (uint64_t)rows_pad, (uint64_t)nclasses};
-    if (!make_map(&ma_hi, mats_hi, 3, adims, TC_M) || !make_map(&ma_lo, mats_lo, 3, adims, TC_M)) {
+    const uint64_t bdims[2] = {(uint64_t)k_pad, (uint64_t)src_nrows};
+    if (!make_map(&ma_hi, mats_hi, 3, adims, TC_M) || !make_map(&ma_lo, mats_lo, 3, adims, TC_M) ||
+        !make_map(&mb_hi, src_hi, 2, bdims, 1) || !make_map(&mb_lo, src_lo, 2, bdims, 1)) {
         set_last_error("m2l_tf32x3: tensor map encoding failed");
         return SUMPY_EINVAL;
     }
@@ -558,7 +638,8 @@ static int m2l_tf32x3_launch(
     a.src_row_base = src_base_ibox; a.zero_row = src_nrows - 1;
     a.tbase = tgt_base_ibox; a.tgt = tgt_expansions; a.status = status;
     dim3 grid(nitems, rows_pad / TC_M);
-    m2l_tf32x3_kernel<<<grid, TC_THREADS, TC_SMEM, as_stream(stream)>>>(a, ma_hi, ma_lo);
+    m2l_tf32x3_kernel<<<grid, TC_THREADS, TC_SMEM, as_stream(stream)>>>(a, ma_hi, ma_lo, mb_hi,
+                                                                        mb_lo);
     return check_launch("m2l_tf32x3_kernel");
 }
 
