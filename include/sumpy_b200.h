@@ -496,6 +496,39 @@ int sumpy_helmholtz_p2e_from_csr_f64(
     const int32_t *box_source_counts_nonchild, const double *sources, int64_t source_stride,
     const double *strength, int32_t tgt_base_ibox, double *tgt_expansions, void *stream);
 
+/* All levels in one launch (one order on every level, flat complex
+ * [nboxes][(order+1)^2] expansions; levels and items as for the Laplace
+ * _levels / _items entries above, FP64 arithmetic):
+ * P2EFromSingleBox and E2PFromSingleBox with per-box levels, E2PFromCSR
+ * (List 3) and P2EFromCSR (List 4) over host-cut work items. The List-3
+ * items' targets take next_pow2(ntargets) lanes (lane groups of one lane
+ * and more); results and locals are added with atomics. */
+int sumpy_helmholtz_p2e_from_single_box_levels_f64(
+    int order, double k, int32_t nsrc_boxes, const int32_t *source_boxes, const int32_t *box_levels,
+    const double *level_rscales, const double *centers, int64_t center_stride,
+    const int32_t *box_source_starts, const int32_t *box_source_counts_nonchild,
+    const double *sources, int64_t source_stride, const double *strength, double *expansions,
+    void *stream);
+
+int sumpy_helmholtz_e2p_from_single_box_levels_f64(
+    int order, double k, int32_t ntgt_boxes, const int32_t *target_boxes, const int32_t *box_levels,
+    const double *level_rscales, const double *centers, int64_t center_stride,
+    const double *src_expansions, const int32_t *box_target_starts,
+    const int32_t *box_target_counts_nonchild, const double *targets, int64_t target_stride,
+    double scale, double *result, void *stream);
+
+int sumpy_helmholtz_e2p_from_items_f64(
+    int order, double k, int32_t nitems, const int32_t *items, const double *level_rscales,
+    const int32_t *source_box_lists, const double *centers, int64_t center_stride,
+    const double *src_expansions, const double *targets, int64_t target_stride, double scale,
+    double *result, void *stream);
+
+int sumpy_helmholtz_p2e_from_items_f64(
+    int order, double k, int32_t nitems, const int32_t *items, const double *level_rscales,
+    const int32_t *source_index, const double *centers, int64_t center_stride,
+    const double *sources, int64_t source_stride, const double *strength,
+    double *tgt_expansions, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -63,6 +63,14 @@ SIGNATURES = {
     "sumpy_e2p_from_single_box_packed_f64": [cint, i32, ptr, ptr, ptr, ptr, i64, ptr, ptr,
                                              i64, dbl, ptr, ptr],
     "sumpy_mpoles_to_f32": [cint, i64, ptr, ptr, ptr],
+    "sumpy_helmholtz_p2e_from_single_box_levels_f64": [cint, dbl, i32, ptr, ptr, ptr, ptr, i64,
+                                                       ptr, ptr, ptr, i64, ptr, ptr, ptr],
+    "sumpy_helmholtz_e2p_from_single_box_levels_f64": [cint, dbl, i32, ptr, ptr, ptr, ptr, i64,
+                                                       ptr, ptr, ptr, ptr, i64, dbl, ptr, ptr],
+    "sumpy_helmholtz_e2p_from_items_f64": [cint, dbl, i32, ptr, ptr, ptr, ptr, i64, ptr, ptr,
+                                           i64, dbl, ptr, ptr],
+    "sumpy_helmholtz_p2e_from_items_f64": [cint, dbl, i32, ptr, ptr, ptr, ptr, i64, ptr, i64,
+                                           ptr, ptr, ptr],
     "sumpy_e2p_from_items_mixed": [cint, i32, ptr, ptr, ptr, ptr, i64, ptr, ptr, i64, dbl,
                                    ptr, ptr],
     "sumpy_p2e_from_items_mixed": [cint, i32, ptr, ptr, ptr, ptr, i64, ptr, i64, ptr, ptr,

@@ -30,56 +30,11 @@
 #include <utility>
 
 #include "common.cuh"
+#include "helmholtz_core.cuh"
 #include "taylor.cuh"
 
 namespace sumpy {
 namespace {
-
-using z2 = double2;
-
-__device__ __forceinline__ z2 zmk(double a, double b) { return make_double2(a, b); }
-__device__ __forceinline__ z2 zadd(z2 a, z2 b) { return zmk(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ z2 zscal(double s, z2 a) { return zmk(s * a.x, s * a.y); }
-__device__ __forceinline__ z2 zmul(z2 a, z2 b)
-{
-    return zmk(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
-}
-// acc + s * a (s real)
-__device__ __forceinline__ z2 zaxpy(double s, z2 a, z2 acc)
-{
-    return zmk(fma(s, a.x, acc.x), fma(s, a.y, acc.y));
-}
-// acc + a * b
-__device__ __forceinline__ z2 zfma(z2 a, z2 b, z2 acc)
-{
-    return zmk(fma(a.x, b.x, fma(-a.y, b.y, acc.x)), fma(a.x, b.y, fma(a.y, b.x, acc.y)));
-}
-
-// C[m][q] of the closed form above; m is one axis of a stored multi-index,
-// so m <= SUMPY_MAX_ORDER.
-constexpr int CM = SUMPY_MAX_ORDER + 1;
-struct FaaTable {
-    double v[CM][CM];
-};
-constexpr FaaTable make_faa_table()
-{
-    FaaTable t{};
-    double f[CM] = {};
-    f[0] = 1.0;
-    for (int i = 1; i < CM; ++i) f[i] = f[i - 1] * i;
-    for (int m = 0; m < CM; ++m)
-        for (int q = 0; q < CM; ++q) {
-            const int a = 2 * q - m, b = m - q;
-            double v = 0.0;
-            if (a >= 0 && b >= 0) {
-                double p2 = 1.0;
-                for (int i = 0; i < b; ++i) p2 *= 2.0;
-                v = f[m] / (f[a] * f[b] * p2);
-            }
-            t.v[m][q] = v;
-        }
-    return t;
-}
 
 // {{{ P2P
 
@@ -277,7 +232,9 @@ __global__ void __launch_bounds__(HP2M_THREADS)
 hp2m_kernel(int p, double rscale, double kappa, const int32_t *__restrict__ boxes,
             const double *__restrict__ centers, int64_t cstride, const int32_t *__restrict__ bss,
             const int32_t *__restrict__ bsc, const double *__restrict__ sources, int64_t sstride,
-            const z2 *__restrict__ q, int32_t base, z2 *__restrict__ out)
+            const z2 *__restrict__ q, int32_t base, z2 *__restrict__ out,
+            const int32_t *__restrict__ box_level = nullptr,
+            const double *__restrict__ level_rscale = nullptr, double k = 0.0)
 {
     extern __shared__ __align__(16) double sm[];
     const int P1 = p + 1;
@@ -289,6 +246,10 @@ hp2m_kernel(int p, double rscale, double kappa, const int32_t *__restrict__ boxe
     const double c[3] = {centers[b], centers[cstride + b], centers[2 * cstride + b]};
     const int32_t s0 = bss[b], ns = bsc[b];
     const int nfull = nfull_of(p);
+    if (level_rscale) {   // all levels in one launch: the box's own level
+        rscale = level_rscale[box_level[blockIdx.x]];
+        kappa = k * k * rscale * rscale;
+    }
     const double rinv = 1.0 / rscale;
 
     for (int t = threadIdx.x; t < P1 * P1 * P1; t += blockDim.x) cube[t] = zmk(0.0, 0.0);
@@ -567,13 +528,18 @@ hl2p_kernel(int p, double rscale, double kappa, int32_t nboxes, const int32_t *_
             const double *__restrict__ centers, int64_t cstride, int32_t sbase,
             const z2 *__restrict__ src, const int32_t *__restrict__ bts,
             const int32_t *__restrict__ btc, const double *__restrict__ targets, int64_t tstride,
-            double scale, z2 *__restrict__ result)
+            double scale, z2 *__restrict__ result, const int32_t *__restrict__ box_level = nullptr,
+            const double *__restrict__ level_rscale = nullptr, double k = 0.0)
 {
     extern __shared__ __align__(16) double sm[];
     const int P1 = p + 1, C = P1 * P1 * P1;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ib = blockIdx.x * HL2P_WARPS + warp;
     if (ib >= nboxes) return;
+    if (level_rscale) {   // all levels in one launch: the box's own level
+        rscale = level_rscale[box_level[ib]];
+        kappa = k * k * rscale * rscale;
+    }
     z2 *cube = reinterpret_cast<z2 *>(sm) + warp * C;
     double *inv = reinterpret_cast<double *>(reinterpret_cast<z2 *>(sm) + HL2P_WARPS * C) +
                   warp * (P1 + 1);
@@ -617,172 +583,6 @@ hl2p_kernel(int p, double rscale, double kappa, int32_t nboxes, const int32_t *_
 // }}}
 
 // {{{ M2P / P2L (derivatives from the closed form, in registers)
-
-// stored index s -> (degree, i, j): s = d^2 + i (d + 1) + j
-__host__ __device__ constexpr int stored_deg(int s)
-{
-    int d = 0;
-    while ((d + 1) * (d + 1) <= s) ++d;
-    return d;
-}
-__host__ __device__ constexpr int stored_i(int s) { return s - stored_deg(s) * stored_deg(s) <= stored_deg(s) ? 0 : 1; }
-__host__ __device__ constexpr int stored_j(int s)
-{
-    return s - stored_deg(s) * stored_deg(s) - stored_i(s) * (stored_deg(s) + 1);
-}
-
-// Scaled form used by the kernels below: with v = x / rs and
-// gt_Q = rs^(2Q) g_Q (= rho^(2Q) gamma_Q),
-//     D(i, j, l) = sum_{q1, q2} C[j][q1] C[l][q2] v1^(2q1-j) v2^(2q2-l) v0^i gt_{q1+q2+i},
-//     gt_0 = e^{ikr}/r, gt_1 = u (ikr - 1) gt_0,
-//     gt_Q = -(2Q - 1) u gt_{Q-1} - (k rs)^2 u gt_{Q-2},  u = (rs/r)^2,
-// so the live state per evaluation point is v and gt_0..P.
-template <int P>
-struct HelmTables {
-    double v0, v1, v2, v1s, v2s;   // v, v1^2, v2^2
-    double gr[P + 1], gi[P + 1];
-};
-
-// a * b that the compiler may neither merge with an identical product of
-// another term nor move: keeps the per-axis factors out of the live
-// register set (merged across all terms they would stay live and spill).
-__device__ __forceinline__ double opaque_mul(double a, double b)
-{
-    double r;
-    asm volatile("mul.rn.f64 %0, %1, %2;" : "=d"(r) : "d"(a), "d"(b));
-    return r;
-}
-
-// The coefficients as compile-time constants (immediates in the code, which
-// the compiler rematerialises instead of keeping loaded values live).
-constexpr FaaTable kFaa = make_faa_table();
-
-// one (q1, q2) product of a term: tr/ti += C[L][Q2] v2^(2 Q2 - L) gt_{Q1+Q2+I}
-template <int P, int I, int L, int Q1, int Q2>
-__device__ __forceinline__ void helm_q2(const HelmTables<P> &t, double &tr, double &ti, double &p2)
-{
-    constexpr double c = kFaa.v[L][Q2];
-    const double a2 = c * p2;
-    tr = fma(a2, t.gr[Q1 + Q2 + I], tr);
-    ti = fma(a2, t.gi[Q1 + Q2 + I], ti);
-    if constexpr (Q2 < L) p2 = opaque_mul(p2, t.v2s);
-}
-
-// the q1 = Q1 slice of a term: sr/si += C[J][Q1] v1^(2 Q1 - J) sum_q2 (...)
-template <int P, int I, int J, int L, int Q1, int... K2>
-__device__ __forceinline__ void helm_q1(const HelmTables<P> &t, double &sr, double &si, double &p1,
-                                        std::integer_sequence<int, K2...>)
-{
-    double tr = 0.0, ti = 0.0;
-    double p2 = opaque_mul((L & 1) ? t.v2 : 1.0, 1.0);
-    (helm_q2<P, I, L, Q1, (L + 1) / 2 + K2>(t, tr, ti, p2), ...);
-    constexpr double c = kFaa.v[J][Q1];
-    const double a1 = c * p1;
-    sr = fma(a1, tr, sr);
-    si = fma(a1, ti, si);
-    if constexpr (Q1 < J) p1 = opaque_mul(p1, t.v1s);
-}
-
-template <int P, int I, int J, int L, int... K1>
-__device__ __forceinline__ z2 helm_term_impl(const HelmTables<P> &t,
-                                             std::integer_sequence<int, K1...>)
-{
-    double sr = 0.0, si = 0.0;
-    // running power v1^(2 q1 - J) (and v2^(2 q2 - L) in helm_q1), produced
-    // by opaque products so that no power is shared across terms
-    double p1 = opaque_mul((J & 1) ? t.v1 : 1.0, 1.0);
-    (helm_q1<P, I, J, L, (J + 1) / 2 + K1>(t, sr, si, p1,
-                                            std::make_integer_sequence<int, L / 2 + 1>{}),
-     ...);
-    return I ? zmk(t.v0 * sr, t.v0 * si) : zmk(sr, si);
-}
-
-// D of the stored coefficient S (compile-time), from the tables
-template <int P, int S>
-__device__ __forceinline__ z2 helm_term(const HelmTables<P> &t)
-{
-    constexpr int d = stored_deg(S), i = stored_i(S), j = stored_j(S), l = d - i - j;
-    return helm_term_impl<P, i, j, l>(t, std::make_integer_sequence<int, j / 2 + 1>{});
-}
-
-// the terms of one degree D (stored indices D^2 .. (D+1)^2 - 1)
-template <int P, int S, typename F>
-__device__ __forceinline__ void helm_step(const HelmTables<P> &t, F &f)
-{
-    f(std::integral_constant<int, S>{}, helm_term<P, S>(t));
-    // ordered after the term's own volatile products: the next term starts
-    // only once this one has been consumed (f fences its registers too)
-    asm volatile("" ::: "memory");
-}
-
-template <int P, int D, typename F, int... R>
-__device__ __forceinline__ void helm_degree(const HelmTables<P> &t, F &f,
-                                            std::integer_sequence<int, R...>)
-{
-    (helm_step<P, D * D + R>(t, f), ...);
-}
-
-// run degree d (a runtime value) with the degree-D code: each degree is its
-// own block, so the scheduler never interleaves more than one degree's
-// 2D + 1 terms (all (P+1)^2 at once would not fit in registers)
-template <int P, typename F, int... D>
-__device__ __forceinline__ void helm_dispatch(int d, const HelmTables<P> &t, F &f,
-                                              std::integer_sequence<int, D...>)
-{
-    ((d == D ? helm_degree<P, D>(t, f, std::make_integer_sequence<int, 2 * D + 1>{})
-             : void()),
-     ...);
-}
-
-// D(mi) = rs^|mi| d^mi (e^{ikr}/r) at x for every stored mi of order <= P,
-// in stored order s = 0, 1, ..., (P+1)^2 - 1: f(std::integral_constant<int, s>, D).
-template <int P, typename F>
-__device__ __forceinline__ void helm_layers(double x0, double x1, double x2, double rs, double k,
-                                            F &&f)
-{
-    HelmTables<P> t;
-    const double r2 = x0 * x0 + x1 * x1 + x2 * x2;
-    const double ri = rsqrt(r2);
-    const double r = r2 * ri;
-    const double rsi = 1.0 / rs;
-    t.v0 = x0 * rsi;
-    t.v1 = x1 * rsi;
-    t.v2 = x2 * rsi;
-    t.v1s = t.v1 * t.v1;
-    t.v2s = t.v2 * t.v2;
-    const double u = rs * rs * ri * ri;
-    double sn, cs;
-    sincos(k * r, &sn, &cs);
-    t.gr[0] = cs * ri;
-    t.gi[0] = sn * ri;
-    if constexpr (P >= 1) {
-        const double kr = k * r;
-        t.gr[1] = u * (-t.gr[0] - kr * t.gi[0]);
-        t.gi[1] = u * (-t.gi[0] + kr * t.gr[0]);
-        const double ku = (k * rs) * (k * rs) * u;
-#pragma unroll
-        for (int q = 2; q <= P; ++q) {
-            t.gr[q] = -(2.0 * q - 1.0) * u * t.gr[q - 1] - ku * t.gr[q - 2];
-            t.gi[q] = -(2.0 * q - 1.0) * u * t.gi[q - 1] - ku * t.gi[q - 2];
-        }
-    }
-#pragma unroll 1
-    for (int d = 0; d <= P; ++d)
-        helm_dispatch<P>(d, t, f, std::make_integer_sequence<int, P + 1>{});
-}
-
-// read-only 16-byte load of p[S], kept in program order and addressed with
-// an immediate offset (plain loads of the multipole would be hoisted above
-// all terms, with one live address each)
-template <int S>
-__device__ __forceinline__ z2 ordered_load(const z2 *p)
-{
-    z2 v;
-    asm volatile("ld.global.nc.v2.f64 {%0, %1}, [%2+%3];"
-                 : "=d"(v.x), "=d"(v.y)
-                 : "l"(p), "n"(S * 16));
-    return v;
-}
 
 constexpr int HM2P_WARPS = 4;
 
@@ -1140,6 +940,56 @@ int sumpy_helmholtz_e2p_from_single_box_f64(int order, double rscale, double k,
         order, rscale, k * k * rscale * rscale, ntgt_boxes, target_boxes, centers, center_stride,
         src_base_ibox, cz(src_expansions), box_target_starts, box_target_counts_nonchild, targets,
         target_stride, scale, mz(result));
+    return check_launch("hl2p_kernel");
+}
+
+int sumpy_helmholtz_p2e_from_single_box_levels_f64(
+    int order, double k, int32_t nsrc_boxes, const int32_t *source_boxes, const int32_t *box_levels,
+    const double *level_rscales, const double *centers, int64_t center_stride,
+    const int32_t *box_source_starts, const int32_t *box_source_counts_nonchild,
+    const double *sources, int64_t source_stride, const double *strength, double *expansions,
+    void *stream)
+{
+    if (!order_ok(order)) { set_last_error("helmholtz p2m levels: unsupported order"); return SUMPY_EUNSUPPORTED; }
+    if (nsrc_boxes < 0) return bad_arg("helmholtz p2m levels: nsrc_boxes < 0");
+    if (nsrc_boxes == 0) return SUMPY_OK;
+    if (!source_boxes || !box_levels || !level_rscales || !centers || !box_source_starts ||
+        !box_source_counts_nonchild || !sources || !strength || !expansions)
+        return bad_arg("helmholtz p2m levels: null pointer argument");
+    const int P1 = order + 1;
+    const size_t smem = sizeof(z2) * P1 * P1 * P1 + sizeof(double) * HP2M_CHUNK * 3 * P1 +
+                        sizeof(z2) * HP2M_CHUNK;
+    int rc = prepare_smem(hp2m_kernel, smem);
+    if (rc) return rc;
+    hp2m_kernel<<<nsrc_boxes, HP2M_THREADS, smem, as_stream(stream)>>>(
+        order, 1.0, 0.0, source_boxes, centers, center_stride, box_source_starts,
+        box_source_counts_nonchild, sources, source_stride, cz(strength), 0, mz(expansions),
+        box_levels, level_rscales, k);
+    return check_launch("hp2m_kernel");
+}
+
+int sumpy_helmholtz_e2p_from_single_box_levels_f64(
+    int order, double k, int32_t ntgt_boxes, const int32_t *target_boxes, const int32_t *box_levels,
+    const double *level_rscales, const double *centers, int64_t center_stride,
+    const double *src_expansions, const int32_t *box_target_starts,
+    const int32_t *box_target_counts_nonchild, const double *targets, int64_t target_stride,
+    double scale, double *result, void *stream)
+{
+    if (!order_ok(order)) { set_last_error("helmholtz l2p levels: unsupported order"); return SUMPY_EUNSUPPORTED; }
+    if (ntgt_boxes < 0) return bad_arg("helmholtz l2p levels: ntgt_boxes < 0");
+    if (ntgt_boxes == 0) return SUMPY_OK;
+    if (!target_boxes || !box_levels || !level_rscales || !centers || !src_expansions ||
+        !box_target_starts || !box_target_counts_nonchild || !targets || !result)
+        return bad_arg("helmholtz l2p levels: null pointer argument");
+    const int P1 = order + 1;
+    const size_t smem = (sizeof(z2) * P1 * P1 * P1 + sizeof(double) * (P1 + 1)) * HL2P_WARPS;
+    int rc = prepare_smem(hl2p_kernel, smem);
+    if (rc) return rc;
+    const unsigned blocks = (unsigned)((ntgt_boxes + HL2P_WARPS - 1) / HL2P_WARPS);
+    hl2p_kernel<<<blocks, 32 * HL2P_WARPS, smem, as_stream(stream)>>>(
+        order, 1.0, 0.0, ntgt_boxes, target_boxes, centers, center_stride, 0, cz(src_expansions),
+        box_target_starts, box_target_counts_nonchild, targets, target_stride, scale, mz(result),
+        box_levels, level_rscales, k);
     return check_launch("hl2p_kernel");
 }
 

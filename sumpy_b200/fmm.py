@@ -467,7 +467,8 @@ class SumpyExpansionWrangler:
             boxes, levs = self._cached_items(
                 "p2m_boxes", (level_start_source_box_nrs, source_boxes), build)
             if boxes.numel():
-                call("sumpy_p2e_from_single_box_levels_f64", _c(self.level_orders[0]),
+                call(self._entry("sumpy_p2e_from_single_box_levels_f64"),
+                     _c(self.level_orders[0]), *self._kargs,
                      _i32(boxes.numel()), dptr(boxes), dptr(levs), dptr(self._level_rscales),
                      dptr(g["centers"]), _i64(self.tree.nboxes), dptr(g["bss"]), dptr(g["bsc"]),
                      dptr(g["sources"]), _i64(self.tree.nsources), dptr(w), dptr(mpoles), st)
@@ -1036,14 +1037,14 @@ class SumpyExpansionWrangler:
 
     @property
     def _merged_levels(self):
-        return (self.merge_levels and not self.helmholtz and not self.gradient
-                and len(set(self.level_orders)) == 1)
+        return (self.merge_levels and not self.gradient and len(set(self.level_orders)) == 1)
 
     @property
     def _items_path(self):
-        """Mixed Laplace List 3 / List 4 through the one-launch item kernels
-        (needs one order on every level: flat [nboxes][ncoeff] storage)."""
-        return (self.item_kernels and self.precision == "mixed" and not self.helmholtz
+        """List 3 / List 4 through the one-launch item kernels (Laplace:
+        mixed form; Helmholtz: both forms, FP64 arithmetic); needs one order
+        on every level (flat [nboxes][ncoeff] storage)."""
+        return (self.item_kernels and (self.precision == "mixed" or self.helmholtz)
                 and not self.gradient and len(set(self.level_orders)) == 1)
 
     @cached_property
@@ -1064,7 +1065,8 @@ class SumpyExpansionWrangler:
                                mpole_exps, pot):
         def build():
             items, lists = m2p_items(self.tree, target_boxes_by_source_level,
-                                     source_boxes_by_level)
+                                     source_boxes_by_level,
+                                     groups=32 if self.helmholtz else M2P_ITEM_GROUPS)
             return (torch.as_tensor(items).to(self.device),
                     torch.as_tensor(lists).to(self.device))
         items, lists = self._cached_items(
@@ -1074,6 +1076,12 @@ class SumpyExpansionWrangler:
         order = self.level_orders[0]
         g = self._geom
         st = stream_ptr()
+        if self.helmholtz:
+            call("sumpy_helmholtz_e2p_from_items_f64", _c(order), _d(self.k),
+                 _i32(items.shape[0]), dptr(items), dptr(self._level_rscales), dptr(lists),
+                 dptr(g["centers"]), _i64(self.tree.nboxes), dptr(mpole_exps),
+                 dptr(g["targets"]), _i64(self.tree.ntargets), _d(self._scale), dptr(pot[0]), st)
+            return pot
         mp32 = torch.empty(self.tree.nboxes * _npad(order), dtype=torch.float32,
                            device=self.device)
         call("sumpy_mpoles_to_f32", _c(order), _i64(self.tree.nboxes), dptr(mpole_exps),
@@ -1128,7 +1136,9 @@ class SumpyExpansionWrangler:
             if items.shape[0]:
                 g = self._geom
                 w = self._weights(src_weight_vecs)
-                call("sumpy_p2e_from_items_mixed", _c(self.level_orders[0]),
+                name = ("sumpy_helmholtz_p2e_from_items_f64" if self.helmholtz
+                        else "sumpy_p2e_from_items_mixed")
+                call(name, _c(self.level_orders[0]), *self._kargs,
                      _i32(items.shape[0]), dptr(items), dptr(self._level_rscales), dptr(sidx),
                      dptr(g["centers"]), _i64(self.tree.nboxes), dptr(g["sources"]),
                      _i64(self.tree.nsources), dptr(w), dptr(local_exps), stream_ptr())
@@ -1185,6 +1195,23 @@ class SumpyExpansionWrangler:
         pot = self.output_zeros(actx)
         g = self._geom
         st = stream_ptr()
+        if self._merged_levels and self.helmholtz and not isinstance(target_boxes, torch.Tensor):
+            def build_h():
+                tb = np.asarray(target_boxes, dtype=np.int64)
+                lev = _box_levels(level_start_target_box_nrs, len(tb))
+                order = np.argsort(-np.asarray(self.tree.box_target_counts_nonchild)[tb],
+                                   kind="stable")
+                return (torch.as_tensor(tb[order].astype(np.int32)).to(self.device),
+                        torch.as_tensor(lev[order].astype(np.int32)).to(self.device))
+            boxes, levs = self._cached_items(
+                "hl2p_boxes", (level_start_target_box_nrs, target_boxes), build_h)
+            if boxes.numel():
+                call("sumpy_helmholtz_e2p_from_single_box_levels_f64", _c(self.level_orders[0]),
+                     _d(self.k), _i32(boxes.numel()), dptr(boxes), dptr(levs),
+                     dptr(self._level_rscales), dptr(g["centers"]), _i64(self.tree.nboxes),
+                     dptr(local_exps), dptr(g["bts"]), dptr(g["btc"]), dptr(g["targets"]),
+                     _i64(self.tree.ntargets), _d(self._scale), dptr(pot[0]), st)
+            return pot
         if self._merged_levels and not isinstance(target_boxes, torch.Tensor):
             def build():
                 items, slots = l2p_items(self.tree, level_start_target_box_nrs, target_boxes)

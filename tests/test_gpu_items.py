@@ -138,3 +138,40 @@ def test_fp64_gemm_m2m_l2l_match_shift_kernels(cuda_device, order):
         outs.append((m.cpu().numpy(), loc.cpu().numpy()))
     assert relerr(outs[0][0], outs[1][0]) < 1e-13
     assert relerr(outs[0][1], outs[1][1]) < 1e-13
+
+
+@pytest.mark.parametrize("order", [3, 14])
+def test_helmholtz_one_launch_stages_match_per_level(cuda_device, order):
+    """Helmholtz P2M / L2P of all levels in one launch and List 3 / List 4
+    over work items against the per-level launches (FP64, same per-pair
+    arithmetic; sums in a different order)."""
+    from sumpy_b200 import HelmholtzKernel
+    src = sphere_plummer(12000, 31)
+    tree, trav, tcls = build_all(src, None, 24)
+    rng = np.random.default_rng(6)
+    q = torch.as_tensor(rng.standard_normal(src.shape[1]) + 1j * rng.standard_normal(src.shape[1]),
+                        device="cuda")
+    knl = HelmholtzKernel(3)
+    ti = SumpyTreeIndependentDataForWrangler(
+        None, lambda o, **kw: MExp(knl, o), lambda o, **kw: LExp(knl, o), [knl],
+        exclude_self=True)
+    outs = []
+    for new in (False, True):
+        w = SumpyExpansionWrangler(ti, trav, np.complex128, lambda *a: order,
+                                   kernel_extra_kwargs={"k": 10.0},
+                                   translation_classes_data=tcls)
+        w.item_kernels = w.merge_levels = new
+        qs = w.reorder_sources(q)
+        mp = w.form_multipoles(None, trav.level_start_source_box_nrs, trav.source_boxes, [qs])
+        mp2 = w.coarsen_multipoles(None, trav.level_start_source_parent_box_nrs,
+                                   trav.source_parent_boxes, mp.clone())
+        pm = w.eval_multipoles(None, trav.target_boxes_sep_smaller_by_source_level,
+                               trav.from_sep_smaller_by_level, mp2)[0]
+        pl = w.form_locals(None, trav.level_start_target_or_target_parent_box_nrs,
+                           trav.target_or_target_parent_boxes, trav.from_sep_bigger_starts,
+                           trav.from_sep_bigger_lists, [qs])
+        pe = w.eval_locals(None, trav.level_start_target_box_nrs, trav.target_boxes, pl)[0]
+        outs.append([t.cpu().numpy() for t in (mp, pm, pl, pe)])
+    for a, b in zip(outs[1], outs[0]):
+        assert np.abs(b).max() > 0
+        assert relerr(a, b) < 1e-12
