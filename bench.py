@@ -884,7 +884,7 @@ def stage_breakdown(w, trav, q_dev, dev, roofline=True, pipe_peaks=None):
                          "includes the TF32 split pre-pass")
         # dram__bytes_read.sum + dram__bytes_write.sum of this launch on the 1M-point
         # workload, one ncu capture per leaf size (profiles/m2l_tf32x3_sphere_plummer_1M_p10.md)
-        captured = {32: 1.227e9 + 0.195e9, 96: 247.1e6 + 37.3e6}
+        captured = {32: 1.227e9 + 0.195e9, 96: 256.6e6 + 38.4e6}
         if mixed and tree.nsources == NPOINTS and n == (ORDER + 1) ** 2 and \
                 MAX_PARTICLES in captured and \
                 int(tree.box_source_counts_nonchild.max()) <= MAX_PARTICLES:

@@ -246,6 +246,31 @@ int sumpy_m2l_translation_classes_tf32x3(
     const float *src_lo, int32_t tgt_base_ibox, double *tgt_expansions, int32_t *status,
     void *stream);
 
+/* The grouped class GEMMs above for any row count n (real values per
+ * expansion: ncoeff, or 2 ncoeff for the real embedding of complex data)
+ * with K split over k_split CTAs per work item (partial products meet in
+ * the FP64 atomic epilogue). Used for the per-level M2M / L2L octant maps
+ * (E2EFromChildren / E2EFromParent, sumpy/fmm.py:576-598, 692-712), whose
+ * small coarse levels would otherwise leave most SMs idle on the
+ * level-serial chain. k_split in [1, ceil(n / 8)] (FP64) or
+ * [1, k_pad / 32] (tf32x3); other arguments as for the entries above. */
+int sumpy_class_gemm_f64(
+    int32_t n, int32_t k_split, int32_t nitems, const int32_t *item_tile,
+    const int32_t *item_group_begin, const int32_t *item_group_end, int32_t tile_width,
+    const int32_t *tile_targets, const double *tile_scale, const int32_t *group_class,
+    const int32_t *group_sources, int32_t nclasses, const double *class_matrices,
+    int32_t src_base_ibox, const double *src_expansions, int32_t tgt_base_ibox,
+    double *tgt_expansions, void *stream);
+
+int sumpy_class_gemm_tf32x3(
+    int32_t n, int32_t k_split, int32_t nitems, const int32_t *item_tile,
+    const int32_t *item_group_begin, const int32_t *item_group_end, int32_t tile_width,
+    const int32_t *tile_targets, const double *tile_scale, const int32_t *group_class,
+    const int32_t *group_sources, int32_t nclasses, const float *mats_hi, const float *mats_lo,
+    int32_t rows_pad, int32_t k_pad, int32_t src_nrows, int32_t src_base_ibox,
+    const float *src_hi, const float *src_lo, int32_t tgt_base_ibox, double *tgt_expansions,
+    int32_t *status, void *stream);
+
 /* Same M2L as sumpy_m2l_translation_classes_tf32x3, for callers that cannot
  * allocate device memory while they run (a host application with a fixed
  * device-memory budget, an allocation-free real-time loop, code where an

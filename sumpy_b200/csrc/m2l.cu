@@ -80,8 +80,12 @@ m2l_f64_kernel(int n, const int32_t *__restrict__ item_tile, const int32_t *__re
     const int row0 = blockIdx.y * ROWS;
     const int tid = threadIdx.x;
     const int tx = tid % 8, ty = tid / 8;
-    const int nkc = (n + KC - 1) / KC;
+    // split K: CTA z of gridDim.z takes k-chunks [kcb, kce) (all when 1)
+    const int nkc_all = (n + KC - 1) / KC;
+    const int kcb = (int)((int64_t)blockIdx.z * nkc_all / gridDim.z);
+    const int nkc = (int)((int64_t)(blockIdx.z + 1) * nkc_all / gridDim.z) - kcb;
     const int total = (g1 - g0) * nkc;
+    if (total <= 0) return;
 
     double acc[8][8];
 #pragma unroll
@@ -109,7 +113,8 @@ m2l_f64_kernel(int n, const int32_t *__restrict__ item_tile, const int32_t *__re
         Chunk<ROWS> ch;
         load_srcs(g0, 0);
         __syncthreads();
-        fetch<ROWS>(ch, mats + (int64_t)group_class[g0] * n * n, src, srcs[0], n, row0, 0, sbase);
+        fetch<ROWS>(ch, mats + (int64_t)group_class[g0] * n * n, src, srcs[0], n, row0,
+                    kcb * KC, sbase);
         store(ch, 0);
         __syncthreads();
         for (int it = 0; it < total; ++it) {
@@ -123,7 +128,7 @@ m2l_f64_kernel(int n, const int32_t *__restrict__ item_tile, const int32_t *__re
                     __syncthreads();
                 }
                 fetch<ROWS>(ch, mats + (int64_t)group_class[g] * n * n, src, srcs[sb], n, row0,
-                            kc * KC, sbase);
+                            (kcb + kc) * KC, sbase);
             }
 #pragma unroll 4
             for (int kk = 0; kk < KC; ++kk) {
@@ -167,9 +172,12 @@ static int m2l_f64_launch(
     const int32_t *item_group_end, int32_t tile_width, const int32_t *tile_targets,
     const double *tile_scale, const int32_t *group_class, const int32_t *group_sources,
     int32_t nclasses, const double *class_matrices, int32_t src_base_ibox,
-    const double *src_expansions, int32_t tgt_base_ibox, double *tgt_expansions, void *stream)
+    const double *src_expansions, int32_t tgt_base_ibox, double *tgt_expansions, void *stream,
+    int32_t k_split = 1)
 {
     if (tile_width != TW) return bad_arg("m2l: tile_width must be 64");
+    if (n < 1 || k_split < 1 || k_split > (n + KC - 1) / KC)
+        return bad_arg("m2l: k_split must be in [1, number of 8-wide k-chunks]");
     if (nitems < 0 || nclasses < 0) return bad_arg("m2l: negative size");
     if (nitems == 0) return SUMPY_OK;
     if (!item_tile || !item_group_begin || !item_group_end || !tile_targets || !tile_scale ||
@@ -177,13 +185,13 @@ static int m2l_f64_launch(
         return bad_arg("m2l: null pointer argument");
     cudaStream_t st = as_stream(stream);
     if (n <= 64) {
-        dim3 grid(nitems, 1);
+        dim3 grid(nitems, 1, k_split);
         m2l_f64_kernel<64><<<grid, 64, 0, st>>>(n, item_tile, item_group_begin, item_group_end,
                                                 tile_targets, tile_scale, group_class,
                                                 group_sources, class_matrices, src_base_ibox,
                                                 src_expansions, tgt_base_ibox, tgt_expansions);
     } else {
-        dim3 grid(nitems, (n + 127) / 128);
+        dim3 grid(nitems, (n + 127) / 128, k_split);
         m2l_f64_kernel<128><<<grid, 128, 0, st>>>(n, item_tile, item_group_begin, item_group_end,
                                                   tile_targets, tile_scale, group_class,
                                                   group_sources, class_matrices, src_base_ibox,
@@ -226,6 +234,21 @@ int sumpy_helmholtz_m2l_translation_classes_f64(
                           item_group_end, tile_width, tile_targets, tile_scale, group_class,
                           group_sources, nclasses, class_matrices, src_base_ibox, src_expansions,
                           tgt_base_ibox, tgt_expansions, stream);
+}
+
+int sumpy_class_gemm_f64(
+    int32_t n, int32_t k_split, int32_t nitems, const int32_t *item_tile,
+    const int32_t *item_group_begin, const int32_t *item_group_end, int32_t tile_width,
+    const int32_t *tile_targets, const double *tile_scale, const int32_t *group_class,
+    const int32_t *group_sources, int32_t nclasses, const double *class_matrices,
+    int32_t src_base_ibox, const double *src_expansions, int32_t tgt_base_ibox,
+    double *tgt_expansions, void *stream)
+{
+    if (n < 1 || n > 2 * ncoeff_of(SUMPY_MAX_ORDER)) return bad_arg("class gemm: bad n");
+    return m2l_f64_launch(n, nitems, item_tile, item_group_begin, item_group_end, tile_width,
+                          tile_targets, tile_scale, group_class, group_sources, nclasses,
+                          class_matrices, src_base_ibox, src_expansions, tgt_base_ibox,
+                          tgt_expansions, stream, k_split);
 }
 
 }  // extern "C"

@@ -300,7 +300,11 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
     const int tile = a.item_tile[item];
     const int g0 = a.item_g0[item], g1 = a.item_g1[item];
     const int ng = g1 - g0;
-    const int nkc = a.k_pad / TC_KC;
+    // split K: CTA z of gridDim.z takes K chunks [kcb, kcb + nkc) of every
+    // group (the host keeps gridDim.z <= the number of chunks)
+    const int nkc_all = a.k_pad / TC_KC;
+    const int kcb = (int)((int64_t)blockIdx.z * nkc_all / gridDim.z);
+    const int nkc = (int)((int64_t)(blockIdx.z + 1) * nkc_all / gridDim.z) - kcb;
     const int total = ng * nkc;
 
     if (TC_GATHER && warp == 0) {
@@ -334,7 +338,7 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
             bool ok = true;
             if (use > 0) ok = mbar_wait_or_abort(empty_bar + 8 * s, (use - 1) & 1, abort_flag);
             if (__any_sync(FULL, !ok || *abort_flag)) break;
-            const int k0 = kc * TC_KC;
+            const int k0 = (kcb + kc) * TC_KC;
             const uint32_t st = base + s * STAGE;
             if (lane == 0) {
                 mbar_expect_tx(full_bar + 8 * s, 4 * PLANE);
@@ -388,7 +392,7 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
             bool ok = true;
             if (use > 0) ok = mbar_wait_or_abort(empty_bar + 8 * s, (use - 1) & 1, abort_flag);
             if (loaders_sync_or(!ok || *abort_flag)) break;
-            const int k0 = kc * TC_KC;
+            const int k0 = (kcb + kc) * TC_KC;
             const uint32_t st = base + s * STAGE;
             if (threadIdx.x == 0) {
                 mbar_expect_tx(full_bar + 8 * s, 2 * PLANE);
@@ -595,9 +599,12 @@ static int m2l_tf32x3_launch(
     const double *tile_scale, const int32_t *group_class, const int32_t *group_sources,
     int32_t nclasses, const float *mats_hi, const float *mats_lo, int32_t rows_pad, int32_t k_pad,
     int32_t src_nrows, int32_t src_base_ibox, const float *src_hi, const float *src_lo,
-    int32_t tgt_base_ibox, double *tgt_expansions, int32_t *status, void *stream)
+    int32_t tgt_base_ibox, double *tgt_expansions, int32_t *status, void *stream,
+    int32_t k_split = 1)
 {
     if (tile_width != TC_TW) return bad_arg("m2l_tf32x3: tile_width must be 128");
+    if (k_split < 1 || k_split > k_pad / TC_KC)
+        return bad_arg("m2l_tf32x3: k_split must be in [1, k_pad / 32]");
     if (rows_pad < n || rows_pad % TC_M) return bad_arg("m2l_tf32x3: rows_pad must be a multiple of 128 >= ncoeff");
     if (k_pad < n || k_pad % 32) return bad_arg("m2l_tf32x3: k_pad must be a multiple of 32 >= ncoeff");
     if (nitems < 0 || nclasses <= 0 || src_nrows < 1) return bad_arg("m2l_tf32x3: bad sizes");
@@ -637,7 +644,7 @@ static int m2l_tf32x3_launch(
     a.src_hi = src_hi; a.src_lo = src_lo;
     a.src_row_base = src_base_ibox; a.zero_row = src_nrows - 1;
     a.tbase = tgt_base_ibox; a.tgt = tgt_expansions; a.status = status;
-    dim3 grid(nitems, rows_pad / TC_M);
+    dim3 grid(nitems, rows_pad / TC_M, k_split);
     m2l_tf32x3_kernel<<<grid, TC_THREADS, TC_SMEM, as_stream(stream)>>>(a, ma_hi, ma_lo, mb_hi,
                                                                         mb_lo);
     return check_launch("m2l_tf32x3_kernel");
@@ -662,6 +669,22 @@ int sumpy_m2l_translation_classes_tf32x3(
                              group_sources, nclasses, mats_hi, mats_lo, rows_pad, k_pad,
                              src_nrows, src_base_ibox, src_hi, src_lo, tgt_base_ibox,
                              tgt_expansions, status, stream);
+}
+
+int sumpy_class_gemm_tf32x3(
+    int32_t n, int32_t k_split, int32_t nitems, const int32_t *item_tile,
+    const int32_t *item_group_begin, const int32_t *item_group_end, int32_t tile_width,
+    const int32_t *tile_targets, const double *tile_scale, const int32_t *group_class,
+    const int32_t *group_sources, int32_t nclasses, const float *mats_hi, const float *mats_lo,
+    int32_t rows_pad, int32_t k_pad, int32_t src_nrows, int32_t src_base_ibox,
+    const float *src_hi, const float *src_lo, int32_t tgt_base_ibox, double *tgt_expansions,
+    int32_t *status, void *stream)
+{
+    if (n < 1 || n > 2 * ncoeff_of(SUMPY_MAX_ORDER)) return bad_arg("class gemm tf32x3: bad n");
+    return m2l_tf32x3_launch(n, nitems, item_tile, item_group_begin, item_group_end, tile_width,
+                             tile_targets, tile_scale, group_class, group_sources, nclasses,
+                             mats_hi, mats_lo, rows_pad, k_pad, src_nrows, src_base_ibox, src_hi,
+                             src_lo, tgt_base_ibox, tgt_expansions, status, stream, k_split);
 }
 
 int sumpy_helmholtz_m2l_translation_classes_tf32x3(

@@ -950,16 +950,33 @@ class SumpyExpansionWrangler:
     def _octant_gemm(self, kind, plan, sview, sbase, tview, tbase, st, fp64=False,
                      parent_level=2):
         mats, hi, lo, rp, kp = self._octant_operator_planes(kind, parent_level)
+        n = mats.shape[1]   # real values per box
+
+        def k_split(row_tiles, nkc, cap):
+            # a level's octant GEMM is on the level-serial chain: few items
+            # also split K (partial sums meet in the FP64 atomic epilogue)
+            want = -(-2 * self._sm_count // max(1, plan["nitems"] * row_tiles))
+            return int(max(1, min(nkc, cap, want)))
+
         if fp64:
-            self._call_m2l_f64(self.level_orders[0], plan, mats, sbase, sview, tbase, tview,
-                               st)
+            ks = k_split(1 if n <= 64 else -(-n // 128), -(-n // 8), 8)
+            call("sumpy_class_gemm_f64", _i32(n), _i32(ks), _i32(plan["nitems"]),
+                 dptr(plan["item_tile"]), dptr(plan["item_g0"]), dptr(plan["item_g1"]),
+                 _i32(M2L_TILE), dptr(plan["tile_targets"]), dptr(plan["tile_scale"]),
+                 dptr(plan["group_class"]), dptr(plan["group_sources"]), _i32(mats.shape[0]),
+                 dptr(mats), _i32(sbase), dptr(sview), _i32(tbase), dptr(tview), st)
             return
-        nb, n = sview.shape[0], mats.shape[1]   # real values per box
+        nb = sview.shape[0]
         ws_hi, ws_lo = self._m2l_workspace(nb, kp)
         call("sumpy_split_tf32x2", _i64(nb), _i32(1), _i32(n), dptr(sview), _i32(1),
              _i32(kp), dptr(ws_hi), dptr(ws_lo), st)
-        self._call_m2l_tc(self.level_orders[0], plan, hi, lo, rp, kp, nb + 1, sbase,
-                          ws_hi, ws_lo, tbase, tview, st)
+        ks = k_split(rp // 128, kp // 32, 4)
+        call("sumpy_class_gemm_tf32x3", _i32(n), _i32(ks), _i32(plan["nitems"]),
+             dptr(plan["item_tile"]), dptr(plan["item_g0"]), dptr(plan["item_g1"]),
+             _i32(M2L_TILE_TC), dptr(plan["tile_targets"]), dptr(plan["tile_scale"]),
+             dptr(plan["group_class"]), dptr(plan["group_sources"]), _i32(plan["nclasses"]),
+             dptr(hi), dptr(lo), _i32(rp), _i32(kp), _i32(nb + 1), _i32(sbase),
+             dptr(ws_hi), dptr(ws_lo), _i32(tbase), dptr(tview), dptr(self._status), st)
 
     @property
     def _gemm_fp64_ok(self):
