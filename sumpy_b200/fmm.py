@@ -294,12 +294,13 @@ class SumpyExpansionWrangler:
         # drive_fmm runs List 1, 3 and 4 on a second stream (sumpy_b200.drive)
         self.concurrent_stages = True
         # one order on every level: M2M and L2L as eight dense maps per level
-        # applied as grouped GEMMs. Mixed form: M2M on the tensor cores
-        # (3xTF32), L2L as an FP64 GEMM (the 3xTF32 L2L compounds its FP32
-        # group sums down the levels: ~3x the mixed form's error on the
-        # 1M-point benchmark); FP64 form: both as FP64 GEMMs. Laplace only for
-        # the FP64 GEMMs; Helmholtz mixed uses the tensor-core M2M.
-        self.tc_m2m = True
+        # applied as grouped GEMMs. Laplace: both as FP64 GEMMs with K split
+        # over CTAs on small levels (on the 1M-point benchmark the FP64 M2M,
+        # 0.21 ms, beats the 3xTF32 tensor-core M2M, 0.29 ms, whose per-level
+        # TF32 split adds a launch to the level-serial chain; the 3xTF32 L2L
+        # also compounds its FP32 group sums down the levels: ~3x the mixed
+        # form's error). Helmholtz mixed: M2M on the tensor cores.
+        self.tc_m2m = self.helmholtz
         self.tc_l2l = False
         self.gemm_l2l = True
         self.gemm_m2m = True
@@ -492,7 +493,7 @@ class SumpyExpansionWrangler:
         if self._tc_translations and self.tc_m2m:
             return self._coarsen_tc(level_start_source_parent_box_nrs, source_parent_boxes,
                                     mpoles)
-        if self.gemm_m2m and self.precision == "fp64" and self._gemm_fp64_ok:
+        if self.gemm_m2m and self._gemm_fp64_ok:
             return self._coarsen_tc(level_start_source_parent_box_nrs, source_parent_boxes,
                                     mpoles, fp64=True)
         lsp = _np_i32(level_start_source_parent_box_nrs)

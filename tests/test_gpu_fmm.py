@@ -229,13 +229,14 @@ def test_mixed_fmm_matches_fp64_fmm(cuda_device):
 @pytest.mark.parametrize("geom", list(GEOMS))
 @pytest.mark.parametrize("order", [4, 10])
 def test_tensor_core_m2m_l2l_match_fp64(cuda_device, geom, order):
-    """Mixed form: M2M and L2L as per-octant 3xTF32 GEMMs against the FP64
-    shift kernels on the same inputs."""
+    """Mixed form with the tensor-core octant maps switched on: M2M and L2L
+    as per-octant 3xTF32 GEMMs against the FP64 form on the same inputs."""
     src, tgt, tree, trav, tcls, q = _setup(geom)
     excl = tgt is None
     w64 = make_wrangler(tree, trav, order, exclude_self=excl)
     wtc = make_wrangler(tree, trav, order, exclude_self=excl, precision="mixed")
     assert wtc._tc_translations
+    wtc.tc_m2m = wtc.tc_l2l = True
     qd = w64.reorder_sources(torch.as_tensor(q, device=cuda_device))
     mp = w64.form_multipoles(None, trav.level_start_source_box_nrs, trav.source_boxes, [qd])
     m64 = w64.coarsen_multipoles(None, trav.level_start_source_parent_box_nrs,
