@@ -405,6 +405,15 @@ int sumpy_e2p_from_single_box_packed_f64(
     const double *src_expansions, const double *targets, int64_t target_stride,
     double scale, double *result, void *stream);
 
+/* The same with the potential's target gradient (E2PFromSingleBox with
+ * gradient outputs): grad is [3][target_stride], assigned like result;
+ * result may be NULL. */
+int sumpy_e2p_from_single_box_packed_grad_f64(
+    int order, int32_t nitems, const int32_t *items, const int32_t *slots,
+    const double *level_rscales, const double *centers, int64_t center_stride,
+    const double *src_expansions, const double *targets, int64_t target_stride,
+    double scale, double *result, double *grad, void *stream);
+
 int sumpy_mpoles_to_f32(int order, int64_t nboxes, const double *src_expansions, float *dst,
                         void *stream);
 
@@ -413,6 +422,14 @@ int sumpy_e2p_from_items_mixed(
     const int32_t *source_box_lists, const double *centers, int64_t center_stride,
     const float *src_expansions_f32, const double *targets, int64_t target_stride,
     double scale, double *result, void *stream);
+
+/* The same with the potential's target gradient added into grad
+ * ([3][target_stride]); result may be NULL. */
+int sumpy_e2p_from_items_grad_mixed(
+    int order, int32_t nitems, const int32_t *items, const double *level_rscales,
+    const int32_t *source_box_lists, const double *centers, int64_t center_stride,
+    const float *src_expansions_f32, const double *targets, int64_t target_stride,
+    double scale, double *result, double *grad, void *stream);
 
 int sumpy_p2e_from_items_mixed(
     int order, int32_t nitems, const int32_t *items, const double *level_rscales,

@@ -63,6 +63,10 @@ SIGNATURES = {
     "sumpy_e2p_from_single_box_packed_f64": [cint, i32, ptr, ptr, ptr, ptr, i64, ptr, ptr,
                                              i64, dbl, ptr, ptr],
     "sumpy_mpoles_to_f32": [cint, i64, ptr, ptr, ptr],
+    "sumpy_e2p_from_items_grad_mixed": [cint, i32, ptr, ptr, ptr, ptr, i64, ptr, ptr, i64, dbl,
+                                        ptr, ptr, ptr],
+    "sumpy_e2p_from_single_box_packed_grad_f64": [cint, i32, ptr, ptr, ptr, ptr, i64, ptr, ptr,
+                                                  i64, dbl, ptr, ptr, ptr],
     "sumpy_class_gemm_f64": [i32, i32, i32, ptr, ptr, ptr, i32, ptr, ptr, ptr, ptr, i32, ptr,
                              i32, ptr, i32, ptr, ptr],
     "sumpy_class_gemm_tf32x3": [i32, i32, i32, ptr, ptr, ptr, i32, ptr, ptr, ptr, ptr, i32, ptr,

@@ -792,14 +792,16 @@ __host__ __device__ constexpr int l2pk_warps()
 // its own box read from shared memory (at p = 10 the eight slot bases,
 // 2288 bytes apart, fall on distinct banks).
 // item = {first slot, number of slots}; slot = {box, first target,
-// number of targets, level}; results are assigned.
-template <int P>
+// number of targets, level}; results are assigned. GRAD: also the three
+// target-coordinate derivatives, from the same x-runs shifted by one in i
+// (d/dx) or taken from the neighbouring (j + 1, k) / (j, k + 1) runs.
+template <int P, bool GRAD = false>
 __global__ void __launch_bounds__(32 * l2pk_warps<P>())
 l2p_packed_kernel(int32_t nitems, const int2 *__restrict__ items, const int4 *__restrict__ slots,
                   const double *__restrict__ level_rscale, const double *__restrict__ centers,
                   int64_t cstride, const double *__restrict__ loc,
                   const double *__restrict__ targets, int64_t tstride, double scale,
-                  double *__restrict__ result)
+                  double *__restrict__ result, double *__restrict__ grad = nullptr)
 {
     constexpr int P1 = P + 1;
     constexpr int N = P1 * P1;
@@ -874,7 +876,37 @@ l2p_packed_kernel(int32_t nitems, const int2 *__restrict__ items, const int4 *__
         }
         pot = fma(yp[j], pj, pot);
     }
-    result[t] = scale * pot;
+    if (result) result[t] = scale * pot;
+    if constexpr (GRAD) {
+        double gx = 0.0, gy = 0.0, gz = 0.0;
+#pragma unroll
+        for (int j = 0; j < P; ++j) {
+            double px = 0.0, py = 0.0, pz = 0.0;
+#pragma unroll
+            for (int k = 0; k < P - j; ++k) {
+                const double *r0 = c + jki_offset<P>(j, k);
+                const double *ry = c + jki_offset<P>(j + 1, k);
+                const double *rz = c + jki_offset<P>(j, k + 1);
+                double sx = 0.0, sy = 0.0, sz = 0.0;
+#pragma unroll
+                for (int i = P - 1 - j - k; i >= 0; --i) {
+                    sx = fma(r0[i + 1], xp[i], sx);
+                    sy = fma(ry[i], xp[i], sy);
+                    sz = fma(rz[i], xp[i], sz);
+                }
+                px = fma(zp[k], sx, px);
+                py = fma(zp[k], sy, py);
+                pz = fma(zp[k], sz, pz);
+            }
+            gx = fma(yp[j], px, gx);
+            gy = fma(yp[j], py, gy);
+            gz = fma(yp[j], pz, gz);
+        }
+        const double gs = scale * rinv;   // d/dt = (1/rscale) d/d(scaled offset)
+        grad[t] = gs * gx;
+        grad[tstride + t] = gs * gy;
+        grad[2 * tstride + t] = gs * gz;
+    }
 }
 
 // }}}
@@ -925,13 +957,17 @@ __global__ void mpole_f32_kernel(int n, int np, int64_t nboxes, const double *__
 
 // item = {first target, first List-3 entry, number of List-3 boxes,
 //         targets (1..32) | source level << 8}
-template <int P>
+// GRAD: also the potential's target-coordinate derivatives, d/dt D[mi] =
+// D[mi + e_d] / rscale, from derivative layers one degree higher (the
+// D(2, j, k) entries reduced by the Laplace identity to mi0 < 2).
+template <int P, bool GRAD = false>
 __global__ void __launch_bounds__(32 * ITEM_WARPS)
 m2p_items_kernel(int32_t nitems, const int4 *__restrict__ items,
                  const double *__restrict__ level_rscale, const int32_t *__restrict__ src_lists,
                  const double *__restrict__ centers, int64_t cstride,
                  const float *__restrict__ mp32, const double *__restrict__ targets,
-                 int64_t tstride, double scale, double *__restrict__ result)
+                 int64_t tstride, double scale, double *__restrict__ result,
+                 double *__restrict__ grad = nullptr)
 {
     constexpr int NP = npad_of(P);
     constexpr int C = NP / 4;
@@ -967,7 +1003,7 @@ m2p_items_kernel(int32_t nitems, const int4 *__restrict__ items,
         cpa_commit();
     };
     stage(0);
-    double acc = 0.0;
+    double acc = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
     for (int r = 0; r < nrounds; ++r) {
         if (r + 1 < nrounds) {
             stage(r + 1);
@@ -982,16 +1018,55 @@ m2p_items_kernel(int32_t nitems, const int4 *__restrict__ items,
             const float *M = buf + (r & 1) * (M2PI_GROUPS * NP) + ph * NP;
             // four partial sums: a dependent chain of N / 4 FMAs, not N
             float a4[4] = {0.f, 0.f, 0.f, 0.f};
-            laplace_layers<P, float>(
-                (float)(tx - centers[sb]), (float)(ty - centers[cstride + sb]),
-                (float)(tz - centers[2 * cstride + sb]), R, Rinv,
-                [&](int s, int, int, int, float v) { a4[s & 3] = fmaf(M[s], v, a4[s & 3]); });
+            if constexpr (GRAD) {
+                float fx = 0.f, fy = 0.f, fz = 0.f;
+                laplace_layers<P + 1, float>(
+                    (float)(tx - centers[sb]), (float)(ty - centers[cstride + sb]),
+                    (float)(tz - centers[2 * cstride + sb]), R, Rinv,
+                    [&](int s, int i, int j, int kk, float v) {
+                        const int deg = i + j + kk;
+                        if (deg <= P) a4[s & 3] = fmaf(M[s], v, a4[s & 3]);
+                        if (deg >= 1) {
+                            if (j >= 1) fy = fmaf(M[stored_index(i, j - 1, kk)], v, fy);
+                            if (kk >= 1) fz = fmaf(M[stored_index(i, j, kk - 1)], v, fz);
+                            if (i == 1) {
+                                fx = fmaf(M[stored_index(0, j, kk)], v, fx);
+                            } else {
+                                if (j >= 2) fx = fmaf(-M[stored_index(1, j - 2, kk)], v, fx);
+                                if (kk >= 2) fx = fmaf(-M[stored_index(1, j, kk - 2)], v, fx);
+                            }
+                        }
+                    });
+                gx += (double)fx;
+                gy += (double)fy;
+                gz += (double)fz;
+            } else {
+                laplace_layers<P, float>(
+                    (float)(tx - centers[sb]), (float)(ty - centers[cstride + sb]),
+                    (float)(tz - centers[2 * cstride + sb]), R, Rinv,
+                    [&](int s, int, int, int, float v) { a4[s & 3] = fmaf(M[s], v, a4[s & 3]); });
+            }
             acc += (double)((a4[0] + a4[1]) + (a4[2] + a4[3]));
         }
         __syncwarp();   // buffer r & 1 is refilled by round r + 2's copies
     }
-    for (int off = g; off < 32; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-    if (active && ph == 0) atomicAdd(result + t, scale * acc);
+    for (int off = g; off < 32; off <<= 1) {
+        acc += __shfl_xor_sync(0xffffffffu, acc, off);
+        if (GRAD) {
+            gx += __shfl_xor_sync(0xffffffffu, gx, off);
+            gy += __shfl_xor_sync(0xffffffffu, gy, off);
+            gz += __shfl_xor_sync(0xffffffffu, gz, off);
+        }
+    }
+    if (active && ph == 0) {
+        if (result) atomicAdd(result + t, scale * acc);
+        if (GRAD) {
+            const double gs = scale / level_rscale[lev];
+            atomicAdd(grad + t, gs * gx);
+            atomicAdd(grad + tstride + t, gs * gy);
+            atomicAdd(grad + 2 * tstride + t, gs * gz);
+        }
+    }
 }
 
 // P2L item = {target box, first entry of the flat List-4 source index
@@ -1453,6 +1528,40 @@ int sumpy_e2p_from_single_box_packed_f64(int order, int32_t nitems, const int32_
 #undef NF_OF
 }
 
+int sumpy_e2p_from_single_box_packed_grad_f64(int order, int32_t nitems, const int32_t *items,
+                                              const int32_t *slots, const double *level_rscales,
+                                              const double *centers, int64_t center_stride,
+                                              const double *src_expansions,
+                                              const double *targets, int64_t target_stride,
+                                              double scale, double *result, double *grad,
+                                              void *stream)
+{
+    if (!order_ok(order)) { set_last_error("l2p packed grad: unsupported order"); return SUMPY_EUNSUPPORTED; }
+    if (nitems < 0) return bad_arg("l2p packed grad: nitems < 0");
+    if (nitems == 0) return SUMPY_OK;
+    if (!items || !slots || !level_rscales || !centers || !src_expansions || !targets || !grad)
+        return bad_arg("l2p packed grad: null pointer argument");
+    if ((reinterpret_cast<uintptr_t>(items) & 7) || (reinterpret_cast<uintptr_t>(slots) & 15))
+        return bad_arg("l2p packed grad: items must be 8-byte and slots 16-byte aligned");
+#define NF_OF(P) ((P + 1) * (P + 2) * (P + 3) / 6)
+#define CALL_L2PKG(P)                                                                            \
+    (prepare_smem(l2p_packed_kernel<P, true>,                                                    \
+                  sizeof(double) * L2PK_SLOTS * NF_OF(P) * l2pk_warps<P>())                      \
+         ? SUMPY_ELAUNCH                                                                         \
+         : (l2p_packed_kernel<P, true><<<(nitems + l2pk_warps<P>() - 1) / l2pk_warps<P>(),       \
+                                         32 * l2pk_warps<P>(),                                   \
+                                         sizeof(double) * L2PK_SLOTS * NF_OF(P) *                \
+                                             l2pk_warps<P>(),                                    \
+                                         as_stream(stream)>>>(                                   \
+                nitems, reinterpret_cast<const int2 *>(items),                                  \
+                reinterpret_cast<const int4 *>(slots), level_rscales, centers, center_stride,   \
+                src_expansions, targets, target_stride, scale, result, grad),                   \
+            check_launch("l2p_packed_kernel")))
+    SUMPY_ORDER_SWITCH(order, CALL_L2PKG)
+#undef CALL_L2PKG
+#undef NF_OF
+}
+
 int sumpy_mpoles_to_f32(int order, int64_t nboxes, const double *src_expansions, float *dst,
                         void *stream)
 {
@@ -1495,6 +1604,37 @@ int sumpy_e2p_from_items_mixed(int order, int32_t nitems, const int32_t *items,
             check_launch("m2p_items_kernel")))
     SUMPY_ORDER_SWITCH(order, CALL_M2PI)
 #undef CALL_M2PI
+}
+
+int sumpy_e2p_from_items_grad_mixed(int order, int32_t nitems, const int32_t *items,
+                                    const double *level_rscales,
+                                    const int32_t *source_box_lists, const double *centers,
+                                    int64_t center_stride, const float *src_expansions_f32,
+                                    const double *targets, int64_t target_stride, double scale,
+                                    double *result, double *grad, void *stream)
+{
+    if (!order_ok(order)) { set_last_error("m2p items grad: unsupported order"); return SUMPY_EUNSUPPORTED; }
+    if (nitems < 0) return bad_arg("m2p items grad: nitems < 0");
+    if (nitems == 0) return SUMPY_OK;
+    if (!items || !level_rscales || !source_box_lists || !centers || !src_expansions_f32 ||
+        !targets || !grad)
+        return bad_arg("m2p items grad: null pointer argument");
+    if ((reinterpret_cast<uintptr_t>(items) | reinterpret_cast<uintptr_t>(src_expansions_f32)) & 15)
+        return bad_arg("m2p items grad: items and FP32 expansions must be 16-byte aligned");
+    const int blocks = (nitems + ITEM_WARPS - 1) / ITEM_WARPS;
+#define CALL_M2PIG(P)                                                                            \
+    (prepare_smem(m2p_items_kernel<P, true>,                                                     \
+                  sizeof(float) * 2 * M2PI_GROUPS * npad_of(P) * ITEM_WARPS)                     \
+         ? SUMPY_ELAUNCH                                                                         \
+         : (m2p_items_kernel<P, true><<<blocks, 32 * ITEM_WARPS,                                 \
+                                        sizeof(float) * 2 * M2PI_GROUPS * npad_of(P) * ITEM_WARPS, \
+                                        as_stream(stream)>>>(                                    \
+                nitems, reinterpret_cast<const int4 *>(items), level_rscales, source_box_lists, \
+                centers, center_stride, src_expansions_f32, targets, target_stride, scale,      \
+                result, grad),                                                                   \
+            check_launch("m2p_items_kernel")))
+    SUMPY_ORDER_SWITCH(order, CALL_M2PIG)
+#undef CALL_M2PIG
 }
 
 int sumpy_p2e_from_items_mixed(int order, int32_t nitems, const int32_t *items,

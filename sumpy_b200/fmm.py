@@ -1055,7 +1055,7 @@ class SumpyExpansionWrangler:
 
     @property
     def _merged_levels(self):
-        return (self.merge_levels and not self.gradient and len(set(self.level_orders)) == 1)
+        return self.merge_levels and len(set(self.level_orders)) == 1
 
     @property
     def _items_path(self):
@@ -1063,7 +1063,7 @@ class SumpyExpansionWrangler:
         mixed form; Helmholtz: both forms, FP64 arithmetic); needs one order
         on every level (flat [nboxes][ncoeff] storage)."""
         return (self.item_kernels and (self.precision == "mixed" or self.helmholtz)
-                and not self.gradient and len(set(self.level_orders)) == 1)
+                and len(set(self.level_orders)) == 1)
 
     @cached_property
     def _level_rscales(self):
@@ -1104,10 +1104,13 @@ class SumpyExpansionWrangler:
                            device=self.device)
         call("sumpy_mpoles_to_f32", _c(order), _i64(self.tree.nboxes), dptr(mpole_exps),
              dptr(mp32), st)
-        call("sumpy_e2p_from_items_mixed", _c(order), _i32(items.shape[0]), dptr(items),
-             dptr(self._level_rscales), dptr(lists), dptr(g["centers"]),
-             _i64(self.tree.nboxes), dptr(mp32), dptr(g["targets"]), _i64(self.tree.ntargets),
-             _d(self._scale), dptr(pot[0]), st)
+        args = (_c(order), _i32(items.shape[0]), dptr(items), dptr(self._level_rscales),
+                dptr(lists), dptr(g["centers"]), _i64(self.tree.nboxes), dptr(mp32),
+                dptr(g["targets"]), _i64(self.tree.ntargets), _d(self._scale), dptr(pot[0]))
+        if self.gradient:
+            call("sumpy_e2p_from_items_grad_mixed", *args, dptr(pot[1]), st)
+        else:
+            call("sumpy_e2p_from_items_mixed", *args, st)
         return pot
 
     def eval_multipoles(self, actx, target_boxes_by_source_level, source_boxes_by_level,
@@ -1238,11 +1241,14 @@ class SumpyExpansionWrangler:
             items, slots = self._cached_items(
                 "l2p_items", (level_start_target_box_nrs, target_boxes), build)
             if items.shape[0]:
-                call("sumpy_e2p_from_single_box_packed_f64", _c(self.level_orders[0]),
-                     _i32(items.shape[0]), dptr(items), dptr(slots), dptr(self._level_rscales),
-                     dptr(g["centers"]), _i64(self.tree.nboxes), dptr(local_exps),
-                     dptr(g["targets"]), _i64(self.tree.ntargets), _d(self._scale),
-                     dptr(pot[0]), st)
+                args = (_c(self.level_orders[0]), _i32(items.shape[0]), dptr(items),
+                        dptr(slots), dptr(self._level_rscales), dptr(g["centers"]),
+                        _i64(self.tree.nboxes), dptr(local_exps), dptr(g["targets"]),
+                        _i64(self.tree.ntargets), _d(self._scale), dptr(pot[0]))
+                if self.gradient:
+                    call("sumpy_e2p_from_single_box_packed_grad_f64", *args, dptr(pot[1]), st)
+                else:
+                    call("sumpy_e2p_from_single_box_packed_f64", *args, st)
             return pot
         ltb = _np_i32(level_start_target_box_nrs)
         boxes = self._dev(target_boxes)

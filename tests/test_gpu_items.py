@@ -175,3 +175,36 @@ def test_helmholtz_one_launch_stages_match_per_level(cuda_device, order):
     for a, b in zip(outs[1], outs[0]):
         assert np.abs(b).max() > 0
         assert relerr(a, b) < 1e-12
+
+
+@pytest.mark.parametrize("order", [4, 10])
+def test_gradient_one_launch_matches_per_level(cuda_device, order):
+    """Gradient outputs (the adjoint's position gradients): List 3 over work
+    items (mixed) and the packed L2P (FP64) against the per-level kernels."""
+    src, tgt = sphere_plummer(20000, 13), uniform_cube(15000, 21) * 3.0 - 1.0
+    tree, trav, tcls = build_all(src, tgt, 32)
+    q = torch.as_tensor(np.random.default_rng(12).standard_normal(src.shape[1]), device="cuda")
+    knl = LaplaceKernel(3)
+    ti = SumpyTreeIndependentDataForWrangler(
+        None, lambda o, **kw: MExp(knl, o), lambda o, **kw: LExp(knl, o), [knl])
+    outs = []
+    for new in (False, True):
+        w = SumpyExpansionWrangler(ti, trav, np.float64, lambda *a: order, precision="mixed",
+                                   translation_classes_data=tcls, gradient=True)
+        w.item_kernels = w.merge_levels = new
+        qs = w.reorder_sources(q)
+        mp = w.form_multipoles(None, trav.level_start_source_box_nrs, trav.source_boxes, [qs])
+        mp = w.coarsen_multipoles(None, trav.level_start_source_parent_box_nrs,
+                                  trav.source_parent_boxes, mp)
+        pm = w.eval_multipoles(None, trav.target_boxes_sep_smaller_by_source_level,
+                               trav.from_sep_smaller_by_level, mp)
+        loc = w.multipole_to_local(None, trav.level_start_target_or_target_parent_box_nrs,
+                                   trav.target_or_target_parent_boxes,
+                                   trav.from_sep_siblings_starts, trav.from_sep_siblings_lists,
+                                   mp)
+        pe = w.eval_locals(None, trav.level_start_target_box_nrs, trav.target_boxes, loc)
+        outs.append(([t.cpu().numpy() for t in pm], [t.cpu().numpy() for t in pe]))
+    for k in range(4):     # potential, d/dx, d/dy, d/dz
+        assert np.abs(outs[0][0][k]).max() > 0
+        assert relerr(outs[1][0][k], outs[0][0][k]) < 1e-6, k
+        assert relerr(outs[1][1][k], outs[0][1][k]) < 1e-12, k
