@@ -67,9 +67,10 @@ int sumpy_p2p_from_csr_f64(
     const double *targets, int64_t target_stride,
     const int32_t *target_to_source, double scale, double *result, void *stream);
 
-/* Same contract, mixed precision: coordinate differences formed in FP64 and
- * rounded to FP32, 1/r and the products in FP32, per-box partial sums in
- * FP32, the target's total in FP64. */
+/* Same contract, mixed precision: each coordinate split into FP32 hi + lo
+ * parts, the pair offset (t_hi - s_hi) + (t_lo - s_lo), 1/r and the products
+ * in FP32, partial sums over each 32 sources in FP32, the target's total in
+ * FP64. */
 int sumpy_p2p_from_csr_mixed(
     int32_t ntgt_boxes, const int32_t *target_boxes,
     const int32_t *source_box_starts, const int32_t *source_box_lists,
