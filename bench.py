@@ -63,7 +63,8 @@ def parse():
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-problem batch")
     ap.add_argument("--no-helmholtz", action="store_true",
                     help="skip the 500k-point Helmholtz workload")
-    ap.add_argument("--only", choices=["mixed", "fp64", "batch", "helmholtz", "uniform"],
+    ap.add_argument("--only", choices=["mixed", "fp64", "batch", "helmholtz", "uniform",
+                                       "matrix"],
                     help="run one workload alone (--steps/--warmup apply) and print its result; "
                          "for profiling")
     ap.add_argument("--eager", action="store_true",
@@ -265,9 +266,11 @@ def main():
         LinearPDEConformingVolumeTaylorMultipoleExpansion as MExp)
     from sumpy_b200.tree import build_all
 
-    if args.only in ("batch", "helmholtz", "uniform"):
+    if args.only in ("batch", "helmholtz", "uniform", "matrix"):
         if args.only == "batch":
             res = batched_bench(dev, steps=args.steps, warmup=args.warmup)
+        elif args.only == "matrix":
+            res = matrix_bench(dev, steps=args.steps, warmup=args.warmup)
         elif args.only == "helmholtz":
             precs = (("mixed", "fp64") if args.helmholtz_precision == "both"
                      else (args.helmholtz_precision,))
@@ -413,7 +416,10 @@ def main():
     adj = adjoint_bench(dev) if world == 1 else None
     batch = batched_bench(dev) if world == 1 and not args.no_batch else None
     helm = helmholtz_bench(dev) if world == 1 and not args.no_helmholtz else None
+    import gc
+    gc.collect()
     uni = uniform_bench(dev, cpu=not args.no_cpu_baseline) if world == 1 else None
+    mat = matrix_bench(dev) if world == 1 else None
 
     value = world * args.npoints / (ms_mx * 1e-3) / 1e6
     line = {
@@ -447,6 +453,7 @@ def main():
         "batched": batch,
         "helmholtz": helm,
         "uniform_p6": uni,
+        "p2p_matrix": mat,
         "stage_ms": stage_ms,
         "roofline": roof,
         "roofline_m2l": roof_m2l,
@@ -647,6 +654,57 @@ def batched_bench(dev, steps=5, warmup=3, nproblems=512, order=8, nseq=16):
     }
 
 
+def matrix_bench(dev, steps=5, warmup=3, n=20_000, nsub=20_000_000):
+    """Interaction matrices (P2PMatrixGenerator / P2PMatrixSubsetGenerator):
+    the dense n x n Laplace matrix of n = 20k points U[0,1]^3 (3.2 GB of
+    FP64 written; HBM-write bound: bytes = 8 per entry), the n/2 x n/2
+    Helmholtz matrix (k = 10, 16 bytes per entry), and 20M random index
+    pairs. CUDA-event time per call, inputs resident; roofline against the
+    measured HBM copy bandwidth."""
+    import torch
+    from sumpy_b200 import (HelmholtzKernel, LaplaceKernel, P2PMatrixGenerator,
+                            P2PMatrixSubsetGenerator)
+    peaks = {}
+    pk = ROOT / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peaks = json.loads(pk.read_text())
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    rng = np.random.default_rng(15)
+    pts = torch.as_tensor(rng.random((3, n)), device=dev)
+
+    def tm(fn):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    out = {}
+    lap = P2PMatrixGenerator([LaplaceKernel(3)])
+    ms = tm(lambda: lap(None, pts, pts, device=dev))
+    gbs = 8.0 * n * n / (ms * 1e-3) / 1e9
+    out["laplace_dense"] = {"shape": [n, n], "ms": ms, "GB_s": gbs, "frac_hbm": gbs / hbm}
+    nh = n // 2
+    hel = P2PMatrixGenerator([HelmholtzKernel(3)])
+    ms = tm(lambda: hel(None, pts[:, :nh], pts[:, :nh], device=dev, k=10.0))
+    gbs = 16.0 * nh * nh / (ms * 1e-3) / 1e9
+    out["helmholtz_dense"] = {"shape": [nh, nh], "k": 10.0, "ms": ms, "GB_s": gbs,
+                              "frac_hbm": gbs / hbm}
+    it = torch.as_tensor(rng.integers(0, n, nsub), device=dev, dtype=torch.int32)
+    js = torch.as_tensor(rng.integers(0, n, nsub), device=dev, dtype=torch.int32)
+    sub = P2PMatrixSubsetGenerator([LaplaceKernel(3)])
+    ms = tm(lambda: sub(None, pts, pts, tgtindices=it, srcindices=js, device=dev))
+    out["laplace_subset"] = {"pairs": nsub, "ms": ms, "Gentries_s": nsub / (ms * 1e-3) / 1e9,
+                             "GB_s_indices_and_result": 16.0 * nsub / (ms * 1e-3) / 1e9}
+    out["peak_hbm_gbs"] = hbm
+    return out
+
+
 def uniform_bench(dev, steps=5, warmup=3, n=20_000, order=6, cpu=True):
     """The reference's own CPU-runnable case: 20k sources and 20k separate
     targets U[0,1]^3 (seeds 15, 18; strengths seed 44), p = 6, max 30 per box,
@@ -667,8 +725,11 @@ def uniform_bench(dev, steps=5, warmup=3, n=20_000, order=6, cpu=True):
     knl = LaplaceKernel(3)
     ti = SumpyTreeIndependentDataForWrangler(
         None, lambda o, **kw: MExp(knl, o), lambda o, **kw: LExp(knl, o), [knl])
+    # replayed from a CUDA graph like the headline: at 20k points the eager
+    # launch sequence is host-bound, and its timing drifts with the state the
+    # earlier workloads leave in the process
     w = SumpyExpansionWrangler(ti, trav, np.float64, lambda *a: order,
-                               translation_classes_data=tcls, device=dev)
+                               translation_classes_data=tcls, device=dev, cuda_graph=True)
     qd = torch.as_tensor(q, device=dev)
     for _ in range(warmup):
         drive_fmm(None, w, [qd])
@@ -681,7 +742,7 @@ def uniform_bench(dev, steps=5, warmup=3, n=20_000, order=6, cpu=True):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
     (ref,) = P2P([knl])(None, tgt, src, (q,), device=dev)
-    out = {"workload": f"uniform {n} sources + {n} targets, p={order}, FP64",
+    out = {"workload": f"uniform {n} sources + {n} targets, p={order}, FP64", "launch": "CUDA graph replay",
            "ms_per_step": ms, "Mpts_s": n / (ms * 1e-3) / 1e6,
            "relL2_vs_direct": float((pot - ref).norm() / ref.norm())}
     if cpu:

@@ -121,6 +121,35 @@ int sumpy_p2p_direct_grad_f64(
     const double *strength, const int32_t *target_to_source, double scale,
     double *result, double *grad, void *stream);
 
+/* Interaction matrix entries. Replace P2PMatrixGenerator.__call__
+ * (sumpy/p2p.py:290-349): result[t * nsources + s] = scale * G(t - s), and
+ * P2PMatrixSubsetGenerator.__call__ (sumpy/p2p.py:354-477): result[m] =
+ * scale * G(targets[tgtindices[m]] - sources[srcindices[m]]); G = 1/r
+ * (Laplace) or e^{ikr}/r (Helmholtz, complex result as interleaved (re, im)
+ * pairs, 16-byte aligned). With target_to_source (may be NULL) the entries
+ * with source == target_to_source[target] are 0 (exclude_self). FP64. */
+int sumpy_p2p_matrix_f64(
+    int64_t ntargets, const double *targets, int64_t target_stride,
+    int64_t nsources, const double *sources, int64_t source_stride,
+    const int32_t *target_to_source, double scale, double *result, void *stream);
+
+int sumpy_helmholtz_p2p_matrix_f64(
+    int64_t ntargets, const double *targets, int64_t target_stride,
+    int64_t nsources, const double *sources, int64_t source_stride,
+    const int32_t *target_to_source, double k, double scale, double *result, void *stream);
+
+int sumpy_p2p_matrix_subset_f64(
+    int64_t nresult, const int32_t *tgtindices, const int32_t *srcindices,
+    const double *targets, int64_t target_stride, const double *sources,
+    int64_t source_stride, const int32_t *target_to_source, double scale, double *result,
+    void *stream);
+
+int sumpy_helmholtz_p2p_matrix_subset_f64(
+    int64_t nresult, const int32_t *tgtindices, const int32_t *srcindices,
+    const double *targets, int64_t target_stride, const double *sources,
+    int64_t source_stride, const int32_t *target_to_source, double k, double scale,
+    double *result, void *stream);
+
 /* ------------------------------------------------------------------ */
 /* P2E                                                                  */
 /* ------------------------------------------------------------------ */

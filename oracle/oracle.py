@@ -241,6 +241,46 @@ def p2p_direct(targets, sources, strengths, target_to_source=None):
 # }}}
 
 
+# {{{ interaction matrix entries
+
+def p2p_matrix_entries(targets, sources, tgtindices, srcindices, target_to_source=None,
+                       helmholtz_k=None):
+    """FP64 entries G(t - s) / (4 pi) at index pairs, numpy: the arithmetic of
+    sumpy's P2PMatrixSubsetGenerator (sumpy/p2p.py:354-477: d = targets[itgt]
+    - sources[isrc], p2p.py:392-397) with the kernel expressions of
+    LaplaceKernel(3) (1/r) or HelmholtzKernel(3) (e^{ikr}/r) and their
+    global scaling 1/(4 pi) (sumpy/kernel.py:639-691, 754-844); with
+    target_to_source the pairs with isrc == target_to_source[itgt] are 0
+    (p2p.py:162-170, 397-398). The dense P2PMatrixGenerator
+    (p2p.py:290-349) is the subset of all pairs."""
+    t = np.asarray(targets, dtype=np.float64)
+    s = np.asarray(sources, dtype=np.float64)
+    it = np.asarray(tgtindices, dtype=np.int64)
+    js = np.asarray(srcindices, dtype=np.int64)
+    d = t[:, it] - s[:, js]
+    r = np.sqrt((d * d).sum(axis=0))
+    self_pair = np.zeros(len(it), dtype=bool)
+    if target_to_source is not None:
+        self_pair = np.asarray(target_to_source, dtype=np.int64)[it] == js
+    r = np.where(self_pair, 1.0, r)
+    if helmholtz_k is None:
+        val = 1.0 / r
+    else:
+        val = np.exp(1j * helmholtz_k * r) / r
+    return np.where(self_pair, 0.0, val) / (4 * np.pi)
+
+
+def p2p_matrix(targets, sources, target_to_source=None, helmholtz_k=None):
+    """The dense [ntargets, nsources] matrix of p2p_matrix_entries."""
+    nt = np.asarray(targets).shape[1]
+    ns = np.asarray(sources).shape[1]
+    it, js = np.meshgrid(np.arange(nt), np.arange(ns), indexing="ij")
+    return p2p_matrix_entries(targets, sources, it.ravel(), js.ravel(), target_to_source,
+                              helmholtz_k).reshape(nt, ns)
+
+# }}}
+
+
 # {{{ whole FMM over a tree
 
 def run_fmm(tree, trav, tcls, order, weights, exclude_self=False,

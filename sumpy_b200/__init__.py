@@ -13,10 +13,12 @@ from sumpy_b200.expansion import (
 )
 from sumpy_b200.fmm import SumpyExpansionWrangler, SumpyTreeIndependentDataForWrangler
 from sumpy_b200.kernel import HelmholtzKernel, LaplaceKernel
-from sumpy_b200.p2p import P2P
+from sumpy_b200.p2p import P2P, P2PMatrixGenerator, P2PMatrixSubsetGenerator
 
 __all__ = [
     "P2P",
+    "P2PMatrixGenerator",
+    "P2PMatrixSubsetGenerator",
     "HelmholtzKernel",
     "LaplaceKernel",
     "LinearPDEConformingVolumeTaylorLocalExpansion",

@@ -63,6 +63,11 @@ SIGNATURES = {
     "sumpy_e2p_from_single_box_packed_f64": [cint, i32, ptr, ptr, ptr, ptr, i64, ptr, ptr,
                                              i64, dbl, ptr, ptr],
     "sumpy_mpoles_to_f32": [cint, i64, ptr, ptr, ptr],
+    "sumpy_p2p_matrix_f64": [i64, ptr, i64, i64, ptr, i64, ptr, dbl, ptr, ptr],
+    "sumpy_helmholtz_p2p_matrix_f64": [i64, ptr, i64, i64, ptr, i64, ptr, dbl, dbl, ptr, ptr],
+    "sumpy_p2p_matrix_subset_f64": [i64, ptr, ptr, ptr, i64, ptr, i64, ptr, dbl, ptr, ptr],
+    "sumpy_helmholtz_p2p_matrix_subset_f64": [i64, ptr, ptr, ptr, i64, ptr, i64, ptr, dbl, dbl,
+                                              ptr, ptr],
     "sumpy_e2p_from_items_grad_mixed": [cint, i32, ptr, ptr, ptr, ptr, i64, ptr, ptr, i64, dbl,
                                         ptr, ptr, ptr],
     "sumpy_e2p_from_single_box_packed_grad_f64": [cint, i32, ptr, ptr, ptr, ptr, i64, ptr, ptr,
