@@ -126,7 +126,7 @@ int sumpy_p2p_direct_grad_f64(
  * P2PMatrixSubsetGenerator.__call__ (sumpy/p2p.py:354-477): result[m] =
  * scale * G(targets[tgtindices[m]] - sources[srcindices[m]]); G = 1/r
  * (Laplace) or e^{ikr}/r (Helmholtz, complex result as interleaved (re, im)
- * pairs, 16-byte aligned). With target_to_source (may be NULL) the entries
+ * pairs); result 16-byte aligned. With target_to_source (may be NULL) the entries
  * with source == target_to_source[target] are 0 (exclude_self). FP64. */
 int sumpy_p2p_matrix_f64(
     int64_t ntargets, const double *targets, int64_t target_stride,
@@ -588,6 +588,15 @@ int sumpy_helmholtz_e2p_from_single_box_levels_f64(
     const double *src_expansions, const int32_t *box_target_starts,
     const int32_t *box_target_counts_nonchild, const double *targets, int64_t target_stride,
     double scale, double *result, void *stream);
+
+/* Helmholtz E2PFromSingleBox of all levels over packed items as
+ * sumpy_e2p_from_single_box_packed_f64 (items of at most 4 slots); the
+ * locals are decompressed with kappa = k^2 rscale^2 of each box's level. */
+int sumpy_helmholtz_e2p_from_single_box_packed_f64(
+    int order, double k, int32_t nitems, const int32_t *items, const int32_t *slots,
+    const double *level_rscales, const double *centers, int64_t center_stride,
+    const double *src_expansions, const double *targets, int64_t target_stride, double scale,
+    double *result, void *stream);
 
 int sumpy_helmholtz_e2p_from_items_f64(
     int order, double k, int32_t nitems, const int32_t *items, const double *level_rscales,

@@ -64,6 +64,8 @@ SIGNATURES = {
                                              i64, dbl, ptr, ptr],
     "sumpy_mpoles_to_f32": [cint, i64, ptr, ptr, ptr],
     "sumpy_p2p_matrix_f64": [i64, ptr, i64, i64, ptr, i64, ptr, dbl, ptr, ptr],
+    "sumpy_helmholtz_e2p_from_single_box_packed_f64": [cint, dbl, i32, ptr, ptr, ptr, ptr, i64,
+                                                       ptr, ptr, i64, dbl, ptr, ptr],
     "sumpy_helmholtz_p2p_matrix_f64": [i64, ptr, i64, i64, ptr, i64, ptr, dbl, dbl, ptr, ptr],
     "sumpy_p2p_matrix_subset_f64": [i64, ptr, ptr, ptr, i64, ptr, i64, ptr, dbl, ptr, ptr],
     "sumpy_helmholtz_p2p_matrix_subset_f64": [i64, ptr, ptr, ptr, i64, ptr, i64, ptr, dbl, dbl,

@@ -762,16 +762,7 @@ p2l_mixed_kernel(double rscale, int32_t ntgt_boxes, const int32_t *__restrict__ 
 
 // {{{ L2P over packed items (all levels in one launch)
 
-// Full coefficients of one box in the layout [(j, k) pairs, j-major][i]:
-// the x-run of pair (j, k) holds i = 0..P-j-k contiguously.
-// (closed form of: the pairs (j', k') before (j, k) times their run lengths)
-template <int P>
-__host__ __device__ constexpr int jki_offset(int j, int k)
-{
-    constexpr int A = P + 1;
-    return A * (A + 1) * (A + 2) / 6 - (A - j) * (A - j + 1) * (A - j + 2) / 6 + k * (A - j) -
-           k * (k - 1) / 2;
-}
+// (coefficients in the [(j, k)][i] layout of jki_offset, taylor.cuh)
 
 constexpr int L2PK_SLOTS = 8;   // boxes per warp item
 

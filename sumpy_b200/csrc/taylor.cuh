@@ -43,6 +43,17 @@ __device__ inline void tri_pair(int t, int m, int &J, int &K)
     K = t;
 }
 
+// Full coefficients of one box in the layout [(j, k) pairs, j-major][i]:
+// the x-run of pair (j, k) holds i = 0..P-j-k contiguously.
+// (closed form of: the pairs (j', k') before (j, k) times their run lengths)
+template <int P>
+__host__ __device__ constexpr int jki_offset(int j, int k)
+{
+    constexpr int A = P + 1;
+    return A * (A + 1) * (A + 2) / 6 - (A - j) * (A - j + 1) * (A - j + 2) / 6 + k * (A - j) -
+           k * (k - 1) / 2;
+}
+
 __device__ inline double ipow(double x, int n)
 {
     double r = 1.0;

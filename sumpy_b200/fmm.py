@@ -52,6 +52,7 @@ M2L_ITEM_GROUPS = 64   # class groups per tensor-core work item (one CTA)
 ITEM_ROUNDS = 4        # rounds (one source box / 32 sources each) per mixed M2P / P2L item
 M2P_ITEM_GROUPS = 8    # lane groups per warp in the M2P item kernel (fixed by the kernel)
 L2P_ITEM_SLOTS = 8     # boxes per packed L2P item (fixed by the kernel)
+HL2P_ITEM_SLOTS = 4    # the same for the Helmholtz packed L2P
 
 
 def _npad(order):
@@ -309,6 +310,8 @@ class SumpyExpansionWrangler:
         self.item_kernels = True
         # P2M and L2P of all levels in one launch (one order on every level)
         self.merge_levels = True
+        # Helmholtz L2P over packed items (False: one warp per box, all levels)
+        self.packed_l2p = True
         # drive_fmm replays the whole evaluation from a CUDA graph (one host
         # call per evaluation instead of one per kernel launch)
         self.cuda_graph = bool(cuda_graph)
@@ -1216,6 +1219,22 @@ class SumpyExpansionWrangler:
         pot = self.output_zeros(actx)
         g = self._geom
         st = stream_ptr()
+        if self._merged_levels and self.helmholtz and self.packed_l2p \
+                and not isinstance(target_boxes, torch.Tensor):
+            def build_hp():
+                items, slots = l2p_items(self.tree, level_start_target_box_nrs, target_boxes,
+                                         max_slots=HL2P_ITEM_SLOTS)
+                return (torch.as_tensor(items).to(self.device),
+                        torch.as_tensor(slots).to(self.device))
+            items, slots = self._cached_items(
+                "hl2p_items", (level_start_target_box_nrs, target_boxes), build_hp)
+            if items.shape[0]:
+                call("sumpy_helmholtz_e2p_from_single_box_packed_f64", _c(self.level_orders[0]),
+                     _d(self.k), _i32(items.shape[0]), dptr(items), dptr(slots),
+                     dptr(self._level_rscales), dptr(g["centers"]), _i64(self.tree.nboxes),
+                     dptr(local_exps), dptr(g["targets"]), _i64(self.tree.ntargets),
+                     _d(self._scale), dptr(pot[0]), st)
+            return pot
         if self._merged_levels and self.helmholtz and not isinstance(target_boxes, torch.Tensor):
             def build_h():
                 tb = np.asarray(target_boxes, dtype=np.int64)

@@ -208,3 +208,29 @@ def test_gradient_one_launch_matches_per_level(cuda_device, order):
         assert np.abs(outs[0][0][k]).max() > 0
         assert relerr(outs[1][0][k], outs[0][0][k]) < 1e-6, k
         assert relerr(outs[1][1][k], outs[0][1][k]) < 1e-12, k
+
+
+@pytest.mark.parametrize("order", [2, 9, 14, 16])
+def test_helmholtz_packed_l2p_matches_per_box(cuda_device, order):
+    """Helmholtz L2P over packed items (several boxes per warp, layout
+    decompression with each box's own kappa) against the warp-per-box L2P."""
+    from sumpy_b200 import HelmholtzKernel
+    src, tgt = sphere_plummer(15000, 41), uniform_cube(9000, 42) * 2.0 - 0.5
+    tree, trav, tcls = build_all(src, tgt, 20)
+    knl = HelmholtzKernel(3)
+    ti = SumpyTreeIndependentDataForWrangler(
+        None, lambda o, **kw: MExp(knl, o), lambda o, **kw: LExp(knl, o), [knl])
+    rng = np.random.default_rng(43)
+    outs = []
+    for packed in (False, True):
+        w = SumpyExpansionWrangler(ti, trav, np.complex128, lambda *a: order,
+                                   kernel_extra_kwargs={"k": 7.0},
+                                   translation_classes_data=tcls)
+        w.packed_l2p = packed
+        loc = torch.as_tensor(
+            rng.standard_normal(w.local_expansion_zeros().numel()) * (1 + 0.5j), device="cuda")
+        rng = np.random.default_rng(43)   # the same locals for both
+        pe = w.eval_locals(None, trav.level_start_target_box_nrs, trav.target_boxes, loc)[0]
+        outs.append(pe.cpu().numpy())
+    assert np.abs(outs[0]).max() > 0
+    assert relerr(outs[1], outs[0]) < 1e-12
