@@ -411,6 +411,28 @@ def main():
     err_mx = rel(pot_mx.cpu().numpy())
     err_64 = rel(drive_fmm(None, w_64, [q_dev])[0].cpu().numpy()) if w_64 is not None else None
 
+    # the metric's accuracy target (relL2 <= 1e-6) is out of reach at p = 10
+    # for this algorithm (the FP64 form gives 3.4e-6); the same workload at
+    # the orders around the target, mixed form, same tree
+    at_target = None
+    if args.npoints == NPOINTS and args.order == ORDER and not args.only and world == 1:
+        at_target = []
+        for p_hi in (11, 12, 13):
+            w_p = SumpyExpansionWrangler(ti, trav, np.float64, lambda k, a, t, lev, p=p_hi: p,
+                                         translation_classes_data=tcls, precision="mixed",
+                                         device=dev, cuda_graph=True)
+            for _ in range(max(1, args.warmup)):
+                drive_fmm(None, w_p, [q_dev])
+            ms_p, _ = timed(lambda: drive_fmm(None, w_p, [q_dev]), args.steps)
+            e_p = rel(drive_fmm(None, w_p, [q_dev])[0].cpu().numpy())
+            w_p.check_status()
+            at_target.append({"order": p_hi, "ms_per_step": ms_p,
+                              "value": args.npoints / (ms_p * 1e-3) / 1e6, "relL2_mixed": e_p,
+                              "meets_1e-6": e_p <= 1e-6})
+            del w_p
+            if e_p <= 1e-6:
+                break
+
     pipes = pipe_peaks_measured(dev)
     stage_ms, roof, roof_m2l = stage_breakdown(w_mx, trav, q_dev, dev, pipe_peaks=pipes)
     adj = adjoint_bench(dev) if world == 1 else None
@@ -447,6 +469,7 @@ def main():
                  "ms_per_step": ms_64},
         "mixed_over_fp64": (ms_64 / ms_mx) if ms_64 else None,
         "fp64_own_best_tree": fp64_best,
+        "order_for_accuracy_target": at_target,
         "mixed_over_fp64_own_best": (fp64_best["ms_per_step"] / ms_mx) if fp64_best else None,
         "adjoint_forward_ratio": adj["ratio"] if adj else None,
         "adjoint": adj,
