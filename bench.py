@@ -46,6 +46,7 @@ FP64_MAX_PARTICLES = 128
 HELMHOLTZ_MAX_PARTICLES = 64   # same sweep for the Helmholtz workload: 32: 46 ms, 64: 21 ms
 BATCH_MAX_PARTICLES = 32       # the batched workload's own setting
 ADJOINT_MAX_PARTICLES = 32
+ACCURACY_MAX_PARTICLES = 128   # the order sweep toward relL2 <= 1e-6 (p = 11..13)
 NSAMPLE = 4096
 
 
@@ -414,24 +415,28 @@ def main():
     # the metric's accuracy target (relL2 <= 1e-6) is out of reach at p = 10
     # for this algorithm (the FP64 form gives 3.4e-6); the same workload at
     # the orders around the target, mixed form, same tree
+    # (leaf size 128: the errors are the same as at 96 within 1 %, the time lower)
     at_target = None
     if args.npoints == NPOINTS and args.order == ORDER and not args.only and world == 1:
         at_target = []
+        tree_a, trav_a, tcls_a = build_all(pts, None, ACCURACY_MAX_PARTICLES)
         for p_hi in (11, 12, 13):
-            w_p = SumpyExpansionWrangler(ti, trav, np.float64, lambda k, a, t, lev, p=p_hi: p,
-                                         translation_classes_data=tcls, precision="mixed",
+            w_p = SumpyExpansionWrangler(ti, trav_a, np.float64, lambda k, a, t, lev, p=p_hi: p,
+                                         translation_classes_data=tcls_a, precision="mixed",
                                          device=dev, cuda_graph=True)
             for _ in range(max(1, args.warmup)):
                 drive_fmm(None, w_p, [q_dev])
             ms_p, _ = timed(lambda: drive_fmm(None, w_p, [q_dev]), args.steps)
             e_p = rel(drive_fmm(None, w_p, [q_dev])[0].cpu().numpy())
             w_p.check_status()
-            at_target.append({"order": p_hi, "ms_per_step": ms_p,
+            at_target.append({"order": p_hi, "max_particles_in_box": ACCURACY_MAX_PARTICLES,
+                              "ms_per_step": ms_p,
                               "value": args.npoints / (ms_p * 1e-3) / 1e6, "relL2_mixed": e_p,
                               "meets_1e-6": e_p <= 1e-6})
             del w_p
             if e_p <= 1e-6:
                 break
+        del tree_a, trav_a, tcls_a
 
     pipes = pipe_peaks_measured(dev)
     stage_ms, roof, roof_m2l = stage_breakdown(w_mx, trav, q_dev, dev, pipe_peaks=pipes)
