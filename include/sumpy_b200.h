@@ -467,6 +467,31 @@ int sumpy_p2e_from_items_mixed(
     const double *sources, int64_t source_stride, const double *strength,
     double *tgt_expansions, void *stream);
 
+/* The same item schedules in FP64 throughout (replacing the per-level
+ * sumpy_e2p_from_csr_f64 / sumpy_p2e_from_csr_f64 loops of
+ * sumpy/fmm.py:645-711 for a uniform-order FMM): src_expansions are the
+ * FP64 multipoles [nboxes][(order+1)^2] (no FP32 copy, no alignment rule);
+ * items as above (16-byte aligned), M2P items built with one-lane groups
+ * (a chunk of ntc targets takes next_pow2(ntc) lanes). The grad form adds
+ * the target gradient into grad ([3][target_stride]); result may be NULL. */
+int sumpy_e2p_from_items_f64(
+    int order, int32_t nitems, const int32_t *items, const double *level_rscales,
+    const int32_t *source_box_lists, const double *centers, int64_t center_stride,
+    const double *src_expansions, const double *targets, int64_t target_stride,
+    double scale, double *result, void *stream);
+
+int sumpy_e2p_from_items_grad_f64(
+    int order, int32_t nitems, const int32_t *items, const double *level_rscales,
+    const int32_t *source_box_lists, const double *centers, int64_t center_stride,
+    const double *src_expansions, const double *targets, int64_t target_stride,
+    double scale, double *result, double *grad, void *stream);
+
+int sumpy_p2e_from_items_f64(
+    int order, int32_t nitems, const int32_t *items, const double *level_rscales,
+    const int32_t *source_index, const double *centers, int64_t center_stride,
+    const double *sources, int64_t source_stride, const double *strength,
+    double *tgt_expansions, void *stream);
+
 /* ------------------------------------------------------------------------
  * 3D Helmholtz kernel G = exp(i k r) / r (sumpy/kernel.py:755-844), the same
  * loopy kernels as above instantiated for HelmholtzKernel(3): complex data

@@ -90,6 +90,11 @@ SIGNATURES = {
                                    ptr, ptr],
     "sumpy_p2e_from_items_mixed": [cint, i32, ptr, ptr, ptr, ptr, i64, ptr, i64, ptr, ptr,
                                    ptr],
+    "sumpy_e2p_from_items_f64": [cint, i32, ptr, ptr, ptr, ptr, i64, ptr, ptr, i64, dbl, ptr,
+                                 ptr],
+    "sumpy_e2p_from_items_grad_f64": [cint, i32, ptr, ptr, ptr, ptr, i64, ptr, ptr, i64, dbl,
+                                      ptr, ptr, ptr],
+    "sumpy_p2e_from_items_f64": [cint, i32, ptr, ptr, ptr, ptr, i64, ptr, i64, ptr, ptr, ptr],
     # Helmholtz
     "sumpy_helmholtz_p2p_from_csr_f64": [i32, ptr, ptr, ptr, ptr, ptr, ptr, ptr, ptr, i64, dbl,
                                          ptr, ptr, i64, ptr, dbl, ptr, ptr],

@@ -1062,17 +1062,23 @@ class SumpyExpansionWrangler:
 
     @property
     def _items_path(self):
-        """List 3 / List 4 through the one-launch item kernels (Laplace:
-        mixed form; Helmholtz: both forms, FP64 arithmetic); needs one order
-        on every level (flat [nboxes][ncoeff] storage)."""
-        return (self.item_kernels and (self.precision == "mixed" or self.helmholtz)
-                and len(set(self.level_orders)) == 1)
+        """List 3 / List 4 through the one-launch item kernels (Laplace mixed:
+        FP32 arithmetic on FP64 offsets; Laplace FP64 and Helmholtz: FP64
+        arithmetic); needs one order on every level (flat [nboxes][ncoeff]
+        storage)."""
+        return self.item_kernels and len(set(self.level_orders)) == 1
 
     @cached_property
     def _level_rscales(self):
         return torch.tensor([self.level_to_rscale(lev) if self.level_orders[lev] else 1.0
                              for lev in range(self.tree.nlevels)],
                             dtype=torch.float64, device=self.device)
+
+    @property
+    def _m2p_f32(self):
+        """Laplace mixed form: the M2P items read an FP32 copy of the
+        multipoles (lane groups of at least 32 / M2P_ITEM_GROUPS lanes)."""
+        return self.precision == "mixed" and not self.helmholtz
 
     def _cached_items(self, key, objs, build):
         hit = self._devcache.get(key)
@@ -1087,7 +1093,7 @@ class SumpyExpansionWrangler:
         def build():
             items, lists = m2p_items(self.tree, target_boxes_by_source_level,
                                      source_boxes_by_level,
-                                     groups=32 if self.helmholtz else M2P_ITEM_GROUPS)
+                                     groups=M2P_ITEM_GROUPS if self._m2p_f32 else 32)
             return (torch.as_tensor(items).to(self.device),
                     torch.as_tensor(lists).to(self.device))
         items, lists = self._cached_items(
@@ -1102,6 +1108,15 @@ class SumpyExpansionWrangler:
                  _i32(items.shape[0]), dptr(items), dptr(self._level_rscales), dptr(lists),
                  dptr(g["centers"]), _i64(self.tree.nboxes), dptr(mpole_exps),
                  dptr(g["targets"]), _i64(self.tree.ntargets), _d(self._scale), dptr(pot[0]), st)
+            return pot
+        if not self._m2p_f32:
+            args = (_c(order), _i32(items.shape[0]), dptr(items), dptr(self._level_rscales),
+                    dptr(lists), dptr(g["centers"]), _i64(self.tree.nboxes), dptr(mpole_exps),
+                    dptr(g["targets"]), _i64(self.tree.ntargets), _d(self._scale), dptr(pot[0]))
+            if self.gradient:
+                call("sumpy_e2p_from_items_grad_f64", *args, dptr(pot[1]), st)
+            else:
+                call("sumpy_e2p_from_items_f64", *args, st)
             return pot
         mp32 = torch.empty(self.tree.nboxes * _npad(order), dtype=torch.float32,
                            device=self.device)
@@ -1161,7 +1176,8 @@ class SumpyExpansionWrangler:
                 g = self._geom
                 w = self._weights(src_weight_vecs)
                 name = ("sumpy_helmholtz_p2e_from_items_f64" if self.helmholtz
-                        else "sumpy_p2e_from_items_mixed")
+                        else "sumpy_p2e_from_items_mixed" if self.precision == "mixed"
+                        else "sumpy_p2e_from_items_f64")
                 call(name, _c(self.level_orders[0]), *self._kargs,
                      _i32(items.shape[0]), dptr(items), dptr(self._level_rscales), dptr(sidx),
                      dptr(g["centers"]), _i64(self.tree.nboxes), dptr(g["sources"]),

@@ -68,6 +68,46 @@ def test_items_match_fp64_and_per_level(cuda_device, mpb, order):
         assert relerr(itm[k], lev[k]) < 1e-6, (k, relerr(itm[k], lev[k]))
 
 
+@pytest.mark.parametrize("mpb", [8, 96])
+@pytest.mark.parametrize("order", [3, 10])
+def test_items_fp64_match_per_level(cuda_device, mpb, order):
+    """FP64 List 3 / List 4 over work items (sumpy_e2p_from_items_f64,
+    sumpy_p2e_from_items_f64) against the per-level FP64 kernels: the same
+    FP64 arithmetic summed in another order (asserted 1e-12)."""
+    src = sphere_plummer(40000, 9)
+    tree, trav, tcls = build_all(src, None, mpb)
+    q = np.random.default_rng(8).standard_normal(src.shape[1])
+    lev = _list3_list4(_wrangler(trav, tcls, order, "fp64", False, True), trav, q)
+    itm = _list3_list4(_wrangler(trav, tcls, order, "fp64", True, True), trav, q)
+    for k in range(2):
+        assert np.abs(lev[k]).max() > 0
+        assert relerr(itm[k], lev[k]) < 1e-12, (k, relerr(itm[k], lev[k]))
+
+
+def test_items_fp64_gradient_match_per_level(cuda_device):
+    src, tgt = sphere_plummer(20000, 17), uniform_cube(12000, 19) * 3.0 - 1.0
+    tree, trav, tcls = build_all(src, tgt, 32)
+    q = torch.as_tensor(np.random.default_rng(14).standard_normal(src.shape[1]), device="cuda")
+    knl = LaplaceKernel(3)
+    ti = SumpyTreeIndependentDataForWrangler(
+        None, lambda o, **kw: MExp(knl, o), lambda o, **kw: LExp(knl, o), [knl])
+    outs = []
+    for new in (False, True):
+        w = SumpyExpansionWrangler(ti, trav, np.float64, lambda *a: 7, precision="fp64",
+                                   translation_classes_data=tcls, gradient=True)
+        w.item_kernels = new
+        qs = w.reorder_sources(q)
+        mp = w.form_multipoles(None, trav.level_start_source_box_nrs, trav.source_boxes, [qs])
+        mp = w.coarsen_multipoles(None, trav.level_start_source_parent_box_nrs,
+                                  trav.source_parent_boxes, mp)
+        pm = w.eval_multipoles(None, trav.target_boxes_sep_smaller_by_source_level,
+                               trav.from_sep_smaller_by_level, mp)
+        outs.append([t.cpu().numpy() for t in pm])
+    for k in range(4):     # potential, d/dx, d/dy, d/dz
+        assert np.abs(outs[0][k]).max() > 0
+        assert relerr(outs[1][k], outs[0][k]) < 1e-12, k
+
+
 def test_items_end_to_end_separate_targets(cuda_device):
     src, tgt = uniform_cube(20000, 15), uniform_cube(15000, 18)
     src[:, :5000] *= 0.05          # a dense cluster: long List 3 / List 4
