@@ -1,4 +1,4 @@
-"""Host-side work items of the one-launch mixed M2P and P2L kernels
+"""Host-side work items of the one-launch M2P and P2L kernels
 (sumpy_b200.fmm.m2p_items / p2l_items): every (target, List-3 box) pair and
 every (target box, List-4 source) pair of the traversal is covered exactly
 once, items respect the kernels' limits (32 targets, lane groups, rounds),
@@ -17,17 +17,20 @@ def traversal(request):
     return build_all(pts, None, request.param)
 
 
-def _lane_groups(ntc):
-    g = 32 // M2P_ITEM_GROUPS
+def _lane_groups(ntc, groups=M2P_ITEM_GROUPS):
+    g = 32 // groups
     while g < ntc:
         g *= 2
     return 32 // g
 
 
-def test_m2p_items_cover_list3_once(traversal):
+# M2P_ITEM_GROUPS: the mixed kernel (FP32 multipoles staged per lane group);
+# 32: the FP64 and Helmholtz kernels (lane groups from one lane)
+@pytest.mark.parametrize("groups", [M2P_ITEM_GROUPS, 32])
+def test_m2p_items_cover_list3_once(traversal, groups):
     tree, trav, _ = traversal
     items, lists = m2p_items(tree, trav.target_boxes_sep_smaller_by_source_level,
-                             trav.from_sep_smaller_by_level)
+                             trav.from_sep_smaller_by_level, groups=groups)
     assert items.dtype == np.int32 and items.flags.c_contiguous and items.shape[1] == 4
     # expected (target, global list entry) pairs and each entry's level
     want, entry_level, off = [], [], 0
@@ -45,7 +48,7 @@ def test_m2p_items_cover_list3_once(traversal):
     got, cost = [], []
     for t0, l0, nb, w in items:
         ntc, lev = w & 0xff, w >> 8
-        nph = _lane_groups(ntc)
+        nph = _lane_groups(ntc, groups)
         assert 1 <= ntc <= 32 and 1 <= nb <= nph * ITEM_ROUNDS
         assert all(entry_level[e] == lev for e in range(l0, l0 + nb))
         got += [(t, e) for t in range(t0, t0 + ntc) for e in range(l0, l0 + nb)]
