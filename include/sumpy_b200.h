@@ -418,10 +418,11 @@ int sumpy_p2e_from_csr_mixed(
  *   source_boxes[i] (its rscale = level_rscales[level]); any box order (the
  *   host lists the largest first). Assigns the boxes' multipoles.
  * sumpy_e2p_from_single_box_packed_f64: items int32 [nitems][2] (8-byte
- *   aligned) = {first slot, number of slots (1..8)}; slots int32 [][4]
+ *   aligned) = {first slot, number of slots (1..4)}; slots int32 [][4]
  *   (16-byte aligned) = {box, first target, number of targets, level}, at
- *   most 32 targets per item, a box's targets in one or more slots.
- *   Assigns scale * potential to each listed target. */
+ *   most 32 targets per item, a box's targets in one or more slots. An item
+ *   of more than 4 slots (more than the warp's shared memory holds) is
+ *   skipped. Assigns scale * potential to each listed target. */
 int sumpy_p2e_from_single_box_levels_f64(
     int order, int32_t nsrc_boxes, const int32_t *source_boxes, const int32_t *box_levels,
     const double *level_rscales, const double *centers, int64_t center_stride,

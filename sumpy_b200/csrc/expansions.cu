@@ -764,7 +764,13 @@ p2l_mixed_kernel(double rscale, int32_t ntgt_boxes, const int32_t *__restrict__ 
 
 // (coefficients in the [(j, k)][i] layout of jki_offset, taylor.cuh)
 
-constexpr int L2PK_SLOTS = 8;   // boxes per warp item
+// boxes per warp item (the host's L2P_ITEM_SLOTS): 4 (measured at 1M points,
+// order 10: 0.144 ms against 0.235 ms with 8, whose shared memory leaves
+// 12 warps per SM; most items of a 96-point-leaf tree hold one box)
+#ifndef SUMPY_L2PK_SLOTS
+#define SUMPY_L2PK_SLOTS 4
+#endif
+constexpr int L2PK_SLOTS = SUMPY_L2PK_SLOTS;
 
 // warps per CTA: four while the slots' coefficients fit in 200 KB, else two
 template <int P>
@@ -773,7 +779,7 @@ __host__ __device__ constexpr int l2pk_warps()
     return 8 * L2PK_SLOTS * (P + 1) * (P + 2) * (P + 3) / 6 * 4 <= 200 * 1024 ? 4 : 2;
 }
 
-// One warp evaluates up to 32 targets taken from up to 8 boxes (slots; a
+// One warp evaluates up to 32 targets taken from up to L2PK_SLOTS boxes (slots; a
 // box with more than 32 targets spans several items). The slots' locals
 // are decompressed together (p - 1 plane sweeps, sumpy's
 // CSEMatVecOperator.matvec), then lane l evaluates its target as
@@ -804,6 +810,9 @@ l2p_packed_kernel(int32_t nitems, const int2 *__restrict__ items, const int4 *__
     double *cubes = sml + warp * (L2PK_SLOTS * NF);
     const int2 item = items[it];
     const int nsl = item.y;
+    // the warp's shared memory holds L2PK_SLOTS slots: an item with more is
+    // skipped rather than written past it (the host builds at most that many)
+    if (nsl < 0 || nsl > L2PK_SLOTS) return;
 
     // this lane's slot and target
     int my = -1, off = lane;

@@ -43,6 +43,9 @@ hl2p_packed_kernel(int32_t nitems, const int2 *__restrict__ items, const int4 *_
     z2 *cubes = reinterpret_cast<z2 *>(smh) + warp * (HL2PK_SLOTS * NF);
     const int2 item = items[it];
     const int nsl = item.y;
+    // the warp's shared memory holds HL2PK_SLOTS slots: an item with more is
+    // skipped rather than written past it (the host builds at most that many)
+    if (nsl < 0 || nsl > HL2PK_SLOTS) return;
 
     int my = -1, off = lane;
     int4 sl = make_int4(0, 0, 0, 0);

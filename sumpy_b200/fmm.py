@@ -51,7 +51,7 @@ M2L_TILE_TC = 128      # tensor-core tile (MMA N)
 M2L_ITEM_GROUPS = 64   # class groups per tensor-core work item (one CTA)
 ITEM_ROUNDS = 4        # rounds (one source box / 32 sources each) per mixed M2P / P2L item
 M2P_ITEM_GROUPS = 8    # lane groups per warp in the M2P item kernel (fixed by the kernel)
-L2P_ITEM_SLOTS = 8     # boxes per packed L2P item (fixed by the kernel)
+L2P_ITEM_SLOTS = 4     # boxes per packed L2P item (fixed by the kernel)
 HL2P_ITEM_SLOTS = 4    # the same for the Helmholtz packed L2P
 
 
@@ -1039,7 +1039,8 @@ class SumpyExpansionWrangler:
             src_lev = tgt_lev - 1
             sbase, sview = self.local_expansions_view(local_exps, src_lev)
             tbase, tview = self.local_expansions_view(local_exps, tgt_lev)
-            self._octant_gemm("l2l", plan, sview, sbase, tview, tbase, st, fp64=fp64)
+            self._octant_gemm("l2l", plan, sview, sbase, tview, tbase, st, fp64=fp64,
+                              parent_level=src_lev)
         return local_exps
 
     # }}}
@@ -1208,7 +1209,7 @@ class SumpyExpansionWrangler:
 
     def refine_locals(self, actx, level_start_target_or_target_parent_box_nrs,
                       target_or_target_parent_boxes, local_exps):
-        tc = self._tc_translations and not self.helmholtz and self.tc_l2l
+        tc = self._tc_translations and self.tc_l2l
         if tc or (self.gemm_l2l and self._gemm_fp64_ok):
             return self._refine_tc(level_start_target_or_target_parent_box_nrs,
                                    target_or_target_parent_boxes, local_exps, fp64=not tc)
@@ -1270,7 +1271,8 @@ class SumpyExpansionWrangler:
             return pot
         if self._merged_levels and not isinstance(target_boxes, torch.Tensor):
             def build():
-                items, slots = l2p_items(self.tree, level_start_target_box_nrs, target_boxes)
+                items, slots = l2p_items(self.tree, level_start_target_box_nrs, target_boxes,
+                                         max_slots=L2P_ITEM_SLOTS)
                 return (torch.as_tensor(items).to(self.device),
                         torch.as_tensor(slots).to(self.device))
             items, slots = self._cached_items(

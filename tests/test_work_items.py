@@ -118,6 +118,12 @@ def test_l2p_packing_covers_targets_once(traversal):
         t0 = tree.box_target_starts[tb]
         want[t0:t0 + tree.box_target_counts_nonchild[tb]] = 1
     np.testing.assert_array_equal(seen, want)
-    # packing is dense: slots cover all items contiguously, lanes mostly used
+    # packing is dense: slots cover all items contiguously, and next fit
+    # closes an item only when it is full (32 targets or L2P_ITEM_SLOTS
+    # slots) or the next slot would not fit
     assert items[0, 0] == 0 and (items[1:, 0] == np.cumsum(items[:, 1])[:-1]).all()
-    assert want.sum() / (32 * len(items)) > 0.75
+    ntg = np.array([slots[f:f + n, 2].sum() for f, n in items])
+    for i in range(len(items) - 1):
+        nxt = slots[items[i + 1, 0], 2]
+        assert ntg[i] == 32 or items[i, 1] == L2P_ITEM_SLOTS or ntg[i] + nxt > 32, i
+    assert want.sum() / (32 * len(items)) > 0.5
