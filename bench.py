@@ -876,6 +876,11 @@ def helmholtz_bench(dev, steps=3, warmup=2, npoints=500_000, order=14, k=10.0,
             # adjoint with respect to the strengths: the FMM on the transposed
             # traversal (sumpy_b200.autograd.HelmholtzFMM's backward)
             from sumpy_b200.adjoint import transpose_traversal
+            import gc
+            # the eager launch sequence allocates per call: start from a
+            # collected caching allocator, as the forward timing did
+            gc.collect()
+            torch.cuda.empty_cache()
             tree_t, trav_t, tcls_t = transpose_traversal(tree, trav, tcls)
             wa = SumpyExpansionWrangler(ti, trav_t, np.complex128, lambda *a: order,
                                         kernel_extra_kwargs={"k": k},
