@@ -1,19 +1,34 @@
 """Benchmark: 3D Laplace FMM evaluation throughput on one B200 (or N replicas).
 
-Workload (one step = one full FMM evaluation, ``drive_fmm``): 1,000,000
-points that are both sources and targets (exclude_self), 50% on the unit
-sphere surface and 50% Plummer (scale 0.1), strengths N(0, 1), expansion
-order 10, max_particles_in_box 32. Synthetic, seeded inputs; the tree,
-interaction lists and M2L tables are built once before timing (reported
-separately). ``value`` is Mpts/s of the mixed-precision form with inputs
-resident in HBM; the FP64 form is timed the same way for the ratio; the
-accuracy of both is the relative L2 error on 4,096 sampled targets against
-an FP64 direct sum. ``e2e`` runs the public API with host buffers (H2D of the
-strengths, D2H of the potentials inside the timed region).
+Headline workload (one step = one full FMM evaluation, ``drive_fmm``):
+1,000,000 points that are both sources and targets (exclude_self), 50% on
+the unit sphere surface and 50% Plummer (scale 0.1), strengths N(0, 1),
+expansion order 10, max_particles_in_box 96. Synthetic, seeded inputs; the
+tree, interaction lists and M2L tables are built once before timing
+(reported separately). ``value`` is Mpts/s of the mixed-precision form with
+inputs resident in HBM; the FP64 form is timed on the same tree for the
+ratio; the accuracy of both is the relative L2 error on 4,096 sampled
+targets against an FP64 direct sum. Order 10 cannot reach relL2 <= 1e-6 on
+this workload (the FP64 form gives 3.4e-6), so the line also carries the
+same workload at the lowest order that does (``accuracy_target``: mixed and
+FP64 on one tree). ``e2e`` runs the public API with host buffers (H2D of
+the strengths, D2H of the potentials inside the timed region).
 
-``--impl reference`` times the FP64 CPU restatement of sumpy's algorithm
-(the oracle, C + OpenMP on all host cores) on a bounded sample of the same
-workload and prints the same metric.
+A default run prints that one JSON line and nothing else on stdout, as soon
+as it is measured; progress goes to stderr with timestamps, and a section
+that runs longer than ``--stall-dump-s`` dumps every thread's Python stack to
+stderr. ``--extras`` adds the other workloads (adjoint, 512-problem batch,
+Helmholtz, 20k uniform case, interaction matrices), each as a JSON line of
+its own after the headline, within ``--budget-s``.
+
+The CPU baseline is the oracle (C + OpenMP, sumpy's algorithm restated) on
+the headline workload itself, one evaluation, run in a child process that
+never imports torch and is killed if it overruns ``--cpu-timeout-s``.
+
+``--impl reference`` times that oracle on the headline workload (same tree,
+order and leaf size; W warm-up and K timed evaluations) and prints the same
+metric; when K + W full evaluations would not fit ``--ref-budget-s`` it
+times a sample of the workload instead and says so (``same_config``).
 
 Multi-GPU (torchrun): each rank evaluates its own replica; no collective on
 the data path (the problem does not shard in this build); value = points of
@@ -22,6 +37,7 @@ all ranks / max over ranks of the step time.
 from __future__ import annotations
 
 import argparse
+import faulthandler
 import json
 import os
 import subprocess
@@ -40,14 +56,28 @@ ORDER = 10
 # max_particles_in_box of the 1M-point workload (the workload leaves it open): the fastest
 # mixed form in a sweep over 32..192 on this GPU (32: 11.0 ms, 64: 10.1, 96: 9.6, 128: 10.0,
 # 192: 13.7 ms; accuracy against the direct sum 3.5e-6 for all). The FP64 form is timed on
-# the same tree (like for like) and, separately, on its own fastest tree (FP64_MAX_PARTICLES).
+# the same tree (like for like) and, with --extras, on its own fastest tree.
 MAX_PARTICLES = 96
 FP64_MAX_PARTICLES = 128
 HELMHOLTZ_MAX_PARTICLES = 64   # same sweep for the Helmholtz workload: 32: 46 ms, 64: 21 ms
 BATCH_MAX_PARTICLES = 32       # the batched workload's own setting
 ADJOINT_MAX_PARTICLES = 32
-ACCURACY_MAX_PARTICLES = 128   # the order sweep toward relL2 <= 1e-6 (p = 11..13)
+# the order that meets relL2 <= 1e-6 on the headline workload (p = 11: 1.7e-6,
+# p = 12: 1.02e-6, p = 13: 9.6e-7 in the mixed form), on its own leaf-128 tree
+ACCURACY_ORDER = 13
+ACCURACY_MAX_PARTICLES = 128
 NSAMPLE = 4096
+
+_T0 = time.perf_counter()
+_STALL_DUMP_S = 240.0
+
+
+def progress(msg):
+    """Timestamped progress on stderr; re-arms the stall dump (a section that
+    runs past the limit prints every thread's Python stack to stderr)."""
+    print(f"[bench {time.perf_counter() - _T0:8.1f} s] {msg}", file=sys.stderr, flush=True)
+    if _STALL_DUMP_S > 0:
+        faulthandler.dump_traceback_later(_STALL_DUMP_S, repeat=True, file=sys.stderr)
 
 
 def parse():
@@ -59,13 +89,23 @@ def parse():
     ap.add_argument("--npoints", type=int, default=NPOINTS)
     ap.add_argument("--order", type=int, default=ORDER)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-timeout-s", type=float, default=240.0,
+                    help="kill the CPU-baseline child process after this long")
+    ap.add_argument("--ref-budget-s", type=float, default=900.0,
+                    help="--impl reference: time budget of the W + K evaluations")
+    ap.add_argument("--budget-s", type=float, default=1500.0,
+                    help="wall-clock budget: sections that would start later are skipped "
+                         "and listed under 'skipped'")
+    ap.add_argument("--stall-dump-s", type=float, default=240.0,
+                    help="dump all Python stacks to stderr when one section runs this long "
+                         "(0: off)")
     ap.add_argument("--no-fp64", action="store_true", help="skip timing the FP64 form")
-    ap.add_argument("--stage-times", action="store_true", help="print per-stage times")
-    ap.add_argument("--no-batch", action="store_true", help="skip the 512-problem batch")
-    ap.add_argument("--no-helmholtz", action="store_true",
-                    help="skip the 500k-point Helmholtz workload")
+    ap.add_argument("--no-accuracy-target", action="store_true",
+                    help="skip the accuracy-target order (p = 13) of the headline workload")
+    ap.add_argument("--extras", action="store_true",
+                    help="after the headline, run the other workloads (one JSON line each)")
     ap.add_argument("--only", choices=["mixed", "fp64", "batch", "helmholtz", "uniform",
-                                       "matrix"],
+                                       "matrix", "adjoint"],
                     help="run one workload alone (--steps/--warmup apply) and print its result; "
                          "for profiling")
     ap.add_argument("--eager", action="store_true",
@@ -84,61 +124,113 @@ def workload(npoints, seed=2024):
 
 # {{{ reference arm / CPU baseline (oracle)
 
-def cpu_fmm_rate(npoints, order, seed=2024, target_seconds=10.0, min_points=5000):
-    """Time the oracle FMM on a sample sized to take about target_seconds."""
-    from oracle import oracle as O
-    from sumpy_b200.tree import build_all
-    n = max(min_points, min(npoints, 20000))
-    while True:
-        pts, q = workload(n, seed)
-        tree, trav, tcls = build_all(pts, None, MAX_PARTICLES)
-        t0 = time.perf_counter()
-        O.run_fmm(tree, trav, tcls, order, q, exclude_self=True)
-        dt = time.perf_counter() - t0
-        if dt > 0.3 * target_seconds or n >= npoints:
-            return n, dt
-        n = min(npoints, int(n * min(8.0, target_seconds / max(dt, 1e-3))))
-
-
 def run_reference(args):
+    """The oracle (FP64 C + OpenMP restatement of sumpy's wrangler stages,
+    ``sumpy/fmm.py:609-1083``) on the headline workload: the same points,
+    tree (leaf size), order and exclude_self as the GPU arm. The first
+    warm-up evaluation sizes the run: if W + K full evaluations would exceed
+    ``--ref-budget-s``, each step becomes a sample of the workload (fewer
+    points, same distribution) sized to fit, and the line says so."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from oracle import oracle as O
     from sumpy_b200.tree import build_all
-    n, _ = cpu_fmm_rate(args.npoints, args.order, target_seconds=4.0)
-    pts, q = workload(n)
+    progress(f"reference: workload {args.npoints} points, p = {args.order}")
+    pts, q = workload(args.npoints)
     tree, trav, tcls = build_all(pts, None, MAX_PARTICLES)
-    for _ in range(args.warmup):
-        O.run_fmm(tree, trav, tcls, args.order, q, exclude_self=True)
-    times = []
-    for _ in range(args.steps):
+    n = args.npoints
+
+    def step():
         t0 = time.perf_counter()
         O.run_fmm(tree, trav, tcls, args.order, q, exclude_self=True)
-        times.append(time.perf_counter() - t0)
+        return time.perf_counter() - t0
+
+    times = []
+    progress("reference: first evaluation (sizes the run)")
+    t1 = step()
+    if args.warmup == 0:
+        times.append(t1)          # the first timed step also sized the run
+    left = max(args.warmup - 1, 0) + args.steps - len(times)
+    same = left * t1 <= args.ref_budget_s
+    if not same:
+        # a sample of the same distribution whose W + K evaluations fit the budget
+        n = max(20_000, int(args.npoints * args.ref_budget_s /
+                            (max(args.warmup + args.steps, 1) * t1)))
+        n = min(n, args.npoints)
+        progress(f"reference: {left} full evaluations would take {left * t1:.0f} s; "
+                 f"timing a {n}-point sample instead")
+        pts, q = workload(n)
+        tree, trav, tcls = build_all(pts, None, MAX_PARTICLES)
+        times = []
+        for _ in range(args.warmup):
+            step()
+    else:
+        for _ in range(max(args.warmup - 1, 0)):
+            step()
+    progress(f"reference: {args.steps} timed evaluations ({t1:.1f} s each)")
+    while len(times) < args.steps:
+        times.append(step())
     tot = sum(times)
     value = n * args.steps / tot / 1e6
-    cores = os.cpu_count()
+    cores = O.num_threads()
+    sample = (f"the headline workload itself ({n} points, p={args.order}, leaf "
+              f"{MAX_PARTICLES}), FP64 C/OpenMP oracle (sumpy's algorithm restated), "
+              f"{cores} threads, {tot / args.steps:.1f} s per evaluation"
+              if same else
+              f"{n}-point sample of the headline distribution, p={args.order}, leaf "
+              f"{MAX_PARTICLES}: {args.warmup + args.steps} evaluations of all "
+              f"{args.npoints} points at "
+              f"{t1:.1f} s would exceed {args.ref_budget_s:.0f} s; FP64 C/OpenMP oracle, "
+              f"{cores} threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Mpts/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"laplace3d_fmm_sphere_plummer_n{args.npoints}_p{args.order}",
-                   "sample_points": n, "order": args.order,
-                   "max_particles_in_box": MAX_PARTICLES, "exclude_self": True},
+                   "npoints": args.npoints, "order": args.order,
+                   "max_particles_in_box": MAX_PARTICLES, "exclude_self": True,
+                   "same_config": same, "points_per_step": n},
         "cpu_baseline": {"value": value, "unit": "Mpts/s", "cores": cores, "kind": "port",
-                         "sample": f"{n}-point sample of the same distribution, p={args.order}, "
-                                   f"FP64 C/OpenMP oracle (sumpy's algorithm restated), "
-                                   f"{cores} threads"},
+                         "sample": sample},
         "e2e": {"value": value, "unit": "Mpts/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    faulthandler.cancel_dump_traceback_later()
     print(json.dumps(line), flush=True)
 
+
+def cpu_baseline_child(args):
+    """One oracle evaluation of the headline workload, timed in a child
+    process (``--impl reference --steps 1 --warmup 0``) that never imports
+    torch; None (with the reason) when it fails or overruns."""
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "LOCAL_WORLD_SIZE")}
+    cmd = [sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--steps", "1",
+           "--warmup", "0", "--npoints", str(args.npoints), "--order", str(args.order),
+           "--ref-budget-s", str(0.5 * args.cpu_timeout_s),
+           "--stall-dump-s", str(args.stall_dump_s)]
+    try:
+        res = subprocess.run(cmd, capture_output=True, text=True, env=env,
+                             timeout=args.cpu_timeout_s)
+    except subprocess.TimeoutExpired as e:
+        err = (e.stderr or b"")
+        err = err.decode(errors="replace") if isinstance(err, bytes) else err
+        sys.stderr.write(err[-4000:])
+        return None, f"oracle child process overran {args.cpu_timeout_s:.0f} s (killed)"
+    sys.stderr.write(res.stderr[-4000:])
+    if res.returncode != 0:
+        return None, f"oracle child process exited {res.returncode}"
+    try:
+        ref = json.loads(res.stdout.strip().splitlines()[-1])
+    except (ValueError, IndexError):
+        return None, "oracle child process printed no result line"
+    cb = dict(ref["cpu_baseline"])
+    cb["same_config"] = ref["config"]["same_config"]
+    return cb, None
+
 # }}}
-
-
 class ClockSampler:
     """SM clock and clock-event reasons sampled DURING a timed region: an NVML
     thread polling every 5 ms (read-only queries), so that even a region of a
@@ -244,292 +336,378 @@ class ClockSampler:
                 "source": "nvml" if self.thread is not None else "nvidia-smi"}
 
 
+class Budget:
+    """Wall-clock budget of the whole run: ``ok(name, need_s)`` says whether
+    a section expected to take ``need_s`` seconds may still start, and
+    records the ones that may not."""
+
+    def __init__(self, seconds):
+        self.seconds = seconds
+        self.skipped = []
+
+    def elapsed(self):
+        return time.perf_counter() - _T0
+
+    def ok(self, name, need_s=0.0):
+        if self.elapsed() + need_s > self.seconds:
+            self.skipped.append(name)
+            progress(f"skip {name}: {self.elapsed():.0f} s used of {self.seconds:.0f} s")
+            return False
+        return True
+
+
 def main():
+    global _STALL_DUMP_S
     args = parse()
+    _STALL_DUMP_S = args.stall_dump_s
+    faulthandler.enable(file=sys.stderr)
     if args.impl == "reference":
         run_reference(args)
         return
+    budget = Budget(args.budget_s)
+    rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
 
+    # CPU baseline first, in a child process without torch, before this
+    # process loads CUDA or competes for the host cores
+    cpu_line, cpu_why = None, "not run (--no-cpu-baseline, --only or N > 1)"
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.only is None:
+        progress("cpu baseline: oracle child process")
+        cpu_line, cpu_why = cpu_baseline_child(args)
+        progress(f"cpu baseline: {cpu_line['value']:.4f} Mpts/s" if cpu_line else
+                 f"cpu baseline: none ({cpu_why})")
+
+    progress("import torch")
     import torch
-    import torch.distributed as dist
 
-    from sumpy_b200.distributed import init as dist_init, max_over_ranks
+    from sumpy_b200.distributed import init as dist_init
     rank, world, local_rank = dist_init("nccl", timeout_s=300)
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
+    from sumpy_b200 import _lib
+    _lib.load_cuda_library()
 
-    from sumpy_b200 import (
-        P2P, LaplaceKernel, SumpyExpansionWrangler, SumpyTreeIndependentDataForWrangler,
-        drive_fmm)
-    from sumpy_b200 import _capi
+    if args.only is not None:
+        res = run_only(args, dev)
+        if rank == 0:
+            print(json.dumps({"only": args.only, "result": res}), flush=True)
+        faulthandler.cancel_dump_traceback_later()
+        return
+
+    line = headline(args, dev, rank, world, local_rank, budget, cpu_line, cpu_why)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    progress("headline printed")
+
+    if args.extras and world == 1:
+        for name, fn in (("fp64_own_best_tree", lambda: fp64_best_tree_bench(dev, args)),
+                         ("batched", lambda: batched_bench(dev)),
+                         ("helmholtz", lambda: helmholtz_bench(dev)),
+                         ("uniform_p6", lambda: uniform_bench(dev)),
+                         ("p2p_matrix", lambda: matrix_bench(dev))):
+            if not budget.ok(name, 30.0):
+                continue
+            progress(f"extra: {name}")
+            import gc
+            gc.collect()
+            torch.cuda.empty_cache()
+            res = fn()
+            print(json.dumps({"extra": name, "result": res}), flush=True)
+        if budget.skipped:
+            print(json.dumps({"extra": "skipped", "result": budget.skipped}), flush=True)
+    faulthandler.cancel_dump_traceback_later()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def laplace_setup(dev, npoints, max_particles):
+    """Points, strengths, tree and the tree-independent data of the headline
+    workload (host objects; the tree build is timed)."""
+    from sumpy_b200 import LaplaceKernel, SumpyTreeIndependentDataForWrangler
     from sumpy_b200.expansion import (
         LinearPDEConformingVolumeTaylorLocalExpansion as LExp,
         LinearPDEConformingVolumeTaylorMultipoleExpansion as MExp)
     from sumpy_b200.tree import build_all
-
-    if args.only in ("batch", "helmholtz", "uniform", "matrix"):
-        if args.only == "batch":
-            res = batched_bench(dev, steps=args.steps, warmup=args.warmup)
-        elif args.only == "matrix":
-            res = matrix_bench(dev, steps=args.steps, warmup=args.warmup)
-        elif args.only == "helmholtz":
-            precs = (("mixed", "fp64") if args.helmholtz_precision == "both"
-                     else (args.helmholtz_precision,))
-            res = helmholtz_bench(dev, steps=args.steps, warmup=args.warmup,
-                                  npoints=args.helmholtz_npoints, precisions=precs)
-        else:
-            res = uniform_bench(dev, steps=args.steps, warmup=args.warmup, cpu=False)
-        if rank == 0:
-            print(json.dumps({"only": args.only, "result": res}), flush=True)
-        return
-
-    # cpu baseline first, before any process pool / GPU work competes for the host
-    cpu_line = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.only is None:
-        n, dt = cpu_fmm_rate(args.npoints, args.order, target_seconds=12.0)
-        cores = os.cpu_count()
-        cpu_line = {"value": n / dt / 1e6, "unit": "Mpts/s", "cores": cores, "kind": "port",
-                    "sample": f"{n}-point sample of the same distribution, p={args.order}, "
-                              f"FP64 C/OpenMP oracle, {cores} threads, {dt:.1f} s"}
-
-    pts, q = workload(args.npoints)
+    pts, q = workload(npoints)
     t0 = time.perf_counter()
-    tree, trav, tcls = build_all(pts, None, MAX_PARTICLES)
+    tree, trav, tcls = build_all(pts, None, max_particles)
     t_tree = time.perf_counter() - t0
     knl = LaplaceKernel(3)
     ti = SumpyTreeIndependentDataForWrangler(
         None, lambda o, **kw: MExp(knl, o), lambda o, **kw: LExp(knl, o), [knl],
         exclude_self=True)
+    return pts, q, tree, trav, tcls, ti, t_tree
 
-    def wrangler(precision, graph=True):
-        # graph: drive_fmm replays the evaluation from a CUDA graph (one host
-        # call per step); the eager form launches each kernel from Python
-        return SumpyExpansionWrangler(ti, trav, np.float64, lambda k, a, t, lev: args.order,
-                                      precision=precision, device=dev, cuda_graph=graph)
 
-    q_dev = torch.as_tensor(q, device=dev)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+def make_wrangler(ti, trav, tcls, order, precision, dev, graph=True):
+    """An expansion wrangler of one order on every level; ``graph``: drive_fmm
+    replays the evaluation from a CUDA graph (one host call per step)."""
+    from sumpy_b200 import SumpyExpansionWrangler
+    return SumpyExpansionWrangler(ti, trav, np.float64, lambda k, a, t, lev, p=order: p,
+                                  translation_classes_data=tcls, precision=precision,
+                                  device=dev, cuda_graph=graph)
 
-    def barrier():
-        if world > 1:
+
+class StepTimer:
+    """Per-step CUDA-event times on the current stream with an L2 flush (a
+    256 MB write, outside the events) before every step; barrier +
+    synchronize on both sides; the max over ranks of the mean step time."""
+
+    def __init__(self, dev, world):
+        import torch
+        self.dev = dev
+        self.world = world
+        self.flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def _barrier(self):
+        if self.world > 1:
+            import torch.distributed as dist
             dist.barrier()
 
-    def timed(fn, steps):
-        """Per-step CUDA-event times with an L2 flush between steps."""
+    def __call__(self, fn, steps):
+        import torch
+        from sumpy_b200.distributed import max_over_ranks
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                for _ in range(steps)]
         torch.cuda.synchronize()
-        barrier()
+        self._barrier()
         for i in range(steps):
-            flush.fill_(float(i))
+            self.flush.fill_(float(i))
             evs[i][0].record()
             fn()
             evs[i][1].record()
         torch.cuda.synchronize()
-        barrier()
+        self._barrier()
         ms = [a.elapsed_time(b) for a, b in evs]
-        return max_over_ranks(sum(ms), device=dev) / steps, ms
+        return max_over_ranks(sum(ms), device=self.dev) / steps, ms
 
-    if args.only in ("mixed", "fp64"):
-        w = wrangler(args.only, graph=not args.eager)
-        for _ in range(max(1, args.warmup)):
-            drive_fmm(None, w, [q_dev])
-        ms, _ = timed(lambda: drive_fmm(None, w, [q_dev]), args.steps)
-        if rank == 0:
-            print(json.dumps({"only": args.only, "result": {
-                "ms_per_step": ms, "Mpts_s": args.npoints / (ms * 1e-3) / 1e6}}), flush=True)
-        return
 
-    # setup (plans, tables, graph capture) outside timing
+def headline(args, dev, rank, world, local_rank, budget, cpu_line, cpu_why):
+    """The headline line: mixed form (graph replay, timed, with clocks and
+    launch count), its eager launches, e2e with host buffers, the FP64 form
+    on the same tree, accuracy on sampled targets, the accuracy-target
+    order, the adjoint through the autograd API, stage times and the
+    roofline of the dominant kernel."""
+    import torch
+    from sumpy_b200 import P2P, LaplaceKernel, _capi, drive_fmm
+
+    progress("headline: workload and tree")
+    pts, q, tree, trav, tcls, ti, t_tree = laplace_setup(dev, args.npoints, MAX_PARTICLES)
+    timer = StepTimer(dev, world)
+    q_dev = torch.as_tensor(q, device=dev)
+
+    progress("headline: mixed form set-up (plans, tables, graph capture)")
     t0 = time.perf_counter()
-    w_mx = wrangler("mixed")
+    w_mx = make_wrangler(ti, trav, tcls, args.order, "mixed", dev)
     drive_fmm(None, w_mx, [q_dev])
     torch.cuda.synchronize()
     t_setup = time.perf_counter() - t0
 
-    # the same evaluation launched kernel by kernel from Python
+    progress("headline: mixed form, kernel-by-kernel launches")
     w_mx.cuda_graph = False
     for _ in range(max(1, args.warmup)):
         drive_fmm(None, w_mx, [q_dev])
-    ms_eager, _ = timed(lambda: drive_fmm(None, w_mx, [q_dev]), args.steps)
+    ms_eager, _ = timer(lambda: drive_fmm(None, w_mx, [q_dev]), args.steps)
     w_mx.cuda_graph = True
 
+    progress("headline: mixed form, graph replay (the timed value)")
     for _ in range(args.warmup):
         drive_fmm(None, w_mx, [q_dev])
     _capi.launch_counter.reset()
     with ClockSampler(local_rank) as clk:
-        ms_mx, _ = timed(lambda: drive_fmm(None, w_mx, [q_dev]), args.steps)
+        ms_mx, _ = timer(lambda: drive_fmm(None, w_mx, [q_dev]), args.steps)
     launches = _capi.launch_counter.value
     clocks = clk.summary()
+    w_mx.check_status()
 
-    # e2e through the public API with host buffers
+    progress("headline: e2e through the public API with pinned host buffers")
     q_host = torch.as_tensor(q).pin_memory()
     pot_host = torch.empty(args.npoints, dtype=torch.float64).pin_memory()
 
     def e2e_step():
-        # strengths copied from pinned host memory into the graph's input
+        # strengths copied from pinned host memory into the graph's input,
+        # potentials copied back to pinned host memory, both inside the events
         (pot,) = drive_fmm(None, w_mx, [q_host])
         pot_host.copy_(pot, non_blocking=True)
 
-    for _ in range(2):
+    for _ in range(max(1, args.warmup)):
         e2e_step()
-    ms_e2e, _ = timed(e2e_step, args.steps)
+    ms_e2e, _ = timer(e2e_step, args.steps)
 
-    # FP64 form
-    ms_64 = None
-    w_64 = None
-    if not args.no_fp64:
-        w_64 = wrangler("fp64")
+    ms_64, w_64 = None, None
+    if not args.no_fp64 and (world > 1 or budget.ok("fp64", 20.0)):
+        progress("headline: FP64 form on the same tree")
+        w_64 = make_wrangler(ti, trav, tcls, args.order, "fp64", dev)
         for _ in range(max(1, args.warmup)):
             drive_fmm(None, w_64, [q_dev])
-        ms_64, _ = timed(lambda: drive_fmm(None, w_64, [q_dev]), args.steps)
+        ms_64, _ = timer(lambda: drive_fmm(None, w_64, [q_dev]), args.steps)
+        w_64.check_status()
 
-    # FP64 on its own fastest tree (larger leaves favour the slower FP64 M2L)
-    fp64_best = None
-    if not args.no_fp64 and args.npoints == NPOINTS and args.order == ORDER:
-        tree_b, trav_b, tcls_b = build_all(pts, None, FP64_MAX_PARTICLES)
-        w_b = SumpyExpansionWrangler(ti, trav_b, np.float64, lambda k, a, t, lev: args.order,
-                                     translation_classes_data=tcls_b, precision="fp64",
-                                     device=dev, cuda_graph=True)
-        for _ in range(max(1, args.warmup)):
-            drive_fmm(None, w_b, [q_dev])
-        ms_b, _ = timed(lambda: drive_fmm(None, w_b, [q_dev]), args.steps)
-        fp64_best = {"max_particles_in_box": FP64_MAX_PARTICLES, "ms_per_step": ms_b,
-                     "value": world * args.npoints / (ms_b * 1e-3) / 1e6}
-        del w_b, tree_b, trav_b, tcls_b
-
-    # accuracy on sampled targets against the FP64 direct sum
+    progress("headline: accuracy on sampled targets against the FP64 direct sum")
+    knl = LaplaceKernel(3)
     rng = np.random.default_rng(99)
     sample = rng.choice(args.npoints, size=min(NSAMPLE, args.npoints), replace=False)
     (ref,) = P2P([knl], exclude_self=True)(None, pts[:, sample], pts, (q,),
                                            target_to_source=sample, device=dev)
-    (pot_mx,) = drive_fmm(None, w_mx, [q_dev])
     ref = ref.cpu().numpy()
 
-    def rel(p):
+    def rel(w):
+        p = drive_fmm(None, w, [q_dev])[0].cpu().numpy()
         return float(np.linalg.norm(p[sample] - ref) / np.linalg.norm(ref))
 
-    err_mx = rel(pot_mx.cpu().numpy())
-    err_64 = rel(drive_fmm(None, w_64, [q_dev])[0].cpu().numpy()) if w_64 is not None else None
+    err_mx = rel(w_mx)
+    err_64 = rel(w_64) if w_64 is not None else None
+    del w_64
+    torch.cuda.empty_cache()
 
-    # the metric's accuracy target (relL2 <= 1e-6) is out of reach at p = 10
-    # for this algorithm (the FP64 form gives 3.4e-6); the same workload at
-    # the orders around the target, mixed form, same tree
-    # (leaf size 128: the errors are the same as at 96 within 1 %, the time lower)
-    at_target = None
-    if args.npoints == NPOINTS and args.order == ORDER and not args.only and world == 1:
-        at_target = []
-        tree_a, trav_a, tcls_a = build_all(pts, None, ACCURACY_MAX_PARTICLES)
-        for p_hi in (11, 12, 13):
-            w_p = SumpyExpansionWrangler(ti, trav_a, np.float64, lambda k, a, t, lev, p=p_hi: p,
-                                         translation_classes_data=tcls_a, precision="mixed",
-                                         device=dev, cuda_graph=True)
-            for _ in range(max(1, args.warmup)):
-                drive_fmm(None, w_p, [q_dev])
-            ms_p, _ = timed(lambda: drive_fmm(None, w_p, [q_dev]), args.steps)
-            e_p = rel(drive_fmm(None, w_p, [q_dev])[0].cpu().numpy())
-            w_p.check_status()
-            at_target.append({"order": p_hi, "max_particles_in_box": ACCURACY_MAX_PARTICLES,
-                              "ms_per_step": ms_p,
-                              "value": args.npoints / (ms_p * 1e-3) / 1e6, "relL2_mixed": e_p,
-                              "meets_1e-6": e_p <= 1e-6})
-            del w_p
-            if e_p <= 1e-6:
-                break
-        if at_target[-1]["meets_1e-6"] and not args.no_fp64:
-            # the FP64 form at the same order and on the same tree: the
-            # metric's mixed-vs-FP64 comparison at relL2 <= 1e-6
-            p_hi = at_target[-1]["order"]
-            w_f = SumpyExpansionWrangler(ti, trav_a, np.float64, lambda k, a, t, lev, p=p_hi: p,
-                                         translation_classes_data=tcls_a, precision="fp64",
-                                         device=dev, cuda_graph=True)
-            for _ in range(max(1, args.warmup)):
-                drive_fmm(None, w_f, [q_dev])
-            ms_f, _ = timed(lambda: drive_fmm(None, w_f, [q_dev]), args.steps)
-            e_f = rel(drive_fmm(None, w_f, [q_dev])[0].cpu().numpy())
-            at_target[-1].update({
-                "fp64_ms_per_step": ms_f, "fp64_value": args.npoints / (ms_f * 1e-3) / 1e6,
-                "relL2_fp64": e_f,
-                "mixed_over_fp64": ms_f / at_target[-1]["ms_per_step"]})
-            del w_f
-        del tree_a, trav_a, tcls_a
+    # the metric's accuracy condition on the same workload: the lowest order
+    # that reaches it, mixed and FP64 forms on one tree
+    at = None
+    if (not args.no_accuracy_target and args.npoints == NPOINTS and args.order == ORDER
+            and world == 1 and budget.ok("accuracy_target", 60.0)):
+        at = accuracy_target(args, dev, pts, q_dev, ti, timer, rel)
 
+    adj = None
+    if world == 1 and budget.ok("adjoint", 60.0):
+        progress("headline: adjoint through the autograd API (200k -> 50k, p = 8)")
+        adj = adjoint_api_bench(dev, steps=max(3, min(args.steps, 10)))
+
+    progress("headline: stage times and roofline")
     pipes = pipe_peaks_measured(dev)
     stage_ms, roof, roof_m2l = stage_breakdown(w_mx, trav, q_dev, dev, pipe_peaks=pipes)
-    adj = adjoint_bench(dev) if world == 1 else None
-    batch = batched_bench(dev) if world == 1 and not args.no_batch else None
-    helm = helmholtz_bench(dev) if world == 1 and not args.no_helmholtz else None
-    import gc
-    gc.collect()
-    uni = uniform_bench(dev, cpu=not args.no_cpu_baseline) if world == 1 else None
-    mat = matrix_bench(dev) if world == 1 else None
 
     value = world * args.npoints / (ms_mx * 1e-3) / 1e6
-    line = {
+    return {
         "metric": METRIC, "value": value, "unit": "Mpts/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mx,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32/3xtf32 with f64 offsets and sums", "data": "synthetic",
         "config": {
             "workload": f"laplace3d_fmm_sphere_plummer_n{args.npoints}_p{args.order}",
             "npoints": args.npoints, "order": args.order,
             "max_particles_in_box": MAX_PARTICLES, "exclude_self": True,
             "precision": "mixed (FP32 near field, M2P, P2L with FP64 offsets and sums; "
-                         "3xTF32 tensor-core M2L and M2M; FP64 elsewhere)",
+                         "3xTF32 tensor-core M2L; FP64 elsewhere)",
+            "accuracy_target": (f"relL2 <= 1e-6 reached at p = {at['order']}, leaf "
+                                f"{ACCURACY_MAX_PARTICLES} (accuracy_target)") if at else None,
             "l2": "flushed between steps (256 MB write outside the timed events)",
             "parallelism": f"replicas x{world}",
             "launch": "drive_fmm replaying a CUDA graph of the whole evaluation "
-                      "(wrangler cuda_graph=True); eager timing beside it",
+                      "(wrangler cuda_graph=True); kernel-by-kernel timing beside it",
             "tree_build_s": round(t_tree, 3), "setup_s": round(t_setup, 3),
         },
         "eager": {"ms_per_step": ms_eager,
                   "value": world * args.npoints / (ms_eager * 1e-3) / 1e6},
-        "accuracy": {"relL2_mixed": err_mx, "relL2_fp64": err_64, "targets_sampled": len(sample),
+        "accuracy": {"relL2_mixed": err_mx, "relL2_fp64": err_64,
+                     "targets_sampled": len(sample),
                      "reference": "FP64 direct sum (GPU kernel sumpy_p2p_direct_f64)"},
         "fp64": {"value": (world * args.npoints / (ms_64 * 1e-3) / 1e6) if ms_64 else None,
                  "ms_per_step": ms_64},
         "mixed_over_fp64": (ms_64 / ms_mx) if ms_64 else None,
-        "fp64_own_best_tree": fp64_best,
-        "order_for_accuracy_target": at_target,
-        "mixed_over_fp64_own_best": (fp64_best["ms_per_step"] / ms_mx) if fp64_best else None,
-        "mixed_over_fp64_at_accuracy_target": (at_target[-1].get("mixed_over_fp64")
-                                               if at_target else None),
+        "accuracy_target": at,
+        "mixed_over_fp64_at_accuracy_target": at.get("mixed_over_fp64") if at else None,
         "adjoint_forward_ratio": adj["ratio"] if adj else None,
         "adjoint": adj,
-        "batched": batch,
-        "helmholtz": helm,
-        "uniform_p6": uni,
-        "p2p_matrix": mat,
         "stage_ms": stage_ms,
         "roofline": roof,
         "roofline_m2l": roof_m2l,
         "measured_pipe_peaks": pipes,
-        "cpu_baseline": cpu_line,
+        "cpu_baseline": cpu_line if cpu_line else {"value": None, "why": cpu_why},
         "e2e": {"value": world * args.npoints / (ms_e2e * 1e-3) / 1e6, "unit": "Mpts/s",
+                "ms_per_step": ms_e2e,
                 "h2d_bytes_per_step": 8 * args.npoints, "d2h_bytes_per_step": 8 * args.npoints},
         "gpu_launches": launches,
         "clocks": clocks,
+        "skipped": list(budget.skipped),
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
 
 
-def adjoint_bench(dev, steps=3, ns=200_000, nt=50_000, order=8):
-    """Backward/forward time ratio of the differentiable potential: 200k
-    sources on the unit sphere perturbed radially by 0.05*N(0,1), 50k
-    targets uniform in the shell 2 <= r <= 3, p = 8, mixed precision, loss
-    0.5*|phi - phi_ref|^2 with phi_ref the FP64 direct sum at the unperturbed
-    positions. Forward = one FMM; backward = transposed-traversal FMM with
-    gradient-form evaluation (strength and source-position gradients). Trees
-    and schedules are built before timing; times are CUDA events."""
+def accuracy_target(args, dev, pts, q_dev, ti, timer, rel):
+    """The headline workload at the lowest order that meets relL2 <= 1e-6
+    (ACCURACY_ORDER, one more if it does not), mixed and FP64 forms on one
+    leaf-128 tree, timed like the headline."""
     import torch
-    from sumpy_b200 import P2P, LaplaceKernel, drive_fmm
-    from sumpy_b200.adjoint import transpose_traversal
-    from sumpy_b200.autograd import _Config, _wrangler
+    from sumpy_b200 import drive_fmm
     from sumpy_b200.tree import build_all
-    rng = np.random.default_rng(7)
+    progress(f"headline: accuracy target (p = {ACCURACY_ORDER}, leaf {ACCURACY_MAX_PARTICLES})")
+    tree_a, trav_a, tcls_a = build_all(pts, None, ACCURACY_MAX_PARTICLES)
+    out = None
+    for p_hi in (ACCURACY_ORDER, ACCURACY_ORDER + 1):
+        w_p = make_wrangler(ti, trav_a, tcls_a, p_hi, "mixed", dev)
+        for _ in range(max(1, args.warmup)):
+            drive_fmm(None, w_p, [q_dev])
+        ms_p, _ = timer(lambda: drive_fmm(None, w_p, [q_dev]), args.steps)
+        e_p = rel(w_p)
+        w_p.check_status()
+        out = {"order": p_hi, "max_particles_in_box": ACCURACY_MAX_PARTICLES,
+               "ms_per_step": ms_p, "value": args.npoints / (ms_p * 1e-3) / 1e6,
+               "relL2_mixed": e_p, "meets_1e-6": e_p <= 1e-6}
+        del w_p
+        if e_p <= 1e-6:
+            break
+    if not args.no_fp64:
+        progress(f"headline: accuracy target, FP64 form at p = {out['order']}")
+        w_f = make_wrangler(ti, trav_a, tcls_a, out["order"], "fp64", dev)
+        for _ in range(max(1, args.warmup)):
+            drive_fmm(None, w_f, [q_dev])
+        ms_f, _ = timer(lambda: drive_fmm(None, w_f, [q_dev]), args.steps)
+        e_f = rel(w_f)
+        w_f.check_status()
+        out.update({"fp64_ms_per_step": ms_f,
+                    "fp64_value": args.npoints / (ms_f * 1e-3) / 1e6, "relL2_fp64": e_f,
+                    "mixed_over_fp64": ms_f / out["ms_per_step"]})
+        del w_f
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_only(args, dev):
+    """One workload alone (profiling): --only mixed|fp64 run the headline
+    workload in that form (graph replay, or --eager)."""
+    import torch
+    from sumpy_b200 import drive_fmm
+    if args.only == "batch":
+        return batched_bench(dev, steps=args.steps, warmup=args.warmup)
+    if args.only == "matrix":
+        return matrix_bench(dev, steps=args.steps, warmup=args.warmup)
+    if args.only == "uniform":
+        return uniform_bench(dev, steps=args.steps, warmup=args.warmup, cpu=False)
+    if args.only == "adjoint":
+        return adjoint_api_bench(dev, steps=args.steps, warmup=args.warmup)
+    if args.only == "helmholtz":
+        precs = (("mixed", "fp64") if args.helmholtz_precision == "both"
+                 else (args.helmholtz_precision,))
+        return helmholtz_bench(dev, steps=args.steps, warmup=args.warmup,
+                               npoints=args.helmholtz_npoints, precisions=precs)
+    pts, q, tree, trav, tcls, ti, t_tree = laplace_setup(dev, args.npoints, MAX_PARTICLES)
+    w = make_wrangler(ti, trav, tcls, args.order, args.only, dev, graph=not args.eager)
+    q_dev = torch.as_tensor(q, device=dev)
+    for _ in range(max(1, args.warmup)):
+        drive_fmm(None, w, [q_dev])
+    ms, _ = StepTimer(dev, 1)(lambda: drive_fmm(None, w, [q_dev]), args.steps)
+    w.check_status()
+    return {"ms_per_step": ms, "Mpts_s": args.npoints / (ms * 1e-3) / 1e6}
+
+
+def fp64_best_tree_bench(dev, args):
+    """The FP64 form on its own fastest tree (larger leaves favour its M2L)."""
+    import torch
+    from sumpy_b200 import drive_fmm
+    pts, q, tree, trav, tcls, ti, _ = laplace_setup(dev, args.npoints, FP64_MAX_PARTICLES)
+    w = make_wrangler(ti, trav, tcls, args.order, "fp64", dev)
+    q_dev = torch.as_tensor(q, device=dev)
+    for _ in range(max(1, args.warmup)):
+        drive_fmm(None, w, [q_dev])
+    ms, _ = StepTimer(dev, 1)(lambda: drive_fmm(None, w, [q_dev]), args.steps)
+    return {"max_particles_in_box": FP64_MAX_PARTICLES, "ms_per_step": ms,
+            "value": args.npoints / (ms * 1e-3) / 1e6}
+
+
+def adjoint_problem(ns=200_000, nt=50_000, seed=7):
+    """The differentiable-potential workload: ns sources on the unit sphere
+    perturbed radially by 0.05*N(0,1), nt targets uniform in the shell
+    2 <= r <= 3, strengths N(0,1); also the unperturbed sphere points."""
+    rng = np.random.default_rng(seed)
     g = rng.standard_normal((3, ns))
     u = g / np.linalg.norm(g, axis=0)
     src = (1 + 0.05 * rng.standard_normal(ns)) * u
@@ -537,48 +715,72 @@ def adjoint_bench(dev, steps=3, ns=200_000, nt=50_000, order=8):
     d /= np.linalg.norm(d, axis=0)
     tgt = np.cbrt(8 + 19 * rng.random(nt)) * d
     q = rng.standard_normal(ns)
+    return src, tgt, q, u
+
+
+def adjoint_api_bench(dev, steps=5, warmup=3, ns=200_000, nt=50_000, order=8):
+    """Backward/forward time of the differentiable potential through the API
+    users call, :class:`sumpy_b200.autograd.LaplaceFMM` (mixed, p = 8): 200k
+    perturbed sphere sources, 50k shell targets, loss 0.5*|phi - phi_ref|^2
+    with phi_ref the FP64 direct sum at the unperturbed positions. A step is
+    ``phi = fmm(q, x_s, x_t)`` and the loss (forward) then ``loss.backward()``
+    (strength and source-position gradients); strengths and source positions
+    are fresh leaf tensors each step. The first call builds the geometry;
+    later calls find every point inside its box and reuse it. CUDA events
+    around each part; gradients checked against the FP64 direct-sum
+    gradients."""
+    import torch
+    from sumpy_b200 import P2P, LaplaceKernel
+    from sumpy_b200.autograd import LaplaceFMM
+    src, tgt, q, u = adjoint_problem(ns, nt)
     knl = [LaplaceKernel(3)]
     (phi_ref,) = P2P(knl)(None, tgt, u, (q,), device=dev)
-    cfg = _Config(order, ADJOINT_MAX_PARTICLES, "mixed", dev)
-    tree, trav, tcls = build_all(src, tgt, ADJOINT_MAX_PARTICLES)
-    tree_t, trav_t, tcls_t = transpose_traversal(tree, trav, tcls)
-    wf = _wrangler(cfg, tree, trav, tcls, False, gradient=False)
-    wb = _wrangler(cfg, tree_t, trav_t, tcls_t, False, gradient=True)
-    qd = torch.as_tensor(q, device=dev)
+    fmm = LaplaceFMM(order=order, max_particles_in_box=ADJOINT_MAX_PARTICLES,
+                     precision="mixed", device=dev)
+    q0 = torch.as_tensor(q, device=dev)
+    s0 = torch.as_tensor(src, device=dev)
+    t0 = torch.as_tensor(tgt, device=dev)
 
-    def fwd():
-        return drive_fmm(None, wf, [qd])[0]
+    def forward():
+        qv = q0.clone().requires_grad_(True)
+        sv = s0.clone().requires_grad_(True)
+        phi = fmm(qv, sv, t0)
+        loss = 0.5 * ((phi - phi_ref) ** 2).sum()
+        return loss, qv, sv, phi
 
-    phi = fwd()
-    gd = (phi - phi_ref).contiguous()
-
-    def bwd():
-        out = drive_fmm(None, wb, [gd])
-        return out[0], qd * torch.stack(out[1:4])
-
-    def tm(fn):
-        for _ in range(2):
-            fn()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(steps):
-            fn()
-        e1.record()
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / steps
-
-    t_f, t_b = tm(fwd), tm(bwd)
-    gq, gsrc = bwd()
-    gdn = gd.cpu().numpy()
+    tb = time.perf_counter()
+    loss, qv, sv, phi = forward()
+    loss.backward()
+    torch.cuda.synchronize()
+    t_first = time.perf_counter() - tb
+    for _ in range(warmup):
+        loss, qv, sv, phi = forward()
+        loss.backward()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)]
+    torch.cuda.synchronize()
+    for e in evs:
+        e[0].record()
+        loss, qv, sv, phi = forward()
+        e[1].record()
+        loss.backward()
+        e[2].record()
+    torch.cuda.synchronize()
+    t_f = sum(e[0].elapsed_time(e[1]) for e in evs) / steps
+    t_b = sum(e[1].elapsed_time(e[2]) for e in evs) / steps
+    gdn = (phi - phi_ref).detach().cpu().numpy()
     psi = P2P(knl, gradient=True)(None, src, tgt, (gdn,), device=dev)
     gq_ref = psi[0]
-    gsrc_ref = qd * torch.stack(psi[1:4])
+    gsrc_ref = q0 * torch.stack(psi[1:4])
     rel = lambda a, b: float((a - b).norm() / b.norm())
     return {"forward_ms": t_f, "backward_ms": t_b, "ratio": t_b / t_f,
-            "grad_strength_relL2_vs_direct": rel(gq, gq_ref),
-            "grad_source_pos_relL2_vs_direct": rel(gsrc, gsrc_ref),
-            "workload": f"sphere(perturbed) {ns} sources -> shell {nt} targets, p={order}, mixed"}
+            "api": "sumpy_b200.autograd.LaplaceFMM (torch.autograd.Function), "
+                   "forward = fmm + loss, backward = loss.backward()",
+            "first_call_s": round(t_first, 3),
+            "geometry_builds": fmm.geometry_builds, "geometry_reuses": fmm.geometry_reuses,
+            "grad_strength_relL2_vs_direct": rel(qv.grad, gq_ref),
+            "grad_source_pos_relL2_vs_direct": rel(sv.grad, gsrc_ref),
+            "workload": f"sphere(perturbed) {ns} sources -> shell {nt} targets, p={order}, "
+                        f"mixed, leaf {ADJOINT_MAX_PARTICLES}"}
 
 
 def batch_problems(nproblems=512):

@@ -301,6 +301,19 @@ int sumpy_class_gemm_tf32x3(
     const float *src_hi, const float *src_lo, int32_t tgt_base_ibox, double *tgt_expansions,
     int32_t *status, void *stream);
 
+/* Budget, in SM clock cycles (clock64), of every barrier wait in the
+ * tensor-core kernels (the M2L above, the class GEMMs and the Helmholtz
+ * M2L), read at each launch. A wait that runs out sets the abort flag of its
+ * CTA; the CTA lets the work it has in flight finish, frees its tensor
+ * memory, writes 1 (timeout) to the launch's status word and returns, so
+ * the context stays usable. cycles <= 0 restores the default (4e9, about
+ * two seconds). Budgets below 1e6 cycles poll the barriers without letting
+ * the hardware suspend the waiting thread. No counterpart in sumpy (its
+ * kernels have no waits); it exists so that tests and callers with a
+ * deadline can bound a launch. Process-wide; returns SUMPY_OK. */
+int sumpy_set_tc_wait_cycles(int64_t cycles);
+int64_t sumpy_get_tc_wait_cycles(void);
+
 /* Same M2L as sumpy_m2l_translation_classes_tf32x3, for callers that cannot
  * allocate device memory while they run (a host application with a fixed
  * device-memory budget, an allocation-free real-time loop, code where an
@@ -310,10 +323,15 @@ int sumpy_class_gemm_tf32x3(
  * and keeps their TF32 planes in a device array built into the library
  * (8 MiB per GPU, held until exit) instead of caller memory; allocates
  * nothing. Limit: (nsrc_boxes + 1) * k_pad <= 1,048,576 and k_pad <= 128
- * (8,191 boxes at order <= 10); larger requests return SUMPY_EINVAL. The
- * first call on a device looks up the array's device address; make that
- * call before any stream capture. All calls share the array: calls that
- * overlap on the GPU race and must be serialised by the caller. */
+ * (8,191 boxes at order <= 10); larger requests return SUMPY_EINVAL. Each
+ * call looks up the array's device address in the current context. With
+ * CUDA's default lazy module loading, the first call into the tensor-core
+ * M2L on a device (this entry point or the regular one) loads the module
+ * and with it reserves the 8 MiB: make one such call while initialising (or
+ * set CUDA_MODULE_LOADING=EAGER), and before any stream capture. All calls
+ * share the array and it keeps the last call's contents (the zero row the
+ * kernel reads is cleared on every call): calls that overlap on the GPU
+ * race and must be serialised by the caller. */
 int sumpy_m2l_translation_classes_tf32x3_noalloc(
     int order, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
     const int32_t *item_group_end, int32_t tile_width, const int32_t *tile_targets,

@@ -24,6 +24,9 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 #define MAXP 32
 
@@ -195,6 +198,16 @@ static void laplace_derivs(const double x[3], double rscale, int maxi0, int maxd
 /* ------------------------------------------------------------------ */
 
 int oracle_ncoeff(int p) { return (p + 1) * (p + 1); }
+
+/* threads a parallel region of this library runs on (the CPU baseline's core count) */
+int oracle_num_threads(void)
+{
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
 int oracle_nfull(int p) { return (p + 1) * (p + 2) * (p + 3) / 6; }
 
 void oracle_stored_ids(int p, int *ids)

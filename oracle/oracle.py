@@ -47,6 +47,11 @@ def lib():
     return _lib
 
 
+def num_threads() -> int:
+    """OpenMP threads the oracle's parallel regions use."""
+    return int(lib().oracle_num_threads())
+
+
 def _ptr(a):
     if a is None:
         return None

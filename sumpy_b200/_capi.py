@@ -44,6 +44,8 @@ SIGNATURES = {
     "sumpy_m2l_translation_classes_f64": [cint, i32, ptr, ptr, ptr, i32, ptr, ptr, ptr, ptr,
                                           i32, ptr, i32, ptr, i32, ptr, ptr],
     "sumpy_split_tf32x2": [i64, i32, i32, ptr, i32, i32, ptr, ptr, ptr],
+    "sumpy_set_tc_wait_cycles": [i64],
+    "sumpy_get_tc_wait_cycles": [],
     "sumpy_m2l_translation_classes_tf32x3": [cint, i32, ptr, ptr, ptr, i32, ptr, ptr, ptr, ptr,
                                              i32, ptr, ptr, i32, i32, i32, i32, ptr, ptr, i32,
                                              ptr, ptr, ptr],
@@ -125,6 +127,7 @@ SIGNATURES = {
 _RESTYPES = {
     "sumpy_version": cint,
     "sumpy_last_error": ctypes.c_char_p,
+    "sumpy_get_tc_wait_cycles": i64,
 }
 
 _lib = None

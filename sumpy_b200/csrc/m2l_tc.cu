@@ -30,6 +30,7 @@
 // budget; on expiry the kernel records an error in *status, lets work in
 // flight finish, frees its tensor memory and returns.
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <mutex>
 #include <string>
@@ -71,7 +72,12 @@ constexpr int STAGE = 4 * PLANE;           // A_hi, A_lo, B_hi, B_lo
 constexpr int TC_SMEM = TC_STAGES * STAGE + 1024 /* alignment slack */ + 256 /* barriers */;
 static_assert(TC_SMEM <= 227 * 1024, "shared memory per CTA");
 constexpr uint32_t TMEM_COLS = 256;         // two 128-column accumulators
-constexpr long long WAIT_CYCLES = 4000000000LL;  // ~2 s at 2 GHz
+// default budget of every wait (~2 s at 2 GHz); a process can lower it with
+// sumpy_set_tc_wait_cycles (tests make waits expire this way)
+constexpr long long WAIT_CYCLES = 4000000000LL;
+// budgets below this poll the barrier without suspending the thread, so that
+// a short budget is measured in cycles rather than in hardware suspend windows
+constexpr long long SHORT_WAIT = 1000000LL;
 
 enum { ST_TIMEOUT_MMA = 1 };
 
@@ -103,6 +109,18 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t addr, uint32_t parity)
     uint32_t ok;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_test_wait(uint32_t addr, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
         " selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(ok)
         : "r"(addr), "r"(parity)
@@ -169,6 +187,7 @@ struct TcArgs {
     int32_t tbase;
     double *tgt;
     int32_t *status;
+    long long wait_cycles;      // budget of each barrier wait (clock64 cycles)
 };
 
 __device__ __forceinline__ void mbar_arrive(uint32_t addr)
@@ -207,12 +226,14 @@ __device__ __forceinline__ void tma_gather4(uint32_t dst, const CUtensorMap *map
 }
 
 // bounded wait that also gives up when another thread has aborted
-__device__ bool mbar_wait_or_abort(uint32_t addr, uint32_t parity, volatile int *abort_flag)
+__device__ bool mbar_wait_or_abort(uint32_t addr, uint32_t parity, volatile int *abort_flag,
+                                   long long limit)
 {
     const long long t0 = clock64();
-    while (!mbar_try_wait(addr, parity)) {
+    const bool poll = limit < SHORT_WAIT;
+    while (!(poll ? mbar_test_wait(addr, parity) : mbar_try_wait(addr, parity))) {
         if (*abort_flag) return false;
-        if (clock64() - t0 > WAIT_CYCLES) {
+        if (clock64() - t0 > limit) {
             *abort_flag = 1;
             return false;
         }
@@ -336,7 +357,7 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
                 if (lane == 0) cls_nxt = a.group_class[g0 + gi + 1];
             }
             bool ok = true;
-            if (use > 0) ok = mbar_wait_or_abort(empty_bar + 8 * s, (use - 1) & 1, abort_flag);
+            if (use > 0) ok = mbar_wait_or_abort(empty_bar + 8 * s, (use - 1) & 1, abort_flag, a.wait_cycles);
             if (__any_sync(FULL, !ok || *abort_flag)) break;
             const int k0 = (kcb + kc) * TC_KC;
             const uint32_t st = base + s * STAGE;
@@ -390,7 +411,7 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
                 if (threadIdx.x == 0) cls_nxt = a.group_class[g0 + gi + 1];
             }
             bool ok = true;
-            if (use > 0) ok = mbar_wait_or_abort(empty_bar + 8 * s, (use - 1) & 1, abort_flag);
+            if (use > 0) ok = mbar_wait_or_abort(empty_bar + 8 * s, (use - 1) & 1, abort_flag, a.wait_cycles);
             if (loaders_sync_or(!ok || *abort_flag)) break;
             const int k0 = (kcb + kc) * TC_KC;
             const uint32_t st = base + s * STAGE;
@@ -428,11 +449,11 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
         if (lane == 0) {
             for (int it = 0; it < total; ++it) {
                 const int s = it % TC_STAGES, use = it / TC_STAGES;
-                if (!mbar_wait_or_abort(full_bar + 8 * s, use & 1, abort_flag)) break;
+                if (!mbar_wait_or_abort(full_bar + 8 * s, use & 1, abort_flag, a.wait_cycles)) break;
                 const int gi = it / nkc, kc = it % nkc;
                 const int acc = gi & 1;
                 if (kc == 0 && gi >= 2 &&
-                    !mbar_wait_or_abort(acce_bar + 8 * acc, ((gi >> 1) - 1) & 1, abort_flag))
+                    !mbar_wait_or_abort(acce_bar + 8 * acc, ((gi >> 1) - 1) & 1, abort_flag, a.wait_cycles))
                     break;
                 tc_fence_after();
                 const uint32_t st = base + s * STAGE;
@@ -462,7 +483,7 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
         bool ok = true;
         for (int gi = 0; gi < ng && ok; ++gi) {
             const int acc = gi & 1;
-            ok = mbar_wait_or_abort(accf_bar + 8 * acc, (gi >> 1) & 1, abort_flag);
+            ok = mbar_wait_or_abort(accf_bar + 8 * acc, (gi >> 1) & 1, abort_flag, a.wait_cycles);
             if (!ok) break;
             tc_fence_after();
             const uint32_t taddr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(acc * TC_TW + half * 64);
@@ -551,6 +572,9 @@ int sumpy_split_tf32x2(int64_t nmat, int32_t rows, int32_t cols, const double *i
     return check_launch("split_tf32x2_kernel");
 }
 
+// budget of the tensor-core kernels' barrier waits, read at each launch
+static std::atomic<long long> g_wait_cycles{WAIT_CYCLES};
+
 using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
                                     const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
                                     const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
@@ -616,17 +640,13 @@ static int m2l_tf32x3_launch(
     if ((reinterpret_cast<uintptr_t>(mats_hi) | reinterpret_cast<uintptr_t>(mats_lo) |
          reinterpret_cast<uintptr_t>(src_hi) | reinterpret_cast<uintptr_t>(src_lo)) & 15)
         return bad_arg("m2l_tf32x3: operand planes must be 16-byte aligned");
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return bad_arg("m2l_tf32x3: no device");
-    static bool attr_set[64] = {};
-    if (!attr_set[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(m2l_tf32x3_kernel,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
-        if (e != cudaSuccess) {
-            set_last_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
-            return SUMPY_ELAUNCH;
-        }
-        attr_set[dev] = true;
+    // set on every launch (a cheap host call): an attribute remembered per
+    // device would be lost with a context that was torn down and recreated
+    cudaError_t e = cudaFuncSetAttribute(m2l_tf32x3_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+    if (e != cudaSuccess) {
+        set_last_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+        return SUMPY_ELAUNCH;
     }
     CUtensorMap ma_hi, ma_lo, mb_hi, mb_lo;
     const uint64_t adims[3] = {(uint64_t)k_pad, (uint64_t)rows_pad, (uint64_t)nclasses};
@@ -644,6 +664,7 @@ static int m2l_tf32x3_launch(
     a.src_hi = src_hi; a.src_lo = src_lo;
     a.src_row_base = src_base_ibox; a.zero_row = src_nrows - 1;
     a.tbase = tgt_base_ibox; a.tgt = tgt_expansions; a.status = status;
+    a.wait_cycles = g_wait_cycles.load(std::memory_order_relaxed);
     dim3 grid(nitems, rows_pad / TC_M, k_split);
     m2l_tf32x3_kernel<<<grid, TC_THREADS, TC_SMEM, as_stream(stream)>>>(a, ma_hi, ma_lo, mb_hi,
                                                                         mb_lo);
@@ -651,6 +672,14 @@ static int m2l_tf32x3_launch(
 }
 
 extern "C" {
+
+int sumpy_set_tc_wait_cycles(int64_t cycles)
+{
+    g_wait_cycles.store(cycles > 0 ? (long long)cycles : WAIT_CYCLES, std::memory_order_relaxed);
+    return SUMPY_OK;
+}
+
+int64_t sumpy_get_tc_wait_cycles(void) { return g_wait_cycles.load(std::memory_order_relaxed); }
 
 int sumpy_m2l_translation_classes_tf32x3(
     int order, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
@@ -719,8 +748,13 @@ int sumpy_helmholtz_m2l_translation_classes_tf32x3(
 //
 // Limits: (nsrc_boxes + 1) * k_pad <= NOALLOC_ROWS * NOALLOC_KPAD floats per
 // plane, i.e. 8,191 source boxes at k_pad = 128 (orders <= 10); larger
-// requests are rejected. Every GPU that loads this library holds the array
-// (8 MiB) until the process exits. All calls share it and it keeps the
+// requests are rejected. Every GPU that loads this library's module holds
+// the array (8 MiB) until the process exits; with CUDA's default lazy module
+// loading the module, and with it the array, is loaded by the first call
+// into this file's kernels on that device (this entry point or the regular
+// tensor-core M2L), so a caller with a fixed budget makes one such call
+// while it initialises (or sets CUDA_MODULE_LOADING=EAGER) and makes it
+// before any stream capture. All calls share the array and it keeps the
 // previous call's contents; the zero row the kernel needs is cleared on
 // every call. Calls that overlap on the GPU (different streams, or another
 // thread) race on the array and must be serialised by the caller.
@@ -728,24 +762,21 @@ constexpr int64_t NOALLOC_ROWS = 8192;
 constexpr int64_t NOALLOC_KPAD = 128;
 static __device__ __align__(256) float g_noalloc_planes[2 * NOALLOC_ROWS * NOALLOC_KPAD];
 
-// Device address of g_noalloc_planes on the current device, looked up once
-// per device (host code cannot use the symbol's name as a device address).
-static float *noalloc_planes(int dev)
+// Device address of g_noalloc_planes in the current device's context. Host
+// code cannot use the symbol's name as a device address, so every call looks
+// the address up (it allocates nothing once the module is loaded); nothing is
+// cached, so a context that was torn down and created again is never used
+// through a stale address.
+static float *noalloc_planes()
 {
-    static float *addr[64] = {};
-    static std::mutex lock;
-    std::lock_guard<std::mutex> guard(lock);
-    if (!addr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_planes);
-        if (e != cudaSuccess) {
-            set_last_error(std::string("m2l_tf32x3_noalloc: cudaGetSymbolAddress: ") +
-                           cudaGetErrorString(e));
-            return nullptr;
-        }
-        addr[dev] = static_cast<float *>(p);
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_planes);
+    if (e != cudaSuccess) {
+        set_last_error(std::string("m2l_tf32x3_noalloc: cudaGetSymbolAddress: ") +
+                       cudaGetErrorString(e));
+        return nullptr;
     }
-    return addr[dev];
+    return static_cast<float *>(p);
 }
 
 int sumpy_m2l_translation_classes_tf32x3_noalloc(
@@ -770,10 +801,7 @@ int sumpy_m2l_translation_classes_tf32x3_noalloc(
         return SUMPY_EINVAL;
     }
     if (nsrc_boxes > 0 && !src_expansions) return bad_arg("m2l_tf32x3_noalloc: null pointer argument");
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
-        return bad_arg("m2l_tf32x3_noalloc: no device");
-    float *hi = noalloc_planes(dev);
+    float *hi = noalloc_planes();
     if (!hi) return SUMPY_ELAUNCH;
     float *lo = hi + NOALLOC_ROWS * NOALLOC_KPAD;
     cudaStream_t st = as_stream(stream);

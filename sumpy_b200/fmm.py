@@ -415,6 +415,22 @@ class SumpyExpansionWrangler:
             raise ValueError("exclude_self needs a tree whose sources are its targets")
         return g
 
+    def set_positions(self, sources=None, targets=None):
+        """Overwrite the device coordinates of the sources and/or targets in
+        place ((3, n) float64 tensors in tree order). Every stage reads the
+        coordinates from these buffers, and the work plans, operator tables
+        and a captured CUDA graph depend only on the boxes, so they stay
+        valid as long as each point stays inside the box it was sorted
+        into; the caller checks that (see :mod:`sumpy_b200.autograd`)."""
+        g = self._geom
+        for key, new in (("sources", sources), ("targets", targets)):
+            if new is None:
+                continue
+            if tuple(new.shape) != tuple(g[key].shape):
+                raise ValueError(f"{key}: shape {tuple(new.shape)}, tree has "
+                                 f"{tuple(g[key].shape)}")
+            g[key].copy_(new)
+
     @property
     def _scale(self):
         return self.tree_indep.target_kernels[0].global_scaling_const
@@ -1046,9 +1062,11 @@ class SumpyExpansionWrangler:
     # }}}
 
     def check_status(self):
-        """Raise if a kernel reported an internal error (synchronises)."""
+        """Raise if a kernel reported an internal error (synchronises); the
+        status is cleared, so the next evaluation starts clean."""
         code = int(self._status.item())
         if code:
+            self._status.zero_()
             raise RuntimeError(f"a tensor-core M2L wait expired (status {code})")
 
     # }}}

@@ -1,0 +1,181 @@
+"""The differentiable potential at its full size, and the geometry cache of
+the autograd API that makes it cheap.
+
+Workload: 200,000 sources on the unit sphere perturbed radially by
+0.05*N(0,1), 50,000 targets uniform in the shell 2 <= r <= 3, p = 8, loss
+0.5*|phi - phi_ref|^2 with phi_ref the FP64 direct sum at the unperturbed
+positions. Gradients with respect to strengths and source positions are
+checked against central finite differences (h = 1e-4, FP64) of the same
+loss on 64 random coordinates (32 strengths, 32 source coordinates).
+
+With the boxes fixed (every displaced point stays in its box, so the
+geometry is reused), the FMM is a smooth function of the positions and the
+backward is the exact derivative of the forward, so FD agrees to its own
+truncation and rounding error (well under 1e-6 for the FP64 form). The
+mixed form's gradient is compared with FD of the FP64 loss, which adds the
+mixed-vs-FP64 difference.
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from tests._pointsets import sphere_plummer
+
+pytestmark = pytest.mark.gpu
+
+
+def shell_problem(ns, nt, seed=7):
+    rng = np.random.default_rng(seed)
+    g = rng.standard_normal((3, ns))
+    u = g / np.linalg.norm(g, axis=0)
+    src = (1 + 0.05 * rng.standard_normal(ns)) * u
+    d = rng.standard_normal((3, nt))
+    d /= np.linalg.norm(d, axis=0)
+    tgt = np.cbrt(8 + 19 * rng.random(nt)) * d
+    q = rng.standard_normal(ns)
+    return src, tgt, q, u
+
+
+def test_geometry_reused_inside_boxes_and_rebuilt_outside(cuda_device):
+    from sumpy_b200.autograd import LaplaceFMM
+    dev = cuda_device
+    src, tgt, q, _ = shell_problem(6000, 2000, seed=3)
+    fmm = LaplaceFMM(order=6, max_particles_in_box=24, precision="fp64", device=dev)
+    qt = torch.as_tensor(q, device=dev)
+    tt = torch.as_tensor(tgt, device=dev)
+    fmm(qt, torch.as_tensor(src, device=dev), tt)
+    assert (fmm.geometry_builds, fmm.geometry_reuses) == (1, 0)
+    # a displacement far below any box size keeps every point in its box
+    moved = src + 1e-11 * np.random.default_rng(1).standard_normal(src.shape)
+    fmm(qt, torch.as_tensor(moved, device=dev), tt)
+    assert (fmm.geometry_builds, fmm.geometry_reuses) == (1, 1)
+    # a point moved across the whole configuration leaves its box
+    far = src.copy()
+    far[:, 0] = -far[:, 0]
+    fmm(qt, torch.as_tensor(far, device=dev), tt)
+    assert (fmm.geometry_builds, fmm.geometry_reuses) == (2, 1)
+    fmm(qt, torch.as_tensor(far, device=dev), tt, rebuild=True)
+    assert fmm.geometry_builds == 3
+
+
+@pytest.mark.parametrize("self_eval", [False, True])
+def test_reused_geometry_matches_oracle_on_moved_points(cuda_device, self_eval):
+    """Moved points on the kept boxes: the FP64 result equals the oracle
+    run on the same boxes with the moved coordinates (1e-12)."""
+    from sumpy_b200.autograd import LaplaceFMM
+    dev = cuda_device
+    if self_eval:
+        src, tgt = sphere_plummer(5000, 9), None
+        q = np.random.default_rng(4).standard_normal(5000)
+    else:
+        src, tgt, q, _ = shell_problem(5000, 2000, seed=5)
+    fmm = LaplaceFMM(order=6, max_particles_in_box=20, precision="fp64", device=dev)
+    qt = torch.as_tensor(q, device=dev)
+    tt = None if tgt is None else torch.as_tensor(tgt, device=dev)
+    fmm(qt, torch.as_tensor(src, device=dev), tt)
+    geo = fmm._cache.geo
+    # move every source by a random fraction of its distance to its box walls
+    s_sorted = geo.src_sorted
+    lo, hi = geo.src_lo, geo.src_hi
+    rng = np.random.default_rng(6)
+    frac = torch.as_tensor(rng.uniform(0.2, 0.8, s_sorted.shape), device=dev)
+    new_sorted = lo + frac * (hi - lo)
+    new = torch.empty_like(new_sorted)
+    new[:, geo.src_perm] = new_sorted
+    tt2 = tt
+    if tgt is not None:
+        # targets move too, inside their boxes
+        fr_t = torch.as_tensor(rng.uniform(0.3, 0.7, geo.tgt_sorted.shape), device=dev)
+        new_t_sorted = geo.tgt_lo + fr_t * (geo.tgt_hi - geo.tgt_lo)
+        tt2 = torch.empty_like(new_t_sorted)
+        tt2[:, geo.tgt_perm] = new_t_sorted
+    phi = fmm(qt, new, tt2)
+    assert (fmm.geometry_builds, fmm.geometry_reuses) == (1, 1)
+    tree = geo.tree
+    ns_host = new_sorted.cpu().numpy()
+    nt_host = ns_host if tgt is None else new_t_sorted.cpu().numpy()
+    tree_moved = dataclasses.replace(tree, sources=ns_host, targets=nt_host)
+    ref = O.run_fmm(tree_moved, geo.trav, geo.tcls, 6, q, exclude_self=self_eval)
+    got = phi.cpu().numpy()
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-12
+
+
+def _fd_coordinates(geo, ns, h, rng, count):
+    """``count`` random (axis, source) coordinates whose points stay inside
+    their boxes when displaced by 2h."""
+    lo = geo.src_lo.cpu().numpy()
+    hi = geo.src_hi.cpu().numpy()
+    perm = geo.src_perm.cpu().numpy()
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(len(perm))
+    out = []
+    while len(out) < count:
+        i = int(rng.integers(ns))
+        d = int(rng.integers(3))
+        k = inv[i]
+        x = geo.src_sorted[d, k].item()
+        if x - 2 * h > lo[d, k] and x + 2 * h < hi[d, k]:
+            out.append((d, i))
+    return out
+
+
+def test_adjoint_full_size_matches_finite_differences(cuda_device):
+    from sumpy_b200 import P2P, LaplaceKernel
+    from sumpy_b200.autograd import LaplaceFMM
+    dev = cuda_device
+    h = 1e-4
+    src, tgt, q, u = shell_problem(200_000, 50_000)
+    (phi_ref,) = P2P([LaplaceKernel(3)])(None, tgt, u, (q,), device=dev)
+    tt = torch.as_tensor(tgt, device=dev)
+    q0 = torch.as_tensor(q, device=dev)
+    s0 = torch.as_tensor(src, device=dev)
+    f64 = LaplaceFMM(order=8, max_particles_in_box=32, precision="fp64", device=dev)
+    fmx = LaplaceFMM(order=8, max_particles_in_box=32, precision="mixed", device=dev)
+
+    def grads(fmm):
+        qv = q0.clone().requires_grad_(True)
+        sv = s0.clone().requires_grad_(True)
+        phi = fmm(qv, sv, tt)
+        (0.5 * ((phi - phi_ref) ** 2).sum()).backward()
+        return qv.grad, sv.grad
+
+    gq64, gs64 = grads(f64)
+    gqmx, gsmx = grads(fmx)
+
+    def loss(qq, ss):
+        phi = f64(qq, ss, tt)
+        return 0.5 * float(((phi - phi_ref) ** 2).sum())
+
+    rng = np.random.default_rng(11)
+    idx_q = rng.choice(len(q), 32, replace=False)
+    coords = _fd_coordinates(f64._cache.geo, len(q), h, rng, 32)
+    fd_q, fd_x = [], []
+    for i in idx_q:
+        qp, qm = q0.clone(), q0.clone()
+        qp[i] += h
+        qm[i] -= h
+        fd_q.append((loss(qp, s0) - loss(qm, s0)) / (2 * h))
+    for d, i in coords:
+        sp, sm = s0.clone(), s0.clone()
+        sp[d, i] += h
+        sm[d, i] -= h
+        fd_x.append((loss(q0, sp) - loss(q0, sm)) / (2 * h))
+    # every displaced evaluation reused the geometry of the first call
+    assert f64.geometry_builds == 1
+    fd_q, fd_x = np.array(fd_q), np.array(fd_x)
+
+    def rel(g, fd):
+        return float(np.linalg.norm(g - fd) / np.linalg.norm(fd))
+
+    pick_q = lambda g: g[torch.as_tensor(idx_q, device=dev)].cpu().numpy()
+    pick_x = lambda g: np.array([g[d, i].item() for d, i in coords])
+    e = {"q64": rel(pick_q(gq64), fd_q), "x64": rel(pick_x(gs64), fd_x),
+         "qmx": rel(pick_q(gqmx), fd_q), "xmx": rel(pick_x(gsmx), fd_x)}
+    # FP64: FD truncation (h^2) and the rounding of the loss differences
+    assert e["q64"] < 1e-6, e
+    assert e["x64"] < 1e-6, e
+    assert e["qmx"] < 1e-5, e
+    assert e["xmx"] < 1e-5, e
