@@ -232,25 +232,50 @@ def cpu_baseline_child(args):
 
 # }}}
 class ClockSampler:
-    """SM clock and clock-event reasons sampled DURING a timed region: an NVML
-    thread polling every 5 ms (read-only queries), so that even a region of a
-    few tens of milliseconds gets samples; nvidia-smi at its 100 ms floor as
-    the fallback when NVML is unavailable."""
+    """SM clock and clock-event reasons sampled DURING a timed region by a
+    daemon thread: NVML polled every 5 ms (read-only queries), so that even a
+    region of a few tens of milliseconds gets samples; nvidia-smi at its
+    100 ms floor when NVML is unavailable. Every NVML call, its
+    initialisation included, runs in that thread: the timed thread never
+    waits on NVML, and leaving the region waits at most a few seconds for
+    the sampler to stop (a sampler that did not answer leaves no samples,
+    and the summary says so)."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
     NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, gpu_index, period_s=0.005):
+        import threading
         self.gpu = gpu_index
         self.period = period_s
         self.proc = None
         self.thread = None
         self.samples = []
         self.max_mhz = None
-        self.out = ""
+        self.source = None
+        self.uuid = None
+        self._stop = threading.Event()
 
-    def _nvml_loop(self, nv, h, bits):
+    def _nvml(self):
+        import pynvml as nv
+        nv.nvmlInit()
+        h = None
+        if self.uuid:
+            for cand in (self.uuid, "GPU-" + self.uuid):
+                try:
+                    h = nv.nvmlDeviceGetHandleByUUID(cand)
+                    break
+                except Exception:  # noqa: BLE001
+                    h = None
+        if h is None:
+            h = nv.nvmlDeviceGetHandleByIndex(self.gpu)
+        self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        bits = [("hw_slowdown", nv.nvmlClocksEventReasonHwSlowdown),
+                ("hw_thermal_slowdown", nv.nvmlClocksEventReasonHwThermalSlowdown),
+                ("sw_thermal_slowdown", nv.nvmlClocksEventReasonSwThermalSlowdown),
+                ("sw_power_cap", nv.nvmlClocksEventReasonSwPowerCap)]
+        self.source = "nvml"
         while not self._stop.is_set():
             try:
                 sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
@@ -260,80 +285,67 @@ class ClockSampler:
                 pass
             self._stop.wait(self.period)
 
+    def _smi(self):
+        self.source = "nvidia-smi"
+        self.proc = subprocess.Popen(
+            ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+             "--format=csv,noheader,nounits", "-lms", "100"],
+            stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        for r in self.proc.stdout:
+            if self._stop.is_set():
+                break
+            r = [x.strip() for x in r.split(",")]
+            if len(r) < 9:
+                continue
+            try:
+                sm = float(r[1])
+                self.max_mhz = float(r[2])
+            except ValueError:
+                continue
+            self.samples.append(
+                (sm, [nm for nm, v in zip(self.NAMES, r[5:9]) if v.lower() == "active"]))
+
+    def _run(self):
+        try:
+            self._nvml()
+            return
+        except Exception:  # noqa: BLE001 (no NVML: fall back to nvidia-smi)
+            pass
+        try:
+            self._smi()
+        except Exception:  # noqa: BLE001 (no sampler at all: no samples)
+            pass
+
     def __enter__(self):
         import threading
         try:
-            import pynvml as nv
-            nv.nvmlInit()
             import torch
-            uuid = None
-            try:
-                uuid = str(torch.cuda.get_device_properties(self.gpu).uuid)
-            except Exception:  # noqa: BLE001
-                uuid = None
-            h = None
-            if uuid:
-                for cand in (uuid, "GPU-" + uuid):
-                    try:
-                        h = nv.nvmlDeviceGetHandleByUUID(cand)
-                        break
-                    except Exception:  # noqa: BLE001
-                        h = None
-            if h is None:
-                h = nv.nvmlDeviceGetHandleByIndex(self.gpu)
-            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
-            bits = [("hw_slowdown", nv.nvmlClocksEventReasonHwSlowdown),
-                    ("hw_thermal_slowdown", nv.nvmlClocksEventReasonHwThermalSlowdown),
-                    ("sw_thermal_slowdown", nv.nvmlClocksEventReasonSwThermalSlowdown),
-                    ("sw_power_cap", nv.nvmlClocksEventReasonSwPowerCap)]
-            self._stop = threading.Event()
-            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h, bits),
-                                           daemon=True)
-            self.thread.start()
-            return self
-        except Exception:  # noqa: BLE001 (no NVML: fall back to nvidia-smi)
-            self.thread = None
-        try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except OSError:
-            self.proc = None
+            self.uuid = str(torch.cuda.get_device_properties(self.gpu).uuid)
+        except Exception:  # noqa: BLE001
+            self.uuid = None
+        self.thread = threading.Thread(target=self._run, daemon=True)
+        self.thread.start()
         return self
 
     def __exit__(self, *exc):
-        if self.thread is not None:
-            self._stop.set()
-            self.thread.join(timeout=2)
-            return
+        self._stop.set()
         if self.proc is not None:
             self.proc.terminate()
             try:
-                self.out, _ = self.proc.communicate(timeout=5)
+                self.proc.wait(timeout=3)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
-                self.out, _ = self.proc.communicate()
-            for r in (self.out or "").strip().splitlines():
-                r = [x.strip() for x in r.split(",")]
-                if len(r) < 9:
-                    continue
-                try:
-                    sm = float(r[1])
-                    self.max_mhz = float(r[2])
-                except ValueError:
-                    continue
-                self.samples.append(
-                    (sm, [nm for nm, v in zip(self.NAMES, r[5:9]) if v.lower() == "active"]))
+        self.thread.join(timeout=3)
 
     def summary(self):
-        if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [], "samples": 0}
-        reasons = sorted({n for _, rs in self.samples for n in rs})
-        return {"sm_mhz": float(np.median([s for s, _ in self.samples])),
+        samples = list(self.samples)
+        if not samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [], "samples": 0,
+                    "source": self.source, "note": "the clock sampler took no sample"}
+        reasons = sorted({n for _, rs in samples for n in rs})
+        return {"sm_mhz": float(np.median([s for s, _ in samples])),
                 "sm_max_mhz": self.max_mhz, "reasons": reasons,
-                "samples": len(self.samples),
-                "source": "nvml" if self.thread is not None else "nvidia-smi"}
+                "samples": len(samples), "source": self.source}
 
 
 class Budget:
@@ -511,12 +523,14 @@ def headline(args, dev, rank, world, local_rank, budget, cpu_line, cpu_why):
     w_mx.cuda_graph = True
 
     progress("headline: mixed form, graph replay (the timed value)")
-    for _ in range(args.warmup):
-        drive_fmm(None, w_mx, [q_dev])
-    _capi.launch_counter.reset()
+    # the sampler starts with the warm-up steps, so that it samples from the
+    # first timed step on
     with ClockSampler(local_rank) as clk:
+        for _ in range(args.warmup):
+            drive_fmm(None, w_mx, [q_dev])
+        _capi.launch_counter.reset()
         ms_mx, _ = timer(lambda: drive_fmm(None, w_mx, [q_dev]), args.steps)
-    launches = _capi.launch_counter.value
+        launches = _capi.launch_counter.value
     clocks = clk.summary()
     w_mx.check_status()
 
@@ -718,7 +732,7 @@ def adjoint_problem(ns=200_000, nt=50_000, seed=7):
     return src, tgt, q, u
 
 
-def adjoint_api_bench(dev, steps=5, warmup=3, ns=200_000, nt=50_000, order=8):
+def adjoint_api_bench(dev, steps=5, warmup=3, ns=200_000, nt=50_000, order=8, fd_check=True):
     """Backward/forward time of the differentiable potential through the API
     users call, :class:`sumpy_b200.autograd.LaplaceFMM` (mixed, p = 8): 200k
     perturbed sphere sources, 50k shell targets, loss 0.5*|phi - phi_ref|^2
@@ -772,7 +786,9 @@ def adjoint_api_bench(dev, steps=5, warmup=3, ns=200_000, nt=50_000, order=8):
     gq_ref = psi[0]
     gsrc_ref = q0 * torch.stack(psi[1:4])
     rel = lambda a, b: float((a - b).norm() / b.norm())
+    fd = adjoint_fd_check(dev, fmm, q0, s0, t0, phi_ref, order) if fd_check else None
     return {"forward_ms": t_f, "backward_ms": t_b, "ratio": t_b / t_f,
+            "fd_check": fd,
             "api": "sumpy_b200.autograd.LaplaceFMM (torch.autograd.Function), "
                    "forward = fmm + loss, backward = loss.backward()",
             "first_call_s": round(t_first, 3),
@@ -781,6 +797,74 @@ def adjoint_api_bench(dev, steps=5, warmup=3, ns=200_000, nt=50_000, order=8):
             "grad_source_pos_relL2_vs_direct": rel(sv.grad, gsrc_ref),
             "workload": f"sphere(perturbed) {ns} sources -> shell {nt} targets, p={order}, "
                         f"mixed, leaf {ADJOINT_MAX_PARTICLES}"}
+
+
+def adjoint_fd_check(dev, fmx, q0, s0, t0, phi_ref, order, h=1e-4, ncoord=32, seed=11):
+    """Central differences (h = 1e-4, FP64 forward on the same boxes) of the
+    loss on ``ncoord`` random strengths and ``ncoord`` random source
+    coordinates (points at least 2h inside their boxes, so the geometry is
+    reused), against: the FP64 adjoint, the mixed adjoint applied to the
+    FP64 residual (the backward's own precision), and the mixed end-to-end
+    gradient (which also carries the mixed forward's error, amplified by the
+    small residual). Relative L2 over each set of coordinates."""
+    import torch
+    from sumpy_b200.autograd import LaplaceFMM
+    f64 = LaplaceFMM(order=order, max_particles_in_box=ADJOINT_MAX_PARTICLES,
+                     precision="fp64", device=dev)
+
+    def grads(fmm, seed_residual=None):
+        qv = q0.clone().requires_grad_(True)
+        sv = s0.clone().requires_grad_(True)
+        phi = fmm(qv, sv, t0)
+        if seed_residual is None:
+            (0.5 * ((phi - phi_ref) ** 2).sum()).backward()
+        else:
+            phi.backward(seed_residual)
+        return qv.grad, sv.grad
+
+    g64 = grads(f64)
+    gmx = grads(fmx)
+    r64 = (f64(q0, s0, t0) - phi_ref).detach()
+    gmb = grads(fmx, r64)
+
+    def loss(qq, ss):
+        return 0.5 * float(((f64(qq, ss, t0) - phi_ref) ** 2).sum())
+
+    geo = f64._cache.geo
+    lo, hi = geo.src_lo.cpu().numpy(), geo.src_hi.cpu().numpy()
+    inv = np.empty(len(q0), dtype=np.int64)
+    inv[geo.src_perm.cpu().numpy()] = np.arange(len(q0))
+    xs = geo.src_sorted.cpu().numpy()
+    rng = np.random.default_rng(seed)
+    iq = rng.choice(len(q0), ncoord, replace=False)
+    coords = []
+    while len(coords) < ncoord:
+        i, d = int(rng.integers(len(q0))), int(rng.integers(3))
+        k = inv[i]
+        if lo[d, k] < xs[d, k] - 2 * h and xs[d, k] + 2 * h < hi[d, k]:
+            coords.append((d, i))
+    fd_q, fd_x = [], []
+    for i in iq:
+        qp, qm = q0.clone(), q0.clone()
+        qp[i] += h
+        qm[i] -= h
+        fd_q.append((loss(qp, s0) - loss(qm, s0)) / (2 * h))
+    for d, i in coords:
+        sp, sm = s0.clone(), s0.clone()
+        sp[d, i] += h
+        sm[d, i] -= h
+        fd_x.append((loss(q0, sp) - loss(q0, sm)) / (2 * h))
+    fd_q, fd_x = np.array(fd_q), np.array(fd_x)
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    pq = lambda g: g[0][torch.as_tensor(iq, device=dev)].cpu().numpy()
+    px = lambda g: np.array([g[1][d, i].item() for d, i in coords])
+    return {"h": h, "coordinates": f"{ncoord} strengths + {ncoord} source coordinates",
+            "geometry_builds_fp64": f64.geometry_builds,
+            "fp64": {"strengths": rel(pq(g64), fd_q), "positions": rel(px(g64), fd_x)},
+            "mixed_backward_on_fp64_residual": {"strengths": rel(pq(gmb), fd_q),
+                                                "positions": rel(px(gmb), fd_x)},
+            "mixed": {"strengths": rel(pq(gmx), fd_q), "positions": rel(px(gmx), fd_x)},
+            "residual_over_phi": float((r64.norm() / (r64 + phi_ref).norm()).item())}
 
 
 def batch_problems(nproblems=512):
