@@ -654,6 +654,47 @@ int sumpy_helmholtz_p2e_from_items_f64(
     const double *sources, int64_t source_stride, const double *strength,
     double *tgt_expansions, void *stream);
 
+/* ------------------------------------------------------------------ */
+/* Tree, interaction lists and translation classes on the GPU           */
+/* ------------------------------------------------------------------ */
+
+/* Build the octree, Lists 1-4 and the translation classes of one problem or
+ * of a forest of independent problems on the GPU. Replaces boxtree's
+ * TreeBuilder / FMMTraversalBuilder / TranslationClassesBuilder as sumpy
+ * calls them (sumpy/fmm.py:356-363; the fields consumed are listed at
+ * sumpy/fmm.py:372-397, 543-592). Same definitions and the same arrays, bit
+ * for bit, as the host builder sumpy_tree_build_in_box (sumpy_b200_tree.h),
+ * for a forest as sumpy_b200.forest.merge_trees of per-problem trees built in
+ * one root box.
+ *
+ * Coordinates are DEVICE arrays in user order (problems concatenated);
+ * ntargets < 0 or tx == NULL: sources are the targets. nproblems > 1:
+ * problem p owns sources [problem_source_starts[p], [p+1]) and targets
+ * [problem_target_starts[p], [p+1]) (HOST int64 arrays of nproblems + 1
+ * entries, from 0 to the counts); nproblems == 1 ignores them. bbox_min
+ * (HOST, 3 doubles) and root_extent fix the root box (every particle must lie
+ * in it); bbox_min == NULL: the particles' bounding cube. Work runs on
+ * `stream`; the call returns when the build is complete. Allocates device
+ * memory (stream-ordered) for its scratch and results: a set-up step, not the
+ * evaluation path. The handle owns the result arrays (boxtree's names; plus
+ * "box_problem", the problem of each box) until sumpy_tree_gpu_free. */
+int sumpy_tree_gpu_build(int64_t nsources, const double *sx, const double *sy, const double *sz,
+                         int64_t ntargets, const double *tx, const double *ty, const double *tz,
+                         int32_t nproblems, const int64_t *problem_source_starts,
+                         const int64_t *problem_target_starts, int max_particles_in_box,
+                         int max_levels, const double *bbox_min, double root_extent,
+                         void *stream, void **handle_out);
+
+/* kind: 0 = int32, 1 = float64; length in elements. */
+int sumpy_tree_gpu_array_info(void *handle, const char *name, int *kind, int64_t *length);
+
+/* Copy a result array to dst (device memory when dst_on_device, else host
+ * memory; a host copy is complete when the call returns). */
+int sumpy_tree_gpu_array_copy(void *handle, const char *name, void *dst, int64_t capacity_bytes,
+                              int dst_on_device, void *stream);
+
+void sumpy_tree_gpu_free(void *handle);
+
 #ifdef __cplusplus
 }
 #endif

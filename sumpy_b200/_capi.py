@@ -45,6 +45,11 @@ SIGNATURES = {
                                           i32, ptr, i32, ptr, i32, ptr, ptr],
     "sumpy_split_tf32x2": [i64, i32, i32, ptr, i32, i32, ptr, ptr, ptr],
     "sumpy_set_tc_wait_cycles": [i64],
+    "sumpy_tree_gpu_build": [i64, ptr, ptr, ptr, i64, ptr, ptr, ptr, i32, ptr, ptr, cint, cint,
+                             ptr, dbl, ptr, ptr],
+    "sumpy_tree_gpu_array_info": [ptr, ctypes.c_char_p, ptr, ptr],
+    "sumpy_tree_gpu_array_copy": [ptr, ctypes.c_char_p, ptr, i64, cint, ptr],
+    "sumpy_tree_gpu_free": [ptr],
     "sumpy_get_tc_wait_cycles": [],
     "sumpy_m2l_translation_classes_tf32x3": [cint, i32, ptr, ptr, ptr, i32, ptr, ptr, ptr, ptr,
                                              i32, ptr, ptr, i32, i32, i32, i32, ptr, ptr, i32,
@@ -128,6 +133,7 @@ _RESTYPES = {
     "sumpy_version": cint,
     "sumpy_last_error": ctypes.c_char_p,
     "sumpy_get_tc_wait_cycles": i64,
+    "sumpy_tree_gpu_free": None,
 }
 
 _lib = None

@@ -261,7 +261,7 @@ def merge_trees(parts):
 
 
 def build_forest(sources, targets=None, max_particles_in_box=30, bbox=None, max_levels=None,
-                 threads=8):
+                 threads=8, device=None):
     """Build one forest over a batch of problems.
 
     :arg sources: list of ``(3, n_i)`` arrays.
@@ -269,6 +269,11 @@ def build_forest(sources, targets=None, max_particles_in_box=30, bbox=None, max_
         exclude_self available) or a list of ``(3, m_i)`` arrays.
     :arg bbox: the common root box as a ``(3, 2)`` array; default the
         bounding cube of all particles of the batch.
+    :arg device: build the whole forest in one pass on this GPU
+        (``sumpy_tree_gpu_build`` with one problem per root box); the same
+        arrays, bit for bit, as per-problem host trees merged by
+        :func:`merge_trees`. Default: host trees built in ``threads`` threads,
+        then merged.
     """
     P = len(sources)
     if targets is not None and len(targets) != P:
@@ -283,6 +288,8 @@ def build_forest(sources, targets=None, max_particles_in_box=30, bbox=None, max_
         ext *= 1 + 1e-9
         lo = lo - 0.5 * (ext - (hi - lo))
         bbox = np.stack([lo, lo + ext], axis=1)
+    if device is not None:
+        return build_forest_gpu(sources, targets, max_particles_in_box, bbox, max_levels, device)
 
     def one(i):
         return build_all(sources[i], None if targets is None else targets[i],
@@ -291,3 +298,38 @@ def build_forest(sources, targets=None, max_particles_in_box=30, bbox=None, max_
     with ThreadPoolExecutor(max_workers=max(1, int(threads))) as ex:
         parts = list(ex.map(one, range(P)))
     return merge_trees(parts)
+
+
+def build_forest_gpu(sources, targets, max_particles_in_box, bbox, max_levels, device):
+    """The forest of :func:`build_forest` built on the GPU in one pass: all
+    problems' particles concatenated, one root box per problem in the common
+    root box ``bbox``."""
+    import torch
+    from sumpy_b200.tree import _objects, _root_box, gpu_tree_handle
+
+    def cat(arrs):
+        ts = [torch.as_tensor(a, dtype=torch.float64).reshape(3, -1) for a in arrs]
+        return torch.cat(ts, dim=1).to(device).contiguous()
+
+    P = len(sources)
+    src = cat(sources)
+    tgt = None if targets is None else cat(targets)
+    src_st = np.zeros(P + 1, dtype=np.int64)
+    np.cumsum([np.shape(s)[1] for s in sources], out=src_st[1:])
+    if targets is None:
+        tgt_st = src_st.copy()
+    else:
+        tgt_st = np.zeros(P + 1, dtype=np.int64)
+        np.cumsum([np.shape(t)[1] for t in targets], out=tgt_st[1:])
+    bmin, ext = _root_box(bbox)
+    H = gpu_tree_handle(src, tgt, max_particles_in_box, max_levels, bmin, ext,
+                        source_starts=src_st, target_starts=None if targets is None else tgt_st)
+    tree, trav, tcls = _objects(H, keep_handle=False)
+    prob = H.get("box_problem")
+    del H
+    order = np.argsort(prob, kind="stable").astype(np.int32)
+    cuts = np.zeros(P + 1, dtype=np.int64)
+    np.cumsum(np.bincount(prob, minlength=P), out=cuts[1:])
+    maps = [order[cuts[i]:cuts[i + 1]] for i in range(P)]
+    return tree, trav, tcls, Forest(nproblems=P, source_starts=src_st, target_starts=tgt_st,
+                                    box_maps=maps)

@@ -156,13 +156,40 @@ class TranslationClassesInfo:
     from_sep_siblings_translation_classes_level_starts: np.ndarray
 
 
-def build_all(sources, targets=None, max_particles_in_box=30, max_levels=None, bbox=None):
+def _root_box(bbox):
+    """(bbox_min, root_extent) of a ``(3, 2)`` per-axis [min, max] box, as
+    boxtree's ``TreeBuilder(..., bbox=...)``: the cube at ``min`` with the
+    largest side."""
+    bb = np.asarray(bbox, dtype=np.float64).reshape(3, 2)
+    return np.ascontiguousarray(bb[:, 0]), float(np.max(bb[:, 1] - bb[:, 0]))
+
+
+def _is_cuda(a):
+    return hasattr(a, "is_cuda") and a.is_cuda
+
+
+def build_all(sources, targets=None, max_particles_in_box=30, max_levels=None, bbox=None,
+              device=None):
     """Build :class:`Tree`, :class:`FMMTraversalInfo` and
-    :class:`TranslationClassesInfo` in one call of the host library.
+    :class:`TranslationClassesInfo` in one native call.
 
     ``bbox``, as boxtree's ``TreeBuilder(..., bbox=...)``: a ``(3, 2)`` array
     of per-axis ``[min, max]``; the root box is the cube at ``min`` with the
-    largest side. Without it the root box is the particles' bounding cube."""
+    largest side. Without it the root box is the particles' bounding cube.
+
+    ``device`` (or sources given as a CUDA tensor): build on that GPU
+    (``sumpy_tree_gpu_build``, the same arrays bit for bit); otherwise on the
+    host (``sumpy_tree_build_in_box``). The returned objects hold host arrays
+    either way."""
+    if device is None and _is_cuda(sources):
+        device = sources.device
+    if device is not None:
+        return build_all_gpu(sources, targets, max_particles_in_box, max_levels, bbox, device)
+    H = _host_handle(sources, targets, max_particles_in_box, max_levels, bbox)
+    return _objects(H)
+
+
+def _host_handle(sources, targets, max_particles_in_box, max_levels, bbox):
     src = _soa(sources, "sources")
     tgt = None if targets is None else _soa(targets, "targets")
     lib = _tree_lib()
@@ -182,9 +209,7 @@ def build_all(sources, targets=None, max_particles_in_box=30, max_levels=None, b
     if bbox is None:
         bmin, ext = None, 0.0
     else:
-        bb = np.asarray(bbox, dtype=np.float64).reshape(3, 2)
-        bmin = np.ascontiguousarray(bb[:, 0])
-        ext = float(np.max(bb[:, 1] - bb[:, 0]))
+        bmin, ext = _root_box(bbox)
     rc = lib.sumpy_tree_build_in_box(
         ctypes.c_int64(src.shape[1]), p(sx), p(sy), p(sz),
         ctypes.c_int64(ntgt),
@@ -196,8 +221,112 @@ def build_all(sources, targets=None, max_particles_in_box=30, max_levels=None, b
         ctypes.byref(h))
     if rc != 0:
         raise ValueError(lib.sumpy_tree_last_error().decode())
-    H = _Handle(h)
+    return _Handle(h)
 
+
+class _GpuHandle:
+    """Result arrays of ``sumpy_tree_gpu_build`` (device memory owned by the
+    native handle until this object goes)."""
+
+    def __init__(self, h):
+        self.h = h
+
+    def _lib(self):
+        from sumpy_b200 import _lib as L
+        return L.load_cuda_library()
+
+    def info(self, name):
+        lib = self._lib()
+        kind = ctypes.c_int()
+        n = ctypes.c_int64()
+        rc = lib.sumpy_tree_gpu_array_info(self.h, name.encode(), ctypes.byref(kind),
+                                           ctypes.byref(n))
+        if rc != 0:
+            raise RuntimeError(lib.sumpy_last_error().decode())
+        return kind.value, n.value
+
+    def get(self, name):
+        """Host copy."""
+        from sumpy_b200._capi import stream_ptr
+        kind, n = self.info(name)
+        arr = np.empty(n, dtype=np.int32 if kind == 0 else np.float64)
+        lib = self._lib()
+        rc = lib.sumpy_tree_gpu_array_copy(self.h, name.encode(),
+                                           arr.ctypes.data_as(ctypes.c_void_p), arr.nbytes, 0,
+                                           stream_ptr())
+        if rc != 0:
+            raise RuntimeError(lib.sumpy_last_error().decode())
+        return arr
+
+    def __del__(self):
+        if self.h:
+            try:
+                self._lib().sumpy_tree_gpu_free(self.h)
+            except Exception:  # noqa: BLE001 (interpreter shutdown)
+                pass
+            self.h = None
+
+
+def _dev_soa(points, name, device):
+    """(3, n) float64 contiguous CUDA tensor of host or device points."""
+    import torch
+    if isinstance(points, (list, tuple)):
+        points = np.stack([np.asarray(p, dtype=np.float64) for p in points])
+    t = torch.as_tensor(points, dtype=torch.float64, device=device).contiguous()
+    if t.ndim != 2 or t.shape[0] != 3:
+        raise ValueError(f"{name} must have shape (3, n); got {tuple(t.shape)}")
+    return t
+
+
+def gpu_tree_handle(src, tgt, max_particles_in_box, max_levels, bmin, ext,
+                    source_starts=None, target_starts=None):
+    """Run ``sumpy_tree_gpu_build`` on (3, n) CUDA tensors (problems given by
+    their int64 start arrays) on the current stream."""
+    import torch
+    from sumpy_b200 import _lib as L
+    from sumpy_b200._capi import stream_ptr
+    lib = L.load_cuda_library()
+    with torch.cuda.device(src.device):
+        nprob = 1 if source_starts is None else len(source_starts) - 1
+        sst = None if source_starts is None else np.ascontiguousarray(source_starts, np.int64)
+        tst = None if target_starts is None else np.ascontiguousarray(target_starts, np.int64)
+        vp = ctypes.c_void_p
+        h = ctypes.c_void_p()
+        rc = lib.sumpy_tree_gpu_build(
+            ctypes.c_int64(src.shape[1]), vp(src[0].data_ptr()), vp(src[1].data_ptr()),
+            vp(src[2].data_ptr()),
+            ctypes.c_int64(-1 if tgt is None else tgt.shape[1]),
+            None if tgt is None else vp(tgt[0].data_ptr()),
+            None if tgt is None else vp(tgt[1].data_ptr()),
+            None if tgt is None else vp(tgt[2].data_ptr()),
+            ctypes.c_int32(nprob),
+            None if sst is None else sst.ctypes.data_as(vp),
+            None if tst is None else tst.ctypes.data_as(vp),
+            ctypes.c_int(int(max_particles_in_box)),
+            ctypes.c_int(0 if max_levels is None else int(max_levels)),
+            None if bmin is None else np.ascontiguousarray(bmin, np.float64).ctypes.data_as(vp),
+            ctypes.c_double(ext), stream_ptr(), ctypes.byref(h))
+        if rc != 0:
+            raise ValueError(lib.sumpy_last_error().decode())
+    return _GpuHandle(h)
+
+
+def build_all_gpu(sources, targets=None, max_particles_in_box=30, max_levels=None, bbox=None,
+                  device="cuda"):
+    """:func:`build_all` on the GPU (``sumpy_tree_gpu_build``): the same
+    arrays, bit for bit, as the host builder; returned as host arrays."""
+    src = _dev_soa(sources, "sources", device)
+    tgt = None if targets is None else _dev_soa(targets, "targets", device)
+    bmin, ext = (None, 0.0) if bbox is None else _root_box(bbox)
+    H = gpu_tree_handle(src, tgt, max_particles_in_box, max_levels, bmin, ext)
+    out = _objects(H, keep_handle=False)
+    del H
+    return out
+
+
+def _objects(H, keep_handle=True):
+    """Tree, traversal and translation classes from a builder handle (host
+    arrays; ``keep_handle``: the tree keeps the handle alive)."""
     nb, nl, ns, nt, sat = (int(x) for x in H.get("scalars"))
     g = H.get
 
@@ -224,7 +353,7 @@ def build_all(sources, targets=None, max_particles_in_box=30, max_levels=None, b
         box_target_counts_cumul=g("box_target_counts_cumul"),
         box_target_counts_nonchild=g("box_target_counts_nonchild"),
         target_to_source=g("target_to_source") if sat else None,
-        _handle=H)
+        _handle=H if keep_handle else None)
 
     tb_all = g("sep_smaller_target_boxes")
     tb_ls = g("sep_smaller_target_boxes_level_starts")

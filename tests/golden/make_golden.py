@@ -1,11 +1,13 @@
 """Generate golden operator vectors by running sumpy's own symbolic expansion code.
 
 This script is test infrastructure. It is run by hand in a container that has
-the sumpy source tree (``SUMPY_REFERENCE`` env var, default ``/root/reference``)
-and sympy installed; the GPU test box never runs it. It writes
+the sumpy source tree (its path in the ``SUMPY_REFERENCE`` environment
+variable, which is required) and sympy installed; the GPU test box never runs it. It writes
 ``tests/golden/laplace3d_operators.json`` and
 ``tests/golden/helmholtz3d_operators.json``, which the tests read
-(``python tests/golden/make_golden.py [laplace] [helmholtz]``).
+(``SUMPY_REFERENCE=<sumpy checkout> python tests/golden/make_golden.py
+[--which laplace helmholtz] [--laplace-orders 2 3 4 5 6 8]
+[--helmholtz-orders 2 3 4]``).
 
 sumpy itself cannot be imported normally here: its package ``__init__`` pulls
 in pyopencl/loopy/boxtree, none of which are installed. The expansion math
@@ -67,7 +69,7 @@ from pathlib import Path
 
 import numpy as np
 
-REF = os.environ.get("SUMPY_REFERENCE", "/root/reference")
+REF = os.environ.get("SUMPY_REFERENCE")
 OUT = Path(__file__).with_name("laplace3d_operators.json")
 
 _PLACEHOLDER_PACKAGES = {
@@ -339,20 +341,28 @@ def generate(knl, orders, out_path, label, complex_valued, extra_subs):
 
 
 def main():
+    import argparse
     global HELM_K
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--which", nargs="+", default=["laplace", "helmholtz"],
+                    choices=["laplace", "helmholtz"])
+    ap.add_argument("--laplace-orders", nargs="+", type=int, default=[2, 3, 4, 5, 6, 8])
+    ap.add_argument("--helmholtz-orders", nargs="+", type=int, default=[2, 3, 4])
+    args = ap.parse_args()
+    if not REF:
+        sys.exit("set SUMPY_REFERENCE to the root of a sumpy source tree")
     _install_placeholders()
     import sympy
     HELM_K = sympy.Rational(5, 2)
     lap, helm = _kernels()
-    which = sys.argv[1:] or ["laplace", "helmholtz"]
-    if "laplace" in which:
-        data = generate(lap, (2, 3, 4, 5), OUT, "laplace", False, {})
+    if "laplace" in args.which:
+        data = generate(lap, tuple(args.laplace_orders), OUT, "laplace", False, {})
         data["kernel"] = "LaplaceKernel(3), expression 1/|d| (scaling applied on output)"
         OUT.write_text(json.dumps(data, indent=1))
         print("wrote", OUT)
-    if "helmholtz" in which:
+    if "helmholtz" in args.which:
         out = OUT.with_name("helmholtz3d_operators.json")
-        data = generate(helm, (2, 3, 4), out, "helmholtz", True,
+        data = generate(helm, tuple(args.helmholtz_orders), out, "helmholtz", True,
                         {sympy.Symbol("k"): HELM_K})
         data["kernel"] = ("HelmholtzKernel(3), expression exp(i k |d|)/|d| with k = 5/2 "
                           "(scaling applied on output); complex values as [re, im]")
