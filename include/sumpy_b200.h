@@ -677,7 +677,10 @@ int sumpy_helmholtz_p2e_from_items_f64(
  * `stream`; the call returns when the build is complete. Allocates device
  * memory (stream-ordered) for its scratch and results: a set-up step, not the
  * evaluation path. The handle owns the result arrays (boxtree's names; plus
- * "box_problem", the problem of each box) until sumpy_tree_gpu_free. */
+ * "box_problem", the problem of each box, and "build_phase_ms", the wall time
+ * of the build's phases: bounding box, keys and sort, levels, boxes and
+ * colleagues, Lists 1-4, List 3 by level, particles and classes) until
+ * sumpy_tree_gpu_free. */
 int sumpy_tree_gpu_build(int64_t nsources, const double *sx, const double *sy, const double *sz,
                          int64_t ntargets, const double *tx, const double *ty, const double *tz,
                          int32_t nproblems, const int64_t *problem_source_starts,

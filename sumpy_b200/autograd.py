@@ -92,9 +92,16 @@ class _Geometry:
     def __init__(self, cfg, src, tgt, make_wrangler):
         self.cfg = cfg
         self.self_eval = tgt is None
-        s = src.detach().to("cpu", torch.float64).numpy()
-        t = None if self.self_eval else tgt.detach().to("cpu", torch.float64).numpy()
-        self.tree, self.trav, self.tcls = build_all(s, t, cfg.max_particles_in_box)
+        if cfg.device.type == "cuda":
+            # the tree is built on the GPU from the device coordinates
+            s = src.detach().to(cfg.device, torch.float64)
+            t = None if self.self_eval else tgt.detach().to(cfg.device, torch.float64)
+            self.tree, self.trav, self.tcls = build_all(s, t, cfg.max_particles_in_box,
+                                                        device=cfg.device)
+        else:
+            s = src.detach().to("cpu", torch.float64).numpy()
+            t = None if self.self_eval else tgt.detach().to("cpu", torch.float64).numpy()
+            self.tree, self.trav, self.tcls = build_all(s, t, cfg.max_particles_in_box)
         self._transposed = None
         self._make = make_wrangler
         self._fwd = {}

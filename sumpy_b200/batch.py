@@ -40,13 +40,17 @@ class BatchedLaplaceFMM:
     :arg bbox: common root box, ``(3, 2)``; default the batch's bounding cube.
     :arg use_graph: replay a captured CUDA graph (True) or launch eagerly.
     :arg autotune: choose ``m2l_item_groups`` by timing (cached on disk).
+    :arg gpu_tree: build the forest on the GPU in one pass (default) instead
+        of host trees merged on the host (the same arrays either way).
     """
 
     def __init__(self, sources, targets=None, order=8, max_particles_in_box=32,
                  precision="mixed", bbox=None, device="cuda", use_graph=True,
-                 autotune=False, m2l_item_groups=None, autotune_cache=None):
+                 autotune=False, m2l_item_groups=None, autotune_cache=None, gpu_tree=True):
         self.device = torch.device(device)
-        tree, trav, tcls, forest = build_forest(sources, targets, max_particles_in_box, bbox)
+        tree, trav, tcls, forest = build_forest(
+            sources, targets, max_particles_in_box, bbox,
+            device=self.device if gpu_tree and self.device.type == "cuda" else None)
         self.tree, self.traversal, self.forest = tree, trav, forest
         knl = LaplaceKernel(3)
         exclude_self = targets is None

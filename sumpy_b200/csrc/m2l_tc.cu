@@ -23,8 +23,8 @@
 // chunks of TC_KC through a ring of shared-memory stages (6 of 32 KB, or 3
 // of 64 KB): a TMA tiled load per operator plane and cp.async row copies of
 // the gathered source multipoles, all completing on the stage's "full"
-// mbarrier (TMA byte count plus one asynchronous cp.async arrival per loader
-// thread). One thread issues the MMAs of a chunk (TC_KC / 8 K-steps x 3
+// mbarrier (TMA byte count plus one arrival per loader warp, made once the
+// warp's cp.async group for the stage has landed). One thread issues the MMAs of a chunk (TC_KC / 8 K-steps x 3
 // products) and commits them to the stage's "empty" mbarrier, which the
 // loader waits on before refilling the stage. Every load fills this CTA's own shared memory only. All waits are bounded by a clock
 // budget; on expiry the kernel records an error in *status, lets work in
@@ -93,10 +93,18 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, uint32
                  : "memory");
 }
 
-// arrive on the mbarrier once this thread's earlier cp.async copies have landed
-__device__ __forceinline__ void cp_async_arrive_noinc(uint32_t mbar)
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+
+// wait until at most N of this thread's committed cp.async groups are pending
+template <int N> __device__ __forceinline__ void cp_async_wait_group()
 {
-    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(mbar) : "memory");
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// make this thread's shared-memory writes visible to the tensor cores (async proxy)
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
 }
 
 __device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count)
@@ -241,19 +249,6 @@ __device__ bool mbar_wait_or_abort(uint32_t addr, uint32_t parity, volatile int 
     return true;
 }
 
-// barrier 1 over the loader warps only, OR-reducing a flag
-__device__ __forceinline__ bool loaders_sync_or(bool v)
-{
-    uint32_t r;
-    asm volatile(
-        "{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n"
-        " bar.red.or.pred p, 1, %2, q;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(r)
-        : "r"((uint32_t)v), "n"(TC_LOADERS)
-        : "memory");
-    return r != 0;
-}
-
 // One CTA per work item = a contiguous range of class groups of one tile.
 // Warp roles: warps 0-2 load (thread 0 also posts the expected TMA bytes),
 // warp 3 lane 0 issues the MMAs, warps 4-11 drain. Each group's product accumulates in one of
@@ -294,13 +289,13 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
     }
     if (threadIdx.x == 32) {
         for (int s = 0; s < TC_STAGES; ++s) {
-            // TMA expect-tx (+ the cp.async arrivals of the copying loaders)
-            mbar_init(full_bar + 8 * s, TC_GATHER ? 1 : TC_LOADERS + 1);
+            // TMA expect-tx + one arrival per copying loader warp
+            mbar_init(full_bar + 8 * s, TC_GATHER ? 1 : TC_LOADERS / 32 + 1);
             mbar_init(empty_bar + 8 * s, 1);
         }
         for (int s = 0; s < 2; ++s) {
             mbar_init(accf_bar + 8 * s, 1);
-            mbar_init(acce_bar + 8 * s, TC_DRAINERS);
+            mbar_init(acce_bar + 8 * s, TC_DRAINERS / 32);
         }
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -403,6 +398,13 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
             load_rows(g0, sb_cur);
             if (threadIdx.x == 0) cls_cur = a.group_class[g0];
         }
+        // Each warp commits a stage's copies as one cp.async group and
+        // announces the stage one iteration later, once the group has landed
+        // (wait_group 1: all but the newest group): one arrival per warp
+        // instead of one per thread keeps the barrier's serialised arrivals
+        // off the critical path.
+        const unsigned FULLMASK = 0xffffffffu;
+        int pending = -1;   // stage whose copies this warp issued but has not announced
         for (int it = 0; it < total; ++it) {
             const int s = it % TC_STAGES, use = it / TC_STAGES;
             const int gi = it / nkc, kc = it % nkc;
@@ -412,7 +414,7 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
             }
             bool ok = true;
             if (use > 0) ok = mbar_wait_or_abort(empty_bar + 8 * s, (use - 1) & 1, abort_flag, a.wait_cycles);
-            if (loaders_sync_or(!ok || *abort_flag)) break;
+            if (__any_sync(FULLMASK, !ok || *abort_flag)) break;
             const int k0 = (kcb + kc) * TC_KC;
             const uint32_t st = base + s * STAGE;
             if (threadIdx.x == 0) {
@@ -437,12 +439,26 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
                     cp_async16(st + 3 * PLANE + dst, a.src_lo + off, bytes);
                 }
             }
-            cp_async_arrive_noinc(full_bar + 8 * s);
+            cp_async_commit();
+            if (pending >= 0) {
+                cp_async_wait_group<1>();
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(full_bar + 8 * pending);
+            }
+            pending = s;
             if (kc == nkc - 1) {
 #pragma unroll
                 for (int u = 0; u < NU; ++u) sb_cur[u] = sb_nxt[u];
                 cls_cur = cls_nxt;
             }
+        }
+        // the last stage (and, after an abort, every copy still in flight)
+        cp_async_wait_group<0>();
+        if (pending >= 0) {
+            fence_proxy_async_smem();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(full_bar + 8 * pending);
         }
     } else if (warp == 3) {
         // ---------------- MMA issuer ----------------
@@ -484,6 +500,7 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
         for (int gi = 0; gi < ng && ok; ++gi) {
             const int acc = gi & 1;
             ok = mbar_wait_or_abort(accf_bar + 8 * acc, (gi >> 1) & 1, abort_flag, a.wait_cycles);
+            ok = __all_sync(0xffffffffu, ok);
             if (!ok) break;
             tc_fence_after();
             const uint32_t taddr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(acc * TC_TW + half * 64);
@@ -495,7 +512,8 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
                 for (int j = 0; j < 16; ++j) acc64[c0 + j] += (double)__uint_as_float(r[j]);
             }
             tc_fence_before();
-            mbar_arrive(acce_bar + 8 * acc);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(acce_bar + 8 * acc);
         }
         if (ok && ng > 0) {
             const int row = row0 + quad * 32 + lane;

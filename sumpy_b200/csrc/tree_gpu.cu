@@ -36,6 +36,7 @@
 #include <thrust/iterator/transform_iterator.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -114,61 +115,67 @@ inline void launched(const char *what) { ck(cudaGetLastError(), what); }
 
 // {{{ bounding box and keys
 
-// per-dimension min / max of the finite coordinates, and a count of the
-// non-finite ones; out = [min x3, max x3] (bit patterns as ordered integers
-// would also do, but FP64 min/max atomics are not native: a block reduction
-// then one thread per block combines through a CAS loop)
-__device__ __forceinline__ void atomic_min_d(double *a, double v)
-{
-    unsigned long long *ua = reinterpret_cast<unsigned long long *>(a);
-    unsigned long long old = *ua;
-    while (v < __longlong_as_double((long long)old)) {
-        const unsigned long long prev = atomicCAS(ua, old, (unsigned long long)__double_as_longlong(v));
-        if (prev == old) break;
-        old = prev;
-    }
-}
-
-__device__ __forceinline__ void atomic_max_d(double *a, double v)
-{
-    unsigned long long *ua = reinterpret_cast<unsigned long long *>(a);
-    unsigned long long old = *ua;
-    while (v > __longlong_as_double((long long)old)) {
-        const unsigned long long prev = atomicCAS(ua, old, (unsigned long long)__double_as_longlong(v));
-        if (prev == old) break;
-        old = prev;
-    }
-}
-
-__global__ void bbox_kernel(int64_t n, const double *__restrict__ x, const double *__restrict__ y,
-                            const double *__restrict__ z, double *out, unsigned long long *nonfinite)
+// per-dimension min / max of the finite coordinates and a count of the
+// non-finite ones: each block reduces its share into partial[block][7]
+// (min x3, max x3, count as a double), one block combines the partials
+__global__ void bbox_partial_kernel(int64_t n, const double *__restrict__ x,
+                                    const double *__restrict__ y, const double *__restrict__ z,
+                                    double *__restrict__ partial)
 {
     double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-    unsigned long long bad = 0;
+    double bad = 0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
         const double p[3] = {x[i], y[i], z[i]};
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            if (!isfinite(p[d])) { ++bad; continue; }
+            if (!isfinite(p[d])) { bad += 1; continue; }
             lo[d] = fmin(lo[d], p[d]);
             hi[d] = fmax(hi[d], p[d]);
         }
     }
     typedef cub::BlockReduce<double, 256> BR;
     __shared__ typename BR::TempStorage tmp;
+    double r[7];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        const double l = BR(tmp).Reduce(lo[d], cub::Min());
+        r[d] = BR(tmp).Reduce(lo[d], cub::Min());
         __syncthreads();
-        const double h = BR(tmp).Reduce(hi[d], cub::Max());
+        r[3 + d] = BR(tmp).Reduce(hi[d], cub::Max());
         __syncthreads();
-        if (threadIdx.x == 0) {
-            atomic_min_d(out + d, l);
-            atomic_max_d(out + 3 + d, h);
-        }
     }
-    if (bad) atomicAdd(nonfinite, bad);
+    r[6] = BR(tmp).Sum(bad);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 7; ++k) partial[7 * (int64_t)blockIdx.x + k] = r[k];
+}
+
+// combine nparts partials (one block of 256 threads) into out[0..6]
+__global__ void bbox_combine_kernel(int nparts, const double *__restrict__ partial,
+                                    double *__restrict__ out)
+{
+    double r[7] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY, 0};
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
+        const double *q = partial + 7 * (int64_t)i;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            r[d] = fmin(r[d], q[d]);
+            r[3 + d] = fmax(r[3 + d], q[3 + d]);
+        }
+        r[6] += q[6];
+    }
+    typedef cub::BlockReduce<double, 256> BR;
+    __shared__ typename BR::TempStorage tmp;
+    double o[7];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        o[d] = BR(tmp).Reduce(r[d], cub::Min());
+        __syncthreads();
+        o[3 + d] = BR(tmp).Reduce(r[3 + d], cub::Max());
+        __syncthreads();
+    }
+    o[6] = BR(tmp).Sum(r[6]);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 7; ++k) out[k] = o[k];
 }
 
 __device__ __forceinline__ uint64_t spread3(uint32_t v)
@@ -256,43 +263,56 @@ void sort_segments(int64_t n, DevBuf &keys, DevBuf &idx, const std::vector<int64
 // {{{ scans
 
 __global__ void write_starts_kernel(int64_t n, const int64_t *__restrict__ incl,
-                                    int32_t *__restrict__ starts)
+                                    int32_t *__restrict__ starts, int64_t *__restrict__ total)
 {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n;
-         i += (int64_t)gridDim.x * blockDim.x)
+         i += (int64_t)gridDim.x * blockDim.x) {
         starts[i] = i == 0 ? 0 : (int32_t)incl[i - 1];
+        if (i == n && total) *total = n == 0 ? 0 : incl[n - 1];
+    }
 }
 
 struct ToI64 {
     __host__ __device__ int64_t operator()(int32_t v) const { return (int64_t)v; }
 };
 
-// starts[0] = 0, starts[i + 1] = cnt[0] + ... + cnt[i] (int32, n + 1 entries);
-// returns the total, which must fit int32
-int64_t scan_counts(const int32_t *cnt, int64_t n, DevBuf &starts, cudaStream_t st)
+// starts[0] = 0, starts[i + 1] = cnt[0] + ... + cnt[i] (int32, n + 1
+// entries); the total goes to *dtotal (device) without waiting for it
+void scan_counts_async(const int32_t *cnt, int64_t n, DevBuf &starts, int64_t *dtotal,
+                       cudaStream_t st)
 {
     starts = dalloc_n<int32_t>(n + 1, st);
-    if (n == 0) {
-        ck(cudaMemsetAsync(starts.p, 0, sizeof(int32_t), st), "memset");
-        return 0;
+    DevBuf incl = dalloc_n<int64_t>(std::max<int64_t>(n, 1), st);
+    if (n > 0) {
+        thrust::transform_iterator<ToI64, const int32_t *, int64_t> it(cnt, ToI64());
+        size_t tmp_bytes = 0;
+        ck(cub::DeviceScan::InclusiveSum(nullptr, tmp_bytes, it, incl.as<int64_t>(), (int)n, st),
+           "cub scan (size)");
+        DevBuf tmp = dalloc(tmp_bytes, st);
+        ck(cub::DeviceScan::InclusiveSum(tmp.p, tmp_bytes, it, incl.as<int64_t>(), (int)n, st),
+           "cub scan");
     }
-    DevBuf incl = dalloc_n<int64_t>(n, st);
-    thrust::transform_iterator<ToI64, const int32_t *, int64_t> it(cnt, ToI64());
-    size_t tmp_bytes = 0;
-    ck(cub::DeviceScan::InclusiveSum(nullptr, tmp_bytes, it, incl.as<int64_t>(), (int)n, st),
-       "cub scan (size)");
-    DevBuf tmp = dalloc(tmp_bytes, st);
-    ck(cub::DeviceScan::InclusiveSum(tmp.p, tmp_bytes, it, incl.as<int64_t>(), (int)n, st),
-       "cub scan");
-    int64_t total = 0;
-    ck(cudaMemcpyAsync(&total, incl.as<int64_t>() + (n - 1), sizeof(int64_t),
-                       cudaMemcpyDeviceToHost, st),
-       "copy scan total");
-    ck(cudaStreamSynchronize(st), "scan");
-    if (total > INT32_MAX) throw Fail{"list or box count exceeds int32"};
-    write_starts_kernel<<<nblocks(n + 1), 256, 0, st>>>(n, incl.as<int64_t>(), starts.as<int32_t>());
+    write_starts_kernel<<<nblocks(n + 1), 256, 0, st>>>(n, incl.as<int64_t>(), starts.as<int32_t>(),
+                                                        dtotal);
     launched("write_starts_kernel");
-    return total;
+}
+
+// host copies of n device int64 values (one wait); each must fit int32
+std::vector<int64_t> read_totals(const DevBuf &dtot, int n, cudaStream_t st)
+{
+    std::vector<int64_t> h(n);
+    ck(cudaMemcpyAsync(h.data(), dtot.p, 8 * (size_t)n, cudaMemcpyDeviceToHost, st), "copy totals");
+    ck(cudaStreamSynchronize(st), "scan");
+    for (int64_t v : h)
+        if (v > INT32_MAX) throw Fail{"list or box count exceeds int32"};
+    return h;
+}
+
+int64_t scan_counts(const int32_t *cnt, int64_t n, DevBuf &starts, cudaStream_t st)
+{
+    DevBuf dtot = dalloc_n<int64_t>(1, st);
+    scan_counts_async(cnt, n, starts, dtot.as<int64_t>(), st);
+    return read_totals(dtot, 1, st)[0];
 }
 
 // }}}
@@ -408,25 +428,50 @@ struct BoxPtrs {
     int64_t nb;
 };
 
-__device__ __forceinline__ int64_t lo_fine(const BoxPtrs &B, int32_t b, int d)
+// One 64-byte record per box for the list traversals: a visit touches one
+// cache line instead of one line per attribute array.
+struct __align__(64) Rec {
+    int32_t c0, c1, c2, level, nsrc, flags, parent, pad;   // flags: 1 = leaf
+    int32_t child[8];                                      // -1: none
+};
+static_assert(sizeof(Rec) == 64, "box record size");
+
+__device__ __forceinline__ Rec load_rec(const Rec *__restrict__ R, int32_t b)
 {
-    const int32_t c = d == 0 ? B.c0[b] : (d == 1 ? B.c1[b] : B.c2[b]);
-    return (int64_t)c << (KEY_BITS - B.level[b]);
+    const int4 *p = reinterpret_cast<const int4 *>(R + b);
+    Rec r;
+    int4 *q = reinterpret_cast<int4 *>(&r);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) q[k] = __ldg(p + k);
+    return r;
 }
 
-__device__ __forceinline__ bool adjacent(const BoxPtrs &B, int32_t a, int32_t b)
+__device__ __forceinline__ bool rec_adjacent(const Rec &a, const Rec &b)
 {
+    const int sa = KEY_BITS - a.level, sb = KEY_BITS - b.level;
+    const int32_t ca[3] = {a.c0, a.c1, a.c2}, cb[3] = {b.c0, b.c1, b.c2};
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        const int64_t la = lo_fine(B, a, d), lb = lo_fine(B, b, d);
-        const int64_t ha = la + ((int64_t)1 << (KEY_BITS - B.level[a]));
-        const int64_t hb = lb + ((int64_t)1 << (KEY_BITS - B.level[b]));
-        if (la > hb || lb > ha) return false;
+        const int64_t la = (int64_t)ca[d] << sa, lb = (int64_t)cb[d] << sb;
+        if (la > lb + ((int64_t)1 << sb) || lb > la + ((int64_t)1 << sa)) return false;
     }
     return true;
 }
 
-__device__ __forceinline__ bool has_src(const BoxPtrs &B, int32_t b) { return B.shi[b] > B.slo[b]; }
+__global__ void pack_records_kernel(BoxPtrs B, Rec *__restrict__ R)
+{
+    for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < B.nb;
+         b += (int64_t)gridDim.x * blockDim.x) {
+        Rec r;
+        r.c0 = B.c0[b]; r.c1 = B.c1[b]; r.c2 = B.c2[b]; r.level = B.level[b];
+        r.nsrc = B.shi[b] - B.slo[b];
+        r.flags = B.leaf[b] ? 1 : 0;
+        r.parent = B.parent[b];
+        r.pad = 0;
+        for (int o = 0; o < 8; ++o) r.child[o] = B.child[8 * b + o];
+        R[b] = r;
+    }
+}
 
 __global__ void leaf_kernel(int64_t nb, const int32_t *__restrict__ child, uint8_t *__restrict__ leaf)
 {
@@ -482,23 +527,25 @@ __global__ void attrs_kernel(BoxPtrs B, double b0, double b1, double b2, double 
 // colleagues of the boxes [b0, b1) of one level: the same-level boxes that
 // touch them (self included), from the parent's colleagues' children, in
 // increasing box number (by induction from the root's list {root})
-__global__ void colleagues_kernel(BoxPtrs B, int32_t b0, int32_t b1, int32_t *__restrict__ coll,
-                                  int32_t *__restrict__ ncoll, int32_t *__restrict__ err)
+__global__ void colleagues_kernel(const Rec *__restrict__ R, int32_t b0, int32_t b1,
+                                  int32_t *__restrict__ coll, int32_t *__restrict__ ncoll,
+                                  int32_t *__restrict__ err)
 {
     for (int64_t b = b0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < b1;
          b += (int64_t)gridDim.x * blockDim.x) {
+        const Rec rb = load_rec(R, (int32_t)b);
         int n = 0;
-        if (B.level[b] == 0) {
+        if (rb.level == 0) {
             coll[MAXCOLL * b] = (int32_t)b;
             n = 1;
         } else {
-            const int32_t par = B.parent[b];
+            const int32_t par = rb.parent;
             const int np = ncoll[par];
             for (int k = 0; k < np; ++k) {
-                const int32_t pc = coll[MAXCOLL * (int64_t)par + k];
+                const Rec rp = load_rec(R, coll[MAXCOLL * (int64_t)par + k]);
                 for (int o = 0; o < 8; ++o) {
-                    const int32_t c = B.child[8 * (int64_t)pc + o];
-                    if (c < 0 || !adjacent(B, c, (int32_t)b)) continue;
+                    const int32_t c = rp.child[o];
+                    if (c < 0 || !rec_adjacent(load_rec(R, c), rb)) continue;
                     if (n < MAXCOLL) coll[MAXCOLL * b + n] = c;
                     else atomicExch(err, 1);
                     ++n;
@@ -539,7 +586,7 @@ __device__ __forceinline__ void sort_segment2(int32_t *a, int32_t *c, int n)
 
 // List 1 and List 3 of each leaf target box. fill == 0: count into n1, n3;
 // fill == 1: write at the offsets s1, s3 and sort each list.
-__global__ void lists13_kernel(BoxPtrs B, const int32_t *__restrict__ coll,
+__global__ void lists13_kernel(const Rec *__restrict__ R, const int32_t *__restrict__ coll,
                                const int32_t *__restrict__ ncoll, int64_t ntb,
                                const int32_t *__restrict__ tboxes, int fill,
                                int32_t *__restrict__ n1, int32_t *__restrict__ n3,
@@ -550,6 +597,7 @@ __global__ void lists13_kernel(BoxPtrs B, const int32_t *__restrict__ coll,
     for (int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it < ntb;
          it += (int64_t)gridDim.x * blockDim.x) {
         const int32_t t = tboxes[it];
+        const Rec rt = load_rec(R, t);
         int32_t stack[STACK];
         int sp = 0;
         int c1 = 0, c3 = 0;
@@ -561,36 +609,42 @@ __global__ void lists13_kernel(BoxPtrs B, const int32_t *__restrict__ coll,
         bool overflow = false;
         while (sp > 0) {
             const int32_t c = stack[--sp];
-            if (B.leaf[c]) {
-                if (has_src(B, c)) {
+            const Rec rc = load_rec(R, c);
+            if (rc.flags & 1) {
+                if (rc.nsrc > 0) {
                     if (fill && c1 < cap1) o1[c1] = c;
                     ++c1;
                 }
                 continue;
             }
             for (int o = 0; o < 8; ++o) {
-                const int32_t d = B.child[8 * (int64_t)c + o];
+                const int32_t d = rc.child[o];
                 if (d < 0) continue;
-                if (adjacent(B, d, t)) {
+                const Rec rd = load_rec(R, d);
+                if (rec_adjacent(rd, rt)) {
                     if (sp < STACK) stack[sp++] = d;
                     else overflow = true;
-                } else if (has_src(B, d)) {
+                } else if (rd.nsrc > 0) {
                     if (fill && c3 < cap3) o3[c3] = d;
                     ++c3;
                 }
             }
         }
         // coarser leaves touching t: leaf colleagues of its ancestors
-        if (B.level[t] > 0) {
-            for (int32_t a = B.parent[t];; a = B.parent[a]) {
+        if (rt.level > 0) {
+            for (int32_t a = rt.parent;;) {
+                const Rec ra = load_rec(R, a);
                 for (int k = 0; k < ncoll[a]; ++k) {
                     const int32_t c = coll[MAXCOLL * (int64_t)a + k];
-                    if (c != a && B.leaf[c] && has_src(B, c) && adjacent(B, c, t)) {
+                    if (c == a) continue;
+                    const Rec rc = load_rec(R, c);
+                    if ((rc.flags & 1) && rc.nsrc > 0 && rec_adjacent(rc, rt)) {
                         if (fill && c1 < cap1) o1[c1] = c;
                         ++c1;
                     }
                 }
-                if (B.level[a] == 0) break;
+                if (ra.level == 0) break;
+                a = ra.parent;
             }
         }
         if (overflow) atomicExch(err, 2);
@@ -607,7 +661,7 @@ __global__ void lists13_kernel(BoxPtrs B, const int32_t *__restrict__ coll,
 
 // List 2 (with the global translation class of each entry) and List 4 of
 // each target-or-target-parent box; same two modes.
-__global__ void lists24_kernel(BoxPtrs B, const int32_t *__restrict__ coll,
+__global__ void lists24_kernel(const Rec *__restrict__ R, const int32_t *__restrict__ coll,
                                const int32_t *__restrict__ ncoll, int64_t nttp,
                                const int32_t *__restrict__ ttp, int fill,
                                int32_t *__restrict__ n2, int32_t *__restrict__ n4,
@@ -618,7 +672,8 @@ __global__ void lists24_kernel(BoxPtrs B, const int32_t *__restrict__ coll,
     for (int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it < nttp;
          it += (int64_t)gridDim.x * blockDim.x) {
         const int32_t b = ttp[it];
-        const int lev = B.level[b];
+        const Rec rb = load_rec(R, b);
+        const int lev = rb.level;
         int c2 = 0, c4 = 0;
         int32_t *o2 = fill ? l2 + s2[it] : nullptr;
         int32_t *oc = fill ? l2cls + s2[it] : nullptr;
@@ -626,15 +681,17 @@ __global__ void lists24_kernel(BoxPtrs B, const int32_t *__restrict__ coll,
         const int cap2 = fill ? s2[it + 1] - s2[it] : 0;
         const int cap4 = fill ? s4[it + 1] - s4[it] : 0;
         if (lev >= 1) {
-            const int32_t par = B.parent[b];
+            const int32_t par = rb.parent;
+            const Rec rpar = load_rec(R, par);
             if (lev >= 2) {
                 for (int k = 0; k < ncoll[par]; ++k) {
-                    const int32_t pc = coll[MAXCOLL * (int64_t)par + k];
+                    const Rec rpc = load_rec(R, coll[MAXCOLL * (int64_t)par + k]);
                     for (int o = 0; o < 8; ++o) {
-                        const int32_t d = B.child[8 * (int64_t)pc + o];
-                        if (d < 0 || !has_src(B, d)) continue;
-                        const int v0 = B.c0[b] - B.c0[d], v1 = B.c1[b] - B.c1[d];
-                        const int v2 = B.c2[b] - B.c2[d];
+                        const int32_t d = rpc.child[o];
+                        if (d < 0) continue;
+                        const Rec rd = load_rec(R, d);
+                        if (rd.nsrc <= 0) continue;
+                        const int v0 = rb.c0 - rd.c0, v1 = rb.c1 - rd.c1, v2 = rb.c2 - rd.c2;
                         if (abs(v0) <= 1 && abs(v1) <= 1 && abs(v2) <= 1) continue;
                         int cls = -1;
                         if (abs(v0) <= 3 && abs(v1) <= 3 && abs(v2) <= 3)
@@ -648,16 +705,20 @@ __global__ void lists24_kernel(BoxPtrs B, const int32_t *__restrict__ coll,
                     }
                 }
             }
-            for (int32_t a = par;; a = B.parent[a]) {
+            for (int32_t a = par;;) {
+                const Rec ra = load_rec(R, a);
                 for (int k = 0; k < ncoll[a]; ++k) {
                     const int32_t c = coll[MAXCOLL * (int64_t)a + k];
-                    if (c != a && B.leaf[c] && has_src(B, c) && adjacent(B, c, par) &&
-                        !adjacent(B, c, b)) {
+                    if (c == a) continue;
+                    const Rec rc = load_rec(R, c);
+                    if ((rc.flags & 1) && rc.nsrc > 0 && rec_adjacent(rc, rpar) &&
+                        !rec_adjacent(rc, rb)) {
                         if (fill && c4 < cap4) o4[c4] = c;
                         ++c4;
                     }
                 }
-                if (B.level[a] == 0) break;
+                if (ra.level == 0) break;
+                a = ra.parent;
             }
         }
         if (fill) {
@@ -671,48 +732,108 @@ __global__ void lists24_kernel(BoxPtrs B, const int32_t *__restrict__ coll,
     }
 }
 
-// entries of each target's List 3 on source level lev: [lo, hi) of its
-// sorted list (box numbers are level-major, so one level is one range)
-__global__ void l3_level_count_kernel(int64_t ntb, const int32_t *__restrict__ s3,
-                                      const int32_t *__restrict__ l3, int32_t box_lo,
-                                      int32_t box_hi, int32_t *__restrict__ first,
-                                      int32_t *__restrict__ cnt, uint8_t *__restrict__ flag)
+// For every target box and every source level: the first entry and the
+// number of entries of its (sorted) List 3 on that level -- box numbers are
+// level-major, so one level is one range of the list.
+__global__ void l3_levels_kernel(int64_t ntb, int nl, const int32_t *__restrict__ s3,
+                                 const int32_t *__restrict__ l3,
+                                 const int32_t *__restrict__ level_start,
+                                 int32_t *__restrict__ first2d, int32_t *__restrict__ cnt2d,
+                                 uint8_t *__restrict__ flag2d)
 {
     for (int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it < ntb;
          it += (int64_t)gridDim.x * blockDim.x) {
-        int32_t a = s3[it], e = s3[it + 1];
-        int32_t lo = a, hi = e;
-        while (lo < hi) { const int32_t m = lo + (hi - lo) / 2; if (l3[m] < box_lo) lo = m + 1; else hi = m; }
-        const int32_t f = lo;
-        lo = f; hi = e;
-        while (lo < hi) { const int32_t m = lo + (hi - lo) / 2; if (l3[m] < box_hi) lo = m + 1; else hi = m; }
-        first[it] = f;
-        cnt[it] = lo - f;
-        flag[it] = lo > f;
+        const int32_t a = s3[it], e = s3[it + 1];
+        int l = 0;
+        int32_t j = a;
+        for (; l < nl; ++l) {
+            const int32_t f = j;
+            while (j < e && l3[j] < level_start[l + 1]) ++j;
+            first2d[(int64_t)l * ntb + it] = f;
+            cnt2d[(int64_t)l * ntb + it] = j - f;
+            flag2d[(int64_t)l * ntb + it] = j > f;
+        }
     }
 }
 
-__global__ void gather_segments_kernel(int64_t nsel, const int32_t *__restrict__ sel,
-                                       const int32_t *__restrict__ first,
-                                       const int32_t *__restrict__ starts,
-                                       const int32_t *__restrict__ src, int32_t *__restrict__ dst)
+// per selected (level, target) k: its count, target box and first entry
+__global__ void l3_selected_kernel(int64_t nsel, int64_t ntb, const int32_t *__restrict__ sel,
+                                   const int32_t *__restrict__ cnt2d,
+                                   const int32_t *__restrict__ first2d,
+                                   const int32_t *__restrict__ tboxes,
+                                   int32_t *__restrict__ csel, int32_t *__restrict__ fsel,
+                                   int32_t *__restrict__ tbsel, int32_t *__restrict__ lsel)
 {
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nsel;
          k += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t it = sel[k];
-        const int32_t a = first[it];
-        for (int32_t j = starts[k]; j < starts[k + 1]; ++j) dst[j] = src[a + (j - starts[k])];
+        const int64_t g = sel[k];
+        csel[k] = cnt2d[g];
+        fsel[k] = first2d[g];
+        tbsel[k] = tboxes[g % ntb];
+        lsel[k] = (int32_t)(g / ntb);
     }
 }
 
-__global__ void problem_of_targets_kernel(int64_t nsel, const int32_t *__restrict__ sel,
-                                          const int32_t *__restrict__ tboxes,
-                                          const int32_t *__restrict__ prob,
-                                          int32_t *__restrict__ key)
+// level boundaries in the selection (lsel ascending): a[l] = first k on
+// level >= l, and the entry offset there
+__global__ void l3_bounds_kernel(int nl, int64_t nsel, const int32_t *__restrict__ lsel,
+                                 const int32_t *__restrict__ starts, int64_t *__restrict__ out)
+{
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l > nl) return;
+    int64_t lo = 0, hi = nsel;
+    while (lo < hi) { const int64_t m = lo + (hi - lo) / 2; if (lsel[m] < l) lo = m + 1; else hi = m; }
+    out[l] = lo;
+    out[nl + 1 + l] = starts[lo];
+}
+
+// each level's CSR starts, [0, c0, c0 + c1, ...], one after the other
+__global__ void l3_starts_kernel(int64_t nsel, int nl, const int32_t *__restrict__ lsel,
+                                 const int32_t *__restrict__ starts,
+                                 const int64_t *__restrict__ bounds, int32_t *__restrict__ out)
+{
+    const int64_t total = nsel + nl;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        if (k < nsel) {
+            const int l = lsel[k];
+            out[k + l] = starts[k] - starts[bounds[l]];
+        } else {
+            const int l = (int)(k - nsel);   // the closing entry of level l
+            const int64_t a = bounds[l], b = bounds[l + 1];
+            out[b + l] = starts[b] - starts[a];
+        }
+    }
+}
+
+// List 3 entries of the selection, level after level
+__global__ void l3_gather_kernel(int64_t nsel, const int32_t *__restrict__ fsel,
+                                 const int32_t *__restrict__ starts,
+                                 const int32_t *__restrict__ l3, int32_t *__restrict__ dst)
+{
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nsel;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t a = fsel[k];
+        for (int32_t j = starts[k]; j < starts[k + 1]; ++j) dst[j] = l3[a + (j - starts[k])];
+    }
+}
+
+// sort key of a selected (level, target): level, then the target's problem
+__global__ void l3_forest_key_kernel(int64_t nsel, int64_t nprob, const int32_t *__restrict__ lsel,
+                                     const int32_t *__restrict__ tbsel,
+                                     const int32_t *__restrict__ prob, uint64_t *__restrict__ key)
 {
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nsel;
          k += (int64_t)gridDim.x * blockDim.x)
-        key[k] = prob[tboxes[sel[k]]];
+        key[k] = (uint64_t)lsel[k] * (uint64_t)nprob + (uint64_t)prob[tbsel[k]];
+}
+
+__global__ void permute_kernel(int64_t n, const int32_t *__restrict__ perm,
+                               const int32_t *__restrict__ src, int32_t *__restrict__ dst)
+{
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * blockDim.x)
+        dst[k] = src[perm[k]];
 }
 
 __global__ void gather_kernel(int64_t n, const int32_t *__restrict__ idx,
@@ -820,21 +941,30 @@ void put_host(State &S, const std::string &name, const std::vector<T> &v, cudaSt
     put(S, name, sizeof(T) == 8 ? 1 : 0, (int64_t)v.size(), std::move(b));
 }
 
-DevBuf select_flagged(const uint8_t *flags, int64_t n, int64_t &count, cudaStream_t st)
+// indices i < n with flags[i] set, ascending, into out (n entries
+// allocated); their number goes to *dcount (device) without waiting
+DevBuf select_flagged_async(const uint8_t *flags, int64_t n, int64_t *dcount, cudaStream_t st)
 {
     DevBuf out = dalloc_n<int32_t>(std::max<int64_t>(n, 1), st);
-    DevBuf dn = dalloc_n<int64_t>(1, st);
+    if (n == 0) {
+        ck(cudaMemsetAsync(dcount, 0, sizeof(int64_t), st), "memset");
+        return out;
+    }
     thrust::counting_iterator<int32_t> it(0);
     size_t tmp_bytes = 0;
-    ck(cub::DeviceSelect::Flagged(nullptr, tmp_bytes, it, flags, out.as<int32_t>(),
-                                  dn.as<int64_t>(), n, st),
+    ck(cub::DeviceSelect::Flagged(nullptr, tmp_bytes, it, flags, out.as<int32_t>(), dcount, n, st),
        "cub select (size)");
     DevBuf tmp = dalloc(tmp_bytes, st);
-    ck(cub::DeviceSelect::Flagged(tmp.p, tmp_bytes, it, flags, out.as<int32_t>(),
-                                  dn.as<int64_t>(), n, st),
+    ck(cub::DeviceSelect::Flagged(tmp.p, tmp_bytes, it, flags, out.as<int32_t>(), dcount, n, st),
        "cub select");
-    ck(cudaMemcpyAsync(&count, dn.p, sizeof(int64_t), cudaMemcpyDeviceToHost, st), "copy count");
-    ck(cudaStreamSynchronize(st), "select");
+    return out;
+}
+
+DevBuf select_flagged(const uint8_t *flags, int64_t n, int64_t &count, cudaStream_t st)
+{
+    DevBuf dn = dalloc_n<int64_t>(1, st);
+    DevBuf out = select_flagged_async(flags, n, dn.as<int64_t>(), st);
+    count = read_totals(dn, 1, st)[0];
     return out;
 }
 
@@ -875,6 +1005,15 @@ State *build(int64_t nsrc, const double *sx, const double *sy, const double *sz,
     if (nsrc > 0 && (!sx || !sy || !sz)) throw Fail{"null source coordinates"};
 
     auto S = std::make_unique<State>();
+    // wall time of each phase (each ends with the stream drained)
+    std::vector<double> phase_ms;
+    auto t_phase = std::chrono::steady_clock::now();
+    auto mark = [&]() {
+        ck(cudaStreamSynchronize(st), "tree build");
+        const auto now = std::chrono::steady_clock::now();
+        phase_ms.push_back(std::chrono::duration<double, std::milli>(now - t_phase).count());
+        t_phase = now;
+    };
     {
         // lexicographic rank of (vx, vy, vz) in [-3,3]^3 \ [-1,1]^3
         int16_t table[343];
@@ -894,27 +1033,28 @@ State *build(int64_t nsrc, const double *sx, const double *sy, const double *sz,
 
     double lo[3], hi[3];
     {
-        DevBuf box = dalloc_n<double>(6, st);
-        DevBuf bad = dalloc_n<unsigned long long>(1, st);
-        const double init[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
-        ck(cudaMemcpyAsync(box.p, init, sizeof(init), cudaMemcpyHostToDevice, st), "init bbox");
-        ck(cudaMemsetAsync(bad.p, 0, sizeof(unsigned long long), st), "memset");
+        constexpr int NPART = 296;   // two blocks per SM per point set
+        DevBuf part = dalloc_n<double>(7 * 2 * NPART, st), box = dalloc_n<double>(7, st);
+        int nparts = 0;
         if (nsrc > 0) {
-            bbox_kernel<<<std::min<unsigned>(nblocks(nsrc), 1184), 256, 0, st>>>(
-                nsrc, sx, sy, sz, box.as<double>(), bad.as<unsigned long long>());
-            launched("bbox_kernel");
+            bbox_partial_kernel<<<NPART, 256, 0, st>>>(nsrc, sx, sy, sz, part.as<double>());
+            launched("bbox_partial_kernel");
+            nparts += NPART;
         }
         if (!sat && ntgt > 0) {
-            bbox_kernel<<<std::min<unsigned>(nblocks(ntgt), 1184), 256, 0, st>>>(
-                ntgt, tx, ty, tz, box.as<double>(), bad.as<unsigned long long>());
-            launched("bbox_kernel");
+            bbox_partial_kernel<<<NPART, 256, 0, st>>>(ntgt, tx, ty, tz,
+                                                       part.as<double>() + 7 * nparts);
+            launched("bbox_partial_kernel");
+            nparts += NPART;
         }
-        double out[6];
-        unsigned long long nbad = 0;
-        ck(cudaMemcpyAsync(out, box.p, sizeof(out), cudaMemcpyDeviceToHost, st), "copy bbox");
-        ck(cudaMemcpyAsync(&nbad, bad.p, sizeof(nbad), cudaMemcpyDeviceToHost, st), "copy bbox");
-        ck(cudaStreamSynchronize(st), "bbox");
-        if (nbad) throw Fail{"non-finite particle coordinate"};
+        double out[7] = {0, 0, 0, 0, 0, 0, 0};
+        if (nparts > 0) {
+            bbox_combine_kernel<<<1, 256, 0, st>>>(nparts, part.as<double>(), box.as<double>());
+            launched("bbox_combine_kernel");
+            ck(cudaMemcpyAsync(out, box.p, sizeof(out), cudaMemcpyDeviceToHost, st), "copy bbox");
+            ck(cudaStreamSynchronize(st), "bbox");
+        }
+        if (out[6] > 0) throw Fail{"non-finite particle coordinate"};
         for (int d = 0; d < 3; ++d) { lo[d] = out[d]; hi[d] = out[3 + d]; }
         if (nsrc + (sat ? 0 : ntgt) == 0) for (int d = 0; d < 3; ++d) { lo[d] = 0; hi[d] = 0; }
     }
@@ -939,6 +1079,8 @@ State *build(int64_t nsrc, const double *sx, const double *sy, const double *sz,
     }
 
     // }}}
+
+    mark();   // bounding box
 
     // {{{ 2. keys and sort
 
@@ -968,6 +1110,8 @@ State *build(int64_t nsrc, const double *sx, const double *sy, const double *sz,
     const uint64_t *tkeys = sat ? skeys.as<uint64_t>() : tkeys_sorted.as<uint64_t>();
 
     // }}}
+
+    mark();   // keys and sort
 
     // {{{ 3. levels
 
@@ -1042,8 +1186,14 @@ State *build(int64_t nsrc, const double *sx, const double *sy, const double *sz,
     BoxPtrs B{blev.as<int32_t>(), bc[0].as<int32_t>(), bc[1].as<int32_t>(), bc[2].as<int32_t>(),
               bslo.as<int32_t>(), bshi.as<int32_t>(), btlo.as<int32_t>(), bthi.as<int32_t>(),
               bpar.as<int32_t>(), bchild.as<int32_t>(), bleaf.as<uint8_t>(), nb};
+    DevBuf recs = dalloc_n<Rec>(nb, st);
+    pack_records_kernel<<<nblocks(nb), 256, 0, st>>>(B, recs.as<Rec>());
+    launched("pack_records_kernel");
+    const Rec *R = recs.as<Rec>();
 
     // }}}
+
+    mark();   // levels
 
     // {{{ 4. box attributes, box sets, colleagues
 
@@ -1084,14 +1234,17 @@ State *build(int64_t nsrc, const double *sx, const double *sy, const double *sz,
                                   "level_start_source_parent_box_nrs",
                                   "level_start_target_or_target_parent_box_nrs"};
         const DevBuf *flags[4] = {&f_src, &f_tgt, &f_sp, &f_ttp};
+        DevBuf dcnt = dalloc_n<int64_t>(4, st);
+        DevBuf sets[4];
+        for (int k = 0; k < 4; ++k)
+            sets[k] = select_flagged_async(flags[k]->as<uint8_t>(), nb, dcnt.as<int64_t>() + k, st);
+        const std::vector<int64_t> cnt = read_totals(dcnt, 4, st);
         for (int k = 0; k < 4; ++k) {
-            int64_t cnt = 0;
-            DevBuf set = select_flagged(flags[k]->as<uint8_t>(), nb, cnt, st);
             DevBuf ls = dalloc_n<int32_t>(nl + 1, st);
             set_level_starts_kernel<<<1, 64 * ((nl + 64) / 64), 0, st>>>(
-                nl, dls.as<int32_t>(), set.as<int32_t>(), cnt, ls.as<int32_t>());
+                nl, dls.as<int32_t>(), sets[k].as<int32_t>(), cnt[k], ls.as<int32_t>());
             launched("set_level_starts_kernel");
-            put(*S, names[k], 0, cnt, std::move(set));
+            put(*S, names[k], 0, cnt[k], std::move(sets[k]));
             put(*S, lsnames[k], 0, nl + 1, std::move(ls));
         }
         put(*S, "level_start_box_nrs", 0, nl + 1, std::move(dls));
@@ -1111,12 +1264,14 @@ State *build(int64_t nsrc, const double *sx, const double *sy, const double *sz,
     ck(cudaMemsetAsync(err.p, 0, 4, st), "memset");
     for (int l = 0; l < nl; ++l) {
         colleagues_kernel<<<nblocks(level_start[l + 1] - level_start[l]), 256, 0, st>>>(
-            B, level_start[l], level_start[l + 1], coll.as<int32_t>(), ncoll.as<int32_t>(),
+            R, level_start[l], level_start[l + 1], coll.as<int32_t>(), ncoll.as<int32_t>(),
             err.as<int32_t>());
         launched("colleagues_kernel");
     }
 
     // }}}
+
+    mark();   // boxes, sets, colleagues
 
     // {{{ 5. lists
 
@@ -1125,120 +1280,134 @@ State *build(int64_t nsrc, const double *sx, const double *sy, const double *sz,
     const int64_t ntb = TB.n, nttp = TTP.n;
     DevBuf n1 = dalloc_n<int32_t>(ntb, st), n3 = dalloc_n<int32_t>(ntb, st);
     lists13_kernel<<<nblocks(ntb, 128), 128, 0, st>>>(
-        B, coll.as<int32_t>(), ncoll.as<int32_t>(), ntb, TB.buf.as<int32_t>(), 0,
+        R, coll.as<int32_t>(), ncoll.as<int32_t>(), ntb, TB.buf.as<int32_t>(), 0,
         n1.as<int32_t>(), n3.as<int32_t>(), nullptr, nullptr, nullptr, nullptr, err.as<int32_t>());
     launched("lists13_kernel");
-    DevBuf s1, s3;
-    const int64_t t1 = scan_counts(n1.as<int32_t>(), ntb, s1, st);
-    const int64_t t3 = scan_counts(n3.as<int32_t>(), ntb, s3, st);
+    DevBuf n2 = dalloc_n<int32_t>(nttp, st), n4 = dalloc_n<int32_t>(nttp, st);
+    lists24_kernel<<<nblocks(nttp, 128), 128, 0, st>>>(
+        R, coll.as<int32_t>(), ncoll.as<int32_t>(), nttp, TTP.buf.as<int32_t>(), 0,
+        n2.as<int32_t>(), n4.as<int32_t>(), nullptr, nullptr, nullptr, nullptr, nullptr,
+        err.as<int32_t>());
+    launched("lists24_kernel");
+    DevBuf s1, s2, s3, s4;
+    DevBuf dtot = dalloc_n<int64_t>(4, st);
+    scan_counts_async(n1.as<int32_t>(), ntb, s1, dtot.as<int64_t>() + 0, st);
+    scan_counts_async(n2.as<int32_t>(), nttp, s2, dtot.as<int64_t>() + 1, st);
+    scan_counts_async(n3.as<int32_t>(), ntb, s3, dtot.as<int64_t>() + 2, st);
+    scan_counts_async(n4.as<int32_t>(), nttp, s4, dtot.as<int64_t>() + 3, st);
+    const std::vector<int64_t> tot = read_totals(dtot, 4, st);
+    const int64_t t1 = tot[0], t2 = tot[1], t3 = tot[2], t4 = tot[3];
     DevBuf l1 = dalloc_n<int32_t>(t1, st), l3 = dalloc_n<int32_t>(t3, st);
     lists13_kernel<<<nblocks(ntb, 128), 128, 0, st>>>(
-        B, coll.as<int32_t>(), ncoll.as<int32_t>(), ntb, TB.buf.as<int32_t>(), 1, nullptr,
+        R, coll.as<int32_t>(), ncoll.as<int32_t>(), ntb, TB.buf.as<int32_t>(), 1, nullptr,
         nullptr, s1.as<int32_t>(), s3.as<int32_t>(), l1.as<int32_t>(), l3.as<int32_t>(),
         err.as<int32_t>());
     launched("lists13_kernel");
 
-    DevBuf n2 = dalloc_n<int32_t>(nttp, st), n4 = dalloc_n<int32_t>(nttp, st);
-    lists24_kernel<<<nblocks(nttp, 128), 128, 0, st>>>(
-        B, coll.as<int32_t>(), ncoll.as<int32_t>(), nttp, TTP.buf.as<int32_t>(), 0,
-        n2.as<int32_t>(), n4.as<int32_t>(), nullptr, nullptr, nullptr, nullptr, nullptr,
-        err.as<int32_t>());
-    launched("lists24_kernel");
-    DevBuf s2, s4;
-    const int64_t t2 = scan_counts(n2.as<int32_t>(), nttp, s2, st);
-    const int64_t t4 = scan_counts(n4.as<int32_t>(), nttp, s4, st);
     DevBuf l2 = dalloc_n<int32_t>(t2, st), l2c = dalloc_n<int32_t>(t2, st),
            l4 = dalloc_n<int32_t>(t4, st);
     lists24_kernel<<<nblocks(nttp, 128), 128, 0, st>>>(
-        B, coll.as<int32_t>(), ncoll.as<int32_t>(), nttp, TTP.buf.as<int32_t>(), 1, nullptr,
+        R, coll.as<int32_t>(), ncoll.as<int32_t>(), nttp, TTP.buf.as<int32_t>(), 1, nullptr,
         nullptr, s2.as<int32_t>(), s4.as<int32_t>(), l2.as<int32_t>(), l2c.as<int32_t>(),
         l4.as<int32_t>(), err.as<int32_t>());
     launched("lists24_kernel");
     check_err(err, st);
 
-    // List 3 by source level
+    mark();   // lists 1-4
+
+    // List 3 by source level: all (level, target) pairs in one pass
     {
-        std::vector<int64_t> tbls(nl + 1, 0), stoff(nl + 1, 0), lioff(nl + 1, 0);
-        std::vector<DevBuf> tb_parts, st_parts, li_parts;
-        std::vector<int64_t> tb_n, st_n, li_n;
-        DevBuf first = dalloc_n<int32_t>(ntb, st), cnt = dalloc_n<int32_t>(ntb, st);
-        DevBuf flag = dalloc_n<uint8_t>(ntb, st);
-        int64_t ntb_tot = 0, nst_tot = 0, nli_tot = 0;
-        for (int l = 0; l < nl; ++l) {
-            tbls[l] = ntb_tot; stoff[l] = nst_tot; lioff[l] = nli_tot;
-            int64_t nsel = 0;
-            DevBuf sel;
-            if (ntb > 0) {
-                l3_level_count_kernel<<<nblocks(ntb), 256, 0, st>>>(
-                    ntb, s3.as<int32_t>(), l3.as<int32_t>(), level_start[l], level_start[l + 1],
-                    first.as<int32_t>(), cnt.as<int32_t>(), flag.as<uint8_t>());
-                launched("l3_level_count_kernel");
-                sel = select_flagged(flag.as<uint8_t>(), ntb, nsel, st);
-                if (nprob > 1 && nsel > 1) {
-                    // a forest lists these targets problem after problem (target
-                    // level, then Morton, inside a problem): stable sort by problem
-                    DevBuf key = dalloc_n<int32_t>(nsel, st), key2 = dalloc_n<int32_t>(nsel, st);
-                    DevBuf sel2 = dalloc_n<int32_t>(nsel, st);
-                    problem_of_targets_kernel<<<nblocks(nsel), 256, 0, st>>>(
-                        nsel, sel.as<int32_t>(), TB.buf.as<int32_t>(),
-                        S->arrays.at("box_problem").buf.as<int32_t>(), key.as<int32_t>());
-                    launched("problem_of_targets_kernel");
-                    size_t tmp_bytes = 0;
-                    ck(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, key.as<int32_t>(),
-                                                       key2.as<int32_t>(), sel.as<int32_t>(),
-                                                       sel2.as<int32_t>(), (int)nsel, 0, 31, st),
-                       "cub sort (size)");
-                    DevBuf tmp = dalloc(tmp_bytes, st);
-                    ck(cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, key.as<int32_t>(),
-                                                       key2.as<int32_t>(), sel.as<int32_t>(),
-                                                       sel2.as<int32_t>(), (int)nsel, 0, 31, st),
-                       "cub sort");
-                    sel = std::move(sel2);
-                }
-            }
-            DevBuf tbsel = dalloc_n<int32_t>(nsel, st), csel = dalloc_n<int32_t>(nsel, st);
-            if (nsel > 0) {
-                gather_kernel<<<nblocks(nsel), 256, 0, st>>>(nsel, sel.as<int32_t>(),
-                                                             TB.buf.as<int32_t>(), tbsel.as<int32_t>());
-                launched("gather_kernel");
-                gather_kernel<<<nblocks(nsel), 256, 0, st>>>(nsel, sel.as<int32_t>(),
-                                                             cnt.as<int32_t>(), csel.as<int32_t>());
-                launched("gather_kernel");
-            }
-            DevBuf starts;
-            const int64_t nent = scan_counts(csel.as<int32_t>(), nsel, starts, st);
-            DevBuf lst = dalloc_n<int32_t>(nent, st);
-            if (nsel > 0) {
-                gather_segments_kernel<<<nblocks(nsel), 256, 0, st>>>(
-                    nsel, sel.as<int32_t>(), first.as<int32_t>(), starts.as<int32_t>(),
-                    l3.as<int32_t>(), lst.as<int32_t>());
-                launched("gather_segments_kernel");
-            }
-            ntb_tot += nsel;
-            nst_tot += nsel + 1;
-            nli_tot += nent;
-            tb_n.push_back(nsel); st_n.push_back(nsel + 1); li_n.push_back(nent);
-            tb_parts.push_back(std::move(tbsel));
-            st_parts.push_back(std::move(starts));
-            li_parts.push_back(std::move(lst));
+        const int64_t n2d = (int64_t)nl * ntb;
+        DevBuf first2d = dalloc_n<int32_t>(n2d, st), cnt2d = dalloc_n<int32_t>(n2d, st);
+        DevBuf flag2d = dalloc_n<uint8_t>(n2d, st);
+        DevBuf dls = dalloc_n<int32_t>(nl + 1, st);
+        ck(cudaMemcpyAsync(dls.p, level_start.data(), 4 * (nl + 1), cudaMemcpyHostToDevice, st),
+           "upload level starts");
+        int64_t nsel = 0;
+        DevBuf sel;
+        if (ntb > 0) {
+            l3_levels_kernel<<<nblocks(ntb), 256, 0, st>>>(ntb, nl, s3.as<int32_t>(),
+                                                           l3.as<int32_t>(), dls.as<int32_t>(),
+                                                           first2d.as<int32_t>(),
+                                                           cnt2d.as<int32_t>(), flag2d.as<uint8_t>());
+            launched("l3_levels_kernel");
+            sel = select_flagged(flag2d.as<uint8_t>(), n2d, nsel, st);
         }
-        tbls[nl] = ntb_tot; stoff[nl] = nst_tot; lioff[nl] = nli_tot;
-        DevBuf tb_all = dalloc_n<int32_t>(ntb_tot, st), st_all = dalloc_n<int32_t>(nst_tot, st),
-               li_all = dalloc_n<int32_t>(nli_tot, st);
-        for (int l = 0; l < nl; ++l) {
-            copy_d2d(tb_all.as<int32_t>() + tbls[l], tb_parts[l].p, 4 * tb_n[l], st);
-            copy_d2d(st_all.as<int32_t>() + stoff[l], st_parts[l].p, 4 * st_n[l], st);
-            copy_d2d(li_all.as<int32_t>() + lioff[l], li_parts[l].p, 4 * li_n[l], st);
+        DevBuf csel = dalloc_n<int32_t>(nsel, st), fsel = dalloc_n<int32_t>(nsel, st),
+               tbsel = dalloc_n<int32_t>(nsel, st), lsel = dalloc_n<int32_t>(nsel, st);
+        if (nsel > 0) {
+            l3_selected_kernel<<<nblocks(nsel), 256, 0, st>>>(
+                nsel, ntb, sel.as<int32_t>(), cnt2d.as<int32_t>(), first2d.as<int32_t>(),
+                TB.buf.as<int32_t>(), csel.as<int32_t>(), fsel.as<int32_t>(),
+                tbsel.as<int32_t>(), lsel.as<int32_t>());
+            launched("l3_selected_kernel");
         }
-        auto i32v = [](const std::vector<int64_t> &v) {
-            return std::vector<int32_t>(v.begin(), v.end());
-        };
-        put(*S, "sep_smaller_target_boxes", 0, ntb_tot, std::move(tb_all));
-        put_host(*S, "sep_smaller_target_boxes_level_starts", i32v(tbls), st);
-        put(*S, "sep_smaller_starts", 0, nst_tot, std::move(st_all));
-        put_host(*S, "sep_smaller_starts_level_offsets", i32v(stoff), st);
-        put(*S, "sep_smaller_lists", 0, nli_tot, std::move(li_all));
-        put_host(*S, "sep_smaller_lists_level_offsets", i32v(lioff), st);
+        if (nprob > 1 && nsel > 1) {
+            // a forest lists one level's targets problem after problem (target
+            // level, then Morton, inside a problem): stable sort by (level, problem)
+            DevBuf key = dalloc_n<uint64_t>(nsel, st), key2 = dalloc_n<uint64_t>(nsel, st);
+            DevBuf iota = dalloc_n<int32_t>(nsel, st), perm = dalloc_n<int32_t>(nsel, st);
+            l3_forest_key_kernel<<<nblocks(nsel), 256, 0, st>>>(
+                nsel, nprob, lsel.as<int32_t>(), tbsel.as<int32_t>(),
+                S->arrays.at("box_problem").buf.as<int32_t>(), key.as<uint64_t>());
+            launched("l3_forest_key_kernel");
+            iota_kernel<<<nblocks(nsel), 256, 0, st>>>(nsel, iota.as<int32_t>());
+            launched("iota_kernel");
+            size_t tmp_bytes = 0;
+            ck(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, key.as<uint64_t>(),
+                                               key2.as<uint64_t>(), iota.as<int32_t>(),
+                                               perm.as<int32_t>(), (int)nsel, 0, 64, st),
+               "cub sort (size)");
+            DevBuf tmp = dalloc(tmp_bytes, st);
+            ck(cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, key.as<uint64_t>(),
+                                               key2.as<uint64_t>(), iota.as<int32_t>(),
+                                               perm.as<int32_t>(), (int)nsel, 0, 64, st),
+               "cub sort");
+            DevBuf *cols[4] = {&csel, &fsel, &tbsel, &lsel};
+            for (DevBuf *c : cols) {
+                DevBuf out = dalloc_n<int32_t>(nsel, st);
+                permute_kernel<<<nblocks(nsel), 256, 0, st>>>(nsel, perm.as<int32_t>(),
+                                                              c->as<int32_t>(), out.as<int32_t>());
+                launched("permute_kernel");
+                *c = std::move(out);
+            }
+        }
+        DevBuf starts;
+        const int64_t nent = scan_counts(csel.as<int32_t>(), nsel, starts, st);
+        DevBuf li_all = dalloc_n<int32_t>(nent, st);
+        DevBuf bounds = dalloc_n<int64_t>(2 * (nl + 1), st);
+        DevBuf st_all = dalloc_n<int32_t>(nsel + nl, st);
+        l3_bounds_kernel<<<1, 64 * ((nl + 64) / 64), 0, st>>>(nl, nsel, lsel.as<int32_t>(),
+                                                              starts.as<int32_t>(),
+                                                              bounds.as<int64_t>());
+        launched("l3_bounds_kernel");
+        if (nsel > 0) {
+            l3_gather_kernel<<<nblocks(nsel), 256, 0, st>>>(nsel, fsel.as<int32_t>(),
+                                                            starts.as<int32_t>(), l3.as<int32_t>(),
+                                                            li_all.as<int32_t>());
+            launched("l3_gather_kernel");
+        }
+        l3_starts_kernel<<<nblocks(nsel + nl), 256, 0, st>>>(nsel, nl, lsel.as<int32_t>(),
+                                                            starts.as<int32_t>(),
+                                                            bounds.as<int64_t>(),
+                                                            st_all.as<int32_t>());
+        launched("l3_starts_kernel");
+        std::vector<int64_t> hb(2 * (nl + 1));
+        ck(cudaMemcpyAsync(hb.data(), bounds.p, 8 * hb.size(), cudaMemcpyDeviceToHost, st),
+           "copy level bounds");
+        ck(cudaStreamSynchronize(st), "list 3 by level");
+        std::vector<int32_t> tbls(nl + 1), stoff(nl + 1), lioff(nl + 1);
+        for (int l = 0; l <= nl; ++l) {
+            tbls[l] = (int32_t)hb[l];
+            stoff[l] = (int32_t)(hb[l] + l);
+            lioff[l] = (int32_t)hb[nl + 1 + l];
+        }
+        put(*S, "sep_smaller_target_boxes", 0, nsel, std::move(tbsel));
+        put_host(*S, "sep_smaller_target_boxes_level_starts", tbls, st);
+        put(*S, "sep_smaller_starts", 0, nsel + nl, std::move(st_all));
+        put_host(*S, "sep_smaller_starts_level_offsets", stoff, st);
+        put(*S, "sep_smaller_lists", 0, nent, std::move(li_all));
+        put_host(*S, "sep_smaller_lists_level_offsets", lioff, st);
     }
     put(*S, "neighbor_source_boxes_starts", 0, ntb + 1, std::move(s1));
     put(*S, "neighbor_source_boxes_lists", 0, t1, std::move(l1));
@@ -1249,6 +1418,8 @@ State *build(int64_t nsrc, const double *sx, const double *sy, const double *sz,
     put(*S, "from_sep_bigger_lists", 0, t4, std::move(l4));
 
     // }}}
+
+    mark();   // list 3 by level
 
     // {{{ 6. particles, translation classes, scalars
 
@@ -1305,6 +1476,8 @@ State *build(int64_t nsrc, const double *sx, const double *sy, const double *sz,
         put_host(*S, "scalars", std::vector<int32_t>{(int32_t)nb, nl, (int32_t)nsrc,
                                                      (int32_t)ntgt, sat ? 1 : 0}, st);
     }
+    mark();   // particles, classes, scalars
+    put_host(*S, "build_phase_ms", phase_ms, st);
     ck(cudaStreamSynchronize(st), "tree build");
     return S.release();
 
