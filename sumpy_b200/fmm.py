@@ -381,12 +381,12 @@ class SumpyExpansionWrangler:
         return self._view(local_exps, level, self._local_level_starts)
 
     def _dev(self, arr, dtype=torch.int32):
-        """Device copy of a host array (cached per array object)."""
+        """Device copy of a host array (cached per array object and dtype)."""
         if isinstance(arr, torch.Tensor):
             if arr.device.type == "cuda":
                 return arr if arr.dtype == dtype else arr.to(dtype)
             return arr.to(self.device, dtype)
-        key = id(arr)
+        key = (id(arr), dtype)
         hit = self._devcache.get(key)
         if hit is not None and hit[0] is arr:
             return hit[1]
@@ -623,62 +623,63 @@ class SumpyExpansionWrangler:
     def _m2l_plan(self, lev, tgt_boxes, starts, lists, tile=M2L_TILE):
         """Regroup one level's List-2 CSR into (tile, class) GEMM groups.
 
-        Targets are ordered by their octant in the parent, so a tile's
-        targets share the same set of valid classes."""
-        M2L_TILE = tile
+        Targets are ordered by their octant in the parent (then by box
+        number), so a tile's targets share the same set of valid classes;
+        target rank r goes to tile r // tile, slot r % tile, and the groups
+        are the distinct (tile, class) pairs in increasing order. Built on
+        the device (sorts, unique and scatters over the level's entries)."""
         key = (lev, id(lists), tile)
         if key in self._m2l_plans:
             return self._m2l_plans[key]
         tc = self.translation_classes_data
         cls_ls = tc.from_sep_siblings_translation_classes_level_starts
-        ncls = int(cls_ls[lev + 1] - cls_ls[lev])
-        classes = _np_i32(tc.from_sep_siblings_translation_classes)
-        tgt_boxes = _np_i32(tgt_boxes)
-        starts = np.asarray(starts, dtype=np.int64)
-        lists = _np_i32(lists)
-        counts = np.diff(starts)
-        has = counts > 0
-        tpos = np.nonzero(has)[0]
-        if len(tpos) == 0:
+        c0 = int(cls_ls[lev])
+        ncls = int(cls_ls[lev + 1]) - c0
+        dev = self.device
+        i64 = torch.int64
+        starts_h = np.asarray(starts, dtype=np.int64)
+        st = torch.as_tensor(starts_h, device=dev)
+        tb = torch.as_tensor(np.asarray(tgt_boxes, dtype=np.int64), device=dev)
+        counts = st[1:] - st[:-1]
+        tpos = torch.nonzero(counts > 0).flatten()
+        if tpos.numel() == 0:
             self._m2l_plans[key] = None
             return None
-        coords = self.tree.box_coords[:, tgt_boxes[tpos]]
+        coords = self._dev(self.tree.box_coords, i64)[:, tb[tpos]]
         octant = (coords[0] & 1) * 4 + (coords[1] & 1) * 2 + (coords[2] & 1)
-        order = np.lexsort((tgt_boxes[tpos], octant))
+        order = torch.sort(octant * (self.tree.nboxes + 1) + tb[tpos]).indices
         tpos = tpos[order]
-        ntiles = (len(tpos) + M2L_TILE - 1) // M2L_TILE
-        tile_targets = np.full(ntiles * M2L_TILE, -1, dtype=np.int32)
-        tile_targets[:len(tpos)] = tgt_boxes[tpos]
-        # entries
-        rank = np.empty(len(tgt_boxes), dtype=np.int64)
-        rank[tpos] = np.arange(len(tpos))
-        ent_tgt = np.repeat(np.arange(len(tgt_boxes)), counts)
-        e0, e1 = int(starts[0]), int(starts[-1])
-        ent_src = lists[e0:e1]
-        ent_cls = classes[e0:e1] - int(cls_ls[lev])
-        if ent_cls.size and (ent_cls.min() < 0 or ent_cls.max() >= ncls):
+        nt = tpos.numel()
+        ntiles = (nt + tile - 1) // tile
+        tile_targets = torch.full((ntiles * tile,), -1, dtype=torch.int32, device=dev)
+        tile_targets[:nt] = tb[tpos].to(torch.int32)
+        rank = torch.empty(tb.numel(), dtype=i64, device=dev)
+        rank[tpos] = torch.arange(nt, dtype=i64, device=dev)
+        ent_tgt = torch.repeat_interleave(torch.arange(tb.numel(), device=dev), counts)
+        e0, e1 = int(starts_h[0]), int(starts_h[-1])
+        ent_src = self._dev(lists, torch.int32)[e0:e1]
+        ent_cls = self._dev(tc.from_sep_siblings_translation_classes, i64)[e0:e1] - c0
+        if ent_cls.numel() and bool((ent_cls.min() < 0) | (ent_cls.max() >= ncls)):
             raise ValueError(f"translation class out of range on level {lev}")
         r = rank[ent_tgt]
-        tile = r // M2L_TILE
-        slot = r % M2L_TILE
-        gkey = tile * ncls + ent_cls
-        uniq, inv = np.unique(gkey, return_inverse=True)
-        ngroups = len(uniq)
-        group_sources = np.full((ngroups, M2L_TILE), -1, dtype=np.int32)
+        slot = r % tile
+        gkey = (r // tile) * ncls + ent_cls
+        uniq, inv = torch.unique(gkey, sorted=True, return_inverse=True)
+        ngroups = uniq.numel()
+        group_sources = torch.full((ngroups, tile), -1, dtype=torch.int32, device=dev)
         group_sources[inv, slot] = ent_src
         group_tile = uniq // ncls
-        group_class = (uniq % ncls).astype(np.int32)
-        tile_group_starts = np.searchsorted(group_tile, np.arange(ntiles + 1)).astype(np.int32)
-        dev = self.device
+        tile_group_starts = torch.searchsorted(
+            group_tile, torch.arange(ntiles + 1, dtype=i64, device=dev)).to(torch.int32)
         plan = {
             "ntiles": ntiles,
             "ngroups": ngroups,
-            "nentries": int(len(ent_src)),
+            "nentries": e1 - e0,
             "nclasses": ncls,
-            "tile_targets": torch.as_tensor(tile_targets).to(dev),
-            "tile_group_starts": torch.as_tensor(tile_group_starts).to(dev),
-            "group_class": torch.as_tensor(group_class).to(dev),
-            "group_sources": torch.as_tensor(group_sources.ravel()).to(dev),
+            "tile_targets": tile_targets,
+            "tile_group_starts": tile_group_starts,
+            "group_class": (uniq % ncls).to(torch.int32),
+            "group_sources": group_sources.reshape(-1),
         }
         self._m2l_plans[key] = plan
         return plan
@@ -724,22 +725,22 @@ class SumpyExpansionWrangler:
         return local_exps
 
     def _tc_items(self, tiles, groups_per_item=None):
-        """Split tiles (group ranges) into work items of at most
-        ``groups_per_item`` (default ``m2l_item_groups``) groups, largest first
-        (CTAs start roughly in launch order). The same schedule serves the
-        FP64 and the tensor-core GEMMs."""
+        """Split tiles (group ranges ``[(g0, g1), ...]`` or an ``(n, 2)``
+        array) into work items of at most ``groups_per_item`` (default
+        ``m2l_item_groups``) groups, in tile order, then longest first (stable:
+        CTAs start roughly in launch order). The same schedule serves the FP64
+        and the tensor-core GEMMs."""
         gpi = int(groups_per_item or self.m2l_item_groups)
-        it_tile, it_g0, it_g1 = [], [], []
-        for tile, (g0, g1) in enumerate(tiles):
-            for a in range(g0, g1, gpi):
-                it_tile.append(tile)
-                it_g0.append(a)
-                it_g1.append(min(g1, a + gpi))
-        it_tile = np.array(it_tile, dtype=np.int32)
-        it_g0 = np.array(it_g0, dtype=np.int32)
-        it_g1 = np.array(it_g1, dtype=np.int32)
+        t = np.asarray(tiles, dtype=np.int64).reshape(-1, 2)
+        g0, g1 = t[:, 0], t[:, 1]
+        nit = np.maximum(g1 - g0 + gpi - 1, 0) // gpi
+        it_tile = np.repeat(np.arange(len(t), dtype=np.int64), nit)
+        j = _expand_ranges(np.zeros(len(t), dtype=np.int64), nit)
+        it_g0 = g0[it_tile] + j * gpi
+        it_g1 = np.minimum(g1[it_tile], it_g0 + gpi)
         order = np.argsort(-(it_g1 - it_g0), kind="stable")
-        return it_tile[order], it_g0[order], it_g1[order]
+        return (it_tile[order].astype(np.int32), it_g0[order].astype(np.int32),
+                it_g1[order].astype(np.int32))
 
     def _m2l_merged_plan(self, levels, ltb, tboxes, starts, lists, tile):
         """One GEMM schedule over all M2L levels: the per-level (tile, class)
@@ -751,6 +752,7 @@ class SumpyExpansionWrangler:
         tt, tsc, gcl, gsrc, tiles = [], [], [], [], []
         mats_list, mats_index = [], {}
         ntiles = ngroups = 0
+        dev = self.device
         for lev in levels:
             a, b = int(ltb[lev]), int(ltb[lev + 1])
             p = self._m2l_plan(lev, tboxes[a:b], starts[a:b + 1], lists, tile)
@@ -761,31 +763,29 @@ class SumpyExpansionWrangler:
             if mkey not in mats_index:
                 mats_index[mkey] = sum(m.shape[0] for m in mats_list)
                 mats_list.append(mats)
-            tgs = p["tile_group_starts"].cpu().numpy()
-            tiles += [(ngroups + int(tgs[i]), ngroups + int(tgs[i + 1]))
-                      for i in range(p["ntiles"])]
-            tt.append(p["tile_targets"].cpu().numpy())
-            tsc.append(np.full(p["ntiles"], mscale))
-            gcl.append(p["group_class"].cpu().numpy() + mats_index[mkey])
-            gsrc.append(p["group_sources"].cpu().numpy())
+            tgs = p["tile_group_starts"].cpu().numpy().astype(np.int64) + ngroups
+            tiles.append(np.stack([tgs[:-1], tgs[1:]], axis=1))
+            tt.append(p["tile_targets"])
+            tsc.append(torch.full((p["ntiles"],), mscale, dtype=torch.float64, device=dev))
+            gcl.append(p["group_class"] + mats_index[mkey])
+            gsrc.append(p["group_sources"])
             ntiles += p["ntiles"]
             ngroups += p["ngroups"]
         if ntiles == 0:
             self._m2l_plans[key] = None
             return None
-        it_tile, it_g0, it_g1 = self._tc_items(tiles)
+        it_tile, it_g0, it_g1 = self._tc_items(np.concatenate(tiles))
         mats = mats_list[0] if len(mats_list) == 1 else torch.cat(mats_list)
-        dev = self.device
         plan = {
             "nitems": len(it_tile), "ntiles": ntiles, "ngroups": ngroups,
             "nclasses": int(mats.shape[0]), "mats": mats,
             "item_tile": torch.as_tensor(it_tile).to(dev),
             "item_g0": torch.as_tensor(it_g0).to(dev),
             "item_g1": torch.as_tensor(it_g1).to(dev),
-            "tile_targets": torch.as_tensor(np.concatenate(tt)).to(dev),
-            "tile_scale": torch.as_tensor(np.concatenate(tsc)).to(dev),
-            "group_class": torch.as_tensor(np.concatenate(gcl).astype(np.int32)).to(dev),
-            "group_sources": torch.as_tensor(np.concatenate(gsrc)).to(dev),
+            "tile_targets": torch.cat(tt),
+            "tile_scale": torch.cat(tsc),
+            "group_class": torch.cat(gcl).to(torch.int32),
+            "group_sources": torch.cat(gsrc),
         }
         self._m2l_plans[key] = plan
         return plan
@@ -795,9 +795,8 @@ class SumpyExpansionWrangler:
         run one launch each)."""
         key = ("items", lev, id(plan), self.m2l_item_groups)
         if key not in self._m2l_plans:
-            tgs = plan["tile_group_starts"].cpu().numpy()
-            tiles = [(int(tgs[i]), int(tgs[i + 1])) for i in range(plan["ntiles"])]
-            it_tile, it_g0, it_g1 = self._tc_items(tiles)
+            tgs = plan["tile_group_starts"].cpu().numpy().astype(np.int64)
+            it_tile, it_g0, it_g1 = self._tc_items(np.stack([tgs[:-1], tgs[1:]], axis=1))
             dev = self.device
             self._m2l_plans[key] = dict(
                 plan, nitems=len(it_tile), item_tile=torch.as_tensor(it_tile).to(dev),
