@@ -310,9 +310,34 @@ int sumpy_class_gemm_tf32x3(
  * two seconds). Budgets below 1e6 cycles poll the barriers without letting
  * the hardware suspend the waiting thread. No counterpart in sumpy (its
  * kernels have no waits); it exists so that tests and callers with a
- * deadline can bound a launch. Process-wide; returns SUMPY_OK. */
+ * deadline can bound a launch. Also bounds the level waits of
+ * sumpy_class_gemm_chain_f64. Process-wide; returns SUMPY_OK. */
 int sumpy_set_tc_wait_cycles(int64_t cycles);
 int64_t sumpy_get_tc_wait_cycles(void);
+
+/* The FP64 class GEMMs of several tree levels chained in one persistent
+ * launch: M2M (E2EFromChildren, sumpy/e2e.py:866-978, driven level by level
+ * by coarsen_multipoles, sumpy/fmm.py:643-695) or L2L (E2EFromParent,
+ * sumpy/e2e.py:985-1083, driven by refine_locals, sumpy/fmm.py:1004-1045) as
+ * octant class GEMMs, where each level's sources are the previous level's
+ * targets. Step L of the chain owns work units [step_unit_start[L],
+ * step_unit_start[L + 1]) -- unit u = (item, row block, k part) with items
+ * from step_item_start[L] and step_ksplit[L] K parts (DEVICE int32 arrays) --
+ * and the item arrays are those of sumpy_class_gemm_f64 with tile_width 64,
+ * concatenated over the steps; expansions of all levels are rows (box ids)
+ * of one flat [nboxes][n] array, accumulated in place. A device counter
+ * hands out units in order; a unit of step L starts when all of step L - 1
+ * have finished (queue: DEVICE int32 [1 + nsteps], cleared by this call).
+ * Each wait is bounded by the budget of sumpy_set_tc_wait_cycles; one that
+ * runs out writes 2 to *status and stops its CTA. total_units (host) sizes
+ * the grid; nsteps <= 64. */
+int sumpy_class_gemm_chain_f64(
+    int32_t n, int32_t nsteps, const int32_t *step_unit_start, const int32_t *step_item_start,
+    const int32_t *step_ksplit, int32_t total_units, const int32_t *item_tile,
+    const int32_t *item_group_begin, const int32_t *item_group_end, int32_t tile_width,
+    const int32_t *tile_targets, const double *tile_scale, const int32_t *group_class,
+    const int32_t *group_sources, const double *class_matrices, double *expansions,
+    int32_t *queue, int32_t *status, void *stream);
 
 /* Same M2L as sumpy_m2l_translation_classes_tf32x3, for callers that cannot
  * allocate device memory while they run (a host application with a fixed

@@ -83,6 +83,8 @@ SIGNATURES = {
                                                   i64, dbl, ptr, ptr, ptr],
     "sumpy_class_gemm_f64": [i32, i32, i32, ptr, ptr, ptr, i32, ptr, ptr, ptr, ptr, i32, ptr,
                              i32, ptr, i32, ptr, ptr],
+    "sumpy_class_gemm_chain_f64": [i32, i32, ptr, ptr, ptr, i32, ptr, ptr, ptr, i32, ptr, ptr,
+                                   ptr, ptr, ptr, ptr, ptr, ptr, ptr],
     "sumpy_class_gemm_tf32x3": [i32, i32, i32, ptr, ptr, ptr, i32, ptr, ptr, ptr, ptr, i32, ptr,
                                 ptr, i32, i32, i32, i32, ptr, ptr, i32, ptr, ptr, ptr],
     "sumpy_helmholtz_p2e_from_single_box_levels_f64": [cint, dbl, i32, ptr, ptr, ptr, ptr, i64,

@@ -12,6 +12,12 @@ namespace sumpy {
 
 void set_last_error(const std::string &msg);
 
+// Budget, in SM clock cycles (clock64), of every bounded wait in the
+// kernels that wait (tensor-core barrier waits, level-chained GEMM steps);
+// default 4e9 (~2 s), process-wide, set by sumpy_set_tc_wait_cycles.
+constexpr long long DEFAULT_WAIT_CYCLES = 4000000000LL;
+long long wait_cycles_budget();
+
 inline int check_launch(const char *what)
 {
     cudaError_t e = cudaGetLastError();

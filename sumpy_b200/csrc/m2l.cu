@@ -19,6 +19,8 @@
 // tx + 8 c (r, c < 8): each shared-memory read of a k-step is conflict-free.
 // The next k-chunk of both operands is fetched into registers while the
 // current one is multiplied.
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace sumpy {
@@ -36,7 +38,9 @@ struct Chunk {
     double b[B_PER];
 };
 
-template <int ROWS>
+// CG: read the source expansions through L2 only (ld.global.cg) -- needed
+// when other CTAs of the same launch wrote them (the level-chained kernel)
+template <int ROWS, bool CG = false>
 __device__ __forceinline__ void fetch(Chunk<ROWS> &ch, const double *__restrict__ A,
                                       const double *__restrict__ src, const int32_t *srcs, int n,
                                       int row0, int k0, int32_t sbase)
@@ -55,18 +59,26 @@ __device__ __forceinline__ void fetch(Chunk<ROWS> &ch, const double *__restrict_
         const int slot = idx / KC, kk = idx % KC;
         const int32_t s = srcs[slot];
         const int k = k0 + kk;
-        ch.b[u] = (s >= 0 && k < n) ? src[(int64_t)(s - sbase) * n + k] : 0.0;
+        const double *p = src + (int64_t)(s - sbase) * n + k;
+        ch.b[u] = (s >= 0 && k < n) ? (CG ? __ldcg(p) : *p) : 0.0;
     }
 }
 
-template <int ROWS>
-__global__ void __launch_bounds__(ROWS)
-m2l_f64_kernel(int n, const int32_t *__restrict__ item_tile, const int32_t *__restrict__ item_g0,
-               const int32_t *__restrict__ item_g1, const int32_t *__restrict__ tile_targets,
-               const double *__restrict__ tile_scale, const int32_t *__restrict__ group_class,
-               const int32_t *__restrict__ group_sources, const double *__restrict__ mats,
-               int32_t sbase, const double *__restrict__ src, int32_t tbase,
-               double *__restrict__ tgt)
+// One work item (a range of class groups of one tile) for output rows
+// [row0, row0 + ROWS) and k-chunks [kcb, kcb + nkc): C += T_c * B_g over the
+// item's groups, accumulated in registers and added to the local expansions
+// with FP64 atomics (items of one tile may overlap in time). Thread (ty, tx)
+// owns rows ty + (ROWS/8) r and target slots tx + 8 c (r, c < 8): each
+// shared-memory read of a k-step is conflict-free. The next k-chunk of both
+// operands is fetched into registers while the current one is multiplied.
+template <int ROWS, bool CG>
+__device__ __forceinline__ void class_gemm_item(
+    int n, int item, int row0, int kcb, int nkc, const int32_t *__restrict__ item_tile,
+    const int32_t *__restrict__ item_g0, const int32_t *__restrict__ item_g1,
+    const int32_t *__restrict__ tile_targets, const double *__restrict__ tile_scale,
+    const int32_t *__restrict__ group_class, const int32_t *__restrict__ group_sources,
+    const double *__restrict__ mats, int32_t sbase, const double *__restrict__ src,
+    int32_t tbase, double *__restrict__ tgt)
 {
     constexpr int NT = ROWS;          // (ROWS / 8) x 8 threads
     constexpr int RG = ROWS / 8;      // row groups
@@ -74,16 +86,10 @@ m2l_f64_kernel(int n, const int32_t *__restrict__ item_tile, const int32_t *__re
     __shared__ double Bs[2][KC][TW + 1];
     __shared__ int32_t srcs[2][TW];
 
-    const int item = blockIdx.x;
     const int tile = item_tile[item];
     const int g0 = item_g0[item], g1 = item_g1[item];
-    const int row0 = blockIdx.y * ROWS;
     const int tid = threadIdx.x;
     const int tx = tid % 8, ty = tid / 8;
-    // split K: CTA z of gridDim.z takes k-chunks [kcb, kce) (all when 1)
-    const int nkc_all = (n + KC - 1) / KC;
-    const int kcb = (int)((int64_t)blockIdx.z * nkc_all / gridDim.z);
-    const int nkc = (int)((int64_t)(blockIdx.z + 1) * nkc_all / gridDim.z) - kcb;
     const int total = (g1 - g0) * nkc;
     if (total <= 0) return;
 
@@ -109,42 +115,40 @@ m2l_f64_kernel(int n, const int32_t *__restrict__ item_tile, const int32_t *__re
         }
     };
 
-    if (total > 0) {
-        Chunk<ROWS> ch;
-        load_srcs(g0, 0);
-        __syncthreads();
-        fetch<ROWS>(ch, mats + (int64_t)group_class[g0] * n * n, src, srcs[0], n, row0,
+    Chunk<ROWS> ch;
+    load_srcs(g0, 0);
+    __syncthreads();
+    fetch<ROWS, CG>(ch, mats + (int64_t)group_class[g0] * n * n, src, srcs[0], n, row0,
                     kcb * KC, sbase);
-        store(ch, 0);
-        __syncthreads();
-        for (int it = 0; it < total; ++it) {
-            const int buf = it & 1;
-            const int nxt = it + 1;
-            if (nxt < total) {
-                const int g = g0 + nxt / nkc, kc = nxt % nkc;
-                const int sb = (g - g0) & 1;
-                if (kc == 0) {
-                    load_srcs(g, sb);
-                    __syncthreads();
-                }
-                fetch<ROWS>(ch, mats + (int64_t)group_class[g] * n * n, src, srcs[sb], n, row0,
+    store(ch, 0);
+    __syncthreads();
+    for (int it = 0; it < total; ++it) {
+        const int buf = it & 1;
+        const int nxt = it + 1;
+        if (nxt < total) {
+            const int g = g0 + nxt / nkc, kc = nxt % nkc;
+            const int sb = (g - g0) & 1;
+            if (kc == 0) {
+                load_srcs(g, sb);
+                __syncthreads();
+            }
+            fetch<ROWS, CG>(ch, mats + (int64_t)group_class[g] * n * n, src, srcs[sb], n, row0,
                             (kcb + kc) * KC, sbase);
-            }
-#pragma unroll 4
-            for (int kk = 0; kk < KC; ++kk) {
-                double a[8], b[8];
-#pragma unroll
-                for (int r = 0; r < 8; ++r) a[r] = As[buf][kk][ty + RG * r];
-#pragma unroll
-                for (int c = 0; c < 8; ++c) b[c] = Bs[buf][kk][tx + 8 * c];
-#pragma unroll
-                for (int r = 0; r < 8; ++r)
-#pragma unroll
-                    for (int c = 0; c < 8; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
-            }
-            if (nxt < total) store(ch, buf ^ 1);
-            __syncthreads();
         }
+#pragma unroll 4
+        for (int kk = 0; kk < KC; ++kk) {
+            double a[8], b[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) a[r] = As[buf][kk][ty + RG * r];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) b[c] = Bs[buf][kk][tx + 8 * c];
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+#pragma unroll
+                for (int c = 0; c < 8; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+        }
+        if (nxt < total) store(ch, buf ^ 1);
+        __syncthreads();
     }
     const double scale = tile_scale[tile];
 #pragma unroll
@@ -157,6 +161,105 @@ m2l_f64_kernel(int n, const int32_t *__restrict__ item_tile, const int32_t *__re
             const int row = row0 + ty + RG * r;
             if (row < n) atomicAdd(o + row, scale * acc[r][c]);
         }
+    }
+}
+
+template <int ROWS>
+__global__ void __launch_bounds__(ROWS)
+m2l_f64_kernel(int n, const int32_t *__restrict__ item_tile, const int32_t *__restrict__ item_g0,
+               const int32_t *__restrict__ item_g1, const int32_t *__restrict__ tile_targets,
+               const double *__restrict__ tile_scale, const int32_t *__restrict__ group_class,
+               const int32_t *__restrict__ group_sources, const double *__restrict__ mats,
+               int32_t sbase, const double *__restrict__ src, int32_t tbase,
+               double *__restrict__ tgt)
+{
+    // split K: CTA z of gridDim.z takes k-chunks [kcb, kcb + nkc) (all when 1)
+    const int nkc_all = (n + KC - 1) / KC;
+    const int kcb = (int)((int64_t)blockIdx.z * nkc_all / gridDim.z);
+    const int nkc = (int)((int64_t)(blockIdx.z + 1) * nkc_all / gridDim.z) - kcb;
+    class_gemm_item<ROWS, false>(n, blockIdx.x, blockIdx.y * ROWS, kcb, nkc, item_tile, item_g0,
+                                 item_g1, tile_targets, tile_scale, group_class, group_sources,
+                                 mats, sbase, src, tbase, tgt);
+}
+
+// Level-chained form for M2M / L2L: the GEMMs of all levels in one
+// persistent launch. Work units (item, row block, k-chunk range) of all
+// levels are numbered level after level in the order the chain runs (M2M:
+// finest parents first; L2L: coarsest children first) and handed out by an
+// atomic counter; a unit of chain step L starts once every unit of step L - 1
+// has finished (a per-step done counter), because its sources are that
+// step's targets. Units are dispatched in order only to running CTAs, so the
+// units a waiting CTA depends on are held by running CTAs: no deadlock, with
+// or without co-residency. Each wait is bounded (the process-wide wait
+// budget); a wait that runs out writes status 2 and stops the CTA.
+// Expansions of every level live in one flat [nboxes][n] array (box ids are
+// rows); sources written earlier in the launch are read through L2.
+struct ChainArgs {
+    int n, nsteps;
+    const int32_t *step_unit_start;    // [nsteps + 1] first unit of each step
+    const int32_t *step_item_start;    // [nsteps] first item of each step
+    const int32_t *step_ksplit;        // [nsteps]
+    int32_t nrowblk;
+    const int32_t *item_tile, *item_g0, *item_g1, *tile_targets;
+    const double *tile_scale;
+    const int32_t *group_class, *group_sources;
+    const double *mats;
+    double *expansions;
+    int32_t *queue;                    // [0] next unit, [1 + L] units of step L done
+    int32_t *status;
+    long long wait_cycles;
+};
+
+constexpr int CHAIN_MAX_STEPS = 64;
+
+template <int ROWS>
+__global__ void __launch_bounds__(ROWS)
+class_gemm_chain_kernel(ChainArgs a)
+{
+    __shared__ int32_t s_unit_start[CHAIN_MAX_STEPS + 1];
+    __shared__ int s_unit, s_stop;
+    for (int i = threadIdx.x; i <= a.nsteps; i += blockDim.x) s_unit_start[i] = a.step_unit_start[i];
+    __syncthreads();
+    const int total = s_unit_start[a.nsteps];
+    const int nkc_all = (a.n + KC - 1) / KC;
+    while (true) {
+        if (threadIdx.x == 0) {
+            s_unit = atomicAdd(a.queue, 1);
+            s_stop = 0;
+        }
+        __syncthreads();
+        const int u = s_unit;
+        if (u >= total) break;
+        int L = 0;
+        while (L + 1 < a.nsteps && s_unit_start[L + 1] <= u) ++L;
+        if (threadIdx.x == 0 && L > 0) {
+            const int need = s_unit_start[L] - s_unit_start[L - 1];
+            const long long t0 = clock64();
+            while (*reinterpret_cast<volatile int32_t *>(a.queue + L) < need) {
+                if (clock64() - t0 > a.wait_cycles) {
+                    s_stop = 1;
+                    if (a.status) atomicExch(a.status, 2);
+                    break;
+                }
+            }
+            __threadfence();
+        }
+        __syncthreads();
+        if (s_stop) break;
+        const int ks = a.step_ksplit[L];
+        const int local = u - s_unit_start[L];
+        const int per_item = a.nrowblk * ks;
+        const int item = a.step_item_start[L] + local / per_item;
+        const int rem = local % per_item;
+        const int y = rem / ks, z = rem % ks;
+        const int kcb = (int)((int64_t)z * nkc_all / ks);
+        const int nkc = (int)((int64_t)(z + 1) * nkc_all / ks) - kcb;
+        class_gemm_item<ROWS, true>(a.n, item, y * ROWS, kcb, nkc, a.item_tile, a.item_g0,
+                                    a.item_g1, a.tile_targets, a.tile_scale, a.group_class,
+                                    a.group_sources, a.mats, 0, a.expansions, 0, a.expansions);
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) atomicAdd(a.queue + 1 + L, 1);
     }
 }
 
@@ -249,6 +352,53 @@ int sumpy_class_gemm_f64(
                           tile_targets, tile_scale, group_class, group_sources, nclasses,
                           class_matrices, src_base_ibox, src_expansions, tgt_base_ibox,
                           tgt_expansions, stream, k_split);
+}
+
+int sumpy_class_gemm_chain_f64(
+    int32_t n, int32_t nsteps, const int32_t *step_unit_start, const int32_t *step_item_start,
+    const int32_t *step_ksplit, int32_t total_units, const int32_t *item_tile,
+    const int32_t *item_group_begin, const int32_t *item_group_end, int32_t tile_width,
+    const int32_t *tile_targets, const double *tile_scale, const int32_t *group_class,
+    const int32_t *group_sources, const double *class_matrices, double *expansions,
+    int32_t *queue, int32_t *status, void *stream)
+{
+    if (n < 1 || n > 2 * ncoeff_of(SUMPY_MAX_ORDER)) return bad_arg("class gemm chain: bad n");
+    if (tile_width != TW) return bad_arg("class gemm chain: tile_width must be 64");
+    if (nsteps < 0 || nsteps > CHAIN_MAX_STEPS) return bad_arg("class gemm chain: nsteps in [0, 64]");
+    if (total_units < 0) return bad_arg("class gemm chain: negative unit count");
+    if (nsteps == 0 || total_units == 0) return SUMPY_OK;
+    if (!step_unit_start || !step_item_start || !step_ksplit || !item_tile || !item_group_begin ||
+        !item_group_end || !tile_targets || !tile_scale || !group_class || !group_sources ||
+        !class_matrices || !expansions || !queue)
+        return bad_arg("class gemm chain: null pointer argument");
+    cudaStream_t st = as_stream(stream);
+    cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(int32_t) * (1 + nsteps), st);
+    if (e != cudaSuccess) return check_launch("class gemm chain: clearing the queue");
+    ChainArgs a;
+    a.n = n; a.nsteps = nsteps;
+    a.step_unit_start = step_unit_start; a.step_item_start = step_item_start;
+    a.step_ksplit = step_ksplit;
+    a.item_tile = item_tile; a.item_g0 = item_group_begin; a.item_g1 = item_group_end;
+    a.tile_targets = tile_targets; a.tile_scale = tile_scale;
+    a.group_class = group_class; a.group_sources = group_sources; a.mats = class_matrices;
+    a.expansions = expansions; a.queue = queue; a.status = status;
+    a.wait_cycles = wait_cycles_budget();
+    int dev = 0, sms = 148, per_sm = 1;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return bad_arg("class gemm chain: no device");
+    if (n <= 64) {
+        a.nrowblk = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, class_gemm_chain_kernel<64>, 64, 0);
+        const int grid = std::max(1, std::min(total_units, sms * std::max(per_sm, 1)));
+        class_gemm_chain_kernel<64><<<grid, 64, 0, st>>>(a);
+    } else {
+        a.nrowblk = (n + 127) / 128;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, class_gemm_chain_kernel<128>, 128, 0);
+        const int grid = std::max(1, std::min(total_units, sms * std::max(per_sm, 1)));
+        class_gemm_chain_kernel<128><<<grid, 128, 0, st>>>(a);
+    }
+    return check_launch("class_gemm_chain_kernel");
 }
 
 }  // extern "C"

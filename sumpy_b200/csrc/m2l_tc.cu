@@ -72,9 +72,7 @@ constexpr int STAGE = 4 * PLANE;           // A_hi, A_lo, B_hi, B_lo
 constexpr int TC_SMEM = TC_STAGES * STAGE + 1024 /* alignment slack */ + 256 /* barriers */;
 static_assert(TC_SMEM <= 227 * 1024, "shared memory per CTA");
 constexpr uint32_t TMEM_COLS = 256;         // two 128-column accumulators
-// default budget of every wait (~2 s at 2 GHz); a process can lower it with
-// sumpy_set_tc_wait_cycles (tests make waits expire this way)
-constexpr long long WAIT_CYCLES = 4000000000LL;
+// (the budget of every wait is wait_cycles_budget(), common.cuh)
 // budgets below this poll the barrier without suspending the thread, so that
 // a short budget is measured in cycles rather than in hardware suspend windows
 constexpr long long SHORT_WAIT = 1000000LL;
@@ -590,9 +588,6 @@ int sumpy_split_tf32x2(int64_t nmat, int32_t rows, int32_t cols, const double *i
     return check_launch("split_tf32x2_kernel");
 }
 
-// budget of the tensor-core kernels' barrier waits, read at each launch
-static std::atomic<long long> g_wait_cycles{WAIT_CYCLES};
-
 using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
                                     const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
                                     const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
@@ -682,7 +677,7 @@ static int m2l_tf32x3_launch(
     a.src_hi = src_hi; a.src_lo = src_lo;
     a.src_row_base = src_base_ibox; a.zero_row = src_nrows - 1;
     a.tbase = tgt_base_ibox; a.tgt = tgt_expansions; a.status = status;
-    a.wait_cycles = g_wait_cycles.load(std::memory_order_relaxed);
+    a.wait_cycles = wait_cycles_budget();
     dim3 grid(nitems, rows_pad / TC_M, k_split);
     m2l_tf32x3_kernel<<<grid, TC_THREADS, TC_SMEM, as_stream(stream)>>>(a, ma_hi, ma_lo, mb_hi,
                                                                         mb_lo);
@@ -690,14 +685,6 @@ static int m2l_tf32x3_launch(
 }
 
 extern "C" {
-
-int sumpy_set_tc_wait_cycles(int64_t cycles)
-{
-    g_wait_cycles.store(cycles > 0 ? (long long)cycles : WAIT_CYCLES, std::memory_order_relaxed);
-    return SUMPY_OK;
-}
-
-int64_t sumpy_get_tc_wait_cycles(void) { return g_wait_cycles.load(std::memory_order_relaxed); }
 
 int sumpy_m2l_translation_classes_tf32x3(
     int order, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,

@@ -348,7 +348,10 @@ def main():
                     choices=["laplace", "helmholtz"])
     ap.add_argument("--laplace-orders", nargs="+", type=int, default=[2, 3, 4, 5, 6, 8])
     ap.add_argument("--helmholtz-orders", nargs="+", type=int, default=[2, 3, 4])
+    ap.add_argument("--out-dir", default=None,
+                    help="write the JSON files here instead of next to this script")
     args = ap.parse_args()
+    out_lap = OUT if args.out_dir is None else Path(args.out_dir) / OUT.name
     if not REF:
         sys.exit("set SUMPY_REFERENCE to the root of a sumpy source tree")
     _install_placeholders()
@@ -356,12 +359,12 @@ def main():
     HELM_K = sympy.Rational(5, 2)
     lap, helm = _kernels()
     if "laplace" in args.which:
-        data = generate(lap, tuple(args.laplace_orders), OUT, "laplace", False, {})
+        data = generate(lap, tuple(args.laplace_orders), out_lap, "laplace", False, {})
         data["kernel"] = "LaplaceKernel(3), expression 1/|d| (scaling applied on output)"
-        OUT.write_text(json.dumps(data, indent=1))
-        print("wrote", OUT)
+        out_lap.write_text(json.dumps(data, indent=1))
+        print("wrote", out_lap)
     if "helmholtz" in args.which:
-        out = OUT.with_name("helmholtz3d_operators.json")
+        out = out_lap.with_name("helmholtz3d_operators.json")
         data = generate(helm, tuple(args.helmholtz_orders), out, "helmholtz", True,
                         {sympy.Symbol("k"): HELM_K})
         data["kernel"] = ("HelmholtzKernel(3), expression exp(i k |d|)/|d| with k = 5/2 "
