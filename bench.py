@@ -992,7 +992,7 @@ def batched_bench(dev, steps=5, warmup=3, nproblems=512, order=8, nseq=16):
             "note": "drive_fmm per problem, warm, same kernels; whole-batch time "
                     "extrapolated by points"},
         "batch_over_one_at_a_time": (ntot / (ms_graph * 1e-3) / 1e6) / seq_rate,
-        "m2l_item_groups": b.wrangler.m2l_item_groups,
+        "schedule": b.schedule,
         "relL2_vs_direct": errs,
         "forest_build_s": round(t_build, 2), "capture_s": round(t_capture, 2),
     }

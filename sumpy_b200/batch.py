@@ -39,7 +39,8 @@ class BatchedLaplaceFMM:
     :arg precision: ``"fp64"`` or ``"mixed"`` (see :class:`SumpyExpansionWrangler`).
     :arg bbox: common root box, ``(3, 2)``; default the batch's bounding cube.
     :arg use_graph: replay a captured CUDA graph (True) or launch eagerly.
-    :arg autotune: choose ``m2l_item_groups`` by timing (cached on disk).
+    :arg autotune: choose the schedule knobs by timing (coordinate descent,
+        cached on disk; :func:`sumpy_b200.autotune.tune_schedule`).
     :arg gpu_tree: build the forest on the GPU in one pass (default) instead
         of host trees merged on the host (the same arrays either way).
     """
@@ -66,10 +67,11 @@ class BatchedLaplaceFMM:
         self._w = torch.zeros(tree.nsources, dtype=torch.float64, device=self.device)
         self._graph = None
         self._out = None
+        self.schedule = self.wrangler.schedule()
         if autotune:
-            from sumpy_b200.autotune import tune_m2l_item_groups
-            tune_m2l_item_groups(self.wrangler, lambda: self._eager(self._w),
-                                 path=autotune_cache)
+            from sumpy_b200.autotune import tune_schedule
+            self.schedule = tune_schedule(self.wrangler, lambda: self._eager(self._w),
+                                          path=autotune_cache)
 
     @property
     def nsources(self):

@@ -326,6 +326,29 @@ class SumpyExpansionWrangler:
         self.m2l_item_groups = int(m2l_item_groups or M2L_ITEM_GROUPS)
         if self.m2l_item_groups < 1:
             raise ValueError("m2l_item_groups must be >= 1")
+        # rounds (one source box / 32 sources each) per List-3 / List-4 item
+        self.item_rounds = ITEM_ROUNDS
+        # the octant (M2M / L2L) GEMMs of a level are cut into enough items
+        # and K parts to cover the SMs this many times
+        self.octant_split = 2
+
+    SCHEDULE_KNOBS = ("m2l_item_groups", "item_rounds", "octant_split", "chain_levels",
+                      "concurrent_stages")
+
+    def set_schedule(self, **knobs):
+        """Change schedule knobs (:attr:`SCHEDULE_KNOBS`); work plans are
+        cached per knob value, and a captured CUDA graph of the evaluation is
+        dropped so that the next call captures the new schedule."""
+        for k, v in knobs.items():
+            if k not in self.SCHEDULE_KNOBS:
+                raise ValueError(f"unknown schedule knob {k!r}")
+            if k in ("m2l_item_groups", "item_rounds", "octant_split") and int(v) < 1:
+                raise ValueError(f"{k} must be >= 1")
+            setattr(self, k, type(getattr(self, k))(v))
+        self._graph_cache = None
+
+    def schedule(self):
+        return {k: getattr(self, k) for k in self.SCHEDULE_KNOBS}
 
     # {{{ geometry, storage
 
@@ -956,7 +979,7 @@ class SumpyExpansionWrangler:
         # it into enough items (CTAs) to cover the GPU twice, down to one
         # octant group per item, so few tiles do not leave one CTA pipelining
         # all eight groups
-        gpi = min(8, max(1, -(-len(groups) // (2 * self._sm_count))))
+        gpi = min(8, max(1, -(-len(groups) // (self.octant_split * self._sm_count))))
         it_tile, it_g0, it_g1 = self._tc_items(tiles, gpi)
         dev = self.device
         plan = {
@@ -982,7 +1005,7 @@ class SumpyExpansionWrangler:
         def k_split(row_tiles, nkc, cap):
             # a level's octant GEMM is on the level-serial chain: few items
             # also split K (partial sums meet in the FP64 atomic epilogue)
-            want = -(-2 * self._sm_count // max(1, plan["nitems"] * row_tiles))
+            want = -(-self.octant_split * self._sm_count // max(1, plan["nitems"] * row_tiles))
             return int(max(1, min(nkc, cap, want)))
 
         if fp64:
@@ -1022,7 +1045,7 @@ class SumpyExpansionWrangler:
             a, b = int(lsp[tgt_lev]), int(lsp[tgt_lev + 1])
             if a == b:
                 continue
-            key = ("m2m-plan", tgt_lev, id(source_parent_boxes), fp64)
+            key = ("m2m-plan", tgt_lev, id(source_parent_boxes), fp64, self.octant_split)
             if key not in self._m2l_plans:
                 parents = parents_all[a:b]
                 kids = child[:, parents]                       # [slot][parent]
@@ -1056,7 +1079,8 @@ class SumpyExpansionWrangler:
             a, b = int(lt[tgt_lev]), int(lt[tgt_lev + 1])
             if a == b:
                 continue
-            key = ("l2l-plan", tgt_lev, id(target_or_target_parent_boxes), fp64)
+            key = ("l2l-plan", tgt_lev, id(target_or_target_parent_boxes), fp64,
+                   self.octant_split)
             if key not in self._m2l_plans:
                 kids = boxes_all[a:b]
                 oc = self._octants(kids)
@@ -1098,7 +1122,7 @@ class SumpyExpansionWrangler:
             unit_start, item_start, ksplit = [0], [], []
             ntiles = ngroups = nitems = 0
             for p in plans:
-                want = -(-2 * self._sm_count // max(1, p["nitems"] * row_tiles))
+                want = -(-self.octant_split * self._sm_count // max(1, p["nitems"] * row_tiles))
                 ks = int(max(1, min(nkc, 8, want)))
                 it_t.append(p["item_tile"] + ntiles)
                 it_a.append(p["item_g0"] + ngroups)
@@ -1187,12 +1211,13 @@ class SumpyExpansionWrangler:
                                mpole_exps, pot):
         def build():
             items, lists = m2p_items(self.tree, target_boxes_by_source_level,
-                                     source_boxes_by_level,
+                                     source_boxes_by_level, rounds=self.item_rounds,
                                      groups=M2P_ITEM_GROUPS if self._m2p_f32 else 32)
             return (torch.as_tensor(items).to(self.device),
                     torch.as_tensor(lists).to(self.device))
         items, lists = self._cached_items(
-            "m2p_items", (target_boxes_by_source_level, source_boxes_by_level), build)
+            ("m2p_items", self.item_rounds),
+            (target_boxes_by_source_level, source_boxes_by_level), build)
         if items.shape[0] == 0:
             return pot
         order = self.level_orders[0]
@@ -1261,11 +1286,12 @@ class SumpyExpansionWrangler:
                 and not isinstance(lists, torch.Tensor):
             def build():
                 items, sidx = p2l_items(self.tree, level_start_target_or_target_parent_box_nrs,
-                                        target_or_target_parent_boxes, starts, lists)
+                                        target_or_target_parent_boxes, starts, lists,
+                                        rounds=self.item_rounds)
                 return (torch.as_tensor(items).to(self.device),
                         torch.as_tensor(sidx).to(self.device))
             items, sidx = self._cached_items(
-                "p2l_items", (level_start_target_or_target_parent_box_nrs,
+                ("p2l_items", self.item_rounds), (level_start_target_or_target_parent_box_nrs,
                               target_or_target_parent_boxes, starts, lists), build)
             if items.shape[0]:
                 g = self._geom

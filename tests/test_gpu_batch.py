@@ -78,13 +78,25 @@ def test_batch_mixed_within_tolerance_of_fp64(cuda_device):
 
 
 def test_autotune_picks_and_caches(cuda_device, tmp_path):
+    """The schedule autotuner searches the knobs, stores the best schedule,
+    and a second batch of the same shape takes it from the cache; any
+    schedule gives the same FP64 result."""
+    import json
+    from sumpy_b200.autotune import SCHEDULE_SPACE
     srcs, rng = _problems(6, 8)
     path = tmp_path / "tune.json"
-    b = BatchedLaplaceFMM(srcs, order=6, precision="mixed", bbox=BOX, device=cuda_device,
+    b = BatchedLaplaceFMM(srcs, order=6, precision="fp64", bbox=BOX, device=cuda_device,
                           autotune=True, autotune_cache=path)
-    assert b.wrangler.m2l_item_groups in (16, 32, 64, 128)
+    for k, v in b.schedule.items():
+        assert v in SCHEDULE_SPACE[k]
     assert path.exists()
+    entry = next(iter(json.loads(path.read_text()).values()))
+    assert entry["best"] == b.schedule and len(entry["tried"]) >= len(SCHEDULE_SPACE)
+    b2 = BatchedLaplaceFMM(srcs, order=6, precision="fp64", bbox=BOX, device=cuda_device,
+                           autotune=True, autotune_cache=path)
+    assert b2.schedule == b.schedule
     w = torch.as_tensor(rng.standard_normal(b.nsources))
-    ref = BatchedLaplaceFMM(srcs, order=6, precision="mixed", bbox=BOX, device=cuda_device,
+    ref = BatchedLaplaceFMM(srcs, order=6, precision="fp64", bbox=BOX, device=cuda_device,
                             use_graph=False, m2l_item_groups=64).evaluate(w)
     assert _rel(b.evaluate(w), ref) < 1e-12
+    b.check_status()
