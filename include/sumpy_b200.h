@@ -723,6 +723,78 @@ int sumpy_tree_gpu_array_copy(void *handle, const char *name, void *dst, int64_t
 
 void sumpy_tree_gpu_free(void *handle);
 
+/* ---- QBX layer potentials (3D Laplace / Helmholtz, FP64) ----
+ *
+ * Replace the loopy kernels of sumpy.qbx.LayerPotential (sumpy/qbx.py:250-340),
+ * LayerPotentialMatrixGenerator (qbx.py:345-420) and
+ * LayerPotentialMatrixSubsetGenerator (qbx.py:425-520) for one (target kernel,
+ * source kernel) pair. With a = center - source and b = target - center
+ * (qbx.py:283-284), each pair contributes the order-`order` local Taylor
+ * expansion about the target's center of the source's kernel, evaluated at the
+ * target, times `scale` (the kernel's global scaling constant, 1/(4 pi)).
+ * Line Taylor and volume Taylor expansions (plain or PDE-compressed) give the
+ * same values; they differ only for target derivatives (modes 1 and 2).
+ *
+ * mode 0: value; 1: target derivative d/da_axis of each line-Taylor
+ * coefficient (qbx.py:121-132); 2: target derivative d/db_axis of a volume
+ * Taylor sum (sumpy/expansion/local.py evaluate with AxisTargetDerivative);
+ * 3: source derivative -d/da_axis (AxisSourceDerivative); 4: directional
+ * source derivative -dir(s) . grad_a (DirectionalSourceDerivative, the
+ * double layer), with source_dirs[d * dir_stride + s]. order in [0, 32].
+ *
+ * Points are DEVICE arrays laid out as x[d * stride + i] (sumpy's (3, n)
+ * C-order arrays, stride = n). Helmholtz strengths and results are complex
+ * (interleaved re, im); k is the real wave number. expansion_radii are not
+ * needed: they only set the expansion's rscale, which cancels. No allocation;
+ * the call launches one kernel on `stream` and returns. */
+int sumpy_qbx_lpot_laplace_f64(int order, int mode, int axis, int64_t ntargets,
+                               const double *targets, int64_t target_stride,
+                               const double *centers, int64_t center_stride, int64_t nsources,
+                               const double *sources, int64_t source_stride,
+                               const double *source_dirs, int64_t dir_stride,
+                               const double *strength, double scale, double *result,
+                               void *stream);
+int sumpy_qbx_lpot_helmholtz_f64(int order, int mode, int axis, double k, int64_t ntargets,
+                                 const double *targets, int64_t target_stride,
+                                 const double *centers, int64_t center_stride, int64_t nsources,
+                                 const double *sources, int64_t source_stride,
+                                 const double *source_dirs, int64_t dir_stride,
+                                 const double *strength, double scale, double *result,
+                                 void *stream);
+
+/* The (ntargets, nsources) row-major matrix of pair values (unit strength). */
+int sumpy_qbx_matrix_laplace_f64(int order, int mode, int axis, int64_t ntargets,
+                                 const double *targets, int64_t target_stride,
+                                 const double *centers, int64_t center_stride,
+                                 int64_t nsources, const double *sources,
+                                 int64_t source_stride, const double *source_dirs,
+                                 int64_t dir_stride, double scale, double *result, void *stream);
+int sumpy_qbx_matrix_helmholtz_f64(int order, int mode, int axis, double k, int64_t ntargets,
+                                   const double *targets, int64_t target_stride,
+                                   const double *centers, int64_t center_stride,
+                                   int64_t nsources, const double *sources,
+                                   int64_t source_stride, const double *source_dirs,
+                                   int64_t dir_stride, double scale, double *result,
+                                   void *stream);
+
+/* Entries (tgtindices[m], srcindices[m]) of that matrix, m < nentries (DEVICE
+ * int32 index arrays, in range: the caller checks). */
+int sumpy_qbx_matrix_subset_laplace_f64(int order, int mode, int axis, int64_t nentries,
+                                        const int32_t *tgtindices, const int32_t *srcindices,
+                                        const double *targets, int64_t target_stride,
+                                        const double *centers, int64_t center_stride,
+                                        const double *sources, int64_t source_stride,
+                                        const double *source_dirs, int64_t dir_stride,
+                                        double scale, double *result, void *stream);
+int sumpy_qbx_matrix_subset_helmholtz_f64(int order, int mode, int axis, double k,
+                                          int64_t nentries, const int32_t *tgtindices,
+                                          const int32_t *srcindices, const double *targets,
+                                          int64_t target_stride, const double *centers,
+                                          int64_t center_stride, const double *sources,
+                                          int64_t source_stride, const double *source_dirs,
+                                          int64_t dir_stride, double scale, double *result,
+                                          void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -50,6 +50,19 @@ SIGNATURES = {
     "sumpy_tree_gpu_array_info": [ptr, ctypes.c_char_p, ptr, ptr],
     "sumpy_tree_gpu_array_copy": [ptr, ctypes.c_char_p, ptr, i64, cint, ptr],
     "sumpy_tree_gpu_free": [ptr],
+    # QBX layer potentials (order, mode, axis[, k], ...)
+    "sumpy_qbx_lpot_laplace_f64": [cint, cint, cint, i64, ptr, i64, ptr, i64, i64, ptr, i64,
+                                   ptr, i64, ptr, dbl, ptr, ptr],
+    "sumpy_qbx_lpot_helmholtz_f64": [cint, cint, cint, dbl, i64, ptr, i64, ptr, i64, i64, ptr,
+                                     i64, ptr, i64, ptr, dbl, ptr, ptr],
+    "sumpy_qbx_matrix_laplace_f64": [cint, cint, cint, i64, ptr, i64, ptr, i64, i64, ptr, i64,
+                                     ptr, i64, dbl, ptr, ptr],
+    "sumpy_qbx_matrix_helmholtz_f64": [cint, cint, cint, dbl, i64, ptr, i64, ptr, i64, i64,
+                                       ptr, i64, ptr, i64, dbl, ptr, ptr],
+    "sumpy_qbx_matrix_subset_laplace_f64": [cint, cint, cint, i64, ptr, ptr, ptr, i64, ptr,
+                                            i64, ptr, i64, ptr, i64, dbl, ptr, ptr],
+    "sumpy_qbx_matrix_subset_helmholtz_f64": [cint, cint, cint, dbl, i64, ptr, ptr, ptr, i64,
+                                              ptr, i64, ptr, i64, ptr, i64, dbl, ptr, ptr],
     "sumpy_get_tc_wait_cycles": [],
     "sumpy_m2l_translation_classes_tf32x3": [cint, i32, ptr, ptr, ptr, i32, ptr, ptr, ptr, ptr,
                                              i32, ptr, ptr, i32, i32, i32, i32, ptr, ptr, i32,

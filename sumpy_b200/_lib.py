@@ -30,7 +30,7 @@ ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["capi.cu", "p2p.cu", "expansions.cu", "m2l.cu", "m2l_tc.cu", "helmholtz.cu",
               "helmholtz_items.cu", "helmholtz_l2p.cu", "p2p_matrix.cu", "laplace_items_f64.cu",
-              "tree_gpu.cu"]
+              "tree_gpu.cu", "qbx.cu"]
 
 _lock = threading.Lock()
 _cuda = None

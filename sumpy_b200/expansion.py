@@ -88,6 +88,48 @@ class LinearPDEConformingVolumeTaylorLocalExpansion(_VolumeTaylorBase):
     path always applies M2L as dense per-class operators."""
     m2l_translation_override: Any = field(default=None, compare=False)
 
+
+@dataclass(frozen=True)
+class VolumeTaylorLocalExpansion(_VolumeTaylorBase):
+    """Uncompressed Taylor local expansion (sumpy/expansion/local.py:512-
+    540): every mi with |mi| <= order. Used here by the QBX layer potential,
+    whose value it determines through sum_{|mi| <= p} D^mi G(a) b^mi / mi!."""
+
+    def get_coefficient_identifiers(self):
+        return list(full_ids(self.order))
+
+    def __len__(self):
+        return (self.order + 1) * (self.order + 2) * (self.order + 3) // 6
+
+
+@dataclass(frozen=True)
+class LineTaylorLocalExpansion:
+    """Taylor expansion along the line from the expansion center to one
+    target (sumpy/expansion/local.py:116-185): coefficients
+    d^i/dtau^i G(a + tau b) at tau = 0, i <= order, evaluated as their sum
+    with 1/i!. Only meaningful where the target is known when coefficients
+    are formed: the QBX layer potential (:mod:`sumpy_b200.qbx`)."""
+    kernel: Any
+    order: int
+    use_rscale: bool | None = None
+
+    def __post_init__(self):
+        if not isinstance(self.kernel.get_base_kernel(), (LaplaceKernel, HelmholtzKernel)):
+            raise NotImplementedError(
+                "only LaplaceKernel(3) and HelmholtzKernel(3) expansions are implemented")
+        if not 0 <= self.order <= 32:
+            raise ValueError(f"order must be in [0, 32], got {self.order}")
+
+    @property
+    def dim(self):
+        return 3
+
+    def get_coefficient_identifiers(self):
+        return [(i,) for i in range(self.order + 1)]
+
+    def __len__(self):
+        return self.order + 1
+
 # }}}
 
 

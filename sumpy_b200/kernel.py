@@ -84,3 +84,81 @@ def is_scale_invariant(kernel) -> bool:
     """Homogeneous kernels whose scaled translation operators depend on the
     level only through a scalar factor (1/r: derivatives scale as 1/rscale)."""
     return isinstance(kernel, LaplaceKernel)
+
+
+# {{{ derivative wrappers (sumpy/kernel.py:2289-2386, directional source derivative)
+
+@dataclass(frozen=True)
+class AxisTargetDerivative:
+    """``sumpy.kernel.AxisTargetDerivative(axis, inner_kernel)``: d/dt_axis."""
+    axis: int
+    inner_kernel: object
+
+    def __post_init__(self):
+        if self.axis not in (0, 1, 2):
+            raise ValueError(f"axis must be 0, 1 or 2, got {self.axis}")
+
+    def get_base_kernel(self):
+        return self.inner_kernel.get_base_kernel()
+
+    @property
+    def global_scaling_const(self):
+        return self.get_base_kernel().global_scaling_const
+
+    @property
+    def is_complex_valued(self):
+        return self.get_base_kernel().is_complex_valued
+
+    def __str__(self):
+        return f"d/dx{self.axis} {self.inner_kernel}"
+
+
+@dataclass(frozen=True)
+class AxisSourceDerivative:
+    """``sumpy.kernel.AxisSourceDerivative(axis, inner_kernel)``: d/ds_axis."""
+    axis: int
+    inner_kernel: object
+
+    def __post_init__(self):
+        if self.axis not in (0, 1, 2):
+            raise ValueError(f"axis must be 0, 1 or 2, got {self.axis}")
+
+    def get_base_kernel(self):
+        return self.inner_kernel.get_base_kernel()
+
+    @property
+    def global_scaling_const(self):
+        return self.get_base_kernel().global_scaling_const
+
+    @property
+    def is_complex_valued(self):
+        return self.get_base_kernel().is_complex_valued
+
+    def __str__(self):
+        return f"d/dy{self.axis} {self.inner_kernel}"
+
+
+@dataclass(frozen=True)
+class DirectionalSourceDerivative:
+    """``sumpy.kernel.DirectionalSourceDerivative(inner_kernel,
+    dir_vec_name)``: n(s) . grad_s, with the per-source direction vectors
+    passed by name (default ``"src_derivative_dir"``, shape (3, nsources));
+    the double-layer kernel."""
+    inner_kernel: object
+    dir_vec_name: str = "src_derivative_dir"
+
+    def get_base_kernel(self):
+        return self.inner_kernel.get_base_kernel()
+
+    @property
+    def global_scaling_const(self):
+        return self.get_base_kernel().global_scaling_const
+
+    @property
+    def is_complex_valued(self):
+        return self.get_base_kernel().is_complex_valued
+
+    def __str__(self):
+        return f"{self.dir_vec_name} . grad_src {self.inner_kernel}"
+
+# }}}

@@ -24,3 +24,18 @@ def sphere_plummer(n, seed, plummer_scale=0.1):
     d = rng.standard_normal((3, n2))
     d /= np.linalg.norm(d, axis=0)
     return np.concatenate([sph, r * d], axis=1)
+
+
+def sphere_quadrature(ntheta):
+    """Nodes and weights of a tensor quadrature on the unit sphere:
+    Gauss-Legendre in cos(theta) (ntheta nodes) times the midpoint rule in
+    phi (2 ntheta nodes); exact for spherical harmonics of degree < 2 ntheta.
+    Returns (points (3, n), weights (n,)); the points are also the normals."""
+    x, w = np.polynomial.legendre.leggauss(ntheta)
+    nphi = 2 * ntheta
+    phi = (np.arange(nphi) + 0.5) * 2.0 * np.pi / nphi
+    ct = np.repeat(x, nphi)
+    st = np.sqrt(1.0 - ct * ct)
+    ph = np.tile(phi, ntheta)
+    pts = np.stack([st * np.cos(ph), st * np.sin(ph), ct])
+    return pts, np.repeat(w, nphi) * (2.0 * np.pi / nphi)

@@ -3,11 +3,12 @@
 This script is test infrastructure. It is run by hand in a container that has
 the sumpy source tree (its path in the ``SUMPY_REFERENCE`` environment
 variable, which is required) and sympy installed; the GPU test box never runs it. It writes
-``tests/golden/laplace3d_operators.json`` and
-``tests/golden/helmholtz3d_operators.json``, which the tests read
+``tests/golden/laplace3d_operators.json``,
+``tests/golden/helmholtz3d_operators.json`` and (``--which qbx``)
+``tests/golden/qbx3d_pairs.json``, which the tests read
 (``SUMPY_REFERENCE=<sumpy checkout> python tests/golden/make_golden.py
-[--which laplace helmholtz] [--laplace-orders 2 3 4 5 6 8]
-[--helmholtz-orders 2 3 4]``).
+[--which laplace helmholtz qbx] [--laplace-orders 2 3 4 5 6 8]
+[--helmholtz-orders 2 3 4] [--qbx-line-orders 3 5 8] ...``).
 
 sumpy itself cannot be imported normally here: its package ``__init__`` pulls
 in pyopencl/loopy/boxtree, none of which are installed. The expansion math
@@ -340,14 +341,107 @@ def generate(knl, orders, out_path, label, complex_valued, extra_subs):
         "cases": cases}
 
 
+QBX_OUT_NAME = "qbx3d_pairs.json"
+
+
+def generate_qbx(lap, helm, line_orders, volume_orders, helm_line_orders,
+                 helm_volume_orders):
+    """Golden values of the QBX pair expression: sumpy's
+    ``LayerPotentialBase._expand`` / ``_evaluate`` (sumpy/qbx.py:113-146) on
+    symbolic a (center - source) and b (target - center), evaluated at fixed
+    inputs with 40-digit arithmetic, for value, target-, source- and
+    directional source-derivative kernels and the line / volume /
+    PDE-compressed local expansions."""
+    import sympy
+
+    import sumpy.expansion.local as local_mod
+    import sumpy.kernel as kernel_mod
+
+    rng = np.random.default_rng(77)
+
+    def exact(x):
+        return sympy.Rational(Fraction(float(x)))
+
+    avec = sympy.Matrix(sympy.symbols("a0:3"))
+    bvec = sympy.Matrix(sympy.symbols("b0:3"))
+    rscale = sympy.Symbol("rscale")
+    dir_name = "dsd"
+
+    def pairs_for(knl):
+        return [
+            ("value", knl, knl, None),
+            ("tgt_deriv_1", kernel_mod.AxisTargetDerivative(1, knl), knl, 1),
+            ("src_deriv_2", knl, kernel_mod.AxisSourceDerivative(2, knl), 2),
+            ("dir_src_deriv", knl, kernel_mod.DirectionalSourceDerivative(knl, dir_name),
+             None),
+        ]
+
+    expansions = {
+        "line": lambda knl, p: local_mod.LineTaylorLocalExpansion(knl, p),
+        "volume": lambda knl, p: local_mod.VolumeTaylorLocalExpansion(knl, p),
+        "compressed": lambda knl, p: local_mod.LinearPDEConformingVolumeTaylorLocalExpansion(
+            knl, p),
+    }
+    plan = []
+    for knl, label, lo, vo, extra in ((lap, "laplace", line_orders, volume_orders, {}),
+                                      (helm, "helmholtz", helm_line_orders,
+                                       helm_volume_orders,
+                                       {sympy.Symbol("k"): HELM_K})):
+        for kind in ("line", "volume", "compressed"):
+            for p in (lo if kind == "line" else vo):
+                plan.append((knl, label, kind, p, extra))
+
+    cases = []
+    for knl, label, kind, order, extra in plan:
+        expn = expansions[kind](knl, order)
+        a = rng.uniform(-0.6, 0.6, 3).round(6) + np.array([0.0, 0.0, 1.0])
+        b = rng.uniform(-0.2, 0.2, 3).round(6)
+        dvec = rng.standard_normal(3)
+        dvec = (dvec / np.linalg.norm(dvec)).round(6)
+        subs = {avec[i]: exact(a[i]) for i in range(3)}
+        subs.update({bvec[i]: exact(b[i]) for i in range(3)})
+        subs.update({sympy.Symbol(f"{dir_name}{i}"): exact(dvec[i]) for i in range(3)})
+        subs[rscale] = exact(0.375)
+        subs.update(extra)
+        for name, tgt_knl, src_knl, _axis in pairs_for(knl):
+            coeffs = expn.coefficients_from_source_vec(
+                [src_knl], avec, bvec, rscale, weights=[1])
+            if kind == "line":
+                coeffs = [tgt_knl.postprocess_at_target(c, avec) for c in coeffs]
+            csyms = list(sympy.symbols(f"q0:{len(coeffs)}"))
+            cvals = {s: sympy.N(sympy.sympify(c).doit().xreplace(subs), 40)
+                     for s, c in zip(csyms, coeffs)}
+            res = expn.evaluate(tgt_knl, csyms, bvec, rscale)
+            v = complex(sympy.N(sympy.sympify(res).doit().xreplace(cvals).xreplace(subs), 40))
+            cases.append({"kernel": label, "expansion": kind, "order": order, "pair": name,
+                          "avec": a.tolist(), "bvec": b.tolist(), "dir": dvec.tolist(),
+                          "value": [v.real, v.imag]})
+        print(f"qbx {label} {kind} order {order} done", flush=True)
+    return {
+        "generator": "tests/golden/make_golden.py --which qbx",
+        "conventions": {"avec": "center - source", "bvec": "target - center",
+                        "dir": "source derivative direction (DirectionalSourceDerivative)",
+                        "value": "pair expression without the kernel scaling, [re, im]"},
+        "pairs": {"value": "target and source kernel = base kernel",
+                  "tgt_deriv_1": "AxisTargetDerivative(1, base) / base",
+                  "src_deriv_2": "base / AxisSourceDerivative(2, base)",
+                  "dir_src_deriv": "base / DirectionalSourceDerivative(base)"},
+        "k": float(HELM_K),
+        "cases": cases}
+
+
 def main():
     import argparse
     global HELM_K
     ap = argparse.ArgumentParser()
     ap.add_argument("--which", nargs="+", default=["laplace", "helmholtz"],
-                    choices=["laplace", "helmholtz"])
+                    choices=["laplace", "helmholtz", "qbx"])
     ap.add_argument("--laplace-orders", nargs="+", type=int, default=[2, 3, 4, 5, 6, 8])
     ap.add_argument("--helmholtz-orders", nargs="+", type=int, default=[2, 3, 4])
+    ap.add_argument("--qbx-line-orders", nargs="+", type=int, default=[3, 5, 8])
+    ap.add_argument("--qbx-volume-orders", nargs="+", type=int, default=[3, 5])
+    ap.add_argument("--qbx-helmholtz-line-orders", nargs="+", type=int, default=[3, 5])
+    ap.add_argument("--qbx-helmholtz-volume-orders", nargs="+", type=int, default=[3])
     ap.add_argument("--out-dir", default=None,
                     help="write the JSON files here instead of next to this script")
     args = ap.parse_args()
@@ -370,6 +464,12 @@ def main():
         data["kernel"] = ("HelmholtzKernel(3), expression exp(i k |d|)/|d| with k = 5/2 "
                           "(scaling applied on output); complex values as [re, im]")
         data["k"] = float(HELM_K)
+        out.write_text(json.dumps(data, indent=1))
+        print("wrote", out)
+    if "qbx" in args.which:
+        out = out_lap.with_name(QBX_OUT_NAME)
+        data = generate_qbx(lap, helm, args.qbx_line_orders, args.qbx_volume_orders,
+                            args.qbx_helmholtz_line_orders, args.qbx_helmholtz_volume_orders)
         out.write_text(json.dumps(data, indent=1))
         print("wrote", out)
 
