@@ -18,7 +18,8 @@ A default run prints that one JSON line and nothing else on stdout, as soon
 as it is measured; progress goes to stderr with timestamps, and a section
 that runs longer than ``--stall-dump-s`` dumps every thread's Python stack to
 stderr. ``--extras`` adds the other workloads (adjoint, 512-problem batch,
-Helmholtz, 20k uniform case, interaction matrices), each as a JSON line of
+Helmholtz, 20k uniform case, interaction matrices, QBX layer potentials),
+each as a JSON line of
 its own after the headline, within ``--budget-s``.
 
 The CPU baseline is the oracle (C + OpenMP, sumpy's algorithm restated) on
@@ -105,7 +106,7 @@ def parse():
     ap.add_argument("--extras", action="store_true",
                     help="after the headline, run the other workloads (one JSON line each)")
     ap.add_argument("--only", choices=["mixed", "fp64", "batch", "helmholtz", "uniform",
-                                       "matrix", "adjoint"],
+                                       "matrix", "adjoint", "qbx"],
                     help="run one workload alone (--steps/--warmup apply) and print its result; "
                          "for profiling")
     ap.add_argument("--eager", action="store_true",
@@ -415,7 +416,8 @@ def main():
                          ("batched", lambda: batched_bench(dev)),
                          ("helmholtz", lambda: helmholtz_bench(dev)),
                          ("uniform_p6", lambda: uniform_bench(dev)),
-                         ("p2p_matrix", lambda: matrix_bench(dev))):
+                         ("p2p_matrix", lambda: matrix_bench(dev)),
+                         ("qbx", lambda: qbx_bench(dev))):
             if not budget.ok(name, 30.0):
                 continue
             progress(f"extra: {name}")
@@ -700,6 +702,8 @@ def run_only(args, dev):
         return uniform_bench(dev, steps=args.steps, warmup=args.warmup, cpu=False)
     if args.only == "adjoint":
         return adjoint_api_bench(dev, steps=args.steps, warmup=args.warmup)
+    if args.only == "qbx":
+        return qbx_bench(dev, steps=args.steps, warmup=args.warmup)
     if args.only == "helmholtz":
         precs = (("mixed", "fp64") if args.helmholtz_precision == "both"
                  else (args.helmholtz_precision,))
@@ -1046,6 +1050,84 @@ def matrix_bench(dev, steps=5, warmup=3, n=20_000, nsub=20_000_000):
     out["laplace_subset"] = {"pairs": nsub, "ms": ms, "Gentries_s": nsub / (ms * 1e-3) / 1e9,
                              "GB_s_indices_and_result": 16.0 * nsub / (ms * 1e-3) / 1e9}
     out["peak_hbm_gbs"] = hbm
+    return out
+
+
+# FP64 operations per pair of the QBX applier's Laplace value (line Taylor,
+# order p): a = c - s (3), |a|^2, a.b, |b|^2 (15), 1/|a| and 1/|a|^2 (3),
+# w and v (2), 7 per recurrence step ((-(2n+1) w T_n - n v T_{n-1}) / (n+1),
+# the sum), and the strength product and sum (2): 25 + 7 p.
+def qbx_laplace_flops_per_pair(p):
+    return 25 + 7 * p
+
+
+def qbx_bench(dev, steps=5, warmup=3, ntheta=200, ntargets=20_000, order=12, k=2.5,
+              cpu=True):
+    """QBX layer potentials (sumpy.qbx.LayerPotential): single and double
+    layer on the unit sphere, sources a Gauss-Legendre x midpoint quadrature
+    (ntheta x 2 ntheta nodes, 80k at ntheta = 200), targets on the sphere
+    with centers at depth 0.15 inside, line Taylor order 12, Laplace and
+    Helmholtz (k = 2.5). Every target sums over every source (sumpy's
+    direct applier). CUDA-event time per call, inputs resident; pairs per
+    second, and for the Laplace value an FP64 rate against the measured
+    DGEMM rate. The CPU leg times the oracle (numpy, one process) on 16
+    targets against all sources."""
+    import torch
+    from sumpy_b200 import (DirectionalSourceDerivative, HelmholtzKernel, LaplaceKernel,
+                            LayerPotential, LineTaylorLocalExpansion)
+    from tests._pointsets import sphere_quadrature
+    src_np, w_np = sphere_quadrature(ntheta)
+    rng = np.random.default_rng(21)
+    g = rng.standard_normal((3, ntargets))
+    tgt_np = g / np.linalg.norm(g, axis=0)
+    ctr_np = tgt_np * 0.85
+    src, tgt, ctr = (torch.as_tensor(x, device=dev) for x in (src_np, tgt_np, ctr_np))
+    dens = torch.as_tensor(w_np * src_np[2], device=dev)
+    nsrc = src_np.shape[1]
+    pairs = float(ntargets) * nsrc
+
+    def tm(fn):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    out = {"nsources": nsrc, "ntargets": ntargets, "order": order, "k": k}
+    peaks = pipe_peaks_measured(dev)
+    for name, base, kw in (("laplace", LaplaceKernel(3), {}),
+                           ("helmholtz", HelmholtzKernel(3), {"k": k})):
+        expn = LineTaylorLocalExpansion(base, order)
+        s_lp = LayerPotential(expn, target_kernels=[base], source_kernels=[base], device=dev)
+        d_lp = LayerPotential(expn, target_kernels=[base],
+                              source_kernels=[DirectionalSourceDerivative(base, "normal")],
+                              device=dev)
+        d = dens if name == "laplace" else dens.to(torch.complex128)
+        ms_s = tm(lambda: s_lp(None, tgt, src, ctr, [d], None, **kw))
+        ms_d = tm(lambda: d_lp(None, tgt, src, ctr, [d], None, normal=src, **kw))
+        out[name] = {"single_layer_ms": ms_s, "double_layer_ms": ms_d,
+                     "single_layer_Gpairs_s": pairs / (ms_s * 1e-3) / 1e9,
+                     "double_layer_Gpairs_s": pairs / (ms_d * 1e-3) / 1e9}
+        if name == "laplace":
+            tf = pairs * qbx_laplace_flops_per_pair(order) / (ms_s * 1e-3) / 1e12
+            out[name]["single_layer_fp64_tflops"] = tf
+            out[name]["frac_of_measured_dgemm"] = tf / peaks["fp64_tflops"]
+    out["fp64_tflops_measured_dgemm"] = peaks["fp64_tflops"]
+    if cpu:
+        from oracle import qbx_oracle as Q
+        sub = 16
+        t0 = time.perf_counter()
+        Q.lpot(order, Q.VALUE, tgt_np[:, :sub], ctr_np[:, :sub], src_np, w_np * src_np[2],
+               scale=1 / (4 * np.pi), block=4)
+        cpu_s = time.perf_counter() - t0
+        out["cpu_oracle"] = {"kind": "port", "cores": 1, "sample": f"{sub} targets x {nsrc} "
+                             "sources, Laplace single layer", "Gpairs_s":
+                             sub * nsrc / cpu_s / 1e9}
     return out
 
 

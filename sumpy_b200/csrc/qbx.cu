@@ -16,13 +16,13 @@
 //     (n + 1) T_{n+1} = -(2n + 1) w T_n - n v T_{n-1}
 //     (the Legendre generating function; P_i(x) rho^i with x the cosine
 //     between -a and b and rho = |b| / |a|): O(p) per pair.
-//   Helmholtz (G = e^{ikr}/r): with r(tau)^2 = R0 + R1 tau + R2 tau^2
-//     (R0 = A, R1 = 2 a.b, R2 = |b|^2), the Taylor coefficients of r, of
-//     E = e^{ikr} and of f = E / r by power-series recurrences:
-//     2 r_0 r_n = Q_n - sum_{0<i<n} r_i r_{n-i},  n E_n = ik sum_{j<=n} j r_j E_{n-j},
-//     r_0 f_n = E_n - sum_{1<=j<=n} r_j f_{n-j}: O(p^2) per pair.
-// Derivatives are carried through the recurrences as dual parts (with
-// respect to w, v, or R0, R1, R2) and combined by the chain rule:
+//   Helmholtz (G = e^{ikr}/r): the addition theorem regrouped by powers of
+//     tau (helmholtz_line below): the Laplace terms T_n times a spherical
+//     Hankel recurrence in n times truncated spherical Bessel series, O(p)
+//     complex and O(p^2 / 4) real operations per pair.
+// Derivatives are carried through the recurrences (with respect to their
+// variables: w, v, and for Helmholtz |a| and k^2 |b|^2) and combined by the
+// chain rule:
 //   target derivative, line Taylor: d/da_axis of each coefficient (sumpy
 //     applies the target kernel's derivative to the coefficients with
 //     respect to avec, qbx.py:128-132);
@@ -70,30 +70,44 @@ struct LapOut {
     double ga[3], gb[3];
 };
 
+// 1 / (n + 1), n <= QBX_MAX_ORDER: the recurrence's divisions, read as
+// broadcasts from the constant cache (every thread is at the same n)
+#define QBX_INV4(n) 1.0 / ((n) + 1.0), 1.0 / ((n) + 2.0), 1.0 / ((n) + 3.0), 1.0 / ((n) + 4.0)
+__constant__ double c_qbx_inv[QBX_MAX_ORDER + 4] = {
+    QBX_INV4(0), QBX_INV4(4), QBX_INV4(8), QBX_INV4(12), QBX_INV4(16), QBX_INV4(20),
+    QBX_INV4(24), QBX_INV4(28), QBX_INV4(32)};
+#undef QBX_INV4
+
 template <bool GRAD>
 __device__ __forceinline__ LapOut laplace_line(int p, const double a[3], const double b[3])
 {
     const double A = a[0] * a[0] + a[1] * a[1] + a[2] * a[2];
     const double D = a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
     const double B2 = b[0] * b[0] + b[1] * b[1] + b[2] * b[2];
-    const double Ainv = 1.0 / A;
+    const double rinv = rsqrt(A);
+    const double Ainv = rinv * rinv;
     const double w = D * Ainv, v = B2 * Ainv;
-    const double rinv = sqrt(Ainv);
     // T_n and, with GRAD, dT_n/dw and dT_n/dv
     double Tm1 = 0.0, T = 1.0, S = 1.0;
     double Wm1 = 0.0, W = 0.0, SW = 0.0;
     double Vm1 = 0.0, V = 0.0, SV = 0.0;
+    double c1 = 1.0, c2 = 0.0;   // 2n + 1, n
+    double cw = w, cv = 0.0;     // (2n + 1) w, n v
+    const double w2 = 2.0 * w;
     for (int n = 0; n < p; ++n) {
-        const double inv = 1.0 / (double)(n + 1);
-        const double c1 = (double)(2 * n + 1), c2 = (double)n;
-        const double Tn = (-c1 * w * T - c2 * v * Tm1) * inv;
+        const double inv = c_qbx_inv[n];
+        const double Tn = -fma(cw, T, cv * Tm1) * inv;
         if (GRAD) {
             const double Wn = (-c1 * (T + w * W) - c2 * v * Wm1) * inv;
             const double Vn = (-c1 * w * V - c2 * (Tm1 + v * Vm1)) * inv;
             Wm1 = W; W = Wn; SW += Wn;
             Vm1 = V; V = Vn; SV += Vn;
+            c1 += 2.0;
+            c2 += 1.0;
         }
         Tm1 = T; T = Tn; S += Tn;
+        cw += w2;
+        cv += v;
     }
     LapOut o;
     o.val = S * rinv;
@@ -114,78 +128,125 @@ struct HelmOut {
     C2 ga[3], gb[3];
 };
 
+// Recurrence constants of the Helmholtz line sum, folded at compile time:
+// hv[n] = 1 / ((2n + 1)(2n - 1)) (n >= 1) and g[n][m] = 1 / ((m + 1)(2n + 2m + 3))
+struct HelmTables {
+    double hv[QBX_MAX_ORDER + 1];
+    double g[QBX_MAX_ORDER + 1][QBX_MAX_ORDER / 2 + 1];
+};
+constexpr HelmTables make_helm_tables()
+{
+    HelmTables t{};
+    for (int n = 0; n <= QBX_MAX_ORDER; ++n) {
+        t.hv[n] = n == 0 ? 0.0 : 1.0 / ((2.0 * n + 1.0) * (2.0 * n - 1.0));
+        for (int m = 0; m <= QBX_MAX_ORDER / 2; ++m)
+            t.g[n][m] = 1.0 / ((m + 1.0) * (2.0 * n + 2.0 * m + 3.0));
+    }
+    return t;
+}
+__constant__ HelmTables c_helm = make_helm_tables();
+
+// The degree-N Taylor coefficient of G(a + tau b) = e^{ik|a + tau b|} / |a + tau b|
+// follows from the addition theorem e^{ik|x - y|}/|x - y| = ik sum_n (2n + 1)
+// j_n(k|x|) h_n(k|y|) P_n(cos) (x = tau b, y = -a) by collecting powers of tau
+// in j_n(k tau |b|) = sum_m (-1)^m (k tau |b|)^{n + 2m} / (2^m m! (2n + 2m + 1)!!).
+// Truncated at total degree p the line sum is
+//   S = sum_{n <= p} T_n(w, v) V_n(r) G_n(Z),
+// with T_n = P_n(x) rho^n the Laplace recurrence's terms (x the cosine between
+// -a and b, rho = |b| / |a|), r = |a|, Z = k^2 |b|^2,
+//   V_n = ik (k r)^n h_n(k r) / (2n - 1)!!:  V_0 = e^{ikr} / r,
+//     V_1 = e^{ikr} (1/r - ik),  V_{n+1} = V_n - (k r)^2 V_{n-1} / ((2n + 1)(2n - 1)),
+//   G_n = sum_{m <= (p - n) / 2} (-Z / 2)^m / (m! prod_{j=1..m} (2n + 2j + 1)).
+// (k -> 0 gives V_n = 1/r, G_n = 1: the Laplace sum.) O(p^2 / 4) real
+// multiply-adds for the G_n and O(p) complex ones: no series convolutions.
+// Derivatives by the chain rule through w, v, r and Z.
 template <bool GRAD>
 __device__ __forceinline__ HelmOut helmholtz_line(int p, double k, const double a[3],
                                                   const double b[3])
 {
-    const double R[3] = {a[0] * a[0] + a[1] * a[1] + a[2] * a[2],
-                         2.0 * (a[0] * b[0] + a[1] * b[1] + a[2] * b[2]),
-                         b[0] * b[0] + b[1] * b[1] + b[2] * b[2]};
-    // series coefficients (real r, complex E and f) and their duals with
-    // respect to R0, R1, R2 (index q)
-    double r[QBX_MAX_ORDER + 1];
-    C2 E[QBX_MAX_ORDER + 1], f[QBX_MAX_ORDER + 1];
-    double dr[GRAD ? 3 : 1][QBX_MAX_ORDER + 1];
-    C2 dE[GRAD ? 3 : 1][QBX_MAX_ORDER + 1], df[GRAD ? 3 : 1][QBX_MAX_ORDER + 1];
-    r[0] = sqrt(R[0]);
-    const double r0inv = 1.0 / r[0];
+    const double A = a[0] * a[0] + a[1] * a[1] + a[2] * a[2];
+    const double D = a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+    const double B2 = b[0] * b[0] + b[1] * b[1] + b[2] * b[2];
+    const double rinv = rsqrt(A);
+    const double Ainv = rinv * rinv;
+    const double r = A * rinv;
+    const double w = D * Ainv, v = B2 * Ainv;
+    const double k2 = k * k;
+    const double K2 = k2 * A;          // (k r)^2
+    const double hz = -0.5 * k2 * B2;  // -Z / 2
     double sn, cs;
-    sincos(k * r[0], &sn, &cs);
-    E[0] = {cs, sn};
-    f[0] = cscale(E[0], r0inv);
+    sincos(k * r, &sn, &cs);
+    const C2 e = {cs, sn};
+    // V_n, V_{n-1}, V_1 and their r derivatives
+    C2 Vc = cscale(e, rinv), Vp = {0.0, 0.0};
+    const C2 V1 = cmul(e, C2{rinv, -k});
+    C2 dVc = {0.0, 0.0}, dVp = {0.0, 0.0}, dV1 = {0.0, 0.0};
     if (GRAD) {
-        for (int q = 0; q < 3; ++q) {
-            dr[q][0] = q == 0 ? 0.5 * r0inv : 0.0;
-            dE[q][0] = cmul(C2{0.0, k * dr[q][0]}, E[0]);
-            df[q][0] = cscale(csub(dE[q][0], cscale(f[0], dr[q][0])), r0inv);
-        }
+        dVc = cmul(e, C2{-Ainv, k * rinv});       // e (ik / r - 1 / r^2)
+        dV1 = cmul(e, C2{k2 - Ainv, k * rinv});   // e (ik / r + k^2 - 1 / r^2)
     }
-    C2 S = f[0];
-    C2 dS[3] = {{0, 0}, {0, 0}, {0, 0}};
-    if (GRAD)
-        for (int q = 0; q < 3; ++q) dS[q] = df[q][0];
-    for (int n = 1; n <= p; ++n) {
-        double rn = n <= 2 ? R[n] : 0.0;
-        for (int i = 1; i < n; ++i) rn -= r[i] * r[n - i];
-        rn *= 0.5 * r0inv;
-        r[n] = rn;
-        C2 En = {0.0, 0.0};
-        for (int j = 1; j <= n; ++j) En = cadd(En, cscale(E[n - j], j * r[j]));
-        En = cmul(C2{0.0, k / (double)n}, En);
-        E[n] = En;
-        C2 fn = En;
-        for (int j = 1; j <= n; ++j) fn = csub(fn, cscale(f[n - j], r[j]));
-        fn = cscale(fn, r0inv);
-        f[n] = fn;
-        S = cadd(S, fn);
-        if (GRAD) {
-            for (int q = 0; q < 3; ++q) {
-                double d = (q == n && n <= 2) ? 1.0 : 0.0;
-                for (int i = 1; i < n; ++i) d -= dr[q][i] * r[n - i] + r[i] * dr[q][n - i];
-                d = (d - 2.0 * dr[q][0] * rn) * 0.5 * r0inv;
-                dr[q][n] = d;
-                C2 dEn = {0.0, 0.0};
-                for (int j = 1; j <= n; ++j)
-                    dEn = cadd(dEn, cadd(cscale(E[n - j], j * dr[q][j]),
-                                         cscale(dE[q][n - j], j * r[j])));
-                dEn = cmul(C2{0.0, k / (double)n}, dEn);
-                dE[q][n] = dEn;
-                C2 dfn = csub(dEn, cscale(fn, dr[q][0]));
-                for (int j = 1; j <= n; ++j)
-                    dfn = csub(dfn, cadd(cscale(f[n - j], dr[q][j]), cscale(df[q][n - j], r[j])));
-                dfn = cscale(dfn, r0inv);
-                df[q][n] = dfn;
-                dS[q] = cadd(dS[q], dfn);
+    double Tm1 = 0.0, T = 1.0, Wm1 = 0.0, W = 0.0, Um1 = 0.0, U = 0.0;
+    double c1 = 1.0, c2 = 0.0;   // 2n + 1, n
+    double cw = w, cv = 0.0;     // (2n + 1) w, n v
+    const double w2 = 2.0 * w;
+    C2 S = {0.0, 0.0}, Sw = {0.0, 0.0}, Sv = {0.0, 0.0}, Sr = {0.0, 0.0}, Sz = {0.0, 0.0};
+    for (int n = 0; n <= p; ++n) {
+        // G_n and, with GRAD, dG_n / dZ = sum_m m c_m Z^{m-1}
+        double G = 1.0, t = 1.0, Gd = 0.0, q = 0.0, mm = 1.0;
+        const int M = (p - n) >> 1;
+        for (int m = 0; m < M; ++m) {
+            const double f = c_helm.g[n][m];
+            t *= hz * f;
+            G += t;
+            if (GRAD) {
+                q = m == 0 ? -0.5 * f : q * hz * f;
+                Gd += mm * q;
+                mm += 1.0;
             }
         }
+        const double TG = T * G;
+        S = cadd(S, cscale(Vc, TG));
+        if (GRAD) {
+            Sw = cadd(Sw, cscale(Vc, W * G));
+            Sv = cadd(Sv, cscale(Vc, U * G));
+            Sr = cadd(Sr, cscale(dVc, TG));
+            Sz = cadd(Sz, cscale(Vc, T * Gd));
+        }
+        if (n == p) break;
+        // T_{n+1} (and dT/dw, dT/dv)
+        const double inv = c_qbx_inv[n];
+        const double Tn = -fma(cw, T, cv * Tm1) * inv;
+        if (GRAD) {
+            const double Wn = (-c1 * (T + w * W) - c2 * v * Wm1) * inv;
+            const double Un = (-c1 * w * U - c2 * (Tm1 + v * Um1)) * inv;
+            Wm1 = W; W = Wn;
+            Um1 = U; U = Un;
+            c1 += 2.0;
+            c2 += 1.0;
+        }
+        Tm1 = T; T = Tn;
+        cw += w2;
+        cv += v;
+        // V_{n+1}
+        C2 Vn = V1, dVn = dV1;
+        if (n > 0) {
+            const double h = c_helm.hv[n];
+            Vn = csub(Vc, cscale(Vp, K2 * h));
+            if (GRAD)
+                dVn = csub(dVc, cadd(cscale(Vp, 2.0 * k2 * r * h), cscale(dVp, K2 * h)));
+        }
+        Vp = Vc; Vc = Vn;
+        if (GRAD) { dVp = dVc; dVc = dVn; }
     }
     HelmOut o;
     o.val = S;
     if (GRAD) {
-        // dR0/da = 2a, dR1/da = 2b, dR1/db = 2a, dR2/db = 2b
         for (int d = 0; d < 3; ++d) {
-            o.ga[d] = cadd(cscale(dS[0], 2.0 * a[d]), cscale(dS[1], 2.0 * b[d]));
-            o.gb[d] = cadd(cscale(dS[1], 2.0 * a[d]), cscale(dS[2], 2.0 * b[d]));
+            const double dw_da = b[d] * Ainv - 2.0 * D * a[d] * Ainv * Ainv;
+            const double dv_da = -2.0 * B2 * a[d] * Ainv * Ainv;
+            o.ga[d] = cadd(cadd(cscale(Sw, dw_da), cscale(Sv, dv_da)), cscale(Sr, a[d] * rinv));
+            o.gb[d] = cadd(cadd(cscale(Sw, a[d] * Ainv), cscale(Sv, 2.0 * b[d] * Ainv)),
+                           cscale(Sz, 2.0 * k2 * b[d]));
         }
     }
     return o;
