@@ -606,7 +606,7 @@ def headline(args, dev, rank, world, local_rank, budget, cpu_line, cpu_why):
         "metric": METRIC, "value": value, "unit": "Mpts/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mx,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32/3xtf32 with f64 offsets and sums", "data": "synthetic",
+        "dtype": "f32/3xf16 (row-scaled) with f64 offsets and sums", "data": "synthetic",
         "config": {
             "workload": f"laplace3d_fmm_sphere_plummer_n{args.npoints}_p{args.order}",
             "npoints": args.npoints, "order": args.order,
@@ -1354,7 +1354,7 @@ def stage_breakdown(w, trav, q_dev, dev, roofline=True, pipe_peaks=None):
                               * np.diff(np.asarray(csr.starts))).sum())
     mixed = w.precision == "mixed"
     kernels = {
-        "m2l": "m2l_tf32x3_kernel" if mixed else "m2l_f64_kernel<128>",
+        "m2l": (f"m2l_tc_kernel<{w.tc_format}>" if mixed else "m2l_f64_kernel<128>"),
         "m2p": "m2p_mixed_kernel<P>" if mixed else "m2p_reg_kernel<P>",
         "p2p": "p2p_csr_kernel<mixed>" if mixed else "p2p_csr_kernel<f64>",
         "p2l": "p2l_mixed_kernel<P>" if mixed else "p2l_reg_kernel<P>",
@@ -1371,12 +1371,17 @@ def stage_breakdown(w, trav, q_dev, dev, roofline=True, pipe_peaks=None):
              "work": {"flops": 2 * n * n * m2l_entries, "entries": m2l_entries,
                       "per_unit": "2 n^2 flops per List-2 entry"}}
         if mixed:
-            r["note"] = ("tcgen05 split-TF32 GEMM; algorithmic flops = 2 n^2 per List-2 entry "
-                         "(not the x3 split products, empty slots or padding); the stage time "
-                         "includes the TF32 split pre-pass")
+            split = "row-scaled F16" if w.tc_format == "f16" else "TF32"
+            r["note"] = (f"tcgen05 split-{split} GEMM (3 products); algorithmic flops = 2 n^2 "
+                         "per List-2 entry (not the x3 split products, empty slots or padding); "
+                         "the stage time includes the split pre-pass; peak: dense bf16 (the "
+                         "f16 rate)")
         # dram__bytes_read.sum + dram__bytes_write.sum of this launch on the 1M-point
-        # workload, one ncu capture per leaf size (profiles/m2l_tf32x3_sphere_plummer_1M_p10.md)
-        captured = {32: 1.227e9 + 0.195e9, 96: 256.6e6 + 38.4e6}
+        # workload, one ncu capture per leaf size and operand format
+        # (profiles/m2l_tc_f16_sphere_plummer_1M_p10.md, and for TF32
+        # profiles/m2l_tf32x3_sphere_plummer_1M_p10.md)
+        captured = ({96: 118.07e6 + 21.16e6} if w.tc_format == "f16"
+                    else {32: 1.227e9 + 0.195e9, 96: 256.6e6 + 38.4e6})
         if mixed and tree.nsources == NPOINTS and n == (ORDER + 1) ** 2 and \
                 MAX_PARTICLES in captured and \
                 int(tree.box_source_counts_nonchild.max()) <= MAX_PARTICLES:

@@ -301,6 +301,46 @@ int sumpy_class_gemm_tf32x3(
     const float *src_hi, const float *src_lo, int32_t tgt_base_ibox, double *tgt_expansions,
     int32_t *status, void *stream);
 
+/* The tensor-core M2L and class GEMMs with f16 operands (default of the
+ * mixed form): each FP64 operand row -- a class-operator row, or one source
+ * box's expansion -- is scaled by a power of two 2^e that brings its largest
+ * magnitude into [2^13, 2^14) and split as hi = f16(x 2^e), lo = f16(x 2^e -
+ * hi) (sumpy_split_f16x2_rowscale, which also writes row_inv = 2^-e; zero
+ * and padding rows: hi = lo = 0, row_inv = 1). The MMAs (kind::f16, FP32
+ * accumulation) form hi*hi + hi*lo + lo*hi per class group, as the tf32x3
+ * form does with TF32 halves: the same ~22 bits per operand, at twice the
+ * tensor rate and with half the operand bytes. The epilogue multiplies each
+ * group's FP32 result by src_rinv[source row], then by mats_rinv[class][row]
+ * (two FP32 products by powers of two, exact while the contribution lies in
+ * the FP32 normal range, as the mixed form's FP32 near field requires) and
+ * adds it to the FP64 sums; no operand row leaves the f16 range whatever its
+ * magnitude. Planes are f16 [..][k_pad] with k_pad a
+ * multiple of 64 (one 128-byte row per pipeline stage); k_split in
+ * [1, k_pad / 64]; mats_rinv [nclasses][rows_pad], src_rinv [src_nrows]
+ * (float). The last source row (src_nrows - 1) is all zeros. Other
+ * arguments as for the tf32x3 entries. */
+int sumpy_split_f16x2_rowscale(
+    int64_t nmat, int32_t rows, int32_t cols, const double *in,
+    int32_t rows_pad, int32_t cols_pad, void *hi, void *lo, float *row_inv, void *stream);
+
+int sumpy_m2l_translation_classes_f16x3(
+    int order, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
+    const int32_t *item_group_end, int32_t tile_width, const int32_t *tile_targets,
+    const double *tile_scale, const int32_t *group_class, const int32_t *group_sources,
+    int32_t nclasses, const void *mats_hi, const void *mats_lo, const float *mats_rinv,
+    int32_t rows_pad, int32_t k_pad, int32_t src_nrows, int32_t src_base_ibox,
+    const void *src_hi, const void *src_lo, const float *src_rinv, int32_t tgt_base_ibox,
+    double *tgt_expansions, int32_t *status, void *stream);
+
+int sumpy_class_gemm_f16x3(
+    int32_t n, int32_t k_split, int32_t nitems, const int32_t *item_tile,
+    const int32_t *item_group_begin, const int32_t *item_group_end, int32_t tile_width,
+    const int32_t *tile_targets, const double *tile_scale, const int32_t *group_class,
+    const int32_t *group_sources, int32_t nclasses, const void *mats_hi, const void *mats_lo,
+    const float *mats_rinv, int32_t rows_pad, int32_t k_pad, int32_t src_nrows,
+    int32_t src_base_ibox, const void *src_hi, const void *src_lo, const float *src_rinv,
+    int32_t tgt_base_ibox, double *tgt_expansions, int32_t *status, void *stream);
+
 /* Budget, in SM clock cycles (clock64), of every barrier wait in the
  * tensor-core kernels (the M2L above, the class GEMMs and the Helmholtz
  * M2L), read at each launch. A wait that runs out sets the abort flag of its
@@ -612,6 +652,16 @@ int sumpy_helmholtz_m2l_translation_classes_tf32x3(
     int32_t nclasses, const float *mats_hi, const float *mats_lo, int32_t rows_pad, int32_t k_pad,
     int32_t src_nrows, int32_t src_base_ibox, const float *src_hi, const float *src_lo,
     int32_t tgt_base_ibox, double *tgt_expansions, int32_t *status, void *stream);
+
+/* Same with f16 operand planes (see sumpy_m2l_translation_classes_f16x3). */
+int sumpy_helmholtz_m2l_translation_classes_f16x3(
+    int order, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
+    const int32_t *item_group_end, int32_t tile_width, const int32_t *tile_targets,
+    const double *tile_scale, const int32_t *group_class, const int32_t *group_sources,
+    int32_t nclasses, const void *mats_hi, const void *mats_lo, const float *mats_rinv,
+    int32_t rows_pad, int32_t k_pad, int32_t src_nrows, int32_t src_base_ibox,
+    const void *src_hi, const void *src_lo, const float *src_rinv, int32_t tgt_base_ibox,
+    double *tgt_expansions, int32_t *status, void *stream);
 
 /* E2PFromSingleBox (sumpy/e2p.py:123-226): result assigned */
 int sumpy_helmholtz_e2p_from_single_box_f64(

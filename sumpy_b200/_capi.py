@@ -44,6 +44,17 @@ SIGNATURES = {
     "sumpy_m2l_translation_classes_f64": [cint, i32, ptr, ptr, ptr, i32, ptr, ptr, ptr, ptr,
                                           i32, ptr, i32, ptr, i32, ptr, ptr],
     "sumpy_split_tf32x2": [i64, i32, i32, ptr, i32, i32, ptr, ptr, ptr],
+    "sumpy_split_f16x2_rowscale": [i64, i32, i32, ptr, i32, i32, ptr, ptr, ptr, ptr],
+    "sumpy_m2l_translation_classes_f16x3": [cint, i32, ptr, ptr, ptr, i32, ptr, ptr, ptr, ptr,
+                                            i32, ptr, ptr, ptr, i32, i32, i32, i32, ptr, ptr,
+                                            ptr, i32, ptr, ptr, ptr],
+    "sumpy_helmholtz_m2l_translation_classes_f16x3": [cint, i32, ptr, ptr, ptr, i32, ptr, ptr,
+                                                      ptr, ptr, i32, ptr, ptr, ptr, i32, i32,
+                                                      i32, i32, ptr, ptr, ptr, i32, ptr, ptr,
+                                                      ptr],
+    "sumpy_class_gemm_f16x3": [i32, i32, i32, ptr, ptr, ptr, i32, ptr, ptr, ptr, ptr, i32, ptr,
+                               ptr, ptr, i32, i32, i32, i32, ptr, ptr, ptr, i32, ptr, ptr,
+                               ptr],
     "sumpy_set_tc_wait_cycles": [i64],
     "sumpy_tree_gpu_build": [i64, ptr, ptr, ptr, i64, ptr, ptr, ptr, i32, ptr, ptr, cint, cint,
                              ptr, dbl, ptr, ptr],

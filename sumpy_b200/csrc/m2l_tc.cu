@@ -36,6 +36,7 @@
 #include <string>
 
 #include <cuda.h>
+#include <cuda_fp16.h>
 
 #include "common.cuh"
 
@@ -151,9 +152,12 @@ __device__ __forceinline__ uint64_t sw_desc(uint32_t saddr)
     return d;
 }
 
-// Instruction descriptor: D f32, A/B tf32, both K-major, N = 128, M = 128.
+// Instruction descriptors: D f32, A/B tf32 (format 2) or f16 (format 0),
+// both K-major, N = 128, M = 128.
 constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_TW >> 3) << 17) |
                            ((uint32_t)(TC_M >> 4) << 24);
+constexpr uint32_t IDESC_F16 = (1u << 4) | ((uint32_t)(TC_TW >> 3) << 17) |
+                               ((uint32_t)(TC_M >> 4) << 24);
 
 __device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t acc)
 {
@@ -162,6 +166,15 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t adesc, uint64_t
         "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
         " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(tmem),
         "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ void mma_f16(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t acc)
+{
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(tmem),
+        "l"(adesc), "l"(bdesc), "r"(IDESC_F16), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z));
 }
 
 __device__ __forceinline__ void mma_commit(uint32_t mbar)
@@ -188,7 +201,9 @@ struct TcArgs {
     const int32_t *tile_targets;
     const double *tile_scale;
     const int32_t *group_class, *group_sources;
-    const float *src_hi, *src_lo;
+    const void *src_hi, *src_lo;       // operand planes (fp32 for tf32, f16 for f16)
+    const float *src_rinv, *mat_rinv;  // f16 form: 2^-e of each source row / operator row
+    int32_t rows_pad;
     int32_t src_row_base, zero_row;
     int32_t tbase;
     double *tgt;
@@ -255,8 +270,9 @@ __device__ bool mbar_wait_or_abort(uint32_t addr, uint32_t parity, volatile int 
 // other: no FP32 sum spans more than one group. Draining warp w covers TMEM
 // lanes 32*(w%4).. and 64 of the 128 columns. The item's sums are added to
 // the local expansions with FP64 atomics (a tile may span several items).
+template <bool F16>
 __global__ void __launch_bounds__(TC_THREADS, 1)
-m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
+m2l_tc_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
                   const __grid_constant__ CUtensorMap map_a_lo,
                   const __grid_constant__ CUtensorMap map_b_hi,
                   const __grid_constant__ CUtensorMap map_b_lo)
@@ -274,6 +290,10 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
     const uint32_t full_bar = bar0, empty_bar = bar0 + 8 * TC_STAGES;
     const uint32_t accf_bar = bar0 + 16 * TC_STAGES, acce_bar = accf_bar + 16;
 
+    // operand element size and K per stage (one ROWB-byte row of K)
+    constexpr int ES = F16 ? 2 : 4;
+    constexpr int KC = ROWB / ES;
+    constexpr bool GATHER = TC_GATHER && !F16;
     const int item = blockIdx.x;
     const int row0 = blockIdx.y * TC_M;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -288,7 +308,7 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
     if (threadIdx.x == 32) {
         for (int s = 0; s < TC_STAGES; ++s) {
             // TMA expect-tx + one arrival per copying loader warp
-            mbar_init(full_bar + 8 * s, TC_GATHER ? 1 : TC_LOADERS / 32 + 1);
+            mbar_init(full_bar + 8 * s, GATHER ? 1 : TC_LOADERS / 32 + 1);
             mbar_init(empty_bar + 8 * s, 1);
         }
         for (int s = 0; s < 2; ++s) {
@@ -301,7 +321,7 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
     if (threadIdx.x == 64) {
         asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&map_a_hi)) : "memory");
         asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&map_a_lo)) : "memory");
-        if (TC_GATHER) {
+        if (GATHER) {
             asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&map_b_hi)) : "memory");
             asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&map_b_lo)) : "memory");
         }
@@ -316,12 +336,12 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
     const int ng = g1 - g0;
     // split K: CTA z of gridDim.z takes K chunks [kcb, kcb + nkc) of every
     // group (the host keeps gridDim.z <= the number of chunks)
-    const int nkc_all = a.k_pad / TC_KC;
+    const int nkc_all = a.k_pad / KC;
     const int kcb = (int)((int64_t)blockIdx.z * nkc_all / gridDim.z);
     const int nkc = (int)((int64_t)(blockIdx.z + 1) * nkc_all / gridDim.z) - kcb;
     const int total = ng * nkc;
 
-    if (TC_GATHER && warp == 0) {
+    if (GATHER && warp == 0) {
         // ---------------- loader (one warp, all TMA) ----------------
         // lane 0: the two operator tiles; lane l: gather4 of slots 4l..4l+3
         // of both source planes (empty slots read the zero row); lane 0
@@ -352,7 +372,7 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
             bool ok = true;
             if (use > 0) ok = mbar_wait_or_abort(empty_bar + 8 * s, (use - 1) & 1, abort_flag, a.wait_cycles);
             if (__any_sync(FULL, !ok || *abort_flag)) break;
-            const int k0 = (kcb + kc) * TC_KC;
+            const int k0 = (kcb + kc) * KC;
             const uint32_t st = base + s * STAGE;
             if (lane == 0) {
                 mbar_expect_tx(full_bar + 8 * s, 4 * PLANE);
@@ -371,7 +391,7 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
                 cls_cur = cls_nxt;
             }
         }
-    } else if (!TC_GATHER && warp < TC_LOADERS / 32) {
+    } else if (!GATHER && warp < TC_LOADERS / 32) {
         // ---------------- loaders ----------------
         // thread 0: TMA tiles of the two operator planes; all 96 threads:
         // cp.async row copies of the two source planes (the gathered
@@ -413,7 +433,7 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
             bool ok = true;
             if (use > 0) ok = mbar_wait_or_abort(empty_bar + 8 * s, (use - 1) & 1, abort_flag, a.wait_cycles);
             if (__any_sync(FULLMASK, !ok || *abort_flag)) break;
-            const int k0 = (kcb + kc) * TC_KC;
+            const int k0 = (kcb + kc) * KC;
             const uint32_t st = base + s * STAGE;
             if (threadIdx.x == 0) {
                 mbar_expect_tx(full_bar + 8 * s, 2 * PLANE);
@@ -431,10 +451,12 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
                         slot * ROWB + ((q ^ (((slot * ROWB) >> 7) & (CPR - 1))) << 4);
                     // empty slots: zero-fill without reading memory (source size 0)
                     const int64_t row = sb >= 0 ? sb - a.src_row_base : a.zero_row;
-                    const int64_t off = row * a.k_pad + k0 + 4 * q;
+                    const int64_t off = (row * a.k_pad + k0) * ES + 16 * q;   // bytes
                     const uint32_t bytes = sb >= 0 ? 16u : 0u;
-                    cp_async16(st + 2 * PLANE + dst, a.src_hi + off, bytes);
-                    cp_async16(st + 3 * PLANE + dst, a.src_lo + off, bytes);
+                    cp_async16(st + 2 * PLANE + dst,
+                               static_cast<const char *>(a.src_hi) + off, bytes);
+                    cp_async16(st + 3 * PLANE + dst,
+                               static_cast<const char *>(a.src_lo) + off, bytes);
                 }
             }
             cp_async_commit();
@@ -475,11 +497,18 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
                 const uint64_t bh = sw_desc(st + 2 * PLANE), bl = sw_desc(st + 3 * PLANE);
                 const uint32_t d = tmem + (uint32_t)(acc * TC_TW);
 #pragma unroll
-                for (int k = 0; k < TC_KC / 8; ++k) {
-                    const uint64_t ko = (uint64_t)(k * 32 >> 4);  // 8 fp32 = 32 bytes along K
-                    mma_tf32(d, ah + ko, bh + ko, (kc > 0 || k > 0) ? 1u : 0u);
-                    mma_tf32(d, ah + ko, bl + ko, 1u);
-                    mma_tf32(d, al + ko, bh + ko, 1u);
+                for (int k = 0; k < ROWB / 32; ++k) {
+                    // one MMA K-step is 32 bytes along K (8 tf32 or 16 f16)
+                    const uint64_t ko = (uint64_t)(k * 32 >> 4);
+                    if (F16) {
+                        mma_f16(d, ah + ko, bh + ko, (kc > 0 || k > 0) ? 1u : 0u);
+                        mma_f16(d, ah + ko, bl + ko, 1u);
+                        mma_f16(d, al + ko, bh + ko, 1u);
+                    } else {
+                        mma_tf32(d, ah + ko, bh + ko, (kc > 0 || k > 0) ? 1u : 0u);
+                        mma_tf32(d, ah + ko, bl + ko, 1u);
+                        mma_tf32(d, al + ko, bh + ko, 1u);
+                    }
                 }
                 mma_commit(empty_bar + 8 * s);
                 if (kc == nkc - 1) mma_commit(accf_bar + 8 * acc);
@@ -497,6 +526,18 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
         bool ok = true;
         for (int gi = 0; gi < ng && ok; ++gi) {
             const int acc = gi & 1;
+            // f16 form: the product of this thread's operator-row scale and
+            // each column's source-row scale (lane l holds columns l and
+            // 32 + l of this warp's 64; shuffled out below); empty slots 0
+            float rs = 1.0f, cs0 = 0.0f, cs1 = 0.0f;
+            if (F16) {
+                const int g = g0 + gi;
+                const int32_t *gs = a.group_sources + (int64_t)g * TC_TW + half * 64;
+                const int32_t s0 = gs[lane], s1 = gs[32 + lane];
+                cs0 = s0 >= 0 ? a.src_rinv[s0 - a.src_row_base] : 0.0f;
+                cs1 = s1 >= 0 ? a.src_rinv[s1 - a.src_row_base] : 0.0f;
+                rs = a.mat_rinv[(int64_t)a.group_class[g] * a.rows_pad + row0 + quad * 32 + lane];
+            }
             ok = mbar_wait_or_abort(accf_bar + 8 * acc, (gi >> 1) & 1, abort_flag, a.wait_cycles);
             ok = __all_sync(0xffffffffu, ok);
             if (!ok) break;
@@ -507,7 +548,19 @@ m2l_tf32x3_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
                 uint32_t r[16];
                 tmem_ld16(taddr + c0, r);
 #pragma unroll
-                for (int j = 0; j < 16; ++j) acc64[c0 + j] += (double)__uint_as_float(r[j]);
+                for (int j = 0; j < 16; ++j) {
+                    if (F16) {
+                        // powers of two, applied in two FP32 products (column
+                        // scale first): exact whenever the contribution lies
+                        // in the FP32 normal range, the range the mixed form's
+                        // FP32 near field needs anyway
+                        const int col = c0 + j;
+                        const float cs = __shfl_sync(0xffffffffu, col < 32 ? cs0 : cs1, col & 31);
+                        acc64[col] += (double)((__uint_as_float(r[j]) * cs) * rs);
+                    } else {
+                        acc64[c0 + j] += (double)__uint_as_float(r[j]);
+                    }
+                }
             }
             tc_fence_before();
             __syncwarp();
@@ -567,12 +620,72 @@ __global__ void split_tf32x2_kernel(int64_t nmat, int rows, int cols, const doub
     }
 }
 
+// f16 hi/lo planes with a power-of-two scale per row: one warp per padded
+// row. Row r of matrix m is scaled by 2^e with e chosen so that the row's
+// largest magnitude lands in [2^13, 2^14) (|e| <= 126), then split as
+// hi = f16(x 2^e), lo = f16(x 2^e - hi); inv[row] = 2^-e. Zero rows and
+// padding rows get hi = lo = 0 and inv = 1. The scaling keeps every row in
+// the f16 exponent range whatever the magnitudes of the data.
+__global__ void split_f16x2_rowscale_kernel(int64_t nrows_total, int rows, int cols,
+                                            const double *__restrict__ in, int rows_pad,
+                                            int cols_pad, __half *__restrict__ hi,
+                                            __half *__restrict__ lo, float *__restrict__ inv)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t wr = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); wr < nrows_total;
+         wr += warps) {
+        const int r = (int)(wr % rows_pad);
+        const int64_t m = wr / rows_pad;
+        const bool real_row = r < rows;
+        const double *row = in + (m * rows + r) * (int64_t)cols;
+        double mx = 0.0;
+        if (real_row)
+            for (int c = lane; c < cols; c += 32) mx = fmax(mx, fabs(row[c]));
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+        int e = 0;
+        if (mx > 0.0) {
+            int ex;
+            frexp(mx, &ex);              // mx = f 2^ex, f in [0.5, 1)
+            e = 14 - ex;                 // mx 2^e in [2^13, 2^14)
+            e = e > 126 ? 126 : (e < -126 ? -126 : e);
+        }
+        __half *h = hi + wr * cols_pad;
+        __half *l = lo + wr * cols_pad;
+        for (int c = lane; c < cols_pad; c += 32) {
+            const double v = (real_row && c < cols) ? ldexp(row[c], e) : 0.0;
+            const __half vh = __double2half(v);
+            h[c] = vh;
+            l[c] = __double2half(v - (double)__half2float(vh));
+        }
+        if (lane == 0) inv[wr] = ldexpf(1.0f, -e);
+    }
+}
+
 }  // namespace
 }  // namespace sumpy
 
 using namespace sumpy;
 
 extern "C" {
+
+int sumpy_split_f16x2_rowscale(int64_t nmat, int32_t rows, int32_t cols, const double *in,
+                               int32_t rows_pad, int32_t cols_pad, void *hi, void *lo,
+                               float *row_inv, void *stream)
+{
+    if (nmat < 0 || rows < 0 || cols < 0 || rows_pad < rows || cols_pad < cols)
+        return bad_arg("split_f16x2_rowscale: bad sizes");
+    if (nmat == 0 || rows_pad == 0 || cols_pad == 0) return SUMPY_OK;
+    if ((rows > 0 && cols > 0 && !in) || !hi || !lo || !row_inv)
+        return bad_arg("split_f16x2_rowscale: null pointer");
+    const int64_t nr = nmat * rows_pad;
+    const int64_t blocks = std::min<int64_t>((nr + 7) / 8, 148 * 16);
+    split_f16x2_rowscale_kernel<<<(unsigned)blocks, 256, 0, as_stream(stream)>>>(
+        nr, rows, cols, in, rows_pad, cols_pad, static_cast<__half *>(hi),
+        static_cast<__half *>(lo), row_inv);
+    return check_launch("split_f16x2_rowscale_kernel");
+}
 
 int sumpy_split_tf32x2(int64_t nmat, int32_t rows, int32_t cols, const double *in,
                        int32_t rows_pad, int32_t cols_pad, float *hi, float *lo, void *stream)
@@ -607,18 +720,21 @@ static EncodeTiledFn encode_tiled_fn()
     return fn;
 }
 
-// fp32 tensor map over [dims[rank-1]]...[dims[0]], ROWB-byte swizzle, box {TC_KC, box1, 1}
-static bool make_map(CUtensorMap *m, const float *ptr, int rank, const uint64_t *dims,
+// fp32 or f16 tensor map over [dims[rank-1]]...[dims[0]], ROWB-byte swizzle,
+// box {one ROWB-byte row of K, box1, 1}
+static bool make_map(CUtensorMap *m, const void *ptr, bool f16, int rank, const uint64_t *dims,
                      uint32_t box1)
 {
     EncodeTiledFn fn = encode_tiled_fn();
     if (!fn) return false;
+    const uint64_t es = f16 ? 2 : 4;
     cuuint64_t gdim[3], gstride[2];
-    cuuint32_t box[3] = {(cuuint32_t)TC_KC, box1, 1}, estr[3] = {1, 1, 1};
+    cuuint32_t box[3] = {(cuuint32_t)(ROWB / es), box1, 1}, estr[3] = {1, 1, 1};
     for (int i = 0; i < rank; ++i) gdim[i] = dims[i];
-    gstride[0] = dims[0] * sizeof(float);
-    if (rank == 3) gstride[1] = dims[0] * dims[1] * sizeof(float);
-    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, const_cast<float *>(ptr), gdim, gstride,
+    gstride[0] = dims[0] * es;
+    if (rank == 3) gstride[1] = dims[0] * dims[1] * es;
+    CUresult r = fn(m, f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank,
+                    const_cast<void *>(ptr), gdim, gstride,
                     box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                     ROWB == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -629,7 +745,78 @@ static bool make_map(CUtensorMap *m, const float *ptr, int rank, const uint64_t 
 
 // n = real coefficients per expansion row: ncoeff for real data, 2 ncoeff for
 // complex data stored as interleaved (re, im) with the real embedding of the
-// complex operators.
+// complex operators. f16: operand planes are f16 with the row scales
+// mats_rinv [nclasses][rows_pad] and src_rinv [src_nrows]; otherwise fp32
+// holding tf32 values (the row-scale pointers are ignored).
+static int m2l_tc_launch(
+    bool f16, int n, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
+    const int32_t *item_group_end, int32_t tile_width, const int32_t *tile_targets,
+    const double *tile_scale, const int32_t *group_class, const int32_t *group_sources,
+    int32_t nclasses, const void *mats_hi, const void *mats_lo, const float *mats_rinv,
+    int32_t rows_pad, int32_t k_pad, int32_t src_nrows, int32_t src_base_ibox,
+    const void *src_hi, const void *src_lo, const float *src_rinv, int32_t tgt_base_ibox,
+    double *tgt_expansions, int32_t *status, void *stream, int32_t k_split = 1)
+{
+    const char *who = f16 ? "m2l_f16x3" : "m2l_tf32x3";
+    const int kc = f16 ? ROWB / 2 : ROWB / 4;   // K per stage
+    if (tile_width != TC_TW) return bad_arg((std::string(who) + ": tile_width must be 128").c_str());
+    if (k_pad < n || k_pad % kc)
+        return bad_arg((std::string(who) + ": k_pad must be a multiple of " + std::to_string(kc) +
+                       " >= ncoeff").c_str());
+    if (k_split < 1 || k_split > k_pad / kc)
+        return bad_arg((std::string(who) + ": k_split must be in [1, k_pad / " +
+                       std::to_string(kc) + "]").c_str());
+    if (rows_pad < n || rows_pad % TC_M)
+        return bad_arg((std::string(who) + ": rows_pad must be a multiple of 128 >= ncoeff").c_str());
+    if (nitems < 0 || nclasses <= 0 || src_nrows < 1)
+        return bad_arg((std::string(who) + ": bad sizes").c_str());
+    if (nitems == 0) return SUMPY_OK;
+    if (!item_tile || !item_group_begin || !item_group_end || !tile_targets || !tile_scale ||
+        !group_class || !group_sources || !mats_hi || !mats_lo || !src_hi || !src_lo ||
+        !tgt_expansions || (f16 && (!mats_rinv || !src_rinv)))
+        return bad_arg((std::string(who) + ": null pointer argument").c_str());
+    if ((reinterpret_cast<uintptr_t>(mats_hi) | reinterpret_cast<uintptr_t>(mats_lo) |
+         reinterpret_cast<uintptr_t>(src_hi) | reinterpret_cast<uintptr_t>(src_lo)) & 15)
+        return bad_arg((std::string(who) + ": operand planes must be 16-byte aligned").c_str());
+    // set on every launch (a cheap host call): an attribute remembered per
+    // device would be lost with a context that was torn down and recreated
+    cudaError_t e = f16 ? cudaFuncSetAttribute(m2l_tc_kernel<true>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM)
+                        : cudaFuncSetAttribute(m2l_tc_kernel<false>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+    if (e != cudaSuccess) {
+        set_last_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+        return SUMPY_ELAUNCH;
+    }
+    CUtensorMap ma_hi, ma_lo, mb_hi, mb_lo;
+    const uint64_t adims[3] = {(uint64_t)k_pad, (uint64_t)rows_pad, (uint64_t)nclasses};
+    const uint64_t bdims[2] = {(uint64_t)k_pad, (uint64_t)src_nrows};
+    if (!make_map(&ma_hi, mats_hi, f16, 3, adims, TC_M) ||
+        !make_map(&ma_lo, mats_lo, f16, 3, adims, TC_M) ||
+        !make_map(&mb_hi, src_hi, f16, 2, bdims, 1) || !make_map(&mb_lo, src_lo, f16, 2, bdims, 1)) {
+        set_last_error(std::string(who) + ": tensor map encoding failed");
+        return SUMPY_EINVAL;
+    }
+    TcArgs a;
+    a.n = n; a.k_pad = k_pad;
+    a.item_tile = item_tile; a.item_g0 = item_group_begin; a.item_g1 = item_group_end;
+    a.tile_targets = tile_targets; a.tile_scale = tile_scale;
+    a.group_class = group_class; a.group_sources = group_sources;
+    a.src_hi = src_hi; a.src_lo = src_lo;
+    a.src_rinv = src_rinv; a.mat_rinv = mats_rinv; a.rows_pad = rows_pad;
+    a.src_row_base = src_base_ibox; a.zero_row = src_nrows - 1;
+    a.tbase = tgt_base_ibox; a.tgt = tgt_expansions; a.status = status;
+    a.wait_cycles = wait_cycles_budget();
+    dim3 grid(nitems, rows_pad / TC_M, k_split);
+    if (f16)
+        m2l_tc_kernel<true><<<grid, TC_THREADS, TC_SMEM, as_stream(stream)>>>(a, ma_hi, ma_lo,
+                                                                             mb_hi, mb_lo);
+    else
+        m2l_tc_kernel<false><<<grid, TC_THREADS, TC_SMEM, as_stream(stream)>>>(a, ma_hi, ma_lo,
+                                                                              mb_hi, mb_lo);
+    return check_launch(f16 ? "m2l_tc_kernel<f16>" : "m2l_tc_kernel<tf32>");
+}
+
 static int m2l_tf32x3_launch(
     int n, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
     const int32_t *item_group_end, int32_t tile_width, const int32_t *tile_targets,
@@ -639,49 +826,11 @@ static int m2l_tf32x3_launch(
     int32_t tgt_base_ibox, double *tgt_expansions, int32_t *status, void *stream,
     int32_t k_split = 1)
 {
-    if (tile_width != TC_TW) return bad_arg("m2l_tf32x3: tile_width must be 128");
-    if (k_split < 1 || k_split > k_pad / TC_KC)
-        return bad_arg("m2l_tf32x3: k_split must be in [1, k_pad / 32]");
-    if (rows_pad < n || rows_pad % TC_M) return bad_arg("m2l_tf32x3: rows_pad must be a multiple of 128 >= ncoeff");
-    if (k_pad < n || k_pad % 32) return bad_arg("m2l_tf32x3: k_pad must be a multiple of 32 >= ncoeff");
-    if (nitems < 0 || nclasses <= 0 || src_nrows < 1) return bad_arg("m2l_tf32x3: bad sizes");
-    if (nitems == 0) return SUMPY_OK;
-    if (!item_tile || !item_group_begin || !item_group_end || !tile_targets || !tile_scale ||
-        !group_class || !group_sources || !mats_hi || !mats_lo || !src_hi || !src_lo ||
-        !tgt_expansions)
-        return bad_arg("m2l_tf32x3: null pointer argument");
-    if ((reinterpret_cast<uintptr_t>(mats_hi) | reinterpret_cast<uintptr_t>(mats_lo) |
-         reinterpret_cast<uintptr_t>(src_hi) | reinterpret_cast<uintptr_t>(src_lo)) & 15)
-        return bad_arg("m2l_tf32x3: operand planes must be 16-byte aligned");
-    // set on every launch (a cheap host call): an attribute remembered per
-    // device would be lost with a context that was torn down and recreated
-    cudaError_t e = cudaFuncSetAttribute(m2l_tf32x3_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
-    if (e != cudaSuccess) {
-        set_last_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
-        return SUMPY_ELAUNCH;
-    }
-    CUtensorMap ma_hi, ma_lo, mb_hi, mb_lo;
-    const uint64_t adims[3] = {(uint64_t)k_pad, (uint64_t)rows_pad, (uint64_t)nclasses};
-    const uint64_t bdims[2] = {(uint64_t)k_pad, (uint64_t)src_nrows};
-    if (!make_map(&ma_hi, mats_hi, 3, adims, TC_M) || !make_map(&ma_lo, mats_lo, 3, adims, TC_M) ||
-        !make_map(&mb_hi, src_hi, 2, bdims, 1) || !make_map(&mb_lo, src_lo, 2, bdims, 1)) {
-        set_last_error("m2l_tf32x3: tensor map encoding failed");
-        return SUMPY_EINVAL;
-    }
-    TcArgs a;
-    a.n = n; a.k_pad = k_pad;
-    a.item_tile = item_tile; a.item_g0 = item_group_begin; a.item_g1 = item_group_end;
-    a.tile_targets = tile_targets; a.tile_scale = tile_scale;
-    a.group_class = group_class; a.group_sources = group_sources;
-    a.src_hi = src_hi; a.src_lo = src_lo;
-    a.src_row_base = src_base_ibox; a.zero_row = src_nrows - 1;
-    a.tbase = tgt_base_ibox; a.tgt = tgt_expansions; a.status = status;
-    a.wait_cycles = wait_cycles_budget();
-    dim3 grid(nitems, rows_pad / TC_M, k_split);
-    m2l_tf32x3_kernel<<<grid, TC_THREADS, TC_SMEM, as_stream(stream)>>>(a, ma_hi, ma_lo, mb_hi,
-                                                                        mb_lo);
-    return check_launch("m2l_tf32x3_kernel");
+    return m2l_tc_launch(false, n, nitems, item_tile, item_group_begin, item_group_end,
+                         tile_width, tile_targets, tile_scale, group_class, group_sources,
+                         nclasses, mats_hi, mats_lo, nullptr, rows_pad, k_pad, src_nrows,
+                         src_base_ibox, src_hi, src_lo, nullptr, tgt_base_ibox, tgt_expansions,
+                         status, stream, k_split);
 }
 
 extern "C" {
@@ -738,6 +887,63 @@ int sumpy_helmholtz_m2l_translation_classes_tf32x3(
                              group_sources, nclasses, mats_hi, mats_lo, rows_pad, k_pad,
                              src_nrows, src_base_ibox, src_hi, src_lo, tgt_base_ibox,
                              tgt_expansions, status, stream);
+}
+
+int sumpy_m2l_translation_classes_f16x3(
+    int order, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
+    const int32_t *item_group_end, int32_t tile_width, const int32_t *tile_targets,
+    const double *tile_scale, const int32_t *group_class, const int32_t *group_sources,
+    int32_t nclasses, const void *mats_hi, const void *mats_lo, const float *mats_rinv,
+    int32_t rows_pad, int32_t k_pad, int32_t src_nrows, int32_t src_base_ibox,
+    const void *src_hi, const void *src_lo, const float *src_rinv, int32_t tgt_base_ibox,
+    double *tgt_expansions, int32_t *status, void *stream)
+{
+    if (order < 0 || order > SUMPY_MAX_ORDER) {
+        set_last_error("m2l_f16x3: unsupported order");
+        return SUMPY_EUNSUPPORTED;
+    }
+    return m2l_tc_launch(true, ncoeff_of(order), nitems, item_tile, item_group_begin,
+                         item_group_end, tile_width, tile_targets, tile_scale, group_class,
+                         group_sources, nclasses, mats_hi, mats_lo, mats_rinv, rows_pad, k_pad,
+                         src_nrows, src_base_ibox, src_hi, src_lo, src_rinv, tgt_base_ibox,
+                         tgt_expansions, status, stream);
+}
+
+int sumpy_helmholtz_m2l_translation_classes_f16x3(
+    int order, int32_t nitems, const int32_t *item_tile, const int32_t *item_group_begin,
+    const int32_t *item_group_end, int32_t tile_width, const int32_t *tile_targets,
+    const double *tile_scale, const int32_t *group_class, const int32_t *group_sources,
+    int32_t nclasses, const void *mats_hi, const void *mats_lo, const float *mats_rinv,
+    int32_t rows_pad, int32_t k_pad, int32_t src_nrows, int32_t src_base_ibox,
+    const void *src_hi, const void *src_lo, const float *src_rinv, int32_t tgt_base_ibox,
+    double *tgt_expansions, int32_t *status, void *stream)
+{
+    if (order < 0 || order > SUMPY_MAX_ORDER) {
+        set_last_error("helmholtz m2l_f16x3: unsupported order");
+        return SUMPY_EUNSUPPORTED;
+    }
+    return m2l_tc_launch(true, 2 * ncoeff_of(order), nitems, item_tile, item_group_begin,
+                         item_group_end, tile_width, tile_targets, tile_scale, group_class,
+                         group_sources, nclasses, mats_hi, mats_lo, mats_rinv, rows_pad, k_pad,
+                         src_nrows, src_base_ibox, src_hi, src_lo, src_rinv, tgt_base_ibox,
+                         tgt_expansions, status, stream);
+}
+
+int sumpy_class_gemm_f16x3(
+    int32_t n, int32_t k_split, int32_t nitems, const int32_t *item_tile,
+    const int32_t *item_group_begin, const int32_t *item_group_end, int32_t tile_width,
+    const int32_t *tile_targets, const double *tile_scale, const int32_t *group_class,
+    const int32_t *group_sources, int32_t nclasses, const void *mats_hi, const void *mats_lo,
+    const float *mats_rinv, int32_t rows_pad, int32_t k_pad, int32_t src_nrows,
+    int32_t src_base_ibox, const void *src_hi, const void *src_lo, const float *src_rinv,
+    int32_t tgt_base_ibox, double *tgt_expansions, int32_t *status, void *stream)
+{
+    if (n < 1 || n > 2 * ncoeff_of(SUMPY_MAX_ORDER)) return bad_arg("class gemm f16x3: bad n");
+    return m2l_tc_launch(true, n, nitems, item_tile, item_group_begin, item_group_end,
+                         tile_width, tile_targets, tile_scale, group_class, group_sources,
+                         nclasses, mats_hi, mats_lo, mats_rinv, rows_pad, k_pad, src_nrows,
+                         src_base_ibox, src_hi, src_lo, src_rinv, tgt_base_ibox, tgt_expansions,
+                         status, stream, k_split);
 }
 
 // ---------------------------------------------------------------------------

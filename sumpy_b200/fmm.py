@@ -303,6 +303,13 @@ class SumpyExpansionWrangler:
         # form's error). Helmholtz mixed: M2M on the tensor cores.
         self.tc_m2m = self.helmholtz
         self.tc_l2l = False
+        # operand format of the tensor-core GEMMs (mixed form): "f16" splits
+        # every operand row into two f16 halves after scaling it by a power
+        # of two (row max in [2^13, 2^14)), the scales undone in the FP64
+        # epilogue; "tf32" splits into two TF32 values. Both keep ~22 bits
+        # per operand with FP32 sums per class group; f16 runs at twice the
+        # tensor rate with half the operand bytes.
+        self.tc_format = "f16"
         self.gemm_l2l = True
         self.gemm_m2m = True
         # FP64 octant GEMMs of all levels in one persistent launch (a device
@@ -842,68 +849,108 @@ class SumpyExpansionWrangler:
              dptr(plan["group_class"]), dptr(plan["group_sources"]), _i32(mats.shape[0]),
              dptr(mats), _i32(sbase), dptr(src), _i32(tbase), dptr(tgt), st)
 
+    @property
+    def _tc_f16(self):
+        if self.tc_format not in ("f16", "tf32"):
+            raise ValueError(f"tc_format must be 'f16' or 'tf32', got {self.tc_format!r}")
+        return self.tc_format == "f16"
+
     @staticmethod
-    def _tc_pads(n):
-        return (n + 127) // 128 * 128, (n + 31) // 32 * 32
+    def _tc_pads(n, f16=False):
+        """Padded rows (MMA M) and K: K is a whole number of 128-byte rows
+        (32 tf32 or 64 f16)."""
+        kq = 64 if f16 else 32
+        return (n + 127) // 128 * 128, (n + kq - 1) // kq * kq
 
     def _m2l_tc_operands(self, mats):
-        """TF32 hi/lo planes [nclasses][rows_pad][k_pad] of a class-operator set."""
-        key = mats.data_ptr()
+        """Split planes [nclasses][rows_pad][k_pad] of a class-operator set:
+        (hi, lo, rows_pad, k_pad, row scales) -- f16 halves with a power-of-two
+        scale per operator row ([nclasses][rows_pad], the inverse scales), or
+        TF32 halves (row scales None)."""
+        f16 = self._tc_f16
+        key = (mats.data_ptr(), f16)
         hit = self._m2l_tc_mats.get(key)
         if hit is not None:
             return hit
         ncls, n, _ = mats.shape
-        rp, kp = self._tc_pads(n)
-        hi = torch.empty((ncls, rp, kp), dtype=torch.float32, device=self.device)
-        lo = torch.empty_like(hi)
-        call("sumpy_split_tf32x2", _i64(ncls), _i32(n), _i32(n), dptr(mats), _i32(rp),
-             _i32(kp), dptr(hi), dptr(lo), stream_ptr())
-        self._m2l_tc_mats[key] = (hi, lo, rp, kp)
+        rp, kp = self._tc_pads(n, f16)
+        if f16:
+            hi = torch.empty((ncls, rp, kp), dtype=torch.float16, device=self.device)
+            lo = torch.empty_like(hi)
+            rinv = torch.empty((ncls, rp), dtype=torch.float32, device=self.device)
+            call("sumpy_split_f16x2_rowscale", _i64(ncls), _i32(n), _i32(n), dptr(mats),
+                 _i32(rp), _i32(kp), dptr(hi), dptr(lo), dptr(rinv), stream_ptr())
+        else:
+            hi = torch.empty((ncls, rp, kp), dtype=torch.float32, device=self.device)
+            lo = torch.empty_like(hi)
+            rinv = None
+            call("sumpy_split_tf32x2", _i64(ncls), _i32(n), _i32(n), dptr(mats), _i32(rp),
+                 _i32(kp), dptr(hi), dptr(lo), stream_ptr())
+        self._m2l_tc_mats[key] = (hi, lo, rp, kp, rinv)
         return self._m2l_tc_mats[key]
 
     def _m2l_workspace(self, nrows, kp):
-        """TF32 hi/lo planes of the source multipoles, [nrows + 1][kp]; the
-        extra last row stays zero (it stands in for empty tile slots)."""
+        """Split planes of the source multipoles, [nrows + 1][kp], and (f16)
+        their row scales; the extra last row stays zero (it stands in for
+        empty tile slots)."""
+        f16 = self._tc_f16
+        dt = torch.float16 if f16 else torch.float32
         need = (nrows + 1) * kp
-        if self._m2l_ws is None or self._m2l_ws[0].numel() < need:
+        ws = self._m2l_ws
+        if ws is None or ws[0].dtype != dt or ws[0].numel() < need or ws[2].numel() < nrows + 1:
             rows = max(nrows, self.tree.nboxes) + 1
-            self._m2l_ws = (torch.empty(rows * kp, dtype=torch.float32, device=self.device),
-                            torch.empty(rows * kp, dtype=torch.float32, device=self.device))
-        hi, lo = self._m2l_ws
+            self._m2l_ws = (torch.empty(rows * kp, dtype=dt, device=self.device),
+                            torch.empty(rows * kp, dtype=dt, device=self.device),
+                            torch.empty(rows, dtype=torch.float32, device=self.device))
+        hi, lo, rinv = self._m2l_ws
         zero = slice(nrows * kp, (nrows + 1) * kp)
         hi[zero].zero_()
         lo[zero].zero_()
-        return hi, lo
+        rinv[nrows:nrows + 1].zero_()
+        return hi, lo, rinv
+
+    def _split_sources(self, nb, n, src, kp, ws, st):
+        """M2L pre-processing: every source expansion (row = box) as split planes."""
+        hi, lo, rinv = ws
+        if self._tc_f16:
+            call("sumpy_split_f16x2_rowscale", _i64(nb), _i32(1), _i32(n), dptr(src), _i32(1),
+                 _i32(kp), dptr(hi), dptr(lo), dptr(rinv), st)
+        else:
+            call("sumpy_split_tf32x2", _i64(nb), _i32(1), _i32(n), dptr(src), _i32(1),
+                 _i32(kp), dptr(hi), dptr(lo), st)
 
     def _launch_m2l_tc_merged(self, plan, mpole_exps, local_exps, st):
-        hi, lo, rp, kp = self._m2l_tc_operands(plan["mats"])
+        ops = self._m2l_tc_operands(plan["mats"])
         n = plan["mats"].shape[1]
         nb = self.tree.nboxes
-        ws_hi, ws_lo = self._m2l_workspace(nb, kp)
-        # M2L pre-processing: every multipole as TF32 hi/lo planes (row = box)
-        call("sumpy_split_tf32x2", _i64(nb), _i32(1), _i32(n), dptr(mpole_exps), _i32(1),
-             _i32(kp), dptr(ws_hi), dptr(ws_lo), st)
-        self._call_m2l_tc(self.level_orders[0], plan, hi, lo, rp, kp, nb + 1, 0, ws_hi, ws_lo,
-                          0, local_exps, st)
+        ws = self._m2l_workspace(nb, ops[3])
+        self._split_sources(nb, n, mpole_exps, ops[3], ws, st)
+        self._call_m2l_tc(self.level_orders[0], plan, ops, nb + 1, 0, ws, 0, local_exps, st)
 
-    def _call_m2l_tc(self, order, plan, hi, lo, rp, kp, src_nrows, sbase, ws_hi, ws_lo,
-                     tbase, tgt, st):
-        call(self._entry("sumpy_m2l_translation_classes_tf32x3"), _c(order),
-             _i32(plan["nitems"]),
-             dptr(plan["item_tile"]), dptr(plan["item_g0"]), dptr(plan["item_g1"]),
-             _i32(M2L_TILE_TC), dptr(plan["tile_targets"]), dptr(plan["tile_scale"]),
-             dptr(plan["group_class"]), dptr(plan["group_sources"]), _i32(plan["nclasses"]),
-             dptr(hi), dptr(lo), _i32(rp), _i32(kp), _i32(src_nrows), _i32(sbase),
-             dptr(ws_hi), dptr(ws_lo), _i32(tbase), dptr(tgt), dptr(self._status), st)
+    def _call_m2l_tc(self, order, plan, ops, src_nrows, sbase, ws, tbase, tgt, st):
+        hi, lo, rp, kp, rinv = ops
+        ws_hi, ws_lo, ws_rinv = ws
+        head = [_c(order), _i32(plan["nitems"]),
+                dptr(plan["item_tile"]), dptr(plan["item_g0"]), dptr(plan["item_g1"]),
+                _i32(M2L_TILE_TC), dptr(plan["tile_targets"]), dptr(plan["tile_scale"]),
+                dptr(plan["group_class"]), dptr(plan["group_sources"]), _i32(plan["nclasses"])]
+        tail = [_i32(tbase), dptr(tgt), dptr(self._status), st]
+        if self._tc_f16:
+            call(self._entry("sumpy_m2l_translation_classes_f16x3"), *head,
+                 dptr(hi), dptr(lo), dptr(rinv), _i32(rp), _i32(kp), _i32(src_nrows),
+                 _i32(sbase), dptr(ws_hi), dptr(ws_lo), dptr(ws_rinv), *tail)
+        else:
+            call(self._entry("sumpy_m2l_translation_classes_tf32x3"), *head,
+                 dptr(hi), dptr(lo), _i32(rp), _i32(kp), _i32(src_nrows), _i32(sbase),
+                 dptr(ws_hi), dptr(ws_lo), *tail)
 
     def _launch_m2l_tc_level(self, lev, items, mats, sbase, sview, tbase, tview, st):
-        hi, lo, rp, kp = self._m2l_tc_operands(mats)
+        ops = self._m2l_tc_operands(mats)
         nb, n = sview.shape[0], mats.shape[1]   # real values per box
-        ws_hi, ws_lo = self._m2l_workspace(nb, kp)
-        call("sumpy_split_tf32x2", _i64(nb), _i32(1), _i32(n), dptr(sview), _i32(1),
-             _i32(kp), dptr(ws_hi), dptr(ws_lo), st)
-        self._call_m2l_tc(self.level_orders[lev], items, hi, lo, rp, kp, nb + 1,
-                          sbase, ws_hi, ws_lo, tbase, tview, st)
+        ws = self._m2l_workspace(nb, ops[3])
+        self._split_sources(nb, n, sview, ops[3], ws, st)
+        self._call_m2l_tc(self.level_orders[lev], items, ops, nb + 1, sbase, ws, tbase, tview,
+                          st)
 
     # {{{ M2M / L2L as per-octant GEMMs on the tensor cores (mixed form)
 
@@ -921,7 +968,7 @@ class SumpyExpansionWrangler:
     def _octant_operator_planes(self, kind, parent_level=2):
         # Laplace: any level pair gives the same maps (take levels 2 -> 3)
         lev = parent_level if self.helmholtz else 2
-        key = ("octant-ops", kind, lev)
+        key = ("octant-ops", kind, lev, self._tc_f16)
         if key not in self._m2l_tc_mats:
             order = self.level_orders[0]
             # rscale as level_to_rscale (sumpy/fmm.py:369-386)
@@ -945,8 +992,7 @@ class SumpyExpansionWrangler:
                 emb[:, :, 1, :, 1] = ops
                 ops = emb.reshape(8, 2 * n, 2 * n)
             mats = torch.as_tensor(ops).to(self.device)
-            hi, lo, rp, kp = self._m2l_tc_operands(mats)
-            self._m2l_tc_mats[key] = (mats, hi, lo, rp, kp)
+            self._m2l_tc_mats[key] = (mats,) + self._m2l_tc_operands(mats)
         return self._m2l_tc_mats[key]
 
     def _octants(self, boxes):
@@ -999,7 +1045,7 @@ class SumpyExpansionWrangler:
 
     def _octant_gemm(self, kind, plan, sview, sbase, tview, tbase, st, fp64=False,
                      parent_level=2):
-        mats, hi, lo, rp, kp = self._octant_operator_planes(kind, parent_level)
+        mats, hi, lo, rp, kp, rinv = self._octant_operator_planes(kind, parent_level)
         n = mats.shape[1]   # real values per box
 
         def k_split(row_tiles, nkc, cap):
@@ -1017,16 +1063,22 @@ class SumpyExpansionWrangler:
                  dptr(mats), _i32(sbase), dptr(sview), _i32(tbase), dptr(tview), st)
             return
         nb = sview.shape[0]
-        ws_hi, ws_lo = self._m2l_workspace(nb, kp)
-        call("sumpy_split_tf32x2", _i64(nb), _i32(1), _i32(n), dptr(sview), _i32(1),
-             _i32(kp), dptr(ws_hi), dptr(ws_lo), st)
-        ks = k_split(rp // 128, kp // 32, 4)
-        call("sumpy_class_gemm_tf32x3", _i32(n), _i32(ks), _i32(plan["nitems"]),
-             dptr(plan["item_tile"]), dptr(plan["item_g0"]), dptr(plan["item_g1"]),
-             _i32(M2L_TILE_TC), dptr(plan["tile_targets"]), dptr(plan["tile_scale"]),
-             dptr(plan["group_class"]), dptr(plan["group_sources"]), _i32(plan["nclasses"]),
-             dptr(hi), dptr(lo), _i32(rp), _i32(kp), _i32(nb + 1), _i32(sbase),
-             dptr(ws_hi), dptr(ws_lo), _i32(tbase), dptr(tview), dptr(self._status), st)
+        ws = self._m2l_workspace(nb, kp)
+        self._split_sources(nb, n, sview, kp, ws, st)
+        f16 = self._tc_f16
+        ks = k_split(rp // 128, kp // (64 if f16 else 32), 4)
+        head = [_i32(n), _i32(ks), _i32(plan["nitems"]),
+                dptr(plan["item_tile"]), dptr(plan["item_g0"]), dptr(plan["item_g1"]),
+                _i32(M2L_TILE_TC), dptr(plan["tile_targets"]), dptr(plan["tile_scale"]),
+                dptr(plan["group_class"]), dptr(plan["group_sources"]), _i32(plan["nclasses"])]
+        tail = [_i32(tbase), dptr(tview), dptr(self._status), st]
+        if f16:
+            call("sumpy_class_gemm_f16x3", *head, dptr(hi), dptr(lo), dptr(rinv), _i32(rp),
+                 _i32(kp), _i32(nb + 1), _i32(sbase), dptr(ws[0]), dptr(ws[1]), dptr(ws[2]),
+                 *tail)
+        else:
+            call("sumpy_class_gemm_tf32x3", *head, dptr(hi), dptr(lo), _i32(rp), _i32(kp),
+                 _i32(nb + 1), _i32(sbase), dptr(ws[0]), dptr(ws[1]), *tail)
 
     @property
     def _gemm_fp64_ok(self):

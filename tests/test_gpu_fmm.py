@@ -193,14 +193,45 @@ def test_split_tf32x2(cuda_device):
     assert float(hi[:, 5:, :].abs().sum() + hi[:, :, 7:].abs().sum()) == 0.0
 
 
+def test_split_f16x2_rowscale(cuda_device):
+    """Rows of very different magnitudes: each scaled by a power of two into
+    [2^13, 2^14) and split into two f16 halves that restore it to ~2^-22."""
+    from sumpy_b200 import _capi
+    g = torch.Generator(device="cpu").manual_seed(3)
+    mags = 10.0 ** torch.linspace(-30, 30, 3 * 6, dtype=torch.float64).reshape(3, 6, 1)
+    x = (torch.randn(3, 6, 7, dtype=torch.float64, generator=g) * mags).to(cuda_device)
+    x[1, 2] = 0.0
+    hi = torch.empty(3, 8, 64, dtype=torch.float16, device=cuda_device)
+    lo = torch.empty_like(hi)
+    inv = torch.empty(3, 8, dtype=torch.float32, device=cuda_device)
+    _capi.call("sumpy_split_f16x2_rowscale", _capi.i64(3), _capi.i32(6), _capi.i32(7),
+               _capi.dptr(x), _capi.i32(8), _capi.i32(64), _capi.dptr(hi), _capi.dptr(lo),
+               _capi.dptr(inv), _capi.stream_ptr())
+    torch.cuda.synchronize()
+    mant, _ = torch.frexp(inv)
+    assert bool((mant == 0.5).all())                               # powers of two
+    rec = (hi[:, :6, :7].double() + lo[:, :6, :7].double()) * inv[:, :6, None].double()
+    rowmax = x.abs().amax(dim=2, keepdim=True).clamp_min(1e-300)
+    assert float(((rec - x).abs() / rowmax).max()) < 2.0 ** -21
+    scaled = hi[:, :6, :7].double().abs().amax(dim=2)
+    nz = x.abs().amax(dim=2) > 0
+    assert bool(((scaled[nz] >= 2.0 ** 13 * (1 - 2 ** -10)) & (scaled[nz] <= 2.0 ** 14)).all())
+    assert float(inv[1, 2]) == 1.0 and float(hi[1, 2].abs().sum()) == 0.0
+    assert float(hi[:, 6:].abs().sum() + hi[:, :, 7:].abs().sum()) == 0.0
+    assert bool((inv[:, 6:] == 1.0).all())
+
+
+@pytest.mark.parametrize("fmt", ["f16", "tf32"])
 @pytest.mark.parametrize("geom", list(GEOMS))
 @pytest.mark.parametrize("order", [4, 10])
-def test_tensor_core_m2l_matches_fp64(cuda_device, geom, order):
-    """3xTF32 tcgen05 M2L against the FP64 GEMM on the same multipoles."""
+def test_tensor_core_m2l_matches_fp64(cuda_device, geom, order, fmt):
+    """3xF16 (row-scaled) and 3xTF32 tcgen05 M2L against the FP64 GEMM on the
+    same multipoles."""
     src, tgt, tree, trav, tcls, q = _setup(geom)
     excl = tgt is None
     w64 = make_wrangler(tree, trav, order, exclude_self=excl)
     wtc = make_wrangler(tree, trav, order, exclude_self=excl, precision="mixed")
+    wtc.tc_format = fmt
     qd = w64.reorder_sources(torch.as_tensor(q, device=cuda_device))
     mp = w64.form_multipoles(None, trav.level_start_source_box_nrs, trav.source_boxes, [qd])
     mp = w64.coarsen_multipoles(None, trav.level_start_source_parent_box_nrs,
@@ -226,9 +257,33 @@ def test_mixed_fmm_matches_fp64_fmm(cuda_device):
     assert relerr(pmx, p64) < 1e-6
 
 
+def test_tensor_core_m2l_scale_invariant(cuda_device):
+    """Strengths scaled by 1e-30 and 1e30: the row-scaled f16 M2L keeps the
+    same relative accuracy (no f16 underflow or overflow)."""
+    src, tgt, tree, trav, tcls, q = _setup("sphere_plummer_self")
+    w64 = make_wrangler(tree, trav, 8, exclude_self=True)
+    wtc = make_wrangler(tree, trav, 8, exclude_self=True, precision="mixed")
+    errs = []
+    for f in (1e-30, 1.0, 1e30):
+        qd = w64.reorder_sources(torch.as_tensor(q * f, device=cuda_device))
+        mp = w64.form_multipoles(None, trav.level_start_source_box_nrs, trav.source_boxes,
+                                 [qd])
+        mp = w64.coarsen_multipoles(None, trav.level_start_source_parent_box_nrs,
+                                    trav.source_parent_boxes, mp)
+        args = (None, trav.level_start_target_or_target_parent_box_nrs,
+                trav.target_or_target_parent_boxes, trav.from_sep_siblings_starts,
+                trav.from_sep_siblings_lists, mp)
+        l64 = w64.multipole_to_local(*args)
+        ltc = wtc.multipole_to_local(*args)
+        wtc.check_status()
+        errs.append(relerr(ltc.cpu(), l64.cpu()))
+    assert max(errs) < 2e-6 and max(errs) < 1.5 * errs[1] + 1e-9, errs
+
+
+@pytest.mark.parametrize("fmt", ["f16", "tf32"])
 @pytest.mark.parametrize("geom", list(GEOMS))
 @pytest.mark.parametrize("order", [4, 10])
-def test_tensor_core_m2m_l2l_match_fp64(cuda_device, geom, order):
+def test_tensor_core_m2m_l2l_match_fp64(cuda_device, geom, order, fmt):
     """Mixed form with the tensor-core octant maps switched on: M2M and L2L
     as per-octant 3xTF32 GEMMs against the FP64 form on the same inputs."""
     src, tgt, tree, trav, tcls, q = _setup(geom)
@@ -237,6 +292,7 @@ def test_tensor_core_m2m_l2l_match_fp64(cuda_device, geom, order):
     wtc = make_wrangler(tree, trav, order, exclude_self=excl, precision="mixed")
     assert wtc._tc_translations
     wtc.tc_m2m = wtc.tc_l2l = True
+    wtc.tc_format = fmt
     qd = w64.reorder_sources(torch.as_tensor(q, device=cuda_device))
     mp = w64.form_multipoles(None, trav.level_start_source_box_nrs, trav.source_boxes, [qd])
     m64 = w64.coarsen_multipoles(None, trav.level_start_source_parent_box_nrs,

@@ -67,7 +67,8 @@ def _level_inputs(w, trav, mp, lev, tile=M2L_TILE_TC):
     it_tile, it_g0, it_g1 = w._tc_items([(int(tgs[i]), int(tgs[i + 1]))
                                          for i in range(plan["ntiles"])])
     mats, mscale = w._m2l_matrices(lev)
-    hi, lo, rp, kp = w._m2l_tc_operands(mats)
+    w.tc_format = "tf32"      # the no-alloc entry point takes TF32 planes
+    hi, lo, rp, kp, _ = w._m2l_tc_operands(mats)
     sbase, sview = w.multipole_expansions_view(mp, lev)
     tbase, tview = w.local_expansions_view(w.local_expansion_zeros(), lev)
     items = [torch.as_tensor(x).to(dev) for x in (it_tile, it_g0, it_g1)]
