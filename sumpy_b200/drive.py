@@ -99,6 +99,7 @@ def _drive_eager(actx, wrangler, src_weight_vecs):
         actx, trav.level_start_source_box_nrs, trav.source_boxes, src_weight_vecs)
     mpole_exps = wrangler.coarsen_multipoles(
         actx, trav.level_start_source_parent_box_nrs, trav.source_parent_boxes, mpole_exps)
+    wrangler.communicate_mpoles(actx, mpole_exps)
 
     potentials = wrangler.eval_direct(
         actx, trav.target_boxes, trav.neighbor_source_boxes_starts,
@@ -163,6 +164,7 @@ def _drive_concurrent(actx, wrangler, trav, src_weight_vecs, crit, side):
         mpole_exps = wrangler.coarsen_multipoles(
             actx, trav.level_start_source_parent_box_nrs, trav.source_parent_boxes,
             mpole_exps)
+        wrangler.communicate_mpoles(actx, mpole_exps)
     with torch.cuda.stream(side):
         potentials = wrangler.eval_direct(
             actx, trav.target_boxes, trav.neighbor_source_boxes_starts,

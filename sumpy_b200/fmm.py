@@ -489,6 +489,12 @@ class SumpyExpansionWrangler:
     def gather_potential_results(self, potentials, tgt_idx_all_ranks=None):
         return potentials
 
+    def communicate_mpoles(self, actx, mpole_exps, return_stats=False):
+        """Exchange of the upward pass's multipoles between ranks (boxtree's
+        distributed hook, called by drive_fmm after coarsen_multipoles);
+        nothing to exchange on one rank."""
+        return None
+
     def finalize_potentials(self, actx, potentials):
         return potentials
 

@@ -438,6 +438,9 @@ class TranslationClassesBuilder:
     def __call__(self, actx, trav, tree, is_translation_per_level=True):
         if not is_translation_per_level:
             raise NotImplementedError("translation classes are built per level")
-        return tree._translation_classes, None
+        # a traversal restricted to part of the tree (sumpy_b200.distributed)
+        # carries the classes of its own List-2 entries
+        own = getattr(trav, "_translation_classes", None)
+        return (own if own is not None else tree._translation_classes), None
 
 # }}}
