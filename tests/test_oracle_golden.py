@@ -1,6 +1,6 @@
 """The FP64 oracle against golden vectors produced by sumpy's own expansion
 code (tests/golden/make_golden.py): P2M, P2L, L2P, M2P, M2M, L2L and M2L at
-orders 2-5, plus the coefficient orderings."""
+every order the file holds (2-6), plus the coefficient orderings."""
 import json
 import os
 
