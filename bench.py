@@ -612,7 +612,8 @@ def headline(args, dev, rank, world, local_rank, budget, cpu_line, cpu_why):
             "npoints": args.npoints, "order": args.order,
             "max_particles_in_box": MAX_PARTICLES, "exclude_self": True,
             "precision": "mixed (FP32 near field, M2P, P2L with FP64 offsets and sums; "
-                         "3xTF32 tensor-core M2L; FP64 elsewhere)",
+                         "tensor-core M2L with row-scaled split-f16 operands (3 products, "
+                         "FP32 sums per class group, FP64 across groups); FP64 elsewhere)",
             "accuracy_target": (f"relL2 <= 1e-6 reached at p = {at['order']}, leaf "
                                 f"{ACCURACY_MAX_PARTICLES} (accuracy_target)") if at else None,
             "l2": "flushed between steps (256 MB write outside the timed events)",
