@@ -106,7 +106,7 @@ def parse():
     ap.add_argument("--extras", action="store_true",
                     help="after the headline, run the other workloads (one JSON line each)")
     ap.add_argument("--only", choices=["mixed", "fp64", "batch", "helmholtz", "uniform",
-                                       "matrix", "adjoint", "qbx"],
+                                       "matrix", "adjoint", "qbx", "m2l_mixed", "m2l_fp64"],
                     help="run one workload alone (--steps/--warmup apply) and print its result; "
                          "for profiling")
     ap.add_argument("--eager", action="store_true",
@@ -710,6 +710,8 @@ def run_only(args, dev):
                  else (args.helmholtz_precision,))
         return helmholtz_bench(dev, steps=args.steps, warmup=args.warmup,
                                npoints=args.helmholtz_npoints, precisions=precs)
+    if args.only in ("m2l_mixed", "m2l_fp64"):
+        return m2l_alone(args, dev, args.only[4:])
     pts, q, tree, trav, tcls, ti, t_tree = laplace_setup(dev, args.npoints, MAX_PARTICLES)
     w = make_wrangler(ti, trav, tcls, args.order, args.only, dev, graph=not args.eager)
     q_dev = torch.as_tensor(q, device=dev)
@@ -718,6 +720,44 @@ def run_only(args, dev):
     ms, _ = StepTimer(dev, 1)(lambda: drive_fmm(None, w, [q_dev]), args.steps)
     w.check_status()
     return {"ms_per_step": ms, "Mpts_s": args.npoints / (ms * 1e-3) / 1e6}
+
+
+def m2l_alone(args, dev, precision):
+    """The headline workload's M2L (all levels) alone, for profiling: one
+    full FMM for the multipoles, W untimed and K timed ``multipole_to_local``
+    calls (CUDA events), the last of them inside the NVTX range "m2l"."""
+    import torch
+    from sumpy_b200 import drive_fmm
+    pts, q, tree, trav, tcls, ti, _ = laplace_setup(dev, args.npoints, MAX_PARTICLES)
+    w = make_wrangler(ti, trav, tcls, args.order, precision, dev, graph=False)
+    qd = torch.as_tensor(q, device=dev)
+    drive_fmm(None, w, [qd])
+    qs = w.reorder_sources(qd)
+    mp = w.coarsen_multipoles(
+        None, trav.level_start_source_parent_box_nrs, trav.source_parent_boxes,
+        w.form_multipoles(None, trav.level_start_source_box_nrs, trav.source_boxes, [qs]))
+    m2l_args = (None, trav.level_start_target_or_target_parent_box_nrs,
+                trav.target_or_target_parent_boxes, trav.from_sep_siblings_starts,
+                trav.from_sep_siblings_lists, mp)
+    for _ in range(max(1, args.warmup)):
+        w.multipole_to_local(*m2l_args)
+    torch.cuda.synchronize()
+    times = []
+    for i in range(max(1, args.steps)):
+        last = i == max(1, args.steps) - 1
+        if last:
+            torch.cuda.nvtx.range_push("m2l")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        w.multipole_to_local(*m2l_args)
+        e1.record()
+        if last:
+            torch.cuda.nvtx.range_pop()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    w.check_status()
+    return {"precision": precision, "m2l_ms": sorted(times)[len(times) // 2],
+            "entries": int(len(trav.from_sep_siblings_lists))}
 
 
 def fp64_best_tree_bench(dev, args):
