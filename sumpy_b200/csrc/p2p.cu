@@ -133,6 +133,9 @@ p2p_csr_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_boxes,
 // added into FP64.
 constexpr int P2PF_WARPS = 8;
 constexpr float P2PF_FAR = 1e18f;
+#ifndef SUMPY_P2PF_MINB
+#define SUMPY_P2PF_MINB 3   // CTAs per SM the value kernel is built for (register cap 85)
+#endif
 
 __device__ __forceinline__ void split_hl(double v, float &hi, float &lo)
 {
@@ -216,8 +219,50 @@ __device__ __forceinline__ void p2p_batch_packed(const float4 *__restrict__ P0,
     acc += a2.x + a2.y;
 }
 
+// The same for two targets per lane: each source pair is read from shared
+// memory once and used for both targets (half the shared loads per pair).
+__device__ __forceinline__ void p2p_batch_packed2(const float4 *__restrict__ P0,
+                                                  const float4 *__restrict__ P1,
+                                                  const float4 *__restrict__ P2,
+                                                  const float4 *__restrict__ P3,
+                                                  const P2PTarget &t, const P2PTarget &u,
+                                                  float &acc, float &acc2)
+{
+    const float2 txh = make_float2(t.xh, t.xh), txl = make_float2(t.xl, t.xl);
+    const float2 tyh = make_float2(t.yh, t.yh), tyl = make_float2(t.yl, t.yl);
+    const float2 tzh = make_float2(t.zh, t.zh), tzl = make_float2(t.zl, t.zl);
+    const float2 uxh = make_float2(u.xh, u.xh), uxl = make_float2(u.xl, u.xl);
+    const float2 uyh = make_float2(u.yh, u.yh), uyl = make_float2(u.yl, u.yl);
+    const float2 uzh = make_float2(u.zh, u.zh), uzl = make_float2(u.zl, u.zl);
+    float2 a2 = make_float2(0.f, 0.f), b2 = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const float4 p0 = P0[m], p1 = P1[m], p2 = P2[m], p3 = P3[m];
+        const float2 sxh = make_float2(p0.x, p0.y), syh = make_float2(p0.z, p0.w);
+        const float2 szh = make_float2(p1.x, p1.y), q = make_float2(p1.z, p1.w);
+        const float2 sxl = make_float2(p2.x, p2.y), syl = make_float2(p2.z, p2.w);
+        const float2 szl = make_float2(p3.x, p3.y);
+        {
+            const float2 dx = __fadd2_rn(__fadd2_rn(txh, sxh), __fadd2_rn(txl, sxl));
+            const float2 dy = __fadd2_rn(__fadd2_rn(tyh, syh), __fadd2_rn(tyl, syl));
+            const float2 dz = __fadd2_rn(__fadd2_rn(tzh, szh), __fadd2_rn(tzl, szl));
+            const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+            a2 = __ffma2_rn(q, make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y)), a2);
+        }
+        {
+            const float2 dx = __fadd2_rn(__fadd2_rn(uxh, sxh), __fadd2_rn(uxl, sxl));
+            const float2 dy = __fadd2_rn(__fadd2_rn(uyh, syh), __fadd2_rn(uyl, syl));
+            const float2 dz = __fadd2_rn(__fadd2_rn(uzh, szh), __fadd2_rn(uzl, szl));
+            const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+            b2 = __ffma2_rn(q, make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y)), b2);
+        }
+    }
+    acc += a2.x + a2.y;
+    acc2 += b2.x + b2.y;
+}
+
 template <bool GRAD>
-__global__ void __launch_bounds__(32 * P2PF_WARPS, 4)
+__global__ void __launch_bounds__(32 * P2PF_WARPS, GRAD ? 4 : SUMPY_P2PF_MINB)
 p2p_flat_mixed_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_boxes,
                       const int32_t *__restrict__ src_box_starts,
                       const int32_t *__restrict__ src_box_lists,
@@ -242,7 +287,10 @@ p2p_flat_mixed_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_box
     const int32_t t0 = box_tgt_starts[tb], nt = box_tgt_counts[tb];
     const int32_t ls = src_box_starts[ib], le = src_box_starts[ib + 1];
 
-    for (int32_t tc = 0; tc < nt; tc += 32) {
+    // more than 32 targets left: a pass of up to 64, two targets per lane
+    // (lane l: targets tc + l and tc + 32 + l) sharing each staged source
+    for (int32_t tc = 0; tc < nt;) {
+        const bool two = !GRAD && nt - tc > 32;
         const int ntc = min(32, nt - tc);
         const int nph = 32 / ntc;
         const int tl = lane % ntc, ph = lane / ntc;
@@ -256,7 +304,18 @@ p2p_flat_mixed_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_box
             split_hl(targets[2 * tstride + t], tg.zh, tg.zl);
             if (target_to_source) self = target_to_source[t];
         }
-        double acc = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+        // the second target of this lane (far away when the pass has none)
+        const bool active2 = two && tc + 32 + lane < nt;
+        const int32_t t2 = t0 + tc + 32 + lane;
+        P2PTarget tg2 = {P2PF_FAR, 0.f, P2PF_FAR, 0.f, P2PF_FAR, 0.f};
+        int32_t self2 = -1;
+        if (active2) {
+            split_hl(targets[t2], tg2.xh, tg2.xl);
+            split_hl(targets[tstride + t2], tg2.yh, tg2.yl);
+            split_hl(targets[2 * tstride + t2], tg2.zh, tg2.zl);
+            if (target_to_source) self2 = target_to_source[t2];
+        }
+        double acc = 0.0, acc2 = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
         for (int32_t w0 = ls; w0 < le; w0 += 32) {
             // one window of up to 32 list entries: lane k holds entry k's
             // source range; inclusive prefix sum of the counts
@@ -275,13 +334,14 @@ p2p_flat_mixed_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_box
             }
             const int32_t S = __shfl_sync(FULL, cum, 31);
             // flat position of this lane's own source in the window, if any
-            int32_t fself = -1;
+            int32_t fself = -1, fself2 = -1;
             if (target_to_source) {
                 for (int k = 0; k < nw; ++k) {
                     const int32_t b0 = __shfl_sync(FULL, bs0, k);
                     const int32_t n = __shfl_sync(FULL, bn, k);
                     const int32_t c = __shfl_sync(FULL, cum, k);
                     if (self >= b0 && self < b0 + n) fself = c - n + (self - b0);
+                    if (self2 >= b0 && self2 < b0 + n) fself2 = c - n + (self2 - b0);
                 }
             }
             // source of flat index f (f < S): entry k = #lanes with cum <= f
@@ -341,8 +401,27 @@ p2p_flat_mixed_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_box
                 }
                 __syncwarp();
                 const int jself = fself - 32 * bt;   // outside [0, 32) if not in this batch
+                const int jself2 = fself2 - 32 * bt;
                 const bool check = __any_sync(FULL, active && jself >= 0 && jself < 32);
-                if (active) {
+                const bool check2 = two &&
+                                    __any_sync(FULL, active2 && jself2 >= 0 && jself2 < 32);
+                if (two) {
+                    // every lane holds a first target (ntc = 32, one phase)
+                    float a = 0.f, a2 = 0.f, dx_ = 0.f, dy_ = 0.f, dz_ = 0.f;
+                    const float4 *H = shi[warp][slot], *L = slo[warp][slot];
+                    if (check || check2) {
+                        // (rare) batches holding a lane's own source: one target at a
+                        // time, the compact loop
+                        p2p_batch<true, false, 0>(H, L, tg, 0, 1, jself, a, dx_, dy_, dz_);
+                        p2p_batch<true, false, 0>(H, L, tg2, 0, 1, jself2, a2, dx_, dy_, dz_);
+                    } else {
+                        p2p_batch_packed2(spk[warp][slot][0], spk[warp][slot][1],
+                                          spk[warp][slot][2], spk[warp][slot][3], tg, tg2, a,
+                                          a2);
+                    }
+                    acc += (double)a;
+                    acc2 += (double)a2;
+                } else if (active) {
                     float a = 0.f, ax = 0.f, ay = 0.f, az = 0.f;
                     const float4 *H = shi[warp][slot], *L = slo[warp][slot];
                     if (nph == 1) {
@@ -365,6 +444,7 @@ p2p_flat_mixed_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_box
             }
             __syncwarp();   // the next window restages slot 0
         }
+        if (active2) result[t2] = scale * acc2;
         // sum the phases (lanes tl, tl + ntc, ...) through shared memory
         red[warp][0][lane] = acc;
         if (GRAD) { red[warp][1][lane] = gx; red[warp][2][lane] = gy; red[warp][3][lane] = gz; }
@@ -387,6 +467,7 @@ p2p_flat_mixed_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_box
             }
         }
         __syncwarp();
+        tc += two ? 64 : 32;
     }
 }
 
