@@ -60,6 +60,14 @@ int sumpy_tree_array_copy(void *handle, const char *name, void *dst, int64_t cap
 
 void sumpy_tree_free(void *handle);
 
+/* Next-fit packing of n sizes (in the given order) into items of total size
+ * <= capacity and at most max_count entries each: item i holds entries
+ * [item_first[i], item_first[i] + item_count[i]). The item arrays need room for
+ * n entries; *nitems_out receives their number. Used to pack the partial
+ * 32-target slots of the one-launch L2P (sumpy_e2p_from_single_box_packed_f64). */
+int sumpy_pack_next_fit(int64_t n, const int32_t *sizes, int32_t capacity, int32_t max_count,
+                        int32_t *item_first, int32_t *item_count, int64_t *nitems_out);
+
 /* Message of the last failed call on this thread. */
 const char *sumpy_tree_last_error(void);
 

@@ -48,10 +48,14 @@ class BatchedLaplaceFMM:
     def __init__(self, sources, targets=None, order=8, max_particles_in_box=32,
                  precision="mixed", bbox=None, device="cuda", use_graph=True,
                  autotune=False, m2l_item_groups=None, autotune_cache=None, gpu_tree=True):
+        import time
         self.device = torch.device(device)
+        t0 = time.perf_counter()
         tree, trav, tcls, forest = build_forest(
             sources, targets, max_particles_in_box, bbox,
             device=self.device if gpu_tree and self.device.type == "cuda" else None)
+        # wall times of the set-up steps (seconds)
+        self.timings = {"forest_s": time.perf_counter() - t0}
         self.tree, self.traversal, self.forest = tree, trav, forest
         knl = LaplaceKernel(3)
         exclude_self = targets is None
@@ -70,8 +74,10 @@ class BatchedLaplaceFMM:
         self.schedule = self.wrangler.schedule()
         if autotune:
             from sumpy_b200.autotune import tune_schedule
+            t0 = time.perf_counter()
             self.schedule = tune_schedule(self.wrangler, lambda: self._eager(self._w),
                                           path=autotune_cache)
+            self.timings["autotune_s"] = time.perf_counter() - t0
 
     @property
     def nsources(self):

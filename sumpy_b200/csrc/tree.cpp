@@ -640,4 +640,35 @@ int sumpy_tree_array_copy(void *handle, const char *name, void *dst, int64_t cap
 
 void sumpy_tree_free(void *handle) { delete static_cast<TreeState *>(handle); }
 
+int sumpy_pack_next_fit(int64_t n, const int32_t *sizes, int32_t capacity, int32_t max_count,
+                        int32_t *item_first, int32_t *item_count, int64_t *nitems_out)
+{
+    if (n < 0 || capacity < 1 || max_count < 1 || !nitems_out || (n > 0 && !sizes) ||
+        (n > 0 && (!item_first || !item_count))) {
+        g_last_error = "pack_next_fit: bad arguments";
+        return 1;
+    }
+    int64_t ni = 0, first = 0, cnt = 0, tot = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        const int64_t r = sizes[i];
+        if (cnt && (tot + r > capacity || cnt == max_count)) {
+            item_first[ni] = (int32_t)first;
+            item_count[ni] = (int32_t)cnt;
+            ++ni;
+            first = i;
+            cnt = 0;
+            tot = 0;
+        }
+        ++cnt;
+        tot += r;
+    }
+    if (cnt) {
+        item_first[ni] = (int32_t)first;
+        item_count[ni] = (int32_t)cnt;
+        ++ni;
+    }
+    *nitems_out = ni;
+    return 0;
+}
+
 }  // extern "C"

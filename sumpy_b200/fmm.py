@@ -146,18 +146,33 @@ def l2p_items(tree, level_starts, target_boxes, max_slots=L2P_ITEM_SLOTS):
     rb = rb[np.argsort(-rem[rb], kind="stable")]
     part = np.stack([tb[rb], bts[tb][rb] + 32 * nfull[rb], rem[rb], lev[rb]], axis=1)
     slots = np.concatenate([full.reshape(-1, 4), part.reshape(-1, 4)]).astype(np.int32)
-    items = [(i, 1) for i in range(len(full))]
-    first, cnt, tot = len(full), 0, 0
-    for i, r in enumerate(part[:, 2], start=len(full)):
-        if cnt and (tot + r > 32 or cnt == max_slots):
-            items.append((first, cnt))
-            first, cnt, tot = i, 0, 0
-        cnt += 1
-        tot += int(r)
-    if cnt:
-        items.append((first, cnt))
-    return (np.ascontiguousarray(np.array(items, dtype=np.int32).reshape(-1, 2)),
+    first, cnt = _pack_next_fit(part[:, 2].astype(np.int32), 32, max_slots)
+    items = np.concatenate([
+        np.stack([np.arange(len(full)), np.ones(len(full), dtype=np.int64)], axis=1),
+        np.stack([first.astype(np.int64) + len(full), cnt.astype(np.int64)], axis=1)])
+    return (np.ascontiguousarray(items.reshape(-1, 2), dtype=np.int32),
             np.ascontiguousarray(slots))
+
+
+def _pack_next_fit(sizes, capacity, max_count):
+    """Next-fit packing (host library sumpy_pack_next_fit): (first, count)
+    of each item, entries in the given order."""
+    import ctypes
+
+    from sumpy_b200._lib import load_tree_library
+    lib = load_tree_library()
+    n = len(sizes)
+    sizes = np.ascontiguousarray(sizes, dtype=np.int32)
+    first = np.empty(max(n, 1), dtype=np.int32)
+    cnt = np.empty(max(n, 1), dtype=np.int32)
+    ni = ctypes.c_int64(0)
+    rc = lib.sumpy_pack_next_fit(
+        ctypes.c_int64(n), sizes.ctypes.data_as(ctypes.c_void_p), ctypes.c_int32(capacity),
+        ctypes.c_int32(max_count), first.ctypes.data_as(ctypes.c_void_p),
+        cnt.ctypes.data_as(ctypes.c_void_p), ctypes.byref(ni))
+    if rc:
+        raise RuntimeError(lib.sumpy_tree_last_error().decode())
+    return first[:ni.value], cnt[:ni.value]
 
 
 def p2l_items(tree, level_starts, target_boxes, starts, lists, rounds=ITEM_ROUNDS):
@@ -584,20 +599,25 @@ class SumpyExpansionWrangler:
         and the longest start first. Results are per target, so the order
         does not change them."""
         def build():
-            tb = np.asarray(target_boxes, dtype=np.int64)
-            st = np.asarray(starts, dtype=np.int64)
-            ls = np.asarray(lists, dtype=np.int64)
-            cnt = np.diff(st)
-            bsc = np.asarray(self.tree.box_source_counts_nonchild, dtype=np.int64)
-            csum = np.concatenate([[0], np.cumsum(bsc[ls])])
-            pairs = np.asarray(self.tree.box_target_counts_nonchild, dtype=np.int64)[tb] * \
-                (csum[st[1:]] - csum[st[:-1]])
-            order = np.argsort(-pairs, kind="stable")
+            # on the device (the forest's lists are long)
+            dev, i64 = self.device, torch.int64
+            tb = torch.as_tensor(np.asarray(target_boxes, dtype=np.int64), device=dev)
+            st = torch.as_tensor(np.asarray(starts, dtype=np.int64), device=dev)
+            ls = torch.as_tensor(np.asarray(lists, dtype=np.int64), device=dev)
+            nent = len(lists)
+            cnt = st[1:] - st[:-1]
+            bsc = self._dev(self.tree.box_source_counts_nonchild, i64)
+            btc = self._dev(self.tree.box_target_counts_nonchild, i64)
+            csum = torch.cat([torch.zeros(1, dtype=i64, device=dev), torch.cumsum(bsc[ls], 0)])
+            pairs = btc[tb] * (csum[st[1:]] - csum[st[:-1]])
+            order = torch.sort(-pairs, stable=True).indices
             ncnt = cnt[order]
-            nst = np.concatenate([[0], np.cumsum(ncnt)])
-            nls = ls[_expand_ranges(st[:-1][order], ncnt)]
-            return tuple(torch.as_tensor(a.astype(np.int32)).to(self.device)
-                         for a in (tb[order], nst, nls))
+            nst = torch.cat([torch.zeros(1, dtype=i64, device=dev), torch.cumsum(ncnt, 0)])
+            # entries of each reordered row: its old start plus 0 .. count - 1
+            row = torch.repeat_interleave(torch.arange(len(ncnt), device=dev), ncnt,
+                                          output_size=nent)
+            ent = st[:-1][order][row] + torch.arange(nent, device=dev) - nst[:-1][row]
+            return tuple(a.to(torch.int32) for a in (tb[order], nst, ls[ent]))
         return self._cached_items(("p2p_sorted", id(lists)), (target_boxes, starts, lists),
                                   build)
 
@@ -699,8 +719,10 @@ class SumpyExpansionWrangler:
         tile_targets[:nt] = tb[tpos].to(torch.int32)
         rank = torch.empty(tb.numel(), dtype=i64, device=dev)
         rank[tpos] = torch.arange(nt, dtype=i64, device=dev)
-        ent_tgt = torch.repeat_interleave(torch.arange(tb.numel(), device=dev), counts)
         e0, e1 = int(starts_h[0]), int(starts_h[-1])
+        # (the output size is known on the host: no device round trip)
+        ent_tgt = torch.repeat_interleave(torch.arange(tb.numel(), device=dev), counts,
+                                          output_size=e1 - e0)
         ent_src = self._dev(lists, torch.int32)[e0:e1]
         ent_cls = self._dev(tc.from_sep_siblings_translation_classes, i64)[e0:e1] - c0
         if ent_cls.numel() and bool((ent_cls.min() < 0) | (ent_cls.max() >= ncls)):
@@ -1018,15 +1040,15 @@ class SumpyExpansionWrangler:
         tile_targets[:nt] = targets
         src = np.full((8, ntiles * tw), -1, dtype=np.int32)
         src[:, :nt] = sources
-        groups, classes, tiles = [], [], []
-        for t in range(ntiles):
-            g0 = len(groups)
-            blk = src[:, t * tw:(t + 1) * tw]
-            for o in range(8):
-                if (blk[o] >= 0).any():
-                    groups.append(blk[o])
-                    classes.append(o)
-            tiles.append((g0, len(groups)))
+        # one group per (tile, octant) with a source, tile-major
+        blk = src.reshape(8, ntiles, tw)
+        present = (blk >= 0).any(axis=2)                        # [8, ntiles]
+        tile_of, oct_of = np.nonzero(present.T)                 # tile-major order
+        groups = blk[oct_of, tile_of]                           # [ngroups, tw]
+        classes = oct_of.astype(np.int32)
+        gcount = present.sum(axis=0)
+        gend = np.cumsum(gcount)
+        tiles = list(zip((gend - gcount).tolist(), gend.tolist()))
         # a level's octant GEMM is on the level-serial M2M / L2L chain: cut
         # it into enough items (CTAs) to cover the GPU twice, down to one
         # octant group per item, so few tiles do not leave one CTA pipelining
@@ -1041,10 +1063,9 @@ class SumpyExpansionWrangler:
             "item_g1": torch.as_tensor(it_g1).to(dev),
             "tile_targets": torch.as_tensor(tile_targets).to(dev),
             "tile_scale": torch.ones(ntiles, dtype=torch.float64, device=dev),
-            "group_class": torch.as_tensor(np.array(classes, dtype=np.int32)).to(dev),
+            "group_class": torch.as_tensor(classes).to(dev),
             "group_sources": torch.as_tensor(
-                np.stack(groups).astype(np.int32).ravel() if groups
-                else np.zeros(0, dtype=np.int32)).to(dev),
+                np.ascontiguousarray(groups, dtype=np.int32).ravel()).to(dev),
         }
         self._m2l_plans[key] = plan
         return plan
