@@ -554,9 +554,12 @@ m2l_tc_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
                         // scale first): exact whenever the contribution lies
                         // in the FP32 normal range, the range the mixed form's
                         // FP32 near field needs anyway
+                        // (an empty slot's scale is 0, the same in every lane
+                        // of the warp: the whole warp skips that column)
                         const int col = c0 + j;
                         const float cs = __shfl_sync(0xffffffffu, col < 32 ? cs0 : cs1, col & 31);
-                        acc64[col] += (double)((__uint_as_float(r[j]) * cs) * rs);
+                        if (cs != 0.0f)
+                            acc64[col] += (double)((__uint_as_float(r[j]) * cs) * rs);
                     } else {
                         acc64[c0 + j] += (double)__uint_as_float(r[j]);
                     }
