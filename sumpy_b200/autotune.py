@@ -17,7 +17,8 @@ schedule of an evaluation has knobs whose best values depend on the workload
 
 The tile shapes of the kernels are fixed by their instruction shapes (the
 tensor-core M2L tile is the MMA's N = 128 target boxes by M = 128
-coefficient rows, K streamed 32 at a time; smaller K steps and a TMA gather
+coefficient rows, K streamed in 128-byte rows, 64 f16 or 32 TF32 values at a
+time; smaller K steps and a TMA gather
 loader were measured slower) and are not searched.
 
 :func:`tune` times each candidate of one knob with CUDA events on the
