@@ -49,15 +49,85 @@ __host__ __device__ constexpr int p2m_warps()
                                                                                             : 2;
 }
 
-// P2M with one warp per box and the full coefficients in registers: lane u
-// owns the (i, j) pairs u, u + 32, ... (i + j <= P) and accumulates the
-// column k = 0..P-i-j of each, so a (source, coefficient) term costs one
-// FMA with a broadcast power w2[k]; per source t = q w0[i] w1[j] is formed
-// once per pair. Sources go 32 at a time, one per lane for the power
-// tables (a/r)^k / k!. The columns are then written to a per-warp compact
-// full-index buffer, compressed by the p-1 plane sweeps (warp-synchronous)
-// and stored. Same arithmetic as p2m_kernel (multipole.py:77-114 and the
-// transposed projection), ordered differently.
+// The P2M kernel's transposed projection as tables, per order P: for the
+// planes i = P..2 in turn, the entries F[i-2, J, K] -= F[i, J-2, K] +
+// F[i, J, K-2] (J + K <= P - i + 2) as full-index triples {dst, a, b, 0}
+// (-1: term absent), and the full index of each stored coefficient.
+__host__ __device__ constexpr int full_index_c(int i, int j, int k)
+{
+    return (i + j + k) * (i + j + k + 1) * (i + j + k + 2) / 6 + i * (i + j + k + 1) -
+           i * (i - 1) / 2 + j;
+}
+
+template <int P>
+struct P2mSweep {
+    static constexpr int ne()
+    {
+        int n = 0;
+        for (int i = P; i >= 2; --i) n += (P - i + 3) * (P - i + 4) / 2;
+        return n;
+    }
+    static constexpr int NE = ne() > 0 ? ne() : 1;
+    int e[4 * NE];
+    int start[P + 2];
+    int stored[(P + 1) * (P + 1)];
+    constexpr P2mSweep() : e(), start(), stored()
+    {
+        int n = 0, pl = 0;
+        for (int i = P; i >= 2; --i, ++pl) {
+            start[pl] = n;
+            const int m = P - i + 2;
+            for (int J = 0; J <= m; ++J)
+                for (int K = 0; J + K <= m; ++K) {
+                    e[4 * n] = full_index_c(i - 2, J, K);
+                    e[4 * n + 1] = J >= 2 ? full_index_c(i, J - 2, K) : -1;
+                    e[4 * n + 2] = K >= 2 ? full_index_c(i, J, K - 2) : -1;
+                    e[4 * n + 3] = 0;
+                    ++n;
+                }
+        }
+        for (; pl < P + 2; ++pl) start[pl] = n;
+        // stored coefficients: degree d = 0..P, (0, j, d - j) for j = 0..d,
+        // then (1, j, d - 1 - j) for j = 0..d-1 (sumpy's order)
+        int s = 0;
+        for (int d = 0; d <= P; ++d) {
+            for (int j = 0; j <= d; ++j) stored[s++] = full_index_c(0, j, d - j);
+            for (int j = 0; j < d; ++j) stored[s++] = full_index_c(1, j, d - 1 - j);
+        }
+    }
+};
+
+template <int P>
+__device__ constexpr P2mSweep<P> p2m_sweep{};
+
+// (i, j) pair t of the P2M kernel, in increasing degree d = i + j (and
+// increasing i within a degree): the pairs of row set u = t / 32 have
+// column lengths P - d + 1 of at most p2m_kmax(u) + 1
+__host__ __device__ constexpr int p2m_pair_degree(int t)
+{
+    int d = 0;
+    while ((d + 1) * (d + 2) / 2 <= t) ++d;
+    return d;
+}
+
+template <int P>
+__host__ __device__ constexpr int p2m_kmax(int u)
+{
+    return P - p2m_pair_degree(32 * u);
+}
+
+// P2M with one warp per box and the full coefficients in registers: lane l
+// owns the (i, j) pairs l, l + 32, ... (pairs in increasing i + j) and
+// accumulates the column k = 0..P-i-j of each, so a (source, coefficient)
+// term costs one FMA with the source's power z[k] = (a_z/r)^k/k!, loaded
+// once per source; per source t = q w0[i] w1[j] is formed once per pair.
+// The pair order bounds the k loop of the second and later row sets at
+// compile time (order 10: 11 + 4 + 1 FMAs per source instead of 3 x 11).
+// Sources go 32 at a time, one per lane for the power tables. The columns
+// are then written to a per-warp compact full-index buffer, compressed by
+// the p-1 plane sweeps (warp-synchronous) and stored. Same arithmetic as
+// p2m_kernel (multipole.py:77-114 and the transposed projection), ordered
+// differently.
 template <int P>
 __global__ void __launch_bounds__(32 * p2m_warps<P>())
 p2m_warp_kernel(double rscale, int32_t nboxes, const int32_t *__restrict__ boxes,
@@ -86,15 +156,15 @@ p2m_warp_kernel(double rscale, int32_t nboxes, const int32_t *__restrict__ boxes
     // all levels in one launch: the box's own level's rscale
     const double rinv = 1.0 / (level_rscale ? level_rscale[box_level[ib]] : rscale);
 
-    // the (i, j) pairs of this lane
-    int pi[NU], pj[NU];
+    // the (i, j) pairs of this lane and their last column
+    int pi[NU], pj[NU], pk[NU];
 #pragma unroll
     for (int u = 0; u < NU; ++u) {
-        int t = lane + 32 * u, i = 0;
-        if (t >= NPAIR) t = 0;  // idle slot, never stored
-        while (t > P - i) { t -= P - i + 1; ++i; }
-        pi[u] = i;
-        pj[u] = t;
+        const int t = lane + 32 * u;
+        const int d = p2m_pair_degree(t < NPAIR ? t : 0);
+        pi[u] = t < NPAIR ? t - d * (d + 1) / 2 : 0;
+        pj[u] = t < NPAIR ? d - pi[u] : 0;
+        pk[u] = t < NPAIR ? P - d : -1;     // -1: idle slot, never accumulated or stored
     }
     double acc[NU][P1];
 #pragma unroll
@@ -114,7 +184,7 @@ p2m_warp_kernel(double rscale, int32_t nboxes, const int32_t *__restrict__ boxes
                 w[warp][d][0][lane] = 1.0;
 #pragma unroll
                 for (int k = 1; k < P1; ++k) {
-                    v = v * a / k;
+                    v = v * a * (1.0 / k);    // a compile-time reciprocal: no division
                     w[warp][d][k][lane] = v;
                 }
             }
@@ -122,13 +192,15 @@ p2m_warp_kernel(double rscale, int32_t nboxes, const int32_t *__restrict__ boxes
         __syncwarp();
         for (int so = 0; so < nsc; ++so) {
             const double qq = qs[warp][so];
+            double z[P1];
+#pragma unroll
+            for (int k = 0; k < P1; ++k) z[k] = w[warp][2][k][so];
 #pragma unroll
             for (int u = 0; u < NU; ++u) {
                 const double t = qq * w[warp][0][pi[u]][so] * w[warp][1][pj[u]][so];
-                const int kmax = P - pi[u] - pj[u];
 #pragma unroll
-                for (int k = 0; k < P1; ++k)
-                    if (k <= kmax) acc[u][k] = fma(t, w[warp][2][k][so], acc[u][k]);
+                for (int k = 0; k <= p2m_kmax<P>(u); ++k)
+                    if (k <= pk[u]) acc[u][k] = fma(t, z[k], acc[u][k]);
             }
         }
         __syncwarp();
@@ -136,34 +208,26 @@ p2m_warp_kernel(double rscale, int32_t nboxes, const int32_t *__restrict__ boxes
     double *F = full[warp];
 #pragma unroll
     for (int u = 0; u < NU; ++u) {
-        if (lane + 32 * u < NPAIR) {
-            const int kmax = P - pi[u] - pj[u];
 #pragma unroll
-            for (int k = 0; k < P1; ++k)
-                if (k <= kmax) F[full_index(pi[u], pj[u], k)] = acc[u][k];
-        }
+        for (int k = 0; k <= p2m_kmax<P>(u); ++k)
+            if (k <= pk[u]) F[full_index(pi[u], pj[u], k)] = acc[u][k];
     }
     __syncwarp();
-    // transposed projection: plane i-2 gathers from plane i, i = P..2
-    for (int i = P; i >= 2; --i) {
-        const int m = P - i + 2;
-        const int npairs = (m + 1) * (m + 2) / 2;
-        for (int t = lane; t < npairs; t += 32) {
-            int J, K;
-            tri_pair(t, m, J, K);
+    // transposed projection: plane i-2 gathers from plane i, i = P..2, by
+    // the precomputed full-index triples of each plane
+    const int4 *sweep = reinterpret_cast<const int4 *>(p2m_sweep<P>.e);
+    for (int pl = 0; pl + 2 <= P; ++pl) {
+        for (int t = p2m_sweep<P>.start[pl] + lane; t < p2m_sweep<P>.start[pl + 1]; t += 32) {
+            const int4 e = __ldg(sweep + t);
             double v = 0.0;
-            if (J >= 2) v += F[full_index(i, J - 2, K)];
-            if (K >= 2) v += F[full_index(i, J, K - 2)];
-            F[full_index(i - 2, J, K)] -= v;
+            if (e.y >= 0) v += F[e.y];
+            if (e.z >= 0) v += F[e.z];
+            F[e.x] -= v;
         }
         __syncwarp();
     }
     double *o = out + (int64_t)(b - base) * N;
-    for (int st = lane; st < N; st += 32) {
-        int i, j, k;
-        stored_mi(st, i, j, k);
-        o[st] = F[full_index(i, j, k)];
-    }
+    for (int st = lane; st < N; st += 32) o[st] = F[__ldg(p2m_sweep<P>.stored + st)];
 }
 
 // }}}
@@ -779,6 +843,49 @@ __host__ __device__ constexpr int l2pk_warps()
     return 8 * L2PK_SLOTS * (P + 1) * (P + 2) * (P + 3) / 6 * 4 <= 200 * 1024 ? 4 : 2;
 }
 
+// The packed L2P's decompression as tables, per order P, in the cube
+// layout of jki_offset: for the planes i = 2..P in turn, the entries
+// c[i, J, K] = -c[i-2, J+2, K] - c[i-2, J, K+2] (J + K <= P - i) as offset
+// triples {dst, a, b, 0}, and the cube offset of each stored coefficient.
+template <int P>
+struct L2pDecomp {
+    static constexpr int ne()
+    {
+        int n = 0;
+        for (int i = 2; i <= P; ++i) n += (P - i + 1) * (P - i + 2) / 2;
+        return n;
+    }
+    static constexpr int NE = ne() > 0 ? ne() : 1;
+    int e[4 * NE];
+    int start[P + 2];
+    int stored[(P + 1) * (P + 1)];
+    constexpr L2pDecomp() : e(), start(), stored()
+    {
+        int n = 0, pl = 0;
+        for (int i = 2; i <= P; ++i, ++pl) {
+            start[pl] = n;
+            const int m = P - i;
+            for (int J = 0; J <= m; ++J)
+                for (int K = 0; J + K <= m; ++K) {
+                    e[4 * n] = jki_offset<P>(J, K) + i;
+                    e[4 * n + 1] = jki_offset<P>(J + 2, K) + i - 2;
+                    e[4 * n + 2] = jki_offset<P>(J, K + 2) + i - 2;
+                    e[4 * n + 3] = 0;
+                    ++n;
+                }
+        }
+        for (; pl < P + 2; ++pl) start[pl] = n;
+        int s = 0;
+        for (int d = 0; d <= P; ++d) {
+            for (int j = 0; j <= d; ++j) stored[s++] = jki_offset<P>(j, d - j);
+            for (int j = 0; j < d; ++j) stored[s++] = jki_offset<P>(j, d - 1 - j) + 1;
+        }
+    }
+};
+
+template <int P>
+__device__ constexpr L2pDecomp<P> l2p_decomp{};
+
 // One warp evaluates up to 32 targets taken from up to L2PK_SLOTS boxes (slots; a
 // box with more than 32 targets spans several items). The slots' locals
 // are decompressed together (p - 1 plane sweeps, sumpy's
@@ -826,23 +933,22 @@ l2p_packed_kernel(int32_t nitems, const int2 *__restrict__ items, const int4 *__
     // stored -> full layout, all slots
     for (int e = lane; e < nsl * N; e += 32) {
         const int q = e / N, st = e - q * N;
-        int i, j, k;
-        stored_mi(st, i, j, k);
         const int32_t b = slots[item.x + q].x;
-        cubes[q * NF + jki_offset<P>(j, k) + i] = loc[(int64_t)b * N + st];
+        cubes[q * NF + __ldg(l2p_decomp<P>.stored + st)] = loc[(int64_t)b * N + st];
     }
     __syncwarp();
-    // decompress: plane i from plane i - 2, i = 2..P (all slots per sweep)
-    for (int i = 2; i <= P; ++i) {
-        const int m = P - i;
-        const int npairs = (m + 1) * (m + 2) / 2;
+    // decompress: plane i from plane i - 2, i = 2..P (all slots per sweep),
+    // by the precomputed offset triples of each plane
+    const int4 *tri = reinterpret_cast<const int4 *>(l2p_decomp<P>.e);
+    for (int pl = 0; pl + 2 <= P; ++pl) {
+        const int e0 = l2p_decomp<P>.start[pl];
+        const int npairs = l2p_decomp<P>.start[pl + 1] - e0;
         for (int e = lane; e < nsl * npairs; e += 32) {
-            const int q = e / npairs;
-            int J, K;
-            tri_pair(e - q * npairs, m, J, K);
+            int q = 0, r = e;
+            while (r >= npairs) { r -= npairs; ++q; }
+            const int4 o = __ldg(tri + e0 + r);
             double *c = cubes + q * NF;
-            c[jki_offset<P>(J, K) + i] =
-                -c[jki_offset<P>(J + 2, K) + i - 2] - c[jki_offset<P>(J, K + 2) + i - 2];
+            c[o.x] = -c[o.y] - c[o.z];
         }
         __syncwarp();
     }
@@ -1070,7 +1176,9 @@ m2p_items_kernel(int32_t nitems, const int4 *__restrict__ items,
 }
 
 // P2L item = {target box, first entry of the flat List-4 source index
-// array, number of sources (<= 32 * rounds), target level}. Each lane keeps
+// array, number of sources (<= 32 * rounds), target level}; one item per
+// warp (a persistent form, each warp running up to 32 items as one software
+// pipeline, measured slower: 0.443 against 0.425 ms at 1M points). Each lane keeps
 // its own FP32 sums q D over its sources in registers (N <= 128) and the
 // warp transposes them through shared memory once per item; higher orders
 // transpose every round.
@@ -1115,17 +1223,34 @@ p2l_items_kernel(int32_t nitems, const int4 *__restrict__ items,
         }
         __syncwarp();
     };
+    // software pipeline over the rounds of 32 sources: a round's coordinates
+    // and strength are loaded while the previous round's derivatives are
+    // computed, and its source indices one round earlier still, so that
+    // only the item's first round waits for memory
+    auto src_at = [&](int32_t k) { return k < cnt ? src_index[f0 + k] : -1; };
+    double nx = 0.0, ny = 0.0, nz = 0.0, nq = 0.0;
+    auto fetch = [&](int32_t s) {
+        if (s >= 0) {
+            nx = sources[s];
+            ny = sources[sstride + s];
+            nz = sources[2 * sstride + s];
+            nq = q[s];
+        }
+    };
+    int32_t s_next = src_at(lane);
+    fetch(s_next);
+    s_next = src_at(32 + lane);
     for (int32_t base = 0; base < cnt; base += 32) {
         const int nsc = min(32, cnt - base);
+        const float dx = (float)(c0 - nx), dy = (float)(c1 - ny), dz = (float)(c2 - nz);
+        const float qq = (float)nq;
+        fetch(s_next);                      // the next round
+        s_next = src_at(base + 64 + lane);  // the round after it
         if (lane < nsc) {
-            const int32_t s = src_index[f0 + base + lane];
-            const float qq = (float)q[s];
-            laplace_layers<P, float>(
-                (float)(c0 - sources[s]), (float)(c1 - sources[sstride + s]),
-                (float)(c2 - sources[2 * sstride + s]), R, Rinv, [&](int k, int, int, int, float v) {
-                    if constexpr (REG) own[k] = fmaf(qq, v, own[k]);
-                    else D[k * DSTRIDE + lane] = qq * v;
-                });
+            laplace_layers<P, float>(dx, dy, dz, R, Rinv, [&](int k, int, int, int, float v) {
+                if constexpr (REG) own[k] = fmaf(qq, v, own[k]);
+                else D[k * DSTRIDE + lane] = qq * v;
+            });
         }
         if constexpr (!REG) transpose_sum(nsc);
     }
