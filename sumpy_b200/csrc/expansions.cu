@@ -41,12 +41,15 @@ __device__ void decompress_cube_warp(double *cube, int p, int lane)
 
 // {{{ P2M
 
+// a source's row of power-table entries in the P2M kernel: P + 1 rounded up
+// to an even count, so that 16-byte loads read two powers at a time
+__host__ __device__ constexpr int p2m_row(int p) { return (p + 2) & ~1; }
+
 // warps per CTA: four while their static tables fit in 48 KB, else two
 template <int P>
 __host__ __device__ constexpr int p2m_warps()
 {
-    return (3 * (P + 1) * 33 + (P + 1) * (P + 2) * (P + 3) / 6 + 32) * 8 * 4 <= 48 * 1024 ? 4
-                                                                                            : 2;
+    return (3 * 32 * p2m_row(P) + (P + 1) * (P + 2) * (P + 3) / 6) * 8 * 4 <= 48 * 1024 ? 4 : 2;
 }
 
 // The P2M kernel's transposed projection as tables, per order P: for the
@@ -119,15 +122,16 @@ __host__ __device__ constexpr int p2m_kmax(int u)
 // P2M with one warp per box and the full coefficients in registers: lane l
 // owns the (i, j) pairs l, l + 32, ... (pairs in increasing i + j) and
 // accumulates the column k = 0..P-i-j of each, so a (source, coefficient)
-// term costs one FMA with the source's power z[k] = (a_z/r)^k/k!, loaded
-// once per source; per source t = q w0[i] w1[j] is formed once per pair.
-// The pair order bounds the k loop of the second and later row sets at
-// compile time (order 10: 11 + 4 + 1 FMAs per source instead of 3 x 11).
-// Sources go 32 at a time, one per lane for the power tables. The columns
-// are then written to a per-warp compact full-index buffer, compressed by
-// the p-1 plane sweeps (warp-synchronous) and stored. Same arithmetic as
-// p2m_kernel (multipole.py:77-114 and the transposed projection), ordered
-// differently.
+// term costs one FMA with the source's power z[k] = (a_z/r)^k/k!, read once
+// per source two at a time; per source t = (q (a_x/r)^i/i!) (a_y/r)^j/j! is
+// formed once per pair. The pair order bounds the k loop of the second and
+// later row sets at compile time (order 10: 11 + 4 + 1 FMAs per source
+// instead of 3 x 11); the entries past a pair's last column are computed
+// and never stored. Sources go 32 at a time, one per lane for the power
+// tables (a source's row of each table contiguous). The columns are then
+// written to a per-warp compact full-index buffer, compressed by the p-1
+// plane sweeps (warp-synchronous) and stored. Same arithmetic as p2m_kernel
+// (multipole.py:77-114 and the transposed projection), ordered differently.
 template <int P>
 __global__ void __launch_bounds__(32 * p2m_warps<P>())
 p2m_warp_kernel(double rscale, int32_t nboxes, const int32_t *__restrict__ boxes,
@@ -139,13 +143,14 @@ p2m_warp_kernel(double rscale, int32_t nboxes, const int32_t *__restrict__ boxes
                 const double *__restrict__ level_rscale = nullptr)
 {
     constexpr int P1 = P + 1;
+    constexpr int RW = p2m_row(P);
     constexpr int NPAIR = P1 * (P1 + 1) / 2;
     constexpr int NU = (NPAIR + 31) / 32;
     constexpr int NFULL = P1 * (P1 + 1) * (P1 + 2) / 6;
     constexpr int N = P1 * P1;
     constexpr int W = p2m_warps<P>();
-    __shared__ double w[W][3][P1][33];   // [axis][power][source] (+1 pad)
-    __shared__ double qs[W][32];
+    // [axis][source][power]; the x powers carry the strength
+    __shared__ __align__(16) double w[W][3][32][RW];
     __shared__ double full[W][NFULL];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ib = blockIdx.x * W + warp;
@@ -164,7 +169,7 @@ p2m_warp_kernel(double rscale, int32_t nboxes, const int32_t *__restrict__ boxes
         const int d = p2m_pair_degree(t < NPAIR ? t : 0);
         pi[u] = t < NPAIR ? t - d * (d + 1) / 2 : 0;
         pj[u] = t < NPAIR ? d - pi[u] : 0;
-        pk[u] = t < NPAIR ? P - d : -1;     // -1: idle slot, never accumulated or stored
+        pk[u] = t < NPAIR ? P - d : -1;     // -1: idle slot, never stored
     }
     double acc[NU][P1];
 #pragma unroll
@@ -176,31 +181,33 @@ p2m_warp_kernel(double rscale, int32_t nboxes, const int32_t *__restrict__ boxes
         const int nsc = min(32, ns - sc);
         if (lane < nsc) {
             const int32_t s = s0 + sc + lane;
-            qs[warp][lane] = q[s];
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 const double a = (c[d] - sources[d * sstride + s]) * rinv;
-                double v = 1.0;
-                w[warp][d][0][lane] = 1.0;
+                double v = d == 0 ? q[s] : 1.0;
+                w[warp][d][lane][0] = v;
 #pragma unroll
                 for (int k = 1; k < P1; ++k) {
                     v = v * a * (1.0 / k);    // a compile-time reciprocal: no division
-                    w[warp][d][k][lane] = v;
+                    w[warp][d][lane][k] = v;
                 }
             }
         }
         __syncwarp();
         for (int so = 0; so < nsc; ++so) {
-            const double qq = qs[warp][so];
-            double z[P1];
+            double z[RW];
+            const double2 *zr = reinterpret_cast<const double2 *>(w[warp][2][so]);
 #pragma unroll
-            for (int k = 0; k < P1; ++k) z[k] = w[warp][2][k][so];
+            for (int k = 0; k < RW / 2; ++k) {
+                const double2 v = zr[k];
+                z[2 * k] = v.x;
+                z[2 * k + 1] = v.y;
+            }
 #pragma unroll
             for (int u = 0; u < NU; ++u) {
-                const double t = qq * w[warp][0][pi[u]][so] * w[warp][1][pj[u]][so];
+                const double t = w[warp][0][so][pi[u]] * w[warp][1][so][pj[u]];
 #pragma unroll
-                for (int k = 0; k <= p2m_kmax<P>(u); ++k)
-                    if (k <= pk[u]) acc[u][k] = fma(t, z[k], acc[u][k]);
+                for (int k = 0; k <= p2m_kmax<P>(u); ++k) acc[u][k] = fma(t, z[k], acc[u][k]);
             }
         }
         __syncwarp();
