@@ -150,6 +150,11 @@ def _finish(actx, wrangler, trav, potentials, local_exps):
 
 
 def _drive_concurrent(actx, wrangler, trav, src_weight_vecs, crit, side):
+    """The chain on ``crit``; List 4, List 3 and List 1 on ``side`` in that
+    order. The chain waits for List 4 alone before L2L (its locals join the
+    List-2 locals there), so List 1 -- the longest independent stage -- runs
+    beside the chain's latency-bound L2L levels and L2P; the potentials of
+    Lists 1 and 3 join after L2P."""
     import torch
     main = torch.cuda.current_stream(crit.device)
     getattr(wrangler, "_geom", None)             # shared device geometry, made on this stream
@@ -166,17 +171,19 @@ def _drive_concurrent(actx, wrangler, trav, src_weight_vecs, crit, side):
             mpole_exps)
         wrangler.communicate_mpoles(actx, mpole_exps)
     with torch.cuda.stream(side):
-        potentials = wrangler.eval_direct(
-            actx, trav.target_boxes, trav.neighbor_source_boxes_starts,
-            trav.neighbor_source_boxes_lists, src_weight_vecs)
         local_result = wrangler.form_locals(
             actx, trav.level_start_target_or_target_parent_box_nrs,
             trav.target_or_target_parent_boxes, trav.from_sep_bigger_starts,
             trav.from_sep_bigger_lists, src_weight_vecs)
+        list4_done = torch.cuda.Event()
+        list4_done.record(side)
         side.wait_stream(crit)                   # multipoles finished
         mpole_result = wrangler.eval_multipoles(
             actx, trav.target_boxes_sep_smaller_by_source_level,
             trav.from_sep_smaller_by_level, mpole_exps)
+        potentials = wrangler.eval_direct(
+            actx, trav.target_boxes, trav.neighbor_source_boxes_starts,
+            trav.neighbor_source_boxes_lists, src_weight_vecs)
         potentials = [a + b for a, b in zip(potentials, mpole_result)]
     mpole_exps.record_stream(side)
     with torch.cuda.stream(crit):
@@ -184,10 +191,17 @@ def _drive_concurrent(actx, wrangler, trav, src_weight_vecs, crit, side):
             actx, trav.level_start_target_or_target_parent_box_nrs,
             trav.target_or_target_parent_boxes, trav.from_sep_siblings_starts,
             trav.from_sep_siblings_lists, mpole_exps)
-        crit.wait_stream(side)                   # join
-        for t in (*potentials, local_result):
-            t.record_stream(crit)
+        crit.wait_event(list4_done)
+        local_result.record_stream(crit)
         local_exps = local_exps + local_result
+        local_exps = wrangler.refine_locals(
+            actx, trav.level_start_target_or_target_parent_box_nrs,
+            trav.target_or_target_parent_boxes, local_exps)
+        local_pot = wrangler.eval_locals(
+            actx, trav.level_start_target_box_nrs, trav.target_boxes, local_exps)
+        crit.wait_stream(side)                   # Lists 1 and 3 finished
+        for t in potentials:
+            t.record_stream(crit)
         for starts, lists in ((trav.from_sep_close_smaller_starts,
                                trav.from_sep_close_smaller_lists),
                               (trav.from_sep_close_bigger_starts,
@@ -196,7 +210,8 @@ def _drive_concurrent(actx, wrangler, trav, src_weight_vecs, crit, side):
                 direct = wrangler.eval_direct(actx, trav.target_boxes, starts, lists,
                                               src_weight_vecs)
                 potentials = [a + b for a, b in zip(potentials, direct)]
-        result = _finish(actx, wrangler, trav, potentials, local_exps)
+        potentials = [a + b for a, b in zip(potentials, local_pot)]
+        result = wrangler.finalize_potentials(actx, wrangler.reorder_potentials(potentials))
     main.wait_stream(crit)
     for t in result:
         t.record_stream(main)
