@@ -19,6 +19,7 @@
 #include "common.cuh"
 #include "derivs.cuh"
 #include "taylor.cuh"
+#include "index_tables.cuh"
 
 namespace sumpy {
 namespace {
@@ -41,82 +42,11 @@ __device__ void decompress_cube_warp(double *cube, int p, int lane)
 
 // {{{ P2M
 
-// a source's row of power-table entries in the P2M kernel: P + 1 rounded up
-// to an even count, so that 16-byte loads read two powers at a time
-__host__ __device__ constexpr int p2m_row(int p) { return (p + 2) & ~1; }
-
 // warps per CTA: four while their static tables fit in 48 KB, else two
 template <int P>
 __host__ __device__ constexpr int p2m_warps()
 {
     return (3 * 32 * p2m_row(P) + (P + 1) * (P + 2) * (P + 3) / 6) * 8 * 4 <= 48 * 1024 ? 4 : 2;
-}
-
-// The P2M kernel's transposed projection as tables, per order P: for the
-// planes i = P..2 in turn, the entries F[i-2, J, K] -= F[i, J-2, K] +
-// F[i, J, K-2] (J + K <= P - i + 2) as full-index triples {dst, a, b, 0}
-// (-1: term absent), and the full index of each stored coefficient.
-__host__ __device__ constexpr int full_index_c(int i, int j, int k)
-{
-    return (i + j + k) * (i + j + k + 1) * (i + j + k + 2) / 6 + i * (i + j + k + 1) -
-           i * (i - 1) / 2 + j;
-}
-
-template <int P>
-struct P2mSweep {
-    static constexpr int ne()
-    {
-        int n = 0;
-        for (int i = P; i >= 2; --i) n += (P - i + 3) * (P - i + 4) / 2;
-        return n;
-    }
-    static constexpr int NE = ne() > 0 ? ne() : 1;
-    int e[4 * NE];
-    int start[P + 2];
-    int stored[(P + 1) * (P + 1)];
-    constexpr P2mSweep() : e(), start(), stored()
-    {
-        int n = 0, pl = 0;
-        for (int i = P; i >= 2; --i, ++pl) {
-            start[pl] = n;
-            const int m = P - i + 2;
-            for (int J = 0; J <= m; ++J)
-                for (int K = 0; J + K <= m; ++K) {
-                    e[4 * n] = full_index_c(i - 2, J, K);
-                    e[4 * n + 1] = J >= 2 ? full_index_c(i, J - 2, K) : -1;
-                    e[4 * n + 2] = K >= 2 ? full_index_c(i, J, K - 2) : -1;
-                    e[4 * n + 3] = 0;
-                    ++n;
-                }
-        }
-        for (; pl < P + 2; ++pl) start[pl] = n;
-        // stored coefficients: degree d = 0..P, (0, j, d - j) for j = 0..d,
-        // then (1, j, d - 1 - j) for j = 0..d-1 (sumpy's order)
-        int s = 0;
-        for (int d = 0; d <= P; ++d) {
-            for (int j = 0; j <= d; ++j) stored[s++] = full_index_c(0, j, d - j);
-            for (int j = 0; j < d; ++j) stored[s++] = full_index_c(1, j, d - 1 - j);
-        }
-    }
-};
-
-template <int P>
-__device__ constexpr P2mSweep<P> p2m_sweep{};
-
-// (i, j) pair t of the P2M kernel, in increasing degree d = i + j (and
-// increasing i within a degree): the pairs of row set u = t / 32 have
-// column lengths P - d + 1 of at most p2m_kmax(u) + 1
-__host__ __device__ constexpr int p2m_pair_degree(int t)
-{
-    int d = 0;
-    while ((d + 1) * (d + 2) / 2 <= t) ++d;
-    return d;
-}
-
-template <int P>
-__host__ __device__ constexpr int p2m_kmax(int u)
-{
-    return P - p2m_pair_degree(32 * u);
 }
 
 // P2M with one warp per box and the full coefficients in registers: lane l
@@ -849,49 +779,6 @@ __host__ __device__ constexpr int l2pk_warps()
 {
     return 8 * L2PK_SLOTS * (P + 1) * (P + 2) * (P + 3) / 6 * 4 <= 200 * 1024 ? 4 : 2;
 }
-
-// The packed L2P's decompression as tables, per order P, in the cube
-// layout of jki_offset: for the planes i = 2..P in turn, the entries
-// c[i, J, K] = -c[i-2, J+2, K] - c[i-2, J, K+2] (J + K <= P - i) as offset
-// triples {dst, a, b, 0}, and the cube offset of each stored coefficient.
-template <int P>
-struct L2pDecomp {
-    static constexpr int ne()
-    {
-        int n = 0;
-        for (int i = 2; i <= P; ++i) n += (P - i + 1) * (P - i + 2) / 2;
-        return n;
-    }
-    static constexpr int NE = ne() > 0 ? ne() : 1;
-    int e[4 * NE];
-    int start[P + 2];
-    int stored[(P + 1) * (P + 1)];
-    constexpr L2pDecomp() : e(), start(), stored()
-    {
-        int n = 0, pl = 0;
-        for (int i = 2; i <= P; ++i, ++pl) {
-            start[pl] = n;
-            const int m = P - i;
-            for (int J = 0; J <= m; ++J)
-                for (int K = 0; J + K <= m; ++K) {
-                    e[4 * n] = jki_offset<P>(J, K) + i;
-                    e[4 * n + 1] = jki_offset<P>(J + 2, K) + i - 2;
-                    e[4 * n + 2] = jki_offset<P>(J, K + 2) + i - 2;
-                    e[4 * n + 3] = 0;
-                    ++n;
-                }
-        }
-        for (; pl < P + 2; ++pl) start[pl] = n;
-        int s = 0;
-        for (int d = 0; d <= P; ++d) {
-            for (int j = 0; j <= d; ++j) stored[s++] = jki_offset<P>(j, d - j);
-            for (int j = 0; j < d; ++j) stored[s++] = jki_offset<P>(j, d - 1 - j) + 1;
-        }
-    }
-};
-
-template <int P>
-__device__ constexpr L2pDecomp<P> l2p_decomp{};
 
 // One warp evaluates up to 32 targets taken from up to L2PK_SLOTS boxes (slots; a
 // box with more than 32 targets spans several items). The slots' locals

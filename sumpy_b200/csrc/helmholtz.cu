@@ -32,6 +32,7 @@
 #include "common.cuh"
 #include "helmholtz_core.cuh"
 #include "taylor.cuh"
+#include "index_tables.cuh"
 
 namespace sumpy {
 namespace {
@@ -203,90 +204,133 @@ hp2p_direct_kernel(int64_t ntgt, const double *__restrict__ targets, int64_t tst
 
 // {{{ P2M
 
-constexpr int HP2M_THREADS = 128;
-constexpr int HP2M_CHUNK = 32;
-
-// full multipole cube -> compressed in place (transposed Helmholtz
-// projection, planes p..2 in turn; plane i-2 gathers from plane i)
-__device__ void h_compress_cube_block(z2 *cube, int p, double kappa)
+// P2M with one warp per box, the Laplace P2M's schedule on complex
+// strengths (p2m_warp_kernel, expansions.cu): lane l owns the (i, j) pairs
+// l, l + 32, ... in increasing i + j and accumulates the real and imaginary
+// parts of their columns k = 0..P-i-j in registers; per source the z powers
+// are read once, two at a time, and t = (a_x/r)^i/i! (a_y/r)^j/j! is formed
+// once per pair and scaled by the strength's two parts. The columns go to a
+// per-warp compact full-index buffer, compressed by the transposed
+// Helmholtz projection, planes P..2 in turn (the sweep table's fourth index
+// is the kappa term), and stored (sumpy/p2e.py:155-261,
+// multipole.py:77-114; sumpy/expansion/__init__.py:754-886).
+template <int P>
+__host__ __device__ constexpr int hp2m_warps()
 {
-    for (int i = p; i >= 2; --i) {
-        const int m = p - i + 2;
-        const int npairs = (m + 1) * (m + 2) / 2;
-        for (int t = threadIdx.x; t < npairs; t += blockDim.x) {
-            int J, K;
-            tri_pair(t, m, J, K);
-            z2 v = zmk(0.0, 0.0);
-            if (J >= 2) v = zadd(v, cube[cube_index(p, i, J - 2, K)]);
-            if (K >= 2) v = zadd(v, cube[cube_index(p, i, J, K - 2)]);
-            if (J + K <= p - i) v = zaxpy(kappa, cube[cube_index(p, i, J, K)], v);
-            z2 &o = cube[cube_index(p, i - 2, J, K)];
-            o = zmk(o.x - v.x, o.y - v.y);
-        }
-        __syncthreads();
-    }
+    return (3 * 32 * p2m_row(P) + 2 * 32 + 2 * (P + 1) * (P + 2) * (P + 3) / 6) * 8 * 2 <=
+                   48 * 1024
+               ? 2
+               : 1;
 }
 
-// P2EFromSingleBox (sumpy/p2e.py:155-261; multipole.py:77-114)
-__global__ void __launch_bounds__(HP2M_THREADS)
-hp2m_kernel(int p, double rscale, double kappa, const int32_t *__restrict__ boxes,
-            const double *__restrict__ centers, int64_t cstride, const int32_t *__restrict__ bss,
-            const int32_t *__restrict__ bsc, const double *__restrict__ sources, int64_t sstride,
-            const z2 *__restrict__ q, int32_t base, z2 *__restrict__ out,
-            const int32_t *__restrict__ box_level = nullptr,
-            const double *__restrict__ level_rscale = nullptr, double k = 0.0)
+template <int P>
+__global__ void __launch_bounds__(32 * hp2m_warps<P>())
+hp2m_warp_kernel(double rscale, double k, int32_t nboxes, const int32_t *__restrict__ boxes,
+                 const double *__restrict__ centers, int64_t cstride,
+                 const int32_t *__restrict__ bss, const int32_t *__restrict__ bsc,
+                 const double *__restrict__ sources, int64_t sstride, const z2 *__restrict__ q,
+                 int32_t base, z2 *__restrict__ out, const int32_t *__restrict__ box_level,
+                 const double *__restrict__ level_rscale)
 {
-    extern __shared__ __align__(16) double sm[];
-    const int P1 = p + 1;
-    z2 *cube = reinterpret_cast<z2 *>(sm);                // P1^3
-    double *pw = reinterpret_cast<double *>(cube + P1 * P1 * P1);  // [CHUNK][3][P1]
-    z2 *qs = reinterpret_cast<z2 *>(pw + HP2M_CHUNK * 3 * P1);     // [CHUNK]
-
-    const int32_t b = boxes[blockIdx.x];
+    constexpr int P1 = P + 1;
+    constexpr int RW = p2m_row(P);
+    constexpr int NPAIR = P1 * (P1 + 1) / 2;
+    constexpr int NU = (NPAIR + 31) / 32;
+    constexpr int NFULL = P1 * (P1 + 1) * (P1 + 2) / 6;
+    constexpr int N = P1 * P1;
+    constexpr int W = hp2m_warps<P>();
+    __shared__ __align__(16) double w[W][3][32][RW];   // [axis][source][power]
+    __shared__ z2 qs[W][32];
+    __shared__ z2 full[W][NFULL];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ib = blockIdx.x * W + warp;
+    if (ib >= nboxes) return;
+    const int32_t b = boxes[ib];
     const double c[3] = {centers[b], centers[cstride + b], centers[2 * cstride + b]};
     const int32_t s0 = bss[b], ns = bsc[b];
-    const int nfull = nfull_of(p);
-    if (level_rscale) {   // all levels in one launch: the box's own level
-        rscale = level_rscale[box_level[blockIdx.x]];
-        kappa = k * k * rscale * rscale;
-    }
-    const double rinv = 1.0 / rscale;
+    // all levels in one launch: the box's own level's rscale
+    const double rs = level_rscale ? level_rscale[box_level[ib]] : rscale;
+    const double rinv = 1.0 / rs, kappa = k * k * rs * rs;
 
-    for (int t = threadIdx.x; t < P1 * P1 * P1; t += blockDim.x) cube[t] = zmk(0.0, 0.0);
-    __syncthreads();
-    for (int sc = 0; sc < ns; sc += HP2M_CHUNK) {
-        const int nsc = min(HP2M_CHUNK, ns - sc);
-        for (int t = threadIdx.x; t < HP2M_CHUNK * 3; t += blockDim.x) {
-            const int s = t / 3, d = t % 3;
-            double *w = pw + (s * 3 + d) * P1;
-            if (s < nsc) {
-                const double a = (c[d] - sources[d * sstride + s0 + sc + s]) * rinv;
-                w[0] = 1.0;
-                for (int kk = 1; kk <= p; ++kk) w[kk] = w[kk - 1] * a / kk;
-                if (d == 0) qs[s] = q[s0 + sc + s];
+    int pi[NU], pj[NU], pk[NU];
+#pragma unroll
+    for (int u = 0; u < NU; ++u) {
+        const int t = lane + 32 * u;
+        const int d = p2m_pair_degree(t < NPAIR ? t : 0);
+        pi[u] = t < NPAIR ? t - d * (d + 1) / 2 : 0;
+        pj[u] = t < NPAIR ? d - pi[u] : 0;
+        pk[u] = t < NPAIR ? P - d : -1;     // -1: idle slot, never stored
+    }
+    double ar[NU][P1], ai[NU][P1];
+#pragma unroll
+    for (int u = 0; u < NU; ++u)
+#pragma unroll
+        for (int kk = 0; kk < P1; ++kk) ar[u][kk] = ai[u][kk] = 0.0;
+
+    for (int32_t sc = 0; sc < ns; sc += 32) {
+        const int nsc = min(32, ns - sc);
+        if (lane < nsc) {
+            const int32_t s = s0 + sc + lane;
+            qs[warp][lane] = q[s];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const double a = (c[d] - sources[d * sstride + s]) * rinv;
+                double v = 1.0;
+                w[warp][d][lane][0] = v;
+#pragma unroll
+                for (int kk = 1; kk < P1; ++kk) {
+                    v = v * a * (1.0 / kk);    // a compile-time reciprocal: no division
+                    w[warp][d][lane][kk] = v;
+                }
             }
         }
-        __syncthreads();
-        for (int f = threadIdx.x; f < nfull; f += blockDim.x) {
-            int i, j, kk;
-            full_mi(f, i, j, kk);
-            z2 acc = zmk(0.0, 0.0);
-            for (int s = 0; s < nsc; ++s)
-                acc = zaxpy(pw[(s * 3 + 0) * P1 + i] * pw[(s * 3 + 1) * P1 + j] *
-                                pw[(s * 3 + 2) * P1 + kk],
-                            qs[s], acc);
-            cube[cube_index(p, i, j, kk)] = zadd(cube[cube_index(p, i, j, kk)], acc);
+        __syncwarp();
+        for (int so = 0; so < nsc; ++so) {
+            double z[RW];
+            const double2 *zr = reinterpret_cast<const double2 *>(w[warp][2][so]);
+#pragma unroll
+            for (int kk = 0; kk < RW / 2; ++kk) {
+                const double2 v = zr[kk];
+                z[2 * kk] = v.x;
+                z[2 * kk + 1] = v.y;
+            }
+            const z2 qq = qs[warp][so];
+#pragma unroll
+            for (int u = 0; u < NU; ++u) {
+                const double t = w[warp][0][so][pi[u]] * w[warp][1][so][pj[u]];
+                const double tr = t * qq.x, ti = t * qq.y;
+#pragma unroll
+                for (int kk = 0; kk <= p2m_kmax<P>(u); ++kk) {
+                    ar[u][kk] = fma(tr, z[kk], ar[u][kk]);
+                    ai[u][kk] = fma(ti, z[kk], ai[u][kk]);
+                }
+            }
         }
-        __syncthreads();
+        __syncwarp();
     }
-    h_compress_cube_block(cube, p, kappa);
-    const int n = ncoeff_of(p);
-    z2 *o = out + (int64_t)(b - base) * n;
-    for (int s = threadIdx.x; s < n; s += blockDim.x) {
-        int i, j, kk;
-        stored_mi(s, i, j, kk);
-        o[s] = cube[cube_index(p, i, j, kk)];
+    z2 *F = full[warp];
+#pragma unroll
+    for (int u = 0; u < NU; ++u) {
+#pragma unroll
+        for (int kk = 0; kk <= p2m_kmax<P>(u); ++kk)
+            if (kk <= pk[u]) F[full_index(pi[u], pj[u], kk)] = zmk(ar[u][kk], ai[u][kk]);
     }
+    __syncwarp();
+    // transposed projection: plane i-2 gathers from plane i, i = P..2
+    const int4 *sweep = reinterpret_cast<const int4 *>(p2m_sweep<P>.e);
+    for (int pl = 0; pl + 2 <= P; ++pl) {
+        for (int t = p2m_sweep<P>.start[pl] + lane; t < p2m_sweep<P>.start[pl + 1]; t += 32) {
+            const int4 e = __ldg(sweep + t);
+            z2 v = zmk(0.0, 0.0);
+            if (e.y >= 0) v = zadd(v, F[e.y]);
+            if (e.z >= 0) v = zadd(v, F[e.z]);
+            if (e.w >= 0) v = zaxpy(kappa, F[e.w], v);
+            F[e.x] = zmk(F[e.x].x - v.x, F[e.x].y - v.y);
+        }
+        __syncwarp();
+    }
+    z2 *o = out + (int64_t)(b - base) * N;
+    for (int st = lane; st < N; st += 32) o[st] = F[__ldg(p2m_sweep<P>.stored + st)];
 }
 
 // }}}
@@ -846,16 +890,15 @@ int sumpy_helmholtz_p2e_from_single_box_f64(int order, double rscale, double k,
     if (!source_boxes || !centers || !box_source_starts || !box_source_counts_nonchild ||
         !sources || !strength || !tgt_expansions)
         return bad_arg("helmholtz p2m: null pointer argument");
-    const int P1 = order + 1;
-    const size_t smem = sizeof(z2) * P1 * P1 * P1 + sizeof(double) * HP2M_CHUNK * 3 * P1 +
-                        sizeof(z2) * HP2M_CHUNK;
-    int rc = prepare_smem(hp2m_kernel, smem);
-    if (rc) return rc;
-    hp2m_kernel<<<nsrc_boxes, HP2M_THREADS, smem, as_stream(stream)>>>(
-        order, rscale, k * k * rscale * rscale, source_boxes, centers, center_stride,
-        box_source_starts, box_source_counts_nonchild, sources, source_stride, cz(strength),
-        tgt_base_ibox, mz(tgt_expansions));
-    return check_launch("hp2m_kernel");
+#define CALL_HP2M(P)                                                                             \
+    (hp2m_warp_kernel<P><<<(nsrc_boxes + hp2m_warps<P>() - 1) / hp2m_warps<P>(),                   \
+                           32 * hp2m_warps<P>(), 0, as_stream(stream)>>>(                          \
+         rscale, k, nsrc_boxes, source_boxes, centers, center_stride, box_source_starts,         \
+         box_source_counts_nonchild, sources, source_stride, cz(strength), tgt_base_ibox,        \
+         mz(tgt_expansions), nullptr, nullptr),                                                  \
+     check_launch("hp2m_warp_kernel"))
+    SUMPY_ORDER_SWITCH(order, CALL_HP2M)
+#undef CALL_HP2M
 }
 
 int sumpy_helmholtz_e2e_from_children_f64(int src_order, int tgt_order, double src_rscale,
@@ -956,16 +999,15 @@ int sumpy_helmholtz_p2e_from_single_box_levels_f64(
     if (!source_boxes || !box_levels || !level_rscales || !centers || !box_source_starts ||
         !box_source_counts_nonchild || !sources || !strength || !expansions)
         return bad_arg("helmholtz p2m levels: null pointer argument");
-    const int P1 = order + 1;
-    const size_t smem = sizeof(z2) * P1 * P1 * P1 + sizeof(double) * HP2M_CHUNK * 3 * P1 +
-                        sizeof(z2) * HP2M_CHUNK;
-    int rc = prepare_smem(hp2m_kernel, smem);
-    if (rc) return rc;
-    hp2m_kernel<<<nsrc_boxes, HP2M_THREADS, smem, as_stream(stream)>>>(
-        order, 1.0, 0.0, source_boxes, centers, center_stride, box_source_starts,
-        box_source_counts_nonchild, sources, source_stride, cz(strength), 0, mz(expansions),
-        box_levels, level_rscales, k);
-    return check_launch("hp2m_kernel");
+#define CALL_HP2M(P)                                                                             \
+    (hp2m_warp_kernel<P><<<(nsrc_boxes + hp2m_warps<P>() - 1) / hp2m_warps<P>(),                   \
+                           32 * hp2m_warps<P>(), 0, as_stream(stream)>>>(                          \
+         1.0, k, nsrc_boxes, source_boxes, centers, center_stride, box_source_starts,            \
+         box_source_counts_nonchild, sources, source_stride, cz(strength), 0, mz(expansions),    \
+         box_levels, level_rscales),                                                             \
+     check_launch("hp2m_warp_kernel"))
+    SUMPY_ORDER_SWITCH(order, CALL_HP2M)
+#undef CALL_HP2M
 }
 
 int sumpy_helmholtz_e2p_from_single_box_levels_f64(

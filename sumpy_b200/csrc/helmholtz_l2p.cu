@@ -12,6 +12,7 @@
 #include "common.cuh"
 #include "helmholtz_core.cuh"
 #include "taylor.cuh"
+#include "index_tables.cuh"
 
 namespace sumpy {
 namespace {
@@ -58,29 +59,39 @@ hl2p_packed_kernel(int32_t nitems, const int2 *__restrict__ items, const int4 *_
     // stored -> full layout, all slots
     for (int e = lane; e < nsl * N; e += 32) {
         const int q = e / N, st = e - q * N;
-        int i, j, kk;
-        stored_mi(st, i, j, kk);
         const int32_t b = slots[item.x + q].x;
-        cubes[q * NF + jki_offset<P>(j, kk) + i] = loc[(int64_t)b * N + st];
+        cubes[q * NF + __ldg(l2p_decomp<P>.stored + st)] = loc[(int64_t)b * N + st];
+    }
+    // each slot's kappa = k^2 rscale^2 of its level, in every lane
+    double kap[HL2PK_SLOTS];
+    {
+        double mine = 0.0;
+        if (lane < nsl) {
+            const double rs = level_rscale[slots[item.x + lane].w];
+            mine = k * k * rs * rs;
+        }
+#pragma unroll
+        for (int q = 0; q < HL2PK_SLOTS; ++q) kap[q] = __shfl_sync(0xffffffffu, mine, q);
     }
     __syncwarp();
     // decompress: plane i from plane i - 2 (all slots per sweep), each slot
-    // with its own level's kappa
-    for (int i = 2; i <= P; ++i) {
-        const int m = P - i;
-        const int npairs = (m + 1) * (m + 2) / 2;
+    // with its own level's kappa, by the precomputed offset triples of each
+    // plane (the u_{mi-2e0} term sits two places before the destination)
+    const int4 *tri = reinterpret_cast<const int4 *>(l2p_decomp<P>.e);
+    for (int pl = 0; pl + 2 <= P; ++pl) {
+        const int e0 = l2p_decomp<P>.start[pl];
+        const int npairs = l2p_decomp<P>.start[pl + 1] - e0;
         for (int e = lane; e < nsl * npairs; e += 32) {
-            const int q = e / npairs;
-            int J, K;
-            tri_pair(e - q * npairs, m, J, K);
-            const double rs = level_rscale[slots[item.x + q].w];
-            const double kappa = k * k * rs * rs;
+            int q = 0, r = e;
+            while (r >= npairs) { r -= npairs; ++q; }
+            const int4 o = __ldg(tri + e0 + r);
+            double kappa = kap[0];
+#pragma unroll
+            for (int qq = 1; qq < HL2PK_SLOTS; ++qq)
+                if (q == qq) kappa = kap[qq];
             z2 *c = cubes + q * NF;
-            const z2 u1 = c[jki_offset<P>(J + 2, K) + i - 2];
-            const z2 u2 = c[jki_offset<P>(J, K + 2) + i - 2];
-            const z2 u0 = c[jki_offset<P>(J, K) + i - 2];
-            c[jki_offset<P>(J, K) + i] =
-                zmk(-u1.x - u2.x - kappa * u0.x, -u1.y - u2.y - kappa * u0.y);
+            const z2 u1 = c[o.y], u2 = c[o.z], u0 = c[o.x - 2];
+            c[o.x] = zmk(-u1.x - u2.x - kappa * u0.x, -u1.y - u2.y - kappa * u0.y);
         }
         __syncwarp();
     }
