@@ -452,91 +452,100 @@ constexpr int HL2L_BOXES = 4;
 
 // E2EFromParent (sumpy/e2e.py:985-1083; local.py:346-464): parent local
 // decompressed with kappa_parent, Taylor-shifted along axes 0, 1, 2
-// (truncated at the parent's order), times (r_child/r_parent)^|mi|,
-// accumulated into the child; HL2L_BOXES children per CTA.
+// (truncated at the parent's order P), times (r_child/r_parent)^|mi|,
+// accumulated into the child; HL2L_BOXES children per CTA. Every multi-index
+// step comes from the compile-time tables of full_shift<P> (the shift terms
+// m + q e_d and the decompression planes in the compact full layout).
+template <int P>
 __global__ void __launch_bounds__(HE2E_THREADS)
-hl2l_kernel(int ps, int pt, double rsrc, double rtgt, double kappa_s, int32_t nboxes,
+hl2l_kernel(int pt, double rsrc, double rtgt, double kappa_s, int32_t nboxes,
             const int32_t *__restrict__ boxes, const int32_t *__restrict__ parent_ids,
             const double *__restrict__ centers, int64_t cstride, int32_t sbase,
             const z2 *__restrict__ src, int32_t tbase, z2 *__restrict__ tgt)
 {
+    constexpr int P1 = P + 1;
+    constexpr int NF = FullShift<P>::NFULL;
+    constexpr int NS = P1 * P1;
+    const FullShift<P> &T = full_shift<P>;
     extern __shared__ __align__(16) double sm[];
-    const int P1 = ps + 1;
-    const int nfull = nfull_of(ps);
     z2 *A = reinterpret_cast<z2 *>(sm);
-    z2 *B = A + HL2L_BOXES * nfull;
-    double *pw = reinterpret_cast<double *>(B + HL2L_BOXES * nfull);
-    uint32_t *tab = reinterpret_cast<uint32_t *>(pw + HL2L_BOXES * 3 * P1);
+    z2 *B = A + HL2L_BOXES * NF;
+    double *pw = reinterpret_cast<double *>(B + HL2L_BOXES * NF);   // [box][axis][P1]
     const int b0 = blockIdx.x * HL2L_BOXES;
     const int nk = min(HL2L_BOXES, nboxes - b0);
-    const int ns = ncoeff_of(ps), nt = ncoeff_of(pt);
 
-    for (int f = threadIdx.x; f < nfull; f += blockDim.x) {
-        int i, j, k;
-        full_mi(f, i, j, k);
-        tab[f] = (uint32_t)i | ((uint32_t)j << 8) | ((uint32_t)k << 16);
-    }
     for (int t = threadIdx.x; t < nk * 3; t += blockDim.x) {
         const int c = t / 3, d = t % 3;
         const int32_t b = boxes[b0 + c];
         const int32_t par = parent_ids[b];
         const double dd = (centers[d * cstride + b] - centers[d * cstride + par]) / rsrc;
         double *w = pw + (c * 3 + d) * P1;
-        w[0] = 1.0;
-        for (int q = 1; q <= ps; ++q) w[q] = w[q - 1] * dd / q;
+        double v = 1.0;
+        w[0] = v;
+#pragma unroll
+        for (int q = 1; q <= P; ++q) {
+            v = v * dd * (1.0 / q);    // a compile-time reciprocal: no division
+            w[q] = v;
+        }
     }
-    for (int t = threadIdx.x; t < nk * ns; t += blockDim.x) {
-        const int c = t / ns, s2 = t % ns;
+    for (int t = threadIdx.x; t < nk * NS; t += blockDim.x) {
+        const int c = t / NS, s2 = t - c * NS;
         const int32_t par = parent_ids[boxes[b0 + c]];
-        int i, j, k;
-        stored_mi(s2, i, j, k);
-        A[c * nfull + full_index(i, j, k)] = src[(int64_t)(par - sbase) * ns + s2];
+        A[c * NF + __ldg(p2m_sweep<P>.stored + s2)] = src[(int64_t)(par - sbase) * NS + s2];
     }
     __syncthreads();
-    for (int i = 2; i <= ps; ++i) {
-        const int m = ps - i;
-        const int npairs = (m + 1) * (m + 2) / 2;
+    const int4 *de = reinterpret_cast<const int4 *>(T.e);
+    for (int pl = 0; pl + 2 <= P; ++pl) {
+        const int e0 = T.dstart[pl], npairs = T.dstart[pl + 1] - e0;
         for (int t = threadIdx.x; t < nk * npairs; t += blockDim.x) {
-            const int c = t / npairs;
-            int J, K;
-            tri_pair(t % npairs, m, J, K);
-            z2 *a = A + c * nfull;
-            const z2 u1 = a[full_index(i - 2, J + 2, K)], u2 = a[full_index(i - 2, J, K + 2)];
-            const z2 u0 = a[full_index(i - 2, J, K)];
-            a[full_index(i, J, K)] = zmk(-u1.x - u2.x - kappa_s * u0.x, -u1.y - u2.y - kappa_s * u0.y);
+            int c = 0, r = t;
+            while (r >= npairs) { r -= npairs; ++c; }
+            const int4 o = __ldg(de + e0 + r);
+            z2 *a = A + c * NF;
+            const z2 u1 = a[o.y], u2 = a[o.z], u0 = a[o.w];
+            a[o.x] = zmk(-u1.x - u2.x - kappa_s * u0.x, -u1.y - u2.y - kappa_s * u0.y);
         }
         __syncthreads();
     }
     z2 *in = A, *out = B;
 #pragma unroll 1
     for (int d = 0; d < 3; ++d) {
-        for (int t = threadIdx.x; t < nk * nfull; t += blockDim.x) {
-            const int c = t / nfull, f = t % nfull;
-            const uint32_t e = tab[f];
-            int m[3] = {(int)(e & 0xff), (int)((e >> 8) & 0xff), (int)(e >> 16)};
-            const int deg = m[0] + m[1] + m[2];
+        const short *ix = T.idx[d];
+        for (int t = threadIdx.x; t < nk * NF; t += blockDim.x) {
+            const int c = t / NF, f = t - c * NF;
+            const int s0 = __ldg(T.start + f), s1 = __ldg(T.start + f + 1);
             const double *w = pw + (c * 3 + d) * P1;
-            const z2 *inc = in + c * nfull;
-            const int md = m[d];
+            const z2 *inc = in + c * NF;
             z2 acc = zmk(0.0, 0.0);
-            for (int q = 0; q <= ps - deg; ++q) {
-                m[d] = md + q;
-                acc = zaxpy(w[q], inc[full_index(m[0], m[1], m[2])], acc);
-            }
-            out[c * nfull + f] = acc;
+            for (int s = s0; s < s1; ++s) acc = zaxpy(w[s - s0], inc[__ldg(ix + s)], acc);
+            out[c * NF + f] = acc;
         }
         __syncthreads();
         z2 *sw = in; in = out; out = sw;
     }
-    const double ratio = rtgt / rsrc;
+    __shared__ double rpow[P1];
+    if (threadIdx.x == 0) {
+        const double ratio = rtgt / rsrc;
+        double v = 1.0;
+        for (int q = 0; q <= P; ++q, v *= ratio) rpow[q] = v;
+    }
+    __syncthreads();
+    const int nt = ncoeff_of(pt);
     for (int t = threadIdx.x; t < nk * nt; t += blockDim.x) {
-        const int c = t / nt, s2 = t % nt;
-        int i, j, k;
-        stored_mi(s2, i, j, k);
-        const int deg = i + j + k;
-        if (deg <= ps) {
+        const int c = t / nt, s2 = t - c * nt;
+        int f, deg;
+        if (pt == P) {
+            f = __ldg(p2m_sweep<P>.stored + s2);
+            deg = T.sdeg[s2];
+        } else {
+            int i, j, k;
+            stored_mi(s2, i, j, k);
+            deg = i + j + k;
+            f = deg <= P ? full_index(i, j, k) : 0;
+        }
+        if (deg <= P) {
             z2 &o = tgt[(int64_t)(boxes[b0 + c] - tbase) * nt + s2];
-            o = zaxpy(ipow(ratio, deg), in[c * nfull + full_index(i, j, k)], o);
+            o = zaxpy(rpow[deg], in[c * NF + f], o);
         }
     }
 }
@@ -946,17 +955,21 @@ int sumpy_helmholtz_e2e_from_parent_f64(int src_order, int tgt_order, double src
     if (ntgt_boxes == 0) return SUMPY_OK;
     if (!target_boxes || !box_parent_ids || !centers || !src_expansions || !tgt_expansions)
         return bad_arg("helmholtz l2l: null pointer argument");
-    const int nfull = (src_order + 1) * (src_order + 2) * (src_order + 3) / 6;
-    const size_t smem = sizeof(z2) * 2 * HL2L_BOXES * nfull +
-                        sizeof(double) * HL2L_BOXES * 3 * (src_order + 1) + sizeof(uint32_t) * nfull;
-    int rc = prepare_smem(hl2l_kernel, smem);
-    if (rc) return rc;
     const unsigned blocks = (unsigned)((ntgt_boxes + HL2L_BOXES - 1) / HL2L_BOXES);
-    hl2l_kernel<<<blocks, HE2E_THREADS, smem, as_stream(stream)>>>(
-        src_order, tgt_order, src_rscale, tgt_rscale, k * k * src_rscale * src_rscale, ntgt_boxes,
-        target_boxes, box_parent_ids, centers, center_stride, src_base_ibox, cz(src_expansions),
-        tgt_base_ibox, mz(tgt_expansions));
-    return check_launch("hl2l_kernel");
+#define CALL_HL2L(P)                                                                             \
+    (prepare_smem(hl2l_kernel<P>, sizeof(z2) * 2 * HL2L_BOXES * FullShift<P>::NFULL +            \
+                                      sizeof(double) * HL2L_BOXES * 3 * (P + 1))                 \
+         ? SUMPY_ELAUNCH                                                                         \
+         : (hl2l_kernel<P><<<blocks, HE2E_THREADS,                                               \
+                             sizeof(z2) * 2 * HL2L_BOXES * FullShift<P>::NFULL +                 \
+                                 sizeof(double) * HL2L_BOXES * 3 * (P + 1),                      \
+                             as_stream(stream)>>>(                                               \
+                tgt_order, src_rscale, tgt_rscale, k * k * src_rscale * src_rscale, ntgt_boxes, \
+                target_boxes, box_parent_ids, centers, center_stride, src_base_ibox,            \
+                cz(src_expansions), tgt_base_ibox, mz(tgt_expansions)),                         \
+            check_launch("hl2l_kernel")))
+    SUMPY_ORDER_SWITCH(src_order, CALL_HL2L)
+#undef CALL_HL2L
 }
 
 int sumpy_helmholtz_e2p_from_single_box_f64(int order, double rscale, double k,

@@ -26,7 +26,7 @@ __host__ __device__ constexpr int full_index_c(int i, int j, int k)
 }
 
 template <int P>
-struct P2mSweep {
+struct alignas(16) P2mSweep {
     static constexpr int ne()
     {
         int n = 0;
@@ -87,7 +87,7 @@ __host__ __device__ constexpr int p2m_kmax(int u)
 // c[i, J, K] = -c[i-2, J+2, K] - c[i-2, J, K+2] (J + K <= P - i) as offset
 // triples {dst, a, b, 0}, and the cube offset of each stored coefficient.
 template <int P>
-struct L2pDecomp {
+struct alignas(16) L2pDecomp {
     static constexpr int ne()
     {
         int n = 0;
@@ -124,6 +124,66 @@ struct L2pDecomp {
 
 template <int P>
 __device__ constexpr L2pDecomp<P> l2p_decomp{};
+
+// Taylor shifts and the PDE decompression in the compact full-index
+// layout (sumpy's order |mi|, mi0, mi1), per order P: for the planes
+// i = 2..P in turn, {dst, a, b, c} with u_dst = -u_a - u_b - kappa u_c
+// (dst = (i, J, K), a = (i-2, J+2, K), b = (i-2, J, K+2), c = (i-2, J, K));
+// and for each axis d and full coefficient f = m, the full indices of
+// m + q e_d, q = 0..P-|m|, at terms start[f] .. start[f + 1] - 1.
+template <int P>
+struct alignas(16) FullShift {
+    static constexpr int NFULL = (P + 1) * (P + 2) * (P + 3) / 6;
+    static constexpr int NT = (P + 1) * (P + 2) * (P + 3) * (P + 4) / 24;
+    static constexpr int ne()
+    {
+        int n = 0;
+        for (int i = 2; i <= P; ++i) n += (P - i + 1) * (P - i + 2) / 2;
+        return n;
+    }
+    static constexpr int NE = ne() > 0 ? ne() : 1;
+    int e[4 * NE];      // first member: read as int4
+    int start[NFULL + 1];
+    short idx[3][NT];
+    int dstart[P + 2];
+    unsigned char sdeg[(P + 1) * (P + 1)];   // degree of each stored coefficient
+    constexpr FullShift() : e(), start(), idx(), dstart(), sdeg()
+    {
+        for (int d = 0, s = 0; d <= P; ++d)
+            for (int r = 0; r < 2 * d + 1; ++r) sdeg[s++] = (unsigned char)d;
+        int f = 0, t = 0;
+        for (int deg = 0; deg <= P; ++deg)
+            for (int i = 0; i <= deg; ++i)
+                for (int j = 0; i + j <= deg; ++j, ++f) {
+                    const int m[3] = {i, j, deg - i - j};
+                    start[f] = t;
+                    for (int q = 0; q <= P - deg; ++q, ++t)
+                        for (int d = 0; d < 3; ++d) {
+                            const int a = m[0] + (d == 0 ? q : 0);
+                            const int b = m[1] + (d == 1 ? q : 0);
+                            const int c = m[2] + (d == 2 ? q : 0);
+                            idx[d][t] = (short)full_index_c(a, b, c);
+                        }
+                }
+        start[NFULL] = t;
+        int n = 0, pl = 0;
+        for (int i = 2; i <= P; ++i, ++pl) {
+            dstart[pl] = n;
+            const int m = P - i;
+            for (int J = 0; J <= m; ++J)
+                for (int K = 0; J + K <= m; ++K, ++n) {
+                    e[4 * n] = full_index_c(i, J, K);
+                    e[4 * n + 1] = full_index_c(i - 2, J + 2, K);
+                    e[4 * n + 2] = full_index_c(i - 2, J, K + 2);
+                    e[4 * n + 3] = full_index_c(i - 2, J, K);
+                }
+        }
+        for (; pl < P + 2; ++pl) dstart[pl] = n;
+    }
+};
+
+template <int P>
+__device__ constexpr FullShift<P> full_shift{};
 
 }  // namespace
 }  // namespace sumpy
