@@ -824,6 +824,19 @@ l2p_packed_kernel(int32_t nitems, const int2 *__restrict__ items, const int4 *__
             if (off < v.z) { my = q; sl = v; } else { off -= v.z; }
         }
     }
+    // this lane's target, its box center and rscale: loaded before the
+    // locals are staged, so that their latency overlaps the staging
+    double tx = 0.0, ty = 0.0, tz = 0.0, cx = 0.0, cy = 0.0, cz = 0.0, rs = 1.0;
+    if (my >= 0) {
+        const int32_t bb = sl.x, tt = sl.y + off;
+        tx = targets[tt];
+        ty = targets[tstride + tt];
+        tz = targets[2 * tstride + tt];
+        cx = centers[bb];
+        cy = centers[cstride + bb];
+        cz = centers[2 * cstride + bb];
+        rs = level_rscale[sl.w];
+    }
     // stored -> full layout, all slots
     for (int e = lane; e < nsl * N; e += 32) {
         const int q = e / N, st = e - q * N;
@@ -847,11 +860,11 @@ l2p_packed_kernel(int32_t nitems, const int2 *__restrict__ items, const int4 *__
         __syncwarp();
     }
     if (my < 0) return;
-    const int32_t b = sl.x, t = sl.y + off;
-    const double rs = level_rscale[sl.w], rinv = 1.0 / rs;
-    const double x = (targets[t] - centers[b]) * rinv;
-    const double y = (targets[tstride + t] - centers[cstride + b]) * rinv;
-    const double z = (targets[2 * tstride + t] - centers[2 * cstride + b]) * rinv;
+    const int32_t t = sl.y + off;
+    const double rinv = 1.0 / rs;
+    const double x = (tx - cx) * rinv;
+    const double y = (ty - cy) * rinv;
+    const double z = (tz - cz) * rinv;
     double xp[P1], yp[P1], zp[P1];
     xp[0] = yp[0] = zp[0] = 1.0;
 #pragma unroll
