@@ -58,7 +58,7 @@ def _setup(geom):
 
 
 @pytest.mark.parametrize("geom", list(GEOMS))
-@pytest.mark.parametrize("order", [3, 6, 10])
+@pytest.mark.parametrize("order", [1, 3, 6, 10, 16])
 def test_stages_match_oracle(cuda_device, geom, order):
     src, tgt, tree, trav, tcls, q = _setup(geom)
     excl = tgt is None

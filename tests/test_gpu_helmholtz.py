@@ -72,7 +72,7 @@ def _setup(geom):
 
 
 @pytest.mark.parametrize("geom", ["uniform_separate", "sphere_self", "sphere_plummer_self"])
-@pytest.mark.parametrize("order", [3, 8])
+@pytest.mark.parametrize("order", [1, 3, 8, 14])
 def test_stages_match_oracle(cuda_device, geom, order):
     src, tgt, tree, trav, tcls, q = _setup(geom)
     excl = tgt is None
