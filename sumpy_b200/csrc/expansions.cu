@@ -1082,6 +1082,91 @@ m2p_items_kernel(int32_t nitems, const int4 *__restrict__ items,
     }
 }
 
+// The potential-only M2P on packed FP32 pairs: each lane group takes two
+// List-3 boxes per round (boxes ph and ph + nph of the round's 2 nph), so
+// every recurrence and accumulation instruction serves both boxes
+// (laplace_layers_x2). A round's 2 nph FP32 multipoles are double-buffered
+// into shared memory by cp.async as in m2p_items_kernel; a missing second
+// box repeats the first and its half of the sum is dropped.
+template <int P>
+__global__ void __launch_bounds__(32 * ITEM_WARPS)
+m2p_items_x2_kernel(int32_t nitems, const int4 *__restrict__ items,
+                    const double *__restrict__ level_rscale, const int32_t *__restrict__ src_lists,
+                    const double *__restrict__ centers, int64_t cstride,
+                    const float *__restrict__ mp32, const double *__restrict__ targets,
+                    int64_t tstride, double scale, double *__restrict__ result)
+{
+    constexpr int NP = npad_of(P);
+    constexpr int C = NP / 4;
+    constexpr int BUF = 2 * M2PI_GROUPS * NP;   // one round: two boxes per lane group
+    extern __shared__ __align__(16) float smi[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int it = blockIdx.x * ITEM_WARPS + warp;
+    if (it >= nitems) return;
+    float *buf = smi + warp * (2 * BUF);
+    const int4 item = items[it];
+    const int32_t t0 = item.x, l0 = item.y, nb = item.z;
+    const int ntc = item.w & 0xff, lev = item.w >> 8;
+    int g = 32 / M2PI_GROUPS;
+    while (g < ntc) g <<= 1;
+    const int nph = 32 / g;
+    const int per = 2 * nph;
+    const int tl = lane & (g - 1), ph = lane / g;
+    const bool active = tl < ntc;
+    const int32_t t = t0 + tl;
+    double tx = 0, ty = 0, tz = 0;
+    if (active) { tx = targets[t]; ty = targets[tstride + t]; tz = targets[2 * tstride + t]; }
+    const double rs = level_rscale[lev];
+    const float R = (float)rs, Rinv = (float)(1.0 / rs);
+    const int nrounds = (nb + per - 1) / per;
+
+    // round r's boxes (2 nph at most) into buffer r & 1
+    auto stage = [&](int r) {
+        const int first = r * per, cnt = min(per, nb - first);
+        float *dst = buf + (r & 1) * BUF;
+        for (int e = lane; e < cnt * C; e += 32) {
+            const int k = e / C, c = e - k * C;
+            const int32_t sb = src_lists[l0 + first + k];
+            cpa16(dst + k * NP + 4 * c, mp32 + (int64_t)sb * NP + 4 * c);
+        }
+        cpa_commit();
+    };
+    stage(0);
+    double acc = 0.0;
+    for (int r = 0; r < nrounds; ++r) {
+        if (r + 1 < nrounds) {
+            stage(r + 1);
+            cpa_wait<1>();
+        } else {
+            cpa_wait<0>();
+        }
+        __syncwarp();
+        const int k1 = r * per + ph, k2 = k1 + nph;
+        if (active && k1 < nb) {
+            const bool two = k2 < nb;
+            const int32_t sb1 = src_lists[l0 + k1];
+            const int32_t sb2 = two ? src_lists[l0 + k2] : sb1;
+            const float *M1 = buf + (r & 1) * BUF + ph * NP;
+            const float *M2 = two ? M1 + nph * NP : M1;
+            const float2 x = make_float2((float)(tx - centers[sb1]), (float)(tx - centers[sb2]));
+            const float2 y = make_float2((float)(ty - centers[cstride + sb1]),
+                                         (float)(ty - centers[cstride + sb2]));
+            const float2 z = make_float2((float)(tz - centers[2 * cstride + sb1]),
+                                         (float)(tz - centers[2 * cstride + sb2]));
+            // two partial sums per box: a dependent chain of N / 2 FMAs
+            float2 a2[2] = {f2(0.f), f2(0.f)};
+            laplace_layers_x2<P>(x, y, z, R, Rinv, [&](int s, int, int, int, float2 v) {
+                a2[s & 1] = __ffma2_rn(make_float2(M1[s], M2[s]), v, a2[s & 1]);
+            });
+            acc += (double)(a2[0].x + a2[1].x);
+            if (two) acc += (double)(a2[0].y + a2[1].y);
+        }
+        __syncwarp();   // buffer r & 1 is refilled by round r + 2's copies
+    }
+    for (int off = g; off < 32; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if (active && ph == 0 && result) atomicAdd(result + t, scale * acc);
+}
+
 // P2L item = {target box, first entry of the flat List-4 source index
 // array, number of sources (<= 32 * rounds), target level}; one item per
 // warp (a persistent form, each warp running up to 32 items as one software
@@ -1625,15 +1710,16 @@ int sumpy_e2p_from_items_mixed(int order, int32_t nitems, const int32_t *items,
         return bad_arg("m2p items: items and FP32 expansions must be 16-byte aligned");
     const int blocks = (nitems + ITEM_WARPS - 1) / ITEM_WARPS;
 #define CALL_M2PI(P)                                                                             \
-    (prepare_smem(m2p_items_kernel<P>, sizeof(float) * 2 * M2PI_GROUPS * npad_of(P) * ITEM_WARPS) \
+    (prepare_smem(m2p_items_x2_kernel<P>,                                                        \
+                  sizeof(float) * 4 * M2PI_GROUPS * npad_of(P) * ITEM_WARPS)                     \
          ? SUMPY_ELAUNCH                                                                         \
-         : (m2p_items_kernel<P><<<blocks, 32 * ITEM_WARPS,                                       \
-                                  sizeof(float) * 2 * M2PI_GROUPS * npad_of(P) * ITEM_WARPS,     \
-                                  as_stream(stream)>>>(                                          \
+         : (m2p_items_x2_kernel<P><<<blocks, 32 * ITEM_WARPS,                                    \
+                                     sizeof(float) * 4 * M2PI_GROUPS * npad_of(P) * ITEM_WARPS,  \
+                                     as_stream(stream)>>>(                                       \
                 nitems, reinterpret_cast<const int4 *>(items), level_rscales, source_box_lists, \
                 centers, center_stride, src_expansions_f32, targets, target_stride, scale,      \
                 result),                                                                         \
-            check_launch("m2p_items_kernel")))
+            check_launch("m2p_items_x2_kernel")))
     SUMPY_ORDER_SWITCH(order, CALL_M2PI)
 #undef CALL_M2PI
 }
