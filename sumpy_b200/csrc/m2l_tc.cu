@@ -204,6 +204,7 @@ struct TcArgs {
     const void *src_hi, *src_lo;       // operand planes (fp32 for tf32, f16 for f16)
     const float *src_rinv, *mat_rinv;  // f16 form: 2^-e of each source row / operator row
     int32_t rows_pad;
+    int32_t a_rows;             // operator rows per TMA box: n when it fits one block of 128
     int32_t src_row_base, zero_row;
     int32_t tbase;
     double *tgt;
@@ -375,7 +376,7 @@ m2l_tc_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
             const int k0 = (kcb + kc) * KC;
             const uint32_t st = base + s * STAGE;
             if (lane == 0) {
-                mbar_expect_tx(full_bar + 8 * s, 4 * PLANE);
+                mbar_expect_tx(full_bar + 8 * s, 2 * a.a_rows * ROWB + 2 * PLANE);
                 tma_load_3d(st, &map_a_hi, k0, row0, cls_cur, full_bar + 8 * s);
                 tma_load_3d(st + PLANE, &map_a_lo, k0, row0, cls_cur, full_bar + 8 * s);
             }
@@ -436,14 +437,16 @@ m2l_tc_kernel(TcArgs a, const __grid_constant__ CUtensorMap map_a_hi,
             const int k0 = (kcb + kc) * KC;
             const uint32_t st = base + s * STAGE;
             if (threadIdx.x == 0) {
-                mbar_expect_tx(full_bar + 8 * s, 2 * PLANE);
+                mbar_expect_tx(full_bar + 8 * s, 2 * a.a_rows * ROWB);
                 tma_load_3d(st, &map_a_hi, k0, row0, cls_cur, full_bar + 8 * s);
                 tma_load_3d(st + PLANE, &map_a_lo, k0, row0, cls_cur, full_bar + 8 * s);
             }
 #pragma unroll
             for (int u = 0; u < NU; ++u) {
                 const int c = threadIdx.x + u * TC_LOADERS;
-                if (c < TC_TW * CPR) {
+                // f16 form: an empty slot's rows are not written at all (the
+                // drain skips its columns, whose source scale is zero)
+                if (c < TC_TW * CPR && (!F16 || sb_cur[u] >= 0)) {
                     const int slot = c / CPR, q = c % CPR;
                     const int32_t sb = sb_cur[u];
                     // the swizzle: 16-byte chunk q of a row XOR address bits 7.. of the row
@@ -794,8 +797,12 @@ static int m2l_tc_launch(
     CUtensorMap ma_hi, ma_lo, mb_hi, mb_lo;
     const uint64_t adims[3] = {(uint64_t)k_pad, (uint64_t)rows_pad, (uint64_t)nclasses};
     const uint64_t bdims[2] = {(uint64_t)k_pad, (uint64_t)src_nrows};
-    if (!make_map(&ma_hi, mats_hi, f16, 3, adims, TC_M) ||
-        !make_map(&ma_lo, mats_lo, f16, 3, adims, TC_M) ||
+    // one 128-row block of operator rows: the TMA box stops at the last real
+    // row (the MMA's rows past it hold stale shared memory and are never
+    // stored); several blocks: whole 128-row boxes of the zero-padded planes
+    const int32_t a_rows = rows_pad == TC_M ? n : TC_M;
+    if (!make_map(&ma_hi, mats_hi, f16, 3, adims, (uint32_t)a_rows) ||
+        !make_map(&ma_lo, mats_lo, f16, 3, adims, (uint32_t)a_rows) ||
         !make_map(&mb_hi, src_hi, f16, 2, bdims, 1) || !make_map(&mb_lo, src_lo, f16, 2, bdims, 1)) {
         set_last_error(std::string(who) + ": tensor map encoding failed");
         return SUMPY_EINVAL;
@@ -806,7 +813,7 @@ static int m2l_tc_launch(
     a.tile_targets = tile_targets; a.tile_scale = tile_scale;
     a.group_class = group_class; a.group_sources = group_sources;
     a.src_hi = src_hi; a.src_lo = src_lo;
-    a.src_rinv = src_rinv; a.mat_rinv = mats_rinv; a.rows_pad = rows_pad;
+    a.src_rinv = src_rinv; a.mat_rinv = mats_rinv; a.rows_pad = rows_pad; a.a_rows = a_rows;
     a.src_row_base = src_base_ibox; a.zero_row = src_nrows - 1;
     a.tbase = tgt_base_ibox; a.tgt = tgt_expansions; a.status = status;
     a.wait_cycles = wait_cycles_budget();
