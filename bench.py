@@ -1427,7 +1427,7 @@ def stage_breakdown(w, trav, q_dev, dev, roofline=True, pipe_peaks=None):
         # workload, one ncu capture per leaf size and operand format
         # (profiles/m2l_tc_f16_sphere_plummer_1M_p10.md, and for TF32
         # profiles/m2l_tf32x3_sphere_plummer_1M_p10.md)
-        captured = ({96: 118.07e6 + 21.16e6} if w.tc_format == "f16"
+        captured = ({96: 116.11e6 + 18.85e6} if w.tc_format == "f16"
                     else {32: 1.227e9 + 0.195e9, 96: 256.6e6 + 38.4e6})
         if mixed and tree.nsources == NPOINTS and n == (ORDER + 1) ** 2 and \
                 MAX_PARTICLES in captured and \
