@@ -219,6 +219,38 @@ __device__ __forceinline__ void p2p_batch_packed(const float4 *__restrict__ P0,
     acc += a2.x + a2.y;
 }
 
+// The same for a target shared by nph lanes (nph = 32 / targets in the pass,
+// boxes of at most 16 targets): the lane of phase ph takes the staged source
+// pairs ph, ph + nph, ... (every pair in exactly one phase), two sources per
+// instruction like p2p_batch_packed; padding sources are far away with
+// q = 0.
+__device__ __forceinline__ void p2p_batch_packed_phased(const float4 *__restrict__ P0,
+                                                        const float4 *__restrict__ P1,
+                                                        const float4 *__restrict__ P2,
+                                                        const float4 *__restrict__ P3,
+                                                        const P2PTarget &t, int ph, int nph,
+                                                        float &acc)
+{
+    const float2 txh = make_float2(t.xh, t.xh), txl = make_float2(t.xl, t.xl);
+    const float2 tyh = make_float2(t.yh, t.yh), tyl = make_float2(t.yl, t.yl);
+    const float2 tzh = make_float2(t.zh, t.zh), tzl = make_float2(t.zl, t.zl);
+    float2 a2 = make_float2(0.f, 0.f);
+#pragma unroll 4
+    for (int m = ph; m < 16; m += nph) {
+        const float4 p0 = P0[m], p1 = P1[m], p2 = P2[m], p3 = P3[m];
+        const float2 dx = __fadd2_rn(__fadd2_rn(txh, make_float2(p0.x, p0.y)),
+                                     __fadd2_rn(txl, make_float2(p2.x, p2.y)));
+        const float2 dy = __fadd2_rn(__fadd2_rn(tyh, make_float2(p0.z, p0.w)),
+                                     __fadd2_rn(tyl, make_float2(p2.z, p2.w)));
+        const float2 dz = __fadd2_rn(__fadd2_rn(tzh, make_float2(p1.x, p1.y)),
+                                     __fadd2_rn(tzl, make_float2(p3.x, p3.y)));
+        const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+        const float2 ri = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+        a2 = __ffma2_rn(make_float2(p1.z, p1.w), ri, a2);
+    }
+    acc += a2.x + a2.y;
+}
+
 // The same for two targets per lane: each source pair is read from shared
 // memory once and used for both targets (half the shared loads per pair).
 __device__ __forceinline__ void p2p_batch_packed2(const float4 *__restrict__ P0,
@@ -434,8 +466,15 @@ p2p_flat_mixed_kernel(int32_t ntgt_boxes, const int32_t *__restrict__ target_box
                                              spk[warp][slot][2], spk[warp][slot][3], tg, a);
                         }
                     } else {
-                        if (check) p2p_batch<true, GRAD, 0>(H, L, tg, ph, nph, jself, a, ax, ay, az);
-                        else p2p_batch<false, GRAD, 0>(H, L, tg, ph, nph, jself, a, ax, ay, az);
+                        if (check) {
+                            p2p_batch<true, GRAD, 0>(H, L, tg, ph, nph, jself, a, ax, ay, az);
+                        } else if constexpr (GRAD) {
+                            p2p_batch<false, GRAD, 0>(H, L, tg, ph, nph, jself, a, ax, ay, az);
+                        } else {
+                            p2p_batch_packed_phased(spk[warp][slot][0], spk[warp][slot][1],
+                                                    spk[warp][slot][2], spk[warp][slot][3], tg,
+                                                    ph, nph, a);
+                        }
                     }
                     acc += (double)a;
                     if (GRAD) { gx += (double)ax; gy += (double)ay; gz += (double)az; }
