@@ -48,8 +48,8 @@ _d = _capi.dbl
 
 M2L_TILE = 64          # FP64 GEMM tile (target boxes)
 M2L_TILE_TC = 128      # tensor-core tile (MMA N)
-M2L_ITEM_GROUPS = 64   # class groups per tensor-core work item (one CTA)
-ITEM_ROUNDS = 4        # rounds (one source box / 32 sources each) per mixed M2P / P2L item
+M2L_ITEM_GROUPS = 96   # class groups per tensor-core work item (one CTA)
+ITEM_ROUNDS = 16       # rounds (one source box / 32 sources each) per mixed M2P / P2L item
 M2P_ITEM_GROUPS = 8    # lane groups per warp in the M2P item kernel (fixed by the kernel)
 L2P_ITEM_SLOTS = 4     # boxes per packed L2P item (fixed by the kernel)
 HL2P_ITEM_SLOTS = 4    # the same for the Helmholtz packed L2P
@@ -352,7 +352,7 @@ class SumpyExpansionWrangler:
         self.item_rounds = ITEM_ROUNDS
         # the octant (M2M / L2L) GEMMs of a level are cut into enough items
         # and K parts to cover the SMs this many times
-        self.octant_split = 2
+        self.octant_split = 1
 
     SCHEDULE_KNOBS = ("m2l_item_groups", "item_rounds", "octant_split", "chain_levels",
                       "concurrent_stages")
