@@ -127,7 +127,7 @@ def tune_m2l_item_groups(wrangler, run, candidates=(16, 32, 64, 128), path=None,
 
 
 SCHEDULE_SPACE = {
-    "m2l_item_groups": (32, 64, 96, 128),
+    "m2l_item_groups": (64, 96, 128, 192),
     "item_rounds": (4, 8, 16, 32),
     "octant_split": (1, 2, 4),
     "chain_levels": (False, True),

@@ -48,7 +48,7 @@ _d = _capi.dbl
 
 M2L_TILE = 64          # FP64 GEMM tile (target boxes)
 M2L_TILE_TC = 128      # tensor-core tile (MMA N)
-M2L_ITEM_GROUPS = 96   # class groups per tensor-core work item (one CTA)
+M2L_ITEM_GROUPS = 192  # class groups per tensor-core work item (one CTA)
 ITEM_ROUNDS = 16       # rounds (one source box / 32 sources each) per mixed M2P / P2L item
 M2P_ITEM_GROUPS = 8    # lane groups per warp in the M2P item kernel (fixed by the kernel)
 L2P_ITEM_SLOTS = 4     # boxes per packed L2P item (fixed by the kernel)
